@@ -1,0 +1,1147 @@
+/*
+ * cirsradg_oracle.cpp -- ORACLE (test infrastructure only; see oracle.h).
+ *
+ * Line-by-line CPU restatement of the reference's correlated-k gradient
+ * forward model.  Each function names the Fortran file:line it follows
+ * (paths relative to the reference repository root).  Written in templated
+ * C++: R = float reproduces the reference's REAL arithmetic (DOUBLE
+ * PRECISION variables stay double), R = double promotes everything.
+ *
+ * Build with -ffp-contract=off so that no multiply-add is fused: gfortran
+ * -O2 on x86-64 evaluates every REAL expression as separate IEEE operations
+ * left to right, and this file spells each expression in that order.
+ */
+#include "oracle.h"
+#include "detexp.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr int kMaxG = RTB_MAXG;
+/* 0: the reference heapsort (default).  1: stable sort by key, ties in
+ * element order -- used by the oracle tests to show which passes depend on
+ * the heapsort's order of tied keys. */
+int g_sort_mode = 0;
+
+template <class R> struct Prec;
+template <> struct Prec<float> {
+    static float EXP(float x) { return orc_det_expf(x); }
+    static float LOG(float x) { return (float)std::log((double)x); }
+    static bool isnan_(float x) { return x != x; }
+};
+template <> struct Prec<double> {
+    static double EXP(double x) { return std::exp(x); }
+    static double LOG(double x) { return std::log(x); }
+    static bool isnan_(double x) { return x != x; }
+};
+
+/* LOCATE: radtran/scatter/locate.f:1-28 (the copy linked into cirsradg;
+ * scatter.a precedes libfrecipes.a on the link line). 1-based result. */
+template <class R>
+int locate(const R* xx, int n, R x) {
+    int jl = 0, ju = n + 1;
+    while (ju - jl > 1) {
+        int jm = (ju + jl) / 2;
+        if ((xx[n - 1] >= xx[0]) == (x >= xx[jm - 1])) jl = jm; else ju = jm;
+    }
+    if (x == xx[0]) return 1;
+    if (x == xx[n - 1]) return n - 1;
+    return jl;
+}
+
+/* SORT2G: radtran/cirsradg/sort2g.f:1-52, Numerical Recipes heapsort that
+ * carries an integer index.  ra/ib are 0-based storage of RA(1..N)/IB(1..N).
+ * N < 2 is not reached by the reference path (NG >= 2 checked by caller). */
+template <class R>
+void sort2g(int n, R* ra0, int* ib0) {
+    if (n < 2) return;
+    R* RA = ra0 - 1;
+    int* IB = ib0 - 1;
+    int L = n / 2 + 1, IR = n;
+    R RRA;
+    int IRB;
+    for (;;) {
+        if (L > 1) {
+            L = L - 1;
+            RRA = RA[L];
+            IRB = IB[L];
+        } else {
+            RRA = RA[IR];
+            IRB = IB[IR];
+            RA[IR] = RA[1];
+            IB[IR] = IB[1];
+            IR = IR - 1;
+            if (IR == 1) {
+                RA[1] = RRA;
+                IB[1] = IRB;
+                return;
+            }
+        }
+        int I = L, J = L + L;
+        while (J <= IR) {
+            if (J < IR) {
+                if (RA[J] < RA[J + 1]) J = J + 1;
+            }
+            if (RRA < RA[J]) {
+                RA[I] = RA[J];
+                IB[I] = IB[J];
+                I = J;
+                J = J + J;
+            } else {
+                J = IR + 1;
+            }
+        }
+        RA[I] = RRA;
+        IB[I] = IRB;
+    }
+}
+
+/* RANKG: radtran/cirsradg/rankg.f:59-152.  grad is [nparam][nloop]
+ * (column iparam of grad(maxrank, maxgas+1)); dkdq is [nparam][ng].
+ * Cumulative g (g_ord, gdist), sum and frac are DOUBLE PRECISION.
+ * perm/split: optional debug capture of the assignment. */
+template <class R>
+int rankg(int nparam, const R* gw, int ng, int nloop, R* weight, R* cont, R* grad,
+          R* k_g, R* dkdq, int16_t* perm, int16_t* split, int16_t* ties = nullptr) {
+    double g_ord[kMaxG + 2];
+    g_ord[0] = 0.0;
+    for (int i = 0; i < ng; ++i) g_ord[i + 1] = g_ord[i] + (double)gw[i];
+    if (g_ord[ng] < 1.0) g_ord[ng] = 1.0;                 /* rankg.f:65-67 */
+
+    std::vector<int> ico(nloop);
+    for (int i = 0; i < nloop; ++i) ico[i] = i + 1;
+    if (g_sort_mode == 0) {
+        sort2g<R>(nloop, cont, ico.data());
+    } else {
+        std::stable_sort(ico.begin(), ico.end(), [&](int a, int b) { return cont[a - 1] < cont[b - 1]; });
+        std::vector<R> c2(nloop);
+        for (int i = 0; i < nloop; ++i) c2[i] = cont[ico[i] - 1];
+        for (int i = 0; i < nloop; ++i) cont[i] = c2[i];
+    }
+
+    std::vector<R> tmp(nloop);
+    for (int i = 0; i < nloop; ++i) tmp[i] = weight[ico[i] - 1];
+    for (int i = 0; i < nloop; ++i) weight[i] = tmp[i];
+    for (int p = 0; p < nparam; ++p) {
+        R* g = grad + (size_t)p * nloop;
+        for (int i = 0; i < nloop; ++i) tmp[i] = g[ico[i] - 1];
+        for (int i = 0; i < nloop; ++i) g[i] = tmp[i];
+    }
+    if (perm) for (int i = 0; i < nloop; ++i) perm[i] = (int16_t)(ico[i] - 1);
+    if (ties) {
+        int n = 0;
+        for (int i = 1; i < nloop; ++i) n += (cont[i] == cont[i - 1]);
+        *ties = (int16_t)n;
+    }
+    if (split) for (int b = 0; b < ng; ++b) split[b] = -1;
+
+    std::vector<double> gdist(nloop + 1);
+    gdist[0] = 0.0;
+    gdist[1] = (double)weight[0];
+    for (int i = 2; i <= nloop; ++i) gdist[i] = (double)weight[i - 1] + gdist[i - 1];
+
+    for (int i = 0; i < ng; ++i) {
+        k_g[i] = 0;
+        for (int p = 0; p < nparam; ++p) dkdq[(size_t)p * ng + i] = 0;
+    }
+    int ig = 1;
+    double sum = 0.0;
+    for (int I = 1; I <= nloop; ++I) {
+        const R c = cont[I - 1], w = weight[I - 1];
+        if (ig > ng) return RTB_ERR_GORD;  /* reference reads g_ord(ng+2): undefined */
+        if (gdist[I] < g_ord[ig]) {
+            k_g[ig - 1] = k_g[ig - 1] + c * w;
+            for (int p = 0; p < nparam; ++p)
+                dkdq[(size_t)p * ng + ig - 1] =
+                    dkdq[(size_t)p * ng + ig - 1] + grad[(size_t)p * nloop + I - 1] * w;
+            sum = sum + (double)w;
+        } else {
+            const double frac = (g_ord[ig] - gdist[I - 1]) / (gdist[I] - gdist[I - 1]);
+            const R sf = (R)frac;
+            k_g[ig - 1] = k_g[ig - 1] + sf * c * w;
+            for (int p = 0; p < nparam; ++p)
+                dkdq[(size_t)p * ng + ig - 1] =
+                    dkdq[(size_t)p * ng + ig - 1] + sf * grad[(size_t)p * nloop + I - 1] * w;
+            sum = sum + frac * (double)w;
+            k_g[ig - 1] = k_g[ig - 1] / (R)sum;
+            for (int p = 0; p < nparam; ++p)
+                dkdq[(size_t)p * ng + ig - 1] = dkdq[(size_t)p * ng + ig - 1] / (R)sum;
+            if (split) split[ig - 1] = (int16_t)(I - 1);
+            ig = ig + 1;
+            sum = (1.0 - frac) * (double)w;
+            if (ig <= ng) {  /* the reference writes k_g(ng+1) of a MAXG array: unused */
+                const R sr = (R)(1.0 - frac);
+                k_g[ig - 1] = sr * c * w;
+                for (int p = 0; p < nparam; ++p)
+                    dkdq[(size_t)p * ng + ig - 1] = sr * grad[(size_t)p * nloop + I - 1] * w;
+            }
+        }
+    }
+    if (ig == ng) {
+        k_g[ig - 1] = k_g[ig - 1] / (R)sum;
+        for (int p = 0; p < nparam; ++p)
+            dkdq[(size_t)p * ng + ig - 1] = dkdq[(size_t)p * ng + ig - 1] / (R)sum;
+    }
+    return RTB_OK;
+}
+
+/* RANKK: radtran/cirsradg/rankk.f:34-117 -- REAL g_ord/gdist/sum/frac,
+ * `<=` test and the ig <= ng guards.  Used by the non-coincident branch of
+ * get_kg (get_kg.f:380-438). */
+template <class R>
+void rankk(const R* gw, int ng, R* cont, R* dcont, R* weight, int nloop, R* k_g, R* dkdt) {
+    R g_ord[kMaxG + 2];
+    g_ord[0] = 0;
+    for (int i = 0; i < ng; ++i) g_ord[i + 1] = g_ord[i] + gw[i];
+    if (g_ord[ng] < (R)1.0) g_ord[ng] = (R)1.0;
+    std::vector<int> ico(nloop);
+    for (int i = 0; i < nloop; ++i) ico[i] = i + 1;
+    sort2g<R>(nloop, cont, ico.data());
+    std::vector<R> tmp(nloop);
+    for (int i = 0; i < nloop; ++i) tmp[i] = weight[ico[i] - 1];
+    for (int i = 0; i < nloop; ++i) weight[i] = tmp[i];
+    for (int i = 0; i < nloop; ++i) tmp[i] = dcont[ico[i] - 1];
+    for (int i = 0; i < nloop; ++i) dcont[i] = tmp[i];
+    std::vector<R> gdist(nloop + 1);
+    gdist[0] = 0;
+    gdist[1] = weight[0];
+    for (int i = 2; i <= nloop; ++i) gdist[i] = weight[i - 1] + gdist[i - 1];
+    for (int i = 0; i < ng; ++i) { k_g[i] = 0; dkdt[i] = 0; }
+    int ig = 1;
+    R sum = 0;
+    for (int I = 1; I <= nloop; ++I) {
+        if (ig <= ng && gdist[I] <= g_ord[ig]) {
+            k_g[ig - 1] = k_g[ig - 1] + cont[I - 1] * weight[I - 1];
+            dkdt[ig - 1] = dkdt[ig - 1] + dcont[I - 1] * weight[I - 1];
+            sum = sum + weight[I - 1];
+        } else {
+            /* with ig > ng the reference reads g_ord(ng+2) and writes
+             * k_g(ng+1); those slots are never used afterwards */
+            if (ig > ng) continue;
+            const R frac = (g_ord[ig] - gdist[I - 1]) / (gdist[I] - gdist[I - 1]);
+            k_g[ig - 1] = k_g[ig - 1] + frac * cont[I - 1] * weight[I - 1];
+            dkdt[ig - 1] = dkdt[ig - 1] + frac * dcont[I - 1] * weight[I - 1];
+            sum = sum + frac * weight[I - 1];
+            k_g[ig - 1] = k_g[ig - 1] / sum;
+            dkdt[ig - 1] = dkdt[ig - 1] / sum;
+            ig = ig + 1;
+            if (ig <= ng) {
+                sum = ((R)1.0 - frac) * weight[I - 1];
+                k_g[ig - 1] = ((R)1.0 - frac) * cont[I - 1] * weight[I - 1];
+                dkdt[ig - 1] = ((R)1.0 - frac) * dcont[I - 1] * weight[I - 1];
+            }
+        }
+    }
+    if (ig == ng) {
+        k_g[ig - 1] = k_g[ig - 1] / sum;
+        dkdt[ig - 1] = dkdt[ig - 1] / sum;
+    }
+}
+
+/* NOVERLAPG: radtran/cirsradg/noverlapg.f:64-198.
+ * k_gn/dkgndt: [ngas][ng]; amount[ngas]; outputs k_g[ng], dkdq[ngas+1][ng]
+ * (column-major dkdq(maxg, maxgas+1) restricted to its first ngas+1 columns).
+ * dbg_perm/dbg_split: per pass (igas-1) records, may be NULL. */
+template <class R>
+int noverlapg(const R* delg, int ng, int ngas, const R* amount, const R* k_gn, const R* dkgndt,
+              R* k_g, R* dkdq, int16_t* dbg_perm, int16_t* dbg_split, int16_t* dbg_ties) {
+    const int nrank = ng * ng;
+    std::vector<R> contri(nrank), weight(nrank), grad((size_t)(ngas + 1) * nrank);
+    R k_g1[kMaxG], k_g2[kMaxG], dk1dT[kMaxG], dk2dT[kMaxG];
+    auto DK = [&](int i, int col) -> R& { return dkdq[(size_t)col * ng + i]; }; /* col 0-based */
+    for (int igas = 1; igas <= ngas - 1; ++igas) {
+        int16_t* pperm = dbg_perm ? dbg_perm + (size_t)(igas - 1) * nrank : nullptr;
+        int16_t* psplit = dbg_split ? dbg_split + (size_t)(igas - 1) * ng : nullptr;
+        if (pperm) for (int i = 0; i < nrank; ++i) pperm[i] = -1;
+        if (psplit) for (int i = 0; i < ng; ++i) psplit[i] = -1;
+        int16_t* pties = dbg_ties ? dbg_ties + (igas - 1) : nullptr;
+        if (pties) *pties = -1;
+        int nloop = 0;
+        if (igas == 1) {
+            const R a1 = amount[igas - 1], a2 = amount[igas];
+            for (int i = 0; i < ng; ++i) {
+                k_g1[i] = k_gn[(size_t)(igas - 1) * ng + i];
+                k_g2[i] = k_gn[(size_t)igas * ng + i];
+                dk1dT[i] = dkgndt[(size_t)(igas - 1) * ng + i];
+                dk2dT[i] = dkgndt[(size_t)igas * ng + i];
+            }
+            if (k_g1[ng - 1] == 0) {                          /* noverlapg.f:88-97 */
+                for (int i = 0; i < ng; ++i) {
+                    k_g[i] = k_g2[i] * a2;
+                    DK(i, igas - 1) = 0;
+                    DK(i, igas) = k_g2[i];
+                    DK(i, igas + 1) = dk2dT[i] * a2;
+                }
+                continue;
+            }
+            if (k_g2[ng - 1] == 0) {                          /* noverlapg.f:99-108 */
+                for (int i = 0; i < ng; ++i) {
+                    k_g[i] = k_g1[i] * a1;
+                    DK(i, igas - 1) = k_g1[i];
+                    DK(i, igas) = 0;
+                    DK(i, igas + 1) = dk1dT[i] * a1;
+                }
+                continue;
+            }
+            for (int i = 0; i < ng; ++i)
+                for (int j = 0; j < ng; ++j) {
+                    weight[nloop] = delg[i] * delg[j];
+                    contri[nloop] = k_g1[i] * a1 + k_g2[j] * a2;
+                    grad[(size_t)(igas - 1) * nrank + nloop] = k_g1[i];
+                    grad[(size_t)igas * nrank + nloop] = k_g2[j];
+                    grad[(size_t)(igas + 1) * nrank + nloop] = dk1dT[i] * a1 + dk2dT[j] * a2;
+                    ++nloop;
+                }
+        } else {
+            const R a2 = amount[igas];
+            for (int i = 0; i < ng; ++i) {
+                k_g1[i] = k_g[i];
+                k_g2[i] = k_gn[(size_t)igas * ng + i];
+                dk1dT[i] = DK(i, igas);           /* dkdq(i, igas+1): dK/dT of the sum */
+                dk2dT[i] = dkgndt[(size_t)igas * ng + i];
+            }
+            if (k_g1[ng - 1] == 0) {                          /* noverlapg.f:152-162 */
+                for (int i = 0; i < ng; ++i) {
+                    k_g[i] = k_g2[i] * a2;
+                    for (int jg = 1; jg <= igas; ++jg) DK(i, jg - 1) = 0;
+                    DK(i, igas) = k_g2[i];
+                    DK(i, igas + 1) = dk2dT[i] * a2;
+                }
+                continue;
+            }
+            if (k_g2[ng - 1] == 0) {                          /* noverlapg.f:164-173 */
+                for (int i = 0; i < ng; ++i) {
+                    k_g[i] = k_g1[i];
+                    DK(i, igas) = 0;
+                    DK(i, igas + 1) = dk1dT[i];
+                }
+                continue;
+            }
+            for (int i = 0; i < ng; ++i)
+                for (int j = 0; j < ng; ++j) {
+                    weight[nloop] = delg[i] * delg[j];
+                    contri[nloop] = k_g1[i] + k_g2[j] * a2;
+                    for (int jg = 1; jg <= igas; ++jg)
+                        grad[(size_t)(jg - 1) * nrank + nloop] = DK(i, jg - 1);
+                    grad[(size_t)igas * nrank + nloop] = k_g2[j];
+                    grad[(size_t)(igas + 1) * nrank + nloop] = dk1dT[i] + dk2dT[j] * a2;
+                    ++nloop;
+                }
+        }
+        int st = rankg<R>(igas + 2, delg, ng, nloop, weight.data(), contri.data(), grad.data(),
+                          k_g, dkdq, pperm, psplit, pties);
+        if (st) return st;
+    }
+    return RTB_OK;
+}
+
+/* Per-layer position in the k-table grid: get_kg.f:117-141 (NT > 0). */
+template <class R>
+struct LayerK {
+    int ioff[4];
+    R u, v, dudt;
+};
+
+template <class R>
+void layer_prep(const orc_tables& t, const R* p, const R* tt, float press, float temp, LayerK<R>& L) {
+    const int np = t.np, nt = t.nt, ng = t.ng;
+    const R pmax = p[np - 1], pmin = p[0], tmax = tt[nt - 1], tmin = tt[0];
+    R P1 = Prec<R>::LOG((R)press);
+    if (P1 < pmin) P1 = pmin;
+    if (P1 > pmax) P1 = pmax;
+    int cp = locate<R>(p, np, P1);
+    if (cp < 1) cp = 1;
+    if (cp >= np) cp = np - 1;
+    L.v = (P1 - p[cp - 1]) / (p[cp] - p[cp - 1]);
+    R T1 = (R)temp;
+    if (T1 < tmin) T1 = tmin;
+    if (T1 > tmax) T1 = tmax;
+    int ct = locate<R>(tt, nt, T1);
+    if (ct < 1) ct = 1;
+    if (ct >= nt) ct = nt - 1;
+    L.u = (T1 - tt[ct - 1]) / (tt[ct] - tt[ct - 1]);
+    L.dudt = (R)1.0 / (tt[ct] - tt[ct - 1]);
+    L.ioff[0] = (nt * ng * (cp - 1)) + (ng * (ct - 1));
+    L.ioff[1] = (nt * ng * cp) + (ng * (ct - 1));
+    L.ioff[2] = (nt * ng * cp) + (ng * ct);
+    L.ioff[3] = (nt * ng * (cp - 1)) + (ng * ct);
+}
+
+/* Table record selection of get_kg.f:189-275 for one (wavenumber, table).
+ * Shared by both precisions (the choice is discrete).  Returns the 0-based
+ * bin n1 and whether the wavenumber is coincident; weight2 for the
+ * non-coincident branch. */
+struct BinSel {
+    int n1;
+    bool coinc;
+    float w2;
+    bool zero;  /* KTEST == 0: all-zero slice (get_kg.f:228-250) */
+};
+
+int select_bin(const orc_tables& t, int itab, float vwave, BinSel& b) {
+    const float vmin = t.vmin[itab], delv = t.delv[itab];
+    if (!(delv > 0.0f)) return RTB_ERR_UNSUPPORTED;  /* irregular tables: not implemented */
+    float eps;
+    if (delv >= 0.0001f) eps = 0.02f * delv; else eps = 0.25f * delv;
+    const int n1 = (int)(((double)vwave + (double)eps - (double)vmin) / (double)delv);
+    const float tmp = vmin + delv * (float)n1;
+    const float frac = std::fabs((float)((double)vwave - (double)tmp));
+    b.n1 = n1;
+    b.coinc = frac < eps;
+    float w2 = (vwave - tmp) / delv;
+    if (w2 > 1.0f) w2 = 1.0f;
+    if (w2 < 0.0f) w2 = 0.0f;
+    b.w2 = w2;
+    const int need = b.coinc ? n1 : n1 + 1;
+    if (n1 < 0 || need >= t.nbin[itab]) return RTB_ERR_RANGE;
+    /* zero probe over the slice at n1 */
+    size_t off = 0;
+    for (int k = 0; k < itab; ++k) off += (size_t)t.nbin[k] * t.np * t.nt * t.ng;
+    const size_t ntab = (size_t)t.np * t.nt * t.ng;
+    const float* s = t.data + off + (size_t)n1 * ntab;
+    bool any = false;
+    for (size_t i = 0; i < ntab; ++i) if (s[i] > 0.0f) { any = true; break; }
+    b.zero = !any;
+    return RTB_OK;
+}
+
+const float* table_slice(const orc_tables& t, int itab, int n1) {
+    size_t off = 0;
+    for (int k = 0; k < itab; ++k) off += (size_t)t.nbin[k] * t.np * t.nt * t.ng;
+    return t.data + off + (size_t)n1 * t.np * t.nt * t.ng;
+}
+
+/* GET_KG interpolation for one layer of one gas: get_kg.f:306-471. */
+template <class R>
+void get_kg_layer(const orc_tables& t, const BinSel& b, const float* tab1, const float* tab2,
+                  const LayerK<R>& L, const R* delg, R* kout, R* dkout) {
+    const int ng = t.ng;
+    R k_g[kMaxG], dkdt[kMaxG];
+    const R U = L.u, V = L.v, DUDT = L.dudt;
+    const int I1 = L.ioff[0], I2 = L.ioff[1], I3 = L.ioff[2], I4 = L.ioff[3];
+    if (b.coinc) {
+        R Y1 = tab1[I1], Y2 = tab1[I2], Y3 = tab1[I3], Y4 = tab1[I4];
+        bool KLOG = !((Y1 <= 0) || (Y2 <= 0) || (Y3 <= 0) || (Y4 <= 0));
+        for (int i = 0; i < ng; ++i) {
+            Y1 = tab1[I1 + i]; Y2 = tab1[I2 + i]; Y3 = tab1[I3 + i]; Y4 = tab1[I4 + i];
+            if (KLOG) {
+                Y1 = Prec<R>::LOG(Y1); Y2 = Prec<R>::LOG(Y2);
+                Y3 = Prec<R>::LOG(Y3); Y4 = Prec<R>::LOG(Y4);
+            }
+            const R a = (R)1.0 - V, bb = (R)1.0 - U;
+            const R X = a * bb * Y1 + V * bb * Y2 + V * U * Y3 + a * U * Y4;
+            const R DXDT = (-(a * Y1) - V * Y2 + V * Y3 + a * Y4) * DUDT;
+            if (KLOG) {
+                k_g[i] = Prec<R>::EXP(X);
+                dkdt[i] = Prec<R>::EXP(X) * DXDT;
+            } else {
+                k_g[i] = X;
+                dkdt[i] = DXDT;
+            }
+        }
+    } else {
+        const R w[2] = {(R)1.0f - (R)b.w2, (R)b.w2};
+        R cont[2 * kMaxG], dcont[2 * kMaxG], fac[2 * kMaxG];
+        int count = 0;
+        for (int loop = 0; loop < 2; ++loop) {
+            const float* tb = loop == 0 ? tab1 : tab2;
+            for (int i = 0; i < ng; ++i) {
+                const R Y1 = tb[I1 + i], Y2 = tb[I2 + i], Y3 = tb[I3 + i], Y4 = tb[I4 + i];
+                const R a = (R)1.0 - V, bb = (R)1.0 - U;
+                const R X = a * bb * Y1 + V * bb * Y2 + V * U * Y3 + a * U * Y4;
+                const R DXDT = (-(a * Y1) - V * Y2 + V * Y3 + a * Y4) * DUDT;
+                cont[count] = X;
+                dcont[count] = DXDT;
+                fac[count] = delg[i] * w[loop];
+                ++count;
+            }
+        }
+        rankk<R>(delg, ng, cont, dcont, fac, count, k_g, dkdt);
+    }
+    for (int i = 0; i < ng; ++i) {                               /* get_kg.f:443-471 */
+        kout[i] = Prec<R>::isnan_(k_g[i]) ? (R)1e-37f : k_g[i];
+        dkout[i] = Prec<R>::isnan_(dkdt[i]) ? (R)1e-37f : dkdt[i];
+    }
+}
+
+/* PINDEX: radtran/radtran/read_ktable.f:201-226 (clamps x1 in place). */
+template <class R>
+int pindex(const R* x, int nx, R& x1) {
+    if (x1 > x[nx - 1]) x1 = x[nx - 1];
+    if (x1 < x[0]) x1 = x[0];
+    int j = 0;
+    for (int i = 1; i <= nx - 1; ++i) {
+        if (x1 >= x[i - 1]) j = i; else break;
+    }
+    return j;
+}
+
+/* CIAREAD: radtran/radtran/ciaread.f:108-198.  alpha/dalpha[9]. */
+template <class R>
+void ciaread(const orc_tables& t, R vv, R temp, R* alpha, R* dalpha) {
+    const int NWN = RTB_CIA_NUMWN, NT = RTB_CIA_NUMT, NP = RTB_CIA_NUMPAIRS;
+    R vvk1_first = 0, vvk1_last = (R)((float)(NWN - 1) * t.dnu);
+    for (int i = 0; i < NP; ++i) { alpha[i] = 0; dalpha[i] = 0; }
+    if (vv > vvk1_last || vv < vvk1_first) return;
+    R tempk1[RTB_CIA_NUMT];
+    for (int i = 0; i < NT; ++i) tempk1[i] = (R)(float)t.cia_temps[i];
+    R temp1;
+    if (temp > tempk1[NT - 1]) temp1 = tempk1[NT - 1]; else temp1 = temp;
+    if (temp < tempk1[0]) temp1 = tempk1[0]; else temp1 = temp;     /* overwrites: ciaread.f:133-157 */
+    /* vvk1(i) = (i-1)*dnu1 as REAL; pindex on that grid */
+    std::vector<R> vvk1(NWN);
+    for (int i = 0; i < NWN; ++i) vvk1[i] = (R)((float)i * t.dnu);
+    R vvc = vv;
+    const int cv = pindex<R>(vvk1.data(), NWN, vvc);
+    const int ct = pindex<R>(tempk1, NT, temp1);
+    for (int i = 0; i < NP; ++i) {
+        const R abs11 = t.kcia[i + NP * (ct - 1) + NP * NT * (cv - 1)];
+        const R abs12 = t.kcia[i + NP * (ct - 1) + NP * NT * cv];
+        const R abs22 = t.kcia[i + NP * ct + NP * NT * cv];
+        const R abs21 = t.kcia[i + NP * ct + NP * NT * (cv - 1)];
+        const R tt = (vv - vvk1[cv - 1]) / (vvk1[cv] - vvk1[cv - 1]);
+        const R u = (temp1 - tempk1[ct - 1]) / (tempk1[ct] - tempk1[ct - 1]);
+        const R dudt = (R)1.0 / (tempk1[ct] - tempk1[ct - 1]);
+        alpha[i] = ((R)1.0 - tt) * ((R)1.0 - u) * abs11 + tt * ((R)1.0 - u) * abs12 +
+                   tt * u * abs22 + ((R)1.0 - tt) * u * abs21;
+        dalpha[i] = (-((R)1.0 - tt) * abs11 - tt * abs12 + tt * abs22 + ((R)1.0 - tt) * abs21) * dudt;
+    }
+}
+
+/* NCIACON: radtran/radtran/nciacon.f:84-310 (the three NIR add-ons co2cia,
+ * n2n2cia, n2h2cia are zero below 3900 cm-1; the caller rejects N2/CO2
+ * runs above that). iabs[5] are 1-based gas numbers (0 = absent). */
+template <class R>
+void nciacon(const orc_tables& t, R v0, R p, R temp, int inormal, int ngas, const int* idgas,
+             const int* isogas, const R* amount, const R* pp, R xlen, R& absorb, int* iabs,
+             R* dabsorb) {
+    R qh2 = 0, qhe = 0, qn2 = 0, qch4 = 0, qco2 = 0;
+    for (int i = 0; i < 5; ++i) { iabs[i] = 0; dabsorb[i] = 0; }
+    dabsorb[5] = 0; dabsorb[6] = 0;
+    for (int i = 0; i < ngas; ++i) {
+        const int id = idgas[i], iso = isogas[i];
+        if (id == 39 && (iso == 0 || iso == 1)) { qh2 = pp[i] / p; iabs[0] = i + 1; }
+        if (id == 40) { qhe = pp[i] / p; iabs[1] = i + 1; }
+        if (id == 22) { qn2 = pp[i] / p; iabs[2] = i + 1; }
+        if (id == 6 && (iso == 0 || iso == 1)) { qch4 = (pp[i] / p); iabs[3] = i + 1; }
+        if (id == 2) { qco2 = pp[i] / p; iabs[4] = i + 1; }
+    }
+    const R AMAGAT = (R)2.68675E19f;
+    const R MODBOLTZA = (R)(10.0f * 1.37947E-23f / 1.013f);
+    R tau;
+    if (xlen == 0) {
+        R XP1 = 0, height = 0;
+        for (int i = 0; i < ngas; ++i)
+            if (pp[i] > XP1) { height = amount[i] * MODBOLTZA * temp / pp[i]; XP1 = pp[i]; }
+        const R P0 = 1.0f, T0 = 273.15f;
+        const R a = p / P0, b = T0 / temp;
+        tau = (a * a) * (b * b) * height;
+    } else {
+        const R height = xlen * (R)1e5f;
+        R XP1 = -1, TOTAM = 0;
+        for (int i = 0; i < ngas; ++i)
+            if (pp[i] > XP1 && pp[i] > 0) { TOTAM = amount[i] * p / pp[i]; XP1 = pp[i]; }
+        const R amag1 = (TOTAM / height) / AMAGAT;
+        tau = height * (amag1 * amag1);
+    }
+    R alpha[9], da[9];
+    ciaread<R>(t, v0, temp, alpha, da);
+    R sum = 0;
+    if (inormal == 0) {
+        sum = sum + (alpha[0] * qh2 * qh2) + (alpha[1] * qh2 * qhe);
+        dabsorb[0] = dabsorb[0] + (R)2 * qh2 * alpha[0] + qhe * alpha[1];
+        dabsorb[1] = dabsorb[1] + qh2 * alpha[1];
+        dabsorb[5] = dabsorb[5] + qh2 * qh2 * da[0] + qh2 * qhe * da[1];
+    } else {
+        sum = sum + (alpha[2] * qh2 * qh2) + (alpha[3] * qh2 * qhe);
+        dabsorb[0] = dabsorb[0] + (R)2 * qh2 * alpha[2] + qhe * alpha[3];
+        dabsorb[1] = dabsorb[1] + qh2 * alpha[3];
+        dabsorb[5] = dabsorb[5] + qh2 * qh2 * da[2] + qh2 * qhe * da[3];
+    }
+    sum = sum + (alpha[4] * qh2 * qn2);
+    dabsorb[0] = dabsorb[0] + qn2 * alpha[4];
+    dabsorb[2] = dabsorb[2] + qh2 * alpha[4];
+    dabsorb[5] = dabsorb[5] + qh2 * qn2 * da[4];
+    sum = sum + (alpha[5] * qn2 * qch4);
+    dabsorb[2] = dabsorb[2] + qch4 * alpha[5];
+    dabsorb[3] = dabsorb[3] + qn2 * alpha[5];
+    dabsorb[5] = dabsorb[5] + qn2 * qch4 * da[5];
+    sum = sum + (alpha[6] * qn2 * qn2);
+    dabsorb[2] = dabsorb[2] + (R)2 * qn2 * alpha[6];
+    dabsorb[5] = dabsorb[5] + qn2 * qn2 * da[6];
+    sum = sum + (alpha[7] * qch4 * qch4);
+    dabsorb[3] = dabsorb[3] + (R)2 * qch4 * alpha[7];
+    dabsorb[5] = dabsorb[5] + qch4 * qch4 * da[7];
+    sum = sum + (alpha[8] * qh2 * qch4);
+    dabsorb[0] = dabsorb[0] + qch4 * alpha[8];
+    dabsorb[3] = dabsorb[3] + qh2 * alpha[8];
+    dabsorb[5] = dabsorb[5] + qh2 * qch4 * da[8];
+    /* co2cia / n2n2cia / n2h2cia: zero below 3900 cm-1 -> adding exact zeros */
+    const R z = 0;
+    sum = sum + z * qco2 * qco2;
+    dabsorb[4] = dabsorb[4] + (R)2 * qco2 * z;
+    sum = sum + z * qn2 * qn2;
+    dabsorb[2] = dabsorb[2] + (R)2 * qn2 * z;
+    sum = sum + z * qn2 * qh2;
+    dabsorb[2] = dabsorb[2] + qh2 * z;
+    dabsorb[0] = dabsorb[0] + qn2 * z;
+    absorb = sum * tau;
+    for (int i = 0; i < 7; ++i) dabsorb[i] = dabsorb[i] * tau;
+}
+
+/* PLANCK_WAVE / PLANCKG_WAVE: radtran/radtran/planck_wave.f:1-42,
+ * planckg_wave.f:1-40.  c1, c2 are REAL literals stored in DOUBLE
+ * parameters; integer powers of the REAL y follow gfortran's expansion. */
+const double kC1 = (double)1.1911e-12f, kC2 = (double)1.439f;
+
+template <class R> R planck_wave(int ispace, R v, R T);
+template <> float planck_wave<float>(int ispace, float v, float T) {
+    float y;
+    double a;
+    if (ispace == 0) { y = v; float y2 = y * y; a = kC1 * (double)(y2 * y); }
+    else { y = 1e4f / v; float y2 = y * y; float y4 = y2 * y2; a = kC1 * (double)(y4 * y) / 1e4; }
+    if (y == 0.0f) return 0.0f;
+    const double tmp = kC2 * (double)y / (double)T;
+    const double b = std::exp(tmp) - 1.;
+    return (float)(a / b);
+}
+template <> double planck_wave<double>(int ispace, double v, double T) {
+    double y, a;
+    if (ispace == 0) { y = v; a = kC1 * (y * y * y); }
+    else { y = 1e4 / v; a = kC1 * (y * y * y * y * y) / 1e4; }
+    if (y == 0.0) return 0.0;
+    return a / std::expm1(kC2 * y / T);
+}
+template <class R> R planckg_wave(int ispace, R v, R T);
+template <> float planckg_wave<float>(int ispace, float v, float T) {
+    float y;
+    double A;
+    const float T2 = T * T;
+    if (ispace == 0) { y = v; float y2 = y * y; A = kC1 * kC2 * (double)(y2 * y2) / (double)T2; }
+    else {
+        y = 1e4f / v; float y2 = y * y; float y3 = y2 * y;
+        A = kC1 * kC2 * (double)(y3 * y3) * (double)1e-4f / (double)T2;
+    }
+    const double tmp = kC2 * (double)y / (double)T;
+    const double e = std::exp(tmp);
+    const double bot = (e - 1.0) * (e - 1.0);
+    const double top = e * A;
+    return (float)(top / bot);
+}
+template <> double planckg_wave<double>(int ispace, double v, double T) {
+    double y, A;
+    if (ispace == 0) { y = v; A = kC1 * kC2 * (y * y * y * y) / (T * T); }
+    else { y = 1e4 / v; A = kC1 * kC2 * (y * y * y * y * y * y) * 1e-4 / (T * T); }
+    const double tmp = kC2 * y / T;
+    const double em1 = std::expm1(tmp);
+    return std::exp(tmp) * A / (em1 * em1);
+}
+
+/* DPEXP: radtran/radtran/dpexp.f */
+template <class R>
+R dpexp(R x) {
+    R y = std::max(x, (R)-500.0f);
+    if (y >= (R)88.7f) y = (R)88.7f;
+    return (R)std::exp((double)y);
+}
+
+/* INTERPEM: radtran/cirsrad/interpem.f:1-37 */
+float interpem(int nem, const float* vem, const float* em, float v, int* err) {
+    if (nem <= 0) return 1.0f;
+    if (v < vem[0] || v > vem[nem - 1]) { *err = RTB_ERR_RANGE; return 0.0f; }
+    float x = 0.0f;
+    for (int i = 0; i < nem - 1; ++i)
+        if (v >= vem[i] && v < vem[i + 1]) {
+            const float f = (v - vem[i]) / (vem[i + 1] - vem[i]);
+            x = (1 - f) * em[i] + f * em[i + 1];
+        }
+    if (v == vem[nem - 1]) x = em[nem - 1];
+    return x;
+}
+
+/* RAYLEIGHJ: radtran/scatter/rayleighj.f:1-35 with faniso(0) = 1
+ * (radtran/scatter/rayleigha.f:55-63). */
+float rayleighj(float v) {
+    const float AH2 = 13.58E-5f, BH2 = 7.52E-3f, AHe = 3.48E-5f, BHe = 2.30E-3f;
+    const float pi = 3.1415927f, fH2 = 0.864f, k = 1.37971e-23f, P0 = 1.013e5f, T0 = 273.15f;
+    const float lambda = 1e-2f / v;
+    float x = 1.0f / (lambda * 1e6f);
+    const float nH2 = AH2 * (1.0f + BH2 * x * x);
+    const float nHe = AHe * (1.0f + BHe * x * x);
+    const float nAir = fH2 * nH2 + (1 - fH2) * nHe;
+    const float delta = 0.0f;
+    const float temp = 32 * (pi * pi * pi) * (nAir * nAir);
+    const float N0 = P0 / (k * T0);
+    x = N0 * lambda * lambda;
+    const float faniso = (6.0f + 3.0f * delta) / (6.0f - 7.0f * delta);
+    return temp * 1e4f * faniso / (3 * (x * x));
+}
+
+/* Column accessors for Fortran arrays with leading dimensions. */
+struct Dims {
+    int ld_lay, ld_con, ld_v, ld_param;
+};
+
+Dims dims_of(const rtb_atm& a) {
+    Dims d;
+    d.ld_lay = a.ld_lay > 0 ? a.ld_lay : RTB_MAXLAY;
+    d.ld_con = a.ld_con > 0 ? a.ld_con : RTB_MAXCON;
+    d.ld_v = a.ld_v > 0 ? a.ld_v : RTB_MAXV;
+    d.ld_param = a.ld_param > 0 ? a.ld_param : (RTB_MAXGAS + 2 + RTB_MAXCON);
+    return d;
+}
+
+int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
+    if (a.nlayer <= 0 || a.ngas <= 0 || a.npath <= 0 || a.nwave <= 0 || a.nv < 0 || a.npro <= 0)
+        return RTB_ERR_ARG;
+    if (a.nlayer > d.ld_lay || a.nlayer > RTB_MAXLAY || a.npath > RTB_MAXPAT ||
+        a.ngas > RTB_MAXGAS || a.ncont > RTB_MAXCON || a.npro > RTB_MAXPRO || a.nv > d.ld_v)
+        return RTB_ERR_LIMIT;
+    if (t.ng > RTB_MAXG || t.np > RTB_MAXK || t.nt > RTB_MAXK) return RTB_ERR_LIMIT;
+    if (t.ng < 2 || t.nt <= 0) return RTB_ERR_UNSUPPORTED;
+    if (a.flagh2p != 0 || a.ilbl != 0 || a.inlte != 0 || a.fwhm != 0.0f) return RTB_ERR_UNSUPPORTED;
+    if (!(a.iform == 0 || a.iform == 2)) return RTB_ERR_UNSUPPORTED;
+    if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
+    for (int k = 0; k < a.ngas; ++k) {
+        if (a.idgas[k] == 91 || a.idgas[k] == 48 || a.idgas[k] == 80) return RTB_ERR_UNSUPPORTED;
+        if (a.ktab[k] >= t.ntab) return RTB_ERR_ARG;
+    }
+    for (int ip = 0; ip < a.npath; ++ip) {
+        const int m = a.imod[ip];
+        if (!(m == 0 || m == 1 || m == 3)) return RTB_ERR_UNSUPPORTED;
+        if (a.nlayin[ip] > d.ld_lay || a.nlayin[ip] > 2 * RTB_MAXPAT) return RTB_ERR_LIMIT;
+        if (a.nlayin[ip] < (m == 3 ? 2 : 1)) return RTB_ERR_UNSUPPORTED;
+        for (int j = 0; j < a.nlayin[ip]; ++j) {
+            const int l = a.layinc[j + (size_t)d.ld_lay * ip];
+            if (l < 1 || l > a.nlayer) return RTB_ERR_LIMIT;
+        }
+    }
+    bool n2co2 = false;
+    for (int k = 0; k < a.ngas; ++k) if (a.idgas[k] == 22 || a.idgas[k] == 2) n2co2 = true;
+    if (n2co2)
+        for (int w = 0; w < a.nwave; ++w) {
+            const float vv = a.ispace == 1 ? 1e4f / a.vwave[w] : a.vwave[w];
+            if (vv >= 3900.0f) return RTB_ERR_UNSUPPORTED;
+        }
+    return RTB_OK;
+}
+
+/* Per-wavenumber work of cirsradg_wave (cirsradg_wave.f:333-1290) for the
+ * IMOD 0/1/3 paths, followed by map2pro + map2xvec and packing
+ * (cirsrtfg_wave.f:397-446).  All scratch is owned by the Work object. */
+template <class R>
+struct Work {
+    std::vector<R> kout, dkout;              /* [ngas][nlayer][ng] */
+    std::vector<R> taucon, utotl;
+    std::vector<R> dtaucondq;                /* [nlayer][nparam] */
+    std::vector<R> kl_g;                     /* [nlayer][ng] */
+    std::vector<R> dkdql;                    /* [nlayer][ngas+1][ng] */
+    std::vector<R> dcoutdq;                  /* [npath][ng][nlaymax][nparam] */
+    std::vector<R> corkout, tempgtsurf;      /* [npath][ng] */
+    std::vector<R> bb, dbdt;                 /* [npath][nlaymax] */
+    std::vector<R> doutputdq;                /* [npath][nlaymax][nparam] */
+    std::vector<R> doutmoddq;                /* [npath][nparam][npro] */
+};
+
+template <class R>
+int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::vector<LayerK<R>>& LK,
+             const std::vector<int>& isw, int iw, Work<R>& W, double* calcout, double* gradients,
+             double* gradtsurf, const orc_debug* dbg) {
+    const int nlayer = a.nlayer, ngas = a.ngas, ng = t.ng, ncont = a.ncont, npath = a.npath;
+    const int nparam = ngas + 1 + ncont;
+    const int nsw = (int)isw.size();
+    const float vwave = a.vwave[iw];
+    float vv = vwave;
+    int err = 0;
+    const float esurf = interpem(a.nem, a.vem, a.emissivity, vwave, &err);
+    if (err) return err;
+    if (a.ispace == 1) vv = 1e4f / vwave;
+    std::vector<R> delg(ng);
+    for (int i = 0; i < ng; ++i) delg[i] = (R)t.delg[i];
+
+    /* utotl: cirsradg_wave.f:418-426 */
+    for (int i = 0; i < nlayer; ++i) {
+        R u = 0;
+        for (int j = 0; j < ngas; ++j) u = u + (R)a.amount[i + (size_t)d.ld_lay * j];
+        W.utotl[i] = u * (R)1.e-20f;
+    }
+    /* get_kg: cirsradg_wave.f:502-506 */
+    for (int k = 0; k < ngas; ++k) {
+        R* ko = &W.kout[(size_t)k * nlayer * ng];
+        R* dko = &W.dkout[(size_t)k * nlayer * ng];
+        const int itab = a.ktab[k];
+        BinSel bs{};
+        bool zero = itab < 0;
+        if (!zero) {
+            int st = select_bin(t, itab, vwave, bs);
+            if (st) return st;
+            zero = bs.zero;
+        }
+        if (zero) {
+            std::fill(ko, ko + (size_t)nlayer * ng, (R)0);
+            std::fill(dko, dko + (size_t)nlayer * ng, (R)0);
+            continue;
+        }
+        const float* tab1 = table_slice(t, itab, bs.n1);
+        const float* tab2 = bs.coinc ? nullptr : table_slice(t, itab, bs.n1 + 1);
+        for (int l = 0; l < nlayer; ++l)
+            get_kg_layer<R>(t, bs, tab1, tab2, LK[l], delg.data(), ko + (size_t)l * ng, dko + (size_t)l * ng);
+    }
+    const float xray = (a.iray > 0 && a.itype != 0) ? rayleighj(vv) * 1E20f : 0.0f;
+    std::vector<R> amo(ngas), kgn((size_t)ngas * ng), dkgn((size_t)ngas * ng), aam(ngas), ppp(ngas);
+    std::vector<R> k_g(ng), dkdq((size_t)(ngas + 1) * ng);
+    /* layer loop: cirsradg_wave.f:510-760 */
+    for (int j = 0; j < nlayer; ++j) {
+        R taucon = 0;
+        R* dtc = &W.dtaucondq[(size_t)j * nparam];
+        for (int k = 0; k < nparam; ++k) dtc[k] = 0;
+        const R p = (R)a.press[j], tt = (R)a.temp[j];
+        for (int k = 0; k < ncont; ++k) {                       /* dust :550-575 */
+            const R tau = (R)a.xsec_ext[k + (size_t)ncont * iw];
+            taucon = taucon + tau * (R)a.cont[k + (size_t)d.ld_con * j];
+            dtc[ngas + 1 + k] = tau;
+        }
+        /* ngascon (:590-611): every continuum flag off -> 0.0 */
+        for (int k = 0; k < ngas; ++k) taucon = taucon + (R)0;
+        for (int ii = 0; ii < ngas; ++ii) {
+            aam[ii] = (R)a.amount[j + (size_t)d.ld_lay * ii];
+            ppp[ii] = (R)a.pp[j + (size_t)d.ld_lay * ii];
+        }
+        R avgcontmp = 0;
+        int iabs[5];
+        R dabs[7];
+        if (t.has_cia) {
+            nciacon<R>(t, (R)vv, p, tt, a.inormal, ngas, a.idgas, a.isogas, aam.data(), ppp.data(),
+                       (R)a.delh[j], avgcontmp, iabs, dabs);
+        } else {
+            avgcontmp = 0;
+            for (int i = 0; i < 5; ++i) iabs[i] = 0;
+            for (int i = 0; i < 7; ++i) dabs[i] = 0;
+        }
+        taucon = taucon + avgcontmp;
+        for (int ii = 0; ii < 5; ++ii) {
+            const int k = iabs[ii];
+            if (k > 0) dtc[k - 1] = dtc[k - 1] + dabs[ii] / (W.utotl[j] * (R)1.0e20f);
+        }
+        dtc[ngas] = dtc[ngas] + dabs[5];
+        if (a.iray > 0 && a.itype != 0) {                        /* :663-691 (IRAY=1) */
+            const R av = W.utotl[j] * (R)xray;
+            taucon = taucon + av;
+            for (int k = 0; k < ngas; ++k) dtc[k] = dtc[k] + (R)xray * (R)1.0e-20f;
+        }
+        W.taucon[j] = taucon;
+        /* gather and overlap: :703-753 */
+        for (int k = 0; k < ngas; ++k) {
+            amo[k] = (R)a.amount[j + (size_t)d.ld_lay * k] * (R)1.0e-20f;
+            for (int l = 0; l < ng; ++l) {
+                kgn[(size_t)k * ng + l] = W.kout[((size_t)k * nlayer + j) * ng + l];
+                dkgn[(size_t)k * ng + l] = W.dkout[((size_t)k * nlayer + j) * ng + l];
+            }
+        }
+        int16_t* pp_ = nullptr;
+        int16_t* ps_ = nullptr;
+        int16_t* pt_ = nullptr;
+        if (dbg && ngas > 1) {
+            const size_t rec = ((size_t)iw * nlayer + j) * (ngas - 1);
+            if (dbg->perm) pp_ = dbg->perm + rec * ng * ng;
+            if (dbg->split) ps_ = dbg->split + rec * ng;
+            if (dbg->ties) pt_ = dbg->ties + rec;
+        }
+        if (ngas == 1) {
+            /* noverlapg's pass loop is empty for one gas: k_g keeps its prior
+             * contents in the reference; defined here as the gas itself. */
+            for (int l = 0; l < ng; ++l) {
+                k_g[l] = kgn[l] * amo[0];
+                dkdq[l] = kgn[l];
+                dkdq[(size_t)ng + l] = dkgn[l] * amo[0];
+            }
+        } else {
+            int st = noverlapg<R>(delg.data(), ng, ngas, amo.data(), kgn.data(), dkgn.data(), k_g.data(),
+                                  dkdq.data(), pp_, ps_, pt_);
+            if (st) return st;
+        }
+        for (int l = 0; l < ng; ++l) {
+            W.kl_g[(size_t)j * ng + l] = k_g[l];
+            for (int k = 0; k < ngas; ++k)
+                W.dkdql[((size_t)j * (ngas + 1) + k) * ng + l] = dkdq[(size_t)k * ng + l] * (R)1.0e-20f;
+            W.dkdql[((size_t)j * (ngas + 1) + ngas) * ng + l] = dkdq[(size_t)ngas * ng + l];
+        }
+    }
+
+    /* g loop: cirsradg_wave.f:776-1035 */
+    const int nlmax = *std::max_element(a.nlayin, a.nlayin + npath);
+    std::vector<R> tautmp(nlayer), dtautmpdq((size_t)nlayer * nparam), taus(nlmax),
+        dtaudq((size_t)nlmax * nparam), dtolddq((size_t)nlmax * nparam), dtrdq((size_t)nlmax * nparam);
+    auto DC = [&](int ip, int ig, int j, int k) -> R& {
+        return W.dcoutdq[(((size_t)ip * ng + ig) * nlmax + j) * nparam + k];
+    };
+    for (int ig = 0; ig < ng; ++ig) {
+        for (int j = 0; j < nlayer; ++j) {
+            tautmp[j] = W.taucon[j] + W.kl_g[(size_t)j * ng + ig];
+            for (int k = 0; k < nparam; ++k) dtautmpdq[(size_t)j * nparam + k] = W.dtaucondq[(size_t)j * nparam + k];
+            for (int k = 0; k < ngas + 1; ++k)
+                dtautmpdq[(size_t)j * nparam + k] =
+                    dtautmpdq[(size_t)j * nparam + k] + W.dkdql[((size_t)j * (ngas + 1) + k) * ng + ig];
+        }
+        for (int ip = 0; ip < npath; ++ip) {
+            const int nlays = a.nlayin[ip];
+            R& cork = W.corkout[(size_t)ip * ng + ig];
+            cork = 0;
+            W.tempgtsurf[(size_t)ip * ng + ig] = 0;
+            for (int j = 0; j < nlays; ++j)
+                for (int k = 0; k < nparam; ++k) DC(ip, ig, j, k) = 0;
+            for (int j = 0; j < nlays; ++j) {
+                const int l = a.layinc[j + (size_t)d.ld_lay * ip] - 1;
+                const R sc = (R)a.scale[j + (size_t)d.ld_lay * ip];
+                taus[j] = tautmp[l] * sc;
+                for (int k = 0; k < nparam; ++k) dtaudq[(size_t)j * nparam + k] = dtautmpdq[(size_t)l * nparam + k] * sc;
+            }
+            const int im = a.imod[ip];
+            if (im == 0 || im == 1) {
+                for (int j = 0; j < nlays; ++j) cork = cork + taus[j];
+                const R tmp = cork;
+                if (im == 0) {
+                    cork = dpexp<R>(-tmp);
+                    const R xfac = 1;
+                    for (int j = 0; j < nlays; ++j)
+                        for (int k1 = 0; k1 < nsw; ++k1) {
+                            const int k = isw[k1];
+                            DC(ip, ig, j, k) = -tmp * cork * dtaudq[(size_t)j * nparam + k] * xfac;
+                        }
+                    cork = cork * xfac;
+                } else {
+                    cork = (R)1. - dpexp<R>(-tmp);
+                    for (int j = 0; j < nlays; ++j)
+                        for (int k1 = 0; k1 < nsw; ++k1) {
+                            const int k = isw[k1];
+                            DC(ip, ig, j, k) = tmp * ((R)1 - cork) * dtaudq[(size_t)j * nparam + k];
+                        }
+                }
+            } else {  /* IMOD = 3: :896-1035 */
+                double trold = 1., taud = 0.0;
+                for (int j = 0; j < nlays; ++j)
+                    for (int k = 0; k < nparam; ++k) {
+                        dtolddq[(size_t)j * nparam + k] = 0;
+                        dtrdq[(size_t)j * nparam + k] = 0;
+                    }
+                const R xfac = 1.;
+                for (int j = 0; j < nlays; ++j) {
+                    if (ig == 0) {
+                        const R Tn = (R)a.emtemp[j + (size_t)d.ld_lay * ip];
+                        W.bb[(size_t)ip * nlmax + j] = planck_wave<R>(a.ispace, (R)vwave, Tn);
+                        W.dbdt[(size_t)ip * nlmax + j] = planckg_wave<R>(a.ispace, (R)vwave, Tn);
+                    }
+                    const R bbj = W.bb[(size_t)ip * nlmax + j];
+                    const double tlayer = std::exp(-(double)taus[j]);
+                    taud = taud + (double)taus[j];
+                    const double tr = trold * tlayer;
+                    cork = cork + xfac * (R)(trold - tr) * bbj;
+                    for (int k1 = 0; k1 < nsw; ++k1) {
+                        const int k = isw[k1];
+                        for (int j1 = 0; j1 <= j; ++j1) {
+                            R& dtr = dtrdq[(size_t)j1 * nparam + k];
+                            if (j1 < j) dtr = dtolddq[(size_t)j1 * nparam + k] * (R)tlayer;
+                            else dtr = -dtaudq[(size_t)j1 * nparam + k] * (R)(tlayer * trold);
+                            DC(ip, ig, j1, k) = DC(ip, ig, j1, k) +
+                                                xfac * bbj * (dtolddq[(size_t)j1 * nparam + k] - dtr);
+                        }
+                        if (k == ngas)  /* temperature column ngas+1 (1-based) */
+                            DC(ip, ig, j, k) = DC(ip, ig, j, k) + xfac * (R)(trold - tr) * W.dbdt[(size_t)ip * nlmax + j];
+                    }
+                    trold = tr;
+                    for (int j1 = 0; j1 <= j; ++j1)
+                        for (int k1 = 0; k1 < nsw; ++k1) {
+                            const int k = isw[k1];
+                            dtolddq[(size_t)j1 * nparam + k] = dtrdq[(size_t)j1 * nparam + k];
+                        }
+                }
+                /* limb test and surface term: :991-1025 */
+                const int j1 = (int)(0.5f * (float)nlays);
+                const float p1 = a.press[a.layinc[(j1 - 1) + (size_t)d.ld_lay * ip] - 1];
+                const float p2 = a.press[a.layinc[(nlays - 1) + (size_t)d.ld_lay * ip] - 1];
+                if (p2 > p1) {
+                    R radground, gradground;
+                    if (a.tsurf <= 0.0f) {
+                        radground = W.bb[(size_t)ip * nlmax + nlays - 1];
+                        gradground = W.dbdt[(size_t)ip * nlmax + nlays - 1];
+                    } else {
+                        radground = (R)esurf * planck_wave<R>(a.ispace, (R)vwave, (R)a.tsurf);
+                        gradground = (R)esurf * planckg_wave<R>(a.ispace, (R)vwave, (R)a.tsurf);
+                    }
+                    cork = cork + xfac * (R)trold * radground;
+                    W.tempgtsurf[(size_t)ip * ng + ig] = xfac * (R)trold * gradground;
+                    for (int j = 0; j < nlays; ++j)
+                        for (int k1 = 0; k1 < nsw; ++k1) {
+                            const int k = isw[k1];
+                            DC(ip, ig, j, k) = DC(ip, ig, j, k) + xfac * radground * dtolddq[(size_t)j * nparam + k];
+                        }
+                }
+            }
+        }
+    }
+    /* g quadrature: :1240-1286 */
+    std::vector<R> output(npath), gtsurf(npath);
+    for (int ip = 0; ip < npath; ++ip) {
+        output[ip] = 0;
+        gtsurf[ip] = 0;
+        for (int j = 0; j < nlmax; ++j)
+            for (int k = 0; k < nparam; ++k) W.doutputdq[((size_t)ip * nlmax + j) * nparam + k] = 0;
+        const int nlay1 = a.nlayin[ip];
+        for (int ig = 0; ig < ng; ++ig) {
+            output[ip] = output[ip] + W.corkout[(size_t)ip * ng + ig] * delg[ig];
+            gtsurf[ip] = gtsurf[ip] + W.tempgtsurf[(size_t)ip * ng + ig] * delg[ig];
+            for (int j = 0; j < nlay1; ++j)
+                for (int k1 = 0; k1 < nsw; ++k1) {
+                    const int k = isw[k1];
+                    R& o = W.doutputdq[((size_t)ip * nlmax + j) * nparam + k];
+                    o = o + DC(ip, ig, j, k) * delg[ig];
+                }
+        }
+    }
+    /* map2pro: radtran/cirsradg/map2pro.f:49-82 */
+    const int npro = a.npro;
+    for (int ip = 0; ip < npath; ++ip)
+        for (int k = 0; k < nparam; ++k)
+            for (int jj = 0; jj < npro; ++jj) {
+                R s = 0;
+                const int nlay1 = a.nlayin[ip];
+                for (int j = 0; j < nlay1; ++j) {
+                    const int lay = a.layinc[j + (size_t)d.ld_lay * ip] - 1;
+                    const R dq = W.doutputdq[((size_t)ip * nlmax + j) * nparam + k];
+                    const float* M;
+                    if (k < ngas) M = a.dam;
+                    else if (k == ngas) M = a.dte;
+                    else M = a.dco;
+                    if (!M) continue;
+                    s = s + dq * (R)M[lay + (size_t)d.ld_lay * jj];
+                }
+                W.doutmoddq[((size_t)ip * nparam + k) * npro + jj] = s;
+            }
+    /* map2xvec: radtran/cirsradg/map2xvec.f:41-55; packing cirsrtfg_wave.f:425-446 */
+    const int nwave = a.nwave, nv = a.nv;
+    for (int ip = 0; ip < npath; ++ip) {
+        calcout[(size_t)nwave * ip + iw] = (double)output[ip];
+        if (gradtsurf) gradtsurf[(size_t)nwave * ip + iw] = (double)gtsurf[ip];
+        for (int iv = 0; iv < nv; ++iv) {
+            R s = 0;
+            for (int ipar = 0; ipar < nparam; ++ipar)
+                for (int ipro = 0; ipro < npro; ++ipro)
+                    s = s + W.doutmoddq[((size_t)ip * nparam + ipar) * npro + ipro] *
+                                (R)a.xmap[iv + (size_t)d.ld_v * (ipar + (size_t)d.ld_param * ipro)];
+            gradients[(size_t)nwave * nv * ip + (size_t)nwave * iv + iw] = (double)s;
+        }
+    }
+    return RTB_OK;
+}
+
+template <class R>
+int run(const orc_tables& t, const rtb_atm& a, double* calcout, double* gradients, double* gradtsurf,
+        const orc_debug* dbg, int nthreads) {
+    const Dims d = dims_of(a);
+    int st = validate(t, a, d);
+    if (st) return st;
+    const int nparam = a.ngas + 1 + a.ncont;
+    /* nsw / isw: cirsrtfg_wave.f:301-313 */
+    std::vector<int> isw;
+    for (int ip = 0; ip < nparam; ++ip) {
+        bool on = false;
+        for (int iv = 0; iv < a.nv && !on; ++iv)
+            for (int ipro = 0; ipro < a.npro; ++ipro)
+                if (a.xmap[iv + (size_t)d.ld_v * (ip + (size_t)d.ld_param * ipro)] != 0.0f) { on = true; break; }
+        if (on) isw.push_back(ip);
+    }
+    std::vector<R> p(t.np), tt(t.nt);
+    for (int i = 0; i < t.np; ++i) p[i] = (R)t.lnp[i];
+    for (int i = 0; i < t.nt; ++i) tt[i] = (R)t.tk[i];
+    std::vector<LayerK<R>> LK(a.nlayer);
+    for (int l = 0; l < a.nlayer; ++l) layer_prep<R>(t, p.data(), tt.data(), a.press[l], a.temp[l], LK[l]);
+
+    auto make_work = [&](Work<R>& W) {
+        const int ng = t.ng, nl = a.nlayer, npath = a.npath;
+        const int nlmax = *std::max_element(a.nlayin, a.nlayin + npath);
+        W.kout.resize((size_t)a.ngas * nl * ng);
+        W.dkout.resize((size_t)a.ngas * nl * ng);
+        W.taucon.resize(nl);
+        W.utotl.resize(nl);
+        W.dtaucondq.resize((size_t)nl * nparam);
+        W.kl_g.resize((size_t)nl * ng);
+        W.dkdql.resize((size_t)nl * (a.ngas + 1) * ng);
+        W.dcoutdq.resize((size_t)npath * ng * nlmax * nparam);
+        W.corkout.resize((size_t)npath * ng);
+        W.tempgtsurf.resize((size_t)npath * ng);
+        W.bb.resize((size_t)npath * nlmax);
+        W.dbdt.resize((size_t)npath * nlmax);
+        W.doutputdq.resize((size_t)npath * nlmax * nparam);
+        W.doutmoddq.resize((size_t)npath * nparam * a.npro);
+    };
+    if (nthreads <= 1) {
+        Work<R> W;
+        make_work(W);
+        for (int iw = 0; iw < a.nwave; ++iw) {
+            st = one_wave<R>(t, a, d, LK, isw, iw, W, calcout, gradients, gradtsurf, dbg);
+            if (st) return st;
+        }
+        return RTB_OK;
+    }
+    std::vector<int> stat(nthreads, RTB_OK);
+    std::vector<std::thread> th;
+    for (int tid = 0; tid < nthreads; ++tid)
+        th.emplace_back([&, tid]() {
+            Work<R> W;
+            make_work(W);
+            for (int iw = tid; iw < a.nwave; iw += nthreads) {
+                int s = one_wave<R>(t, a, d, LK, isw, iw, W, calcout, gradients, gradtsurf, nullptr);
+                if (s) { stat[tid] = s; return; }
+            }
+        });
+    for (auto& x : th) x.join();
+    for (int s : stat) if (s) return s;
+    return RTB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_cirsrtfg_wave(const orc_tables* tab, const rtb_atm* atm, int precision, double* calcout,
+                      double* gradients, double* gradtsurf, const orc_debug* dbg) {
+    if (!tab || !atm || !calcout || !gradients) return RTB_ERR_ARG;
+    if (precision == ORC_MIXED) return run<float>(*tab, *atm, calcout, gradients, gradtsurf, dbg, 1);
+    return run<double>(*tab, *atm, calcout, gradients, gradtsurf, nullptr, 1);
+}
+
+int orc_cirsrtfg_wave_mt(const orc_tables* tab, const rtb_atm* atm, int precision, double* calcout,
+                         double* gradients, double* gradtsurf, int nthreads) {
+    if (!tab || !atm || !calcout || !gradients) return RTB_ERR_ARG;
+    if (precision == ORC_MIXED) return run<float>(*tab, *atm, calcout, gradients, gradtsurf, nullptr, nthreads);
+    return run<double>(*tab, *atm, calcout, gradients, gradtsurf, nullptr, nthreads);
+}
+
+float orc_det_expf_c(float x) { return orc_det_expf(x); }
+
+void orc_set_sort_mode(int mode) { g_sort_mode = mode; }
+
+int orc_locate(const float* xx, int n, float x) { return locate<float>(xx, n, x); }
+
+void orc_sort2g(int n, float* ra, int* ib) {
+    std::vector<int> ico(n);
+    for (int i = 0; i < n; ++i) ico[i] = i + 1;
+    sort2g<float>(n, ra, ico.data());
+    for (int i = 0; i < n; ++i) ib[i] = ico[i] - 1;
+}
+
+int orc_rankg(int nparam, const float* gw, int ng, int nloop, const float* weight, const float* cont,
+              const float* grad, float* k_g, float* dkdq, int16_t* perm, int16_t* split) {
+    std::vector<float> w(weight, weight + nloop), c(cont, cont + nloop), g(grad, grad + (size_t)nparam * nloop);
+    return rankg<float>(nparam, gw, ng, nloop, w.data(), c.data(), g.data(), k_g, dkdq, perm, split);
+}
+
+float orc_planck_wave(int ispace, float v, float t) { return planck_wave<float>(ispace, v, t); }
+float orc_planckg_wave(int ispace, float v, float t) { return planckg_wave<float>(ispace, v, t); }
+
+}  // extern "C"

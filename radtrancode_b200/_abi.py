@@ -1,0 +1,77 @@
+"""ctypes mirror of the structures declared in include/radtran_b200.h.
+
+Only layout lives here; loading of the shared library is in ``_lib.py``.
+"""
+import ctypes as C
+
+import numpy as np
+
+RTB_OK = 0
+RTB_ERR_ARG = 1
+RTB_ERR_LIMIT = 2
+RTB_ERR_UNSUPPORTED = 3
+RTB_ERR_CUDA = 4
+RTB_ERR_NOTABLE = 5
+RTB_ERR_NONPD = 6
+RTB_ERR_RANGE = 7
+RTB_ERR_GORD = 8
+RTB_ERR_BUDGET = 9
+
+STATUS_NAMES = {
+    0: "RTB_OK", 1: "RTB_ERR_ARG", 2: "RTB_ERR_LIMIT", 3: "RTB_ERR_UNSUPPORTED",
+    4: "RTB_ERR_CUDA", 5: "RTB_ERR_NOTABLE", 6: "RTB_ERR_NONPD", 7: "RTB_ERR_RANGE",
+    8: "RTB_ERR_GORD", 9: "RTB_ERR_BUDGET",
+}
+
+MAXLAY, MAXPAT, MAXGAS, MAXCON, MAXG, MAXK, MAXV, MAXPRO = 400, 200, 30, 10, 51, 30, 401, 200
+CIA_NUMPAIRS, CIA_NUMT, CIA_NUMWN = 9, 25, 1501
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+
+class RtbAtm(C.Structure):
+    _fields_ = [
+        ("nlayer", C.c_int), ("ngas", C.c_int), ("ncont", C.c_int), ("npath", C.c_int),
+        ("npro", C.c_int), ("nv", C.c_int), ("nwave", C.c_int),
+        ("ld_lay", C.c_int), ("ld_con", C.c_int), ("ld_v", C.c_int), ("ld_param", C.c_int),
+        ("press", _fp), ("temp", _fp), ("delh", _fp), ("pp", _fp), ("amount", _fp), ("cont", _fp),
+        ("idgas", _ip), ("isogas", _ip), ("ktab", _ip),
+        ("nlayin", _ip), ("imod", _ip), ("layinc", _ip), ("scale", _fp), ("emtemp", _fp),
+        ("dte", _fp), ("dam", _fp), ("dco", _fp), ("dfp", _fp),
+        ("xmap", _fp),
+        ("vwave", _fp), ("xsec_ext", _fp),
+        ("inormal", C.c_int), ("iray", C.c_int), ("itype", C.c_int), ("ispace", C.c_int),
+        ("flagh2p", C.c_int), ("ilbl", C.c_int), ("inlte", C.c_int), ("iform", C.c_int),
+        ("tsurf", C.c_float), ("fwhm", C.c_float),
+        ("nem", C.c_int), ("vem", _fp), ("emissivity", _fp),
+    ]
+
+
+class RtbFwdStats(C.Structure):
+    _fields_ = [
+        ("cells", C.c_longlong), ("sort_passes", C.c_longlong), ("tie_passes", C.c_longlong),
+        ("exact_passes", C.c_longlong), ("irregular_passes", C.c_longlong), ("ms_kernel", C.c_float),
+    ]
+
+
+def fptr(a):
+    """float* of a contiguous float32 numpy array (None -> NULL)."""
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and (a.flags.c_contiguous or a.flags.f_contiguous), a.dtype
+    return a.ctypes.data_as(_fp)
+
+
+def iptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and (a.flags.c_contiguous or a.flags.f_contiguous), a.dtype
+    return a.ctypes.data_as(_ip)
+
+
+def dptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64
+    return a.ctypes.data_as(C.POINTER(C.c_double))

@@ -1,0 +1,72 @@
+"""Loader of the in-tree shared library libradtran_b200.so.
+
+The library is the product: a missing or unloadable library is an error,
+never a reason to fall back to another implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+from . import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libradtran_b200.so")
+CSRC = os.path.join(HERE, "csrc")
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the CUDA sources for sm_100a into the package directory."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", CSRC], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run radtrancode_b200._lib.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        fp = C.POINTER(C.c_float)
+        ip = C.POINTER(C.c_int)
+        dp = C.POINTER(C.c_double)
+        L.rtb_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.rtb_create.restype = C.c_int
+        L.rtb_destroy.argtypes = [vp]
+        L.rtb_destroy.restype = None
+        L.rtb_last_error.argtypes = [vp]
+        L.rtb_last_error.restype = C.c_char_p
+        L.rtb_version.restype = C.c_char_p
+        L.rtb_set_ktables.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, fp, fp, fp, fp, fp, ip, fp]
+        L.rtb_set_ktables.restype = C.c_int
+        L.rtb_set_cia.argtypes = [vp, C.c_float, dp, fp]
+        L.rtb_set_cia.restype = C.c_int
+        L.rtb_cirsrtfg_wave.argtypes = [vp, C.POINTER(_abi.RtbAtm), fp, fp, fp]
+        L.rtb_cirsrtfg_wave.restype = C.c_int
+        L.rtb_cirsrtfg_wave_batch.argtypes = [vp, C.c_int, C.POINTER(_abi.RtbAtm), C.POINTER(fp), C.POINTER(fp),
+                                              C.POINTER(fp)]
+        L.rtb_cirsrtfg_wave_batch.restype = C.c_int
+        L.rtb_get_fwd_stats.argtypes = [vp, C.POINTER(_abi.RtbFwdStats)]
+        L.rtb_get_fwd_stats.restype = C.c_int
+        L.rtb_set_debug.argtypes = [vp, C.c_int]
+        L.rtb_set_debug.restype = C.c_int
+        L.rtb_set_strict_ties.argtypes = [vp, C.c_int]
+        L.rtb_set_strict_ties.restype = C.c_int
+        p16 = C.POINTER(C.c_int16)
+        L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
+        L.rtb_get_debug_bins.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+# every symbol include/radtran_b200.h declares
+EXPORTED = [
+    "rtb_create", "rtb_destroy", "rtb_last_error", "rtb_version", "rtb_set_ktables", "rtb_set_cia",
+    "rtb_cirsrtfg_wave", "rtb_cirsrtfg_wave_batch", "rtb_get_fwd_stats", "rtb_set_debug",
+    "rtb_get_debug_bins", "rtb_set_strict_ties",
+]

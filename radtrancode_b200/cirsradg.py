@@ -1,0 +1,124 @@
+"""Python face of the B200 CIRSRADG forward model (C ABI in
+include/radtran_b200.h).
+
+``Context`` mirrors the reference's call sequence: ``read_klist`` (k-table
+residency) -> ``ciaread`` (CIA table) -> ``cirsrtfg_wave`` (all wavenumbers
+of one forward + Jacobian call, radtran/cirsradg/cirsrtfg_wave.f:1-3), with
+the same argument meaning and output packing.  Errors are raised as
+``RtbError`` carrying the status code and the library's message, where the
+reference would STOP.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi, _lib
+
+
+class RtbError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Context:
+    """One device context (one CUDA device, one host thread at a time)."""
+
+    def __init__(self, device: int = 0):
+        self._L = _lib.lib()
+        h = C.c_void_p()
+        st = self._L.rtb_create(device, C.byref(h))
+        if st != 0:
+            raise RtbError(st, f"rtb_create(device={device}) failed: no usable CUDA device")
+        self._h = h
+        self.tables = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.rtb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int):
+        if st != 0:
+            raise RtbError(st, self._L.rtb_last_error(self._h).decode())
+
+    # -- resident tables --------------------------------------------------
+    def set_ktables(self, kt):
+        """read_klist equivalent: upload the run's k-tables once."""
+        self._check(self._L.rtb_set_ktables(
+            self._h, kt.ntab, kt.np_, kt.nt, kt.ng, _abi.fptr(kt.lnp), _abi.fptr(kt.tk), _abi.fptr(kt.delg),
+            _abi.fptr(kt.vmin), _abi.fptr(kt.delv), _abi.iptr(kt.nbin), _abi.fptr(kt.data)))
+        self.tables = kt
+
+    def set_cia(self, cia):
+        """ciaread's one-time table read."""
+        self._check(self._L.rtb_set_cia(self._h, float(cia.dnu), _abi.dptr(cia.temps), _abi.fptr(cia.kcia)))
+
+    def set_strict_ties(self, on: bool):
+        self._check(self._L.rtb_set_strict_ties(self._h, int(bool(on))))
+
+    def set_debug(self, on: bool):
+        self._check(self._L.rtb_set_debug(self._h, int(bool(on))))
+
+    # -- forward model ------------------------------------------------------
+    def cirsrtfg_wave(self, job):
+        """Forward model + Jacobian of one job.  Returns (calcout, gradients,
+        gradtsurf) as float32 arrays packed as cirsrtfg_wave.f:425-446."""
+        n1, n2, n3 = job.out_shapes()
+        calcout = np.zeros(n1, np.float32)
+        grads = np.zeros(n2, np.float32)
+        gts = np.zeros(n3, np.float32)
+        s = job.as_struct()
+        self._check(self._L.rtb_cirsrtfg_wave(self._h, C.byref(s), _abi.fptr(calcout), _abi.fptr(grads),
+                                              _abi.fptr(gts)))
+        return calcout, grads, gts
+
+    def cirsrtfg_wave_batch(self, jobs, outs=None):
+        """Batched forward model: one launch for all jobs.  Returns a list of
+        (calcout, gradients, gradtsurf)."""
+        n = len(jobs)
+        structs = (_abi.RtbAtm * n)()
+        keep = []
+        if outs is None:
+            outs = []
+            for j in jobs:
+                a, b, c = j.out_shapes()
+                outs.append((np.zeros(a, np.float32), np.zeros(b, np.float32), np.zeros(c, np.float32)))
+        fp = C.POINTER(C.c_float)
+        p1, p2, p3 = (fp * n)(), (fp * n)(), (fp * n)()
+        for i, j in enumerate(jobs):
+            s = j.as_struct()
+            keep.append(s)
+            structs[i] = s
+            p1[i], p2[i], p3[i] = _abi.fptr(outs[i][0]), _abi.fptr(outs[i][1]), _abi.fptr(outs[i][2])
+        self._check(self._L.rtb_cirsrtfg_wave_batch(self._h, n, structs, p1, p2, p3))
+        return outs
+
+    def stats(self) -> dict:
+        s = _abi.RtbFwdStats()
+        self._check(self._L.rtb_get_fwd_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def debug_bins(self, job):
+        npass = max(job.ngas - 1, 1)
+        ng = self.tables.ng
+        perm = np.full((job.nwave, job.nlayer, npass, ng * ng), -1, np.int16)
+        split = np.full((job.nwave, job.nlayer, npass, ng), -1, np.int16)
+        p16 = C.POINTER(C.c_int16)
+        self._check(self._L.rtb_get_debug_bins(self._h, perm.ctypes.data_as(p16), perm.size,
+                                               split.ctypes.data_as(p16), split.size))
+        return perm, split

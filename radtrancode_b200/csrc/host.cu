@@ -1,0 +1,852 @@
+// host.cu -- C ABI (include/radtran_b200.h), device residency and the host
+// side of the forward model: validation (check_limits.f), the discrete
+// set-up the reference does per wavenumber and per layer (get_kg.f record
+// choice and P/T location, ciaread/nciacon constants, isw selection of
+// cirsrtfg_wave.f:301-313) and the sparse composition of map2pro and
+// map2xvec.  No compute path runs on the CPU: the forward model itself is
+// fwd_kernel.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/radtran_b200.h"
+#include "rtb_common.h"
+
+namespace rtb {
+int fwd_smem_bytes(int ng, int Lmax, int nsw, int ncol, int nlmax, int npath);
+cudaError_t launch_fwd(const BatchDev& B, int Lmax, int nsw, int ncol, int nlmax, int npath, int grid,
+                       cudaStream_t st);
+}  // namespace rtb
+
+using namespace rtb;
+
+namespace {
+
+// growable device buffer
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t c = std::max(n, (size_t)4096);
+        c = c + c / 4;
+        cudaError_t e = cudaMalloc(&p, c);
+        if (e == cudaSuccess) cap = c;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct HostPinned {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t c = std::max(n, (size_t)4096);
+        c = c + c / 4;
+        cudaError_t e = cudaMallocHost(&p, c);
+        if (e == cudaSuccess) cap = c;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct rtb_context {
+    int device = 0;
+    int nsm = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    // k-tables
+    int ntab = 0, np = 0, nt = 0, ng = 0;
+    std::vector<float> lnp, tk, delg;
+    std::vector<double> g_ord;
+    std::vector<float> vmin, delv;
+    std::vector<int> nbin;
+    std::vector<int64_t> tab_off;            // element offset of each table
+    std::vector<std::vector<uint8_t>> nonzero;  // [tab][bin]: any value > 0 (get_kg.f:228-250)
+    DevBuf d_raw, d_log, d_delg, d_gord;
+    // CIA
+    int has_cia = 0;
+    float dnu = 0.0f;
+    std::vector<float> cia_tk;               // sngl(temps)
+    DevBuf d_kcia;
+    // per-call arena
+    DevBuf d_in, d_out, d_diag;
+    HostPinned h_in, h_out;
+    // options and diagnostics
+    int strict_ties = 0;
+    int debug = 0;
+    DevBuf d_dbg_perm, d_dbg_split;
+    size_t dbg_perm_n = 0, dbg_split_n = 0;
+    rtb_fwd_stats stats{};
+};
+
+namespace {
+
+int fail(rtb_context* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                 \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(ctx, RTB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// LOCATE (radtran/scatter/locate.f:1-28), 1-based
+int locate_f(const float* xx, int n, float x) {
+    int jl = 0, ju = n + 1;
+    while (ju - jl > 1) {
+        const int jm = (ju + jl) / 2;
+        if ((xx[n - 1] >= xx[0]) == (x >= xx[jm - 1])) jl = jm; else ju = jm;
+    }
+    if (x == xx[0]) return 1;
+    if (x == xx[n - 1]) return n - 1;
+    return jl;
+}
+
+// PINDEX (radtran/radtran/read_ktable.f:201-226); clamps x1 in place, 1-based
+int pindex_f(const float* x, int nx, float& x1) {
+    if (x1 > x[nx - 1]) x1 = x[nx - 1];
+    if (x1 < x[0]) x1 = x[0];
+    int j = 0;
+    for (int i = 1; i <= nx - 1; ++i) {
+        if (x1 >= x[i - 1]) j = i; else break;
+    }
+    return j;
+}
+
+// RAYLEIGHJ (radtran/scatter/rayleighj.f) with faniso(0) = 1
+float rayleighj_f(float v) {
+    const float AH2 = 13.58E-5f, BH2 = 7.52E-3f, AHe = 3.48E-5f, BHe = 2.30E-3f;
+    const float pi = 3.1415927f, fH2 = 0.864f, k = 1.37971e-23f, P0 = 1.013e5f, T0 = 273.15f;
+    const float lambda = 1e-2f / v;
+    float x = 1.0f / (lambda * 1e6f);
+    const float nH2 = AH2 * (1.0f + BH2 * x * x);
+    const float nHe = AHe * (1.0f + BHe * x * x);
+    const float nAir = fH2 * nH2 + (1 - fH2) * nHe;
+    const float delta = 0.0f;
+    const float temp = 32 * (pi * pi * pi) * (nAir * nAir);
+    const float N0 = P0 / (k * T0);
+    x = N0 * lambda * lambda;
+    const float faniso = (6.0f + 3.0f * delta) / (6.0f - 7.0f * delta);
+    return temp * 1e4f * faniso / (3 * (x * x));
+}
+
+// planck_wave / planckg_wave (radtran/radtran/planck_wave.f, planckg_wave.f)
+void planck_host(int ispace, float v, float T, float& B, float& dB) {
+    const double c1 = (double)1.1911e-12f, c2 = (double)1.439f;
+    double y;
+    if (ispace == 0) y = v; else y = 1e4 / v;
+    if (y == 0.0) { B = 0; dB = 0; return; }
+    const double x = c2 * y / T;
+    const double a = ispace == 0 ? c1 * y * y * y : c1 * y * y * y * y * y / 1e4;
+    const double em1 = std::expm1(x);
+    B = (float)(a / em1);
+    dB = (float)(a / em1 * (x / T) * (em1 + 1.0) / em1);
+}
+
+// INTERPEM (radtran/cirsrad/interpem.f)
+int interpem_f(int nem, const float* vem, const float* em, float v, float& out) {
+    if (nem <= 0) { out = 1.0f; return RTB_OK; }
+    if (v < vem[0] || v > vem[nem - 1]) return RTB_ERR_RANGE;
+    float x = 0.0f;
+    for (int i = 0; i < nem - 1; ++i)
+        if (v >= vem[i] && v < vem[i + 1]) {
+            const float f = (v - vem[i]) / (vem[i + 1] - vem[i]);
+            x = (1 - f) * em[i] + f * em[i + 1];
+        }
+    if (v == vem[nem - 1]) x = em[nem - 1];
+    out = x;
+    return RTB_OK;
+}
+
+// host staging of one batch
+struct Staging {
+    std::vector<SpecDev> spec;
+    std::vector<int64_t> item_start;
+    std::vector<LayerDev> lay;
+    std::vector<float> amo;
+    std::vector<WaveDev> wave;
+    std::vector<int64_t> wg_slice;
+    std::vector<float> xsec, cont;
+    std::vector<int> p_layinc;
+    std::vector<float> p_scale, p_emtemp;
+    std::vector<int> map_colptr, map_row;
+    std::vector<float> map_val;
+    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1;
+    int64_t n_out = 0, n_jac = 0;
+};
+
+struct Dims {
+    int ld_lay, ld_con, ld_v, ld_param;
+};
+
+int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
+    Dims d;
+    d.ld_lay = a.ld_lay > 0 ? a.ld_lay : RTB_MAXLAY;
+    d.ld_con = a.ld_con > 0 ? a.ld_con : RTB_MAXCON;
+    d.ld_v = a.ld_v > 0 ? a.ld_v : RTB_MAXV;
+    d.ld_param = a.ld_param > 0 ? a.ld_param : (RTB_MAXGAS + 2 + RTB_MAXCON);
+    // ---- limits and supported options (check_limits.f:1-74) ----
+    if (a.nlayer <= 0 || a.ngas <= 0 || a.npath <= 0 || a.nwave <= 0 || a.nv < 0 || a.npro <= 0)
+        return fail(c, RTB_ERR_ARG, "non-positive size (nlayer=%d ngas=%d npath=%d nwave=%d npro=%d)", a.nlayer,
+                    a.ngas, a.npath, a.nwave, a.npro);
+    if (!a.press || !a.temp || !a.delh || !a.pp || !a.amount || !a.idgas || !a.isogas || !a.ktab || !a.nlayin ||
+        !a.imod || !a.layinc || !a.scale || !a.emtemp || !a.dte || !a.dam || !a.xmap || !a.vwave)
+        return fail(c, RTB_ERR_ARG, "NULL input array");
+    if (a.nlayer > d.ld_lay || a.nlayer > RTB_MAXLAY || a.npath > RTB_MAXPAT || a.ngas > RTB_MAXGAS ||
+        a.ncont > RTB_MAXCON || a.npro > RTB_MAXPRO || a.nv > d.ld_v || a.nv > RTB_MAXV)
+        return fail(c, RTB_ERR_LIMIT, "array limit exceeded (check_limits.f)");
+    if (a.flagh2p != 0) return fail(c, RTB_ERR_UNSUPPORTED, "flagh2p=1 (nparacon path) not implemented");
+    if (a.ilbl != 0) return fail(c, RTB_ERR_UNSUPPORTED, "ILBL != 0 (line-by-line tables) not implemented");
+    if (a.inlte != 0) return fail(c, RTB_ERR_UNSUPPORTED, "non-LTE emission temperatures not implemented");
+    if (a.fwhm != 0.0f) return fail(c, RTB_ERR_UNSUPPORTED, "FWHM != 0 convolution not implemented");
+    if (!(a.iform == 0 || a.iform == 2)) return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d not implemented", a.iform);
+    if (a.iray > 1) return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (only Jovian Rayleigh, iray=1)", a.iray);
+    if (a.npath > 4) return fail(c, RTB_ERR_UNSUPPORTED, "more than 4 paths per spectrum");
+    if (a.ncont > 0 && (!a.cont || !a.xsec_ext || !a.dco)) return fail(c, RTB_ERR_ARG, "dust arrays missing");
+    const int ng = c->ng;
+    if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
+    bool n2co2 = false;
+    for (int k = 0; k < a.ngas; ++k) {
+        const int id = a.idgas[k];
+        if (id == 91 || id == 48 || id == 80)
+            return fail(c, RTB_ERR_UNSUPPORTED, "gas id %d needs the H-/electron continuum", id);
+        if (a.ktab[k] >= c->ntab) return fail(c, RTB_ERR_ARG, "ktab[%d]=%d >= ntab", k, a.ktab[k]);
+        if (id == 22 || id == 2) n2co2 = true;
+    }
+    int nlmax = 0;
+    for (int ip = 0; ip < a.npath; ++ip) {
+        const int m = a.imod[ip];
+        if (!(m == 0 || m == 1 || m == 3)) return fail(c, RTB_ERR_UNSUPPORTED, "IMOD=%d not implemented", m);
+        const int nl = a.nlayin[ip];
+        if (nl > d.ld_lay || nl > 2 * RTB_MAXPAT) return fail(c, RTB_ERR_LIMIT, "nlayin exceeds maxinc");
+        if (nl < (m == 3 ? 2 : 1)) return fail(c, RTB_ERR_UNSUPPORTED, "path with %d layers", nl);
+        for (int j = 0; j < nl; ++j) {
+            const int l = a.layinc[j + (size_t)d.ld_lay * ip];
+            if (l < 1 || l > a.nlayer) return fail(c, RTB_ERR_LIMIT, "layinc exceeds nlayer");
+        }
+        nlmax = std::max(nlmax, nl);
+    }
+    const int nparam = a.ngas + 1 + a.ncont;
+    // ---- isw (cirsrtfg_wave.f:301-313) ----
+    std::vector<int> isw;
+    for (int ip = 0; ip < nparam; ++ip) {
+        bool on = false;
+        for (int ipro = 0; ipro < a.npro && !on; ++ipro)
+            for (int iv = 0; iv < a.nv; ++iv)
+                if (a.xmap[iv + (size_t)d.ld_v * (ip + (size_t)d.ld_param * ipro)] != 0.0f) { on = true; break; }
+        if (on) isw.push_back(ip);
+    }
+    if ((int)isw.size() > kMaxSw)
+        return fail(c, RTB_ERR_UNSUPPORTED, "%d active gradient parameters (device limit %d)", (int)isw.size(), kMaxSw);
+    SpecDev S;
+    memset(&S, 0, sizeof S);
+    S.nlayer = a.nlayer;
+    S.ngas = a.ngas;
+    S.npath = a.npath;
+    S.nwave = a.nwave;
+    S.nv = a.nv;
+    S.ncont = a.ncont;
+    S.nsw = (int)isw.size();
+    S.nlmax = nlmax;
+    S.sw_T = -1;
+    S.ispace = a.ispace;
+    S.inormal = a.inormal;
+    S.iray = (a.iray > 0 && a.itype != 0) ? 1 : 0;
+    S.has_cia = c->has_cia;
+    S.tsurf_pos = a.tsurf > 0.0f ? 1 : 0;
+    for (int s = 0; s < kMaxSw; ++s) { S.isw[s] = -1; S.col_of_param[s] = -1; }
+    for (int cc = 0; cc < kMaxCols; ++cc) S.col_gas[cc] = -1;
+    int ncol = 0;
+    for (int s = 0; s < S.nsw; ++s) {
+        S.isw[s] = isw[s];
+        if (isw[s] <= a.ngas) {   // a gas amount or the temperature: tracked through the overlap
+            if (ncol >= kMaxCols) return fail(c, RTB_ERR_UNSUPPORTED, "too many tracked gradient columns");
+            S.col_gas[ncol] = isw[s];
+            S.col_of_param[s] = ncol;
+            ++ncol;
+        }
+        if (isw[s] == a.ngas) S.sw_T = s;
+    }
+    S.ncol = ncol;
+    for (int ip = 0; ip < a.npath; ++ip) {
+        S.nlayin[ip] = a.nlayin[ip];
+        S.imod[ip] = a.imod[ip];
+    }
+    // ---- per-layer set-up ----
+    S.lay_off = (int64_t)st.lay.size();
+    S.lg_off = (int64_t)st.amo.size();
+    S.lc_off = (int64_t)st.cont.size();
+    const int np = c->np, nt = c->nt;
+    const float pmax = c->lnp[np - 1], pmin = c->lnp[0], tmax = c->tk[nt - 1], tmin = c->tk[0];
+    for (int l = 0; l < a.nlayer; ++l) {
+        LayerDev L;
+        memset(&L, 0, sizeof L);
+        // get_kg.f:117-141
+        float P1 = (float)std::log((double)a.press[l]);
+        if (P1 < pmin) P1 = pmin;
+        if (P1 > pmax) P1 = pmax;
+        int cp = locate_f(c->lnp.data(), np, P1);
+        if (cp < 1) cp = 1;
+        if (cp >= np) cp = np - 1;
+        L.v = (P1 - c->lnp[cp - 1]) / (c->lnp[cp] - c->lnp[cp - 1]);
+        float T1 = a.temp[l];
+        if (T1 < tmin) T1 = tmin;
+        if (T1 > tmax) T1 = tmax;
+        int ct = locate_f(c->tk.data(), nt, T1);
+        if (ct < 1) ct = 1;
+        if (ct >= nt) ct = nt - 1;
+        L.u = (T1 - c->tk[ct - 1]) / (c->tk[ct] - c->tk[ct - 1]);
+        L.dudt = 1.0f / (c->tk[ct] - c->tk[ct - 1]);
+        L.ioff[0] = (nt * ng * (cp - 1)) + (ng * (ct - 1));
+        L.ioff[1] = (nt * ng * cp) + (ng * (ct - 1));
+        L.ioff[2] = (nt * ng * cp) + (ng * ct);
+        L.ioff[3] = (nt * ng * (cp - 1)) + (ng * ct);
+        // utotl (cirsradg_wave.f:418-426)
+        float u = 0.0f;
+        for (int k = 0; k < a.ngas; ++k) u = u + a.amount[l + (size_t)d.ld_lay * k];
+        L.utotl = u * 1.e-20f;
+        // nciacon.f:113-177 constants
+        float qh2 = 0, qhe = 0, qn2 = 0, qch4 = 0, qco2 = 0;
+        for (int i = 0; i < 5; ++i) L.iabs[i] = -1;
+        const float p = a.press[l], T = a.temp[l];
+        for (int i = 0; i < a.ngas; ++i) {
+            const int id = a.idgas[i], iso = a.isogas[i];
+            const float ppi = a.pp[l + (size_t)d.ld_lay * i];
+            if (id == 39 && (iso == 0 || iso == 1)) { qh2 = ppi / p; L.iabs[0] = i; }
+            if (id == 40) { qhe = ppi / p; L.iabs[1] = i; }
+            if (id == 22) { qn2 = ppi / p; L.iabs[2] = i; }
+            if (id == 6 && (iso == 0 || iso == 1)) { qch4 = (ppi / p); L.iabs[3] = i; }
+            if (id == 2) { qco2 = ppi / p; L.iabs[4] = i; }
+        }
+        L.q[0] = qh2; L.q[1] = qhe; L.q[2] = qn2; L.q[3] = qch4; L.q[4] = qco2;
+        const float xlen = a.delh[l];
+        const float AMAGAT = 2.68675E19f, MODBOLTZA = 10.0f * 1.37947E-23f / 1.013f;
+        float tau;
+        if (xlen == 0.0f) {
+            float XP1 = 0, height = 0;
+            for (int i = 0; i < a.ngas; ++i) {
+                const float ppi = a.pp[l + (size_t)d.ld_lay * i];
+                if (ppi > XP1) { height = a.amount[l + (size_t)d.ld_lay * i] * MODBOLTZA * T / ppi; XP1 = ppi; }
+            }
+            const float aa = p / 1.0f, bb = 273.15f / T;
+            tau = (aa * aa) * (bb * bb) * height;
+        } else {
+            const float height = xlen * 1e5f;
+            float XP1 = -1, TOTAM = 0;
+            for (int i = 0; i < a.ngas; ++i) {
+                const float ppi = a.pp[l + (size_t)d.ld_lay * i];
+                if (ppi > XP1 && ppi > 0) { TOTAM = a.amount[l + (size_t)d.ld_lay * i] * p / ppi; XP1 = ppi; }
+            }
+            const float amag1 = (TOTAM / height) / AMAGAT;
+            tau = height * (amag1 * amag1);
+        }
+        L.cia_tau = tau;
+        if (c->has_cia) {
+            // ciaread.f:133-157 (the second test overwrites the first; pindex clamps)
+            const float* tk1 = c->cia_tk.data();
+            float temp1;
+            if (T > tk1[RTB_CIA_NUMT - 1]) temp1 = tk1[RTB_CIA_NUMT - 1]; else temp1 = T;
+            if (T < tk1[0]) temp1 = tk1[0]; else temp1 = T;
+            const int ctc = pindex_f(tk1, RTB_CIA_NUMT, temp1);
+            L.cia_ct = ctc - 1;
+            L.cia_u = (temp1 - tk1[ctc - 1]) / (tk1[ctc] - tk1[ctc - 1]);
+            L.cia_dudt = 1.0f / (tk1[ctc] - tk1[ctc - 1]);
+        } else {
+            L.cia_ct = -1;
+        }
+        st.lay.push_back(L);
+        for (int k = 0; k < a.ngas; ++k) st.amo.push_back(a.amount[l + (size_t)d.ld_lay * k] * 1.0e-20f);
+        for (int k = 0; k < a.ncont; ++k) st.cont.push_back(a.cont[k + (size_t)d.ld_con * l]);
+    }
+    // ---- per-wavenumber set-up ----
+    S.wave_off = (int64_t)st.wave.size();
+    S.wg_off = (int64_t)st.wg_slice.size();
+    S.wc_off = (int64_t)st.xsec.size();
+    std::vector<float> vvk1;
+    if (c->has_cia) {
+        vvk1.resize(RTB_CIA_NUMWN);
+        for (int i = 0; i < RTB_CIA_NUMWN; ++i) vvk1[i] = (float)i * c->dnu;
+    }
+    for (int iw = 0; iw < a.nwave; ++iw) {
+        WaveDev W;
+        memset(&W, 0, sizeof W);
+        const float vwave = a.vwave[iw];
+        W.vwave = vwave;
+        float esurf;
+        if (interpem_f(a.nem, a.vem, a.emissivity, vwave, esurf))
+            return fail(c, RTB_ERR_RANGE, "surface emissivity table does not cover %g (interpem.f)", vwave);
+        const float vv = a.ispace == 1 ? 1e4f / vwave : vwave;
+        if (n2co2 && vv >= 3900.0f)
+            return fail(c, RTB_ERR_UNSUPPORTED, "N2/CO2 near-IR CIA (co2cia/n2n2cia/n2h2cia) not implemented");
+        W.cia_cv = -1;
+        if (c->has_cia && !(vv > vvk1[RTB_CIA_NUMWN - 1] || vv < vvk1[0])) {
+            float vvc = vv;
+            const int cv = pindex_f(vvk1.data(), RTB_CIA_NUMWN, vvc);
+            W.cia_cv = cv - 1;
+            W.cia_t = (vv - vvk1[cv - 1]) / (vvk1[cv] - vvk1[cv - 1]);
+        }
+        W.xray = S.iray ? rayleighj_f(vv) * 1E20f : 0.0f;
+        if (a.tsurf > 0.0f) {
+            float B, dB;
+            planck_host(a.ispace, vwave, a.tsurf, B, dB);
+            W.radground_s = esurf * B;
+            W.gradground_s = esurf * dB;
+        }
+        st.wave.push_back(W);
+        // table record choice (get_kg.f:189-275)
+        for (int k = 0; k < a.ngas; ++k) {
+            const int itab = a.ktab[k];
+            int64_t slice = -1;
+            if (itab >= 0) {
+                const float vmin = c->vmin[itab], delv = c->delv[itab];
+                if (!(delv > 0.0f)) return fail(c, RTB_ERR_UNSUPPORTED, "irregular k-table grid (delv <= 0)");
+                float eps;
+                if (delv >= 0.0001f) eps = 0.02f * delv; else eps = 0.25f * delv;
+                const int n1 = (int)(((double)vwave + (double)eps - (double)vmin) / (double)delv);
+                const float tmp = vmin + delv * (float)n1;
+                const float frac = std::fabs((float)((double)vwave - (double)tmp));
+                const bool coinc = frac < eps;
+                if (!coinc)
+                    return fail(c, RTB_ERR_UNSUPPORTED,
+                                "wavenumber %g is not on the k-table grid (non-coincident branch)", vwave);
+                if (n1 < 0 || n1 >= c->nbin[itab])
+                    return fail(c, RTB_ERR_RANGE, "wavenumber %g outside k-table %d", vwave, itab);
+                if (c->nonzero[itab][n1])
+                    slice = c->tab_off[itab] + (int64_t)n1 * np * nt * ng;
+            }
+            st.wg_slice.push_back(slice);
+        }
+        for (int k = 0; k < a.ncont; ++k) st.xsec.push_back(a.xsec_ext[k + (size_t)a.ncont * iw]);
+    }
+    // ---- paths ----
+    S.path_off = (int64_t)st.p_layinc.size();
+    S.nonlimb_mask = 0;
+    for (int ip = 0; ip < a.npath; ++ip) {
+        const int nl = a.nlayin[ip];
+        for (int j = 0; j < nlmax; ++j) {
+            if (j < nl) {
+                st.p_layinc.push_back(a.layinc[j + (size_t)d.ld_lay * ip] - 1);
+                st.p_scale.push_back(a.scale[j + (size_t)d.ld_lay * ip]);
+                st.p_emtemp.push_back(a.emtemp[j + (size_t)d.ld_lay * ip]);
+            } else {
+                st.p_layinc.push_back(0);
+                st.p_scale.push_back(0.0f);
+                st.p_emtemp.push_back(1.0f);
+            }
+        }
+        if (a.imod[ip] == 3) {   // limb test of cirsradg_wave.f:983-988
+            const int j1 = (int)(0.5f * (float)nl);
+            const float p1 = a.press[a.layinc[(j1 - 1) + (size_t)d.ld_lay * ip] - 1];
+            const float p2 = a.press[a.layinc[(nl - 1) + (size_t)d.ld_lay * ip] - 1];
+            if (p2 > p1) S.nonlimb_mask |= 1 << ip;
+        }
+    }
+    // ---- map2pro o map2xvec: sparse (s, j) -> iv per path ----
+    S.map_off = (int64_t)st.map_colptr.size();
+    {
+        const int nsw = S.nsw, nv = a.nv, npro = a.npro;
+        // nonzero xmap entries per (param, level)
+        std::vector<std::vector<std::pair<int, float>>> xm((size_t)nparam * npro);
+        for (int s = 0; s < nsw; ++s) {
+            const int k = isw[s];
+            for (int lev = 0; lev < npro; ++lev)
+                for (int iv = 0; iv < nv; ++iv) {
+                    const float v = a.xmap[iv + (size_t)d.ld_v * (k + (size_t)d.ld_param * lev)];
+                    if (v != 0.0f) xm[(size_t)k * npro + lev].push_back({iv, v});
+                }
+        }
+        for (int ip = 0; ip < a.npath; ++ip) {
+            const int nl = a.nlayin[ip];
+            std::vector<double> T((size_t)nv * nlmax * std::max(nsw, 1), 0.0);
+            std::vector<uint8_t> touched(T.size(), 0);
+            for (int s = 0; s < nsw; ++s) {
+                const int k = isw[s];
+                const float* M = k < a.ngas ? a.dam : (k == a.ngas ? a.dte : a.dco);
+                if (!M) continue;
+                for (int j = 0; j < nl; ++j) {
+                    const int lay = a.layinc[j + (size_t)d.ld_lay * ip] - 1;
+                    for (int lev = 0; lev < npro; ++lev) {
+                        const float m = M[lay + (size_t)d.ld_lay * lev];
+                        if (m == 0.0f) continue;
+                        for (const auto& e : xm[(size_t)k * npro + lev]) {
+                            const size_t idx = (size_t)e.first * nlmax * nsw + (size_t)j * nsw + s;
+                            T[idx] += (double)m * (double)e.second;
+                            touched[idx] = 1;
+                        }
+                    }
+                }
+            }
+            for (int iv = 0; iv < nv; ++iv) {
+                st.map_colptr.push_back((int)st.map_row.size());
+                for (int r = 0; r < nlmax * nsw; ++r) {
+                    const size_t idx = (size_t)iv * nlmax * nsw + r;
+                    if (touched[idx]) {
+                        st.map_row.push_back(r);
+                        st.map_val.push_back((float)T[idx]);
+                    }
+                }
+            }
+            st.map_colptr.push_back((int)st.map_row.size());
+        }
+    }
+    S.out_off = st.n_out;
+    S.jac_off = st.n_jac;
+    st.n_out += (int64_t)a.npath * a.nwave;
+    st.n_jac += (int64_t)a.npath * a.nv * a.nwave;
+    st.item_start.push_back(st.item_start.back() + a.nwave);
+    st.spec.push_back(S);
+    st.Lmax = std::max(st.Lmax, a.nlayer);
+    st.nsw_max = std::max(st.nsw_max, S.nsw);
+    st.ncol_max = std::max(st.ncol_max, S.ncol);
+    st.nlmax_max = std::max(st.nlmax_max, nlmax);
+    st.npath_max = std::max(st.npath_max, a.npath);
+    return RTB_OK;
+}
+
+template <class T>
+size_t bytes_of(const std::vector<T>& v) {
+    return v.size() * sizeof(T);
+}
+
+int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calcout, float* const* gradients,
+              float* const* gradtsurf) {
+    if (!c || nspec <= 0 || !atms) return fail(c, RTB_ERR_ARG, "bad batch arguments");
+    if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
+    if (c->ng > 22 || c->ng < 2) return fail(c, RTB_ERR_UNSUPPORTED, "NG=%d outside the device range 2..22", c->ng);
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    Staging st;
+    st.item_start.push_back(0);
+    for (int s = 0; s < nspec; ++s) {
+        const int r = pack_spectrum(c, atms[s], st);
+        if (r) return r;
+    }
+    // smem budget
+    const int smem = fwd_smem_bytes(c->ng, st.Lmax, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max);
+    int smem_max = 0;
+    CUDA_TRY(c, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    if (smem > smem_max)
+        return fail(c, RTB_ERR_UNSUPPORTED, "spectrum needs %d B of shared memory (device %d)", smem, smem_max);
+    // pack inputs into one pinned buffer
+    struct Seg {
+        const void* src;
+        size_t n;
+        size_t off;
+    };
+    std::vector<Seg> segs;
+    size_t off = 0;
+    auto add = [&](const void* p, size_t n) {
+        off = (off + 255) & ~(size_t)255;
+        segs.push_back({p, n, off});
+        off += n;
+        return segs.size() - 1;
+    };
+    const size_t i_spec = add(st.spec.data(), bytes_of(st.spec));
+    const size_t i_item = add(st.item_start.data(), bytes_of(st.item_start));
+    const size_t i_lay = add(st.lay.data(), bytes_of(st.lay));
+    const size_t i_amo = add(st.amo.data(), bytes_of(st.amo));
+    const size_t i_wave = add(st.wave.data(), bytes_of(st.wave));
+    const size_t i_wg = add(st.wg_slice.data(), bytes_of(st.wg_slice));
+    const size_t i_xsec = add(st.xsec.data(), bytes_of(st.xsec));
+    const size_t i_cont = add(st.cont.data(), bytes_of(st.cont));
+    const size_t i_pl = add(st.p_layinc.data(), bytes_of(st.p_layinc));
+    const size_t i_ps = add(st.p_scale.data(), bytes_of(st.p_scale));
+    const size_t i_pe = add(st.p_emtemp.data(), bytes_of(st.p_emtemp));
+    const size_t i_mc = add(st.map_colptr.data(), bytes_of(st.map_colptr));
+    const size_t i_mr = add(st.map_row.data(), bytes_of(st.map_row));
+    const size_t i_mv = add(st.map_val.data(), bytes_of(st.map_val));
+    const size_t in_bytes = off + 256;
+    CUDA_TRY(c, c->h_in.ensure(in_bytes));
+    CUDA_TRY(c, c->d_in.ensure(in_bytes));
+    for (const auto& s : segs)
+        if (s.n) memcpy((char*)c->h_in.p + s.off, s.src, s.n);
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_in.p, c->h_in.p, off, cudaMemcpyHostToDevice, c->stream));
+    const size_t out_bytes = (size_t)(2 * st.n_out + st.n_jac) * sizeof(float);
+    CUDA_TRY(c, c->d_out.ensure(out_bytes));
+    CUDA_TRY(c, c->h_out.ensure(out_bytes));
+    CUDA_TRY(c, c->d_diag.ensure(64));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, c->stream));
+    auto dp = [&](size_t i) { return (const void*)((const char*)c->d_in.p + segs[i].off); };
+    BatchDev B;
+    memset(&B, 0, sizeof B);
+    B.nspec = nspec;
+    B.nitems = st.item_start.back();
+    B.item_start = (const int64_t*)dp(i_item);
+    B.spec = (const SpecDev*)dp(i_spec);
+    B.lay = (const LayerDev*)dp(i_lay);
+    B.amo = (const float*)dp(i_amo);
+    B.wave = (const WaveDev*)dp(i_wave);
+    B.wg_slice = (const int64_t*)dp(i_wg);
+    B.xsec = (const float*)dp(i_xsec);
+    B.cont = (const float*)dp(i_cont);
+    B.p_layinc = (const int*)dp(i_pl);
+    B.p_scale = (const float*)dp(i_ps);
+    B.p_emtemp = (const float*)dp(i_pe);
+    B.map_colptr = (const int*)dp(i_mc);
+    B.map_row = (const int*)dp(i_mr);
+    B.map_val = (const float*)dp(i_mv);
+    // map_colptr entries are relative to this batch's map_row array: absolute already
+    B.ktab_raw = (const float*)c->d_raw.p;
+    B.ktab_log = (const float*)c->d_log.p;
+    B.np = c->np;
+    B.nt = c->nt;
+    B.ng = c->ng;
+    B.delg = (const float*)c->d_delg.p;
+    B.g_ord = (const double*)c->d_gord.p;
+    B.kcia = (const float*)c->d_kcia.p;
+    float* dout = (float*)c->d_out.p;
+    B.calcout = dout;
+    B.gradtsurf = dout + st.n_out;
+    B.gradients = dout + 2 * st.n_out;
+    B.status = (unsigned*)c->d_diag.p;
+    B.counters = (unsigned long long*)((char*)c->d_diag.p + 8);
+    B.strict_ties = c->strict_ties;
+    if (c->debug) {
+        const rtb_atm& a0 = atms[0];
+        const size_t npass = a0.ngas > 1 ? a0.ngas - 1 : 1;
+        c->dbg_perm_n = (size_t)a0.nwave * a0.nlayer * npass * c->ng * c->ng;
+        c->dbg_split_n = (size_t)a0.nwave * a0.nlayer * npass * c->ng;
+        CUDA_TRY(c, c->d_dbg_perm.ensure(c->dbg_perm_n * 2));
+        CUDA_TRY(c, c->d_dbg_split.ensure(c->dbg_split_n * 2));
+        CUDA_TRY(c, cudaMemsetAsync(c->d_dbg_perm.p, 0xff, c->dbg_perm_n * 2, c->stream));
+        CUDA_TRY(c, cudaMemsetAsync(c->d_dbg_split.p, 0xff, c->dbg_split_n * 2, c->stream));
+        B.dbg_perm = (int16_t*)c->d_dbg_perm.p;
+        B.dbg_split = (int16_t*)c->d_dbg_split.p;
+    }
+    const int per_sm = 2;
+    int64_t grid = (int64_t)c->nsm * per_sm;
+    if (grid > B.nitems) grid = B.nitems;
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    CUDA_TRY(c, launch_fwd(B, st.Lmax, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max, (int)grid, c->stream));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_out.p, c->d_out.p, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+    unsigned long long diag[8];
+    CUDA_TRY(c, cudaMemcpyAsync(diag, c->d_diag.p, 64, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    const unsigned status = (unsigned)(diag[0] & 0xffffffffu);
+    c->stats.cells = 0;
+    for (int s = 0; s < nspec; ++s) c->stats.cells += (long long)atms[s].nlayer * atms[s].nwave;
+    c->stats.sort_passes = (long long)diag[1];
+    c->stats.tie_passes = (long long)diag[2];
+    c->stats.exact_passes = (long long)diag[3];
+    c->stats.irregular_passes = (long long)diag[4];
+    c->stats.ms_kernel = ms;
+    if (status & kStGord) return fail(c, RTB_ERR_GORD, "g-ordinate walk ran past NG (rankg.f:118-147)");
+    // scatter outputs to the caller's buffers
+    const float* h = (const float*)c->h_out.p;
+    for (int s = 0; s < nspec; ++s) {
+        const SpecDev& S = st.spec[s];
+        const rtb_atm& a = atms[s];
+        const size_t no = (size_t)a.npath * a.nwave, nj = (size_t)a.npath * a.nv * a.nwave;
+        if (calcout && calcout[s]) memcpy(calcout[s], h + S.out_off, no * sizeof(float));
+        if (gradtsurf && gradtsurf[s]) memcpy(gradtsurf[s], h + st.n_out + S.out_off, no * sizeof(float));
+        if (gradients && gradients[s]) memcpy(gradients[s], h + 2 * st.n_out + S.jac_off, nj * sizeof(float));
+    }
+    return RTB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* rtb_version(void) { return "radtrancode_b200 0.1 (sm_100a)"; }
+
+int rtb_create(int device, rtb_context** out) {
+    if (!out) return RTB_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= device || device < 0) return RTB_ERR_CUDA;
+    rtb_context* c = new rtb_context();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return RTB_ERR_CUDA; }
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return RTB_ERR_CUDA;
+    }
+    *out = c;
+    return RTB_OK;
+}
+
+void rtb_destroy(rtb_context* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->d_raw.release();
+    c->d_log.release();
+    c->d_delg.release();
+    c->d_gord.release();
+    c->d_kcia.release();
+    c->d_in.release();
+    c->d_out.release();
+    c->d_diag.release();
+    c->d_dbg_perm.release();
+    c->d_dbg_split.release();
+    c->h_in.release();
+    c->h_out.release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* rtb_last_error(const rtb_context* c) { return c ? c->err.c_str() : "no context"; }
+
+int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const float* lnp, const float* tk,
+                    const float* delg, const float* vmin, const float* delv, const int* nbin, const float* data) {
+    if (!c) return RTB_ERR_ARG;
+    if (ntab <= 0 || np < 2 || nt < 2 || ng < 1 || !lnp || !tk || !delg || !vmin || !delv || !nbin || !data)
+        return fail(c, RTB_ERR_ARG, "bad k-table arguments");
+    if (np > RTB_MAXK || nt > RTB_MAXK || ng > RTB_MAXG || ntab > RTB_MAXGAS)
+        return fail(c, RTB_ERR_LIMIT, "k-table grid exceeds MAXK/MAXG");
+    if (ng > kMaxNg) return fail(c, RTB_ERR_UNSUPPORTED, "NG=%d > %d", ng, kMaxNg);
+    // the FP64 cumulative-weight scan is exact in any order when every
+    // product delg(i)*delg(j) >= 2^-28 and the total stays below 2
+    double sdelg = 0.0;
+    for (int i = 0; i < ng; ++i) {
+        if (!(delg[i] >= 6.103515625e-05f)) return fail(c, RTB_ERR_UNSUPPORTED, "delg below 2^-14");
+        sdelg += delg[i];
+    }
+    if (sdelg > 1.5) return fail(c, RTB_ERR_UNSUPPORTED, "sum of delg > 1.5");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    c->ntab = 0;
+    c->np = np;
+    c->nt = nt;
+    c->ng = ng;
+    c->lnp.assign(lnp, lnp + np);
+    c->tk.assign(tk, tk + nt);
+    c->delg.assign(delg, delg + ng);
+    c->g_ord.assign(ng + 1, 0.0);
+    for (int i = 0; i < ng; ++i) c->g_ord[i + 1] = c->g_ord[i] + (double)delg[i];
+    if (c->g_ord[ng] < 1.0) c->g_ord[ng] = 1.0;
+    c->vmin.assign(vmin, vmin + ntab);
+    c->delv.assign(delv, delv + ntab);
+    c->nbin.assign(nbin, nbin + ntab);
+    c->tab_off.assign(ntab, 0);
+    c->nonzero.assign(ntab, {});
+    const int64_t slice = (int64_t)np * nt * ng;
+    int64_t total = 0;
+    for (int t = 0; t < ntab; ++t) {
+        if (nbin[t] <= 0) return fail(c, RTB_ERR_ARG, "table %d has no bins", t);
+        c->tab_off[t] = total;
+        total += (int64_t)nbin[t] * slice;
+    }
+    std::vector<float> lg((size_t)total);
+    for (int t = 0; t < ntab; ++t) {
+        c->nonzero[t].assign(nbin[t], 0);
+        for (int b = 0; b < nbin[t]; ++b) {
+            const float* s = data + c->tab_off[t] + (int64_t)b * slice;
+            uint8_t any = 0;
+            for (int64_t i = 0; i < slice; ++i)
+                if (s[i] > 0.0f) { any = 1; break; }
+            c->nonzero[t][b] = any;
+        }
+    }
+    for (int64_t i = 0; i < total; ++i) lg[i] = (float)std::log((double)data[i]);
+    CUDA_TRY(c, c->d_raw.ensure((size_t)total * 4));
+    CUDA_TRY(c, c->d_log.ensure((size_t)total * 4));
+    CUDA_TRY(c, c->d_delg.ensure(4 * 64));
+    CUDA_TRY(c, c->d_gord.ensure(8 * 64));
+    CUDA_TRY(c, cudaMemcpy(c->d_raw.p, data, (size_t)total * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(c->d_log.p, lg.data(), (size_t)total * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(c->d_delg.p, delg, (size_t)ng * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(c->d_gord.p, c->g_ord.data(), (size_t)(ng + 1) * 8, cudaMemcpyHostToDevice));
+    c->ntab = ntab;
+    return RTB_OK;
+}
+
+int rtb_set_cia(rtb_context* c, float dnu, const double* temps, const float* kcia) {
+    if (!c) return RTB_ERR_ARG;
+    if (!temps || !kcia || !(dnu > 0.0f)) return fail(c, RTB_ERR_ARG, "bad CIA arguments");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    c->dnu = dnu;
+    c->cia_tk.resize(RTB_CIA_NUMT);
+    for (int i = 0; i < RTB_CIA_NUMT; ++i) c->cia_tk[i] = (float)temps[i];
+    const size_t n = (size_t)RTB_CIA_NUMPAIRS * RTB_CIA_NUMT * RTB_CIA_NUMWN;
+    CUDA_TRY(c, c->d_kcia.ensure(n * 4));
+    CUDA_TRY(c, cudaMemcpy(c->d_kcia.p, kcia, n * 4, cudaMemcpyHostToDevice));
+    c->has_cia = 1;
+    return RTB_OK;
+}
+
+int rtb_cirsrtfg_wave(rtb_context* c, const rtb_atm* atm, float* calcout, float* gradients, float* gradtsurf) {
+    if (!c || !atm || !calcout || !gradients) return fail(c, RTB_ERR_ARG, "NULL argument");
+    return run_batch(c, 1, atm, &calcout, &gradients, &gradtsurf);
+}
+
+int rtb_cirsrtfg_wave_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calcout,
+                            float* const* gradients, float* const* gradtsurf) {
+    return run_batch(c, nspec, atms, calcout, gradients, gradtsurf);
+}
+
+int rtb_get_fwd_stats(const rtb_context* c, rtb_fwd_stats* out) {
+    if (!c || !out) return RTB_ERR_ARG;
+    *out = c->stats;
+    return RTB_OK;
+}
+
+int rtb_set_debug(rtb_context* c, int on) {
+    if (!c) return RTB_ERR_ARG;
+    c->debug = on ? 1 : 0;
+    return RTB_OK;
+}
+
+int rtb_set_strict_ties(rtb_context* c, int on) {
+    if (!c) return RTB_ERR_ARG;
+    c->strict_ties = on ? 1 : 0;
+    return RTB_OK;
+}
+
+int rtb_get_debug_bins(const rtb_context* c, int16_t* perm, size_t n_perm, int16_t* split, size_t n_split) {
+    if (!c || !c->debug) return RTB_ERR_ARG;
+    if (perm) {
+        if (n_perm < c->dbg_perm_n) return RTB_ERR_ARG;
+        if (cudaMemcpy(perm, c->d_dbg_perm.p, c->dbg_perm_n * 2, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return RTB_ERR_CUDA;
+    }
+    if (split) {
+        if (n_split < c->dbg_split_n) return RTB_ERR_ARG;
+        if (cudaMemcpy(split, c->d_dbg_split.p, c->dbg_split_n * 2, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return RTB_ERR_CUDA;
+    }
+    return RTB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// rtb_common.h -- data layout shared by the host orchestration (host.cu)
+// and the forward kernel (fwd_kernel.cu).
+//
+// A launch processes a *batch* of spectra.  Every per-spectrum input is
+// packed by the host into flat device arrays; a SpecDev descriptor holds the
+// offsets.  Work items are (spectrum, wavenumber) pairs: one CTA per item.
+#pragma once
+#include <stdint.h>
+
+namespace rtb {
+
+constexpr int kMaxNg = 32;        // one lane per g-ordinate
+constexpr int kMaxCols = 8;       // tracked gradient columns in the overlap (active gases + T)
+constexpr int kMaxSw = 8;         // active Jacobian columns (isw) per spectrum
+constexpr int kMaxGasDev = 30;    // MAXGAS
+constexpr int kWarps = 8;         // warps per CTA of the forward kernel
+constexpr int kThreads = kWarps * 32;
+
+// status bits accumulated by the kernel (OR-ed into a device word)
+constexpr unsigned kStGord = 1u;       // g-walk ran past NG with elements left
+constexpr unsigned kStNanKey = 2u;     // NaN sort key met (handled by the exact path)
+constexpr unsigned kStRange = 4u;      // index outside a table
+
+// per-layer constants prepared on the host (get_kg.f:117-141, ciaread.f:108-198,
+// nciacon.f:84-177), identical arithmetic to the oracle
+struct LayerDev {
+    int ioff[4];          // offsets of the 4 (P,T) corners inside a (np,nt,ng) slice
+    float u, v, dudt;     // get_kg interpolation weights
+    float utotl;          // sum of amounts * 1e-20
+    int cia_ct;           // CIA temperature index (0-based), -1 = no CIA
+    float cia_u, cia_dudt;
+    float cia_tau;        // height * amagat^2 of nciacon
+    float q[5];           // qh2, qhe, qn2, qch4, qco2
+    int iabs[5];          // 0-based gas index or -1
+    float taudust;        // unused slot (dust is per wavenumber)
+};
+
+// per-wavenumber constants
+struct WaveDev {
+    float vwave;          // calculation wavenumber
+    int cia_cv;           // CIA wavenumber index (0-based), -1 = outside the table -> zero
+    float cia_t;          // CIA wavenumber weight
+    float xray;           // Rayleigh x-section * 1e20 (0 if off)
+    float radground_s;    // esurf*B(tsurf) when tsurf > 0
+    float gradground_s;   // esurf*dB/dT(tsurf)
+};
+
+// per-spectrum descriptor
+struct SpecDev {
+    int nlayer, ngas, npath, nwave, nv, ncont, nsw, nlmax;
+    int ncol;             // tracked overlap columns
+    int tsurf_pos;        // tsurf > 0
+    int nonlimb_mask;     // bit p: path p adds the surface term (cirsradg_wave.f:985-1000)
+    int ispace;
+    int inormal;
+    int iray;             // IRAY > 0 and ITYPE != 0
+    int has_cia;
+    int64_t lay_off;      // LayerDev index of layer 0
+    int64_t lg_off;       // (layer, gas) arrays: index of (0,0); [nlayer][ngas]
+    int64_t wave_off;     // WaveDev index of wavenumber 0
+    int64_t wg_off;       // (wave, gas) arrays: [nwave][ngas] table slice offsets
+    int64_t wc_off;       // (wave, cont) dust x-sections [nwave][ncont]
+    int64_t lc_off;       // (layer, cont) dust amounts [nlayer][ncont]
+    int64_t path_off;     // path-position arrays [npath][nlmax]
+    int64_t map_off;      // map CSC: colptr index of (path 0, iv 0); [npath][nv+1]
+    int64_t out_off;      // calcout/gradtsurf index of (path 0, wave 0)
+    int64_t jac_off;      // gradients index of (path 0, iv 0, wave 0)
+    int nlayin[4];        // up to 4 paths per spectrum on the device path
+    int imod[4];
+    int isw[kMaxSw];      // active parameters (0-based param ids)
+    int col_of_param[kMaxSw]; // tracked overlap column of isw[s] (-1: continuum only)
+    int col_gas[kMaxCols];    // gas index of tracked column c (ngas = temperature)
+    int sw_T;             // s index of the temperature column, -1 if inactive
+};
+
+struct BatchDev {
+    int nspec;
+    int64_t nitems;              // sum of nwave
+    const int64_t* item_start;   // [nspec+1] prefix sum of nwave
+    const SpecDev* spec;
+    const LayerDev* lay;
+    const float* amo;            // [.. nlayer][ngas] amount*1e-20
+    const WaveDev* wave;
+    const int64_t* wg_slice;     // [.. nwave][ngas] element offset of the table slice, -1 = zero
+    const float* xsec;           // [.. nwave][ncont]
+    const float* cont;           // [.. nlayer][ncont]
+    const int* p_layinc;         // [.. npath][nlmax] 0-based layer
+    const float* p_scale;
+    const float* p_emtemp;
+    const int* map_colptr;       // [.. npath][nv+1] into map_row/map_val (absolute)
+    const int* map_row;          // s*nlmax + j
+    const float* map_val;
+    // tables
+    const float* ktab_raw;       // k*1e20, record order
+    const float* ktab_log;       // (float)log((double)k)
+    int np, nt, ng;
+    const float* delg;           // [ng]
+    const double* g_ord;         // [ng+1], g_ord[ng] forced >= 1 (rankg.f:65-67)
+    const float* kcia;           // (9,25,1501) Fortran order
+    // outputs
+    float* calcout;
+    float* gradients;
+    float* gradtsurf;
+    // diagnostics
+    unsigned* status;
+    unsigned long long* counters;  // [0] sort passes [1] tie passes [2] risky/exact passes [3] irregular
+    int strict_ties;               // 1: exact heapsort for every pass with tied keys
+    int16_t* dbg_perm;             // debug capture for spectrum 0 (may be null)
+    int16_t* dbg_split;
+};
+
+}  // namespace rtb

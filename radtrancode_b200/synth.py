@@ -1,0 +1,297 @@
+"""Seeded synthetic workloads for the correlated-k gradient forward model.
+
+The reference measures on no public dataset; these generators build the
+workloads its own thermal-emission retrievals run on (a nadir giant-planet
+atmosphere, k-tables in .kta record order, a CIA table of the ciaread
+format) with the shapes and value distributions fixed by the configurations:
+
+* ``config1``: 40 layers, H2/He + CH4, 100 wavenumbers 1200-1350 cm-1,
+  k-table 20 P x 10 T x 20 g, NX = 41.
+* ``config2``: 120 layers, H2/He + CH4, C2H6, C2H2, NH3, 2000 wavenumbers
+  600-1400 cm-1, k-tables 20 P x 15 T x 20 g, NX = 124.
+* ``config3``: batches of uneven spectra drawn around config 2.
+
+Arrays use the Fortran layouts of the reference's COMMON blocks (column
+major, leading dimensions recorded in the job) so they can be handed to the
+C ABI (include/radtran_b200.h) unchanged.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+from . import _abi
+
+BAR_TO_ATM = 0.986923
+AMU = 1.66053907e-27
+KB = 1.380649e-23
+GRAV = 24.79          # m s-2 (Jupiter)
+MMW = 2.3             # mean molecular weight, amu
+
+# (HITRAN-style local id, isotope) of the gases of the configurations
+H2, HE, CH4, C2H6, C2H2, NH3 = (39, 0), (40, 0), (6, 0), (27, 0), (26, 0), (11, 0)
+ABSORBERS_C2 = [CH4, C2H6, C2H2, NH3]
+VMR = {H2: 0.86, HE: 0.136, CH4: 2e-3, C2H6: 4e-6, C2H2: 1e-7, NH3: 1e-4}
+
+
+def gauss_legendre_01(ng: int):
+    """Gauss-Legendre ordinates and weights on [0, 1] (sum of weights = 1)."""
+    x, w = np.polynomial.legendre.leggauss(ng)
+    return ((x + 1.0) * 0.5).astype(np.float32), (w * 0.5).astype(np.float32)
+
+
+@dataclasses.dataclass
+class KTables:
+    """k-tables of a run, laid out as rtb_set_ktables expects."""
+    np_: int
+    nt: int
+    ng: int
+    lnp: np.ndarray        # (np,) float32, ln(p / atm)
+    tk: np.ndarray         # (nt,) float32
+    g_ord: np.ndarray      # (ng,) float32
+    delg: np.ndarray       # (ng,) float32
+    vmin: np.ndarray       # (ntab,) float32
+    delv: np.ndarray       # (ntab,) float32
+    nbin: np.ndarray       # (ntab,) int32
+    data: np.ndarray       # concatenated float32 records
+    gases: list            # (id, iso) of each table
+
+    @property
+    def ntab(self) -> int:
+        return len(self.gases)
+
+    def table(self, i: int) -> np.ndarray:
+        """Table i as an array [nbin, np, nt, ng] (a view)."""
+        n = self.np_ * self.nt * self.ng
+        off = int(sum(int(self.nbin[k]) for k in range(i))) * n
+        return self.data[off: off + int(self.nbin[i]) * n].reshape(int(self.nbin[i]), self.np_, self.nt, self.ng)
+
+
+@dataclasses.dataclass
+class CIATable:
+    dnu: float
+    temps: np.ndarray      # (25,) float64
+    kcia: np.ndarray       # float32, Fortran (9, 25, 1501) flattened in Fortran order
+
+
+def make_ktables(gases, *, np_=20, nt=15, ng=20, vmin=600.0, delv=0.4, nbin=2000, seed=0,
+                 p_top_bar=1e-4, p_bot_bar=10.0, t_min=70.0, t_max=200.0, sigma=2.0,
+                 median=1e-22) -> KTables:
+    """Lognormal k-tables, monotone in g, stored x1e20 (cm2 x 1e20)."""
+    rng = np.random.default_rng(seed)
+    p_atm = np.geomspace(p_top_bar, p_bot_bar, np_) * BAR_TO_ATM
+    lnp = np.log(p_atm.astype(np.float32).astype(np.float64)).astype(np.float32)
+    tk = np.linspace(t_min, t_max, nt).astype(np.float32)
+    g_ord, delg = gauss_legendre_01(ng)
+    mu = np.log(median * 1e20)
+    tabs = []
+    for _ in gases:
+        z = rng.standard_normal((nbin, np_, nt, ng))
+        z.sort(axis=-1)
+        tabs.append(np.exp(mu + sigma * z).astype(np.float32).ravel())
+    data = np.concatenate(tabs) if tabs else np.zeros(0, np.float32)
+    n = len(gases)
+    return KTables(np_, nt, ng, lnp, tk, g_ord, delg,
+                   np.full(n, vmin, np.float32), np.full(n, delv, np.float32),
+                   np.full(n, nbin, np.int32), data, list(gases))
+
+
+def make_cia(seed=0, dnu=1.0) -> CIATable:
+    """Smooth lognormal H2-H2 and H2-He CIA (pairs 1, 2; others zero)."""
+    temps = np.linspace(40.0, 400.0, _abi.CIA_NUMT)
+    v = np.arange(_abi.CIA_NUMWN, dtype=np.float64) * dnu
+    k = np.zeros((_abi.CIA_NUMPAIRS, _abi.CIA_NUMT, _abi.CIA_NUMWN), np.float64)
+    vv = np.maximum(v, 1.0)
+    for pair, (amp, v0, s, gam) in enumerate([(2e-8, 500.0, 0.6, -0.5), (0.8e-8, 700.0, 0.7, -0.3)]):
+        shape = np.exp(-0.5 * (np.log(vv / v0) / s) ** 2)
+        shape[v == 0] = 0.0
+        k[pair] = amp * shape[None, :] * (temps[:, None] / 150.0) ** gam
+    return CIATable(float(dnu), temps.astype(np.float64), k.astype(np.float32).ravel(order="F"))
+
+
+@dataclasses.dataclass
+class Job:
+    """One cirsrtfg_wave call in the reference's Fortran array layout."""
+    nlayer: int
+    ngas: int
+    npath: int
+    npro: int
+    nv: int
+    nwave: int
+    ld_lay: int
+    ld_v: int
+    ld_param: int
+    press: np.ndarray
+    temp: np.ndarray
+    delh: np.ndarray
+    pp: np.ndarray          # (ld_lay, ngas) F
+    amount: np.ndarray      # (ld_lay, ngas) F
+    idgas: np.ndarray
+    isogas: np.ndarray
+    ktab: np.ndarray
+    nlayin: np.ndarray
+    imod: np.ndarray
+    layinc: np.ndarray      # (ld_lay, npath) F, 1-based
+    scale: np.ndarray       # (ld_lay, npath) F
+    emtemp: np.ndarray
+    dte: np.ndarray         # (ld_lay, npro) F
+    dam: np.ndarray
+    xmap: np.ndarray        # (ld_v, ld_param, npro) F
+    vwave: np.ndarray
+    vem: np.ndarray
+    emissivity: np.ndarray
+    inormal: int = 0
+    iray: int = 0
+    itype: int = 11
+    ispace: int = 0
+    tsurf: float = 0.0
+    iform: int = 0
+    # bookkeeping for the synthetic state vector (not part of the ABI)
+    vmr: np.ndarray | None = None
+    ncol: np.ndarray | None = None
+    xscale: np.ndarray | None = None
+
+    @property
+    def nparam(self) -> int:
+        return self.ngas + 1
+
+    def as_struct(self) -> _abi.RtbAtm:
+        s = _abi.RtbAtm()
+        s.nlayer, s.ngas, s.ncont, s.npath = self.nlayer, self.ngas, 0, self.npath
+        s.npro, s.nv, s.nwave = self.npro, self.nv, self.nwave
+        s.ld_lay, s.ld_con, s.ld_v, s.ld_param = self.ld_lay, 1, self.ld_v, self.ld_param
+        f, i = _abi.fptr, _abi.iptr
+        s.press, s.temp, s.delh = f(self.press), f(self.temp), f(self.delh)
+        s.pp, s.amount, s.cont = f(self.pp), f(self.amount), None
+        s.idgas, s.isogas, s.ktab = i(self.idgas), i(self.isogas), i(self.ktab)
+        s.nlayin, s.imod, s.layinc = i(self.nlayin), i(self.imod), i(self.layinc)
+        s.scale, s.emtemp = f(self.scale), f(self.emtemp)
+        s.dte, s.dam, s.dco, s.dfp = f(self.dte), f(self.dam), None, None
+        s.xmap = f(self.xmap)
+        s.vwave, s.xsec_ext = f(self.vwave), None
+        s.inormal, s.iray, s.itype, s.ispace = self.inormal, self.iray, self.itype, self.ispace
+        s.flagh2p, s.ilbl, s.inlte, s.iform = 0, 0, 0, self.iform
+        s.tsurf, s.fwhm = float(self.tsurf), 0.0
+        s.nem, s.vem, s.emissivity = len(self.vem), f(self.vem), f(self.emissivity)
+        s._keep = self   # keep the arrays alive with the struct
+        return s
+
+    def out_shapes(self):
+        return (self.npath * self.nwave,), (self.npath * self.nv * self.nwave,), (self.npath * self.nwave,)
+
+
+def _levels(nlayer):
+    p_lev = np.geomspace(10.0, 1e-4, nlayer + 1) * 1e5      # Pa, bottom first
+    p_lay = np.sqrt(p_lev[:-1] * p_lev[1:])
+    return p_lev, p_lay
+
+
+def temperature_profile(p_pa, rng, noise=3.0):
+    """Smooth 110-170 K profile in ln p (tanh) plus seeded N(0, noise) K."""
+    x = np.log(p_pa / 1e5)            # ln(p / bar): +2.3 at 10 bar, -9.2 at 1e-4 bar
+    t = 140.0 + 30.0 * np.tanh((x + 2.0) / 2.5)
+    return t + noise * rng.standard_normal(p_pa.shape)
+
+
+def make_job(tables: KTables, absorbers, *, nlayer, seed, iw0=0, nwave=None, theta_deg=0.0,
+             vmr_perturb=0.0, ld_lay=None, temp=None, xscale=None) -> Job:
+    """Nadir thermal-emission job on `nlayer` layers (10 -> 1e-4 bar).
+
+    State vector (NX = nlayer + len(absorbers)): model-0 temperature at each
+    level (xmap = 1) and one model-3 scale factor per absorber
+    (xmap = vmr * exp(x), nemesis/subprofretg.f:735-741)."""
+    rng = np.random.default_rng(seed)
+    L = int(nlayer)
+    ld = int(ld_lay or L)
+    p_lev, p_lay = _levels(L)
+    if temp is None:
+        temp = temperature_profile(p_lay, rng)
+    temp = np.asarray(temp, np.float64)
+    gases = [H2, HE] + list(absorbers)
+    ng_ = len(gases)
+    ncol = (p_lev[:-1] - p_lev[1:]) / (MMW * AMU * GRAV) * 1e-4          # molecules cm-2
+    H = KB * temp / (MMW * AMU * GRAV) / 1e3                                # km
+    delh = H * np.log(p_lev[:-1] / p_lev[1:])
+    vmr = np.zeros((L, ng_))
+    for k, g in enumerate(gases):
+        prof = np.full(L, VMR[g])
+        if vmr_perturb > 0 and k >= 2:
+            prof = prof * np.exp(vmr_perturb * rng.standard_normal(L))
+        vmr[:, k] = prof
+    if xscale is None:
+        xscale = np.zeros(len(absorbers))
+    xscale = np.asarray(xscale, np.float64)
+    vmr_eff = vmr.copy()
+    vmr_eff[:, 2:] *= np.exp(xscale)[None, :]
+    press_atm = (p_lay / 1e5 * BAR_TO_ATM).astype(np.float32)
+
+    def fa(shape):
+        return np.zeros(shape, np.float32, order="F")
+
+    pp = fa((ld, ng_))
+    amount = fa((ld, ng_))
+    pp[:L] = (vmr_eff * press_atm[:, None].astype(np.float64)).astype(np.float32)
+    amount[:L] = (vmr_eff * ncol[:, None]).astype(np.float32)
+    tab_of = {g: i for i, g in enumerate(tables.gases)}
+    ktab = np.array([tab_of.get(g, -1) for g in gases], np.int32)
+    nbin = int(tables.nbin[0])
+    if nwave is None:
+        nwave = nbin - iw0
+    vwave = (tables.vmin[0] + tables.delv[0] * np.arange(iw0, iw0 + nwave, dtype=np.float32)).astype(np.float32)
+    layinc = np.zeros((ld, 1), np.int32, order="F")
+    layinc[:L, 0] = np.arange(L, 0, -1)          # top layer first (atmg.f:348-352)
+    scale = fa((ld, 1))
+    scale[:L, 0] = np.float32(1.0 / np.cos(np.deg2rad(theta_deg)))
+    emtemp = fa((ld, 1))
+    emtemp[:L, 0] = temp.astype(np.float32)[layinc[:L, 0] - 1]
+    npro = L
+    dte = fa((ld, npro))
+    dam = fa((ld, npro))
+    idx = np.arange(L)
+    dte[idx, idx] = 1.0
+    dam[idx, idx] = ncol.astype(np.float32)
+    nparam = ng_ + 1
+    nv = L + len(absorbers)
+    xmap = np.zeros((nv, nparam, npro), np.float32, order="F")
+    xmap[idx, ng_, idx] = 1.0                                  # temperature, model 0
+    for a in range(len(absorbers)):
+        xmap[L + a, 2 + a, :] = (vmr[:, 2 + a] * np.exp(xscale[a])).astype(np.float32)
+    return Job(nlayer=L, ngas=ng_, npath=1, npro=npro, nv=nv, nwave=int(nwave), ld_lay=ld, ld_v=nv,
+               ld_param=nparam, press=np.ascontiguousarray(press_atm), temp=temp.astype(np.float32),
+               delh=delh.astype(np.float32), pp=pp, amount=amount,
+               idgas=np.array([g[0] for g in gases], np.int32), isogas=np.array([g[1] for g in gases], np.int32),
+               ktab=ktab, nlayin=np.array([L], np.int32), imod=np.array([3], np.int32), layinc=layinc,
+               scale=scale, emtemp=emtemp, dte=dte, dam=dam, xmap=xmap, vwave=vwave,
+               vem=np.array([0.0, 1e5], np.float32), emissivity=np.array([1.0, 1.0], np.float32),
+               vmr=vmr, ncol=ncol, xscale=xscale)
+
+
+def config1(seed=1001):
+    tables = make_ktables([CH4], np_=20, nt=10, ng=20, vmin=1200.0, delv=1.5, nbin=100, seed=seed)
+    job = make_job(tables, [CH4], nlayer=40, seed=seed + 1)
+    return tables, make_cia(seed), job
+
+
+def config2(seed=1002, nwave=None, nlayer=120, nbin=2000):
+    tables = make_ktables(ABSORBERS_C2, np_=20, nt=15, ng=20, vmin=600.0, delv=0.4, nbin=nbin, seed=seed)
+    job = make_job(tables, ABSORBERS_C2, nlayer=nlayer, seed=seed + 1, nwave=nwave, vmr_perturb=0.3)
+    return tables, make_cia(seed), job
+
+
+def config3_jobs(tables: KTables, nspec: int, seed=1003):
+    """Uneven batch: W ~ U[200, 2000] contiguous window of the config-2 grid,
+    L ~ U[40, 120], 1-4 absorbers from the config-2 set, theta ~ U[0, 70] deg."""
+    rng = np.random.default_rng(seed)
+    nbin = int(tables.nbin[0])
+    jobs = []
+    for s in range(nspec):
+        w = int(rng.integers(200, min(2000, nbin) + 1))
+        iw0 = int(rng.integers(0, nbin - w + 1))
+        L = int(rng.integers(40, 121))
+        na = int(rng.integers(1, 5))
+        absorbers = [ABSORBERS_C2[i] for i in sorted(rng.choice(4, size=na, replace=False))]
+        theta = float(rng.uniform(0.0, 70.0))
+        jobs.append(make_job(tables, absorbers, nlayer=L, seed=int(rng.integers(1 << 30)), iw0=iw0,
+                             nwave=w, theta_deg=theta, vmr_perturb=0.3))
+    return jobs

@@ -1,0 +1,315 @@
+"""Benchmark of the B200 CIRSRADG forward model + analytic Jacobian.
+
+Workload (one step): one nadir thermal-emission spectrum of 120 layers,
+H2/He + CH4, C2H6, C2H2, NH3 random-overlapped (NG = 20), 2000 wavenumbers,
+Jacobian over NX = 124 state elements -- the full-size single-spectrum
+configuration.  Inputs are the seeded synthetic workload of
+radtrancode_b200/synth.py (the reference measures on no public data set).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value`: spectra/s with inputs resident in HBM (CUDA events on the launching
+stream around K launches; the k-tables, 384 MB of raw + log k, exceed the
+126 MB L2, so no flush is needed between steps).  `e2e`: the same metric
+through the public C ABI call (rtb_cirsrtfg_wave) with host buffers, the
+host->device copy of the inputs and the device->host copy of the radiance
+and Jacobian inside the timed region.  Multi-GPU: one process per GPU
+(torchrun), every rank runs its own spectra (independent units, no data-path
+collective), weak scaling, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+Jacobian spectra/s & retrievals/s at ≤1e-4 rel err; retrieval p50/p99 ms"
+WORKLOAD = ("single spectrum, full size: 120 layers, H2/He + CH4/C2H6/C2H2/NH3 random overlap (NG=20), "
+            "2000 wavenumbers 600-1400 cm-1, k-tables 20P x 15T x 20g, Jacobian NX=124")
+CPU_SAMPLE_WAVES = 1000       # bounded CPU-baseline sample (half the spectrum)
+ACC_SAMPLE_WAVES = 48         # FP64-oracle accuracy sample
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the forward kernel from the committed ncu
+    summary (profiles/fwd_kernel_config2.md, line 'dram_bytes_per_launch:')."""
+    path = os.path.join(ROOT, "profiles", "fwd_kernel_config2.md")
+    try:
+        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def algorithmic_bytes(kt, job, in_bytes, out_bytes):
+    """Bytes a launch must move at least: every distinct (P, T) corner of the
+    ln k table touched by the layers' bilinear stencils, per gas and
+    wavenumber (NG values of 4 B, plus the g=0 raw value the KLOG test reads),
+    plus the CIA table cells touched, the packed inputs and the outputs."""
+    lnp = kt.lnp.astype(np.float32)
+    tk = kt.tk.astype(np.float32)
+    p1 = np.clip(np.log(job.press.astype(np.float64)).astype(np.float32), lnp[0], lnp[-1])
+    cp = np.clip(np.searchsorted(lnp, p1, side="right"), 1, kt.np_ - 1)
+    t1 = np.clip(job.temp, tk[0], tk[-1])
+    ct = np.clip(np.searchsorted(tk, t1, side="right"), 1, kt.nt - 1)
+    corners = set()
+    for a, b in zip(cp, ct):
+        for da in (-1, 0):
+            for db in (-1, 0):
+                corners.add((int(a) + da, int(b) + db))
+    ntabgas = int(np.sum(job.ktab >= 0))
+    table = ntabgas * job.nwave * len(corners) * (kt.ng * 4 + 4)
+    cia = job.nwave * 2 * 2 * 9 * 4 * len(set(int(x) for x in np.clip(job.temp // 15, 0, 24)))
+    return table + cia + in_bytes + out_bytes
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reference_arm(args, rank):
+    """The reference's CPU path on the host cores.  No Fortran compiler exists
+    here or on the GPU host, so the reference Fortran cannot be built; the
+    arm runs the oracle (the C++ restatement of the reference Fortran,
+    oracle/) on all host threads, each step a bounded sample of the same
+    workload."""
+    if rank != 0:
+        return
+    from oracle import pyoracle as po
+    from radtrancode_b200 import synth
+    kt, cia, job = synth.config2()
+    sample = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0, nwave=CPU_SAMPLE_WAVES,
+                            vmr_perturb=0.3)
+    nthr = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        po.cirsrtfg_wave(kt, cia, synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0,
+                                                 nwave=nthr, vmr_perturb=0.3), po.ORC_MIXED, nthreads=nthr)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        po.cirsrtfg_wave(kt, cia, sample, po.ORC_MIXED, nthreads=nthr)
+        times.append(time.perf_counter() - t)
+    t_step = statistics.mean(times)
+    frac = CPU_SAMPLE_WAVES / job.nwave
+    value = frac / t_step
+    out = {
+        "metric": METRIC, "value": value, "unit": "spectra/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3 / frac,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 transmissions)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"{CPU_SAMPLE_WAVES} of 2000 wavenumbers per step"},
+        "cpu_baseline": {"value": value, "unit": "spectra/s", "cores": nthr, "kind": "port",
+                         "sample": f"{CPU_SAMPLE_WAVES} of 2000 wavenumbers per step, {nthr} threads; "
+                                   "C++ restatement of the reference Fortran (no Fortran compiler on the host)"},
+        "e2e": {"value": value, "unit": "spectra/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(out))
+
+
+def cpu_baseline_and_accuracy(kt, cia, job, gpu_out):
+    """Rank-0 CPU baseline (oracle port on all host threads, bounded sample)
+    and the accuracy of the measured GPU result against the FP64 oracle on a
+    sample of the same spectrum."""
+    from oracle import pyoracle as po
+    from radtrancode_b200 import synth
+    nthr = os.cpu_count() or 1
+    sample = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0, nwave=CPU_SAMPLE_WAVES,
+                            vmr_perturb=0.3)
+    t = time.perf_counter()
+    po.cirsrtfg_wave(kt, cia, sample, po.ORC_MIXED, nthreads=nthr)
+    dt = time.perf_counter() - t
+    base = {"value": (CPU_SAMPLE_WAVES / job.nwave) / dt, "unit": "spectra/s", "cores": nthr, "kind": "port",
+            "sample": f"{CPU_SAMPLE_WAVES} of 2000 wavenumbers of the same spectrum, {nthr} threads, "
+                      "C++ restatement of the reference Fortran (no Fortran compiler on the host)"}
+    stride = job.nwave // ACC_SAMPLE_WAVES
+    acc_rad, acc_jac = 0.0, 0.0
+    c, g, _ = gpu_out
+    G = g.reshape(job.nv, job.nwave)
+    for iw0 in range(0, job.nwave, stride * 8):
+        sj = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=iw0, nwave=8, vmr_perturb=0.3)
+        c64, g64, _ = po.cirsrtfg_wave(kt, cia, sj, po.ORC_FP64, nthreads=min(nthr, 8))
+        acc_rad = max(acc_rad, float(np.max(np.abs(c[iw0:iw0 + 8] - c64) / np.abs(c64))))
+        R = g64.reshape(job.nv, 8)
+        scale = np.maximum(np.max(np.abs(G), axis=1, keepdims=True), 1e-300)
+        acc_jac = max(acc_jac, float(np.max(np.abs(G[:, iw0:iw0 + 8] - R) / scale)))
+    return base, {"radiance_max_rel_err": acc_rad, "jacobian_max_rel_err": acc_jac,
+                  "sample_wavenumbers": len(range(0, job.nwave, stride * 8)) * 8, "vs": "FP64 oracle"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from radtrancode_b200 import cirsradg, synth
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    kt, cia, _ = synth.config2()
+    # weak scaling: every rank its own spectrum (seeded by rank)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003 + 7919 * rank, nwave=2000,
+                         vmr_perturb=0.3)
+    ctx = cirsradg.Context(local)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.prepare([job])
+    for _ in range(args.warmup):
+        ctx.launch()
+    stream.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        ctx.launch()
+    ev1.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    gpu_out = ctx.fetch()[0]
+    st = ctx.stats()
+    ms_step = ms_total / args.steps
+    # e2e through the public C ABI with host buffers (wall clock per call;
+    # the call itself waits for its device->host copy)
+    ctx.set_stream(None)
+    for _ in range(max(1, args.warmup)):
+        ctx.cirsrtfg_wave(job)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.cirsrtfg_wave(job)
+    t_e2e = (time.perf_counter() - t0) / args.steps
+    barrier()
+    st_e2e = ctx.stats()
+    if world > 1:
+        tt = torch.tensor([ms_step, t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_step, t_e2e = float(tt[0]), float(tt[1])
+    if rank == 0:
+        hbm, how = peaks()
+        ab = algorithmic_bytes(kt, job, st_e2e["h2d_bytes"], st_e2e["d2h_bytes"])
+        achieved = ab / (ms_step * 1e-3) / 1e9
+        traffic = profile_traffic()
+        out = {
+            "metric": METRIC, "value": world * 1000.0 / ms_step, "unit": "spectra/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 g-weight scans)", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "spectra_per_step_per_gpu": 1,
+                       "l2": "inputs larger than L2: 384 MB of k-tables (raw + ln k) vs 126 MB L2, no flush",
+                       "parallelism": f"dp{world} (independent spectra per rank)"},
+            "e2e": {"value": world / t_e2e, "unit": "spectra/s", "h2d_bytes_per_step": st_e2e["h2d_bytes"],
+                    "d2h_bytes_per_step": st_e2e["d2h_bytes"]},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": f"{how} (MEASURED_PEAKS.json hbm_gbs, burst)",
+                         "algorithmic_bytes_per_launch": ab, "kernel": "fwd_kernel"},
+            "overlap_passes": {"sorted": st["sort_passes"], "with_ties": st["tie_passes"],
+                               "reference_heapsort": st["exact_passes"], "irregular": st["irregular_passes"]},
+            "clocks": clk,
+        }
+        if world == 1:
+            base, acc = cpu_baseline_and_accuracy(kt, cia, job, gpu_out)
+            out["cpu_baseline"] = base
+            out["accuracy"] = acc
+        print(json.dumps(out))
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

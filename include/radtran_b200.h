@@ -163,6 +163,22 @@ int rtb_cirsrtfg_wave_batch(rtb_context* ctx, int nspec, const rtb_atm* atms,
                             float* const* calcout, float* const* gradients,
                             float* const* gradtsurf);
 
+/* The same call split in three, for callers that keep a batch resident on
+ * the device and replay it (a retrieval re-running its forward model, a
+ * benchmark timing the kernel alone):
+ *   rtb_fwd_prepare  validate, pack and upload the batch (synchronous);
+ *   rtb_fwd_launch   run the forward kernel on the resident batch,
+ *                    asynchronously on the context's stream;
+ *   rtb_fwd_fetch    wait, then copy the outputs to the caller's buffers.
+ * rtb_set_stream makes the context issue its work on a caller-owned CUDA
+ * stream (a cudaStream_t passed as an opaque pointer; NULL restores the
+ * context's own stream). */
+int rtb_fwd_prepare(rtb_context* ctx, int nspec, const rtb_atm* atms);
+int rtb_fwd_launch(rtb_context* ctx);
+int rtb_fwd_fetch(rtb_context* ctx, float* const* calcout, float* const* gradients,
+                  float* const* gradtsurf);
+int rtb_set_stream(rtb_context* ctx, void* stream);
+
 /* Diagnostics of the last forward call: (wavenumber, layer) cells, overlap
  * passes that sorted, passes with tied sort keys, passes that took the
  * reference heapsort (a tie that could move a g-bin boundary, a NaN key, or
@@ -171,6 +187,7 @@ int rtb_cirsrtfg_wave_batch(rtb_context* ctx, int nspec, const rtb_atm* atms,
  * the forward kernel. */
 typedef struct rtb_fwd_stats {
     long long cells, sort_passes, tie_passes, exact_passes, irregular_passes;
+    long long h2d_bytes, d2h_bytes;   /* host<->device bytes of the call */
     float ms_kernel;
 } rtb_fwd_stats;
 int rtb_get_fwd_stats(const rtb_context* ctx, rtb_fwd_stats* out);

@@ -61,6 +61,7 @@ def lib():
         L.orc_locate.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_float]
         L.orc_calc_phiret.restype = C.c_float
         L.orc_calc_phiret_diag.restype = C.c_float
+        L.orc_dinvertm_chol.restype = C.c_int
         _lib = L
     return _lib
 

@@ -57,6 +57,14 @@ def lib() -> C.CDLL:
         L.rtb_set_debug.restype = C.c_int
         L.rtb_set_strict_ties.argtypes = [vp, C.c_int]
         L.rtb_set_strict_ties.restype = C.c_int
+        L.rtb_fwd_prepare.argtypes = [vp, C.c_int, C.POINTER(_abi.RtbAtm)]
+        L.rtb_fwd_prepare.restype = C.c_int
+        L.rtb_fwd_launch.argtypes = [vp]
+        L.rtb_fwd_launch.restype = C.c_int
+        L.rtb_fwd_fetch.argtypes = [vp, C.POINTER(fp), C.POINTER(fp), C.POINTER(fp)]
+        L.rtb_fwd_fetch.restype = C.c_int
+        L.rtb_set_stream.argtypes = [vp, vp]
+        L.rtb_set_stream.restype = C.c_int
         p16 = C.POINTER(C.c_int16)
         L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
         L.rtb_get_debug_bins.restype = C.c_int
@@ -68,5 +76,6 @@ def lib() -> C.CDLL:
 EXPORTED = [
     "rtb_create", "rtb_destroy", "rtb_last_error", "rtb_version", "rtb_set_ktables", "rtb_set_cia",
     "rtb_cirsrtfg_wave", "rtb_cirsrtfg_wave_batch", "rtb_get_fwd_stats", "rtb_set_debug",
-    "rtb_get_debug_bins", "rtb_set_strict_ties",
+    "rtb_get_debug_bins", "rtb_set_strict_ties", "rtb_fwd_prepare", "rtb_fwd_launch", "rtb_fwd_fetch",
+    "rtb_set_stream",
 ]

@@ -108,6 +108,40 @@ class Context:
         self._check(self._L.rtb_cirsrtfg_wave_batch(self._h, n, structs, p1, p2, p3))
         return outs
 
+    # -- resident batch: prepare once, launch many times ------------------
+    def prepare(self, jobs):
+        n = len(jobs)
+        structs = (_abi.RtbAtm * n)()
+        self._prepared_keep = []
+        for i, j in enumerate(jobs):
+            s = j.as_struct()
+            self._prepared_keep.append(s)
+            structs[i] = s
+        self._check(self._L.rtb_fwd_prepare(self._h, n, structs))
+        self._prepared_jobs = list(jobs)
+
+    def launch(self):
+        self._check(self._L.rtb_fwd_launch(self._h))
+
+    def fetch(self):
+        jobs = self._prepared_jobs
+        n = len(jobs)
+        outs = []
+        fp = C.POINTER(C.c_float)
+        p1, p2, p3 = (fp * n)(), (fp * n)(), (fp * n)()
+        for i, j in enumerate(jobs):
+            a, b, c = j.out_shapes()
+            o = (np.zeros(a, np.float32), np.zeros(b, np.float32), np.zeros(c, np.float32))
+            outs.append(o)
+            p1[i], p2[i], p3[i] = _abi.fptr(o[0]), _abi.fptr(o[1]), _abi.fptr(o[2])
+        self._check(self._L.rtb_fwd_fetch(self._h, p1, p2, p3))
+        return outs
+
+    def set_stream(self, handle):
+        """Issue the context's work on a caller-owned cudaStream_t (int handle,
+        e.g. torch.cuda.Stream().cuda_stream); None restores the own stream."""
+        self._check(self._L.rtb_set_stream(self._h, C.c_void_p(handle) if handle else None))
+
     def stats(self) -> dict:
         s = _abi.RtbFwdStats()
         self._check(self._L.rtb_get_fwd_stats(self._h, C.byref(s)))

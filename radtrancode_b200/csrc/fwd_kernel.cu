@@ -895,8 +895,10 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
                     if (y >= 88.7f) y = 88.7f;
                     const float e = (float)exp((double)y);
                     float out, dr;
+                    // IMOD 0: dcoutdq = -tau*T*dtau/dq; IMOD 1: tau*(1-A)*dtau/dq with
+                    // 1-A formed as T itself (no cancellation when T < 2^-25)
                     if (im == 0) { out = e; dr = -tsum * e; }
-                    else { out = 1.0f - e; dr = tsum * (1.0f - out); }
+                    else { out = 1.0f - e; dr = tsum * e; }
                     for (int j = 0; j < nlays; ++j) { drdt[j * ng + g] = dr; trd[j * ng + g] = 0.0f; }
                     rad[g] = out;
                     gts[g] = 0.0f;

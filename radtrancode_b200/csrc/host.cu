@@ -100,6 +100,16 @@ struct rtb_context {
     // options and diagnostics
     int strict_ties = 0;
     int debug = 0;
+    cudaStream_t user_stream = nullptr;   // caller-provided stream (NULL: own stream)
+    // resident batch (rtb_fwd_prepare)
+    int prepared = 0;
+    BatchDev B{};
+    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, grid = 1;
+    std::vector<SpecDev> spec_host;
+    std::vector<int> spec_npath, spec_nv, spec_nwave, spec_nlayer;
+    int64_t n_out = 0, n_jac = 0;
+    size_t in_bytes = 0, out_bytes = 0;
+    long long cells = 0;
     DevBuf d_dbg_perm, d_dbg_split;
     size_t dbg_perm_n = 0, dbg_split_n = 0;
     rtb_fwd_stats stats{};
@@ -542,25 +552,26 @@ size_t bytes_of(const std::vector<T>& v) {
     return v.size() * sizeof(T);
 }
 
-int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calcout, float* const* gradients,
-              float* const* gradtsurf) {
+cudaStream_t stream_of(rtb_context* c) { return c->user_stream ? c->user_stream : c->stream; }
+
+// pack + upload a batch; the device copy stays resident until the next prepare
+int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
     if (!c || nspec <= 0 || !atms) return fail(c, RTB_ERR_ARG, "bad batch arguments");
     if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
     if (c->ng > 22 || c->ng < 2) return fail(c, RTB_ERR_UNSUPPORTED, "NG=%d outside the device range 2..22", c->ng);
     CUDA_TRY(c, cudaSetDevice(c->device));
+    c->prepared = 0;
     Staging st;
     st.item_start.push_back(0);
     for (int s = 0; s < nspec; ++s) {
         const int r = pack_spectrum(c, atms[s], st);
         if (r) return r;
     }
-    // smem budget
     const int smem = fwd_smem_bytes(c->ng, st.Lmax, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max);
     int smem_max = 0;
     CUDA_TRY(c, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     if (smem > smem_max)
         return fail(c, RTB_ERR_UNSUPPORTED, "spectrum needs %d B of shared memory (device %d)", smem, smem_max);
-    // pack inputs into one pinned buffer
     struct Seg {
         const void* src;
         size_t n;
@@ -591,16 +602,16 @@ int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calc
     const size_t in_bytes = off + 256;
     CUDA_TRY(c, c->h_in.ensure(in_bytes));
     CUDA_TRY(c, c->d_in.ensure(in_bytes));
-    for (const auto& s : segs)
-        if (s.n) memcpy((char*)c->h_in.p + s.off, s.src, s.n);
-    CUDA_TRY(c, cudaMemcpyAsync(c->d_in.p, c->h_in.p, off, cudaMemcpyHostToDevice, c->stream));
+    for (const auto& sg : segs)
+        if (sg.n) memcpy((char*)c->h_in.p + sg.off, sg.src, sg.n);
+    const cudaStream_t strm = stream_of(c);
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_in.p, c->h_in.p, off, cudaMemcpyHostToDevice, strm));
     const size_t out_bytes = (size_t)(2 * st.n_out + st.n_jac) * sizeof(float);
     CUDA_TRY(c, c->d_out.ensure(out_bytes));
     CUDA_TRY(c, c->h_out.ensure(out_bytes));
     CUDA_TRY(c, c->d_diag.ensure(64));
-    CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, c->stream));
     auto dp = [&](size_t i) { return (const void*)((const char*)c->d_in.p + segs[i].off); };
-    BatchDev B;
+    BatchDev& B = c->B;
     memset(&B, 0, sizeof B);
     B.nspec = nspec;
     B.nitems = st.item_start.back();
@@ -618,7 +629,6 @@ int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calc
     B.map_colptr = (const int*)dp(i_mc);
     B.map_row = (const int*)dp(i_mr);
     B.map_val = (const float*)dp(i_mv);
-    // map_colptr entries are relative to this batch's map_row array: absolute already
     B.ktab_raw = (const float*)c->d_raw.p;
     B.ktab_log = (const float*)c->d_log.p;
     B.np = c->np;
@@ -641,43 +651,90 @@ int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calc
         c->dbg_split_n = (size_t)a0.nwave * a0.nlayer * npass * c->ng;
         CUDA_TRY(c, c->d_dbg_perm.ensure(c->dbg_perm_n * 2));
         CUDA_TRY(c, c->d_dbg_split.ensure(c->dbg_split_n * 2));
-        CUDA_TRY(c, cudaMemsetAsync(c->d_dbg_perm.p, 0xff, c->dbg_perm_n * 2, c->stream));
-        CUDA_TRY(c, cudaMemsetAsync(c->d_dbg_split.p, 0xff, c->dbg_split_n * 2, c->stream));
+        CUDA_TRY(c, cudaMemsetAsync(c->d_dbg_perm.p, 0xff, c->dbg_perm_n * 2, strm));
+        CUDA_TRY(c, cudaMemsetAsync(c->d_dbg_split.p, 0xff, c->dbg_split_n * 2, strm));
         B.dbg_perm = (int16_t*)c->d_dbg_perm.p;
         B.dbg_split = (int16_t*)c->d_dbg_split.p;
     }
-    const int per_sm = 2;
-    int64_t grid = (int64_t)c->nsm * per_sm;
+    int64_t grid = (int64_t)c->nsm * 2;
     if (grid > B.nitems) grid = B.nitems;
-    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-    CUDA_TRY(c, launch_fwd(B, st.Lmax, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max, (int)grid, c->stream));
-    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
-    CUDA_TRY(c, cudaMemcpyAsync(c->h_out.p, c->d_out.p, out_bytes, cudaMemcpyDeviceToHost, c->stream));
+    c->grid = (int)grid;
+    c->Lmax = st.Lmax;
+    c->nsw_max = st.nsw_max;
+    c->ncol_max = st.ncol_max;
+    c->nlmax_max = st.nlmax_max;
+    c->npath_max = st.npath_max;
+    c->spec_host = st.spec;
+    c->spec_npath.clear();
+    c->spec_nv.clear();
+    c->spec_nwave.clear();
+    c->spec_nlayer.clear();
+    c->cells = 0;
+    for (int s = 0; s < nspec; ++s) {
+        c->spec_npath.push_back(atms[s].npath);
+        c->spec_nv.push_back(atms[s].nv);
+        c->spec_nwave.push_back(atms[s].nwave);
+        c->spec_nlayer.push_back(atms[s].nlayer);
+        c->cells += (long long)atms[s].nlayer * atms[s].nwave;
+    }
+    c->n_out = st.n_out;
+    c->n_jac = st.n_jac;
+    c->in_bytes = off;
+    c->out_bytes = out_bytes;
+    c->prepared = 1;
+    return RTB_OK;
+}
+
+int launch(rtb_context* c) {
+    if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const cudaStream_t strm = stream_of(c);
+    CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, strm));
+    CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
+    CUDA_TRY(c, launch_fwd(c->B, c->Lmax, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, strm));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, strm));
+    return RTB_OK;
+}
+
+int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float* const* gradtsurf) {
+    if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const cudaStream_t strm = stream_of(c);
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_out.p, c->d_out.p, c->out_bytes, cudaMemcpyDeviceToHost, strm));
     unsigned long long diag[8];
-    CUDA_TRY(c, cudaMemcpyAsync(diag, c->d_diag.p, 64, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(diag, c->d_diag.p, 64, cudaMemcpyDeviceToHost, strm));
+    CUDA_TRY(c, cudaStreamSynchronize(strm));
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     const unsigned status = (unsigned)(diag[0] & 0xffffffffu);
-    c->stats.cells = 0;
-    for (int s = 0; s < nspec; ++s) c->stats.cells += (long long)atms[s].nlayer * atms[s].nwave;
+    c->stats.cells = c->cells;
     c->stats.sort_passes = (long long)diag[1];
     c->stats.tie_passes = (long long)diag[2];
     c->stats.exact_passes = (long long)diag[3];
     c->stats.irregular_passes = (long long)diag[4];
     c->stats.ms_kernel = ms;
+    c->stats.h2d_bytes = (long long)c->in_bytes;
+    c->stats.d2h_bytes = (long long)c->out_bytes;
     if (status & kStGord) return fail(c, RTB_ERR_GORD, "g-ordinate walk ran past NG (rankg.f:118-147)");
-    // scatter outputs to the caller's buffers
     const float* h = (const float*)c->h_out.p;
-    for (int s = 0; s < nspec; ++s) {
-        const SpecDev& S = st.spec[s];
-        const rtb_atm& a = atms[s];
-        const size_t no = (size_t)a.npath * a.nwave, nj = (size_t)a.npath * a.nv * a.nwave;
+    for (size_t s = 0; s < c->spec_host.size(); ++s) {
+        const SpecDev& S = c->spec_host[s];
+        const size_t no = (size_t)c->spec_npath[s] * c->spec_nwave[s];
+        const size_t nj = (size_t)c->spec_npath[s] * c->spec_nv[s] * c->spec_nwave[s];
         if (calcout && calcout[s]) memcpy(calcout[s], h + S.out_off, no * sizeof(float));
-        if (gradtsurf && gradtsurf[s]) memcpy(gradtsurf[s], h + st.n_out + S.out_off, no * sizeof(float));
-        if (gradients && gradients[s]) memcpy(gradients[s], h + 2 * st.n_out + S.jac_off, nj * sizeof(float));
+        if (gradtsurf && gradtsurf[s]) memcpy(gradtsurf[s], h + c->n_out + S.out_off, no * sizeof(float));
+        if (gradients && gradients[s]) memcpy(gradients[s], h + 2 * c->n_out + S.jac_off, nj * sizeof(float));
     }
     return RTB_OK;
+}
+
+int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calcout, float* const* gradients,
+              float* const* gradtsurf) {
+    int r = prepare(c, nspec, atms);
+    if (r) return r;
+    r = launch(c);
+    if (r) return r;
+    return fetch(c, calcout, gradients, gradtsurf);
 }
 
 }  // namespace
@@ -814,6 +871,20 @@ int rtb_cirsrtfg_wave(rtb_context* c, const rtb_atm* atm, float* calcout, float*
 int rtb_cirsrtfg_wave_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calcout,
                             float* const* gradients, float* const* gradtsurf) {
     return run_batch(c, nspec, atms, calcout, gradients, gradtsurf);
+}
+
+int rtb_fwd_prepare(rtb_context* c, int nspec, const rtb_atm* atms) { return prepare(c, nspec, atms); }
+
+int rtb_fwd_launch(rtb_context* c) { return launch(c); }
+
+int rtb_fwd_fetch(rtb_context* c, float* const* calcout, float* const* gradients, float* const* gradtsurf) {
+    return fetch(c, calcout, gradients, gradtsurf);
+}
+
+int rtb_set_stream(rtb_context* c, void* stream) {
+    if (!c) return RTB_ERR_ARG;
+    c->user_stream = (cudaStream_t)stream;
+    return RTB_OK;
 }
 
 int rtb_get_fwd_stats(const rtb_context* c, rtb_fwd_stats* out) {

@@ -205,9 +205,8 @@ def make_job(tables: KTables, absorbers, *, nlayer, seed, iw0=0, nwave=None, the
     L = int(nlayer)
     ld = int(ld_lay or L)
     p_lev, p_lay = _levels(L)
-    if temp is None:
-        temp = temperature_profile(p_lay, rng)
-    temp = np.asarray(temp, np.float64)
+    t_default = temperature_profile(p_lay, rng)     # always drawn: keeps the seeded stream aligned
+    temp = t_default if temp is None else np.asarray(temp, np.float64)
     gases = [H2, HE] + list(absorbers)
     ng_ = len(gases)
     ncol = (p_lev[:-1] - p_lev[1:]) / (MMW * AMU * GRAV) * 1e-4          # molecules cm-2

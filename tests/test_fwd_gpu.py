@@ -1,0 +1,188 @@
+"""GPU parity tests of the forward model + Jacobian against the oracle.
+
+Every comparison runs the CUDA kernels through the C ABI (radtrancode_b200
+Context -> libradtran_b200.so) and the oracle on the same seeded inputs.
+Tolerances: tests/helpers.py."""
+import copy
+import os
+
+import numpy as np
+import pytest
+
+from radtrancode_b200 import synth
+from tests.helpers import JAC_TOL, RAD_TOL, assignment, jac_err, rad_err
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _run(ctx, kt, cia, job):
+    ctx.set_ktables(kt)
+    if cia is not None:
+        ctx.set_cia(cia)
+    return ctx.cirsrtfg_wave(job)
+
+
+def test_config1_against_fp64_oracle_and_golden(ctx, oracle):
+    kt, cia, job = synth.config1()
+    c, g, gt = _run(ctx, kt, cia, job)
+    gold = np.load(os.path.join(GOLDEN, "c1.npz"))
+    assert rad_err(c, gold["calcout64"]) <= RAD_TOL
+    assert jac_err(g, gold["gradients64"], job.nv) <= JAC_TOL
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+    assert np.max(np.abs(gt - gt64)) <= RAD_TOL * np.max(np.abs(gt64))
+
+
+@pytest.mark.parametrize("strict", [False, True])
+def test_config2_small_bins_bit_exact(ctx, oracle, strict):
+    """Integer g-bin assignment of every sorted overlap pass identical to the
+    mixed-precision oracle (the reference's REAL/DOUBLE semantics)."""
+    kt, cia, job = synth.config2(nwave=16, nlayer=60, nbin=16)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_strict_ties(strict)
+    ctx.set_debug(True)
+    try:
+        c, g, gt = ctx.cirsrtfg_wave(job)
+        perm, split = ctx.debug_bins(job)
+        st = ctx.stats()
+    finally:
+        ctx.set_debug(False)
+        ctx.set_strict_ties(False)
+    (c0, g0, gt0), (operm, osplit, oties) = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED, debug=True)
+    assert st["sort_passes"] == int((operm[..., 0] >= 0).sum())
+    assert st["tie_passes"] == int((oties > 0).sum())
+    a_gpu = assignment(perm, split, kt.ng)
+    a_orc = assignment(operm, osplit, kt.ng)
+    assert np.array_equal(a_gpu, a_orc)
+    assert np.array_equal(split, osplit)
+    if strict:
+        # every pass with a tie took the reference heapsort: the whole order matches
+        assert np.array_equal(perm, operm)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+
+
+def test_config2_golden_fixture(ctx):
+    kt, cia, job = synth.config2(nwave=8, nlayer=30, nbin=8)
+    c, g, gt = _run(ctx, kt, cia, job)
+    gold = np.load(os.path.join(GOLDEN, "c2s.npz"))
+    assert rad_err(c, gold["calcout64"]) <= RAD_TOL
+    assert jac_err(g, gold["gradients64"], job.nv) <= JAC_TOL
+
+
+def test_fortran_leading_dimensions(ctx, oracle):
+    """Arrays dimensioned MAXLAY x MAXGAS etc. as the COMMON blocks hold them."""
+    kt, cia, _ = synth.config2(nwave=6, nlayer=30, nbin=6)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=30, seed=9, nwave=6, ld_lay=400)
+    c, g, gt = _run(ctx, kt, cia, job)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+
+
+@pytest.mark.parametrize("variant", ["tsurf", "rayleigh", "slant", "imod0", "imod1", "limb", "two_paths",
+                                     "no_cia"])
+def test_path_variants(ctx, oracle, variant):
+    kt, cia, _ = synth.config2(nwave=5, nlayer=24, nbin=5)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=24, seed=21, nwave=5)
+    use_cia = cia
+    if variant == "tsurf":
+        job.tsurf = 175.0
+        job.vem = np.array([500.0, 1500.0], np.float32)
+        job.emissivity = np.array([0.9, 0.7], np.float32)
+    elif variant == "rayleigh":
+        job.iray = 1
+    elif variant == "slant":
+        job.scale[:job.nlayer, 0] = 1.7
+    elif variant in ("imod0", "imod1"):
+        job.imod[0] = int(variant[-1])
+    elif variant == "limb":
+        # path goes down then up again: the bottom of the path is not the deepest layer
+        L = job.nlayer
+        half = np.arange(L, L // 2, -1)
+        job.layinc[:, 0] = 0
+        path = np.concatenate([half, half[::-1]])
+        job.layinc[:path.size, 0] = path
+        job.nlayin[0] = path.size
+        job.emtemp[:path.size, 0] = job.temp[path - 1]
+        job.scale[:path.size, 0] = 1.0
+    elif variant == "two_paths":
+        j2 = copy.deepcopy(job)
+        L = job.nlayer
+        lay = np.zeros((L, 2), np.int32, order="F")
+        lay[:, 0] = job.layinc[:L, 0]
+        lay[:, 1] = job.layinc[:L, 0]
+        sc = np.zeros((L, 2), np.float32, order="F")
+        sc[:, 0] = 1.0
+        sc[:, 1] = 2.0
+        em = np.zeros((L, 2), np.float32, order="F")
+        em[:, 0] = job.emtemp[:L, 0]
+        em[:, 1] = job.emtemp[:L, 0]
+        j2.npath, j2.layinc, j2.scale, j2.emtemp = 2, lay, sc, em
+        j2.nlayin = np.array([L, L], np.int32)
+        j2.imod = np.array([3, 3], np.int32)
+        job = j2
+    elif variant == "no_cia":
+        use_cia = None
+    if use_cia is None:
+        # a fresh context: the device context keeps a CIA table once loaded
+        from radtrancode_b200 import cirsradg
+        with cirsradg.Context(0) as c2:
+            c2.set_ktables(kt)
+            c, g, gt = c2.cirsrtfg_wave(job)
+    else:
+        c, g, gt = _run(ctx, kt, use_cia, job)
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, use_cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.npath * job.nv) <= JAC_TOL
+    if variant == "tsurf":
+        assert np.max(np.abs(gt - gt64)) <= RAD_TOL * np.max(np.abs(gt64))
+
+
+def test_unsupported_options_raise(ctx):
+    from radtrancode_b200 import cirsradg
+    kt, cia, job = synth.config1()
+    ctx.set_ktables(kt)
+    j = copy.deepcopy(job)
+    j.imod[0] = 15
+    with pytest.raises(cirsradg.RtbError, match="UNSUPPORTED"):
+        ctx.cirsrtfg_wave(j)
+    j = copy.deepcopy(job)
+    j.vwave = j.vwave + np.float32(0.7)        # between table wavenumbers
+    with pytest.raises(cirsradg.RtbError, match="UNSUPPORTED"):
+        ctx.cirsrtfg_wave(j)
+    j = copy.deepcopy(job)
+    j.vem = np.array([1250.0, 1300.0], np.float32)   # interpem.f range error
+    with pytest.raises(cirsradg.RtbError, match="RANGE"):
+        ctx.cirsrtfg_wave(j)
+
+
+def test_full_size_config2_properties(ctx):
+    """Full config-2 size (120 layers, 4 absorbers, 2000 wavenumbers), where
+    the oracle is too slow to run in a test: size-independent properties --
+    finite positive radiance bounded by the Planck envelope of the profile,
+    determinism, and agreement with the same spectrum computed in pieces."""
+    kt, cia, job = synth.config2()
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c, g, gt = ctx.cirsrtfg_wave(job)
+    c2, g2, gt2 = ctx.cirsrtfg_wave(job)
+    assert np.array_equal(c, c2) and np.array_equal(g, g2)
+    assert np.all(np.isfinite(c)) and np.all(c > 0) and np.all(np.isfinite(g))
+    v = job.vwave.astype(np.float64)
+    c1_, c2_ = 1.1911e-12, 1.439
+    Bmin = c1_ * v ** 3 / np.expm1(c2_ * v / job.temp.min())
+    Bmax = c1_ * v ** 3 / np.expm1(c2_ * v / job.temp.max())
+    assert np.all(c >= 0.999 * Bmin) and np.all(c <= 1.001 * Bmax)
+    # the same wavenumbers in two halves give identical results (no cross-wavenumber state)
+    j1 = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0, nwave=1000, vmr_perturb=0.3)
+    j2 = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=1000, nwave=1000, vmr_perturb=0.3)
+    ca, ga, _ = ctx.cirsrtfg_wave(j1)
+    cb, gb, _ = ctx.cirsrtfg_wave(j2)
+    assert np.array_equal(np.concatenate([ca, cb]), c)
+    G = g.reshape(job.nv, -1)
+    assert np.array_equal(np.concatenate([ga.reshape(job.nv, -1), gb.reshape(job.nv, -1)], axis=1), G)

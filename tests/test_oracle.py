@@ -1,0 +1,252 @@
+"""CPU tests of the oracle (the C++ restatement in oracle/): known-answer
+tests, finite differences, invariants and the committed golden fixtures."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from radtrancode_b200 import synth
+from tests.helpers import jac_err, rad_err
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _golden_input_digest(kt, cia, job):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mg", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.input_digest(kt, cia, job), mg
+
+
+# ---------------------------------------------------------------- det exp
+def test_detexp_matches_golden_bits(oracle):
+    g = np.load(os.path.join(GOLDEN, "detexp.npz"))
+    y = oracle.det_expf(g["x"])
+    assert np.array_equal(y.view(np.uint32), g["y"].view(np.uint32))
+
+
+def test_detexp_is_correctly_rounded_almost_everywhere(oracle):
+    x = np.random.default_rng(3).uniform(-30.0, 30.0, 20000).astype(np.float32)
+    y = oracle.det_expf(x)
+    ref = np.exp(x.astype(np.float64)).astype(np.float32)
+    ulps = np.abs(y.view(np.int32).astype(np.int64) - ref.view(np.int32).astype(np.int64))
+    assert ulps.max() <= 1
+    assert (ulps == 0).mean() > 0.9999
+
+
+# ---------------------------------------------------------------- locate
+def test_locate_endpoint_snapping(oracle):
+    import ctypes as C
+    xx = np.array([1.0, 2.0, 3.0, 4.0], np.float32)
+    p = xx.ctypes.data_as(C.POINTER(C.c_float))
+    L = oracle.lib()
+    assert L.orc_locate(p, 4, 1.0) == 1          # x == xx(1) -> 1
+    assert L.orc_locate(p, 4, 4.0) == 3          # x == xx(n) -> n-1
+    assert L.orc_locate(p, 4, 2.5) == 2
+    assert L.orc_locate(p, 4, 0.5) == 0          # below range
+    assert L.orc_locate(p, 4, 9.0) == 4          # above range
+    xd = xx[::-1].copy()
+    pd = xd.ctypes.data_as(C.POINTER(C.c_float))
+    assert L.orc_locate(pd, 4, 2.5) == 2         # decreasing table
+
+
+# ---------------------------------------------------------------- heapsort
+def _nr_heapsort_py(ra):
+    """Independent pure-Python restatement of sort2g.f for small arrays."""
+    ra = [None] + list(ra)
+    ib = [None] + list(range(len(ra) - 1))
+    n = len(ra) - 1
+    L, IR = n // 2 + 1, n
+    while True:
+        if L > 1:
+            L -= 1
+            rra, irb = ra[L], ib[L]
+        else:
+            rra, irb = ra[IR], ib[IR]
+            ra[IR], ib[IR] = ra[1], ib[1]
+            IR -= 1
+            if IR == 1:
+                ra[1], ib[1] = rra, irb
+                return ra[1:], ib[1:]
+        i, j = L, L + L
+        while j <= IR:
+            if j < IR and ra[j] < ra[j + 1]:
+                j += 1
+            if rra < ra[j]:
+                ra[i], ib[i] = ra[j], ib[j]
+                i, j = j, j + j
+            else:
+                j = IR + 1
+        ra[i], ib[i] = rra, irb
+
+
+@pytest.mark.parametrize("n,levels", [(2, 2), (7, 3), (50, 5), (400, 40), (400, 400)])
+def test_sort2g_matches_python_heapsort_with_ties(oracle, n, levels):
+    rng = np.random.default_rng(n + levels)
+    a = rng.integers(0, levels, n).astype(np.float32)
+    s, ib = oracle.sort2g(a)
+    s_py, ib_py = _nr_heapsort_py(a.tolist())
+    assert np.array_equal(s, np.array(s_py, np.float32))
+    assert np.array_equal(ib, np.array(ib_py))
+    assert np.all(np.diff(s) >= 0)
+
+
+# ---------------------------------------------------------------- rankg
+def test_rankg_conserves_weighted_k_and_is_monotone(oracle):
+    ng = 20
+    _, delg = synth.gauss_legendre_01(ng)
+    rng = np.random.default_rng(11)
+    k1 = np.sort(rng.lognormal(0, 2, ng)).astype(np.float32)
+    k2 = np.sort(rng.lognormal(-1, 2, ng)).astype(np.float32)
+    cont = (k1[:, None] + k2[None, :]).astype(np.float32).ravel()
+    weight = (delg[:, None] * delg[None, :]).astype(np.float32).ravel()
+    grad = np.stack([np.repeat(k1, ng), np.tile(k2, ng)]).astype(np.float32)
+    st, k_g, dkdq, perm, split = oracle.rankg(delg, weight, cont, grad)
+    assert st == 0
+    assert np.all(np.diff(k_g) >= 0)
+    lhs = float(np.sum(k_g.astype(np.float64) * delg))
+    rhs = float(np.sum(cont.astype(np.float64) * weight))
+    assert abs(lhs - rhs) / rhs < 1e-5
+    assert sorted(perm.tolist()) == list(range(ng * ng))
+    closed = split[split >= 0]
+    assert closed.size >= ng - 1 and np.all(np.diff(closed) > 0)
+
+
+# ---------------------------------------------------------------- forward KATs
+def test_golden_fixtures_reproduced(oracle):
+    for name, (kt, cia, job) in [("c1", synth.config1()), ("c2s", synth.config2(nwave=8, nlayer=30, nbin=8))]:
+        g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+        dig, _ = _golden_input_digest(kt, cia, job)
+        assert str(g["input_sha256"]) == dig, f"{name}: synthetic generator changed"
+        (c, gr, gt), (perm, split, ties) = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED, debug=True)
+        assert np.array_equal(c, g["calcout"]) and np.array_equal(gr, g["gradients"])
+        c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+        assert np.array_equal(c64, g["calcout64"]) and np.array_equal(g64, g["gradients64"])
+        if perm is not None:
+            assert hashlib.sha256(perm.tobytes()).hexdigest() == str(g["perm_sha256"])
+            assert np.array_equal(split, g["split"])
+
+
+def _isothermal(job, T):
+    job.temp[:] = T
+    job.emtemp[:job.nlayer, 0] = T
+    return job
+
+
+def test_isothermal_atmosphere_radiates_planck(oracle):
+    kt, cia, job = synth.config2(nwave=6, nlayer=24, nbin=6)
+    job = _isothermal(job, 150.0)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    v = job.vwave.astype(np.float64)
+    c1, c2 = float(np.float32(1.1911e-12)), float(np.float32(1.439))
+    # every g-ordinate radiates B(T); the quadrature weights (REAL) sum to 1 +- 1 ulp
+    B = c1 * v ** 3 / np.expm1(c2 * v / 150.0) * float(np.sum(kt.delg.astype(np.float64)))
+    assert np.max(np.abs(c64 - B) / B) < 1e-12
+    G = g64.reshape(job.nv, -1)
+    L = job.nlayer
+    # gas-scale columns vanish for an isothermal atmosphere over a B(T) surface
+    assert np.max(np.abs(G[L:])) < 1e-12 * np.max(np.abs(G[:L]))
+
+
+def test_zero_table_gas_leaves_result_unchanged(oracle):
+    kt, cia, job1 = synth.config2(nwave=6, nlayer=20, nbin=6)
+    kt_z = synth.KTables(kt.np_, kt.nt, kt.ng, kt.lnp, kt.tk, kt.g_ord, kt.delg, kt.vmin, kt.delv, kt.nbin,
+                         kt.data.copy(), kt.gases)
+    kt_z.table(1)[:] = 0.0     # C2H6 table all zero: get_kg.f:228-250 zero probe, noverlapg skip branch
+    kt_1 = synth.KTables(kt.np_, kt.nt, kt.ng, kt.lnp, kt.tk, kt.g_ord, kt.delg, kt.vmin[:1], kt.delv[:1],
+                         kt.nbin[:1], kt.table(0).ravel().copy(), kt.gases[:1])
+    job_a = synth.make_job(kt_z, [synth.CH4, synth.C2H6], nlayer=20, seed=5, nwave=6)
+    job_b = synth.make_job(kt_1, [synth.CH4], nlayer=20, seed=5, nwave=6)
+    ca, ga, _ = oracle.cirsrtfg_wave(kt_z, cia, job_a, oracle.ORC_MIXED)
+    cb, gb, _ = oracle.cirsrtfg_wave(kt_1, cia, job_b, oracle.ORC_MIXED)
+    assert np.array_equal(ca, cb)
+    Ga = ga.reshape(job_a.nv, -1)
+    Gb = gb.reshape(job_b.nv, -1)
+    assert np.array_equal(Ga[:job_b.nv], Gb)       # T columns and the CH4 scale
+
+
+def test_mixed_precision_agrees_with_fp64(oracle):
+    kt, cia, job = synth.config2(nwave=10, nlayer=40, nbin=10)
+    c, g, gt = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED)
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) < 1e-5
+    assert jac_err(g, g64, job.nv) < 1e-4
+
+
+def test_finite_difference_jacobian_fp64(oracle):
+    """Analytic dR/dx of the FP64 oracle against central differences of its
+    own forward model (temperature of chosen levels, gas scale factors)."""
+    kt, cia, job = synth.config2(nwave=4, nlayer=20, nbin=4)
+    absorbers = synth.ABSORBERS_C2
+    base_T = job.temp.astype(np.float64).copy()
+    c0, g0, gts0 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    G = g0.reshape(job.nv, -1)
+    L = job.nlayer
+
+    def run(T=None, xscale=None):
+        j = synth.make_job(kt, absorbers, nlayer=L, seed=1003, nwave=4, vmr_perturb=0.3,
+                           temp=base_T if T is None else T, xscale=xscale)
+        j.delh[:] = job.delh           # layer thickness held fixed, as the analytic gradient assumes
+        return oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_FP64)[0]
+
+    for lev in (0, 7, 19):
+        h = 2e-3
+        Tp = base_T.copy(); Tp[lev] += h
+        Tm = base_T.copy(); Tm[lev] -= h
+        # the layer arrays are REAL: divide by the step that survives float32 rounding
+        h2 = float(np.float32(Tp[lev])) - float(np.float32(Tm[lev]))
+        fd = (run(T=Tp) - run(T=Tm)) / h2
+        ana = G[lev].copy()
+        if lev == 0:
+            # with TSURF <= 0 the surface radiates B(T) of the bottom layer; the
+            # reference returns that dependence separately as gradtsurf
+            # (cirsradg_wave.f:993-1006), not inside the layer gradient
+            ana = ana + gts0
+        scale = np.max(np.abs(ana))
+        # piecewise-linear table interpolation and the rank rebinning have kinks:
+        # the check is at the Jacobian acceptance level
+        assert np.max(np.abs(fd - ana)) / scale < 1e-3, lev
+    for a in range(len(absorbers)):
+        h = 1e-4
+        xp = np.zeros(len(absorbers)); xp[a] = h
+        fd = (run(xscale=xp) - run(xscale=-xp)) / (2 * h)
+        scale = np.max(np.abs(G[L + a]))
+        assert np.max(np.abs(fd - G[L + a])) / scale < 1e-3, a
+
+
+def test_unsupported_options_are_reported(oracle):
+    kt, cia, job = synth.config1()
+    job.imod[0] = 15       # multiple scattering STOPs in the reference
+    with pytest.raises(RuntimeError, match="UNSUPPORTED"):
+        oracle.cirsrtfg_wave(kt, cia, job)
+
+
+# ---------------------------------------------------------------- real CIA data
+ISOTEST = "/root/reference/raddata/isotest.tab"
+
+
+def read_cia_tab(path):
+    """gfortran sequential unformatted file of ciaread.f:77-98: record 1 =
+    25 DOUBLE temperatures, record 2 = REAL kcia(9, 25, 1501)."""
+    raw = open(path, "rb").read()
+    n1 = np.frombuffer(raw[0:4], np.int32)[0]
+    temps = np.frombuffer(raw[4:4 + n1], np.float64).copy()
+    o = 4 + n1 + 4
+    n2 = np.frombuffer(raw[o:o + 4], np.int32)[0]
+    kcia = np.frombuffer(raw[o + 4:o + 4 + n2], np.float32).copy()
+    return temps, kcia
+
+
+@pytest.mark.skipif(not os.path.exists(ISOTEST), reason="reference data not mounted")
+def test_real_cia_table_isotest(oracle):
+    temps, kcia = read_cia_tab(ISOTEST)
+    assert temps.size == 25 and kcia.size == 9 * 25 * 1501
+    assert np.all(np.diff(temps) > 0) and np.all(np.isfinite(kcia))
+    kt, _, job = synth.config1()
+    cia = synth.CIATable(1.0, temps, kcia)
+    c, g, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    c0, _, _ = oracle.cirsrtfg_wave(kt, None, job, oracle.ORC_FP64)
+    assert np.all(np.isfinite(c)) and np.all(c > 0)
+    assert np.any(c != c0)     # the H2-H2/H2-He continuum changes the spectrum

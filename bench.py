@@ -203,13 +203,35 @@ def cpu_baseline_and_accuracy(kt, cia, job, gpu_out):
                   "sample_wavenumbers": len(range(0, job.nwave, stride * 8)) * 8, "vs": "FP64 oracle"}
 
 
+def profile_case(args):
+    """Reduced case for ncu captures: the same spectrum cut to its first
+    `--profile-waves` wavenumbers, warm-up + `--steps` launches."""
+    from radtrancode_b200 import cirsradg, synth
+    kt, cia, _ = synth.config2()
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, nwave=args.profile_waves, vmr_perturb=0.3)
+    with cirsradg.Context(0) as ctx:
+        ctx.set_ktables(kt)
+        ctx.set_cia(cia)
+        ctx.prepare([job])
+        for _ in range(args.warmup + args.steps):
+            ctx.launch()
+            ctx.fetch()
+            print(json.dumps({"profile_waves": args.profile_waves, "ms_kernel": ctx.stats()["ms_kernel"]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-waves", type=int, default=0,
+                    help="profiling case: only launch the forward kernel on the first N wavenumbers of the "
+                         "workload (steps launches after warmup), print the kernel time, skip e2e and baselines")
     args = ap.parse_args()
+    if args.profile_waves:
+        profile_case(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

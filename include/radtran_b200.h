@@ -187,6 +187,7 @@ int rtb_set_stream(rtb_context* ctx, void* stream);
  * the forward kernel. */
 typedef struct rtb_fwd_stats {
     long long cells, sort_passes, tie_passes, exact_passes, irregular_passes;
+    long long block_passes;           /* passes sorted by row-block ranks (no merge) */
     long long h2d_bytes, d2h_bytes;   /* host<->device bytes of the call */
     float ms_kernel;
 } rtb_fwd_stats;

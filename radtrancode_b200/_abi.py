@@ -51,7 +51,7 @@ class RtbAtm(C.Structure):
 class RtbFwdStats(C.Structure):
     _fields_ = [
         ("cells", C.c_longlong), ("sort_passes", C.c_longlong), ("tie_passes", C.c_longlong),
-        ("exact_passes", C.c_longlong), ("irregular_passes", C.c_longlong),
+        ("exact_passes", C.c_longlong), ("irregular_passes", C.c_longlong), ("block_passes", C.c_longlong),
         ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong), ("ms_kernel", C.c_float),
     ]
 

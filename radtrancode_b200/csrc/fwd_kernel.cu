@@ -3,27 +3,31 @@
 // with map2pro/map2xvec (radtran/cirsradg/map2pro.f, map2xvec.f).
 //
 // One CTA (8 warps) owns one (spectrum, wavenumber) work item at a time and
-// loops over items grid-stride (persistent).  Stages:
+// loops over items grid-stride (persistent grid, one scratch slot per CTA).
 //   A  per layer (one warp each): k-table interpolation of every gas
 //      (get_kg.f:306-378), continuum optical depth and its derivatives
 //      (nciacon.f, dust, Rayleigh: cirsradg_wave.f:510-691) and the random
-//      overlap of the gas k-distributions (noverlapg.f/rankg.f) with a
-//      warp-wide bitonic sort of the NG*NG combinations, an exact FP64 scan
-//      of the weights and one lane per g-bin for the rebinning sums.
-//      Results (tau and dtau/dq per g) stay in shared memory.
+//      overlap of the gas k-distributions (noverlapg.f/rankg.f).  The NG*NG
+//      combined keys k1(i)*a1 + k2(j)*a2 form NG sorted rows when both
+//      distributions are monotone in g (every k-distribution is), so they are
+//      sorted by a stable warp merge sort of those rows; otherwise by a warp
+//      bitonic network.  The FP64 cumulative weights come from a warp scan
+//      (exact in any order), and the rebinning sums of rankg.f:118-146 run as
+//      (bin, column) tasks in the reference's order.  tau and dtau/dq per g
+//      go to the CTA's scratch slot (L2-resident).
 //   B  per path (one warp, one lane per g): Planck, transmissions, radiance
-//      and dR/dtau of every layer by a suffix sum, which replaces the
-//      O(L^2) recurrence of cirsradg_wave.f:954-978 by O(L) exact algebra.
+//      and dR/dtau of every layer by a suffix sum, which replaces the O(L^2)
+//      recurrence of cirsradg_wave.f:954-978 by O(L) exact algebra.
 //   C  g-quadrature of the layer Jacobian (cirsradg_wave.f:1240-1286).
 //   D  layer -> state vector through a precomputed sparse map
-//      (map2pro o map2xvec), written in the packing of cirsrtfg_wave.f:425-446.
+//      (map2pro o map2xvec), packed as cirsrtfg_wave.f:425-446.
 //
 // Bit-exactness of the g-bin assignment: every operation that feeds a sort
 // key or a bin boundary is an explicitly rounded IEEE operation in the
 // reference's order (no FMA contraction); the cumulative weights are FP64
-// sums of FP32 products >= 2^-28, which are exact in any order; tied keys
-// whose order could move a bin boundary take the reference's heapsort
-// (sort2g.f) in-kernel.
+// sums of FP32 products >= 2^-28, exact in any order; a pass whose bin
+// boundaries fall inside a run of tied keys (where the reference's unstable
+// heapsort order decides the bins) takes that heapsort (sort2g.f) in-kernel.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -34,13 +38,21 @@ namespace rtb {
 
 namespace {
 
-constexpr int kE = 16;               // sort elements per lane (NG*NG <= 512)
-constexpr int kN = 32 * kE;
+constexpr int kN = 484;              // largest NG*NG (NG <= 22)
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBlockMax = 6;         // largest row block sorted by ranks (else merge)
+
+__device__ __forceinline__ unsigned long long shfl_up64(unsigned long long v, int d) {
+    unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+    lo = __shfl_up_sync(kFull, lo, d);
+    hi = __shfl_up_sync(kFull, hi, d);
+    return ((unsigned long long)hi << 32) | lo;
+}
 
 __device__ __forceinline__ unsigned long long shfl_xor64(unsigned long long v, int m) {
     unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-    lo = __shfl_xor_sync(0xffffffffu, lo, m);
-    hi = __shfl_xor_sync(0xffffffffu, hi, m);
+    lo = __shfl_xor_sync(kFull, lo, m);
+    hi = __shfl_xor_sync(kFull, hi, m);
     return ((unsigned long long)hi << 32) | lo;
 }
 
@@ -54,53 +66,15 @@ __device__ __forceinline__ float funkey(unsigned k) {
     return __uint_as_float(u);
 }
 
-// Warp bitonic sort of 32*kE packed (key, index) words; element lane*kE + r
-// lives in v[r]; ascending.
-__device__ __forceinline__ void warp_bitonic(unsigned long long (&v)[kE], int lane) {
-#pragma unroll
-    for (int k = 2; k <= kN; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            if (j >= kE) {
-                const int lm = j / kE;
-                const bool lower = (lane & lm) == 0;
-#pragma unroll
-                for (int r = 0; r < kE; ++r) {
-                    const unsigned long long o = shfl_xor64(v[r], lm);
-                    const int idx = lane * kE + r;
-                    const bool up = (idx & k) == 0;
-                    const bool keep_min = (up == lower);
-                    const unsigned long long mn = v[r] < o ? v[r] : o;
-                    const unsigned long long mx = v[r] < o ? o : v[r];
-                    v[r] = keep_min ? mn : mx;
-                }
-            } else {
-#pragma unroll
-                for (int r = 0; r < kE; ++r) {
-                    const int p = r ^ j;
-                    if (p > r) {
-                        const int idx = lane * kE + r;
-                        const bool up = (idx & k) == 0;
-                        const unsigned long long a = v[r], b = v[p];
-                        const bool sw = up ? (a > b) : (a < b);
-                        v[r] = sw ? b : a;
-                        v[p] = sw ? a : b;
-                    }
-                }
-            }
-        }
-    }
-}
-
 // NR heapsort of radtran/cirsradg/sort2g.f:1-52 on shared memory (one thread);
 // ra/ib hold RA(1..n)/IB(1..n) at ra[0..n-1].
-__device__ void heapsort_sort2g(int n, float* ra0, short* ib0) {
+__device__ __noinline__ void heapsort_sort2g(int n, float* ra0, unsigned short* ib0) {
     if (n < 2) return;
     float* RA = ra0 - 1;
-    short* IB = ib0 - 1;
+    unsigned short* IB = ib0 - 1;
     int L = n / 2 + 1, IR = n;
     float RRA;
-    short IRB;
+    unsigned short IRB;
     for (;;) {
         if (L > 1) {
             L = L - 1;
@@ -137,42 +111,36 @@ __device__ void heapsort_sort2g(int n, float* ra0, short* ib0) {
     }
 }
 
-// Shared-memory layout (bytes), identical on host and device.
-struct Layout {
-    int warp_bytes;       // per-warp scratch of stage A
-    int off_gord;         // double[kMaxNg+1]
-    int off_delg;         // float[kMaxNg]
-    int off_tau;          // float[Lmax][ng]
-    int off_dtau;         // float[Lmax][nsw][ng]
-    int off_region;       // aliased: per-warp scratch (A) / path arrays (B-D)
-    int path_bytes;       // per path in the region
-    int total;
-};
+__host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 
-__host__ __device__ inline int align8(int x) { return (x + 7) & ~7; }
-
-// per-warp scratch sub-offsets
+// per-warp scratch sub-offsets (bytes).  bufA holds the sorted (key, element)
+// words of a pass; bufB is the merge's second buffer, then the per-bin row and
+// column weight sums R[b][i], C[b][j] (2*ng*ng floats <= 4096 B for ng <= 22).
 struct WarpOff {
-    int splitfrac, keys, idx, k1, k2, dk1, dk2, kg, colA, colB, splitpos, total;
+    int bufA, bufB, splitfrac, k1, k2, dk1, dk2, kg, normf, splitpos, colA, colB, total;
 };
 __host__ __device__ inline WarpOff warp_off(int ncol) {
     WarpOff w;
     int o = 0;
+    const int nc = ncol > 0 ? ncol : 1;
+    // 8 B words; the free buffer also holds R, C (2*ng*ng floats) and the
+    // element bins (ng*ng bytes): 9 B per element
+    w.bufA = o; o += align16(9 * kN);
+    w.bufB = o; o += align16(9 * kN);
     w.splitfrac = o; o += 8 * kMaxNg;
-    w.keys = o; o += 4 * kN;
-    w.idx = o; o += 2 * kN;
     w.k1 = o; o += 4 * kMaxNg;
     w.k2 = o; o += 4 * kMaxNg;
     w.dk1 = o; o += 4 * kMaxNg;
     w.dk2 = o; o += 4 * kMaxNg;
     w.kg = o; o += 4 * kMaxNg;
-    w.colA = o; o += 4 * kMaxNg * (ncol > 0 ? ncol : 1);
-    w.colB = o; o += 4 * kMaxNg * (ncol > 0 ? ncol : 1);
+    w.normf = o; o += 4 * kMaxNg;
     w.splitpos = o; o += 4 * kMaxNg;
-    w.total = align8(o);
+    w.colA = o; o += 4 * kMaxNg * nc;
+    w.colB = o; o += 4 * kMaxNg * nc;
+    w.total = align16(o);
     return w;
 }
-// per-path sub-offsets inside the region (stages B-D)
+// per-path sub-offsets (stages B-D)
 struct PathOff {
     int drdt, trd, bb, dbdt, dq, rad, gts, total;
 };
@@ -186,31 +154,30 @@ __host__ __device__ inline PathOff path_off(int nlmax, int ng, int nsw) {
     p.dq = o; o += 4 * nlmax * (nsw > 0 ? nsw : 1);
     p.rad = o; o += 4 * kMaxNg;
     p.gts = o; o += 4 * kMaxNg;
-    p.total = align8(o);
+    p.total = align16(o);
     return p;
 }
 
-__host__ __device__ inline Layout make_layout(int ng, int Lmax, int nsw, int ncol, int nlmax, int npath) {
+struct Layout {
+    int warp_bytes, path_bytes, off_gord, off_delg, off_region, total;
+};
+__host__ __device__ inline Layout make_layout(int ng, int nsw, int ncol, int nlmax, int npath) {
     Layout Lo;
     Lo.warp_bytes = warp_off(ncol).total;
-    int o = 0;
-    Lo.off_gord = o; o += 8 * (kMaxNg + 1);
-    Lo.off_delg = o; o += 4 * kMaxNg;
-    o = align8(o);
-    Lo.off_tau = o; o += 4 * Lmax * ng;
-    Lo.off_dtau = o; o += 4 * Lmax * (nsw > 0 ? nsw : 1) * ng;
-    o = align8(o);
-    Lo.off_region = o;
     Lo.path_bytes = path_off(nlmax, ng, nsw).total;
+    int o = 0;
+    Lo.off_gord = o; o += 8 * (kMaxNg + 3);
+    Lo.off_delg = o; o += 4 * kMaxNg;
+    o = align16(o);
+    Lo.off_region = o;
     const int a = kWarps * Lo.warp_bytes, b = npath * Lo.path_bytes;
     o += a > b ? a : b;
     Lo.total = o;
     return Lo;
 }
 
-// per-warp accumulation of diagnostics, flushed once per work item
 struct Diag {
-    unsigned long long sort_passes, tie_passes, exact_passes, irregular;
+    unsigned long long sort_passes, tie_passes, exact_passes, irregular, block_passes;
 };
 
 // ---------------------------------------------------------------------------
@@ -254,9 +221,9 @@ __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, co
 
 // continuum optical depth of one layer and its active derivatives
 // (cirsradg_wave.f:526-691 with nciacon.f:84-310 / ciaread.f:108-198).
-// Every lane computes the same scalars.
+// Lanes 0..8 interpolate one CIA pair each; the sums run on every lane.
 __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, const LayerDev& L, const WaveDev& W,
-                                           int64_t iw_glob, int64_t il_glob, float (&dtc)[kMaxSw]) {
+                                           int64_t iw_glob, int64_t il_glob, int lane, float (&dtc)[kMaxSw]) {
 #pragma unroll
     for (int s = 0; s < kMaxSw; ++s) dtc[s] = 0.0f;
     float taucon = 0.0f;
@@ -269,10 +236,9 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
     }
     float absorb = 0.0f, dab[7] = {0, 0, 0, 0, 0, 0, 0};
     if (S.has_cia) {
-        float alpha[9], da[9];
-#pragma unroll
-        for (int p = 0; p < 9; ++p) { alpha[p] = 0.0f; da[p] = 0.0f; }
-        if (W.cia_cv >= 0) {
+        float my_a = 0.0f, my_d = 0.0f;
+        if (W.cia_cv >= 0 && lane < 9) {
+            const int p = lane;
             const float t = W.cia_t, u = L.cia_u;
             const float omt = __fsub_rn(1.0f, t), omu = __fsub_rn(1.0f, u);
             const float* kc = B.kcia;
@@ -280,31 +246,34 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
             const int64_t b12 = 9 * ((int64_t)L.cia_ct + 25 * ((int64_t)W.cia_cv + 1));
             const int64_t b22 = 9 * ((int64_t)L.cia_ct + 1 + 25 * ((int64_t)W.cia_cv + 1));
             const int64_t b21 = 9 * ((int64_t)L.cia_ct + 1 + 25 * (int64_t)W.cia_cv);
+            const float a11 = __ldg(kc + b11 + p), a12 = __ldg(kc + b12 + p);
+            const float a22 = __ldg(kc + b22 + p), a21 = __ldg(kc + b21 + p);
+            float x = __fmul_rn(__fmul_rn(omt, omu), a11);
+            x = __fadd_rn(x, __fmul_rn(__fmul_rn(t, omu), a12));
+            x = __fadd_rn(x, __fmul_rn(__fmul_rn(t, u), a22));
+            x = __fadd_rn(x, __fmul_rn(__fmul_rn(omt, u), a21));
+            float d = -__fmul_rn(omt, a11);
+            d = __fsub_rn(d, __fmul_rn(t, a12));
+            d = __fadd_rn(d, __fmul_rn(t, a22));
+            d = __fadd_rn(d, __fmul_rn(omt, a21));
+            my_a = x;
+            my_d = __fmul_rn(d, L.cia_dudt);
+        }
+        float alpha[9], da[9];
 #pragma unroll
-            for (int p = 0; p < 9; ++p) {
-                const float a11 = __ldg(kc + b11 + p), a12 = __ldg(kc + b12 + p);
-                const float a22 = __ldg(kc + b22 + p), a21 = __ldg(kc + b21 + p);
-                float x = __fmul_rn(__fmul_rn(omt, omu), a11);
-                x = __fadd_rn(x, __fmul_rn(__fmul_rn(t, omu), a12));
-                x = __fadd_rn(x, __fmul_rn(__fmul_rn(t, u), a22));
-                x = __fadd_rn(x, __fmul_rn(__fmul_rn(omt, u), a21));
-                float d = -__fmul_rn(omt, a11);
-                d = __fsub_rn(d, __fmul_rn(t, a12));
-                d = __fadd_rn(d, __fmul_rn(t, a22));
-                d = __fadd_rn(d, __fmul_rn(omt, a21));
-                alpha[p] = x;
-                da[p] = __fmul_rn(d, L.cia_dudt);
-            }
+        for (int p = 0; p < 9; ++p) {
+            alpha[p] = __shfl_sync(kFull, my_a, p);
+            da[p] = __shfl_sync(kFull, my_d, p);
         }
         const float qh2 = L.q[0], qhe = L.q[1], qn2 = L.q[2], qch4 = L.q[3], qco2 = L.q[4];
         float sum = 0.0f;
-        const int o = S.inormal == 0 ? 0 : 2;
-        sum = __fadd_rn(__fadd_rn(sum, __fmul_rn(__fmul_rn(alpha[o], qh2), qh2)),
-                        __fmul_rn(__fmul_rn(alpha[o + 1], qh2), qhe));
-        dab[0] = __fadd_rn(__fadd_rn(dab[0], __fmul_rn(__fmul_rn(2.0f, qh2), alpha[o])), __fmul_rn(qhe, alpha[o + 1]));
-        dab[1] = __fadd_rn(dab[1], __fmul_rn(qh2, alpha[o + 1]));
-        dab[5] = __fadd_rn(__fadd_rn(dab[5], __fmul_rn(__fmul_rn(qh2, qh2), da[o])),
-                           __fmul_rn(__fmul_rn(qh2, qhe), da[o + 1]));
+        const bool eq = S.inormal == 0;
+        const float ao = eq ? alpha[0] : alpha[2], ao1 = eq ? alpha[1] : alpha[3];
+        const float dao = eq ? da[0] : da[2], dao1 = eq ? da[1] : da[3];
+        sum = __fadd_rn(__fadd_rn(sum, __fmul_rn(__fmul_rn(ao, qh2), qh2)), __fmul_rn(__fmul_rn(ao1, qh2), qhe));
+        dab[0] = __fadd_rn(__fadd_rn(dab[0], __fmul_rn(__fmul_rn(2.0f, qh2), ao)), __fmul_rn(qhe, ao1));
+        dab[1] = __fadd_rn(dab[1], __fmul_rn(qh2, ao1));
+        dab[5] = __fadd_rn(__fadd_rn(dab[5], __fmul_rn(__fmul_rn(qh2, qh2), dao)), __fmul_rn(__fmul_rn(qh2, qhe), dao1));
         sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(alpha[4], qh2), qn2));
         dab[0] = __fadd_rn(dab[0], __fmul_rn(qn2, alpha[4]));
         dab[2] = __fadd_rn(dab[2], __fmul_rn(qh2, alpha[4]));
@@ -333,6 +302,7 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
     }
     taucon = __fadd_rn(taucon, absorb);
     const float den = __fmul_rn(L.utotl, 1.0e20f);
+#pragma unroll
     for (int ii = 0; ii < 5; ++ii) {
         const int k = L.iabs[ii];
         if (k < 0) continue;
@@ -357,303 +327,441 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
 
 // ---------------------------------------------------------------------------
 // One overlap pass with sorting (noverlapg.f:110-147/175-190 + rankg.f).
-// Inputs in the warp scratch: k1[i], k2[j], dk1[i], dk2[j] and the previous
-// columns colP[c][i].  Outputs: new k_g in kg[], new columns in colN[c][].
+// Warp scratch holds k1[i], k2[j], dk1[i], dk2[j] and the previous gradient
+// columns colP[c][i]; the pass writes the new distribution to kg[] and the
+// new columns to colN[c][].  An element (i, j) travels as the 64-bit word
+// fkey(key) << 32 | i << 5 | j: its low half orders like the reference's
+// element number i*ng + j, so word order is the stable key order.
 struct PassCtx {
-    int ng, nloop, ncol, first, igas;   // igas: 0-based index of the gas being added
+    int ng, nloop, ncol, first, igas;
     float a1, a2;
 };
 
-__device__ __forceinline__ float elem_grad(const PassCtx& P, const SpecDev& S, int c, int i, int j,
-                                           const float* k1, const float* k2, const float* dk1, const float* dk2,
-                                           const float* colP) {
-    const int g = S.col_gas[c];
-    if (g == S.ngas) {   // temperature column
-        if (P.first) return __fadd_rn(__fmul_rn(dk1[i], P.a1), __fmul_rn(dk2[j], P.a2));
-        return __fadd_rn(dk1[i], __fmul_rn(dk2[j], P.a2));
+struct WarpPtr {
+    unsigned long long *bufA, *bufB;
+    float *k1, *k2, *dk1, *dk2, *kg, *normf;
+    double* splitfrac;
+    int* splitpos;
+};
+
+__device__ __forceinline__ float key_of(const PassCtx& P, const WarpPtr& wp, int i, int j) {
+    return P.first ? __fadd_rn(__fmul_rn(wp.k1[i], P.a1), __fmul_rn(wp.k2[j], P.a2))
+                   : __fadd_rn(wp.k1[i], __fmul_rn(wp.k2[j], P.a2));
+}
+
+__device__ __forceinline__ unsigned long long pack(float key, int i, int j) {
+    return ((unsigned long long)fkey(key) << 32) | (unsigned)((i << 5) | j);
+}
+
+// Stable merge sort of ng sorted rows of ng words (row i = elements i*ng ..
+// i*ng+ng-1).  The rows start in buffer `start`; returns the buffer holding
+// the result.  Each lane produces a contiguous chunk of every level's output
+// from one merge-path search.  Within a merge every word of the left run
+// has a smaller element part than every word of the right run, so comparing
+// whole words is the stable merge.
+__device__ int merge_rows(const WarpPtr& wp, int ng, int lane, int start) {
+    const int n = ng * ng;
+    const int ch = (n + 31) >> 5;
+    int cur = start;
+    for (int run = ng; run < n; run <<= 1) {
+        const unsigned long long* ki = cur ? wp.bufB : wp.bufA;
+        unsigned long long* ko = cur ? wp.bufA : wp.bufB;
+        const int k0 = lane * ch;
+        const int k1 = min(k0 + ch, n);
+        if (k0 < k1) {
+            const int two = run << 1;
+            int ms = (k0 / two) * two;
+            int m = min(run, n - ms);
+            int ny = max(0, min(run, n - ms - run));
+            const int kk = k0 - ms;
+            int lo = max(0, kk - ny), hi = min(kk, m);
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (ki[ms + mid] < ki[ms + run + kk - mid - 1]) lo = mid + 1; else hi = mid;
+            }
+            int a = lo, b = kk - lo;
+            unsigned long long xa = a < m ? ki[ms + a] : ~0ull;
+            unsigned long long yb = b < ny ? ki[ms + run + b] : ~0ull;
+            for (int k = k0; k < k1; ++k) {
+                if (k == ms + m + ny) {       // next pair of runs starts here
+                    ms = k;
+                    m = min(run, n - ms);
+                    ny = max(0, min(run, n - ms - run));
+                    a = 0;
+                    b = 0;
+                    xa = m > 0 ? ki[ms] : ~0ull;
+                    yb = ny > 0 ? ki[ms + run] : ~0ull;
+                }
+                if (xa < yb) {
+                    ko[k] = xa;
+                    ++a;
+                    xa = a < m ? ki[ms + a] : ~0ull;
+                } else {
+                    ko[k] = yb;
+                    ++b;
+                    yb = b < ny ? ki[ms + run + b] : ~0ull;
+                }
+            }
+        }
+        __syncwarp();
+        cur ^= 1;
     }
-    if (g == P.igas) return k2[j];
-    if (P.first) return g == 0 ? k1[i] : 0.0f;
+    return cur;
+}
+
+// gradient value of tracked column c for element (i, j) (noverlapg.f:125-127,
+// 184-187); used by the sequential (irregular) walk only
+__device__ __forceinline__ float elem_grad(const PassCtx& P, int gcol, int c, int i, int j, const WarpPtr& wp,
+                                           const float* colP, int ngas) {
+    if (gcol == ngas) {
+        if (P.first) return __fadd_rn(__fmul_rn(wp.dk1[i], P.a1), __fmul_rn(wp.dk2[j], P.a2));
+        return __fadd_rn(wp.dk1[i], __fmul_rn(wp.dk2[j], P.a2));
+    }
+    if (gcol == P.igas) return wp.k2[j];
+    if (P.first) return gcol == 0 ? wp.k1[i] : 0.0f;
+    if (gcol > P.igas) return 0.0f;
     return colP[c * kMaxNg + i];
 }
 
-__device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P, char* wsm, const WarpOff& wo,
-                          const double* g_ord, const float* delg, int lane, Diag& dg, float* colP, float* colN,
-                          int16_t* dbg_perm, int16_t* dbg_split) {
-    float* keys_s = (float*)(wsm + wo.keys);
-    short* idx_s = (short*)(wsm + wo.idx);
-    const float* k1 = (const float*)(wsm + wo.k1);
-    const float* k2 = (const float*)(wsm + wo.k2);
-    const float* dk1 = (const float*)(wsm + wo.dk1);
-    const float* dk2 = (const float*)(wsm + wo.dk2);
-    float* kg = (float*)(wsm + wo.kg);
-    double* splitfrac = (double*)(wsm + wo.splitfrac);
-    int* splitpos = (int*)(wsm + wo.splitpos);
+__device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
+                          const double* g_ord, const float* delg, int lane, Diag& dg, const float* colP,
+                          float* colN, int16_t* dbg_perm, int16_t* dbg_split) {
     const int ng = P.ng, nloop = P.nloop;
-
-    auto key_of = [&](int e) -> float {
-        const int i = e / ng, j = e - (e / ng) * ng;
-        return P.first ? __fadd_rn(__fmul_rn(k1[i], P.a1), __fmul_rn(k2[j], P.a2))
-                       : __fadd_rn(k1[i], __fmul_rn(k2[j], P.a2));
-    };
-
-    // fast path: bitonic sort of (key, element) -> stable order of ties
-    unsigned long long v[kE];
-#pragma unroll
-    for (int r = 0; r < kE; ++r) {
-        const int e = lane * kE + r;
-        const float key = e < nloop ? key_of(e) : __int_as_float(0x7f800000);
-        v[r] = ((unsigned long long)fkey(key) << 32) | (unsigned)e;
-    }
-    warp_bitonic(v, lane);
-    float kr[kE];
-    int ir[kE];
-#pragma unroll
-    for (int r = 0; r < kE; ++r) {
-        kr[r] = funkey((unsigned)(v[r] >> 32));
-        ir[r] = (int)(v[r] & 0xffffffffu);
-    }
-
-    bool exact = false;
-    double gd[kE], gprev0;
-    int cc[kE], cprev0;
-    bool irregular = false, gerr = false;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        // FP64 cumulative weights (exact in any order) and bin counts
-        double run = 0.0;
-#pragma unroll
-        for (int r = 0; r < kE; ++r) {
-            const int p = lane * kE + r;
-            float w = 0.0f;
-            if (p < nloop) {
-                const int e = ir[r], i = e / ng, j = e - (e / ng) * ng;
-                w = __fmul_rn(delg[i], delg[j]);
+    // ---- sort --------------------------------------------------------------
+    // The words of row i, k1(i)[*a1] + k2(j)*a2 over j, are sorted when k2 is
+    // monotone and a2 >= 0.  If every row's first word exceeds the last word
+    // of the row before it (and the rows are in order), row-major order is
+    // already the sorted order; otherwise the rows are merged.  Other inputs
+    // take the bitonic network.
+    bool monoB = P.a2 >= 0.0f && (!P.first || P.a1 >= 0.0f);
+    if (lane + 1 < ng) monoB = monoB && (wp.k2[lane] <= wp.k2[lane + 1]);
+    monoB = __all_sync(kFull, monoB);
+    const unsigned long long* A = wp.bufA;
+    if (monoB) {
+        unsigned long long* W = wp.bufB;            // row-major words
+        {
+            int i = lane / ng, j = lane - (lane / ng) * ng;
+            for (int e = lane; e < nloop; e += 32) {
+                W[e] = pack(key_of(P, wp, i, j), i, j);
+                j += 32;
+                while (j >= ng) { j -= ng; ++i; }
             }
-            run = __dadd_rn(run, (double)w);
-            gd[r] = run;
+        }
+        __syncwarp();
+        bool disjoint = true;
+        if (lane + 1 < ng) disjoint = W[(lane + 1) * ng] > W[lane * ng + ng - 1];
+        disjoint = __all_sync(kFull, disjoint);
+        if (disjoint) {
+            A = W;
+            dg.block_passes += (lane == 0);
+        } else if (merge_rows(wp, ng, lane, 1) != 0) {
+            A = W;
+        }
+    }
+    // inputs whose rows are not sorted (a k-distribution not monotone in g)
+    // take the reference heapsort below
+    const bool need_exact = !monoB;
+
+    // ---- cumulative weights, bin boundaries, tie checks --------------------
+    // Each lane takes a chunk of consecutive sorted positions: FP64 prefix of
+    // the weights (exact in any order) into scratch; then one lane per g
+    // boundary binary-searches its split position (the first position whose
+    // cumulative weight reaches g_ord(b+1), rankg.f:119-129) and forms the
+    // split fraction.
+    const int ch = (nloop + 31) >> 5;
+    const int p0 = min(lane * ch, nloop), p1 = min(p0 + ch, nloop);
+    bool exact = false, irregular = false, gerr = false;
+    int c_last = 0;
+    // the reference heapsort on the elements in nloop order (sort2g.f); its
+    // scratch lives in the buffer not holding A, its result replaces A
+    auto heapsort_pass = [&]() {
+        __syncwarp();
+        unsigned long long* Aw = (A == wp.bufA) ? wp.bufA : wp.bufB;
+        float* hk = (float*)((A == wp.bufA) ? wp.bufB : wp.bufA);
+        unsigned short* hi_ = (unsigned short*)(hk + nloop);
+        for (int e = lane; e < nloop; e += 32) {
+            const int i = e / ng, j = e - i * ng;
+            hk[e] = key_of(P, wp, i, j);
+            hi_[e] = (unsigned short)(e + 1);
+        }
+        __syncwarp();
+        if (lane == 0) heapsort_sort2g(nloop, hk, hi_);
+        __syncwarp();
+        for (int p = lane; p < nloop; p += 32) {
+            const int e = (int)hi_[p] - 1;
+            const int i = e / ng, j = e - i * ng;
+            Aw[p] = pack(hk[p], i, j);
+        }
+        __syncwarp();
+        A = Aw;
+        exact = true;
+        dg.exact_passes += (lane == 0);
+    };
+    if (need_exact) heapsort_pass();
+    double* gd = nullptr;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        gd = (double*)((A == wp.bufA) ? wp.bufB : wp.bufA);   // free buffer
+        double run = 0.0;
+        unsigned kbp = p0 >= 1 && p0 < p1 ? (unsigned)(A[p0 - 1] >> 32) : 0u;
+        bool anytie = false, nan = false;
+        for (int p = p0; p < p1; ++p) {
+            const unsigned long long word = A[p];
+            const unsigned q = (unsigned)word & 0xffffu;
+            const unsigned kb = (unsigned)(word >> 32);
+            run = __dadd_rn(run, (double)__fmul_rn(delg[q >> 5], delg[q & 31]));
+            gd[p] = run;
+            anytie |= (p >= 1 && kb == kbp);         // fkey folds -0 onto +0
+            const float kp = funkey(kb);
+            nan |= (kp != kp);
+            kbp = kb;
         }
         double incl = run;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const double t = __shfl_up_sync(0xffffffffu, incl, o);
+            const double t = __shfl_up_sync(kFull, incl, o);
             if (lane >= o) incl = __dadd_rn(incl, t);
         }
-        const double base = __dsub_rn(incl, run);   // exact (all partial sums are exact)
-        gprev0 = base;
-#pragma unroll
-        for (int r = 0; r < kE; ++r) gd[r] = __dadd_rn(gd[r], base);
-        // c(p) = #{b in 1..ng : g_ord[b] <= gdist(p)}
-#pragma unroll
-        for (int r = 0; r < kE; ++r) {
-            int lo = 0, hi = ng;   // count in [0, ng]
+        const double base = __dsub_rn(incl, run);   // exact: every partial sum is exact
+        for (int p = p0; p < p1; ++p) gd[p] = __dadd_rn(gd[p], base);
+        __syncwarp();
+        int sp = nloop;
+        bool risky = false;
+        if (lane < ng) {
+            const double gb = g_ord[lane + 1];
+            int lo = 0, hi = nloop;
             while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (g_ord[mid] <= gd[r]) lo = mid; else hi = mid - 1;
+                const int mid = (lo + hi) >> 1;
+                if (gd[mid] >= gb) hi = mid; else lo = mid + 1;
             }
-            cc[r] = lo;
+            sp = lo;
+            if (sp < nloop) {
+                const unsigned long long word = A[sp];
+                const unsigned q = (unsigned)word & 0xffffu;
+                const unsigned kb = (unsigned)(word >> 32);
+                const double gprev = sp > 0 ? gd[sp - 1] : 0.0;
+                wp.splitpos[lane] = sp;
+                wp.splitfrac[lane] = __ddiv_rn(__dsub_rn(gb, gprev), (double)__fmul_rn(delg[q >> 5], delg[q & 31]));
+                const bool tl = sp >= 1 && kb == (unsigned)(A[sp - 1] >> 32);
+                const bool tr = sp + 1 < nloop && kb == (unsigned)(A[sp + 1] >> 32);
+                risky = tl || tr;
+            } else {
+                wp.splitpos[lane] = -1;
+            }
         }
-        cprev0 = __shfl_up_sync(0xffffffffu, cc[kE - 1], 1);
-        if (lane == 0) cprev0 = 0;
-        const float kprev0 = __shfl_up_sync(0xffffffffu, kr[kE - 1], 1);
-        const float knext0 = __shfl_down_sync(0xffffffffu, kr[0], 1);
-        bool risky = false, anytie = false, nan = false;
-        irregular = false;
-        gerr = false;
-#pragma unroll
-        for (int r = 0; r < kE; ++r) {
-            const int p = lane * kE + r;
-            if (p >= nloop) continue;
-            const int cp = r == 0 ? cprev0 : cc[r - 1];
-            const float kp = r == 0 ? kprev0 : kr[r - 1];
-            const float kn = r == kE - 1 ? knext0 : kr[r + 1];
-            const bool tl = p >= 1 && kr[r] == kp;
-            const bool tr = p + 1 < nloop && kr[r] == kn;
-            const bool split = cc[r] > cp;
-            if (split && (tl || tr)) risky = true;
-            anytie |= tl;
-            nan |= (kr[r] != kr[r]);
-            if (cc[r] - cp >= 2) irregular = true;
-            if (cp >= ng) gerr = true;
-        }
-        risky = __any_sync(0xffffffffu, risky);
-        anytie = __any_sync(0xffffffffu, anytie);
-        nan = __any_sync(0xffffffffu, nan);
-        irregular = __any_sync(0xffffffffu, irregular);
-        gerr = __any_sync(0xffffffffu, gerr);
+        // one element crossing two boundaries: equal split positions
+        const int sp_next = __shfl_down_sync(kFull, sp, 1);
+        irregular = __any_sync(kFull, lane + 1 < ng && sp < nloop && sp == sp_next);
+        c_last = __popc(__ballot_sync(kFull, lane < ng && sp < nloop));
+        const int sp_last = __shfl_sync(kFull, sp, ng - 1);
+        gerr = c_last == ng && sp_last < nloop - 1;    // elements left after the last boundary
+        risky = __any_sync(kFull, risky);
+        anytie = __any_sync(kFull, anytie);
+        nan = __any_sync(kFull, nan);
         if (attempt == 0) {
             dg.sort_passes += (lane == 0);
             dg.tie_passes += (lane == 0 && anytie);
         }
         if (exact || !(risky || nan || (B.strict_ties && anytie))) break;
-        // exact path: the reference heapsort on the elements in nloop order
-        exact = true;
-        dg.exact_passes += (lane == 0);
-        for (int e = lane; e < nloop; e += 32) {
-            keys_s[e] = key_of(e);
-            idx_s[e] = (short)(e + 1);
-        }
-        __syncwarp();
-        if (lane == 0) heapsort_sort2g(nloop, keys_s, idx_s);
-        __syncwarp();
-#pragma unroll
-        for (int r = 0; r < kE; ++r) {
-            const int p = lane * kE + r;
-            kr[r] = p < nloop ? keys_s[p] : __int_as_float(0x7f800000);
-            ir[r] = p < nloop ? (int)idx_s[p] - 1 : p;
-        }
-        __syncwarp();
+        heapsort_pass();
     }
     if (gerr) atomicOr(B.status, kStGord);
-
-    // publish the sorted sequence
-#pragma unroll
-    for (int r = 0; r < kE; ++r) {
-        const int p = lane * kE + r;
-        if (p < nloop) {
-            keys_s[p] = kr[r];
-            idx_s[p] = (short)ir[r];
-        }
-    }
-    if (lane < kMaxNg) splitpos[lane] = -1;
     __syncwarp();
     if (dbg_perm) {
-        for (int p = lane; p < nloop; p += 32) dbg_perm[p] = idx_s[p];
+        for (int p = lane; p < nloop; p += 32) {
+            const unsigned q = (unsigned)A[p] & 0xffffu;
+            dbg_perm[p] = (int16_t)((q >> 5) * ng + (q & 31));
+        }
+        if (lane < ng && !irregular) dbg_split[lane] = (int16_t)wp.splitpos[lane];
     }
 
     if (irregular) {
+        const int ncol = P.ncol;
         // sequential rankg walk (rankg.f:118-152) by lane 0
         dg.irregular += (lane == 0);
         if (lane == 0) {
-            for (int b = 0; b < ng; ++b) {
-                kg[b] = 0.0f;
-                for (int c = 0; c < P.ncol; ++c) colN[c * kMaxNg + b] = 0.0f;
+            for (int bb = 0; bb < ng; ++bb) {
+                wp.kg[bb] = 0.0f;
+                for (int c = 0; c < ncol; ++c) colN[c * kMaxNg + bb] = 0.0f;
             }
             int ig = 0;
             double sum = 0.0, gprev = 0.0;
             for (int p = 0; p < nloop; ++p) {
-                const int e = idx_s[p], i = e / ng, j = e - (e / ng) * ng;
-                const float c = keys_s[p];
+                const unsigned long long word = A[p];
+                const unsigned q = (unsigned)word & 0xffffu;
+                const int i = q >> 5, j = q & 31;
+                const float cval = funkey((unsigned)(word >> 32));
                 const float w = __fmul_rn(delg[i], delg[j]);
                 const double gcur = __dadd_rn(gprev, (double)w);
                 if (ig >= ng) { atomicOr(B.status, kStGord); break; }
                 if (gcur < g_ord[ig + 1]) {
-                    kg[ig] = __fadd_rn(kg[ig], __fmul_rn(c, w));
-                    for (int cc2 = 0; cc2 < P.ncol; ++cc2)
-                        colN[cc2 * kMaxNg + ig] = __fadd_rn(colN[cc2 * kMaxNg + ig],
-                            __fmul_rn(elem_grad(P, S, cc2, i, j, k1, k2, dk1, dk2, colP), w));
+                    wp.kg[ig] = __fadd_rn(wp.kg[ig], __fmul_rn(cval, w));
+                    for (int c = 0; c < ncol; ++c)
+                        colN[c * kMaxNg + ig] = __fadd_rn(colN[c * kMaxNg + ig],
+                            __fmul_rn(elem_grad(P, S.col_gas[c], c, i, j, wp, colP, S.ngas), w));
                     sum = __dadd_rn(sum, (double)w);
                 } else {
                     const double frac = __ddiv_rn(__dsub_rn(g_ord[ig + 1], gprev), __dsub_rn(gcur, gprev));
                     const float sf = __double2float_rn(frac);
-                    kg[ig] = __fadd_rn(kg[ig], __fmul_rn(__fmul_rn(sf, c), w));
-                    for (int cc2 = 0; cc2 < P.ncol; ++cc2)
-                        colN[cc2 * kMaxNg + ig] = __fadd_rn(colN[cc2 * kMaxNg + ig],
-                            __fmul_rn(__fmul_rn(sf, elem_grad(P, S, cc2, i, j, k1, k2, dk1, dk2, colP)), w));
+                    wp.kg[ig] = __fadd_rn(wp.kg[ig], __fmul_rn(__fmul_rn(sf, cval), w));
+                    for (int c = 0; c < ncol; ++c)
+                        colN[c * kMaxNg + ig] = __fadd_rn(colN[c * kMaxNg + ig],
+                            __fmul_rn(__fmul_rn(sf, elem_grad(P, S.col_gas[c], c, i, j, wp, colP, S.ngas)), w));
                     sum = __dadd_rn(sum, __dmul_rn(frac, (double)w));
                     const float fs = __double2float_rn(sum);
-                    kg[ig] = __fdiv_rn(kg[ig], fs);
-                    for (int cc2 = 0; cc2 < P.ncol; ++cc2)
-                        colN[cc2 * kMaxNg + ig] = __fdiv_rn(colN[cc2 * kMaxNg + ig], fs);
+                    wp.kg[ig] = __fdiv_rn(wp.kg[ig], fs);
+                    for (int c = 0; c < ncol; ++c) colN[c * kMaxNg + ig] = __fdiv_rn(colN[c * kMaxNg + ig], fs);
                     if (dbg_split) dbg_split[ig] = (int16_t)p;
                     ig = ig + 1;
                     sum = __dmul_rn(__dsub_rn(1.0, frac), (double)w);
                     if (ig < ng) {
                         const float sr = __double2float_rn(__dsub_rn(1.0, frac));
-                        kg[ig] = __fmul_rn(__fmul_rn(sr, c), w);
-                        for (int cc2 = 0; cc2 < P.ncol; ++cc2)
-                            colN[cc2 * kMaxNg + ig] =
-                                __fmul_rn(__fmul_rn(sr, elem_grad(P, S, cc2, i, j, k1, k2, dk1, dk2, colP)), w);
+                        wp.kg[ig] = __fmul_rn(__fmul_rn(sr, cval), w);
+                        for (int c = 0; c < ncol; ++c)
+                            colN[c * kMaxNg + ig] =
+                                __fmul_rn(__fmul_rn(sr, elem_grad(P, S.col_gas[c], c, i, j, wp, colP, S.ngas)), w);
                     }
                 }
                 gprev = gcur;
             }
             if (ig == ng - 1) {
                 const float fs = __double2float_rn(sum);
-                kg[ig] = __fdiv_rn(kg[ig], fs);
-                for (int cc2 = 0; cc2 < P.ncol; ++cc2) colN[cc2 * kMaxNg + ig] = __fdiv_rn(colN[cc2 * kMaxNg + ig], fs);
+                wp.kg[ig] = __fdiv_rn(wp.kg[ig], fs);
+                for (int c = 0; c < ncol; ++c) colN[c * kMaxNg + ig] = __fdiv_rn(colN[c * kMaxNg + ig], fs);
             }
         }
         __syncwarp();
         return;
     }
 
-    // regular walk: publish split positions and fractions
-#pragma unroll
-    for (int r = 0; r < kE; ++r) {
-        const int p = lane * kE + r;
-        if (p >= nloop) continue;
-        const int cp = r == 0 ? cprev0 : cc[r - 1];
-        if (cc[r] > cp) {
-            const double gp = r == 0 ? gprev0 : gd[r - 1];
-            splitpos[cp] = p;
-            splitfrac[cp] = __ddiv_rn(__dsub_rn(g_ord[cp + 1], gp), __dsub_rn(gd[r], gp));
-        }
-    }
-    // c_last = c(nloop-1)
-    const int last_lane = (nloop - 1) / kE, last_r = (nloop - 1) - ((nloop - 1) / kE) * kE;
-    int my_last = 0;
-#pragma unroll
-    for (int r = 0; r < kE; ++r)
-        if (r == last_r) my_last = cc[r];
-    const int c_last = __shfl_sync(0xffffffffu, my_last, last_lane);
-    __syncwarp();
-    if (dbg_split && lane < ng) dbg_split[lane] = (short)splitpos[lane];
-
-    // one lane per bin: sums in the reference's order (rankg.f:118-146)
-    const int b = lane;
-    if (b < ng) {
-        float k = 0.0f;
-        float cs[kMaxCols];
-#pragma unroll
-        for (int c = 0; c < kMaxCols; ++c) cs[c] = 0.0f;
-#define RTB_FOR_COL(c2) _Pragma("unroll") for (int c2 = 0; c2 < kMaxCols; ++c2) if (c2 < P.ncol)
-        if (b <= c_last && (b < ng)) {
+    // ---- k(g): one lane per bin (rankg.f:118-146) -------------------------
+    // split remainder, whole elements, split fraction, then / sngl(sum), every
+    // operation rounded as in the reference; the divisor is kept for the
+    // gradient columns.
+    if (lane < ng) {
+        const int bb = lane;
+        float acc = 0.0f, nf = 0.0f;        // nf == 0: bin never reached
+        if (bb <= c_last) {
             double sum = 0.0;
             int p = 0;
-            if (b > 0) {
-                const int s = splitpos[b - 1];
-                const double frac = splitfrac[b - 1];
-                const int e = idx_s[s], i = e / ng, j = e - (e / ng) * ng;
-                const float c = keys_s[s], w = __fmul_rn(delg[i], delg[j]);
+            if (bb > 0) {
+                const int s = wp.splitpos[bb - 1];
+                const double frac = wp.splitfrac[bb - 1];
+                const unsigned long long word = A[s];
+                const unsigned q = (unsigned)word & 0xffffu;
+                const float w = __fmul_rn(delg[q >> 5], delg[q & 31]);
                 const float sr = __double2float_rn(__dsub_rn(1.0, frac));
-                k = __fmul_rn(__fmul_rn(sr, c), w);
-                RTB_FOR_COL(cc2)
-                    cs[cc2] = __fmul_rn(__fmul_rn(sr, elem_grad(P, S, cc2, i, j, k1, k2, dk1, dk2, colP)), w);
+                acc = __fmul_rn(__fmul_rn(sr, funkey((unsigned)(word >> 32))), w);
                 sum = __dmul_rn(__dsub_rn(1.0, frac), (double)w);
                 p = s + 1;
             }
-            const bool closes = b < c_last;
-            const int pend = closes ? splitpos[b] : nloop;   // exclusive end of whole elements
+            const bool closes = bb < c_last;
+            const int pend = closes ? wp.splitpos[bb] : nloop;
             for (; p < pend; ++p) {
-                const int e = idx_s[p], i = e / ng, j = e - (e / ng) * ng;
-                const float c = keys_s[p], w = __fmul_rn(delg[i], delg[j]);
-                k = __fadd_rn(k, __fmul_rn(c, w));
-                RTB_FOR_COL(cc2)
-                    cs[cc2] = __fadd_rn(cs[cc2], __fmul_rn(elem_grad(P, S, cc2, i, j, k1, k2, dk1, dk2, colP), w));
+                const unsigned long long word = A[p];
+                const unsigned q = (unsigned)word & 0xffffu;
+                const float w = __fmul_rn(delg[q >> 5], delg[q & 31]);
+                acc = __fadd_rn(acc, __fmul_rn(funkey((unsigned)(word >> 32)), w));
                 sum = __dadd_rn(sum, (double)w);
             }
+            nf = 1.0f;
             if (closes) {
-                const int s = splitpos[b];
-                const double frac = splitfrac[b];
-                const int e = idx_s[s], i = e / ng, j = e - (e / ng) * ng;
-                const float c = keys_s[s], w = __fmul_rn(delg[i], delg[j]);
+                const int s = wp.splitpos[bb];
+                const double frac = wp.splitfrac[bb];
+                const unsigned long long word = A[s];
+                const unsigned q = (unsigned)word & 0xffffu;
+                const float w = __fmul_rn(delg[q >> 5], delg[q & 31]);
                 const float sf = __double2float_rn(frac);
-                k = __fadd_rn(k, __fmul_rn(__fmul_rn(sf, c), w));
-                RTB_FOR_COL(cc2)
-                    cs[cc2] = __fadd_rn(cs[cc2], __fmul_rn(__fmul_rn(sf, elem_grad(P, S, cc2, i, j, k1, k2, dk1, dk2, colP)), w));
+                acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(sf, funkey((unsigned)(word >> 32))), w));
                 sum = __dadd_rn(sum, __dmul_rn(frac, (double)w));
-                const float fs = __double2float_rn(sum);
-                k = __fdiv_rn(k, fs);
-                RTB_FOR_COL(cc2) cs[cc2] = __fdiv_rn(cs[cc2], fs);
-            } else if (b == ng - 1) {
-                const float fs = __double2float_rn(sum);
-                k = __fdiv_rn(k, fs);
-                RTB_FOR_COL(cc2) cs[cc2] = __fdiv_rn(cs[cc2], fs);
+                nf = __double2float_rn(sum);
+                acc = __fdiv_rn(acc, nf);
+            } else if (bb == ng - 1) {
+                nf = __double2float_rn(sum);
+                acc = __fdiv_rn(acc, nf);
             }
         }
-        kg[b] = k;
-        RTB_FOR_COL(cc2) colN[cc2 * kMaxNg + b] = cs[cc2];
-#undef RTB_FOR_COL
+        wp.kg[bb] = acc;
+        wp.normf[bb] = nf;
+    }
+    // ---- gradient columns ----------------------------------------------------
+    // They feed the Jacobian alone (never a sort key), so they need not follow
+    // the reference's summation order.  Each column is linear in the element
+    // weights: sum over bin b of v(i,j) w f = sum_i u(i) R[b][i] + sum_j v(j) C[b][j]
+    // with R[b][i] / C[b][j] the weight of row i / column j falling in bin b.
+    // Lane x walks row x and column x in key order (bins are monotone along
+    // both), flushing one partial sum per bin: deterministic, no atomics.
+    const int ncol = P.ncol;
+    float* R = (float*)gd;                   // gd is free again
+    float* Cw = R + ng * ng;
+    unsigned char* eb = (unsigned char*)(Cw + ng * ng);   // bin of element e (0x80: split)
+    for (int t = lane; t < 2 * ng * ng; t += 32) R[t] = 0.0f;
+    {
+        // bins of this lane's positions
+        int b = 0;
+        while (b < ng && wp.splitpos[b] >= 0 && wp.splitpos[b] < p0) ++b;
+        for (int p = p0; p < p1; ++p) {
+            const unsigned q = (unsigned)A[p] & 0xffffu;
+            const bool split = b < ng && wp.splitpos[b] == p;
+            eb[(q >> 5) * ng + (q & 31)] = (unsigned char)(b | (split ? 0x80 : 0));
+            if (split) ++b;
+        }
+    }
+    __syncwarp();
+    if (lane < ng) {
+        const int x = lane;
+        for (int pass = 0; pass < 2; ++pass) {      // 0: row x -> R, 1: column x -> C
+            float* dst = pass == 0 ? R : Cw;
+            int cur = -1;
+            float acc = 0.0f;
+            for (int y = 0; y < ng; ++y) {
+                const int e = pass == 0 ? x * ng + y : y * ng + x;
+                const unsigned char code = eb[e];
+                const int b = code & 0x7f;
+                const float w = delg[x] * delg[y];
+                if (b != cur) {
+                    if (cur >= 0 && cur < ng) dst[cur * ng + x] += acc;
+                    cur = b;
+                    acc = 0.0f;
+                }
+                if (code & 0x80) {
+                    const float f = (float)wp.splitfrac[b];
+                    dst[b * ng + x] += acc + f * w;
+                    cur = b + 1;
+                    acc = (1.0f - f) * w;
+                } else {
+                    acc += w;
+                }
+            }
+            if (cur >= 0 && cur < ng) dst[cur * ng + x] += acc;
+        }
+    }
+    __syncwarp();
+    for (int task = lane; task < ncol * ng; task += 32) {
+        const int c = task / ng, bb = task - c * ng;
+        const float nf = wp.normf[bb];
+        const int gcol = S.col_gas[c];
+        float acc = 0.0f;
+        if (nf != 0.0f) {
+            const float* Rb = R + bb * ng;
+            const float* Cb = Cw + bb * ng;
+            if (gcol == S.ngas) {                 // temperature: dk1(i)[*a1] + dk2(j)*a2
+                float su = 0.0f, sv = 0.0f;
+                for (int t = 0; t < ng; ++t) {
+                    su = fmaf(wp.dk1[t], Rb[t], su);
+                    sv = fmaf(wp.dk2[t], Cb[t], sv);
+                }
+                acc = (P.first ? su * P.a1 : su) + sv * P.a2;
+            } else if (gcol == P.igas) {          // the gas being added: k2(j)
+                for (int t = 0; t < ng; ++t) acc = fmaf(wp.k2[t], Cb[t], acc);
+            } else if (gcol < P.igas) {           // an earlier gas
+                if (!P.first || gcol == 0) {
+                    const float* u = P.first ? wp.k1 : colP + c * kMaxNg;
+                    for (int t = 0; t < ng; ++t) acc = fmaf(u[t], Rb[t], acc);
+                }
+            }
+            acc = acc / nf;
+        }
+        colN[c * kMaxNg + bb] = acc;
     }
     __syncwarp();
 }
@@ -669,30 +777,46 @@ __device__ __forceinline__ void planck_fp32(int ispace, float vwave, float T, fl
     const float x = c2 * y / T;
     const float em1 = expm1f(x);
     B = a / em1;
-    // dB/dT = B * (x/T) * e^x/(e^x-1)
     dBdT = B * (x / T) * ((em1 + 1.0f) / em1);
 }
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 2)
-fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int npath_max) {
+__global__ void __launch_bounds__(kThreads, 5)
+fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) {
     extern __shared__ __align__(16) char smem[];
-    const Layout Lo = make_layout(B.ng, Lmax, nsw_max, ncol_max, nlmax_max, npath_max);
+    __shared__ SpecDev S_sh;
+    const Layout Lo = make_layout(B.ng, nsw_max, ncol_max, nlmax_max, npath_max);
     const WarpOff wo = warp_off(ncol_max);
     const PathOff po = path_off(nlmax_max, B.ng, nsw_max);
     double* g_ord = (double*)(smem + Lo.off_gord);
     float* delg = (float*)(smem + Lo.off_delg);
-    float* tau_s = (float*)(smem + Lo.off_tau);
-    float* dtau_s = (float*)(smem + Lo.off_dtau);
     char* region = smem + Lo.off_region;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ng = B.ng;
-    for (int i = tid; i <= ng; i += kThreads) g_ord[i] = B.g_ord[i];
+    // per-CTA scratch slot in global memory (L2-resident): tau[l][g], dtau[l][s][g]
+    float* tau_s = B.cell_scratch + (int64_t)blockIdx.x * B.cell_slot;
+    float* dtau_s = tau_s + (int64_t)B.cell_Lmax * ng;
+    for (int i = tid; i <= ng + 2; i += kThreads) g_ord[i] = i <= ng ? B.g_ord[i] : __longlong_as_double(0x7ff0000000000000ll);
     for (int i = tid; i < ng; i += kThreads) delg[i] = B.delg[i];
-    Diag dg{0, 0, 0, 0};
+    Diag dg{0, 0, 0, 0, 0};
     __syncthreads();
+
+    char* wsm = region + warp * Lo.warp_bytes;
+    WarpPtr wp;
+    wp.bufA = (unsigned long long*)(wsm + wo.bufA);
+    wp.bufB = (unsigned long long*)(wsm + wo.bufB);
+    wp.k1 = (float*)(wsm + wo.k1);
+    wp.k2 = (float*)(wsm + wo.k2);
+    wp.dk1 = (float*)(wsm + wo.dk1);
+    wp.dk2 = (float*)(wsm + wo.dk2);
+    wp.kg = (float*)(wsm + wo.kg);
+    wp.normf = (float*)(wsm + wo.normf);
+    wp.splitfrac = (double*)(wsm + wo.splitfrac);
+    wp.splitpos = (int*)(wsm + wo.splitpos);
+    float* colA = (float*)(wsm + wo.colA);
+    float* colB = (float*)(wsm + wo.colB);
 
     for (int64_t item = blockIdx.x; item < B.nitems; item += gridDim.x) {
         // locate the spectrum of this item
@@ -702,7 +826,6 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
             if (B.item_start[mid] <= item) lo = mid; else hi = mid - 1;
         }
         const int sidx = lo;
-        __shared__ SpecDev S_sh;
         {
             const int* src = (const int*)(B.spec + sidx);
             int* dst = (int*)&S_sh;
@@ -716,24 +839,16 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
         const int nsw = S.nsw, ncol = S.ncol;
 
         // ---------------- stage A: layers --------------------------------
-        char* wsm = region + warp * Lo.warp_bytes;
-        float* colA = (float*)(wsm + wo.colA);
-        float* colB = (float*)(wsm + wo.colB);
-        float* k1s = (float*)(wsm + wo.k1);
-        float* k2s = (float*)(wsm + wo.k2);
-        float* dk1s = (float*)(wsm + wo.dk1);
-        float* dk2s = (float*)(wsm + wo.dk2);
-        float* kgs = (float*)(wsm + wo.kg);
         for (int l = warp; l < S.nlayer; l += kWarps) {
             const int64_t il_glob = S.lay_off + l;
             const LayerDev L = B.lay[il_glob];
             float dtc[kMaxSw];
-            const float taucon = continuum(B, S, L, W, iw_glob, il_glob, dtc);
+            const float taucon = continuum(B, S, L, W, iw_glob, il_glob, lane, dtc);
             const float* amo = B.amo + S.lg_off + (int64_t)l * S.ngas;
             const int64_t* slices = B.wg_slice + S.wg_off + (int64_t)iw * S.ngas;
             float* colP = colA;
             float* colN = colB;
-            float kgv;   // lane value of the running k-distribution
+            float kgv;
             if (S.ngas == 1) {
                 float k0, d0;
                 get_kg_lane(B, slices[0], L, lane, k0, d0);
@@ -754,8 +869,8 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
                     const float a2 = amo[ig];
                     const float a1 = first ? amo[0] : 1.0f;
                     const float k1e = first ? k1v : kgv;
-                    const bool z1 = __shfl_sync(0xffffffffu, k1e, ng - 1) == 0.0f;
-                    const bool z2 = __shfl_sync(0xffffffffu, k2v, ng - 1) == 0.0f;
+                    const bool z1 = __shfl_sync(kFull, k1e, ng - 1) == 0.0f;
+                    const bool z2 = __shfl_sync(kFull, k2v, ng - 1) == 0.0f;
                     int16_t* dp = nullptr;
                     int16_t* dsp = nullptr;
                     if (B.dbg_perm && sidx == 0) {
@@ -786,36 +901,34 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
                                 if (first) {
                                     if (g == S.ngas) v = __fmul_rn(d1v, a1);
                                     else if (g == 0) v = k1v;
-                                    else if (g == 1) v = 0.0f;
                                     else v = 0.0f;
                                 } else {
                                     if (g == ig) v = 0.0f;
-                                    else v = colP[c * kMaxNg + lane];   // T column unchanged, earlier gases kept
+                                    else v = colP[c * kMaxNg + lane];
                                 }
                                 colN[c * kMaxNg + lane] = v;
                             }
                         }
                         kgv = first ? __fmul_rn(k1v, a1) : kgv;
                     } else {
-                        // stage the operands for arbitrary-lane access
                         if (lane < ng) {
-                            k1s[lane] = k1e;
-                            k2s[lane] = k2v;
+                            wp.k1[lane] = k1e;
+                            wp.k2[lane] = k2v;
                             float d1e = d1v;
                             if (!first) {
                                 d1e = 0.0f;
                                 for (int c = 0; c < ncol; ++c)
                                     if (S.col_gas[c] == S.ngas) d1e = colP[c * kMaxNg + lane];
                             }
-                            dk1s[lane] = d1e;
-                            dk2s[lane] = d2v;
+                            wp.dk1[lane] = d1e;
+                            wp.dk2[lane] = d2v;
                         }
                         __syncwarp();
                         PassCtx P;
                         P.ng = ng; P.nloop = ng * ng; P.ncol = ncol; P.first = first; P.igas = ig;
                         P.a1 = a1; P.a2 = a2;
-                        sort_pass(B, S, P, wsm, wo, g_ord, delg, lane, dg, colP, colN, dp, dsp);
-                        kgv = lane < ng ? kgs[lane] : 0.0f;
+                        sort_pass(B, S, P, wp, g_ord, delg, lane, dg, colP, colN, dp, dsp);
+                        kgv = lane < ng ? wp.kg[lane] : 0.0f;
                     }
                     __syncwarp();
                     float* t = colP; colP = colN; colN = t;
@@ -868,7 +981,7 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
                         const float td = -expm1f(-tau) * tr;
                         const float trn = tr * expf(-tau);
                         R = fmaf(bb[j], td, R);
-                        drdt[j * ng + g] = trn;     // transmission to the top of layer j's bottom
+                        drdt[j * ng + g] = trn;
                         trd[j * ng + g] = td;
                         tr = trn;
                     }
@@ -894,9 +1007,9 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
                     float y = fmaxf(-tsum, -500.0f);
                     if (y >= 88.7f) y = 88.7f;
                     const float e = (float)exp((double)y);
-                    float out, dr;
                     // IMOD 0: dcoutdq = -tau*T*dtau/dq; IMOD 1: tau*(1-A)*dtau/dq with
                     // 1-A formed as T itself (no cancellation when T < 2^-25)
+                    float out, dr;
                     if (im == 0) { out = e; dr = -tsum * e; }
                     else { out = 1.0f - e; dr = tsum * e; }
                     for (int j = 0; j < nlays; ++j) { drdt[j * ng + g] = dr; trd[j * ng + g] = 0.0f; }
@@ -928,8 +1041,7 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
                 if (em && s == S.sw_T) {
                     const float dB = dbdt[j];
                     const float* td = trd + j * ng;
-                    for (int g = 0; g < ng; ++g)
-                        acc = fmaf(delg[g], fmaf(dr[g], dt[g] * sc, td[g] * dB), acc);
+                    for (int g = 0; g < ng; ++g) acc = fmaf(delg[g], fmaf(dr[g], dt[g] * sc, td[g] * dB), acc);
                 } else {
                     for (int g = 0; g < ng; ++g) acc = fmaf(delg[g], dr[g] * (dt[g] * sc), acc);
                 }
@@ -967,20 +1079,27 @@ fwd_kernel(BatchDev B, int Lmax, int nsw_max, int ncol_max, int nlmax_max, int n
         if (dg.tie_passes) atomicAdd(B.counters + 1, dg.tie_passes);
         if (dg.exact_passes) atomicAdd(B.counters + 2, dg.exact_passes);
         if (dg.irregular) atomicAdd(B.counters + 3, dg.irregular);
+        if (dg.block_passes) atomicAdd(B.counters + 4, dg.block_passes);
     }
 }
 
 // host-side helpers exported to host.cu
-int fwd_smem_bytes(int ng, int Lmax, int nsw, int ncol, int nlmax, int npath) {
-    return make_layout(ng, Lmax, nsw, ncol, nlmax, npath).total;
+int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath) {
+    return make_layout(ng, nsw, ncol, nlmax, npath).total;
 }
 
-cudaError_t launch_fwd(const BatchDev& B, int Lmax, int nsw, int ncol, int nlmax, int npath, int grid,
-                       cudaStream_t st) {
-    const int smem = fwd_smem_bytes(B.ng, Lmax, nsw, ncol, nlmax, npath);
+int fwd_blocks_per_sm(int smem) {
+    int nb = 0;
+    if (cudaFuncSetAttribute(fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fwd_kernel, kThreads, smem) != cudaSuccess) return 0;
+    return nb;
+}
+
+cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st) {
+    const int smem = fwd_smem_bytes(B.ng, nsw, ncol, nlmax, npath);
     cudaError_t e = cudaFuncSetAttribute(fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    fwd_kernel<<<grid, kThreads, smem, st>>>(B, Lmax, nsw, ncol, nlmax, npath);
+    fwd_kernel<<<grid, kThreads, smem, st>>>(B, nsw, ncol, nlmax, npath);
     return cudaGetLastError();
 }
 

@@ -20,9 +20,9 @@
 #include "rtb_common.h"
 
 namespace rtb {
-int fwd_smem_bytes(int ng, int Lmax, int nsw, int ncol, int nlmax, int npath);
-cudaError_t launch_fwd(const BatchDev& B, int Lmax, int nsw, int ncol, int nlmax, int npath, int grid,
-                       cudaStream_t st);
+int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath);
+int fwd_blocks_per_sm(int smem);
+cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st);
 }  // namespace rtb
 
 using namespace rtb;
@@ -95,7 +95,7 @@ struct rtb_context {
     std::vector<float> cia_tk;               // sngl(temps)
     DevBuf d_kcia;
     // per-call arena
-    DevBuf d_in, d_out, d_diag;
+    DevBuf d_in, d_out, d_diag, d_cells;
     HostPinned h_in, h_out;
     // options and diagnostics
     int strict_ties = 0;
@@ -567,11 +567,13 @@ int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
         const int r = pack_spectrum(c, atms[s], st);
         if (r) return r;
     }
-    const int smem = fwd_smem_bytes(c->ng, st.Lmax, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max);
+    const int smem = fwd_smem_bytes(c->ng, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max);
     int smem_max = 0;
     CUDA_TRY(c, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     if (smem > smem_max)
         return fail(c, RTB_ERR_UNSUPPORTED, "spectrum needs %d B of shared memory (device %d)", smem, smem_max);
+    const int bpsm = fwd_blocks_per_sm(smem);
+    if (bpsm <= 0) return fail(c, RTB_ERR_CUDA, "forward kernel cannot be resident (smem %d B)", smem);
     struct Seg {
         const void* src;
         size_t n;
@@ -656,9 +658,15 @@ int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
         B.dbg_perm = (int16_t*)c->d_dbg_perm.p;
         B.dbg_split = (int16_t*)c->d_dbg_split.p;
     }
-    int64_t grid = (int64_t)c->nsm * 2;
+    int64_t grid = (int64_t)c->nsm * bpsm;
     if (grid > B.nitems) grid = B.nitems;
     c->grid = (int)grid;
+    // one scratch slot per CTA: tau[Lmax][ng] + dtau[Lmax][nsw][ng]
+    B.cell_Lmax = st.Lmax;
+    B.cell_slot = (int64_t)st.Lmax * c->ng * (1 + st.nsw_max);
+    B.cell_slot = (B.cell_slot + 63) & ~(int64_t)63;
+    CUDA_TRY(c, c->d_cells.ensure((size_t)grid * B.cell_slot * sizeof(float)));
+    B.cell_scratch = (float*)c->d_cells.p;
     c->Lmax = st.Lmax;
     c->nsw_max = st.nsw_max;
     c->ncol_max = st.ncol_max;
@@ -691,7 +699,7 @@ int launch(rtb_context* c) {
     const cudaStream_t strm = stream_of(c);
     CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, strm));
     CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
-    CUDA_TRY(c, launch_fwd(c->B, c->Lmax, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, strm));
+    CUDA_TRY(c, launch_fwd(c->B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, strm));
     CUDA_TRY(c, cudaEventRecord(c->ev1, strm));
     return RTB_OK;
 }
@@ -712,6 +720,7 @@ int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float*
     c->stats.tie_passes = (long long)diag[2];
     c->stats.exact_passes = (long long)diag[3];
     c->stats.irregular_passes = (long long)diag[4];
+    c->stats.block_passes = (long long)diag[5];
     c->stats.ms_kernel = ms;
     c->stats.h2d_bytes = (long long)c->in_bytes;
     c->stats.d2h_bytes = (long long)c->out_bytes;
@@ -774,6 +783,7 @@ void rtb_destroy(rtb_context* c) {
     c->d_in.release();
     c->d_out.release();
     c->d_diag.release();
+    c->d_cells.release();
     c->d_dbg_perm.release();
     c->d_dbg_split.release();
     c->h_in.release();

@@ -13,7 +13,7 @@ constexpr int kMaxNg = 32;        // one lane per g-ordinate
 constexpr int kMaxCols = 8;       // tracked gradient columns in the overlap (active gases + T)
 constexpr int kMaxSw = 8;         // active Jacobian columns (isw) per spectrum
 constexpr int kMaxGasDev = 30;    // MAXGAS
-constexpr int kWarps = 8;         // warps per CTA of the forward kernel
+constexpr int kWarps = 4;         // warps per CTA of the forward kernel
 constexpr int kThreads = kWarps * 32;
 
 // status bits accumulated by the kernel (OR-ed into a device word)
@@ -97,6 +97,10 @@ struct BatchDev {
     const float* delg;           // [ng]
     const double* g_ord;         // [ng+1], g_ord[ng] forced >= 1 (rankg.f:65-67)
     const float* kcia;           // (9,25,1501) Fortran order
+    // per-CTA scratch slots (tau, dtau/dq of every layer of the current item)
+    float* cell_scratch;
+    int64_t cell_slot;             // floats per slot
+    int cell_Lmax;                 // layers per slot
     // outputs
     float* calcout;
     float* gradients;

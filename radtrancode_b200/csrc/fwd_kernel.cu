@@ -656,6 +656,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             }
             const bool closes = bb < c_last;
             const int pend = closes ? wp.splitpos[bb] : nloop;
+#pragma unroll 4
             for (; p < pend; ++p) {
                 const unsigned long long word = A[p];
                 const unsigned q = (unsigned)word & 0xffffu;
@@ -713,6 +714,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             float* dst = pass == 0 ? R : Cw;
             int cur = -1;
             float acc = 0.0f;
+#pragma unroll 4
             for (int y = 0; y < ng; ++y) {
                 const int e = pass == 0 ? x * ng + y : y * ng + x;
                 const unsigned char code = eb[e];
@@ -746,16 +748,19 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             const float* Cb = Cw + bb * ng;
             if (gcol == S.ngas) {                 // temperature: dk1(i)[*a1] + dk2(j)*a2
                 float su = 0.0f, sv = 0.0f;
+#pragma unroll 4
                 for (int t = 0; t < ng; ++t) {
                     su = fmaf(wp.dk1[t], Rb[t], su);
                     sv = fmaf(wp.dk2[t], Cb[t], sv);
                 }
                 acc = (P.first ? su * P.a1 : su) + sv * P.a2;
             } else if (gcol == P.igas) {          // the gas being added: k2(j)
+#pragma unroll 4
                 for (int t = 0; t < ng; ++t) acc = fmaf(wp.k2[t], Cb[t], acc);
             } else if (gcol < P.igas) {           // an earlier gas
                 if (!P.first || gcol == 0) {
                     const float* u = P.first ? wp.k1 : colP + c * kMaxNg;
+#pragma unroll 4
                     for (int t = 0; t < ng; ++t) acc = fmaf(u[t], Rb[t], acc);
                 }
             }

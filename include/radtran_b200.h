@@ -212,6 +212,37 @@ int rtb_get_debug_bins(const rtb_context* ctx, int16_t* perm, size_t n_perm,
  * boundary; 1 takes it for every pass that has a tie. */
 int rtb_set_strict_ties(rtb_context* ctx, int on);
 
+/* rtb_fwd_launch_static -- rtb_fwd_launch without the context's scratch.
+ * No counterpart in the reference (the reference has no device memory).
+ *
+ * Some callers must not allocate device memory at the moment they run the
+ * forward model: an application that reserves its whole device-memory budget
+ * at start-up and hands the library nothing more, or a retrieval or serving
+ * loop that keeps cudaMalloc/cudaFree out of its steady state because those
+ * calls can synchronise the device and stall every other stream on it.  This
+ * entry point runs the forward kernel on the batch resident from
+ * rtb_fwd_prepare and allocates nothing: the kernel's per-block scratch (the
+ * optical depths and their derivatives for every layer of the wavenumber a
+ * block is working on) comes from one array compiled into the library,
+ * RTB_STATIC_SCRATCH_BYTES per device, instead of the context's scratch.
+ * Outputs, status and statistics are read with rtb_fwd_fetch as usual.
+ *
+ * First call: the first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current) and keeps it for
+ * the process; make that first call before any stream capture is started.
+ * Limit: a batch whose per-block slot (layers x NG x (1 + gradient columns)
+ * floats) does not fit in RTB_STATIC_SCRATCH_BYTES is refused with
+ * RTB_ERR_LIMIT; a batch whose slots fit fewer blocks than rtb_fwd_launch
+ * would use runs on that many blocks.  Nothing in the array needs to start at
+ * zero; the status and counter words that do are cleared on the stream by
+ * every call.
+ * Races: the array is one per device, shared by every context of the process
+ * on that device.  Two calls whose kernels can overlap in time (different
+ * streams, contexts or host threads on the same device) overwrite each
+ * other's scratch; order them on one stream or with events. */
+#define RTB_STATIC_SCRATCH_BYTES (32u << 20)
+int rtb_fwd_launch_static(rtb_context* ctx);
+
 #ifdef __cplusplus
 }
 #endif

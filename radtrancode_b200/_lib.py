@@ -65,6 +65,8 @@ def lib() -> C.CDLL:
         L.rtb_fwd_fetch.restype = C.c_int
         L.rtb_set_stream.argtypes = [vp, vp]
         L.rtb_set_stream.restype = C.c_int
+        L.rtb_fwd_launch_static.argtypes = [vp]
+        L.rtb_fwd_launch_static.restype = C.c_int
         p16 = C.POINTER(C.c_int16)
         L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
         L.rtb_get_debug_bins.restype = C.c_int
@@ -77,5 +79,5 @@ EXPORTED = [
     "rtb_create", "rtb_destroy", "rtb_last_error", "rtb_version", "rtb_set_ktables", "rtb_set_cia",
     "rtb_cirsrtfg_wave", "rtb_cirsrtfg_wave_batch", "rtb_get_fwd_stats", "rtb_set_debug",
     "rtb_get_debug_bins", "rtb_set_strict_ties", "rtb_fwd_prepare", "rtb_fwd_launch", "rtb_fwd_fetch",
-    "rtb_set_stream",
+    "rtb_set_stream", "rtb_fwd_launch_static",
 ]

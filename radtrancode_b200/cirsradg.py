@@ -123,6 +123,11 @@ class Context:
     def launch(self):
         self._check(self._L.rtb_fwd_launch(self._h))
 
+    def launch_static(self):
+        """rtb_fwd_launch_static: the same launch with its scratch taken from
+        the library's fixed per-device array, allocating nothing."""
+        self._check(self._L.rtb_fwd_launch_static(self._h))
+
     def fetch(self):
         jobs = self._prepared_jobs
         n = len(jobs)

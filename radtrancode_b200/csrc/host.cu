@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -746,6 +747,57 @@ int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calc
     return fetch(c, calcout, gradients, gradtsurf);
 }
 
+// Scratch of rtb_fwd_launch_static: one fixed array per device, part of the
+// library's device image, so that the call never goes to the allocator.  The
+// kernel writes every entry of a slot before it reads it, so nothing here has
+// to start at zero.
+static __device__ __align__(256) float g_fwd_static_scratch[RTB_STATIC_SCRATCH_BYTES / sizeof(float)];
+
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_mu;
+void* g_static_addr[kMaxStaticDevices] = {};
+
+// device address of g_fwd_static_scratch on c->device (current), looked up
+// once per device and kept for the process
+int static_scratch_addr(rtb_context* c, float** out) {
+    if (c->device >= kMaxStaticDevices)
+        return fail(c, RTB_ERR_LIMIT, "static scratch supports devices 0..%d", kMaxStaticDevices - 1);
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[c->device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_fwd_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(c, RTB_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed on device %d: %s", c->device,
+                        cudaGetErrorString(e));
+        g_static_addr[c->device] = p;
+    }
+    *out = (float*)g_static_addr[c->device];
+    return RTB_OK;
+}
+
+int launch_static(rtb_context* c) {
+    if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    float* base = nullptr;
+    const int r = static_scratch_addr(c, &base);
+    if (r) return r;
+    const size_t slot_bytes = (size_t)c->B.cell_slot * sizeof(float);
+    const size_t nslot = (size_t)RTB_STATIC_SCRATCH_BYTES / slot_bytes;
+    if (nslot < 1)
+        return fail(c, RTB_ERR_LIMIT,
+                    "forward scratch slot of %zu B (%d layers x NG %d x %d columns) exceeds the static scratch of %u B",
+                    slot_bytes, c->Lmax, c->ng, 1 + c->nsw_max, (unsigned)RTB_STATIC_SCRATCH_BYTES);
+    const int grid = nslot < (size_t)c->grid ? (int)nslot : c->grid;
+    BatchDev B = c->B;
+    B.cell_scratch = base;
+    const cudaStream_t strm = stream_of(c);
+    CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, strm));
+    CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
+    CUDA_TRY(c, launch_fwd(B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, grid, strm));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, strm));
+    return RTB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -914,6 +966,8 @@ int rtb_set_strict_ties(rtb_context* c, int on) {
     c->strict_ties = on ? 1 : 0;
     return RTB_OK;
 }
+
+int rtb_fwd_launch_static(rtb_context* c) { return launch_static(c); }
 
 int rtb_get_debug_bins(const rtb_context* c, int16_t* perm, size_t n_perm, int16_t* split, size_t n_split) {
     if (!c || !c->debug) return RTB_ERR_ARG;

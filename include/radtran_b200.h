@@ -212,6 +212,115 @@ int rtb_get_debug_bins(const rtb_context* ctx, int16_t* perm, size_t n_perm,
  * boundary; 1 takes it for every pass that has a tie. */
 int rtb_set_strict_ties(rtb_context* ctx, int on);
 
+/* ---------------------------------------------------------------------- */
+/* Optimal-estimation Newton step (calc_gain_matrix + calcnextxn)          */
+/* ---------------------------------------------------------------------- */
+
+/* How the device forms K^T Se^-1 K:
+ *   RTB_HESS_TC   tensor cores: Se^-1/2 K split into bf16 hi + lo parts,
+ *                 three products per tile, FP32 accumulation; then `refine`
+ *                 steps of iterative refinement in FP64 (default, refine 1);
+ *   RTB_HESS_FP64 FP64 on the CUDA cores (the all-FP64 solve).
+ * The Cholesky factorisation and the solves are FP64 in both. */
+#define RTB_HESS_TC   0
+#define RTB_HESS_FP64 1
+int rtb_set_newton_mode(rtb_context* ctx, int hessian, int refine);
+
+/* rtb_newton_step_batch -- the Newton step of nret independent retrievals
+ * with diagonal Se (nemesis/calc_gain_matrix.f:123-163 for nx < ny, with
+ * radtran/matrices/dinvertm.f jmod=2, then nemesis/calcnextxn.f:64-104):
+ *     x_out = xa + D (y - yn) - AA (xa - xn)
+ * computed as xa + C^-1 K^T Se^-1 (y - yn + K (xn - xa)), C = K^T Se^-1 K +
+ * Sa^-1, without forming D or AA.  All arrays are host memory, retrieval r at
+ * r * (its size):
+ *   kk     [nret][nx][ny]  K^T: the `gradients` packing of rtb_cirsrtfg_wave
+ *                          for one path, i.e. Fortran kk(ny, nx) with leading
+ *                          dimension ny
+ *   sei    [nret][ny]      diagonal of Se^-1 (the reference's dense sei(my,my)
+ *                          is diagonal in every NEMESIS caller)
+ *   sai    [nret][nx][nx]  Sa^-1
+ *   xa, xn [nret][nx], y, yn [nret][ny]
+ *   x_out  [nret][nx]      out
+ *   nonpd  [nret]          out, may be NULL: 1 where a Cholesky pivot was <= 0
+ *                          and replaced by 1 (dcholdc.f:69-84; the reference
+ *                          continues the same way)
+ *   resid  [nret]          out, may be NULL: ||rhs - C dx|| / ||rhs|| of the
+ *                          final solve, C applied in FP64
+ * 1 <= nx <= 128 on the device (NX = 124 at full size), nx < ny. */
+int rtb_newton_step_batch(rtb_context* ctx, int nret, int nx, int ny, const float* kk, const double* sei,
+                          const double* sai, const float* xa, const float* xn, const float* y,
+                          const float* yn, float* x_out, int* nonpd, double* resid);
+
+/* calc_phiret (nemesis/calc_phiret.f:49-102) for nret retrievals, diagonal
+ * Se: phi = (yn-y)^T Se^-1 (yn-y) + (xn-xa)^T Sa^-1 (xn-xa), chisq = the
+ * first term, both REAL as in the reference.  Layouts as above. */
+int rtb_calc_phiret_batch(rtb_context* ctx, int nret, int nx, int ny, const float* y, const float* yn,
+                          const double* sei, const float* xn, const float* xa, const double* sai,
+                          float* phi, float* chisq);
+
+/* dinvertm (radtran/matrices/dinvertm.f jmod=2): inverse of nret symmetric
+ * positive-definite n x n matrices (row-major, a[r*n*n]) by an FP64 Cholesky
+ * factorisation on the device; n <= 128.  nonpd as above. */
+int rtb_spd_inverse_batch(rtb_context* ctx, int nret, int n, const double* a, double* ainv, int* nonpd);
+
+/* ---------------------------------------------------------------------- */
+/* Retrieval loop (coreret Levenberg-Marquardt iteration)                  */
+/* ---------------------------------------------------------------------- */
+
+/* One retrieval of the layer-state model: the state vector is
+ *   x[l]          temperature of layer l, l < nlayer (model 0, one level
+ *                 per layer: DTE = identity, npro = nlayer)
+ *   x[nlayer + a] natural log of a scale factor of gas scale_gas[a]
+ *                 (model 3, nemesis/subprofretg.f:735-741): amount, pp and
+ *                 the gas's xmap column at state x are those of `atm` times
+ *                 exp(x[nlayer + a])
+ * so nx = nlayer + nscale.  `atm` is the atmosphere at scale factor 1 (its
+ * temp is replaced by x, emtemp follows temp through layinc); it must have
+ * one path, and its xmap must hold the matching derivatives (T rows 1, gas
+ * rows the gas's vmr per level).  Host pointers; read during the call only. */
+typedef struct rtb_retrieval_spec {
+    const rtb_atm* atm;
+    int nscale;
+    const int* scale_gas;     /* [nscale] 0-based gas index into atm */
+    const float* y;           /* [ny] measurement, ny = atm->nwave */
+    const double* sei;        /* [ny] diagonal of Se^-1 */
+    const double* sa;         /* [nx][nx] a priori covariance */
+    const float* xa;          /* [nx] a priori state */
+    const float* x0;          /* [nx] first guess; NULL = xa */
+} rtb_retrieval_spec;
+
+typedef struct rtb_retrieval_opts {
+    int kiter;                /* Newton iterations (coreret.f:592 loop bound) */
+    float phlimit;            /* convergence limit on the % change of phi (coreret.f:1003) */
+    float dchisq_stop;        /* > 0: also stop when |chisq change| < this after an accepted step
+                                 (a rule the reference does not have); <= 0: off */
+    int max_batch;            /* retrievals resident at once (0 = all) */
+} rtb_retrieval_opts;
+
+typedef struct rtb_retrieval_result {
+    float* x;                 /* [nx] out: final state (caller buffer) */
+    float* yn;                /* [ny] out: spectrum at x (caller buffer, may be NULL) */
+    float phi, chisq;         /* cost and chi^2 at x (calc_phiret) */
+    float alambda;            /* final Marquardt brake */
+    int iterations;           /* iterations taken */
+    int forwards;             /* forward-model evaluations, the first included */
+    int converged;            /* 0 kiter reached, 1 phlimit rule, 2 coreret.f:1022-1062
+                                 alternate rule, 3 dchisq_stop */
+    int nonpd;                /* a Cholesky pivot was replaced in some step */
+    double ms;                /* wall time from start of the call to this result */
+} rtb_retrieval_result;
+
+/* Run nret retrievals to completion.  All retrievals iterate together: each
+ * round runs one Newton step on the device for every retrieval whose K
+ * changed, then one batched forward+Jacobian launch for every trial state,
+ * then the cost on the device, and the coreret decision per retrieval
+ * (accept: alambda *= 0.3; reject: *= 10, cap 1e10; trial states with T < 1
+ * or a NaN are rejected before the forward model, coreret.f:642-790).
+ * K, spectra, Se^-1, Sa^-1 and the states stay in device memory between
+ * rounds. */
+int rtb_retrieve_batch(rtb_context* ctx, int nret, const rtb_retrieval_spec* specs,
+                       const rtb_retrieval_opts* opts, rtb_retrieval_result* results);
+
 /* rtb_fwd_launch_static -- rtb_fwd_launch without the context's scratch.
  * No counterpart in the reference (the reference has no device memory).
  *

@@ -125,6 +125,21 @@ float orc_calc_phiret_diag(int ny, const float* y, const float* yn,
 /* dinvertm(jmod=2): Cholesky inverse with the A*Ainv check; returns icheck */
 int orc_dinvertm_chol(int n, int lda, const double* a, double* ainv);
 
+/* --- retrieval loop (nemesis/coreret.f:520-1106) for the layer-state
+ *     model of rtb_retrieve_batch ------------------------------------- */
+#define ORC_TRACE_MAX 64
+typedef struct orc_retrieval_trace {
+    int n;                          /* iterations recorded */
+    float phi[ORC_TRACE_MAX];       /* cost of the trial state (0: rejected before the forward model) */
+    int verdict[ORC_TRACE_MAX];     /* 0 rejected before the forward model, 1 accepted, 2 rejected */
+    float alambda[ORC_TRACE_MAX];   /* brake after the iteration */
+} orc_retrieval_trace;
+/* spectrum yn[ny] and kk[nx][ny] (gradients packing) at state x */
+int orc_forward_state(const orc_tables* tab, const rtb_retrieval_spec* s, const float* x, int precision,
+                      int nthreads, float* yn, float* kk);
+int orc_retrieve(const orc_tables* tab, const rtb_retrieval_spec* s, const rtb_retrieval_opts* o, int precision,
+                 int nthreads, rtb_retrieval_result* res, orc_retrieval_trace* tr);
+
 #ifdef __cplusplus
 }
 #endif

@@ -141,3 +141,85 @@ def rankg(gw, weight, cont, grad):
                      _abi.fptr(cont), _abi.fptr(grad), _abi.fptr(k_g), _abi.fptr(dkdq),
                      perm.ctypes.data_as(C.POINTER(C.c_int16)), split.ctypes.data_as(C.POINTER(C.c_int16)))
     return st, k_g, dkdq, perm, split
+
+
+class OrcTrace(C.Structure):
+    _fields_ = [("n", C.c_int), ("phi", C.c_float * 64), ("verdict", C.c_int * 64), ("alambda", C.c_float * 64)]
+
+
+def forward_state(kt, cia, case, x, precision=ORC_MIXED, nthreads=1):
+    """Spectrum yn[ny] and K^T [nx, ny] of a retrieval case at state x."""
+    L = lib()
+    t = tables_struct(kt, cia)
+    s = case.as_struct()
+    x = np.ascontiguousarray(x, np.float32)
+    yn = np.zeros(case.ny, np.float32)
+    kk = np.zeros((case.nx, case.ny), np.float32)
+    st = L.orc_forward_state(C.byref(t), C.byref(s), _abi.fptr(x), precision, nthreads, _abi.fptr(yn),
+                             _abi.fptr(kk))
+    if st != 0:
+        raise RuntimeError(f"oracle status {_abi.STATUS_NAMES.get(st, st)}")
+    return yn, kk
+
+
+def retrieve(kt, cia, case, kiter=10, phlimit=0.1, dchisq_stop=0.0, precision=ORC_MIXED, nthreads=1):
+    """coreret restatement on one case: (result dict, trace dict)."""
+    L = lib()
+    t = tables_struct(kt, cia)
+    s = case.as_struct()
+    o = _abi.RtbRetrievalOpts(kiter, phlimit, dchisq_stop, 0)
+    x = np.zeros(case.nx, np.float32)
+    yn = np.zeros(case.ny, np.float32)
+    r = _abi.RtbRetrievalResult()
+    r.x, r.yn = _abi.fptr(x), _abi.fptr(yn)
+    tr = OrcTrace()
+    st = L.orc_retrieve(C.byref(t), C.byref(s), C.byref(o), precision, nthreads, C.byref(r), C.byref(tr))
+    if st != 0:
+        raise RuntimeError(f"oracle status {_abi.STATUS_NAMES.get(st, st)}")
+    res = {k: getattr(r, k) for k in _abi.RESULT_KEYS}
+    res["x"], res["yn"] = x, yn
+    trace = {"phi": np.array(tr.phi[:tr.n], np.float32), "verdict": np.array(tr.verdict[:tr.n]),
+             "alambda": np.array(tr.alambda[:tr.n], np.float32)}
+    return res, trace
+
+
+def newton_step(kk, sei, sai, xa, xn, y, yn):
+    """calc_gain_matrix (diagonal Se, dense D and AA) + calcnextxn for one
+    retrieval: kk [nx, ny] (Fortran kk(ny, nx)), sei [ny], sai [nx, nx]."""
+    L = lib()
+    kk = np.ascontiguousarray(kk, np.float32)
+    nx, ny = kk.shape
+    sai = np.asfortranarray(sai, np.float64)
+    sei = np.ascontiguousarray(sei, np.float64)
+    dd = np.zeros((nx, ny), order="F")
+    aa = np.zeros((nx, nx), order="F")
+    dp = C.POINTER(C.c_double)
+    L.orc_calc_gain_matrix_diag(nx, ny, nx, ny, _abi.fptr(kk), sai.ctypes.data_as(dp), sei.ctypes.data_as(dp),
+                                dd.ctypes.data_as(dp), aa.ctypes.data_as(dp), None)
+    x_out = np.zeros(nx, np.float32)
+    f = lambda a: _abi.fptr(np.ascontiguousarray(a, np.float32))
+    xa, xn, y, yn = (np.ascontiguousarray(a, np.float32) for a in (xa, xn, y, yn))
+    L.orc_calcnextxn(nx, ny, nx, f(xa), f(xn), f(y), f(yn), dd.ctypes.data_as(dp), aa.ctypes.data_as(dp),
+                     _abi.fptr(x_out))
+    return x_out
+
+
+def calc_phiret(y, yn, sei, xn, xa, sai):
+    L = lib()
+    dp = C.POINTER(C.c_double)
+    y, yn, xn, xa = (np.ascontiguousarray(a, np.float32) for a in (y, yn, xn, xa))
+    sei = np.ascontiguousarray(sei, np.float64)
+    sai = np.asfortranarray(sai, np.float64)
+    chisq = C.c_float(0.0)
+    phi = L.orc_calc_phiret_diag(len(y), _abi.fptr(y), _abi.fptr(yn), sei.ctypes.data_as(dp), len(xn), len(xn),
+                                 _abi.fptr(xn), _abi.fptr(xa), sai.ctypes.data_as(dp), C.byref(chisq))
+    return np.float32(phi), np.float32(chisq.value)
+
+
+def dinvertm(a):
+    L = lib()
+    dp = C.POINTER(C.c_double)
+    a = np.asfortranarray(a, np.float64)
+    out = np.zeros_like(a, order="F")
+    ic = L.orc_dinvertm_chol(a.shape[0], a.shape[0], a.ctypes.data_as(dp), out.ctypes.data_as(dp))
+    return out, ic

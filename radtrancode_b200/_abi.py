@@ -56,6 +56,29 @@ class RtbFwdStats(C.Structure):
     ]
 
 
+class RtbRetrievalSpec(C.Structure):
+    _fields_ = [
+        ("atm", C.POINTER(RtbAtm)), ("nscale", C.c_int), ("scale_gas", _ip),
+        ("y", _fp), ("sei", C.POINTER(C.c_double)), ("sa", C.POINTER(C.c_double)),
+        ("xa", _fp), ("x0", _fp),
+    ]
+
+
+class RtbRetrievalOpts(C.Structure):
+    _fields_ = [("kiter", C.c_int), ("phlimit", C.c_float), ("dchisq_stop", C.c_float), ("max_batch", C.c_int)]
+
+
+class RtbRetrievalResult(C.Structure):
+    _fields_ = [
+        ("x", _fp), ("yn", _fp), ("phi", C.c_float), ("chisq", C.c_float), ("alambda", C.c_float),
+        ("iterations", C.c_int), ("forwards", C.c_int), ("converged", C.c_int), ("nonpd", C.c_int),
+        ("ms", C.c_double),
+    ]
+
+
+RESULT_KEYS = ("phi", "chisq", "alambda", "iterations", "forwards", "converged", "nonpd", "ms")
+
+
 def fptr(a):
     """float* of a contiguous float32 numpy array (None -> NULL)."""
     if a is None:

@@ -142,6 +142,76 @@ class Context:
         self._check(self._L.rtb_fwd_fetch(self._h, p1, p2, p3))
         return outs
 
+    # -- optimal-estimation Newton step and retrieval ----------------------
+    def set_newton_mode(self, hessian=0, refine=1):
+        """hessian 0: K^T Se^-1 K on tensor cores + `refine` refinement
+        steps; 1: all FP64."""
+        self._check(self._L.rtb_set_newton_mode(self._h, hessian, refine))
+
+    def newton_step_batch(self, kk, sei, sai, xa, xn, y, yn):
+        """calc_gain_matrix + calcnextxn for a batch: kk [nret, nx, ny],
+        sei [nret, ny], sai [nret, nx, nx], xa/xn [nret, nx], y/yn [nret, ny].
+        Returns (x_out [nret, nx], nonpd [nret], resid [nret])."""
+        kk = np.ascontiguousarray(kk, np.float32)
+        nret, nx, ny = kk.shape
+        f32 = lambda a: np.ascontiguousarray(a, np.float32)
+        f64 = lambda a: np.ascontiguousarray(a, np.float64)
+        sei, sai, xa, xn, y, yn = f64(sei), f64(sai), f32(xa), f32(xn), f32(y), f32(yn)
+        x_out = np.zeros((nret, nx), np.float32)
+        nonpd = np.zeros(nret, np.int32)
+        resid = np.zeros(nret, np.float64)
+        self._check(self._L.rtb_newton_step_batch(
+            self._h, nret, nx, ny, _abi.fptr(kk), _abi.dptr(sei), _abi.dptr(sai), _abi.fptr(xa), _abi.fptr(xn),
+            _abi.fptr(y), _abi.fptr(yn), _abi.fptr(x_out), _abi.iptr(nonpd), _abi.dptr(resid)))
+        return x_out, nonpd, resid
+
+    def calc_phiret_batch(self, y, yn, sei, xn, xa, sai):
+        f32 = lambda a: np.ascontiguousarray(a, np.float32)
+        f64 = lambda a: np.ascontiguousarray(a, np.float64)
+        y, yn, sei, xn, xa, sai = f32(y), f32(yn), f64(sei), f32(xn), f32(xa), f64(sai)
+        nret, ny = y.shape
+        nx = xn.shape[1]
+        phi = np.zeros(nret, np.float32)
+        chisq = np.zeros(nret, np.float32)
+        self._check(self._L.rtb_calc_phiret_batch(
+            self._h, nret, nx, ny, _abi.fptr(y), _abi.fptr(yn), _abi.dptr(sei), _abi.fptr(xn), _abi.fptr(xa),
+            _abi.dptr(sai), _abi.fptr(phi), _abi.fptr(chisq)))
+        return phi, chisq
+
+    def spd_inverse_batch(self, a):
+        a = np.ascontiguousarray(a, np.float64)
+        nret, n, _ = a.shape
+        out = np.zeros_like(a)
+        nonpd = np.zeros(nret, np.int32)
+        self._check(self._L.rtb_spd_inverse_batch(self._h, nret, n, _abi.dptr(a), _abi.dptr(out),
+                                                  _abi.iptr(nonpd)))
+        return out, nonpd
+
+    def retrieve_batch(self, cases, kiter=10, phlimit=0.1, dchisq_stop=0.0, max_batch=0):
+        """rtb_retrieve_batch on synth.RetrievalCase objects; one result
+        dict per case (x, yn, phi, chisq, alambda, iterations, forwards,
+        converged, nonpd, ms)."""
+        n = len(cases)
+        specs = (_abi.RtbRetrievalSpec * n)()
+        res = (_abi.RtbRetrievalResult * n)()
+        keep, outs = [], []
+        for i, c in enumerate(cases):
+            s = c.as_struct()
+            keep.append(s)
+            specs[i] = s
+            x = np.zeros(c.nx, np.float32)
+            yn = np.zeros(c.ny, np.float32)
+            outs.append((x, yn))
+            res[i].x, res[i].yn = _abi.fptr(x), _abi.fptr(yn)
+        o = _abi.RtbRetrievalOpts(kiter, phlimit, dchisq_stop, max_batch)
+        self._check(self._L.rtb_retrieve_batch(self._h, n, specs, C.byref(o), res))
+        out = []
+        for i in range(n):
+            d = {k: getattr(res[i], k) for k in _abi.RESULT_KEYS}
+            d["x"], d["yn"] = outs[i]
+            out.append(d)
+        return out
+
     def set_stream(self, handle):
         """Issue the context's work on a caller-owned cudaStream_t (int handle,
         e.g. torch.cuda.Stream().cuda_stream); None restores the own stream."""

@@ -1,0 +1,151 @@
+// context.h -- internal: the device context behind the C ABI and the
+// batch staging shared by the forward entry points (host.cu) and the
+// retrieval engine (retrieval.cu).  Not installed; the public interface is
+// include/radtran_b200.h.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/radtran_b200.h"
+#include "rtb_common.h"
+
+namespace rtb {
+int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath);
+int fwd_blocks_per_sm(int smem);
+cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st);
+
+// growable device buffer / pinned host buffer (grow-only, freed by release)
+// growable device buffer
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t c = std::max(n, (size_t)4096);
+        c = c + c / 4;
+        cudaError_t e = cudaMalloc(&p, c);
+        if (e == cudaSuccess) cap = c;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+struct HostPinned {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t c = std::max(n, (size_t)4096);
+        c = c + c / 4;
+        cudaError_t e = cudaMallocHost(&p, c);
+        if (e == cudaSuccess) cap = c;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+// host staging of one batch
+struct Staging {
+    std::vector<SpecDev> spec;
+    std::vector<int64_t> item_start;
+    std::vector<LayerDev> lay;
+    std::vector<float> amo;
+    std::vector<WaveDev> wave;
+    std::vector<int64_t> wg_slice;
+    std::vector<float> xsec, cont;
+    std::vector<int> p_layinc;
+    std::vector<float> p_scale, p_emtemp;
+    std::vector<int> map_colptr, map_row;
+    std::vector<float> map_val;
+    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1;
+    int64_t n_out = 0, n_jac = 0;
+};
+
+// where a batch's outputs go: the context's own arena (nullptr) or caller
+// device arrays, with per-spectrum element offsets
+struct OutPlace {
+    float* calcout;
+    float* gradtsurf;
+    float* gradients;
+    const int64_t* out_off;   // [nspec] into calcout / gradtsurf
+    const int64_t* jac_off;   // [nspec] into gradients
+};
+
+int fail(rtb_context* c, int code, const char* fmt, ...);
+int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st);
+int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* place);
+int launch(rtb_context* c);
+cudaStream_t stream_of(rtb_context* c);
+
+}  // namespace rtb
+
+// the context is the opaque handle of the C ABI (global namespace)
+struct rtb_context {
+    int device = 0;
+    int nsm = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    // k-tables
+    int ntab = 0, np = 0, nt = 0, ng = 0;
+    std::vector<float> lnp, tk, delg;
+    std::vector<double> g_ord;
+    std::vector<float> vmin, delv;
+    std::vector<int> nbin;
+    std::vector<int64_t> tab_off;            // element offset of each table
+    std::vector<std::vector<uint8_t>> nonzero;  // [tab][bin]: any value > 0 (get_kg.f:228-250)
+    rtb::DevBuf d_raw, d_log, d_delg, d_gord;
+    // CIA
+    int has_cia = 0;
+    float dnu = 0.0f;
+    std::vector<float> cia_tk;               // sngl(temps)
+    rtb::DevBuf d_kcia;
+    // per-call arena
+    rtb::DevBuf d_in, d_out, d_diag, d_cells;
+    rtb::HostPinned h_in, h_out;
+    // options and diagnostics
+    int strict_ties = 0;
+    int debug = 0;
+    cudaStream_t user_stream = nullptr;   // caller-provided stream (NULL: own stream)
+    // resident batch (rtb_fwd_prepare)
+    int prepared = 0;
+    int placed = 0;                       // outputs of the resident batch go to caller device arrays
+    rtb::BatchDev B{};
+    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, grid = 1;
+    std::vector<rtb::SpecDev> spec_host;
+    std::vector<int> spec_npath, spec_nv, spec_nwave, spec_nlayer;
+    int64_t n_out = 0, n_jac = 0;
+    size_t in_bytes = 0, out_bytes = 0;
+    long long cells = 0;
+    rtb::DevBuf d_dbg_perm, d_dbg_split;
+    size_t dbg_perm_n = 0, dbg_split_n = 0;
+    rtb_fwd_stats stats{};
+    // Newton step
+    int newton_hess = 0;                  // RTB_HESS_TC / RTB_HESS_FP64
+    int newton_refine = 1;
+    rtb::DevBuf d_nt32, d_nt64, d_ntsmall, d_ntdesc;
+};
+
+#define CUDA_TRY(ctx, call)                                                                 \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(ctx, RTB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)

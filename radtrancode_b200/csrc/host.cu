@@ -17,106 +17,11 @@
 #include <string>
 #include <vector>
 
-#include "../../include/radtran_b200.h"
-#include "rtb_common.h"
-
-namespace rtb {
-int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath);
-int fwd_blocks_per_sm(int smem);
-cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st);
-}  // namespace rtb
+#include "context.h"
 
 using namespace rtb;
 
-namespace {
-
-// growable device buffer
-struct DevBuf {
-    void* p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t n) {
-        if (n <= cap) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        size_t c = std::max(n, (size_t)4096);
-        c = c + c / 4;
-        cudaError_t e = cudaMalloc(&p, c);
-        if (e == cudaSuccess) cap = c;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
-struct HostPinned {
-    void* p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t n) {
-        if (n <= cap) return cudaSuccess;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-        size_t c = std::max(n, (size_t)4096);
-        c = c + c / 4;
-        cudaError_t e = cudaMallocHost(&p, c);
-        if (e == cudaSuccess) cap = c;
-        return e;
-    }
-    void release() {
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
-
-}  // namespace
-
-struct rtb_context {
-    int device = 0;
-    int nsm = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::string err;
-    // k-tables
-    int ntab = 0, np = 0, nt = 0, ng = 0;
-    std::vector<float> lnp, tk, delg;
-    std::vector<double> g_ord;
-    std::vector<float> vmin, delv;
-    std::vector<int> nbin;
-    std::vector<int64_t> tab_off;            // element offset of each table
-    std::vector<std::vector<uint8_t>> nonzero;  // [tab][bin]: any value > 0 (get_kg.f:228-250)
-    DevBuf d_raw, d_log, d_delg, d_gord;
-    // CIA
-    int has_cia = 0;
-    float dnu = 0.0f;
-    std::vector<float> cia_tk;               // sngl(temps)
-    DevBuf d_kcia;
-    // per-call arena
-    DevBuf d_in, d_out, d_diag, d_cells;
-    HostPinned h_in, h_out;
-    // options and diagnostics
-    int strict_ties = 0;
-    int debug = 0;
-    cudaStream_t user_stream = nullptr;   // caller-provided stream (NULL: own stream)
-    // resident batch (rtb_fwd_prepare)
-    int prepared = 0;
-    BatchDev B{};
-    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, grid = 1;
-    std::vector<SpecDev> spec_host;
-    std::vector<int> spec_npath, spec_nv, spec_nwave, spec_nlayer;
-    int64_t n_out = 0, n_jac = 0;
-    size_t in_bytes = 0, out_bytes = 0;
-    long long cells = 0;
-    DevBuf d_dbg_perm, d_dbg_split;
-    size_t dbg_perm_n = 0, dbg_split_n = 0;
-    rtb_fwd_stats stats{};
-};
-
-namespace {
+namespace rtb {
 
 int fail(rtb_context* c, int code, const char* fmt, ...) {
     char buf[512];
@@ -128,12 +33,9 @@ int fail(rtb_context* c, int code, const char* fmt, ...) {
     return code;
 }
 
-#define CUDA_TRY(ctx, call)                                                                 \
-    do {                                                                                    \
-        cudaError_t e_ = (call);                                                            \
-        if (e_ != cudaSuccess)                                                              \
-            return fail(ctx, RTB_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
-    } while (0)
+}  // namespace rtb
+
+namespace {
 
 // LOCATE (radtran/scatter/locate.f:1-28), 1-based
 int locate_f(const float* xx, int n, float x) {
@@ -204,25 +106,14 @@ int interpem_f(int nem, const float* vem, const float* em, float v, float& out) 
 }
 
 // host staging of one batch
-struct Staging {
-    std::vector<SpecDev> spec;
-    std::vector<int64_t> item_start;
-    std::vector<LayerDev> lay;
-    std::vector<float> amo;
-    std::vector<WaveDev> wave;
-    std::vector<int64_t> wg_slice;
-    std::vector<float> xsec, cont;
-    std::vector<int> p_layinc;
-    std::vector<float> p_scale, p_emtemp;
-    std::vector<int> map_colptr, map_row;
-    std::vector<float> map_val;
-    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1;
-    int64_t n_out = 0, n_jac = 0;
-};
 
 struct Dims {
     int ld_lay, ld_con, ld_v, ld_param;
 };
+
+}  // namespace
+
+namespace rtb {
 
 int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     Dims d;
@@ -556,7 +447,7 @@ size_t bytes_of(const std::vector<T>& v) {
 cudaStream_t stream_of(rtb_context* c) { return c->user_stream ? c->user_stream : c->stream; }
 
 // pack + upload a batch; the device copy stays resident until the next prepare
-int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
+int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* place) {
     if (!c || nspec <= 0 || !atms) return fail(c, RTB_ERR_ARG, "bad batch arguments");
     if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
     if (c->ng > 22 || c->ng < 2) return fail(c, RTB_ERR_UNSUPPORTED, "NG=%d outside the device range 2..22", c->ng);
@@ -575,6 +466,11 @@ int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
         return fail(c, RTB_ERR_UNSUPPORTED, "spectrum needs %d B of shared memory (device %d)", smem, smem_max);
     const int bpsm = fwd_blocks_per_sm(smem);
     if (bpsm <= 0) return fail(c, RTB_ERR_CUDA, "forward kernel cannot be resident (smem %d B)", smem);
+    if (place)
+        for (int sp = 0; sp < nspec; ++sp) {
+            st.spec[sp].out_off = place->out_off[sp];
+            st.spec[sp].jac_off = place->jac_off[sp];
+        }
     struct Seg {
         const void* src;
         size_t n;
@@ -609,9 +505,11 @@ int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
         if (sg.n) memcpy((char*)c->h_in.p + sg.off, sg.src, sg.n);
     const cudaStream_t strm = stream_of(c);
     CUDA_TRY(c, cudaMemcpyAsync(c->d_in.p, c->h_in.p, off, cudaMemcpyHostToDevice, strm));
-    const size_t out_bytes = (size_t)(2 * st.n_out + st.n_jac) * sizeof(float);
-    CUDA_TRY(c, c->d_out.ensure(out_bytes));
-    CUDA_TRY(c, c->h_out.ensure(out_bytes));
+    const size_t out_bytes = place ? 0 : (size_t)(2 * st.n_out + st.n_jac) * sizeof(float);
+    if (!place) {
+        CUDA_TRY(c, c->d_out.ensure(out_bytes));
+        CUDA_TRY(c, c->h_out.ensure(out_bytes));
+    }
     CUDA_TRY(c, c->d_diag.ensure(64));
     auto dp = [&](size_t i) { return (const void*)((const char*)c->d_in.p + segs[i].off); };
     BatchDev& B = c->B;
@@ -640,10 +538,16 @@ int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
     B.delg = (const float*)c->d_delg.p;
     B.g_ord = (const double*)c->d_gord.p;
     B.kcia = (const float*)c->d_kcia.p;
-    float* dout = (float*)c->d_out.p;
-    B.calcout = dout;
-    B.gradtsurf = dout + st.n_out;
-    B.gradients = dout + 2 * st.n_out;
+    if (place) {
+        B.calcout = place->calcout;
+        B.gradtsurf = place->gradtsurf;
+        B.gradients = place->gradients;
+    } else {
+        float* dout = (float*)c->d_out.p;
+        B.calcout = dout;
+        B.gradtsurf = dout + st.n_out;
+        B.gradients = dout + 2 * st.n_out;
+    }
     B.status = (unsigned*)c->d_diag.p;
     B.counters = (unsigned long long*)((char*)c->d_diag.p + 8);
     B.strict_ties = c->strict_ties;
@@ -690,9 +594,12 @@ int prepare(rtb_context* c, int nspec, const rtb_atm* atms) {
     c->n_jac = st.n_jac;
     c->in_bytes = off;
     c->out_bytes = out_bytes;
+    c->placed = place ? 1 : 0;
     c->prepared = 1;
     return RTB_OK;
 }
+
+int prepare(rtb_context* c, int nspec, const rtb_atm* atms) { return prepare_ex(c, nspec, atms, nullptr); }
 
 int launch(rtb_context* c) {
     if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
@@ -707,6 +614,7 @@ int launch(rtb_context* c) {
 
 int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float* const* gradtsurf) {
     if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
+    if (c->placed) return fail(c, RTB_ERR_ARG, "the resident batch belongs to the retrieval engine");
     CUDA_TRY(c, cudaSetDevice(c->device));
     const cudaStream_t strm = stream_of(c);
     CUDA_TRY(c, cudaMemcpyAsync(c->h_out.p, c->d_out.p, c->out_bytes, cudaMemcpyDeviceToHost, strm));
@@ -798,7 +706,7 @@ int launch_static(rtb_context* c) {
     return RTB_OK;
 }
 
-}  // namespace
+}  // namespace rtb
 
 extern "C" {
 
@@ -838,6 +746,10 @@ void rtb_destroy(rtb_context* c) {
     c->d_cells.release();
     c->d_dbg_perm.release();
     c->d_dbg_split.release();
+    c->d_nt32.release();
+    c->d_nt64.release();
+    c->d_ntsmall.release();
+    c->d_ntdesc.release();
     c->h_in.release();
     c->h_out.release();
     if (c->ev0) cudaEventDestroy(c->ev0);

@@ -17,6 +17,7 @@ C ABI (include/radtran_b200.h) unchanged.
 """
 from __future__ import annotations
 
+import ctypes as C
 import dataclasses
 
 import numpy as np
@@ -294,3 +295,80 @@ def config3_jobs(tables: KTables, nspec: int, seed=1003):
         jobs.append(make_job(tables, absorbers, nlayer=L, seed=int(rng.integers(1 << 30)), iw0=iw0,
                              nwave=w, theta_deg=theta, vmr_perturb=0.3))
     return jobs
+
+
+# --------------------------------------------------------------------- retrievals
+@dataclasses.dataclass
+class RetrievalCase:
+    """One optimal-estimation retrieval of the layer-state model
+    (rtb_retrieval_spec): x[l] = T of layer l, x[nlayer + a] = ln scale of
+    gas scale_gas[a].  `job` is the atmosphere at scale factor 1."""
+    job: Job
+    scale_gas: np.ndarray      # int32 [nscale]
+    xa: np.ndarray             # float32 [nx]
+    sa: np.ndarray             # float64 [nx, nx]
+    sei: np.ndarray            # float64 [ny]
+    x_true: np.ndarray         # float32 [nx]
+    y: np.ndarray | None = None
+    x0: np.ndarray | None = None
+
+    @property
+    def nx(self):
+        return self.job.nv
+
+    @property
+    def ny(self):
+        return self.job.nwave
+
+    def as_struct(self):
+        s = _abi.RtbRetrievalSpec()
+        atm = self.job.as_struct()
+        s.atm = C.pointer(atm)
+        s.nscale = len(self.scale_gas)
+        s.scale_gas = _abi.iptr(self.scale_gas)
+        s.y = _abi.fptr(self.y)
+        s.sei = _abi.dptr(self.sei)
+        s.sa = _abi.dptr(self.sa)
+        s.xa = _abi.fptr(self.xa)
+        s.x0 = _abi.fptr(self.x0)
+        s._keep = (self, atm)
+        return s
+
+
+def prior_covariance(p_lay, n_scale, sig_t=3.0, sig_scale=0.5, clen=1.5):
+    """Sa: temperature block with exponential correlation in ln p,
+    sqrt(sx_ii sx_jj) exp(-|ln p_i - ln p_j| / clen) (the form of
+    nemesis/readapriori.f:239-246), 3 K; uncorrelated log scales, 50 %."""
+    lnp = np.log(p_lay)
+    L = len(p_lay)
+    sa = np.zeros((L + n_scale, L + n_scale))
+    sa[:L, :L] = sig_t * sig_t * np.exp(-np.abs(lnp[:, None] - lnp[None, :]) / clen)
+    sa[L:, L:] = np.eye(n_scale) * sig_scale * sig_scale
+    return sa
+
+
+def make_retrieval(tables: KTables, absorbers, *, nlayer, seed, iw0=0, nwave=None, theta_deg=0.0,
+                   noise=1e-9, vmr_perturb=0.3) -> RetrievalCase:
+    """Retrieval case with a priori = smooth T profile and unit gas scales;
+    the true state is a seeded draw from Sa.  The measurement y is set by
+    the caller (forward model at x_true plus noise, see `observe`)."""
+    rng = np.random.default_rng(seed)
+    p_lev, p_lay = _levels(nlayer)
+    t_prior = temperature_profile(p_lay, rng, noise=0.0)
+    job = make_job(tables, absorbers, nlayer=nlayer, seed=seed + 1, iw0=iw0, nwave=nwave, theta_deg=theta_deg,
+                   vmr_perturb=vmr_perturb, temp=t_prior)
+    ns = len(absorbers)
+    xa = np.concatenate([t_prior, np.zeros(ns)]).astype(np.float32)
+    sa = prior_covariance(p_lay, ns)
+    x_true = (xa + np.linalg.cholesky(sa) @ rng.standard_normal(len(xa))).astype(np.float32)
+    sei = np.full(job.nwave, 1.0 / (noise * noise))
+    return RetrievalCase(job=job, scale_gas=np.arange(2, 2 + ns, dtype=np.int32), xa=xa, sa=sa, sei=sei,
+                         x_true=x_true)
+
+
+def observe(case: RetrievalCase, spectrum, seed, noise=1e-9):
+    """y = F(x_true) + N(0, noise) with F evaluated by the caller."""
+    rng = np.random.default_rng(seed)
+    case.y = (np.asarray(spectrum, np.float64) + noise * rng.standard_normal(case.ny)).astype(np.float32)
+    return case
+

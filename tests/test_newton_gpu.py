@@ -1,0 +1,149 @@
+"""GPU parity tests of the Newton step, the cost function, the SPD inverse
+and the retrieval loop against the oracle (oracle/newton_oracle.cpp,
+oracle/coreret_oracle.cpp), all through the C ABI.
+
+Tolerances (stated per result):
+  Newton step  max_i |x_gpu - x_ref| <= tol * max_i |x_ref - xa| + 4 ulp(x_ref),
+               tol = 1e-3 on tensor cores with one refinement step, 1e-6 all-FP64
+  phi, chisq   relative 1e-6 (FP64 sums, REAL result)
+  Sa^-1        relative to max |Sa^-1|: 1e-10
+  retrieval    same number of iterations, forward evaluations and stop rule as
+               the oracle; |x_gpu - x_ref| <= 1e-3 prior sigma; phi relative 1e-3
+"""
+import numpy as np
+import pytest
+
+from radtrancode_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = {0: 1e-3, 1: 1e-6}
+
+
+def _case(oracle, kt, cia, absorbers, nlayer, seed, nwave=None, nthreads=1):
+    case = synth.make_retrieval(kt, absorbers, nlayer=nlayer, seed=seed, nwave=nwave)
+    y_true, _ = oracle.forward_state(kt, cia, case, case.x_true, nthreads=nthreads)
+    return synth.observe(case, y_true, seed=seed + 1)
+
+
+@pytest.fixture(scope="module")
+def c1(oracle):
+    kt, cia, _ = synth.config1()
+    return kt, cia, [_case(oracle, kt, cia, [synth.CH4], 40, s) for s in (5, 7, 9)]
+
+
+@pytest.fixture(scope="module")
+def c2s(oracle):
+    kt, cia, _ = synth.config2()
+    return kt, cia, [_case(oracle, kt, cia, synth.ABSORBERS_C2, 120, 21, nwave=300, nthreads=8)]
+
+
+def _newton_inputs(oracle, kt, cia, cases, shift):
+    rows = []
+    for i, case in enumerate(cases):
+        xn = case.x_true.copy()
+        xn[:case.job.nlayer] += np.float32(shift * (i + 1))
+        yn, kk = oracle.forward_state(kt, cia, case, xn, nthreads=8)
+        sai, ic = oracle.dinvertm(case.sa)
+        rows.append((kk, case.sei, sai, case.xa, xn, case.y, yn))
+    return [np.stack(a) for a in zip(*rows)]
+
+
+def _ulp(x):
+    return np.spacing(np.abs(x).astype(np.float32))
+
+
+@pytest.mark.parametrize("hess", [0, 1])
+@pytest.mark.parametrize("which", ["c1", "c2s"])
+def test_newton_step_matches_reference_algebra(ctx, oracle, c1, c2s, hess, which):
+    kt, cia, cases = c1 if which == "c1" else c2s
+    kk, sei, sai, xa, xn, y, yn = _newton_inputs(oracle, kt, cia, cases, 2.0)
+    ref = np.stack([oracle.newton_step(*a) for a in zip(kk, sei, sai, xa, xn, y, yn)])
+    ctx.set_newton_mode(hess, 1)
+    try:
+        x, nonpd, resid = ctx.newton_step_batch(kk, sei, sai, xa, xn, y, yn)
+    finally:
+        ctx.set_newton_mode(0, 1)
+    assert not nonpd.any()
+    for r in range(len(ref)):
+        step = np.max(np.abs(ref[r] - xa[r]))
+        assert np.all(np.abs(x[r] - ref[r]) <= TOL_STEP[hess] * step + 4 * _ulp(ref[r])), r
+    assert np.all(resid < (1e-4 if hess == 0 else 1e-10))
+
+
+def test_refinement_reduces_residual(ctx, oracle, c2s):
+    kt, cia, cases = c2s
+    args = _newton_inputs(oracle, kt, cia, cases, 1.0)
+    res = []
+    try:
+        for refine in (0, 1, 2):
+            ctx.set_newton_mode(0, refine)
+            res.append(ctx.newton_step_batch(*args)[2][0])
+    finally:
+        ctx.set_newton_mode(0, 1)
+    assert res[1] < res[0] and res[2] < res[1]
+
+
+def test_phiret_matches_oracle(ctx, oracle, c1):
+    kt, cia, cases = c1
+    kk, sei, sai, xa, xn, y, yn = _newton_inputs(oracle, kt, cia, cases, 0.5)
+    phi, chisq = ctx.calc_phiret_batch(y, yn, sei, xn, xa, sai)
+    for r in range(len(phi)):
+        p, c = oracle.calc_phiret(y[r], yn[r], sei[r], xn[r], xa[r], sai[r])
+        assert abs(phi[r] - p) <= 1e-6 * abs(p)
+        assert abs(chisq[r] - c) <= 1e-6 * abs(c)
+
+
+def test_spd_inverse_matches_dinvertm(ctx, oracle, c2s):
+    _, _, cases = c2s
+    sa = np.stack([cases[0].sa, cases[0].sa * 2.0])
+    inv, nonpd = ctx.spd_inverse_batch(sa)
+    assert not nonpd.any()
+    for r in range(2):
+        ref, ic = oracle.dinvertm(sa[r])
+        assert ic == 0
+        assert np.max(np.abs(inv[r] - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+def test_spd_inverse_flags_non_positive_pivot(ctx):
+    a = np.diag([1.0, -2.0, 3.0])[None]
+    inv, nonpd = ctx.spd_inverse_batch(a)
+    assert nonpd[0] == 1
+    assert np.isfinite(inv).all()
+
+
+@pytest.mark.parametrize("hess", [1, 0])
+def test_retrieve_batch_matches_oracle(ctx, oracle, c1, hess):
+    kt, cia, cases = c1
+    cases = [c for c in cases]
+    far = synth.make_retrieval(kt, [synth.CH4], nlayer=40, seed=9)
+    far.y = cases[2].y
+    far.x0 = far.xa.copy()
+    far.x0[-1] = 8.0                     # rejections on the way (coreret.f:1060-1064)
+    cases.append(far)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_newton_mode(hess, 1)
+    try:
+        got = ctx.retrieve_batch(cases, kiter=10, phlimit=0.1)
+    finally:
+        ctx.set_newton_mode(0, 1)
+    for case, g in zip(cases, got):
+        ref, tr = oracle.retrieve(kt, cia, case, kiter=10, phlimit=0.1)
+        assert (g["converged"], g["iterations"], g["forwards"]) == (ref["converged"], ref["iterations"],
+                                                                   ref["forwards"])
+        sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
+        assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
+        assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
+
+
+def test_retrieve_batch_result_independent_of_batch(ctx, c1):
+    kt, cia, cases = c1
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    together = ctx.retrieve_batch(cases, kiter=10)
+    for case, t in zip(cases, together):
+        alone = ctx.retrieve_batch([case], kiter=10)[0]
+        assert np.array_equal(alone["x"], t["x"])
+        assert np.array_equal(alone["yn"], t["yn"])
+        assert (alone["phi"], alone["iterations"]) == (t["phi"], t["iterations"])

@@ -50,6 +50,14 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def tensor_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 def profile_traffic():
     """DRAM bytes per launch of the forward kernel from the committed ncu
     summary (profiles/fwd_kernel_config2.md, line 'dram_bytes_per_launch:')."""
@@ -203,6 +211,86 @@ def cpu_baseline_and_accuracy(kt, cia, job, gpu_out):
                   "sample_wavenumbers": len(range(0, job.nwave, stride * 8)) * 8, "vs": "FP64 oracle"}
 
 
+RET_SAMPLE = 64               # full-size retrievals timed in the default run
+RET_FP64_SAMPLE = 16          # of those, re-run with the all-FP64 Newton step
+NEWTON_BATCH = 296            # retrievals per timed Newton-step launch (2 per SM)
+RET_WORKLOAD = ("optimal-estimation retrievals, full size: NX=124 (120 layer T + 4 log gas scales), NY=2000, "
+                "10 Newton iterations max, phlimit 0.1 %, Sa exponential correlation 1.5 scale heights "
+                "3 K / 50 %, Se diagonal (1e-9)^2, y = F(x_true) + N(0, 1e-9), x_true ~ N(xa, Sa)")
+
+
+def retrieval_cases(ctx, kt, n, seed0=4000):
+    """Full-size retrieval cases; observations from the device forward model
+    at the true states (one batched launch) plus seeded noise."""
+    from radtrancode_b200 import synth
+    cases = [synth.make_retrieval(kt, synth.ABSORBERS_C2, nlayer=120, seed=seed0 + 17 * i, nwave=2000)
+             for i in range(n)]
+    outs = ctx.cirsrtfg_wave_batch([synth.job_at_state(c, c.x_true) for c in cases])
+    for i, c in enumerate(cases):
+        synth.observe(c, outs[i][0], seed=seed0 + 17 * i + 1)
+    return cases, outs
+
+
+def retrieval_leg(ctx, kt, cia, bf16_peak):
+    """Retrievals/s and completion-time percentiles of the batched engine
+    (rtb_retrieve_batch), the mixed-precision result against the all-FP64
+    device solve, the Newton kernel against the tensor peak, and the oracle
+    retrieval on the host cores."""
+    from oracle import pyoracle as po
+    cases, outs = retrieval_cases(ctx, kt, RET_SAMPLE)
+    ctx.set_newton_mode(0, 1)
+    t = time.perf_counter()
+    res = ctx.retrieve_batch(cases, kiter=10, phlimit=0.1)
+    dt = time.perf_counter() - t
+    lat = np.array([r["ms"] for r in res])
+    ctx.set_newton_mode(1, 0)
+    try:
+        res64 = ctx.retrieve_batch(cases[:RET_FP64_SAMPLE], kiter=10, phlimit=0.1)
+    finally:
+        ctx.set_newton_mode(0, 1)
+    dx, same = 0.0, 0
+    for c, a, b in zip(cases, res, res64):
+        sig = np.sqrt(np.diag(c.sa))
+        dx = max(dx, float(np.max(np.abs(a["x"] - b["x"]) / sig)))
+        same += int(a["iterations"] == b["iterations"] and a["converged"] == b["converged"])
+    # Newton-step kernel alone: NEWTON_BATCH retrievals of K at the true states
+    pick = [i % RET_SAMPLE for i in range(NEWTON_BATCH)]
+    kk = np.stack([outs[i][1].reshape(124, 2000) for i in pick])
+    sai = np.stack([np.linalg.inv(cases[i].sa) for i in pick])
+    sei = np.stack([cases[i].sei for i in pick])
+    xa = np.stack([cases[i].xa for i in pick])
+    y = np.stack([cases[i].y for i in pick])
+    yn = np.stack([outs[i][0] for i in pick])
+    ms_newton = []
+    for _ in range(4):
+        ctx.newton_step_batch(kk, sei, sai, xa, xa, y, yn)
+        ms_newton.append(ctx.newton_stats()["ms_kernel"])
+    ms_n = statistics.median(ms_newton[1:])
+    flops = NEWTON_BATCH * (2.0 * 124 * 124 * 2000 + 2.0 * 124 * 2000)
+    tflops = flops / (ms_n * 1e-3) / 1e12
+    # the oracle's retrieval on the host cores: one case, all threads
+    nthr = os.cpu_count() or 1
+    t = time.perf_counter()
+    po.retrieve(kt, cia, cases[0], kiter=10, phlimit=0.1, nthreads=nthr)
+    t_cpu = time.perf_counter() - t
+    return {
+        "workload": RET_WORKLOAD, "retrievals": RET_SAMPLE, "value": RET_SAMPLE / dt, "unit": "retrievals/s",
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "latency_note": "completion time from the start of the batched call (all admitted at once)",
+        "iterations_mean": float(np.mean([r["iterations"] for r in res])),
+        "forwards_mean": float(np.mean([r["forwards"] for r in res])),
+        "converged": int(sum(r["converged"] > 0 for r in res)),
+        "newton": {"hessian": "bf16 hi/lo split on tensor cores (mma.sync m16n8k16), FP32 accumulation, "
+                              "1 FP64 refinement step; FP64 Cholesky",
+                   "vs_fp64_solve": {"retrievals": RET_FP64_SAMPLE, "max_dx_over_prior_sigma": dx,
+                                     "same_iterations_and_stop_rule": same}},
+        "newton_kernel": {"batch": NEWTON_BATCH, "ms": ms_n, "achieved_tflops": tflops, "peak_tflops": bf16_peak,
+                          "frac": tflops / bf16_peak, "flops_per_retrieval": "2 NX^2 NY + 2 NX NY"},
+        "cpu_baseline": {"value": 1.0 / t_cpu, "unit": "retrievals/s", "cores": nthr, "kind": "port",
+                         "sample": f"1 retrieval of the same workload, oracle coreret restatement, {nthr} threads"},
+    }
+
+
 def profile_case(args):
     """Reduced case for ncu captures: the same spectrum cut to its first
     `--profile-waves` wavenumbers, warm-up + `--steps` launches."""
@@ -228,6 +316,7 @@ def main():
     ap.add_argument("--profile-waves", type=int, default=0,
                     help="profiling case: only launch the forward kernel on the first N wavenumbers of the "
                          "workload (steps launches after warmup), print the kernel time, skip e2e and baselines")
+    ap.add_argument("--no-retrieval", action="store_true", help="skip the retrieval leg")
     args = ap.parse_args()
     if args.profile_waves:
         profile_case(args)
@@ -326,6 +415,8 @@ def main():
             base, acc = cpu_baseline_and_accuracy(kt, cia, job, gpu_out)
             out["cpu_baseline"] = base
             out["accuracy"] = acc
+            if not args.no_retrieval:
+                out["retrieval"] = retrieval_leg(ctx, kt, cia, tensor_peak())
         print(json.dumps(out))
     ctx.close()
     if world > 1:

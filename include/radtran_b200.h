@@ -251,6 +251,14 @@ int rtb_newton_step_batch(rtb_context* ctx, int nret, int nx, int ny, const floa
                           const double* sai, const float* xa, const float* xn, const float* y,
                           const float* yn, float* x_out, int* nonpd, double* resid);
 
+/* Device time of the last rtb_newton_step_batch kernel (Newton step of
+ * `retrievals` retrievals, transfers excluded). */
+typedef struct rtb_newton_stats {
+    long long retrievals;
+    float ms_kernel;
+} rtb_newton_stats;
+int rtb_get_newton_stats(const rtb_context* ctx, rtb_newton_stats* out);
+
 /* calc_phiret (nemesis/calc_phiret.f:49-102) for nret retrievals, diagonal
  * Se: phi = (yn-y)^T Se^-1 (yn-y) + (xn-xa)^T Sa^-1 (xn-xa), chisq = the
  * first term, both REAL as in the reference.  Layouts as above. */

@@ -76,6 +76,10 @@ class RtbRetrievalResult(C.Structure):
     ]
 
 
+class RtbNewtonStats(C.Structure):
+    _fields_ = [("retrievals", C.c_longlong), ("ms_kernel", C.c_float)]
+
+
 RESULT_KEYS = ("phi", "chisq", "alambda", "iterations", "forwards", "converged", "nonpd", "ms")
 
 

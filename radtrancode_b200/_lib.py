@@ -78,6 +78,8 @@ def lib() -> C.CDLL:
         L.rtb_retrieve_batch.argtypes = [vp, C.c_int, C.POINTER(_abi.RtbRetrievalSpec),
                                          C.POINTER(_abi.RtbRetrievalOpts), C.POINTER(_abi.RtbRetrievalResult)]
         L.rtb_retrieve_batch.restype = C.c_int
+        L.rtb_get_newton_stats.argtypes = [vp, C.POINTER(_abi.RtbNewtonStats)]
+        L.rtb_get_newton_stats.restype = C.c_int
         p16 = C.POINTER(C.c_int16)
         L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
         L.rtb_get_debug_bins.restype = C.c_int
@@ -91,5 +93,5 @@ EXPORTED = [
     "rtb_cirsrtfg_wave", "rtb_cirsrtfg_wave_batch", "rtb_get_fwd_stats", "rtb_set_debug",
     "rtb_get_debug_bins", "rtb_set_strict_ties", "rtb_fwd_prepare", "rtb_fwd_launch", "rtb_fwd_fetch",
     "rtb_set_stream", "rtb_fwd_launch_static", "rtb_set_newton_mode", "rtb_newton_step_batch",
-    "rtb_calc_phiret_batch", "rtb_spd_inverse_batch", "rtb_retrieve_batch",
+    "rtb_calc_phiret_batch", "rtb_spd_inverse_batch", "rtb_retrieve_batch", "rtb_get_newton_stats",
 ]

@@ -165,6 +165,11 @@ class Context:
             _abi.fptr(y), _abi.fptr(yn), _abi.fptr(x_out), _abi.iptr(nonpd), _abi.dptr(resid)))
         return x_out, nonpd, resid
 
+    def newton_stats(self) -> dict:
+        s = _abi.RtbNewtonStats()
+        self._check(self._L.rtb_get_newton_stats(self._h, C.byref(s)))
+        return {"retrievals": s.retrievals, "ms_kernel": s.ms_kernel}
+
     def calc_phiret_batch(self, y, yn, sei, xn, xa, sai):
         f32 = lambda a: np.ascontiguousarray(a, np.float32)
         f64 = lambda a: np.ascontiguousarray(a, np.float64)

@@ -141,6 +141,7 @@ struct rtb_context {
     int newton_hess = 0;                  // RTB_HESS_TC / RTB_HESS_FP64
     int newton_refine = 1;
     rtb::DevBuf d_nt32, d_nt64, d_ntsmall, d_ntdesc;
+    rtb_newton_stats newton_stats{};
 };
 
 #define CUDA_TRY(ctx, call)                                                                 \

@@ -596,8 +596,10 @@ int rtb_newton_step_batch(rtb_context* c, int nret, int nx, int ny, const float*
     CUDA_TRY(c, h2d(c->d_ntdesc, desc, st));
     unsigned* status = (unsigned*)c->d_ntsmall.p;
     double* dres = (double*)((char*)c->d_ntsmall.p + ((4 * (size_t)nret + 15) & ~(size_t)15));
+    CUDA_TRY(c, cudaEventRecord(c->ev0, st));
     CUDA_TRY(c, launch_newton_step((const NewtonDev*)c->d_ntdesc.p, nret, c->newton_hess, c->newton_refine, status,
                                    resid ? dres : nullptr, st));
+    CUDA_TRY(c, cudaEventRecord(c->ev1, st));
     CUDA_TRY(c, cudaMemcpy2DAsync(x_out, nx * 4, F + o_xo, nxa * 4, nx * 4, nret, cudaMemcpyDeviceToHost, st));
     std::vector<unsigned> sts(nret);
     CUDA_TRY(c, cudaMemcpyAsync(sts.data(), status, 4 * (size_t)nret, cudaMemcpyDeviceToHost, st));
@@ -605,6 +607,16 @@ int rtb_newton_step_batch(rtb_context* c, int nret, int nx, int ny, const float*
     CUDA_TRY(c, cudaStreamSynchronize(st));
     if (nonpd)
         for (int r = 0; r < nret; ++r) nonpd[r] = (sts[r] & kNtNonPd) ? 1 : 0;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->newton_stats.retrievals = nret;
+    c->newton_stats.ms_kernel = ms;
+    return RTB_OK;
+}
+
+int rtb_get_newton_stats(const rtb_context* c, rtb_newton_stats* out) {
+    if (!c || !out) return RTB_ERR_ARG;
+    *out = c->newton_stats;
     return RTB_OK;
 }
 

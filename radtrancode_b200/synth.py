@@ -372,3 +372,22 @@ def observe(case: RetrievalCase, spectrum, seed, noise=1e-9):
     case.y = (np.asarray(spectrum, np.float64) + noise * rng.standard_normal(case.ny)).astype(np.float32)
     return case
 
+
+
+def job_at_state(case: RetrievalCase, x) -> Job:
+    """The case's atmosphere at state x, by the mapping rtb_retrieve_batch
+    applies: temp = x[:nlayer] (emtemp along the path), amount, pp and the
+    gas's xmap rows times exp(x[nlayer + a]) in float32."""
+    j = case.job
+    L = j.nlayer
+    x = np.asarray(x, np.float32)
+    amount, pp, xmap = j.amount.copy(order="F"), j.pp.copy(order="F"), j.xmap.copy(order="F")
+    for a, g in enumerate(case.scale_gas):
+        f = np.float32(np.exp(np.float64(x[L + a])))
+        amount[:L, g] = amount[:L, g] * f
+        pp[:L, g] = pp[:L, g] * f
+        xmap[:, g, :] = xmap[:, g, :] * f
+    temp = x[:L].copy()
+    emtemp = j.emtemp.copy(order="F")
+    emtemp[:L, 0] = temp[j.layinc[:L, 0] - 1]
+    return dataclasses.replace(j, temp=temp, amount=amount, pp=pp, xmap=xmap, emtemp=emtemp)

@@ -219,6 +219,56 @@ RET_WORKLOAD = ("optimal-estimation retrievals, full size: NX=124 (120 layer T +
                 "3 K / 50 %, Se diagonal (1e-9)^2, y = F(x_true) + N(0, 1e-9), x_true ~ N(xa, Sa)")
 
 
+BATCH_SPECTRA = 1024          # uneven spectra in the batched leg (the 4096 of the batching workload: --batch-spectra)
+BATCH_TUNE = 256              # sub-batch the autotuner times
+
+
+def batch_leg(ctx, kt, nspec):
+    """Uneven-spectra batch in one persistent launch: default schedule vs
+    the autotuned schedule replayed through a CUDA graph, and the batched
+    C-ABI call end to end."""
+    from radtrancode_b200 import synth
+    jobs = synth.config3_jobs(kt, nspec, seed=1003)
+    nwave = sum(j.nwave for j in jobs)
+    ctx.prepare(jobs[:BATCH_TUNE])
+    tune = ctx.autotune()
+    t = time.perf_counter()
+    ctx.prepare(jobs)
+    t_prep = time.perf_counter() - t
+
+    def timed(n):
+        ms = []
+        for _ in range(n):
+            ctx.launch()
+            ctx.fetch()
+            ms.append(ctx.stats()["ms_kernel"])
+        return ms[-1]
+    ctx.set_schedule(0, 0)
+    ms_default = timed(2)
+    ctx.set_schedule(tune["schedule"], tune["blocks_per_sm"])
+    ctx.use_graph(True)
+    ms_tuned = timed(3)
+    ctx.use_graph(False)
+    ctx.set_schedule(0, 0)
+    t = time.perf_counter()
+    ctx.cirsrtfg_wave_batch(jobs)
+    t_e2e = time.perf_counter() - t
+    st = ctx.stats()
+    return {
+        "workload": f"{nspec} uneven spectra: W~U[200,2000] of the 2000-bin grid, L~U[40,120], 1-4 of the four "
+                    "absorbers, theta~U[0,70 deg], one persistent launch",
+        "spectra": nspec, "wavenumbers": nwave,
+        "value": nspec / (ms_tuned * 1e-3), "unit": "spectra/s",
+        "ms_launch_tuned_graph": ms_tuned, "ms_launch_default": ms_default,
+        "tuned": {"schedule": ["static", "dynamic", "dynamic longest-first"][tune["schedule"]],
+                  "blocks_per_sm": tune["blocks_per_sm"], "candidates": tune["candidates"],
+                  "tuned_on_spectra": BATCH_TUNE},
+        "prepare_s": t_prep,
+        "e2e": {"value": nspec / t_e2e, "unit": "spectra/s", "h2d_bytes": st["h2d_bytes"],
+                "d2h_bytes": st["d2h_bytes"], "note": "rtb_cirsrtfg_wave_batch with host buffers, default schedule"},
+    }
+
+
 def retrieval_cases(ctx, kt, n, seed0=4000):
     """Full-size retrieval cases; observations from the device forward model
     at the true states (one batched launch) plus seeded noise."""
@@ -317,6 +367,8 @@ def main():
                     help="profiling case: only launch the forward kernel on the first N wavenumbers of the "
                          "workload (steps launches after warmup), print the kernel time, skip e2e and baselines")
     ap.add_argument("--no-retrieval", action="store_true", help="skip the retrieval leg")
+    ap.add_argument("--batch-spectra", type=int, default=BATCH_SPECTRA,
+                    help="uneven spectra in the batched leg (0 skips it)")
     args = ap.parse_args()
     if args.profile_waves:
         profile_case(args)
@@ -415,6 +467,8 @@ def main():
             base, acc = cpu_baseline_and_accuracy(kt, cia, job, gpu_out)
             out["cpu_baseline"] = base
             out["accuracy"] = acc
+            if args.batch_spectra > 0:
+                out["batch"] = batch_leg(ctx, kt, args.batch_spectra)
             if not args.no_retrieval:
                 out["retrieval"] = retrieval_leg(ctx, kt, cia, tensor_peak())
         print(json.dumps(out))

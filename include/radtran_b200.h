@@ -212,6 +212,35 @@ int rtb_get_debug_bins(const rtb_context* ctx, int16_t* perm, size_t n_perm,
  * boundary; 1 takes it for every pass that has a tie. */
 int rtb_set_strict_ties(rtb_context* ctx, int on);
 
+/* Schedule of the resident batch's launches.  A launch runs one block per
+ * (spectrum, wavenumber) work item at a time on nsm x blocks_per_sm resident
+ * blocks:
+ *   schedule 0  static: block b takes items b, b + grid, ...
+ *   schedule 1  dynamic: blocks pull the next item from a counter
+ *   schedule 2  dynamic, items issued longest first (spectra ordered by a
+ *               cost model: layers x overlap passes x gradient columns)
+ * blocks_per_sm 0 = the occupancy maximum.  Results do not depend on the
+ * schedule (each item is computed by one block, in the same order). */
+int rtb_fwd_set_schedule(rtb_context* ctx, int schedule, int blocks_per_sm);
+
+/* Time the resident batch under every schedule and the three highest
+ * occupancies (two launches each, the second timed), keep the fastest and
+ * report it.  Every candidate runs the whole batch: tune on a
+ * representative batch and carry the result to larger ones with
+ * rtb_fwd_set_schedule. */
+typedef struct rtb_fwd_tune {
+    int schedule;
+    int blocks_per_sm;
+    float ms;          /* launch time of the chosen configuration */
+    int candidates;    /* configurations timed */
+} rtb_fwd_tune;
+int rtb_fwd_autotune(rtb_context* ctx, rtb_fwd_tune* out);
+
+/* on = 1: rtb_fwd_launch replays a CUDA graph of one launch (status clear +
+ * forward kernel), captured at the first launch after rtb_fwd_prepare or a
+ * schedule change; on = 0: plain launches. */
+int rtb_fwd_use_graph(rtb_context* ctx, int on);
+
 /* ---------------------------------------------------------------------- */
 /* Optimal-estimation Newton step (calc_gain_matrix + calcnextxn)          */
 /* ---------------------------------------------------------------------- */

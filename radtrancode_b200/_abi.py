@@ -76,6 +76,10 @@ class RtbRetrievalResult(C.Structure):
     ]
 
 
+class RtbFwdTune(C.Structure):
+    _fields_ = [("schedule", C.c_int), ("blocks_per_sm", C.c_int), ("ms", C.c_float), ("candidates", C.c_int)]
+
+
 class RtbNewtonStats(C.Structure):
     _fields_ = [("retrievals", C.c_longlong), ("ms_kernel", C.c_float)]
 

@@ -80,6 +80,12 @@ def lib() -> C.CDLL:
         L.rtb_retrieve_batch.restype = C.c_int
         L.rtb_get_newton_stats.argtypes = [vp, C.POINTER(_abi.RtbNewtonStats)]
         L.rtb_get_newton_stats.restype = C.c_int
+        L.rtb_fwd_set_schedule.argtypes = [vp, C.c_int, C.c_int]
+        L.rtb_fwd_set_schedule.restype = C.c_int
+        L.rtb_fwd_autotune.argtypes = [vp, C.POINTER(_abi.RtbFwdTune)]
+        L.rtb_fwd_autotune.restype = C.c_int
+        L.rtb_fwd_use_graph.argtypes = [vp, C.c_int]
+        L.rtb_fwd_use_graph.restype = C.c_int
         p16 = C.POINTER(C.c_int16)
         L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
         L.rtb_get_debug_bins.restype = C.c_int
@@ -94,4 +100,5 @@ EXPORTED = [
     "rtb_get_debug_bins", "rtb_set_strict_ties", "rtb_fwd_prepare", "rtb_fwd_launch", "rtb_fwd_fetch",
     "rtb_set_stream", "rtb_fwd_launch_static", "rtb_set_newton_mode", "rtb_newton_step_batch",
     "rtb_calc_phiret_batch", "rtb_spd_inverse_batch", "rtb_retrieve_batch", "rtb_get_newton_stats",
+    "rtb_fwd_set_schedule", "rtb_fwd_autotune", "rtb_fwd_use_graph",
 ]

@@ -123,6 +123,17 @@ class Context:
     def launch(self):
         self._check(self._L.rtb_fwd_launch(self._h))
 
+    def set_schedule(self, schedule, blocks_per_sm=0):
+        self._check(self._L.rtb_fwd_set_schedule(self._h, schedule, blocks_per_sm))
+
+    def autotune(self) -> dict:
+        t = _abi.RtbFwdTune()
+        self._check(self._L.rtb_fwd_autotune(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def use_graph(self, on=True):
+        self._check(self._L.rtb_fwd_use_graph(self._h, 1 if on else 0))
+
     def launch_static(self):
         """rtb_fwd_launch_static: the same launch with its scratch taken from
         the library's fixed per-device array, allocating nothing."""

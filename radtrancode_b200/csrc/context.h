@@ -92,6 +92,8 @@ int fail(rtb_context* c, int code, const char* fmt, ...);
 int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st);
 int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* place);
 int launch(rtb_context* c);
+int apply_schedule(rtb_context* c);
+void drop_graph(rtb_context* c);
 cudaStream_t stream_of(rtb_context* c);
 
 }  // namespace rtb
@@ -137,6 +139,18 @@ struct rtb_context {
     rtb::DevBuf d_dbg_perm, d_dbg_split;
     size_t dbg_perm_n = 0, dbg_split_n = 0;
     rtb_fwd_stats stats{};
+    // schedule of the resident batch (rtb_fwd_set_schedule / rtb_fwd_autotune)
+    int sched = 0;                        // 0 static, 1 dynamic, 2 dynamic cost-ordered
+    int occ = 0;                          // blocks per SM (0 = the occupancy maximum)
+    int bpsm_max = 1;
+    std::vector<int64_t> item_start_host;
+    std::vector<float> spec_cost;
+    int order_ready = 0;
+    rtb::DevBuf d_order;
+    // CUDA graph of one launch of the resident batch (rtb_fwd_use_graph)
+    int use_graph = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
     // Newton step
     int newton_hess = 0;                  // RTB_HESS_TC / RTB_HESS_FP64
     int newton_refine = 1;

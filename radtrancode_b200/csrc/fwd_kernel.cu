@@ -823,7 +823,22 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
     float* colA = (float*)(wsm + wo.colA);
     float* colB = (float*)(wsm + wo.colB);
 
-    for (int64_t item = blockIdx.x; item < B.nitems; item += gridDim.x) {
+    __shared__ long long s_next;
+    int64_t k_static = blockIdx.x;
+    for (;;) {
+        // next work item: grid-stride, or pulled from the launch's counter
+        // (dynamic schedule); item_order maps the issue order to items
+        int64_t k;
+        if (B.work_next) {
+            if (tid == 0) s_next = (long long)atomicAdd(B.work_next, 1ull);
+            __syncthreads();
+            k = s_next;
+        } else {
+            k = k_static;
+            k_static += gridDim.x;
+        }
+        if (k >= B.nitems) break;
+        const int64_t item = B.item_order ? (int64_t)B.item_order[k] : k;
         // locate the spectrum of this item
         int lo = 0, hi = B.nspec - 1;
         while (lo < hi) {

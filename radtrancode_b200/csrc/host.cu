@@ -566,6 +566,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     int64_t grid = (int64_t)c->nsm * bpsm;
     if (grid > B.nitems) grid = B.nitems;
     c->grid = (int)grid;
+    c->bpsm_max = bpsm;
     // one scratch slot per CTA: tau[Lmax][ng] + dtau[Lmax][nsw][ng]
     B.cell_Lmax = st.Lmax;
     B.cell_slot = (int64_t)st.Lmax * c->ng * (1 + st.nsw_max);
@@ -583,19 +584,64 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     c->spec_nwave.clear();
     c->spec_nlayer.clear();
     c->cells = 0;
+    c->spec_cost.clear();
     for (int s = 0; s < nspec; ++s) {
         c->spec_npath.push_back(atms[s].npath);
         c->spec_nv.push_back(atms[s].nv);
         c->spec_nwave.push_back(atms[s].nwave);
         c->spec_nlayer.push_back(atms[s].nlayer);
         c->cells += (long long)atms[s].nlayer * atms[s].nwave;
+        // cost model of one item (wavenumber): layers x (1 + sorting overlap passes) x gradient columns
+        int nabs = 0;
+        for (int k = 0; k < atms[s].ngas; ++k) nabs += atms[s].ktab[k] >= 0 ? 1 : 0;
+        c->spec_cost.push_back((float)atms[s].nlayer * (1.0f + 4.0f * std::max(nabs - 1, 0)) *
+                               (2.0f + st.spec[s].nsw));
     }
+    c->item_start_host = st.item_start;
+    c->order_ready = 0;
     c->n_out = st.n_out;
     c->n_jac = st.n_jac;
     c->in_bytes = off;
     c->out_bytes = out_bytes;
     c->placed = place ? 1 : 0;
     c->prepared = 1;
+    return apply_schedule(c);
+}
+
+void drop_graph(rtb_context* c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->gexec = nullptr;
+    c->graph = nullptr;
+}
+
+// grid, work counter and issue order of the resident batch from (sched, occ)
+int apply_schedule(rtb_context* c) {
+    drop_graph(c);
+    BatchDev& B = c->B;
+    const int b = c->occ > 0 ? std::min(c->occ, c->bpsm_max) : c->bpsm_max;
+    int64_t grid = (int64_t)c->nsm * b;
+    if (grid > B.nitems) grid = B.nitems;
+    c->grid = (int)std::max<int64_t>(grid, 1);
+    B.work_next = c->sched >= 1 ? (unsigned long long*)((char*)c->d_diag.p + 48) : nullptr;
+    B.item_order = nullptr;
+    if (c->sched == 2) {
+        if (!c->order_ready) {
+            // longest-processing-time first: spectra by decreasing item cost, items of a spectrum together
+            const int nspec = (int)c->spec_cost.size();
+            std::vector<int> sp(nspec);
+            for (int i = 0; i < nspec; ++i) sp[i] = i;
+            std::stable_sort(sp.begin(), sp.end(), [&](int a, int b2) { return c->spec_cost[a] > c->spec_cost[b2]; });
+            std::vector<int> order;
+            order.reserve((size_t)B.nitems);
+            for (int s : sp)
+                for (int64_t it = c->item_start_host[s]; it < c->item_start_host[s + 1]; ++it) order.push_back((int)it);
+            CUDA_TRY(c, c->d_order.ensure(order.size() * sizeof(int)));
+            CUDA_TRY(c, cudaMemcpy(c->d_order.p, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+            c->order_ready = 1;
+        }
+        B.item_order = (const int*)c->d_order.p;
+    }
     return RTB_OK;
 }
 
@@ -605,6 +651,27 @@ int launch(rtb_context* c) {
     if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
     CUDA_TRY(c, cudaSetDevice(c->device));
     const cudaStream_t strm = stream_of(c);
+    if (c->use_graph) {
+        if (!c->gexec) {
+            // one launch of the resident batch (status clear + forward kernel) as a graph
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(c, cudaStreamBeginCapture(strm, cudaStreamCaptureModeRelaxed));
+            cudaError_t e = cudaMemsetAsync(c->d_diag.p, 0, 64, strm);
+            if (e == cudaSuccess) e = launch_fwd(c->B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, strm);
+            const cudaError_t e2 = cudaStreamEndCapture(strm, &g);
+            if (e != cudaSuccess || e2 != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return fail(c, RTB_ERR_CUDA, "graph capture of the forward launch failed: %s",
+                            cudaGetErrorString(e != cudaSuccess ? e : e2));
+            }
+            c->graph = g;
+            CUDA_TRY(c, cudaGraphInstantiate(&c->gexec, g, 0));
+        }
+        CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
+        CUDA_TRY(c, cudaGraphLaunch(c->gexec, strm));
+        CUDA_TRY(c, cudaEventRecord(c->ev1, strm));
+        return RTB_OK;
+    }
     CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, strm));
     CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
     CUDA_TRY(c, launch_fwd(c->B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, strm));
@@ -746,6 +813,8 @@ void rtb_destroy(rtb_context* c) {
     c->d_cells.release();
     c->d_dbg_perm.release();
     c->d_dbg_split.release();
+    drop_graph(c);
+    c->d_order.release();
     c->d_nt32.release();
     c->d_nt64.release();
     c->d_ntsmall.release();
@@ -880,6 +949,66 @@ int rtb_set_strict_ties(rtb_context* c, int on) {
 }
 
 int rtb_fwd_launch_static(rtb_context* c) { return launch_static(c); }
+
+int rtb_fwd_set_schedule(rtb_context* c, int schedule, int blocks_per_sm) {
+    if (!c) return RTB_ERR_ARG;
+    if (schedule < 0 || schedule > 2 || blocks_per_sm < 0)
+        return fail(c, RTB_ERR_ARG, "schedule %d, blocks_per_sm %d", schedule, blocks_per_sm);
+    c->sched = schedule;
+    c->occ = blocks_per_sm;
+    if (!c->prepared) return RTB_OK;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    return apply_schedule(c);
+}
+
+int rtb_fwd_autotune(rtb_context* c, rtb_fwd_tune* out) {
+    if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const cudaStream_t strm = stream_of(c);
+    const int keep_graph = c->use_graph;
+    c->use_graph = 0;
+    float best = 3.4e38f;
+    int best_s = 0, best_b = c->bpsm_max, n = 0;
+    for (int sch = 0; sch <= 2; ++sch)
+        for (int b = c->bpsm_max; b >= 1 && b >= c->bpsm_max - 2; --b) {
+            c->sched = sch;
+            c->occ = b;
+            int r = apply_schedule(c);
+            if (r) return r;
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2; ++rep) {   // the second launch is timed
+                r = launch(c);
+                if (r) return r;
+                CUDA_TRY(c, cudaStreamSynchronize(strm));
+                CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            }
+            ++n;
+            if (ms < best) {
+                best = ms;
+                best_s = sch;
+                best_b = b;
+            }
+        }
+    c->sched = best_s;
+    c->occ = best_b;
+    c->use_graph = keep_graph;
+    const int r = apply_schedule(c);
+    if (r) return r;
+    if (out) {
+        out->schedule = best_s;
+        out->blocks_per_sm = best_b;
+        out->ms = best;
+        out->candidates = n;
+    }
+    return RTB_OK;
+}
+
+int rtb_fwd_use_graph(rtb_context* c, int on) {
+    if (!c) return RTB_ERR_ARG;
+    c->use_graph = on ? 1 : 0;
+    drop_graph(c);
+    return RTB_OK;
+}
 
 int rtb_get_debug_bins(const rtb_context* c, int16_t* perm, size_t n_perm, int16_t* split, size_t n_split) {
     if (!c || !c->debug) return RTB_ERR_ARG;

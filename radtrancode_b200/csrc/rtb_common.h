@@ -111,6 +111,10 @@ struct BatchDev {
     int strict_ties;               // 1: exact heapsort for every pass with tied keys
     int16_t* dbg_perm;             // debug capture for spectrum 0 (may be null)
     int16_t* dbg_split;
+    // schedule (autotuned): issue order of the items, and the dynamic
+    // work counter (zero at launch; nullptr = static grid-stride)
+    const int* item_order;
+    unsigned long long* work_next;
 };
 
 }  // namespace rtb

@@ -269,6 +269,90 @@ def batch_leg(ctx, kt, nspec):
     }
 
 
+SERVE_RATE = 2000.0           # offered requests/s, Poisson
+SERVE_WINDOW = 0.25           # s of arrivals in the default run (the serving workload's 60 s: --serve-window 60)
+SERVE_PLAIN = 24              # requests run one at a time for the plain per-request form
+SERVE_BUDGET = 16 << 30       # HBM arena of the server
+
+
+def serving_cases(ctx, kt, n, seed=5000):
+    """Requests with the uneven-batch size distribution: W~U[200,2000],
+    L~U[40,120], 1-4 absorbers, theta~U[0,70 deg]; observations from the
+    device forward model at the true states plus noise."""
+    from radtrancode_b200 import synth
+    rng = np.random.default_rng(seed)
+    cases = []
+    for i in range(n):
+        w = int(rng.integers(200, 2001))
+        iw0 = int(rng.integers(0, 2000 - w + 1))
+        L = int(rng.integers(40, 121))
+        na = int(rng.integers(1, 5))
+        ab = [synth.ABSORBERS_C2[k] for k in sorted(rng.choice(4, size=na, replace=False))]
+        cases.append(synth.make_retrieval(kt, ab, nlayer=L, seed=seed + 7 * i + 1, nwave=w, iw0=iw0,
+                                          theta_deg=float(rng.uniform(0.0, 70.0))))
+    outs = ctx.cirsrtfg_wave_batch([synth.job_at_state(c, c.x_true) for c in cases])
+    for i, c in enumerate(cases):
+        synth.observe(c, outs[i][0], seed=seed + 7 * i + 2)
+    return cases
+
+
+def serving_leg(ctx, kt, window, rate):
+    """Poisson arrivals into the continuous-batching server; latency from
+    each request's arrival time to its completion.  Beside it the plain
+    per-request GPU form (one retrieval at a time through
+    rtb_retrieve_batch)."""
+    from radtrancode_b200 import cirsradg
+    rng = np.random.default_rng(77)
+    arr = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * window * 1.5) + 16))
+    arr = arr[arr < window]
+    n = len(arr)
+    cases = serving_cases(ctx, kt, n)
+    lat, its, rounds, peak_active = [], [], 0, 0
+    i, pending = 0, {}
+    t0 = time.perf_counter()
+    with cirsradg.Server(ctx, SERVE_BUDGET, kiter=15, phlimit=0.1, dchisq_stop=0.1) as srv:
+        while i < n or pending:
+            now = time.perf_counter() - t0
+            while i < n and arr[i] <= now:
+                pending[srv.submit(cases[i])] = arr[i]
+                i += 1
+            if not pending:
+                time.sleep(max(0.0, arr[i] - now))
+                continue
+            active, _ = srv.step()
+            rounds += 1
+            peak_active = max(peak_active, active)
+            t = time.perf_counter() - t0
+            for rid in list(pending):
+                r = srv.poll(rid)
+                if r is not None:
+                    lat.append((t - pending.pop(rid)) * 1e3)
+                    its.append(r["iterations"])
+    t_total = time.perf_counter() - t0
+    plain = []
+    t = time.perf_counter()
+    for c in cases[:SERVE_PLAIN]:
+        t1 = time.perf_counter()
+        ctx.retrieve_batch([c], kiter=15, phlimit=0.1, dchisq_stop=0.1)
+        plain.append((time.perf_counter() - t1) * 1e3)
+    t_plain = time.perf_counter() - t
+    lat = np.array(lat)
+    return {
+        "workload": f"Poisson arrivals at {rate:.0f} req/s for {window} s ({n} requests), sizes of the uneven batch, "
+                    "up to 15 Newton iterations, early exit at |delta chi2| < 0.1, HBM budget "
+                    f"{SERVE_BUDGET >> 30} GiB",
+        "requests": n, "value": n / t_total, "unit": "retrievals/s", "wall_s": t_total, "rounds": rounds,
+        "peak_in_flight": peak_active,
+        "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
+        "p99_ms": float(np.percentile(lat, 99)), "iterations_mean": float(np.mean(its)),
+        "latency_note": "from the request's arrival time; the offered rate is above the service rate, so "
+                        "latency includes the wait for the backlog",
+        "plain_per_request": {"requests": SERVE_PLAIN, "value": SERVE_PLAIN / t_plain, "unit": "retrievals/s",
+                              "p50_ms": float(np.percentile(plain, 50)), "p99_ms": float(np.percentile(plain, 99)),
+                              "note": "one request at a time, rtb_retrieve_batch of one, service time only"},
+    }
+
+
 def retrieval_cases(ctx, kt, n, seed0=4000):
     """Full-size retrieval cases; observations from the device forward model
     at the true states (one batched launch) plus seeded noise."""
@@ -367,6 +451,8 @@ def main():
                     help="profiling case: only launch the forward kernel on the first N wavenumbers of the "
                          "workload (steps launches after warmup), print the kernel time, skip e2e and baselines")
     ap.add_argument("--no-retrieval", action="store_true", help="skip the retrieval leg")
+    ap.add_argument("--serve-window", type=float, default=SERVE_WINDOW,
+                    help="seconds of Poisson arrivals in the serving leg (0 skips it)")
     ap.add_argument("--batch-spectra", type=int, default=BATCH_SPECTRA,
                     help="uneven spectra in the batched leg (0 skips it)")
     args = ap.parse_args()
@@ -471,6 +557,8 @@ def main():
                 out["batch"] = batch_leg(ctx, kt, args.batch_spectra)
             if not args.no_retrieval:
                 out["retrieval"] = retrieval_leg(ctx, kt, cia, tensor_peak())
+            if args.serve_window > 0:
+                out["serving"] = serving_leg(ctx, kt, args.serve_window, SERVE_RATE)
         print(json.dumps(out))
     ctx.close()
     if world > 1:

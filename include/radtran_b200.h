@@ -344,7 +344,7 @@ typedef struct rtb_retrieval_result {
     int converged;            /* 0 kiter reached, 1 phlimit rule, 2 coreret.f:1022-1062
                                  alternate rule, 3 dchisq_stop */
     int nonpd;                /* a Cholesky pivot was replaced in some step */
-    double ms;                /* wall time from start of the call to this result */
+    double ms;                /* wall time from submission (start of the call) to completion */
 } rtb_retrieval_result;
 
 /* Run nret retrievals to completion.  All retrievals iterate together: each
@@ -357,6 +357,32 @@ typedef struct rtb_retrieval_result {
  * rounds. */
 int rtb_retrieve_batch(rtb_context* ctx, int nret, const rtb_retrieval_spec* specs,
                        const rtb_retrieval_opts* opts, rtb_retrieval_result* results);
+
+/* ---------------------------------------------------------------------- */
+/* Retrieval server (continuous batching)                                  */
+/* ---------------------------------------------------------------------- */
+
+/* A request loop over the same engine: requests are submitted at any time,
+ * admitted first come first served whenever their device state fits in the
+ * arena of hbm_budget_bytes (K of the current and the trial state, the
+ * measurement and the two spectra, Se^-1, Sa, Sa^-1), and join the next
+ * round; each round runs one batched Newton step, one batched
+ * forward+Jacobian launch over every request in flight, whatever its size,
+ * and the costs.  A request's result does not depend on what else is in
+ * flight.  One host thread drives a server (submit, step, poll). */
+typedef struct rtb_server rtb_server;
+int  rtb_server_create(rtb_context* ctx, size_t hbm_budget_bytes, const rtb_retrieval_opts* opts,
+                       rtb_server** out);
+void rtb_server_destroy(rtb_server* srv);
+/* copies the inputs (they may be freed on return); RTB_ERR_BUDGET if the
+ * request could never fit the budget */
+int  rtb_server_submit(rtb_server* srv, const rtb_retrieval_spec* spec, long long* id);
+/* one round; reports the requests in flight and waiting */
+int  rtb_server_step(rtb_server* srv, int* active, int* queued);
+/* *done = 1 and the result (x, yn into the caller's buffers; ms = latency
+ * from submission to completion) once request id has finished; each result
+ * is returned once */
+int  rtb_server_poll(rtb_server* srv, long long id, int* done, rtb_retrieval_result* result);
 
 /* rtb_fwd_launch_static -- rtb_fwd_launch without the context's scratch.
  * No counterpart in the reference (the reference has no device memory).

@@ -86,6 +86,16 @@ def lib() -> C.CDLL:
         L.rtb_fwd_autotune.restype = C.c_int
         L.rtb_fwd_use_graph.argtypes = [vp, C.c_int]
         L.rtb_fwd_use_graph.restype = C.c_int
+        L.rtb_server_create.argtypes = [vp, C.c_size_t, C.POINTER(_abi.RtbRetrievalOpts), C.POINTER(vp)]
+        L.rtb_server_create.restype = C.c_int
+        L.rtb_server_destroy.argtypes = [vp]
+        L.rtb_server_destroy.restype = None
+        L.rtb_server_submit.argtypes = [vp, C.POINTER(_abi.RtbRetrievalSpec), C.POINTER(C.c_longlong)]
+        L.rtb_server_submit.restype = C.c_int
+        L.rtb_server_step.argtypes = [vp, ip, ip]
+        L.rtb_server_step.restype = C.c_int
+        L.rtb_server_poll.argtypes = [vp, C.c_longlong, ip, C.POINTER(_abi.RtbRetrievalResult)]
+        L.rtb_server_poll.restype = C.c_int
         p16 = C.POINTER(C.c_int16)
         L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
         L.rtb_get_debug_bins.restype = C.c_int
@@ -100,5 +110,6 @@ EXPORTED = [
     "rtb_get_debug_bins", "rtb_set_strict_ties", "rtb_fwd_prepare", "rtb_fwd_launch", "rtb_fwd_fetch",
     "rtb_set_stream", "rtb_fwd_launch_static", "rtb_set_newton_mode", "rtb_newton_step_batch",
     "rtb_calc_phiret_batch", "rtb_spd_inverse_batch", "rtb_retrieve_batch", "rtb_get_newton_stats",
-    "rtb_fwd_set_schedule", "rtb_fwd_autotune", "rtb_fwd_use_graph",
+    "rtb_fwd_set_schedule", "rtb_fwd_autotune", "rtb_fwd_use_graph", "rtb_server_create", "rtb_server_destroy",
+    "rtb_server_submit", "rtb_server_step", "rtb_server_poll",
 ]

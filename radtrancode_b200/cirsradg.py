@@ -247,3 +247,56 @@ class Context:
         self._check(self._L.rtb_get_debug_bins(self._h, perm.ctypes.data_as(p16), perm.size,
                                                split.ctypes.data_as(p16), split.size))
         return perm, split
+
+
+class Server:
+    """Continuous-batching retrieval server (rtb_server_*): submit requests
+    at any time, call step() to run rounds, poll() for finished results."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int, kiter=10, phlimit=0.1, dchisq_stop=0.0):
+        self._ctx = ctx
+        self._L = ctx._L
+        o = _abi.RtbRetrievalOpts(kiter, phlimit, dchisq_stop, 0)
+        h = C.c_void_p()
+        ctx._check(self._L.rtb_server_create(ctx._h, hbm_budget_bytes, C.byref(o), C.byref(h)))
+        self._h = h
+        self._cases = {}
+
+    def close(self):
+        if self._h:
+            self._L.rtb_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, case) -> int:
+        s = case.as_struct()
+        rid = C.c_longlong()
+        self._ctx._check(self._L.rtb_server_submit(self._h, C.byref(s), C.byref(rid)))
+        self._cases[rid.value] = case
+        return rid.value
+
+    def step(self):
+        a, q = C.c_int(), C.c_int()
+        self._ctx._check(self._L.rtb_server_step(self._h, C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def poll(self, rid):
+        case = self._cases[rid]
+        r = _abi.RtbRetrievalResult()
+        x = np.zeros(case.nx, np.float32)
+        yn = np.zeros(case.ny, np.float32)
+        r.x, r.yn = _abi.fptr(x), _abi.fptr(yn)
+        done = C.c_int()
+        self._ctx._check(self._L.rtb_server_poll(self._h, rid, C.byref(done), C.byref(r)))
+        if not done.value:
+            return None
+        del self._cases[rid]
+        d = {k: getattr(r, k) for k in _abi.RESULT_KEYS}
+        d["x"], d["yn"] = x, yn
+        return d
+

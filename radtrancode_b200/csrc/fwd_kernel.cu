@@ -40,22 +40,6 @@ namespace {
 
 constexpr int kN = 484;              // largest NG*NG (NG <= 22)
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kBlockMax = 6;         // largest row block sorted by ranks (else merge)
-
-__device__ __forceinline__ unsigned long long shfl_up64(unsigned long long v, int d) {
-    unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-    lo = __shfl_up_sync(kFull, lo, d);
-    hi = __shfl_up_sync(kFull, hi, d);
-    return ((unsigned long long)hi << 32) | lo;
-}
-
-__device__ __forceinline__ unsigned long long shfl_xor64(unsigned long long v, int m) {
-    unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
-    lo = __shfl_xor_sync(kFull, lo, m);
-    hi = __shfl_xor_sync(kFull, hi, m);
-    return ((unsigned long long)hi << 32) | lo;
-}
-
 // order-preserving map of a float onto uint32 (-0 folded onto +0 first)
 __device__ __forceinline__ unsigned fkey(float f) {
     unsigned u = __float_as_uint(__fadd_rn(f, 0.0f));

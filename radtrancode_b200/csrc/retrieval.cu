@@ -15,6 +15,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <vector>
 
 #include "context.h"
@@ -165,132 +167,39 @@ void set_state(AtmWork& w, const float* x) {
     }
 }
 
-// ---------------------------------------------------------------- one resident group
-struct Ret {
+// ---------------------------------------------------------------- the retrieval engine
+// One retrieval in flight.  Device memory: a block of the engine's arena
+// (K of the current and the trial state, y and the two spectra, Se^-1,
+// Sa^-1, Sa and the Newton scratch) and a row of the state area (xa, xn,
+// xn1, x_out).
+struct Slot {
+    long long id = 0;
     int nx = 0, ny = 0, nlayer = 0;
-    // device offsets: floats into f32 (K pair), ysl (spectra), xsl (states); doubles into f64
-    int64_t k_off = 0, yn_off = 0, y_off = 0, x_off = 0, sei_off = 0, sai_off = 0, sa_off = 0, work_off = 0;
-    int cur = 0;                      // which K / yn buffer holds the current state
-    std::vector<float> xa, xn, xn1, x_out;
+    size_t bytes = 0, off = 0;        // arena block
+    int xrow = -1;                    // row of the state area
+    int phase = 0;                    // 0: first forward model pending; 1: iterating
+    int cur = 0;                      // which K / spectrum buffer holds the current state
+    std::vector<float> xa, xn, xn1, x_out, y;
+    std::vector<double> sei, sa;
     float phi = 0, ophi = 0, chisq = 0, ochisq = 0, alambda = 1.0f;
-    int iter = 0, forwards = 0, converged = 0, done = 0, nonpd = 0, need_newton = 1, trial = 0;
-    double t_done = 0;
+    int iter = 0, forwards = 0, converged = 0, done = 0, nonpd = 0, need_newton = 1;
+    double t_submit = 0, t_done = 0;
+    rtb_retrieval_result res{};
     AtmWork w;
+    // arena layout (element offsets from the block start)
+    int64_t k_elems() const { return 2 * (int64_t)nx * ny; }
+    int64_t y_elems() const { return 3 * al4(ny); }
 };
 
-struct Group {
-    std::vector<Ret> r;
-    DevBuf kbuf, ybuf, gts, xbuf, f64, nt_desc, phi_desc, small;
-    int64_t nk = 0, ny_tot = 0, nxs = 0, n64 = 0;
-};
-
-int newton_round(rtb_context* c, Group& G, const std::vector<int>& ids, cudaStream_t st) {
-    if (ids.empty()) return RTB_OK;
-    std::vector<NewtonDev> desc;
-    float* K = (float*)G.kbuf.p;
-    float* Y = (float*)G.ybuf.p;
-    float* X = (float*)G.xbuf.p;
-    double* D = (double*)G.f64.p;
-    for (int i : ids) {
-        const Ret& R = G.r[i];
-        NewtonDev d;
-        d.nx = R.nx;
-        d.ny = R.ny;
-        d.kt = K + R.k_off + (int64_t)R.cur * R.nx * R.ny;
-        d.y = Y + R.y_off;
-        d.yn = Y + R.yn_off + (int64_t)R.cur * al4(R.ny);
-        d.sei = D + R.sei_off;
-        d.sai = D + R.sai_off;
-        d.xa = X + R.x_off;
-        d.xn = X + R.x_off + al4(R.nx);
-        d.x_out = X + R.x_off + 3 * al4(R.nx);
-        d.work = D + R.work_off;
-        desc.push_back(d);
-    }
-    CUDA_TRY(c, h2d(G.nt_desc, desc, st));
-    unsigned* status = (unsigned*)G.small.p;
-    CUDA_TRY(c, launch_newton_step((const NewtonDev*)G.nt_desc.p, (int)ids.size(), c->newton_hess, c->newton_refine,
-                                   status, nullptr, st));
-    return RTB_OK;
+size_t slot_bytes(int nx, int ny) {
+    const size_t f = (size_t)(2 * (int64_t)nx * ny + 3 * al4(ny)) * 4;
+    const size_t d = (size_t)(2 * al4(ny) + 2 * (int64_t)nx * nx) * 8;
+    return (((f + 7) & ~(size_t)7) + d + 255) & ~(size_t)255;
 }
 
-int phi_round(rtb_context* c, Group& G, const std::vector<int>& ids, bool trial, cudaStream_t st) {
-    if (ids.empty()) return RTB_OK;
-    std::vector<PhiDev> desc;
-    float* Y = (float*)G.ybuf.p;
-    float* X = (float*)G.xbuf.p;
-    double* D = (double*)G.f64.p;
-    for (int i : ids) {
-        const Ret& R = G.r[i];
-        PhiDev d;
-        d.nx = R.nx;
-        d.ny = R.ny;
-        d.y = Y + R.y_off;
-        d.yn = Y + R.yn_off + (int64_t)(trial ? 1 - R.cur : R.cur) * al4(R.ny);
-        d.sei = D + R.sei_off;
-        d.sai = D + R.sai_off;
-        d.xn = X + R.x_off + (trial ? 2 : 1) * al4(R.nx);
-        d.xa = X + R.x_off;
-        desc.push_back(d);
-    }
-    CUDA_TRY(c, h2d(G.phi_desc, desc, st));
-    float* ph = (float*)((char*)G.small.p + 4 * (size_t)G.r.size());
-    CUDA_TRY(c, launch_phi((const PhiDev*)G.phi_desc.p, (int)ids.size(), ph, ph + G.r.size(), st));
-    return RTB_OK;
-}
-
-// forward + Jacobian of the listed retrievals at xn (trial=false, into the
-// current buffers) or xn1 (trial=true, into the other buffers)
-int forward_round(rtb_context* c, Group& G, const std::vector<int>& ids, bool trial) {
-    if (ids.empty()) return RTB_OK;
-    std::vector<rtb_atm> atms;
-    std::vector<int64_t> oo, jo;
-    for (int i : ids) {
-        Ret& R = G.r[i];
-        set_state(R.w, trial ? R.xn1.data() : R.xn.data());
-        atms.push_back(R.w.a);
-        const int b = trial ? 1 - R.cur : R.cur;
-        oo.push_back(R.yn_off + (int64_t)b * al4(R.ny));
-        jo.push_back(R.k_off + (int64_t)b * R.nx * R.ny);
-        R.forwards++;
-    }
-    OutPlace pl;
-    pl.calcout = (float*)G.ybuf.p;
-    pl.gradtsurf = (float*)G.gts.p;
-    pl.gradients = (float*)G.kbuf.p;
-    pl.out_off = oo.data();
-    pl.jac_off = jo.data();
-    int r = prepare_ex(c, (int)ids.size(), atms.data(), &pl);
-    if (r) return r;
-    r = launch(c);
-    if (r) return r;
-    return RTB_OK;
-}
-
-int upload_states(rtb_context* c, Group& G, cudaStream_t st) {
-    std::vector<float> xs((size_t)G.nxs, 0.0f);
-    for (const Ret& R : G.r) {
-        const int64_t s = al4(R.nx);
-        std::copy(R.xa.begin(), R.xa.end(), xs.begin() + R.x_off);
-        std::copy(R.xn.begin(), R.xn.end(), xs.begin() + R.x_off + s);
-        std::copy(R.xn1.begin(), R.xn1.end(), xs.begin() + R.x_off + 2 * s);
-    }
-    CUDA_TRY(c, cudaMemcpyAsync(G.xbuf.p, xs.data(), xs.size() * sizeof(float), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(c, cudaStreamSynchronize(st));   // xs is a local
-    return RTB_OK;
-}
-
-int check_status(rtb_context* c, cudaStream_t st) {
-    CUDA_TRY(c, cudaStreamSynchronize(st));
-    unsigned long long diag[8];
-    CUDA_TRY(c, cudaMemcpy(diag, c->d_diag.p, 64, cudaMemcpyDeviceToHost));
-    if ((unsigned)(diag[0] & 0xffffffffu) & kStGord)
-        return fail(c, RTB_ERR_GORD, "g-ordinate walk ran past NG (rankg.f:118-147)");
-    return RTB_OK;
-}
-
-// coreret.f:621-700: next trial state, or a rejection before the forward model
-bool make_trial(Ret& R) {
+// coreret.f:621-700 and :757-766: the next trial state, or its rejection
+// before the forward model (NaN, log variable out of range, T < 1)
+bool make_trial(Slot& R) {
     const int nx = R.nx;
     R.xn1.resize(nx);
     for (int i = 0; i < nx; ++i) {
@@ -305,7 +214,7 @@ bool make_trial(Ret& R) {
             return false;
         }
     }
-    for (int i = 0; i < R.nlayer; ++i)                       // :757-766, model-0 temperature
+    for (int i = 0; i < R.nlayer; ++i)                       // model-0 temperature
         if (R.xn1[i] < 1.0f) {
             R.alambda = std::min(R.alambda * 10.0f, 1e10f);
             return false;
@@ -313,8 +222,8 @@ bool make_trial(Ret& R) {
     return true;
 }
 
-// coreret.f:957-1062 for one evaluated trial state
-void decide(Ret& R, float phi, float chisq, const rtb_retrieval_opts& o, double t) {
+// coreret.f:957-1062 for one evaluated trial state (REAL arithmetic)
+void decide(Slot& R, float phi, float chisq, const rtb_retrieval_opts& o) {
     const float tphi = 100.0f * (R.ophi - phi) / R.ophi;
     const float abstphi = std::fabs(tphi);
     auto accept = [&]() {
@@ -334,7 +243,7 @@ void decide(Ret& R, float phi, float chisq, const rtb_retrieval_opts& o, double 
             R.ophi = phi;
             R.alambda = R.alambda * 0.3f;
         }
-        if (!R.done && o.dchisq_stop > 0.0f && dchi < o.dchisq_stop) {
+        if (!R.done && o.dchisq_stop > 0.0f && dchi < o.dchisq_stop) {   // the optional early exit
             R.converged = 3;
             R.done = 1;
         }
@@ -350,189 +259,353 @@ void decide(Ret& R, float phi, float chisq, const rtb_retrieval_opts& o, double 
     } else {
         R.alambda = std::min(R.alambda * 10.0f, 1e10f);
     }
-    if (R.done) R.t_done = t;
 }
 
-int run_group(rtb_context* c, const rtb_retrieval_spec* specs, int n, const rtb_retrieval_opts& o,
-              rtb_retrieval_result* res, double t0) {
-    const cudaStream_t st = stream_of(c);
-    Group G;
-    G.r.resize(n);
-    // ---- layout
-    int64_t nk = 0, nys = 0, nxs = 0, n64 = 0;
-    for (int i = 0; i < n; ++i) {
-        Ret& R = G.r[i];
-        const rtb_retrieval_spec& s = specs[i];
-        if (!s.atm || !s.y || !s.sei || !s.sa || !s.xa) return fail(c, RTB_ERR_ARG, "retrieval %d: NULL input", i);
-        int e = build_work(c, s, R.w);
-        if (e) return e;
-        R.nlayer = s.atm->nlayer;
-        R.nx = s.atm->nv;
-        R.ny = s.atm->nwave;
-        R.k_off = nk;
-        nk += 2 * (int64_t)R.nx * R.ny;
-        R.y_off = nys;
-        R.yn_off = nys + al4(R.ny);
-        nys += 3 * al4(R.ny);
-        R.x_off = nxs;
-        nxs += 4 * al4(R.nx);
-        R.sei_off = n64;
-        n64 += al4(R.ny);
-        R.sai_off = n64;
-        n64 += (int64_t)R.nx * R.nx;
-        R.sa_off = n64;
-        n64 += (int64_t)R.nx * R.nx;
-        R.work_off = n64;
-        n64 += al4(R.ny);
-        R.xa.assign(s.xa, s.xa + R.nx);
-        R.xn.assign(s.x0 ? s.x0 : s.xa, (s.x0 ? s.x0 : s.xa) + R.nx);
-        R.xn1 = R.xn;
-        R.x_out = R.xn;
+constexpr int kXRow = 4 * kNewtonMaxNx;   // floats per state-area row: xa | xn | xn1 | x_out
+
+struct Engine {
+    rtb_context* c = nullptr;
+    rtb_retrieval_opts o{10, 0.1f, 0.0f, 0};
+    size_t budget = 0;
+    DevBuf arena, xarea, nt_desc, phi_desc, small;
+    std::map<size_t, size_t> free_list;   // offset -> size
+    std::vector<int> free_rows;
+    int rows = 0;
+    std::deque<Slot*> queue;
+    std::vector<Slot*> active;
+    std::map<long long, Slot*> finished;
+    long long next_id = 1;
+    double t0 = 0;
+    ~Engine() {
+        for (Slot* s : queue) delete s;
+        for (Slot* s : active) delete s;
+        for (auto& kv : finished) delete kv.second;
+        arena.release();
+        xarea.release();
+        nt_desc.release();
+        phi_desc.release();
+        small.release();
     }
-    G.nk = nk;
-    G.ny_tot = nys;
-    G.nxs = nxs;
-    G.n64 = n64;
-    CUDA_TRY(c, G.kbuf.ensure((size_t)nk * 4));
-    CUDA_TRY(c, G.ybuf.ensure((size_t)nys * 4));
-    CUDA_TRY(c, G.gts.ensure((size_t)nys * 4));
-    CUDA_TRY(c, G.xbuf.ensure((size_t)nxs * 4));
-    CUDA_TRY(c, G.f64.ensure((size_t)n64 * 8));
-    CUDA_TRY(c, G.small.ensure((size_t)12 * n + 64));
-    // ---- resident inputs: y, Se^-1, Sa (-> Sa^-1 on the device)
-    {
-        std::vector<float> ys((size_t)nys, 0.0f);
-        std::vector<double> ds((size_t)n64, 0.0);
-        for (int i = 0; i < n; ++i) {
-            const Ret& R = G.r[i];
-            std::copy(specs[i].y, specs[i].y + R.ny, ys.begin() + R.y_off);
-            std::copy(specs[i].sei, specs[i].sei + R.ny, ds.begin() + R.sei_off);
-            std::copy(specs[i].sa, specs[i].sa + (size_t)R.nx * R.nx, ds.begin() + R.sa_off);
+
+    float* F() const { return (float*)arena.p; }
+    float* K(const Slot& s, int b) const { return F() + s.off / 4 + (int64_t)b * s.nx * s.ny; }
+    float* Yb(const Slot& s) const { return F() + s.off / 4 + s.k_elems(); }          // y
+    float* Yn(const Slot& s, int b) const { return Yb(s) + (1 + b) * al4(s.ny); }     // spectrum b
+    double* Db(const Slot& s) const {
+        const size_t f = (size_t)(s.k_elems() + s.y_elems()) * 4;
+        return (double*)((char*)arena.p + s.off + ((f + 7) & ~(size_t)7));
+    }
+    double* Sei(const Slot& s) const { return Db(s); }
+    double* Work(const Slot& s) const { return Db(s) + al4(s.ny); }
+    double* Sai(const Slot& s) const { return Db(s) + 2 * al4(s.ny); }
+    double* Sa(const Slot& s) const { return Sai(s) + (int64_t)s.nx * s.nx; }
+    float* X(const Slot& s, int part) const { return (float*)xarea.p + (int64_t)s.xrow * kXRow + part * kNewtonMaxNx; }
+
+    int init(rtb_context* ctx, const rtb_retrieval_opts& opts, size_t bytes) {
+        c = ctx;
+        o = opts;
+        budget = bytes;
+        CUDA_TRY(c, arena.ensure(budget));
+        free_list.clear();
+        free_list[0] = budget;
+        t0 = now_ms();
+        return RTB_OK;
+    }
+
+    bool alloc(size_t n, size_t& off) {
+        for (auto it = free_list.begin(); it != free_list.end(); ++it)
+            if (it->second >= n) {
+                off = it->first;
+                const size_t rest = it->second - n;
+                free_list.erase(it);
+                if (rest) free_list[off + n] = rest;
+                return true;
+            }
+        return false;
+    }
+
+    void release(size_t off, size_t n) {
+        auto it = free_list.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_list.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_list.erase(nx);
         }
-        CUDA_TRY(c, cudaMemcpyAsync(G.ybuf.p, ys.data(), ys.size() * 4, cudaMemcpyHostToDevice, st));
-        CUDA_TRY(c, cudaMemcpyAsync(G.f64.p, ds.data(), ds.size() * 8, cudaMemcpyHostToDevice, st));
-        double* D = (double*)G.f64.p;
-        for (int i = 0; i < n; ++i) {   // one launch per distinct nx would also do; inversion is one-time
-            const Ret& R = G.r[i];
-            CUDA_TRY(c, launch_spd_inverse(D + R.sa_off, D + R.sai_off, R.nx, 0, 1, nullptr, st));
+        if (it != free_list.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_list.erase(it);
+            }
         }
+    }
+
+    int submit(const rtb_retrieval_spec& sp, long long* id) {
+        if (!sp.atm || !sp.y || !sp.sei || !sp.sa || !sp.xa) return fail(c, RTB_ERR_ARG, "retrieval: NULL input");
+        Slot* s = new Slot;
+        int e = build_work(c, sp, s->w);
+        if (e) {
+            delete s;
+            return e;
+        }
+        s->nlayer = sp.atm->nlayer;
+        s->nx = sp.atm->nv;
+        s->ny = sp.atm->nwave;
+        s->bytes = slot_bytes(s->nx, s->ny);
+        if (s->bytes > budget) {
+            delete s;
+            return fail(c, RTB_ERR_BUDGET, "retrieval needs %zu B, budget %zu B", slot_bytes(sp.atm->nv, sp.atm->nwave),
+                        budget);
+        }
+        s->xa.assign(sp.xa, sp.xa + s->nx);
+        const float* x0 = sp.x0 ? sp.x0 : sp.xa;
+        s->xn.assign(x0, x0 + s->nx);
+        s->xn1 = s->xn;
+        s->x_out = s->xn;
+        s->y.assign(sp.y, sp.y + s->ny);
+        s->sei.assign(sp.sei, sp.sei + s->ny);
+        s->sa.assign(sp.sa, sp.sa + (size_t)s->nx * s->nx);
+        s->id = next_id++;
+        s->t_submit = now_ms();
+        queue.push_back(s);
+        if (id) *id = s->id;
+        return RTB_OK;
+    }
+
+    // admit queued retrievals, first come first served, while the arena has room
+    int admit(cudaStream_t st) {
+        std::vector<Slot*> adm;
+        while (!queue.empty()) {
+            if (o.max_batch > 0 && (int)(active.size() + adm.size()) >= o.max_batch) break;
+            Slot* s = queue.front();
+            size_t off;
+            if (!alloc(s->bytes, off)) break;
+            s->off = off;
+            queue.pop_front();
+            adm.push_back(s);
+        }
+        if (adm.empty()) return RTB_OK;
+        // state-area rows (grow: the whole area is re-uploaded every round)
+        for (Slot* s : adm) {
+            if (free_rows.empty()) free_rows.push_back(rows++);
+            s->xrow = free_rows.back();
+            free_rows.pop_back();
+        }
+        CUDA_TRY(c, xarea.ensure((size_t)rows * kXRow * 4));
+        for (Slot* s : adm) {
+            CUDA_TRY(c, cudaMemcpyAsync(Yb(*s), s->y.data(), (size_t)s->ny * 4, cudaMemcpyHostToDevice, st));
+            CUDA_TRY(c, cudaMemcpyAsync(Sei(*s), s->sei.data(), (size_t)s->ny * 8, cudaMemcpyHostToDevice, st));
+            CUDA_TRY(c, cudaMemcpyAsync(Sa(*s), s->sa.data(), (size_t)s->nx * s->nx * 8, cudaMemcpyHostToDevice, st));
+            CUDA_TRY(c, launch_spd_inverse(Sa(*s), Sai(*s), s->nx, 0, 1, nullptr, st));
+            active.push_back(s);
+        }
+        CUDA_TRY(c, cudaStreamSynchronize(st));   // host copies of y/sei/sa stay alive until here
+        return RTB_OK;
+    }
+
+    int upload_x(cudaStream_t st) {
+        std::vector<float> xs((size_t)rows * kXRow, 0.0f);
+        for (const Slot* s : active) {
+            float* r = xs.data() + (size_t)s->xrow * kXRow;
+            std::copy(s->xa.begin(), s->xa.end(), r);
+            std::copy(s->xn.begin(), s->xn.end(), r + kNewtonMaxNx);
+            std::copy(s->xn1.begin(), s->xn1.end(), r + 2 * kNewtonMaxNx);
+        }
+        CUDA_TRY(c, cudaMemcpyAsync(xarea.p, xs.data(), xs.size() * 4, cudaMemcpyHostToDevice, st));
         CUDA_TRY(c, cudaStreamSynchronize(st));
+        return RTB_OK;
     }
-    std::vector<int> all(n);
-    for (int i = 0; i < n; ++i) all[i] = i;
-    std::vector<float> ph(2 * (size_t)n);
-    // ---- initial forward model and cost (coreret.f:520-557)
-    {
-        int e = upload_states(c, G, st);
-        if (e) return e;
-        e = forward_round(c, G, all, false);
-        if (e) return e;
-        e = check_status(c, st);
-        if (e) return e;
-        e = phi_round(c, G, all, false, st);
-        if (e) return e;
-        CUDA_TRY(c, cudaMemcpyAsync(ph.data(), (char*)G.small.p + 4 * (size_t)n, 8 * (size_t)n,
-                                    cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(c, cudaStreamSynchronize(st));
-        for (int i = 0; i < n; ++i) {
-            Ret& R = G.r[i];
-            R.phi = R.ophi = ph[i];
-            R.chisq = R.ochisq = ph[n + i];
-            R.alambda = 1.0f;
+
+    int newton(const std::vector<Slot*>& v, cudaStream_t st) {
+        std::vector<NewtonDev> desc;
+        for (const Slot* s : v) {
+            NewtonDev d;
+            d.nx = s->nx;
+            d.ny = s->ny;
+            d.kt = K(*s, s->cur);
+            d.y = Yb(*s);
+            d.yn = Yn(*s, s->cur);
+            d.sei = Sei(*s);
+            d.sai = Sai(*s);
+            d.xa = X(*s, 0);
+            d.xn = X(*s, 1);
+            d.x_out = X(*s, 3);
+            d.work = Work(*s);
+            desc.push_back(d);
         }
+        CUDA_TRY(c, h2d(nt_desc, desc, st));
+        CUDA_TRY(c, small.ensure(12 * v.size() + 64));
+        CUDA_TRY(c, launch_newton_step((const NewtonDev*)nt_desc.p, (int)v.size(), c->newton_hess, c->newton_refine,
+                                       (unsigned*)small.p, nullptr, st));
+        std::vector<float> xs((size_t)rows * kXRow);
+        std::vector<unsigned> sts(v.size());
+        CUDA_TRY(c, cudaMemcpyAsync(xs.data(), xarea.p, xs.size() * 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(c, cudaMemcpyAsync(sts.data(), small.p, 4 * v.size(), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(c, cudaStreamSynchronize(st));
+        for (size_t k = 0; k < v.size(); ++k) {
+            Slot& s = *v[k];
+            const float* xo = xs.data() + (size_t)s.xrow * kXRow + 3 * kNewtonMaxNx;
+            s.x_out.assign(xo, xo + s.nx);
+            if (sts[k] & kNtNonPd) s.nonpd = 1;
+            s.need_newton = 0;
+        }
+        return RTB_OK;
     }
-    // ---- iterations (coreret.f:591-1106)
-    for (;;) {
-        std::vector<int> act;
-        for (int i = 0; i < n; ++i)
-            if (!G.r[i].done) act.push_back(i);
-        if (act.empty()) break;
-        std::vector<int> nt;
-        for (int i : act)
-            if (G.r[i].need_newton) nt.push_back(i);
+
+    // forward model of each listed retrieval (the first at xn into the
+    // current buffers, later ones at xn1 into the other buffers), then phi
+    int forward_phi(const std::vector<Slot*>& v, std::vector<float>& ph, cudaStream_t st) {
+        std::vector<rtb_atm> atms;
+        std::vector<int64_t> oo, jo;
+        for (Slot* s : v) {
+            const bool first = s->phase == 0;
+            set_state(s->w, first ? s->xn.data() : s->xn1.data());
+            atms.push_back(s->w.a);
+            const int b = first ? s->cur : 1 - s->cur;
+            oo.push_back(Yn(*s, b) - F());
+            jo.push_back(K(*s, b) - F());
+            s->forwards++;
+        }
+        OutPlace pl;
+        pl.calcout = F();
+        pl.gradtsurf = nullptr;
+        pl.gradients = F();
+        pl.out_off = oo.data();
+        pl.jac_off = jo.data();
+        int r = prepare_ex(c, (int)v.size(), atms.data(), &pl);
+        if (r) return r;
+        r = launch(c);
+        if (r) return r;
+        CUDA_TRY(c, cudaStreamSynchronize(st));
+        unsigned long long diag[8];
+        CUDA_TRY(c, cudaMemcpy(diag, c->d_diag.p, 64, cudaMemcpyDeviceToHost));
+        if ((unsigned)(diag[0] & 0xffffffffu) & kStGord)
+            return fail(c, RTB_ERR_GORD, "g-ordinate walk ran past NG (rankg.f:118-147)");
+        std::vector<PhiDev> desc;
+        for (const Slot* s : v) {
+            const bool first = s->phase == 0;
+            PhiDev d;
+            d.nx = s->nx;
+            d.ny = s->ny;
+            d.y = Yb(*s);
+            d.yn = Yn(*s, first ? s->cur : 1 - s->cur);
+            d.sei = Sei(*s);
+            d.sai = Sai(*s);
+            d.xn = X(*s, first ? 1 : 2);
+            d.xa = X(*s, 0);
+            desc.push_back(d);
+        }
+        CUDA_TRY(c, h2d(phi_desc, desc, st));
+        CUDA_TRY(c, small.ensure(12 * v.size() + 64));
+        float* out = (float*)small.p;
+        CUDA_TRY(c, launch_phi((const PhiDev*)phi_desc.p, (int)v.size(), out, out + v.size(), st));
+        ph.resize(2 * v.size());
+        CUDA_TRY(c, cudaMemcpyAsync(ph.data(), out, 8 * v.size(), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(c, cudaStreamSynchronize(st));
+        return RTB_OK;
+    }
+
+    void finish(Slot* s) {
+        s->done = 1;
+        s->t_done = now_ms();
+        rtb_retrieval_result& r = s->res;
+        r.phi = s->phi;
+        r.chisq = s->chisq;
+        r.alambda = s->alambda;
+        r.iterations = s->iter;
+        r.forwards = s->forwards;
+        r.converged = s->converged;
+        r.nonpd = s->nonpd;
+        r.ms = s->t_done - s->t_submit;
+    }
+
+    // one round: admissions, Newton steps, trial states, one batched
+    // forward+Jacobian launch, the costs, the coreret decisions, retirements
+    int round() {
+        const cudaStream_t st = stream_of(c);
+        int e = admit(st);
+        if (e) return e;
+        if (active.empty()) return RTB_OK;
+        std::vector<Slot*> nt;
+        for (Slot* s : active)
+            if (s->phase == 1 && s->need_newton) nt.push_back(s);
         if (!nt.empty()) {
-            int e = upload_states(c, G, st);
+            e = upload_x(st);
             if (e) return e;
-            e = newton_round(c, G, nt, st);
+            e = newton(nt, st);
             if (e) return e;
-            std::vector<float> xs((size_t)G.nxs);
-            std::vector<unsigned> sts(n);
-            CUDA_TRY(c, cudaMemcpyAsync(xs.data(), G.xbuf.p, xs.size() * 4, cudaMemcpyDeviceToHost, st));
-            CUDA_TRY(c, cudaMemcpyAsync(sts.data(), G.small.p, 4 * nt.size(), cudaMemcpyDeviceToHost, st));
-            CUDA_TRY(c, cudaStreamSynchronize(st));
-            for (size_t k = 0; k < nt.size(); ++k) {
-                Ret& R = G.r[nt[k]];
-                const float* xo = xs.data() + R.x_off + 3 * al4(R.nx);
-                R.x_out.assign(xo, xo + R.nx);
-                if (sts[k] & kNtNonPd) R.nonpd = 1;
-                R.need_newton = 0;
-            }
         }
-        std::vector<int> fw;
-        for (int i : act) {
-            Ret& R = G.r[i];
-            R.iter++;
-            if (make_trial(R)) {
-                fw.push_back(i);
-            } else if (R.iter >= o.kiter) {
-                R.done = 1;
-                R.t_done = now_ms() - t0;
+        std::vector<Slot*> fw;
+        for (Slot* s : active) {
+            if (s->phase == 0) {
+                fw.push_back(s);
+                continue;
             }
+            s->iter++;
+            if (make_trial(*s)) fw.push_back(s);
+            else if (s->iter >= o.kiter) finish(s);
         }
         if (!fw.empty()) {
-            int e = upload_states(c, G, st);
+            e = upload_x(st);
             if (e) return e;
-            e = forward_round(c, G, fw, true);
+            std::vector<float> ph;
+            e = forward_phi(fw, ph, st);
             if (e) return e;
-            e = check_status(c, st);
-            if (e) return e;
-            e = phi_round(c, G, fw, true, st);
-            if (e) return e;
-            CUDA_TRY(c, cudaMemcpyAsync(ph.data(), (char*)G.small.p + 4 * (size_t)n, 8 * (size_t)n,
-                                        cudaMemcpyDeviceToHost, st));
-            CUDA_TRY(c, cudaStreamSynchronize(st));
-            const double t = now_ms() - t0;
-            for (size_t k = 0; k < fw.size(); ++k) {
-                Ret& R = G.r[fw[k]];
-                decide(R, ph[k], ph[n + k], o, t);
-                if (!R.done && R.iter >= o.kiter) {
-                    R.done = 1;
-                    R.t_done = t;
+            const size_t n = fw.size();
+            for (size_t k = 0; k < n; ++k) {
+                Slot& s = *fw[k];
+                if (s.phase == 0) {                 // coreret.f:554-582
+                    s.phi = s.ophi = ph[k];
+                    s.chisq = s.ochisq = ph[n + k];
+                    s.alambda = 1.0f;
+                    s.phase = 1;
+                    s.need_newton = 1;
+                    continue;
                 }
+                decide(s, ph[k], ph[n + k], o);
+                if (s.done) finish(&s);
+                else if (s.iter >= o.kiter) finish(&s);
             }
         }
-    }
-    // ---- results: state, spectrum of the current buffers
-    std::vector<float> ys((size_t)G.ny_tot);
-    CUDA_TRY(c, cudaMemcpyAsync(ys.data(), G.ybuf.p, ys.size() * 4, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(c, cudaStreamSynchronize(st));
-    for (int i = 0; i < n; ++i) {
-        const Ret& R = G.r[i];
-        rtb_retrieval_result& o2 = res[i];
-        if (o2.x) std::copy(R.xn.begin(), R.xn.end(), o2.x);
-        if (o2.yn) {
-            const float* y = ys.data() + R.yn_off + (int64_t)R.cur * al4(R.ny);
-            std::copy(y, y + R.ny, o2.yn);
+        // retire
+        std::vector<Slot*> keep;
+        for (Slot* s : active) {
+            if (!s->done) {
+                keep.push_back(s);
+                continue;
+            }
+            s->res.x = nullptr;
+            s->res.yn = nullptr;
+            // the result spectrum stays readable until the slot's block is released here
+            s->y.resize(s->ny);
+            CUDA_TRY(c, cudaMemcpy(s->y.data(), Yn(*s, s->cur), (size_t)s->ny * 4, cudaMemcpyDeviceToHost));
+            release(s->off, s->bytes);
+            free_rows.push_back(s->xrow);
+            finished[s->id] = s;
         }
-        o2.phi = R.phi;
-        o2.chisq = R.chisq;
-        o2.alambda = R.alambda;
-        o2.iterations = R.iter;
-        o2.forwards = R.forwards;
-        o2.converged = R.converged;
-        o2.nonpd = R.nonpd;
-        o2.ms = R.t_done;
+        active.swap(keep);
+        return RTB_OK;
     }
-    G.kbuf.release();
-    G.ybuf.release();
-    G.gts.release();
-    G.xbuf.release();
-    G.f64.release();
-    G.nt_desc.release();
-    G.phi_desc.release();
-    G.small.release();
-    return RTB_OK;
-}
+
+    // copy a finished retrieval's result out (x, yn into the caller's buffers)
+    int take(long long id, rtb_retrieval_result* out, bool erase) {
+        auto it = finished.find(id);
+        if (it == finished.end()) return 0;
+        Slot* s = it->second;
+        float* x = out->x;
+        float* yn = out->yn;
+        *out = s->res;
+        out->x = x;
+        out->yn = yn;
+        if (x) std::copy(s->xn.begin(), s->xn.end(), x);
+        if (yn) std::copy(s->y.begin(), s->y.end(), yn);
+        if (erase) {
+            delete s;
+            finished.erase(it);
+        }
+        return 1;
+    }
+};
 
 }  // namespace
 
@@ -695,13 +768,79 @@ int rtb_retrieve_batch(rtb_context* c, int nret, const rtb_retrieval_spec* specs
     if (opts) o = *opts;
     if (o.kiter < 1) return fail(c, RTB_ERR_ARG, "kiter < 1");
     CUDA_TRY(c, cudaSetDevice(c->device));
-    const double t0 = now_ms();
-    const int chunk = o.max_batch > 0 ? o.max_batch : nret;
-    for (int s = 0; s < nret; s += chunk) {
-        const int n = std::min(chunk, nret - s);
-        const int r = run_group(c, specs + s, n, o, results + s, t0);
+    // arena: every retrieval resident at once, or the max_batch largest
+    std::vector<size_t> sz(nret);
+    for (int i = 0; i < nret; ++i) {
+        if (!specs[i].atm) return fail(c, RTB_ERR_ARG, "retrieval %d: NULL atmosphere", i);
+        sz[i] = slot_bytes(specs[i].atm->nv, specs[i].atm->nwave);
+    }
+    std::sort(sz.begin(), sz.end(), std::greater<size_t>());
+    const int m = o.max_batch > 0 ? std::min(o.max_batch, nret) : nret;
+    size_t need = 0;
+    for (int i = 0; i < m; ++i) need += sz[i];
+    Engine E;
+    int r = E.init(c, o, need);
+    if (r) return r;
+    std::vector<long long> ids(nret);
+    for (int i = 0; i < nret; ++i) {
+        r = E.submit(specs[i], &ids[i]);
         if (r) return r;
     }
+    while (!E.queue.empty() || !E.active.empty()) {
+        r = E.round();
+        if (r) return r;
+    }
+    for (int i = 0; i < nret; ++i) E.take(ids[i], &results[i], true);
+    return RTB_OK;
+}
+
+struct rtb_server {
+    rtb::Engine E;
+};
+
+int rtb_server_create(rtb_context* c, size_t hbm_budget_bytes, const rtb_retrieval_opts* opts, rtb_server** out) {
+    if (!c || !out) return RTB_ERR_ARG;
+    *out = nullptr;
+    if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
+    if (hbm_budget_bytes < 4096) return fail(c, RTB_ERR_ARG, "budget of %zu B", hbm_budget_bytes);
+    rtb_retrieval_opts o{10, 0.1f, 0.0f, 0};
+    if (opts) o = *opts;
+    if (o.kiter < 1) return fail(c, RTB_ERR_ARG, "kiter < 1");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    rtb_server* s = new rtb_server;
+    const int r = s->E.init(c, o, hbm_budget_bytes);
+    if (r) {
+        delete s;
+        return r;
+    }
+    *out = s;
+    return RTB_OK;
+}
+
+void rtb_server_destroy(rtb_server* s) {
+    if (!s) return;
+    cudaSetDevice(s->E.c->device);
+    cudaStreamSynchronize(stream_of(s->E.c));
+    delete s;
+}
+
+int rtb_server_submit(rtb_server* s, const rtb_retrieval_spec* spec, long long* id) {
+    if (!s || !spec) return RTB_ERR_ARG;
+    return s->E.submit(*spec, id);
+}
+
+int rtb_server_step(rtb_server* s, int* active, int* queued) {
+    if (!s) return RTB_ERR_ARG;
+    CUDA_TRY(s->E.c, cudaSetDevice(s->E.c->device));
+    const int r = s->E.round();
+    if (active) *active = (int)s->E.active.size();
+    if (queued) *queued = (int)s->E.queue.size();
+    return r;
+}
+
+int rtb_server_poll(rtb_server* s, long long id, int* done, rtb_retrieval_result* result) {
+    if (!s || !done || !result) return RTB_ERR_ARG;
+    *done = s->E.take(id, result, true);
     return RTB_OK;
 }
 

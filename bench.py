@@ -441,6 +441,27 @@ def profile_case(args):
             print(json.dumps({"profile_waves": args.profile_waves, "ms_kernel": ctx.stats()["ms_kernel"]}))
 
 
+def profile_newton(args):
+    """Reduced case for ncu captures of the Newton-step kernel:
+    `--profile-newton` full-size retrievals (NX=124, NY=2000) with seeded
+    K of the forward model's magnitude, warm-up + `--steps` launches."""
+    from radtrancode_b200 import cirsradg, synth
+    n, nx, ny = args.profile_newton, 124, 2000
+    rng = np.random.default_rng(11)
+    p_lev, p_lay = synth._levels(120)
+    sa = synth.prior_covariance(p_lay, 4)
+    sai = np.broadcast_to(np.linalg.inv(sa), (n, nx, nx))
+    kk = (rng.standard_normal((n, nx, ny)) * 1e-9).astype(np.float32)
+    sei = np.full((n, ny), 1e18)
+    xa = np.full((n, nx), 150.0, np.float32)
+    y = (rng.standard_normal((n, ny)) * 1e-8).astype(np.float32)
+    yn = np.zeros((n, ny), np.float32)
+    with cirsradg.Context(0) as ctx:
+        for _ in range(args.warmup + args.steps):
+            ctx.newton_step_batch(kk, sei, sai, xa, xa, y, yn)
+            print(json.dumps({"profile_newton": n, "ms_kernel": ctx.newton_stats()["ms_kernel"]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -455,9 +476,14 @@ def main():
                     help="seconds of Poisson arrivals in the serving leg (0 skips it)")
     ap.add_argument("--batch-spectra", type=int, default=BATCH_SPECTRA,
                     help="uneven spectra in the batched leg (0 skips it)")
+    ap.add_argument("--profile-newton", type=int, default=0,
+                    help="profiling case: only the Newton-step kernel on N full-size retrievals")
     args = ap.parse_args()
     if args.profile_waves:
         profile_case(args)
+        return
+    if args.profile_newton:
+        profile_newton(args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

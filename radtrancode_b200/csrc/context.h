@@ -69,12 +69,14 @@ struct Staging {
     std::vector<float> amo;
     std::vector<WaveDev> wave;
     std::vector<int64_t> wg_slice;
+    std::vector<float> wg_w2;         // [.. nwave][ngas] upper-point weight, < 0 coincident
+    bool any_noncoinc = false;
     std::vector<float> xsec, cont;
     std::vector<int> p_layinc;
     std::vector<float> p_scale, p_emtemp;
     std::vector<int> map_colptr, map_row;
     std::vector<float> map_val;
-    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1;
+    int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, ngas_max = 1;
     int64_t n_out = 0, n_jac = 0;
 };
 

@@ -167,6 +167,119 @@ struct Diag {
 // ---------------------------------------------------------------------------
 // get_kg for one gas at one layer: lane g < ng returns k(g), dk/dT(g)
 // (get_kg.f:320-378 coincident branch, NaN -> 1e-37 at :443-471).
+// RANKK (radtran/cirsradg/rankk.f:34-117) on one thread: REAL cumulative
+// ordinates and distribution summed in the reference's order, the `<=` test,
+// the split fraction and the ig <= ng guards.  cont/dcont/weight are sorted
+// and permuted in place (sort2g heapsort); ico is scratch.
+__device__ void rankk_lane(int ng, const float* gw, int nloop, float* cont, float* dcont, float* weight,
+                                        unsigned short* ico, float* tmp, float* k_g, float* dkdt) {
+    float g_ord[kMaxNg + 1];
+    g_ord[0] = 0.0f;
+    for (int i = 0; i < ng; ++i) g_ord[i + 1] = __fadd_rn(g_ord[i], gw[i]);
+    if (g_ord[ng] < 1.0f) g_ord[ng] = 1.0f;
+    for (int i = 0; i < nloop; ++i) ico[i] = (unsigned short)i;
+    heapsort_sort2g(nloop, cont, ico);
+    for (int i = 0; i < nloop; ++i) tmp[i] = weight[ico[i]];
+    for (int i = 0; i < nloop; ++i) weight[i] = tmp[i];
+    for (int i = 0; i < nloop; ++i) tmp[i] = dcont[ico[i]];
+    for (int i = 0; i < nloop; ++i) dcont[i] = tmp[i];
+    // gdist(I) in tmp[I], I = 0..nloop
+    tmp[0] = 0.0f;
+    tmp[1] = weight[0];
+    for (int i = 2; i <= nloop; ++i) tmp[i] = __fadd_rn(weight[i - 1], tmp[i - 1]);
+    for (int i = 0; i < ng; ++i) {
+        k_g[i] = 0.0f;
+        dkdt[i] = 0.0f;
+    }
+    int ig = 1;
+    float sum = 0.0f;
+    for (int I = 1; I <= nloop; ++I) {
+        const float c = cont[I - 1], dc = dcont[I - 1], w = weight[I - 1];
+        if (ig <= ng && tmp[I] <= g_ord[ig]) {
+            k_g[ig - 1] = __fadd_rn(k_g[ig - 1], __fmul_rn(c, w));
+            dkdt[ig - 1] = __fadd_rn(dkdt[ig - 1], __fmul_rn(dc, w));
+            sum = __fadd_rn(sum, w);
+        } else {
+            if (ig > ng) continue;      // the reference writes past NG here; those slots are never read
+            const float frac = __fdiv_rn(__fsub_rn(g_ord[ig], tmp[I - 1]), __fsub_rn(tmp[I], tmp[I - 1]));
+            k_g[ig - 1] = __fadd_rn(k_g[ig - 1], __fmul_rn(__fmul_rn(frac, c), w));
+            dkdt[ig - 1] = __fadd_rn(dkdt[ig - 1], __fmul_rn(__fmul_rn(frac, dc), w));
+            sum = __fadd_rn(sum, __fmul_rn(frac, w));
+            k_g[ig - 1] = __fdiv_rn(k_g[ig - 1], sum);
+            dkdt[ig - 1] = __fdiv_rn(dkdt[ig - 1], sum);
+            ig = ig + 1;
+            if (ig <= ng) {
+                const float rest = __fsub_rn(1.0f, frac);
+                sum = __fmul_rn(rest, w);
+                k_g[ig - 1] = __fmul_rn(__fmul_rn(rest, c), w);
+                dkdt[ig - 1] = __fmul_rn(__fmul_rn(rest, dc), w);
+            }
+        }
+    }
+    if (ig == ng) {
+        k_g[ig - 1] = __fdiv_rn(k_g[ig - 1], sum);
+        dkdt[ig - 1] = __fdiv_rn(dkdt[ig - 1], sum);
+    }
+}
+
+// linear bilinear interpolation of one g of one table slice (no logarithms:
+// the non-coincident branch of get_kg.f:396-420)
+__device__ __forceinline__ void interp_lin(const float* t, const LayerDev& L, int g, float& X, float& DXDT) {
+    const float Y1 = __ldg(t + L.ioff[0] + g), Y2 = __ldg(t + L.ioff[1] + g);
+    const float Y3 = __ldg(t + L.ioff[2] + g), Y4 = __ldg(t + L.ioff[3] + g);
+    const float U = L.u, V = L.v;
+    const float a = __fsub_rn(1.0f, V), b = __fsub_rn(1.0f, U);
+    X = __fmul_rn(__fmul_rn(a, b), Y1);
+    X = __fadd_rn(X, __fmul_rn(__fmul_rn(V, b), Y2));
+    X = __fadd_rn(X, __fmul_rn(__fmul_rn(V, U), Y3));
+    X = __fadd_rn(X, __fmul_rn(__fmul_rn(a, U), Y4));
+    float D = -__fmul_rn(a, Y1);
+    D = __fsub_rn(D, __fmul_rn(V, Y2));
+    D = __fadd_rn(D, __fmul_rn(V, Y3));
+    D = __fadd_rn(D, __fmul_rn(a, Y4));
+    DXDT = __fmul_rn(D, L.dudt);
+}
+
+// get_kg for a wavenumber between two table points (get_kg.f:380-438):
+// 2 NG linearly interpolated values, weighted (1 - w2) delg and w2 delg,
+// rank-rebinned by rankk on lane 0.  scr: per-warp shared scratch of at least
+// 8 * kMaxNg floats + 2 * kMaxNg shorts.  Called by the whole warp.
+__device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w2, const LayerDev& L, int lane, float* scr,
+                               float& k, float& dk) {
+    const int ng = B.ng;
+    float* cont = scr;
+    float* dcont = scr + 2 * kMaxNg;
+    float* fac = scr + 4 * kMaxNg;
+    float* tmp = scr + 6 * kMaxNg;                  // 2 ng + 1 entries
+    float* kg = scr + 8 * kMaxNg + 2;
+    float* dkg = kg + kMaxNg;
+    unsigned short* ico = (unsigned short*)(dkg + kMaxNg);
+    k = 0.0f;
+    dk = 0.0f;
+    if (slice < 0) return;
+    if (lane < ng) {
+        const int64_t step = (int64_t)B.np * B.nt * ng;
+        const float w1 = __fsub_rn(1.0f, w2);
+        for (int loop = 0; loop < 2; ++loop) {
+            float X, D;
+            interp_lin(B.ktab_raw + slice + loop * step, L, lane, X, D);
+            cont[loop * ng + lane] = X;
+            dcont[loop * ng + lane] = D;
+            fac[loop * ng + lane] = __fmul_rn(B.delg[lane], loop ? w2 : w1);
+        }
+    }
+    __syncwarp();
+    if (lane == 0) rankk_lane(ng, B.delg, 2 * ng, cont, dcont, fac, ico, tmp, kg, dkg);
+    __syncwarp();
+    if (lane < ng) {
+        k = kg[lane];
+        dk = dkg[lane];
+        if (k != k) k = 1e-37f;
+        if (dk != dk) dk = 1e-37f;
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, const LayerDev& L, int lane,
                                             float& k, float& dk) {
     k = 0.0f;
@@ -842,6 +955,27 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
         const WaveDev W = B.wave[iw_glob];
         const int nsw = S.nsw, ncol = S.ncol;
 
+        // ---------------- stage A0: non-coincident gases -----------------
+        // k-distributions of gases whose wavenumber falls between two table
+        // points (rankk on lane 0), parked per (layer, gas) in the slot for
+        // stage A; each warp handles the layers it takes in stage A
+        if (B.wg_w2) {
+            const float* w2s = B.wg_w2 + S.wg_off + (int64_t)iw * S.ngas;
+            const int64_t* slices = B.wg_slice + S.wg_off + (int64_t)iw * S.ngas;
+            for (int l = warp; l < S.nlayer; l += kWarps) {
+                const LayerDev L = B.lay[S.lay_off + l];
+                float* ncw = tau_s + B.nc_off + ((int64_t)l * S.ngas) * kMaxNg * 2;
+                for (int g = 0; g < S.ngas; ++g)
+                    if (w2s[g] >= 0.0f) {
+                        float kv, dv;
+                        get_kg_lane_nc(B, slices[g], w2s[g], L, lane, (float*)wp.bufA, kv, dv);
+                        if (lane < ng) {
+                            ncw[(g * kMaxNg + lane) * 2] = kv;
+                            ncw[(g * kMaxNg + lane) * 2 + 1] = dv;
+                        }
+                    }
+            }
+        }
         // ---------------- stage A: layers --------------------------------
         for (int l = warp; l < S.nlayer; l += kWarps) {
             const int64_t il_glob = S.lay_off + l;
@@ -850,12 +984,22 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
             const float taucon = continuum(B, S, L, W, iw_glob, il_glob, lane, dtc);
             const float* amo = B.amo + S.lg_off + (int64_t)l * S.ngas;
             const int64_t* slices = B.wg_slice + S.wg_off + (int64_t)iw * S.ngas;
+            const float* w2s = B.wg_w2 ? B.wg_w2 + S.wg_off + (int64_t)iw * S.ngas : nullptr;
+            const float* ncw = w2s ? tau_s + B.nc_off + ((int64_t)l * S.ngas) * kMaxNg * 2 : nullptr;
+            auto get_kg = [&](int g, float& kv, float& dv) {
+                if (w2s && w2s[g] >= 0.0f) {
+                    kv = lane < ng ? ncw[(g * kMaxNg + lane) * 2] : 0.0f;
+                    dv = lane < ng ? ncw[(g * kMaxNg + lane) * 2 + 1] : 0.0f;
+                } else {
+                    get_kg_lane(B, slices[g], L, lane, kv, dv);
+                }
+            };
             float* colP = colA;
             float* colN = colB;
             float kgv;
             if (S.ngas == 1) {
                 float k0, d0;
-                get_kg_lane(B, slices[0], L, lane, k0, d0);
+                get_kg(0, k0, d0);
                 const float a0 = amo[0];
                 kgv = __fmul_rn(k0, a0);
                 if (lane < ng)
@@ -864,12 +1008,12 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                 float* t = colP; colP = colN; colN = t;
             } else {
                 float k1v, d1v;
-                get_kg_lane(B, slices[0], L, lane, k1v, d1v);
+                get_kg(0, k1v, d1v);
                 kgv = 0.0f;
                 for (int ig = 1; ig < S.ngas; ++ig) {
                     const bool first = ig == 1;
                     float k2v, d2v;
-                    get_kg_lane(B, slices[ig], L, lane, k2v, d2v);
+                    get_kg(ig, k2v, d2v);
                     const float a2 = amo[ig];
                     const float a1 = first ? amo[0] : 1.0f;
                     const float k1e = first ? k1v : kgv;

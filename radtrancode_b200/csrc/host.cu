@@ -333,6 +333,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         for (int k = 0; k < a.ngas; ++k) {
             const int itab = a.ktab[k];
             int64_t slice = -1;
+            float w2 = -1.0f;                  // < 0: coincident wavenumber
             if (itab >= 0) {
                 const float vmin = c->vmin[itab], delv = c->delv[itab];
                 if (!(delv > 0.0f)) return fail(c, RTB_ERR_UNSUPPORTED, "irregular k-table grid (delv <= 0)");
@@ -342,15 +343,21 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
                 const float tmp = vmin + delv * (float)n1;
                 const float frac = std::fabs((float)((double)vwave - (double)tmp));
                 const bool coinc = frac < eps;
-                if (!coinc)
-                    return fail(c, RTB_ERR_UNSUPPORTED,
-                                "wavenumber %g is not on the k-table grid (non-coincident branch)", vwave);
-                if (n1 < 0 || n1 >= c->nbin[itab])
+                // between two table points: weight of the upper one (get_kg.f:380-395)
+                if (!coinc) {
+                    w2 = (vwave - tmp) / delv;
+                    if (w2 > 1.0f) w2 = 1.0f;
+                    if (w2 < 0.0f) w2 = 0.0f;
+                    st.any_noncoinc = true;
+                }
+                const int need = coinc ? n1 : n1 + 1;
+                if (n1 < 0 || need >= c->nbin[itab])
                     return fail(c, RTB_ERR_RANGE, "wavenumber %g outside k-table %d", vwave, itab);
                 if (c->nonzero[itab][n1])
                     slice = c->tab_off[itab] + (int64_t)n1 * np * nt * ng;
             }
             st.wg_slice.push_back(slice);
+            st.wg_w2.push_back(w2);
         }
         for (int k = 0; k < a.ncont; ++k) st.xsec.push_back(a.xsec_ext[k + (size_t)a.ncont * iw]);
     }
@@ -436,6 +443,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     st.ncol_max = std::max(st.ncol_max, S.ncol);
     st.nlmax_max = std::max(st.nlmax_max, nlmax);
     st.npath_max = std::max(st.npath_max, a.npath);
+    st.ngas_max = std::max(st.ngas_max, a.ngas);
     return RTB_OK;
 }
 
@@ -490,6 +498,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     const size_t i_amo = add(st.amo.data(), bytes_of(st.amo));
     const size_t i_wave = add(st.wave.data(), bytes_of(st.wave));
     const size_t i_wg = add(st.wg_slice.data(), bytes_of(st.wg_slice));
+    const size_t i_w2 = add(st.wg_w2.data(), st.any_noncoinc ? bytes_of(st.wg_w2) : 0);
     const size_t i_xsec = add(st.xsec.data(), bytes_of(st.xsec));
     const size_t i_cont = add(st.cont.data(), bytes_of(st.cont));
     const size_t i_pl = add(st.p_layinc.data(), bytes_of(st.p_layinc));
@@ -522,6 +531,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     B.amo = (const float*)dp(i_amo);
     B.wave = (const WaveDev*)dp(i_wave);
     B.wg_slice = (const int64_t*)dp(i_wg);
+    B.wg_w2 = st.any_noncoinc ? (const float*)dp(i_w2) : nullptr;
     B.xsec = (const float*)dp(i_xsec);
     B.cont = (const float*)dp(i_cont);
     B.p_layinc = (const int*)dp(i_pl);
@@ -570,6 +580,8 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     // one scratch slot per CTA: tau[Lmax][ng] + dtau[Lmax][nsw][ng]
     B.cell_Lmax = st.Lmax;
     B.cell_slot = (int64_t)st.Lmax * c->ng * (1 + st.nsw_max);
+    B.nc_off = B.cell_slot;
+    if (st.any_noncoinc) B.cell_slot += (int64_t)st.Lmax * st.ngas_max * kMaxNg * 2;
     B.cell_slot = (B.cell_slot + 63) & ~(int64_t)63;
     CUDA_TRY(c, c->d_cells.ensure((size_t)grid * B.cell_slot * sizeof(float)));
     B.cell_scratch = (float*)c->d_cells.p;

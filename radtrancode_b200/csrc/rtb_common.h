@@ -82,6 +82,7 @@ struct BatchDev {
     const float* amo;            // [.. nlayer][ngas] amount*1e-20
     const WaveDev* wave;
     const int64_t* wg_slice;     // [.. nwave][ngas] element offset of the table slice, -1 = zero
+    const float* wg_w2;          // [.. nwave][ngas] non-coincident weight of slice+1 (< 0: coincident); may be null
     const float* xsec;           // [.. nwave][ncont]
     const float* cont;           // [.. nlayer][ncont]
     const int* p_layinc;         // [.. npath][nlmax] 0-based layer
@@ -101,6 +102,8 @@ struct BatchDev {
     float* cell_scratch;
     int64_t cell_slot;             // floats per slot
     int cell_Lmax;                 // layers per slot
+    int64_t nc_off;                // floats from the slot start to the non-coincident k area
+                                   // [layer][gas][kMaxNg][2] (k, dk/dT), when wg_w2 is set
     // outputs
     float* calcout;
     float* gradients;

@@ -152,8 +152,8 @@ def test_unsupported_options_raise(ctx):
     with pytest.raises(cirsradg.RtbError, match="UNSUPPORTED"):
         ctx.cirsrtfg_wave(j)
     j = copy.deepcopy(job)
-    j.vwave = j.vwave + np.float32(0.7)        # between table wavenumbers
-    with pytest.raises(cirsradg.RtbError, match="UNSUPPORTED"):
+    j.vwave = j.vwave + np.float32(0.7)        # the last one needs a table point past the grid (get_kg.f:210-226)
+    with pytest.raises(cirsradg.RtbError, match="RANGE"):
         ctx.cirsrtfg_wave(j)
     j = copy.deepcopy(job)
     j.vem = np.array([1250.0, 1300.0], np.float32)   # interpem.f range error
@@ -186,3 +186,37 @@ def test_full_size_config2_properties(ctx):
     assert np.array_equal(np.concatenate([ca, cb]), c)
     G = g.reshape(job.nv, -1)
     assert np.array_equal(np.concatenate([ga.reshape(job.nv, -1), gb.reshape(job.nv, -1)], axis=1), G)
+
+
+def _off_grid(job, kt, shift):
+    """The job moved between the k-table points: vwave = vmin + delv (i + shift)."""
+    j = copy.deepcopy(job)
+    j.vwave = (kt.vmin[0] + kt.delv[0] * (np.arange(j.nwave) + shift)).astype(np.float32)
+    return j
+
+
+@pytest.mark.parametrize("shift", [0.37, 0.93])
+def test_noncoincident_wavenumbers(ctx, oracle, shift):
+    """get_kg.f:380-438 + rankk.f: two table points weighted and rank-rebinned.
+    Radiance and Jacobian within tolerance of the FP64 oracle; the g-bins of
+    the overlap passes built on those k values bit-exact with the mixed
+    oracle."""
+    kt, cia, job = synth.config2(nwave=12, nlayer=40, nbin=16)
+    j = _off_grid(job, kt, shift)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_debug(True)
+    try:
+        c, g, gt = ctx.cirsrtfg_wave(j)
+        perm, split = ctx.debug_bins(j)
+    finally:
+        ctx.set_debug(False)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, j.nv) <= JAC_TOL
+    (cm, gm, _), (operm, osplit, _) = oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_MIXED, debug=True)
+    assert np.array_equal(assignment(perm, split, kt.ng), assignment(operm, osplit, kt.ng))
+    assert np.array_equal(split, osplit)
+    # the coincident spectrum differs: the branch was taken
+    c0, _, _ = ctx.cirsrtfg_wave(job)
+    assert not np.array_equal(c0, c)

@@ -97,6 +97,13 @@ __device__ __noinline__ void heapsort_sort2g(int n, float* ra0, unsigned short* 
 
 __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 
+// bytes of one element buffer: NG^2 64-bit words, or the gradient-column
+// scratch of sort_pass (U/V tables 4 NG float4, first/last partials
+// 2 x kMaxCols x 32 floats, inside-chunk bins kMaxCols x NG floats, 2 x 32
+// shorts), whichever is larger, for NG up to 22
+constexpr int kNgDev = 22;
+constexpr int kGradScratch = 64 * kNgDev + 8 * kMaxCols * 32 + 4 * kMaxCols * kNgDev + 128;
+constexpr int kElemBuf = ((8 * kN > kGradScratch ? 8 * kN : kGradScratch) + 15) & ~15;
 // per-warp scratch sub-offsets (bytes).  bufA holds the sorted (key, element)
 // words of a pass; bufB is the merge's second buffer, then the per-bin row and
 // column weight sums R[b][i], C[b][j] (2*ng*ng floats <= 4096 B for ng <= 22).
@@ -107,10 +114,10 @@ __host__ __device__ inline WarpOff warp_off(int ncol) {
     WarpOff w;
     int o = 0;
     const int nc = ncol > 0 ? ncol : 1;
-    // 8 B words; the free buffer also holds R, C (2*ng*ng floats) and the
-    // element bins (ng*ng bytes): 9 B per element
-    w.bufA = o; o += align16(9 * kN);
-    w.bufB = o; o += align16(9 * kN);
+    // 8 B words (the element buffers); the free one also holds the FP64
+    // cumulative weights and, later, the gradient-column tables and partials
+    w.bufA = o; o += kElemBuf;
+    w.bufB = o; o += kElemBuf;
     w.splitfrac = o; o += 8 * kMaxNg;
     w.k1 = o; o += 4 * kMaxNg;
     w.k2 = o; o += 4 * kMaxNg;
@@ -753,7 +760,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             }
             const bool closes = bb < c_last;
             const int pend = closes ? wp.splitpos[bb] : nloop;
-#pragma unroll 4
+#pragma unroll 1
             for (; p < pend; ++p) {
                 const unsigned long long word = A[p];
                 const unsigned q = (unsigned)word & 0xffffu;
@@ -783,87 +790,127 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     }
     // ---- gradient columns ----------------------------------------------------
     // They feed the Jacobian alone (never a sort key), so they need not follow
-    // the reference's summation order.  Each column is linear in the element
-    // weights: sum over bin b of v(i,j) w f = sum_i u(i) R[b][i] + sum_j v(j) C[b][j]
-    // with R[b][i] / C[b][j] the weight of row i / column j falling in bin b.
-    // Lane x walks row x and column x in key order (bins are monotone along
-    // both), flushing one partial sum per bin: deterministic, no atomics.
-    const int ncol = P.ncol;
-    float* R = (float*)gd;                   // gd is free again
-    float* Cw = R + ng * ng;
-    unsigned char* eb = (unsigned char*)(Cw + ng * ng);   // bin of element e (0x80: split)
-    for (int t = lane; t < 2 * ng * ng; t += 32) R[t] = 0.0f;
+    // the reference's summation order.  Every column is v_c(i, j) = U[i][c] +
+    // V[j][c] (T: dk1(i)[a1] + dk2(j) a2; earlier gas: u(i); added gas: k2(j)).
+    // Bin b of column c is the sum over its sorted positions of w * v_c (split
+    // elements shared f : 1 - f).  Each lane sums its chunk of positions per
+    // bin: the first and the last bin of the chunk as partials, bins wholly
+    // inside directly; one lane per bin then adds the partials of the lanes it
+    // spans, in lane order (deterministic, no atomics).
     {
-        // bins of this lane's positions
+        const int ncol = P.ncol;
+        float4* UV = (float4*)gd;                  // U rows [ng][2 float4], then V rows [ng][2 float4]
+        float* Fp = (float*)(UV + 4 * ng);         // [kMaxCols][32] first-bin partial
+        float* Lp = Fp + kMaxCols * 32;            // [kMaxCols][32] last-bin partial
+        float* Mid = Lp + kMaxCols * 32;           // [kMaxCols][ng] bins inside one chunk
+        short* B0 = (short*)(Mid + kMaxCols * ng); // [32] first bin of each lane's chunk
+        short* BL = B0 + 32;                       // [32] last bin of each lane's chunk
+        if (lane < ng) {
+            const int x = lane;
+            float u[kMaxCols], v[kMaxCols];
+#pragma unroll
+            for (int c = 0; c < kMaxCols; ++c) {
+                u[c] = 0.0f;
+                v[c] = 0.0f;
+                if (c < ncol) {
+                    const int gcol = S.col_gas[c];
+                    if (gcol == S.ngas) {                  // temperature: dk1(i)[*a1] + dk2(j)*a2
+                        u[c] = P.first ? wp.dk1[x] * P.a1 : wp.dk1[x];
+                        v[c] = wp.dk2[x] * P.a2;
+                    } else if (gcol == P.igas) {           // the gas being added: k2(j)
+                        v[c] = wp.k2[x];
+                    } else if (gcol < P.igas) {            // an earlier gas
+                        if (!P.first) u[c] = colP[c * kMaxNg + x];
+                        else if (gcol == 0) u[c] = wp.k1[x];
+                    }
+                }
+            }
+            UV[2 * x] = make_float4(u[0], u[1], u[2], u[3]);
+            UV[2 * x + 1] = make_float4(u[4], u[5], u[6], u[7]);
+            UV[2 * ng + 2 * x] = make_float4(v[0], v[1], v[2], v[3]);
+            UV[2 * ng + 2 * x + 1] = make_float4(v[4], v[5], v[6], v[7]);
+        }
+        __syncwarp();
         int b = 0;
-        while (b < ng && wp.splitpos[b] >= 0 && wp.splitpos[b] < p0) ++b;
+        {
+            int lo = 0, hi = c_last;                // first boundary at or after p0
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (wp.splitpos[mid] < p0) lo = mid + 1; else hi = mid;
+            }
+            b = lo;
+        }
+        const int b0 = b;
+        int nsp = b < c_last ? wp.splitpos[b] : nloop;
+        float acc[kMaxCols], first[kMaxCols];
+        bool in_first = true;
+#pragma unroll
+        for (int c = 0; c < kMaxCols; ++c) {
+            acc[c] = 0.0f;
+            first[c] = 0.0f;
+        }
+#pragma unroll 1
         for (int p = p0; p < p1; ++p) {
             const unsigned q = (unsigned)A[p] & 0xffffu;
-            const bool split = b < ng && wp.splitpos[b] == p;
-            eb[(q >> 5) * ng + (q & 31)] = (unsigned char)(b | (split ? 0x80 : 0));
-            if (split) ++b;
-        }
-    }
-    __syncwarp();
-    if (lane < ng) {
-        const int x = lane;
-        for (int pass = 0; pass < 2; ++pass) {      // 0: row x -> R, 1: column x -> C
-            float* dst = pass == 0 ? R : Cw;
-            int cur = -1;
-            float acc = 0.0f;
-#pragma unroll 4
-            for (int y = 0; y < ng; ++y) {
-                const int e = pass == 0 ? x * ng + y : y * ng + x;
-                const unsigned char code = eb[e];
-                const int b = code & 0x7f;
-                const float w = delg[x] * delg[y];
-                if (b != cur) {
-                    if (cur >= 0 && cur < ng) dst[cur * ng + x] += acc;
-                    cur = b;
-                    acc = 0.0f;
+            const int i = q >> 5, j = q & 31;
+            const float w = __fmul_rn(delg[i], delg[j]);
+            const float4 u0 = UV[2 * i], u1 = UV[2 * i + 1];
+            const float4 v0 = UV[2 * ng + 2 * j], v1 = UV[2 * ng + 2 * j + 1];
+            const float val[kMaxCols] = {w * (u0.x + v0.x), w * (u0.y + v0.y), w * (u0.z + v0.z),
+                                         w * (u0.w + v0.w), w * (u1.x + v1.x), w * (u1.y + v1.y),
+                                         w * (u1.z + v1.z), w * (u1.w + v1.w)};
+            if (p == nsp) {                         // the split element closes bin b
+                const float f = (float)wp.splitfrac[b];
+#pragma unroll
+                for (int c = 0; c < kMaxCols; ++c) {
+                    const float t = fmaf(f, val[c], acc[c]);
+                    if (in_first) first[c] = t;
+                    else if (c < ncol) Mid[c * ng + b] = t;
+                    acc[c] = (1.0f - f) * val[c];
                 }
-                if (code & 0x80) {
-                    const float f = (float)wp.splitfrac[b];
-                    dst[b * ng + x] += acc + f * w;
-                    cur = b + 1;
-                    acc = (1.0f - f) * w;
-                } else {
-                    acc += w;
+                in_first = false;
+                ++b;
+                nsp = b < c_last ? wp.splitpos[b] : nloop;
+            } else {
+#pragma unroll
+                for (int c = 0; c < kMaxCols; ++c) acc[c] += val[c];
+            }
+        }
+        if (p0 < p1) {
+#pragma unroll
+            for (int c = 0; c < kMaxCols; ++c)
+                if (c < ncol) {
+                    Fp[c * 32 + lane] = in_first ? acc[c] : first[c];
+                    Lp[c * 32 + lane] = in_first ? 0.0f : acc[c];
+                }
+        }
+        B0[lane] = (short)(p0 < p1 ? b0 : -1);
+        BL[lane] = (short)(p0 < p1 ? b : -1);
+        __syncwarp();
+        if (lane < ng) {
+            const int bb = lane;
+            const float nf = wp.normf[bb];
+            float tot[kMaxCols];
+#pragma unroll
+            for (int c = 0; c < kMaxCols; ++c) tot[c] = 0.0f;
+            if (nf != 0.0f && bb <= c_last) {
+                const int sp0 = bb == 0 ? 0 : wp.splitpos[bb - 1];
+                const int sp1 = bb < c_last ? wp.splitpos[bb] : nloop - 1;
+                const int L0 = sp0 / ch, L1 = sp1 / ch;
+#pragma unroll 1
+                for (int L = L0; L <= L1; ++L) {
+                    const int lb0 = B0[L], lbl = BL[L];
+                    const float* src = lb0 == bb ? Fp + L : (lbl == bb ? Lp + L : Mid + bb);
+                    const int stride = (lb0 == bb || lbl == bb) ? 32 : ng;
+#pragma unroll
+                    for (int c = 0; c < kMaxCols; ++c)
+                        if (c < ncol) tot[c] += src[c * stride];
                 }
             }
-            if (cur >= 0 && cur < ng) dst[cur * ng + x] += acc;
+#pragma unroll
+            for (int c = 0; c < kMaxCols; ++c)
+                if (c < ncol) colN[c * kMaxNg + bb] = nf != 0.0f ? tot[c] / nf : 0.0f;
         }
-    }
-    __syncwarp();
-    for (int task = lane; task < ncol * ng; task += 32) {
-        const int c = task / ng, bb = task - c * ng;
-        const float nf = wp.normf[bb];
-        const int gcol = S.col_gas[c];
-        float acc = 0.0f;
-        if (nf != 0.0f) {
-            const float* Rb = R + bb * ng;
-            const float* Cb = Cw + bb * ng;
-            if (gcol == S.ngas) {                 // temperature: dk1(i)[*a1] + dk2(j)*a2
-                float su = 0.0f, sv = 0.0f;
-#pragma unroll 4
-                for (int t = 0; t < ng; ++t) {
-                    su = fmaf(wp.dk1[t], Rb[t], su);
-                    sv = fmaf(wp.dk2[t], Cb[t], sv);
-                }
-                acc = (P.first ? su * P.a1 : su) + sv * P.a2;
-            } else if (gcol == P.igas) {          // the gas being added: k2(j)
-#pragma unroll 4
-                for (int t = 0; t < ng; ++t) acc = fmaf(wp.k2[t], Cb[t], acc);
-            } else if (gcol < P.igas) {           // an earlier gas
-                if (!P.first || gcol == 0) {
-                    const float* u = P.first ? wp.k1 : colP + c * kMaxNg;
-#pragma unroll 4
-                    for (int t = 0; t < ng; ++t) acc = fmaf(u[t], Rb[t], acc);
-                }
-            }
-            acc = acc / nf;
-        }
-        colN[c * kMaxNg + bb] = acc;
     }
     __syncwarp();
 }

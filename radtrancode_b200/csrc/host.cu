@@ -15,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "context.h"
@@ -24,12 +25,16 @@ using namespace rtb;
 namespace rtb {
 
 int fail(rtb_context* c, int code, const char* fmt, ...) {
+    static std::mutex mu;   // batch packing reports from several host threads
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
     vsnprintf(buf, sizeof buf, fmt, ap);
     va_end(ap);
-    if (c) c->err = buf;
+    if (c) {
+        std::lock_guard<std::mutex> lk(mu);
+        c->err = buf;
+    }
     return code;
 }
 
@@ -448,6 +453,84 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
 }
 
 template <class T>
+void append_vec(std::vector<T>& d, const std::vector<T>& s) {
+    d.insert(d.end(), s.begin(), s.end());
+}
+
+// concatenate a privately packed staging onto dst, rebasing its offsets
+void append_staging(Staging& dst, const Staging& src) {
+    const int64_t lay = dst.lay.size(), amo = dst.amo.size(), cont = dst.cont.size(), wave = dst.wave.size();
+    const int64_t wg = dst.wg_slice.size(), xsec = dst.xsec.size(), path = dst.p_layinc.size();
+    const int64_t colptr = dst.map_colptr.size(), rows = dst.map_row.size(), items = dst.item_start.back();
+    for (SpecDev S : src.spec) {
+        S.lay_off += lay;
+        S.lg_off += amo;
+        S.lc_off += cont;
+        S.wave_off += wave;
+        S.wg_off += wg;
+        S.wc_off += xsec;
+        S.path_off += path;
+        S.map_off += colptr;
+        S.out_off += dst.n_out;
+        S.jac_off += dst.n_jac;
+        dst.spec.push_back(S);
+    }
+    for (size_t i = 1; i < src.item_start.size(); ++i) dst.item_start.push_back(src.item_start[i] + items);
+    append_vec(dst.lay, src.lay);
+    append_vec(dst.amo, src.amo);
+    append_vec(dst.wave, src.wave);
+    append_vec(dst.wg_slice, src.wg_slice);
+    append_vec(dst.wg_w2, src.wg_w2);
+    append_vec(dst.xsec, src.xsec);
+    append_vec(dst.cont, src.cont);
+    append_vec(dst.p_layinc, src.p_layinc);
+    append_vec(dst.p_scale, src.p_scale);
+    append_vec(dst.p_emtemp, src.p_emtemp);
+    append_vec(dst.map_row, src.map_row);
+    append_vec(dst.map_val, src.map_val);
+    for (int v : src.map_colptr) dst.map_colptr.push_back(v + (int)rows);
+    dst.Lmax = std::max(dst.Lmax, src.Lmax);
+    dst.nsw_max = std::max(dst.nsw_max, src.nsw_max);
+    dst.ncol_max = std::max(dst.ncol_max, src.ncol_max);
+    dst.nlmax_max = std::max(dst.nlmax_max, src.nlmax_max);
+    dst.npath_max = std::max(dst.npath_max, src.npath_max);
+    dst.ngas_max = std::max(dst.ngas_max, src.ngas_max);
+    dst.any_noncoinc = dst.any_noncoinc || src.any_noncoinc;
+    dst.n_out += src.n_out;
+    dst.n_jac += src.n_jac;
+}
+
+// pack a batch: contiguous ranges of spectra on host threads, each into its
+// own staging, concatenated in order (the same result as packing one by one)
+int pack_batch(rtb_context* c, int nspec, const rtb_atm* atms, Staging& st) {
+    st.item_start.assign(1, 0);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nthr = std::min<int>(std::min<unsigned>(hw, 32u), nspec / 4);
+    if (nthr <= 1) {
+        for (int s = 0; s < nspec; ++s) {
+            const int r = pack_spectrum(c, atms[s], st);
+            if (r) return r;
+        }
+        return RTB_OK;
+    }
+    std::vector<Staging> part(nthr);
+    std::vector<int> status(nthr, RTB_OK);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthr; ++t)
+        th.emplace_back([&, t]() {
+            const int s0 = (int)((int64_t)nspec * t / nthr), s1 = (int)((int64_t)nspec * (t + 1) / nthr);
+            Staging& p = part[t];
+            p.item_start.assign(1, 0);
+            for (int s = s0; s < s1 && status[t] == RTB_OK; ++s) status[t] = pack_spectrum(c, atms[s], p);
+        });
+    for (auto& x : th) x.join();
+    for (int t = 0; t < nthr; ++t)
+        if (status[t]) return status[t];
+    for (int t = 0; t < nthr; ++t) append_staging(st, part[t]);
+    return RTB_OK;
+}
+
+template <class T>
 size_t bytes_of(const std::vector<T>& v) {
     return v.size() * sizeof(T);
 }
@@ -462,11 +545,8 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     CUDA_TRY(c, cudaSetDevice(c->device));
     c->prepared = 0;
     Staging st;
-    st.item_start.push_back(0);
-    for (int s = 0; s < nspec; ++s) {
-        const int r = pack_spectrum(c, atms[s], st);
-        if (r) return r;
-    }
+    const int r0 = pack_batch(c, nspec, atms, st);
+    if (r0) return r0;
     const int smem = fwd_smem_bytes(c->ng, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max);
     int smem_max = 0;
     CUDA_TRY(c, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));

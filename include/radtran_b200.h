@@ -163,6 +163,22 @@ int rtb_cirsrtfg_wave_batch(rtb_context* ctx, int nspec, const rtb_atm* atms,
                             float* const* calcout, float* const* gradients,
                             float* const* gradtsurf);
 
+/* Per-wavenumber compatibility form of cirsradg_wave (radtran/cirsradg/
+ * cirsradg_wave.f:1-5, outputs :1240-1267) for A/B checks against the
+ * reference one wavenumber at a time: the layer and path arrays as for
+ * rtb_cirsrtfg_wave with atm->nwave == 1 (xmap, dte, dam, dco, npro and nv are
+ * ignored), the active parameters isw[nsw] (0-based parameter ids: gases
+ * 0..ngas-1, temperature ngas, dust ngas+1..; increasing, nsw <= 8) and:
+ *   output[npath]           radiance of every path
+ *   gtsurf[npath]           d output / d tsurf (may be NULL)
+ *   doutputdq(ld_pat, ld_lay, ld_param)  d output(ipath) / d q(layer j of the
+ *                           path, parameter k), zero outside isw, as the
+ *                           reference's doutputdq(maxpat, maxlay, ...).
+ * One wavenumber per call keeps the GPU mostly idle; rtb_cirsrtfg_wave is
+ * the form to use for whole spectra. */
+int rtb_cirsradg_wave(rtb_context* ctx, const rtb_atm* atm, int nsw, const int* isw, float* output,
+                      float* gtsurf, float* doutputdq, int ld_pat, int ld_lay, int ld_param);
+
 /* The same call split in three, for callers that keep a batch resident on
  * the device and replay it (a retrieval re-running its forward model, a
  * benchmark timing the kernel alone):
@@ -294,6 +310,23 @@ int rtb_get_newton_stats(const rtb_context* ctx, rtb_newton_stats* out);
 int rtb_calc_phiret_batch(rtb_context* ctx, int nret, int nx, int ny, const float* y, const float* yn,
                           const double* sei, const float* xn, const float* xa, const double* sai,
                           float* phi, float* chisq);
+
+/* The reference's own interface for one retrieval, on the device in FP64:
+ * calc_gain_matrix (nemesis/calc_gain_matrix.f:1-163, the nx < ny branch) with
+ * a diagonal Se:
+ *   kk   REAL kk(ldy, nx), column-major (Fortran kk_in): K(i, j) = dy_i / dx_j
+ *   sxi  DOUBLE sxi(ldx, nx): Sa^-1
+ *   sei  DOUBLE sei(ny): diagonal of Se^-1
+ *   dd   DOUBLE dd(ldx, ny), out: gain matrix D = (K^T Se^-1 K + Sa^-1)^-1 K^T Se^-1
+ *   aa   DOUBLE aa(ldx, nx), out: averaging kernels AA = D K
+ *   nonpd  out, may be NULL: a Cholesky pivot was <= 0 (dcholdc.f:69-84)
+ * and calcnextxn (nemesis/calcnextxn.f:1-109): x_out = x0 + D (y - yn) -
+ * AA (x0 - xn) with D, AA as returned above.  Both run every product on the
+ * device; rtb_newton_step_batch is the batched form that never forms D. */
+int rtb_calc_gain_matrix(rtb_context* ctx, int nx, int ny, int ldx, int ldy, const float* kk,
+                         const double* sxi, const double* sei, double* dd, double* aa, int* nonpd);
+int rtb_calcnextxn(rtb_context* ctx, int nx, int ny, int ldx, const float* x0, const float* xn,
+                   const float* y, const float* yn, const double* dd, const double* aa, float* x_out);
 
 /* dinvertm (radtran/matrices/dinvertm.f jmod=2): inverse of nret symmetric
  * positive-definite n x n matrices (row-major, a[r*n*n]) by an FP64 Cholesky

@@ -183,6 +183,35 @@ def retrieve(kt, cia, case, kiter=10, phlimit=0.1, dchisq_stop=0.0, precision=OR
     return res, trace
 
 
+def gain_matrix(kk, sei, sai):
+    """calc_gain_matrix (diagonal Se): kk [nx, ny] (Fortran kk(ny, nx)).
+    Returns (dd [nx, ny], aa [nx, nx]) as Fortran-ordered float64 arrays."""
+    L = lib()
+    kk = np.ascontiguousarray(kk, np.float32)
+    nx, ny = kk.shape
+    sai = np.asfortranarray(sai, np.float64)
+    sei = np.ascontiguousarray(sei, np.float64)
+    dd = np.zeros((nx, ny), order="F")
+    aa = np.zeros((nx, nx), order="F")
+    dp = C.POINTER(C.c_double)
+    L.orc_calc_gain_matrix_diag(nx, ny, nx, ny, _abi.fptr(kk), sai.ctypes.data_as(dp), sei.ctypes.data_as(dp),
+                                dd.ctypes.data_as(dp), aa.ctypes.data_as(dp), None)
+    return dd, aa
+
+
+def calcnextxn(xa, xn, y, yn, dd, aa):
+    L = lib()
+    dp = C.POINTER(C.c_double)
+    dd = np.asfortranarray(dd, np.float64)
+    aa = np.asfortranarray(aa, np.float64)
+    nx, ny = dd.shape
+    xa, xn, y, yn = (np.ascontiguousarray(a, np.float32) for a in (xa, xn, y, yn))
+    x_out = np.zeros(nx, np.float32)
+    L.orc_calcnextxn(nx, ny, nx, _abi.fptr(xa), _abi.fptr(xn), _abi.fptr(y), _abi.fptr(yn),
+                     dd.ctypes.data_as(dp), aa.ctypes.data_as(dp), _abi.fptr(x_out))
+    return x_out
+
+
 def newton_step(kk, sei, sai, xa, xn, y, yn):
     """calc_gain_matrix (diagonal Se, dense D and AA) + calcnextxn for one
     retrieval: kk [nx, ny] (Fortran kk(ny, nx)), sei [ny], sai [nx, nx]."""

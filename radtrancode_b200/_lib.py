@@ -96,6 +96,13 @@ def lib() -> C.CDLL:
         L.rtb_server_step.restype = C.c_int
         L.rtb_server_poll.argtypes = [vp, C.c_longlong, ip, C.POINTER(_abi.RtbRetrievalResult)]
         L.rtb_server_poll.restype = C.c_int
+        L.rtb_calc_gain_matrix.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, fp, dp, dp, dp, dp, ip]
+        L.rtb_calc_gain_matrix.restype = C.c_int
+        L.rtb_calcnextxn.argtypes = [vp, C.c_int, C.c_int, C.c_int, fp, fp, fp, fp, dp, dp, fp]
+        L.rtb_calcnextxn.restype = C.c_int
+        L.rtb_cirsradg_wave.argtypes = [vp, C.POINTER(_abi.RtbAtm), C.c_int, ip, fp, fp, fp, C.c_int, C.c_int,
+                                        C.c_int]
+        L.rtb_cirsradg_wave.restype = C.c_int
         p16 = C.POINTER(C.c_int16)
         L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
         L.rtb_get_debug_bins.restype = C.c_int
@@ -111,5 +118,6 @@ EXPORTED = [
     "rtb_set_stream", "rtb_fwd_launch_static", "rtb_set_newton_mode", "rtb_newton_step_batch",
     "rtb_calc_phiret_batch", "rtb_spd_inverse_batch", "rtb_retrieve_batch", "rtb_get_newton_stats",
     "rtb_fwd_set_schedule", "rtb_fwd_autotune", "rtb_fwd_use_graph", "rtb_server_create", "rtb_server_destroy",
-    "rtb_server_submit", "rtb_server_step", "rtb_server_poll",
+    "rtb_server_submit", "rtb_server_step", "rtb_server_poll", "rtb_calc_gain_matrix", "rtb_calcnextxn",
+    "rtb_cirsradg_wave",
 ]

@@ -87,6 +87,20 @@ class Context:
                                               _abi.fptr(gts)))
         return calcout, grads, gts
 
+    def cirsradg_wave(self, job, isw):
+        """rtb_cirsradg_wave on a one-wavenumber job: (output [npath],
+        gtsurf [npath], doutputdq [npath, nlayer, nparam])."""
+        assert job.nwave == 1
+        isw = np.ascontiguousarray(isw, np.int32)
+        npath, nparam = job.npath, job.nparam
+        out = np.zeros(npath, np.float32)
+        gts = np.zeros(npath, np.float32)
+        dq = np.zeros((npath, job.nlayer, nparam), np.float32, order="F")
+        s = job.as_struct()
+        self._check(self._L.rtb_cirsradg_wave(self._h, C.byref(s), len(isw), _abi.iptr(isw), _abi.fptr(out),
+                                              _abi.fptr(gts), _abi.fptr(dq), npath, job.nlayer, nparam))
+        return out, gts, dq
+
     def cirsrtfg_wave_batch(self, jobs, outs=None):
         """Batched forward model: one launch for all jobs.  Returns a list of
         (calcout, gradients, gradtsurf)."""
@@ -180,6 +194,32 @@ class Context:
         s = _abi.RtbNewtonStats()
         self._check(self._L.rtb_get_newton_stats(self._h, C.byref(s)))
         return {"retrievals": s.retrievals, "ms_kernel": s.ms_kernel}
+
+    def calc_gain_matrix(self, kk, sxi, sei):
+        """calc_gain_matrix for one retrieval: kk [nx, ny] (Fortran kk(ny, nx)),
+        sxi [nx, nx] (Sa^-1), sei [ny] (diagonal of Se^-1).  Returns
+        (dd [nx, ny], aa [nx, nx], nonpd)."""
+        kk = np.ascontiguousarray(kk, np.float32)
+        nx, ny = kk.shape
+        sxi = np.asfortranarray(sxi, np.float64)
+        sei = np.ascontiguousarray(sei, np.float64)
+        dd = np.zeros((nx, ny), np.float64, order="F")
+        aa = np.zeros((nx, nx), np.float64, order="F")
+        nonpd = C.c_int()
+        self._check(self._L.rtb_calc_gain_matrix(self._h, nx, ny, nx, ny, _abi.fptr(kk), _abi.dptr(sxi),
+                                                 _abi.dptr(sei), _abi.dptr(dd), _abi.dptr(aa), C.byref(nonpd)))
+        return dd, aa, nonpd.value
+
+    def calcnextxn(self, x0, xn, y, yn, dd, aa):
+        f32 = lambda a: np.ascontiguousarray(a, np.float32)
+        x0, xn, y, yn = f32(x0), f32(xn), f32(y), f32(yn)
+        dd = np.asfortranarray(dd, np.float64)
+        aa = np.asfortranarray(aa, np.float64)
+        nx, ny = dd.shape
+        x_out = np.zeros(nx, np.float32)
+        self._check(self._L.rtb_calcnextxn(self._h, nx, ny, nx, _abi.fptr(x0), _abi.fptr(xn), _abi.fptr(y),
+                                           _abi.fptr(yn), _abi.dptr(dd), _abi.dptr(aa), _abi.fptr(x_out)))
+        return x_out
 
     def calc_phiret_batch(self, y, yn, sei, xn, xa, sai):
         f32 = lambda a: np.ascontiguousarray(a, np.float32)

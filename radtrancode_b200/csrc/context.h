@@ -139,6 +139,7 @@ struct rtb_context {
     size_t in_bytes = 0, out_bytes = 0;
     long long cells = 0;
     rtb::DevBuf d_dbg_perm, d_dbg_split;
+    rtb::DevBuf d_dq;                     // per-path-position derivatives (rtb_cirsradg_wave)
     size_t dbg_perm_n = 0, dbg_split_n = 0;
     rtb_fwd_stats stats{};
     // schedule of the resident batch (rtb_fwd_set_schedule / rtb_fwd_autotune)

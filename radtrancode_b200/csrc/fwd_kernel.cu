@@ -1249,6 +1249,10 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
         for (int p = 0; p < S.npath; ++p) {
             char* ps = region + p * Lo.path_bytes;
             const float* dq = (const float*)(ps + po.dq);
+            if (B.dq_out) {
+                float* o = B.dq_out + ((S.wave_off + iw) * B.dq_npath + p) * B.dq_stride;
+                for (int t = tid; t < S.nlayin[p] * nsw; t += kThreads) o[t] = dq[t];
+            }
             const int* cp = B.map_colptr + S.map_off + (int64_t)p * (S.nv + 1);
             for (int iv = tid; iv < S.nv; iv += kThreads) {
                 float acc = 0.0f;

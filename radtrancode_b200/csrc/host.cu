@@ -907,6 +907,7 @@ void rtb_destroy(rtb_context* c) {
     c->d_dbg_split.release();
     drop_graph(c);
     c->d_order.release();
+    c->d_dq.release();
     c->d_nt32.release();
     c->d_nt64.release();
     c->d_ntsmall.release();
@@ -1099,6 +1100,64 @@ int rtb_fwd_use_graph(rtb_context* c, int on) {
     if (!c) return RTB_ERR_ARG;
     c->use_graph = on ? 1 : 0;
     drop_graph(c);
+    return RTB_OK;
+}
+
+int rtb_cirsradg_wave(rtb_context* c, const rtb_atm* atm, int nsw, const int* isw, float* output, float* gtsurf,
+                      float* doutputdq, int ld_pat, int ld_lay, int ld_param) {
+    if (!c) return RTB_ERR_ARG;
+    if (!atm || atm->nwave != 1 || nsw < 0 || nsw > kMaxSw || (nsw > 0 && !isw) || !output || !doutputdq)
+        return fail(c, RTB_ERR_ARG, "cirsradg_wave: bad arguments (one wavenumber, 0 <= nsw <= %d)", kMaxSw);
+    const rtb_atm& a0 = *atm;
+    const int nparam = a0.ngas + 1 + a0.ncont;
+    if (ld_pat < a0.npath || ld_lay < a0.nlayer || ld_param < nparam)
+        return fail(c, RTB_ERR_ARG, "cirsradg_wave: doutputdq leading dimensions too small");
+    for (int s = 0; s < nsw; ++s)
+        if (isw[s] < 0 || isw[s] >= nparam || (s > 0 && isw[s] <= isw[s - 1]))
+            return fail(c, RTB_ERR_ARG, "cirsradg_wave: isw must increase within 0..%d", nparam - 1);
+    // a one-element state that selects exactly the isw parameters, so that
+    // the set-up derives the same isw (cirsrtfg_wave.f:301-313); its mapped
+    // Jacobian is not used
+    const int ldl = a0.ld_lay > 0 ? a0.ld_lay : RTB_MAXLAY;
+    std::vector<float> xm(nparam, 0.0f), zl(ldl, 0.0f);
+    for (int s = 0; s < nsw; ++s) xm[isw[s]] = 1.0f;
+    rtb_atm a = a0;
+    a.nv = 1;
+    a.npro = 1;
+    a.ld_v = 1;
+    a.ld_param = nparam;
+    a.xmap = xm.data();
+    a.dte = zl.data();
+    a.dam = zl.data();
+    a.dco = a0.ncont > 0 ? zl.data() : nullptr;
+    int r = prepare(c, 1, &a);
+    if (r) return r;
+    const int64_t stride = (int64_t)c->nlmax_max * c->nsw_max;
+    CUDA_TRY(c, c->d_dq.ensure((size_t)a.npath * stride * sizeof(float) + 16));
+    drop_graph(c);
+    c->B.dq_out = (float*)c->d_dq.p;
+    c->B.dq_stride = stride;
+    c->B.dq_npath = a.npath;
+    r = launch(c);
+    c->B.dq_out = nullptr;
+    if (r) return r;
+    std::vector<float> co(a.npath), gr(a.npath), gt(a.npath), dq((size_t)a.npath * stride);
+    float* pc = co.data();
+    float* pg = gr.data();
+    float* pt = gt.data();
+    r = fetch(c, &pc, &pg, &pt);
+    if (r) return r;
+    CUDA_TRY(c, cudaMemcpy(dq.data(), c->d_dq.p, dq.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    // cirsradg_wave.f:1240-1267: zero, then the isw columns of the path's layers
+    for (int ip = 0; ip < a.npath; ++ip) {
+        output[ip] = co[ip];
+        if (gtsurf) gtsurf[ip] = gt[ip];
+        for (int k = 0; k < nparam; ++k)
+            for (int j = 0; j < ld_lay; ++j) doutputdq[ip + (size_t)ld_pat * (j + (size_t)ld_lay * k)] = 0.0f;
+        for (int j = 0; j < a.nlayin[ip]; ++j)
+            for (int s = 0; s < nsw; ++s)
+                doutputdq[ip + (size_t)ld_pat * (j + (size_t)ld_lay * isw[s])] = dq[ip * stride + j * nsw + s];
+    }
     return RTB_OK;
 }
 

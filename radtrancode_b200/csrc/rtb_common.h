@@ -118,6 +118,11 @@ struct BatchDev {
     // work counter (zero at launch; nullptr = static grid-stride)
     const int* item_order;
     unsigned long long* work_next;
+    // per-path-position derivatives dR/dq (cirsradg_wave's doutputdq) of every
+    // item, [wave][npath][dq_stride] with dq_stride = nlmax x nsw; nullptr = off
+    float* dq_out;
+    int64_t dq_stride;
+    int dq_npath;
 };
 
 }  // namespace rtb

@@ -220,3 +220,30 @@ def test_noncoincident_wavenumbers(ctx, oracle, shift):
     # the coincident spectrum differs: the branch was taken
     c0, _, _ = ctx.cirsrtfg_wave(job)
     assert not np.array_equal(c0, c)
+
+
+def test_cirsradg_wave_compat_matches_cirsrtfg_wave(ctx):
+    """The per-wavenumber form (cirsradg_wave's output and doutputdq): its
+    radiance is the whole-spectrum call's bit for bit, and map2pro + map2xvec
+    of its doutputdq (done here in FP64) give the whole-spectrum Jacobian."""
+    import dataclasses
+    kt, cia, job = synth.config2(nwave=6, nlayer=40, nbin=8)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c, g, gt = ctx.cirsrtfg_wave(job)
+    G = g.reshape(job.nv, job.nwave).astype(np.float64)
+    L, ngas = job.nlayer, job.ngas
+    isw = [2, 3, 4, 5, ngas]                      # the absorbers and T: the parameters xmap touches
+    lay = job.layinc[:L, 0] - 1
+    scale = np.maximum(np.max(np.abs(G), axis=1), 1e-300)
+    for iw in (0, 3, 5):
+        j1 = dataclasses.replace(job, nwave=1, vwave=job.vwave[iw:iw + 1].copy())
+        out, gts, dq = ctx.cirsradg_wave(j1, isw)
+        assert out[0] == c[iw] and gts[0] == gt[iw]
+        assert not dq[:, :, [0, 1]].any()          # H2, He: not in isw
+        Gh = np.zeros(job.nv)
+        for k in isw:
+            M = (job.dte if k == ngas else job.dam).astype(np.float64)
+            per_level = dq[0, :L, k].astype(np.float64) @ M[lay, :]
+            Gh += job.xmap[:, k, :].astype(np.float64) @ per_level
+        assert np.all(np.abs(Gh - G[:, iw]) <= 1e-5 * scale)

@@ -71,6 +71,23 @@ def test_newton_step_matches_reference_algebra(ctx, oracle, c1, c2s, hess, which
     assert np.all(resid < (1e-4 if hess == 0 else 1e-10))
 
 
+def test_drop_in_gain_matrix_and_calcnextxn(ctx, oracle, c1, c2s):
+    """The reference's interface (D and AA returned, then calcnextxn) against
+    the oracle's dense restatement; FP64 throughout, so 1e-9 of the largest
+    entry for D and AA and REAL rounding for x_out."""
+    for kt, cia, cases in (c1, c2s):
+        kk, sei, sai, xa, xn, y, yn = _newton_inputs(oracle, kt, cia, cases[:1], 2.0)
+        dd, aa, nonpd = ctx.calc_gain_matrix(kk[0], sai[0], sei[0])
+        dd_r, aa_r = oracle.gain_matrix(kk[0], sei[0], sai[0])
+        assert nonpd == 0
+        assert np.max(np.abs(dd - dd_r)) <= 1e-9 * np.max(np.abs(dd_r))
+        assert np.max(np.abs(aa - aa_r)) <= 1e-9 * np.max(np.abs(aa_r))
+        x = ctx.calcnextxn(xa[0], xn[0], y[0], yn[0], dd, aa)
+        x_r = oracle.calcnextxn(xa[0], xn[0], y[0], yn[0], dd_r, aa_r)
+        step = np.max(np.abs(x_r - xa[0]))
+        assert np.all(np.abs(x - x_r) <= 1e-6 * step + 2 * _ulp(x_r))
+
+
 def test_refinement_reduces_residual(ctx, oracle, c2s):
     kt, cia, cases = c2s
     args = _newton_inputs(oracle, kt, cia, cases, 1.0)

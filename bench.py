@@ -462,6 +462,32 @@ def profile_newton(args):
             print(json.dumps({"profile_newton": n, "ms_kernel": ctx.newton_stats()["ms_kernel"]}))
 
 
+def profile_aux(args):
+    """Reduced case for ncu captures of the small kernels of the Newton-step
+    interface: `--profile-aux` retrievals (NX=124, NY=2000) through
+    calc_phiret, the Sa inverse, then one calc_gain_matrix + calcnextxn."""
+    from radtrancode_b200 import cirsradg, synth
+    n, nx, ny = args.profile_aux, 124, 2000
+    rng = np.random.default_rng(12)
+    p_lev, p_lay = synth._levels(120)
+    sa = synth.prior_covariance(p_lay, 4)
+    sai1 = np.linalg.inv(sa)
+    sai = np.broadcast_to(sai1, (n, nx, nx))
+    sei = np.full((n, ny), 1e18)
+    xa = np.full((n, nx), 150.0, np.float32)
+    xn = xa + rng.standard_normal((n, nx)).astype(np.float32)
+    y = (rng.standard_normal((n, ny)) * 1e-8).astype(np.float32)
+    yn = np.zeros((n, ny), np.float32)
+    kk = (rng.standard_normal((nx, ny)) * 1e-9).astype(np.float32)
+    with cirsradg.Context(0) as ctx:
+        for _ in range(args.warmup + args.steps):
+            phi, _ = ctx.calc_phiret_batch(y, yn, sei, xn, xa, sai)
+            ctx.spd_inverse_batch(np.broadcast_to(sa, (n, nx, nx)))
+            dd, aa, _ = ctx.calc_gain_matrix(kk, sai1, sei[0])
+            x = ctx.calcnextxn(xa[0], xn[0], y[0], yn[0], dd, aa)
+            print(json.dumps({"profile_aux": n, "phi0": float(phi[0]), "x0": float(x[0])}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -478,7 +504,12 @@ def main():
                     help="uneven spectra in the batched leg (0 skips it)")
     ap.add_argument("--profile-newton", type=int, default=0,
                     help="profiling case: only the Newton-step kernel on N full-size retrievals")
+    ap.add_argument("--profile-aux", type=int, default=0,
+                    help="profiling case: the small kernels of the Newton-step interface on N retrievals")
     args = ap.parse_args()
+    if args.profile_aux:
+        profile_aux(args)
+        return
     if args.profile_waves:
         profile_case(args)
         return

@@ -98,6 +98,21 @@ int rtb_set_ktables(rtb_context* ctx, int ntab, int np, int nt, int ng,
  *   kcia         REAL kcia(9, 25, 1501), Fortran order (pair fastest). */
 int rtb_set_cia(rtb_context* ctx, float dnu, const double* temps, const float* kcia);
 
+/* The reference's table files, read on the host (no device work):
+ * rtb_load_ktables reads ntab .kta files (read_klist.f / read_khead.f:33-110
+ * header, then the records from IREC0 on) and loads them with
+ * rtb_set_ktables; the tables must share the P, T and g grid (the /INTERPK/
+ * block of get_kg.f:100-101) and a regular wavenumber grid.  idgas/isogas
+ * (may be NULL) receive each file's gas and isotope ids.
+ * rtb_kta_header reads one header (no context needed).
+ * rtb_load_cia reads a CIA .tab file (ciaread.f:77-98: sequential
+ * unformatted, 25 DOUBLE temperatures then REAL kcia(9,25,1501)) and loads it
+ * with rtb_set_cia. */
+int rtb_kta_header(const char* path, int* np, int* nt, int* ng, int* npoint, float* vmin, float* delv,
+                   int* idgas, int* isogas);
+int rtb_load_ktables(rtb_context* ctx, int ntab, const char* const* paths, int* idgas, int* isogas);
+int rtb_load_cia(rtb_context* ctx, const char* path, float dnu);
+
 /* ---------------------------------------------------------------------- */
 /* Forward model + Jacobian (cirsrtfg_wave replacement)                    */
 /* ---------------------------------------------------------------------- */

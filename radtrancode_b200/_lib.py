@@ -103,6 +103,12 @@ def lib() -> C.CDLL:
         L.rtb_cirsradg_wave.argtypes = [vp, C.POINTER(_abi.RtbAtm), C.c_int, ip, fp, fp, fp, C.c_int, C.c_int,
                                         C.c_int]
         L.rtb_cirsradg_wave.restype = C.c_int
+        L.rtb_kta_header.argtypes = [C.c_char_p, ip, ip, ip, ip, fp, fp, ip, ip]
+        L.rtb_kta_header.restype = C.c_int
+        L.rtb_load_ktables.argtypes = [vp, C.c_int, C.POINTER(C.c_char_p), ip, ip]
+        L.rtb_load_ktables.restype = C.c_int
+        L.rtb_load_cia.argtypes = [vp, C.c_char_p, C.c_float]
+        L.rtb_load_cia.restype = C.c_int
         p16 = C.POINTER(C.c_int16)
         L.rtb_get_debug_bins.argtypes = [vp, p16, C.c_size_t, p16, C.c_size_t]
         L.rtb_get_debug_bins.restype = C.c_int
@@ -119,5 +125,5 @@ EXPORTED = [
     "rtb_calc_phiret_batch", "rtb_spd_inverse_batch", "rtb_retrieve_batch", "rtb_get_newton_stats",
     "rtb_fwd_set_schedule", "rtb_fwd_autotune", "rtb_fwd_use_graph", "rtb_server_create", "rtb_server_destroy",
     "rtb_server_submit", "rtb_server_step", "rtb_server_poll", "rtb_calc_gain_matrix", "rtb_calcnextxn",
-    "rtb_cirsradg_wave",
+    "rtb_cirsradg_wave", "rtb_kta_header", "rtb_load_ktables", "rtb_load_cia",
 ]

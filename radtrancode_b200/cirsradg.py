@@ -11,6 +11,7 @@ reference would STOP.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -63,6 +64,19 @@ class Context:
             self._h, kt.ntab, kt.np_, kt.nt, kt.ng, _abi.fptr(kt.lnp), _abi.fptr(kt.tk), _abi.fptr(kt.delg),
             _abi.fptr(kt.vmin), _abi.fptr(kt.delv), _abi.iptr(kt.nbin), _abi.fptr(kt.data)))
         self.tables = kt
+
+    def load_ktables(self, paths):
+        """read_klist equivalent from .kta files; returns [(idgas, isogas)]."""
+        n = len(paths)
+        arr = (C.c_char_p * n)(*[os.fsencode(p) for p in paths])
+        ids = np.zeros(n, np.int32)
+        isos = np.zeros(n, np.int32)
+        self._check(self._L.rtb_load_ktables(self._h, n, arr, _abi.iptr(ids), _abi.iptr(isos)))
+        return list(zip(ids.tolist(), isos.tolist()))
+
+    def load_cia(self, path, dnu=1.0):
+        """ciaread equivalent from a CIA .tab file."""
+        self._check(self._L.rtb_load_cia(self._h, os.fsencode(path), float(dnu)))
 
     def set_cia(self, cia):
         """ciaread's one-time table read."""

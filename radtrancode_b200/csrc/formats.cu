@@ -1,0 +1,172 @@
+// formats.cu -- the reference's table files, read on the host and handed to
+// rtb_set_ktables / rtb_set_cia.
+//
+// .kta (radtran/cirsrad/read_khead.f:33-110, written by
+// radtran/radtran/calc_fnktablec.f:304-367): a direct-access file of 4-byte
+// records (RECL = ISYS() = 4 with gfortran).  Records, 1-based: 1 IREC0,
+// 2 NPOINT, 3 VMIN, 4 DELV, 5 FWHM, 6 NP, 7 NT, 8 NG, 9 IDGAS, 10 ISOGAS,
+// 11.. G_ORD(NG), DEL_G(NG), two spare records, PRESS(NP) in atm, TEMP(NT)
+// (or TEMP2(NP,|NT|) when NT < 0), VCEN(NPOINT) when DELV <= 0; the k values
+// (x 1e20) from record IREC0 on, bin by bin, (P, T, g) with g fastest
+// (get_kg.f:137-140, 211, 293-296).
+//
+// CIA .tab (radtran/radtran/ciaread.f:77-98): a sequential unformatted file
+// with two records, 25 DOUBLE temperatures and REAL kcia(9, 25, 1501), each
+// framed by 4-byte length markers.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "context.h"
+
+namespace rtb {
+
+namespace {
+
+struct File {
+    FILE* f = nullptr;
+    explicit File(const char* p) : f(p ? std::fopen(p, "rb") : nullptr) {}
+    ~File() {
+        if (f) std::fclose(f);
+    }
+};
+
+struct Kta {
+    int irec0 = 0, npoint = 0, np = 0, nt = 0, ng = 0, idgas = 0, isogas = 0;
+    float vmin = 0, delv = 0, fwhm = 0;
+    std::vector<float> press, temp, delg;
+};
+
+// 1-based 4-byte record n of a direct-access file
+bool rec4(FILE* f, long n, void* out) {
+    if (std::fseek(f, (n - 1) * 4L, SEEK_SET) != 0) return false;
+    return std::fread(out, 4, 1, f) == 1;
+}
+
+bool recs4(FILE* f, long n, size_t count, void* out) {
+    if (std::fseek(f, (n - 1) * 4L, SEEK_SET) != 0) return false;
+    return std::fread(out, 4, count, f) == count;
+}
+
+// read_khead.f:47-110; returns an RTB status, message in err
+int read_kta_header(FILE* f, Kta& k, std::string& err) {
+    bool ok = rec4(f, 1, &k.irec0) && rec4(f, 2, &k.npoint) && rec4(f, 3, &k.vmin) && rec4(f, 4, &k.delv) &&
+              rec4(f, 5, &k.fwhm) && rec4(f, 6, &k.np) && rec4(f, 7, &k.nt) && rec4(f, 8, &k.ng) &&
+              rec4(f, 9, &k.idgas) && rec4(f, 10, &k.isogas);
+    if (!ok) {
+        err = "short .kta header";
+        return RTB_ERR_ARG;
+    }
+    if (k.np <= 0 || k.np > RTB_MAXK || k.ng <= 0 || k.ng > RTB_MAXG - 1 || k.npoint <= 0 || k.nt == 0 ||
+        std::abs(k.nt) > RTB_MAXK) {
+        err = "implausible .kta sizes (NP, NT, NG, NPOINT)";
+        return RTB_ERR_LIMIT;
+    }
+    if (k.nt < 0) {
+        err = ".kta with pressure-dependent temperatures (NT < 0) not supported";
+        return RTB_ERR_UNSUPPORTED;
+    }
+    if (!(k.delv > 0.0f)) {
+        err = ".kta on an irregular wavenumber grid (DELV <= 0) not supported";
+        return RTB_ERR_UNSUPPORTED;
+    }
+    k.delg.resize(k.ng);
+    k.press.resize(k.np);
+    k.temp.resize(k.nt);
+    ok = recs4(f, 11 + k.ng, k.ng, k.delg.data()) && recs4(f, 11 + 2 * k.ng + 2, k.np, k.press.data()) &&
+         recs4(f, 11 + 2 * k.ng + 2 + k.np, k.nt, k.temp.data());
+    if (!ok) {
+        err = "short .kta header arrays";
+        return RTB_ERR_ARG;
+    }
+    if (k.irec0 < 11 + 2 * k.ng + 2 + k.np + k.nt) {
+        err = "IREC0 points into the .kta header";
+        return RTB_ERR_ARG;
+    }
+    return RTB_OK;
+}
+
+}  // namespace
+
+}  // namespace rtb
+
+using namespace rtb;
+
+extern "C" {
+
+int rtb_kta_header(const char* path, int* np, int* nt, int* ng, int* npoint, float* vmin, float* delv, int* idgas,
+                   int* isogas) {
+    File fl(path);
+    if (!fl.f) return RTB_ERR_ARG;
+    Kta k;
+    std::string err;
+    const int r = read_kta_header(fl.f, k, err);
+    if (r) return r;
+    if (np) *np = k.np;
+    if (nt) *nt = k.nt;
+    if (ng) *ng = k.ng;
+    if (npoint) *npoint = k.npoint;
+    if (vmin) *vmin = k.vmin;
+    if (delv) *delv = k.delv;
+    if (idgas) *idgas = k.idgas;
+    if (isogas) *isogas = k.isogas;
+    return RTB_OK;
+}
+
+int rtb_load_ktables(rtb_context* c, int ntab, const char* const* paths, int* idgas, int* isogas) {
+    if (!c) return RTB_ERR_ARG;
+    if (ntab <= 0 || !paths) return fail(c, RTB_ERR_ARG, "load_ktables: no files");
+    std::vector<Kta> hd(ntab);
+    std::vector<float> vmin(ntab), delv(ntab), data;
+    std::vector<int> nbin(ntab);
+    for (int t = 0; t < ntab; ++t) {
+        File fl(paths[t]);
+        if (!fl.f) return fail(c, RTB_ERR_ARG, "cannot open %s", paths[t] ? paths[t] : "(null)");
+        std::string err;
+        const int r = read_kta_header(fl.f, hd[t], err);
+        if (r) return fail(c, r, "%s: %s", paths[t], err.c_str());
+        const Kta& k = hd[t];
+        // every table shares the /INTERPK/ grid of get_kg.f:100-101
+        if (t > 0 && (k.np != hd[0].np || k.nt != hd[0].nt || k.ng != hd[0].ng || k.press != hd[0].press ||
+                      k.temp != hd[0].temp || k.delg != hd[0].delg))
+            return fail(c, RTB_ERR_UNSUPPORTED, "%s: P/T/g grid differs from %s", paths[t], paths[0]);
+        const size_t n = (size_t)k.npoint * k.np * k.nt * k.ng;
+        const size_t off = data.size();
+        data.resize(off + n);
+        if (!recs4(fl.f, k.irec0, n, data.data() + off))
+            return fail(c, RTB_ERR_ARG, "%s: fewer k records than NPOINT x NP x NT x NG", paths[t]);
+        vmin[t] = k.vmin;
+        delv[t] = k.delv;
+        nbin[t] = k.npoint;
+        if (idgas) idgas[t] = k.idgas;
+        if (isogas) isogas[t] = k.isogas;
+    }
+    const Kta& k0 = hd[0];
+    std::vector<float> lnp(k0.np);
+    for (int i = 0; i < k0.np; ++i) lnp[i] = logf(k0.press[i]);   // PRESS(J) = LOG(PRESS(J)), read_khead.f:83
+    return rtb_set_ktables(c, ntab, k0.np, k0.nt, k0.ng, lnp.data(), k0.temp.data(), k0.delg.data(), vmin.data(),
+                           delv.data(), nbin.data(), data.data());
+}
+
+int rtb_load_cia(rtb_context* c, const char* path, float dnu) {
+    if (!c) return RTB_ERR_ARG;
+    File fl(path);
+    if (!fl.f) return fail(c, RTB_ERR_ARG, "cannot open %s", path ? path : "(null)");
+    const size_t nt = RTB_CIA_NUMT, nk = (size_t)RTB_CIA_NUMPAIRS * RTB_CIA_NUMT * RTB_CIA_NUMWN;
+    double temps[RTB_CIA_NUMT];
+    std::vector<float> kcia(nk);
+    int32_t m1 = 0, m2 = 0, m3 = 0, m4 = 0;
+    bool ok = std::fread(&m1, 4, 1, fl.f) == 1 && m1 == (int32_t)(nt * 8) && std::fread(temps, 8, nt, fl.f) == nt &&
+              std::fread(&m2, 4, 1, fl.f) == 1 && m2 == m1;
+    ok = ok && std::fread(&m3, 4, 1, fl.f) == 1 && m3 == (int32_t)(nk * 4) &&
+         std::fread(kcia.data(), 4, nk, fl.f) == nk && std::fread(&m4, 4, 1, fl.f) == 1 && m4 == m3;
+    if (!ok)
+        return fail(c, RTB_ERR_ARG, "%s: not a CIA table (two unformatted records: 25 DOUBLE, REAL(9,25,1501))",
+                    path);
+    return rtb_set_cia(c, dnu, temps, kcia.data());
+}
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+"""The reference's table formats: .kta headers read without a device (CPU),
+and whole runs loaded from .kta and CIA .tab files against the same tables
+handed over in memory (GPU)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from radtrancode_b200 import _lib, synth
+from tests.helpers import JAC_TOL, RAD_TOL, jac_err, rad_err
+from tests.tablefiles import write_cia_tab, write_kta
+
+
+def _header(path):
+    L = _lib.lib()
+    ip = lambda: C.c_int()
+    np_, nt, ng, npt, ida, iso = ip(), ip(), ip(), ip(), ip(), ip()
+    vmin, delv = C.c_float(), C.c_float()
+    st = L.rtb_kta_header(os.fsencode(path), C.byref(np_), C.byref(nt), C.byref(ng), C.byref(npt),
+                          C.byref(vmin), C.byref(delv), C.byref(ida), C.byref(iso))
+    return st, (np_.value, nt.value, ng.value, npt.value, vmin.value, delv.value, ida.value, iso.value)
+
+
+def test_kta_header(tmp_path):
+    _lib.build()
+    kt, _, _ = synth.config1()
+    p = str(tmp_path / "ch4.kta")
+    write_kta(p, kt, 0, 6, 0)
+    st, h = _header(p)
+    assert st == 0
+    assert h == (kt.np_, kt.nt, kt.ng, int(kt.nbin[0]), float(kt.vmin[0]), float(kt.delv[0]), 6, 0)
+
+
+def test_kta_unsupported_and_short_files(tmp_path):
+    _lib.build()
+    kt, _, _ = synth.config1()
+    p = str(tmp_path / "t2.kta")
+    write_kta(p, kt, 0, 6, 0, nt_sign=-1)           # TEMP2(NP, |NT|) tables
+    assert _header(p)[0] == 3                        # RTB_ERR_UNSUPPORTED
+    q = str(tmp_path / "short.kta")
+    open(q, "wb").write(open(p, "rb").read()[:20])
+    assert _header(q)[0] == 1                        # RTB_ERR_ARG
+    assert _header(str(tmp_path / "missing.kta"))[0] == 1
+
+
+@pytest.mark.gpu
+def test_run_from_files_matches_in_memory_tables(ctx, tmp_path):
+    kt, cia, job = synth.config2(nwave=24, nlayer=60, nbin=24)
+    paths = []
+    for i, gas in enumerate(kt.gases):
+        p = str(tmp_path / f"gas{i}.kta")
+        write_kta(p, kt, i, gas[0], gas[1])
+        paths.append(p)
+    ctab = str(tmp_path / "cia.tab")
+    write_cia_tab(ctab, cia)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c0, g0, gt0 = ctx.cirsrtfg_wave(job)
+    ids = ctx.load_ktables(paths)
+    ctx.load_cia(ctab, cia.dnu)
+    assert ids == [tuple(g) for g in kt.gases]
+    c, g, gt = ctx.cirsrtfg_wave(job)
+    assert rad_err(c, c0) <= RAD_TOL
+    assert jac_err(g, g0, job.nv) <= JAC_TOL
+    ctx.set_ktables(kt)                  # leave the session context as the other tests expect

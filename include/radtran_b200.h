@@ -342,6 +342,12 @@ int rtb_calc_gain_matrix(rtb_context* ctx, int nx, int ny, int ldx, int ldy, con
                          const double* sxi, const double* sei, double* dd, double* aa, int* nonpd);
 int rtb_calcnextxn(rtb_context* ctx, int nx, int ny, int ldx, const float* x0, const float* xn,
                    const float* y, const float* yn, const double* dd, const double* aa, float* x_out);
+/* calc_serr (nemesis/calc_serr.f) after the last iteration, diagonal Se:
+ * sm = D Se D^T (measurement error), sn = (AA - I) Sa (AA - I)^T (smoothing
+ * error), st = sn + sm; sx REAL(ldx, nx), se REAL(ny) (the diagonal of
+ * se_in), dd and aa as from rtb_calc_gain_matrix; outputs REAL(ldx, nx). */
+int rtb_calc_serr(rtb_context* ctx, int nx, int ny, int ldx, const float* sx, const float* se,
+                  const double* dd, const double* aa, float* st, float* sn, float* sm);
 
 /* dinvertm (radtran/matrices/dinvertm.f jmod=2): inverse of nret symmetric
  * positive-definite n x n matrices (row-major, a[r*n*n]) by an FP64 Cholesky

@@ -188,6 +188,38 @@ void orc_calcnextxn(int nx, int ny, int ldx, const float* x0, const float* xn, c
     for (int i = 0; i < nx; ++i) x_out[i] = x0[i] + (float)(x2[i] - x1[i]);
 }
 
+/* calc_serr.f (sm = dd se dd^T, sn = (aa - I) sx (aa - I)^T, st = sn + sm),
+ * diagonal se; REAL outputs (ldx, nx). */
+void orc_calc_serr_diag(int nx, int ny, int ldx, const float* sx_in, const float* se_diag, const double* dd_in,
+                        const double* aa_in, float* st_out, float* sn_out, float* sm_out) {
+    std::vector<double> a((size_t)nx * ny), dt((size_t)ny * nx), sm((size_t)nx * nx), b((size_t)nx * nx),
+        e((size_t)nx * nx), c((size_t)nx * nx), sn((size_t)nx * nx);
+    /* a = dd*se: the off-diagonal products of the dense se are exact zeros */
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            a[i + (size_t)nx * j] = dd_in[i + (size_t)ldx * j] * (double)se_diag[j];
+            dt[j + (size_t)ny * i] = dd_in[i + (size_t)ldx * j];
+        }
+    dmult(a.data(), nx, nx, ny, dt.data(), ny, nx, sm.data(), nx);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < nx; ++j) {
+            b[i + (size_t)nx * j] = (double)sx_in[i + (size_t)ldx * j];
+            e[i + (size_t)nx * j] = aa_in[i + (size_t)ldx * j];
+        }
+    for (int i = 0; i < nx; ++i) e[i + (size_t)nx * i] = e[i + (size_t)nx * i] - 1.0;
+    dmult(e.data(), nx, nx, nx, b.data(), nx, nx, c.data(), nx);
+    std::vector<double> et((size_t)nx * nx);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < nx; ++j) et[i + (size_t)nx * j] = e[j + (size_t)nx * i];
+    dmult(c.data(), nx, nx, nx, et.data(), nx, nx, sn.data(), nx);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < nx; ++j) {
+            const size_t k = i + (size_t)nx * j, o = i + (size_t)ldx * j;
+            sm_out[o] = (float)sm[k];
+            sn_out[o] = (float)sn[k];
+            st_out[o] = (float)(sm[k] + sn[k]);
+        }
+}
 float orc_calc_phiret(int ny, int ldy, const float* y, const float* yn, const double* sei, int nx, int ldx,
                       const float* xn, const float* xa, const double* sai, float* chisq) {
     std::vector<double> b(ny), a(ny);

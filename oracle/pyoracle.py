@@ -252,3 +252,19 @@ def dinvertm(a):
     out = np.zeros_like(a, order="F")
     ic = L.orc_dinvertm_chol(a.shape[0], a.shape[0], a.ctypes.data_as(dp), out.ctypes.data_as(dp))
     return out, ic
+
+
+def calc_serr(sx, se_diag, dd, aa):
+    """calc_serr (diagonal Se): returns (st, sn, sm) [nx, nx] float32 (Fortran order)."""
+    L = lib()
+    dp = C.POINTER(C.c_double)
+    dd = np.asfortranarray(dd, np.float64)
+    aa = np.asfortranarray(aa, np.float64)
+    nx, ny = dd.shape
+    sx = np.asfortranarray(sx, np.float32)
+    se = np.ascontiguousarray(se_diag, np.float32)
+    out = [np.zeros((nx, nx), np.float32, order="F") for _ in range(3)]
+    L.orc_calc_serr_diag(nx, ny, nx, _abi.fptr(sx), _abi.fptr(se), dd.ctypes.data_as(dp), aa.ctypes.data_as(dp),
+                         _abi.fptr(out[0]), _abi.fptr(out[1]), _abi.fptr(out[2]))
+    return tuple(out)
+

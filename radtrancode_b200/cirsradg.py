@@ -224,6 +224,18 @@ class Context:
                                                  _abi.dptr(sei), _abi.dptr(dd), _abi.dptr(aa), C.byref(nonpd)))
         return dd, aa, nonpd.value
 
+    def calc_serr(self, sx, se_diag, dd, aa):
+        """calc_serr: (st, sn, sm) [nx, nx] float32 from Sa, diag(Se), D, AA."""
+        dd = np.asfortranarray(dd, np.float64)
+        aa = np.asfortranarray(aa, np.float64)
+        nx, ny = dd.shape
+        sx = np.asfortranarray(sx, np.float32)
+        se = np.ascontiguousarray(se_diag, np.float32)
+        out = [np.zeros((nx, nx), np.float32, order="F") for _ in range(3)]
+        self._check(self._L.rtb_calc_serr(self._h, nx, ny, nx, _abi.fptr(sx), _abi.fptr(se), _abi.dptr(dd),
+                                          _abi.dptr(aa), _abi.fptr(out[0]), _abi.fptr(out[1]), _abi.fptr(out[2])))
+        return tuple(out)
+
     def calcnextxn(self, x0, xn, y, yn, dd, aa):
         f32 = lambda a: np.ascontiguousarray(a, np.float32)
         x0, xn, y, yn = f32(x0), f32(xn), f32(y), f32(yn)

@@ -1,8 +1,9 @@
-// gain.cu -- drop-in calc_gain_matrix and calcnextxn on the device.
+// gain.cu -- drop-in calc_gain_matrix, calcnextxn and calc_serr on the device.
 //
 // Reference: nemesis/calc_gain_matrix.f:123-163 (nx < ny branch: C = K^T Se^-1 K
 // + Sa^-1, A = C^-1 by dinvertm jmod=2, D = A K^T Se^-1, AA = D K) and
-// nemesis/calcnextxn.f:64-104 (x_out = x0 + D (y - yn) - AA (x0 - xn)).  The
+// nemesis/calcnextxn.f:64-104 (x_out = x0 + D (y - yn) - AA (x0 - xn)) and
+// nemesis/calc_serr.f (Sm = D Se D^T, Sn = (AA - I) Sa (AA - I)^T, St = Sn + Sm).  The
 // reference works in DOUBLE PRECISION on promoted REAL inputs; so do these
 // kernels (FP64 on the CUDA cores; the sizes are small: 2 NX^2 NY flops per
 // product).  The fused batched step (newton.cu) is the fast path; these
@@ -76,6 +77,14 @@ nextxn_kernel(int nx, int ny, const double* __restrict__ dd, int64_t ldx, const 
     if (lane == 0) x_out[a] = x0[a] + (float)(x2 - x1);
 }
 
+// E = aa - I, aa(ldx, nx) column-major -> E row-major [nx][nx]
+__global__ void aa_minus_identity(int nx, const double* __restrict__ aa, int64_t ldx, double* __restrict__ E) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nx * nx) return;
+    const int a = e / nx, b = e - a * nx;
+    E[e] = aa[a + ldx * b] - (a == b ? 1.0 : 0.0);
+}
+
 template <class TA, class TB>
 cudaError_t gemm(int M, int N, int K, const TA* A, int64_t am, int64_t ak, const TB* B, int64_t bk, int64_t bn,
                  const double* sk, const double* sn, const double* add, int64_t dm, int64_t dn, double* C,
@@ -140,6 +149,58 @@ int rtb_calc_gain_matrix(rtb_context* c, int nx, int ny, int ldx, int ldy, const
         for (int b = 0; b < nx; ++b) aa[a + (size_t)ldx * b] = ha[(size_t)a * nx + b];
     }
     if (nonpd) *nonpd = (hs & kNtNonPd) ? 1 : 0;
+    return RTB_OK;
+}
+
+int rtb_calc_serr(rtb_context* c, int nx, int ny, int ldx, const float* sx, const float* se, const double* dd,
+                  const double* aa, float* st, float* sn, float* sm) {
+    if (!c) return RTB_ERR_ARG;
+    if (nx <= 0 || ny <= 0 || ldx < nx || !sx || !se || !dd || !aa || !st || !sn || !sm)
+        return fail(c, RTB_ERR_ARG, "calc_serr: bad arguments");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const cudaStream_t st_ = stream_of(c);
+    const size_t nn = (size_t)nx * nx, ndl = (size_t)ldx * ny, nal = (size_t)ldx * nx;
+    // f64: D (ldx, ny) | AA (ldx, nx) | se [ny] | Sa [nx][nx] col-major | E | C | Sm | Sn | St
+    CUDA_TRY(c, c->d_nt64.ensure((ndl + nal + ny + 6 * nn) * 8));
+    double* D = (double*)c->d_nt64.p;
+    double* AA = D + ndl;
+    double* sed = AA + nal;
+    double* sxd = sed + ny;
+    double* E = sxd + nn;
+    double* Cm = E + nn;
+    double* Sm = Cm + nn;
+    double* Sn = Sm + nn;
+    double* St = Sn + nn;
+    std::vector<double> h_se(se, se + ny), h_sx(nn);
+    for (int j = 0; j < nx; ++j)
+        for (int i = 0; i < nx; ++i) h_sx[i + (size_t)nx * j] = (double)sx[i + (size_t)ldx * j];
+    CUDA_TRY(c, cudaMemcpyAsync(D, dd, ndl * 8, cudaMemcpyHostToDevice, st_));
+    CUDA_TRY(c, cudaMemcpyAsync(AA, aa, nal * 8, cudaMemcpyHostToDevice, st_));
+    CUDA_TRY(c, cudaMemcpyAsync(sed, h_se.data(), (size_t)ny * 8, cudaMemcpyHostToDevice, st_));
+    CUDA_TRY(c, cudaMemcpyAsync(sxd, h_sx.data(), nn * 8, cudaMemcpyHostToDevice, st_));
+    // Sm(a, b) = sum_i D(a, i) Se(i) D(b, i)
+    CUDA_TRY(c, (gemm<double, double>(nx, nx, ny, D, 1, ldx, D, ldx, 1, sed, nullptr, nullptr, 0, 0, Sm, nx, 1,
+                                      st_)));
+    aa_minus_identity<<<(int)((nn + 255) / 256), 256, 0, st_>>>(nx, AA, ldx, E);
+    CUDA_TRY(c, cudaGetLastError());
+    // C = E Sa, Sn = C E^T, St = C E^T + Sm
+    CUDA_TRY(c, (gemm<double, double>(nx, nx, nx, E, nx, 1, sxd, 1, nx, nullptr, nullptr, nullptr, 0, 0, Cm, nx, 1,
+                                      st_)));
+    CUDA_TRY(c, (gemm<double, double>(nx, nx, nx, Cm, nx, 1, E, 1, nx, nullptr, nullptr, nullptr, 0, 0, Sn, nx, 1,
+                                      st_)));
+    CUDA_TRY(c, (gemm<double, double>(nx, nx, nx, Cm, nx, 1, E, 1, nx, nullptr, nullptr, Sm, nx, 1, St, nx, 1,
+                                      st_)));
+    std::vector<double> h((size_t)3 * nn);
+    CUDA_TRY(c, cudaMemcpyAsync(h.data(), Sm, 3 * nn * 8, cudaMemcpyDeviceToHost, st_));
+    CUDA_TRY(c, cudaStreamSynchronize(st_));
+    // REAL outputs (ldx, nx), column-major (calc_serr.f sngl copies)
+    for (int a = 0; a < nx; ++a)
+        for (int b = 0; b < nx; ++b) {
+            const size_t k = (size_t)a * nx + b, o = a + (size_t)ldx * b;
+            sm[o] = (float)h[k];
+            sn[o] = (float)h[nn + k];
+            st[o] = (float)h[2 * nn + k];
+        }
     return RTB_OK;
 }
 

@@ -88,6 +88,23 @@ def test_drop_in_gain_matrix_and_calcnextxn(ctx, oracle, c1, c2s):
         assert np.all(np.abs(x - x_r) <= 1e-6 * step + 2 * _ulp(x_r))
 
 
+def test_calc_serr_matches_oracle(ctx, oracle, c2s):
+    """Final error covariances (calc_serr.f) from the device D and AA, against
+    the oracle's restatement on the same D and AA: REAL outputs within 1e-5 of
+    the largest entry."""
+    kt, cia, cases = c2s
+    kk, sei, sai, xa, xn, y, yn = _newton_inputs(oracle, kt, cia, cases[:1], 2.0)
+    dd, aa, _ = ctx.calc_gain_matrix(kk[0], sai[0], sei[0])
+    sx = cases[0].sa.astype(np.float32)
+    se = (1.0 / sei[0]).astype(np.float32)
+    got = ctx.calc_serr(sx, se, dd, aa)
+    ref = oracle.calc_serr(sx, se, dd, aa)
+    for g, r in zip(got, ref):
+        assert np.max(np.abs(g - r)) <= 1e-5 * np.max(np.abs(r))
+    st, sn, sm = got
+    assert np.allclose(st, sn + sm, rtol=1e-5, atol=1e-5 * np.max(np.abs(st)))
+
+
 def test_refinement_reduces_residual(ctx, oracle, c2s):
     kt, cia, cases = c2s
     args = _newton_inputs(oracle, kt, cia, cases, 1.0)

@@ -178,6 +178,17 @@ int rtb_cirsrtfg_wave_batch(rtb_context* ctx, int nspec, const rtb_atm* atms,
                             float* const* calcout, float* const* gradients,
                             float* const* gradtsurf);
 
+/* Instrument convolution, cirsconv (radtran/cirsrad/cirsconv.f:12-160), of
+ * nser series y[nser][nwave] on the calculation grid vwave to nconv channels
+ * vconv: FWHM > 0 averages a natural cubic spline of each series over a
+ * square bin of width fwhm (20-point trapezoid); FWHM = 0 copies (nconv must
+ * equal nwave); FWHM < 0 (filter-file channels) is not implemented.  With
+ * rtb_cirsrtfg_wave called at FWHM = 0 this gives cirsrtfg_wave's outputs for
+ * FWHM > 0 (cirsrtfg_wave.f:448-516 convolves calcout, gradtsurf and every
+ * Jacobian row the same way).  yout[nser][nconv]. */
+int rtb_cirsconv(rtb_context* ctx, int nwave, const float* vwave, int nser, const float* y, float fwhm,
+                 int nconv, const float* vconv, float* yout);
+
 /* Per-wavenumber compatibility form of cirsradg_wave (radtran/cirsradg/
  * cirsradg_wave.f:1-5, outputs :1240-1267) for A/B checks against the
  * reference one wavenumber at a time: the layer and path arrays as for

@@ -265,3 +265,88 @@ float orc_calc_phiret_diag(int ny, const float* y, const float* yn, const double
 }
 
 }  // extern "C"
+
+/* ---- instrument convolution (radtran/cirsrad/cirsconv.f:12-160, FWHM > 0
+ * and FWHM = 0) with CSPLINE (rtm_util/cspline.f) and CSPLINT
+ * (rtm_util/csplint.f); REAL arithmetic as the reference, DOUBLE sums. ---- */
+namespace {
+void cspline_nat(const float* X, const float* Y, int N, float* Y2, std::vector<float>& U) {
+    U.assign(N, 0.0f);
+    Y2[0] = 0.0f;                                   /* YP1 > .99E30: natural */
+    U[0] = 0.0f;
+    for (int I = 1; I < N - 1; ++I) {
+        const float SIG = (X[I] - X[I - 1]) / (X[I + 1] - X[I - 1]);
+        const float P = SIG * Y2[I - 1] + 2.0f;
+        Y2[I] = (SIG - 1.0f) / P;
+        if (X[I - 1] == X[I] || X[I] == X[I + 1]) {
+            U[I] = U[I - 1];
+            continue;
+        }
+        U[I] = (6.0f * ((Y[I + 1] - Y[I]) / (X[I + 1] - X[I]) - (Y[I] - Y[I - 1]) / (X[I] - X[I - 1])) /
+                    (X[I + 1] - X[I - 1]) - SIG * U[I - 1]) / P;
+    }
+    const float QN = 0.0f, UN = 0.0f;              /* YPN > .99E30 */
+    Y2[N - 1] = (UN - QN * U[N - 2]) / (QN * Y2[N - 2] + 1.0f);
+    for (int K = N - 2; K >= 0; --K) Y2[K] = Y2[K] * Y2[K + 1] + U[K];
+}
+
+float csplint(const float* XA, const float* YA, const float* Y2A, int N, float X) {
+    int KLO = 1, KHI = N;
+    while (KHI - KLO > 1) {
+        const int K = (KHI + KLO) / 2;
+        if (XA[K - 1] > X) KHI = K; else KLO = K;
+    }
+    const double H = (double)(XA[KHI - 1] - XA[KLO - 1]);
+    const double A = (double)(XA[KHI - 1] - X) / H;
+    const double B = (double)(X - XA[KLO - 1]) / H;
+    const double Y1 = A * (double)YA[KLO - 1] + B * (double)YA[KHI - 1] +
+                      ((A * A * A - A) * (double)Y2A[KLO - 1] + (B * B * B - B) * (double)Y2A[KHI - 1]) * (H * H) /
+                          6.0;
+    return std::fabs(Y1) > 1.00E-37 ? (float)Y1 : 1.00E-37f;
+}
+}  // namespace
+
+extern "C" int orc_cirsconv(int nwave, const float* vwave, const float* y, float fwhm, int nconv,
+                            const float* vconv, float* yout) {
+    if (fwhm == 0.0f) {
+        for (int i = 0; i < nconv; ++i) yout[i] = y[i];
+        return RTB_OK;
+    }
+    if (fwhm < 0.0f || nwave < 2) return RTB_ERR_UNSUPPORTED;
+    std::vector<float> xc(vwave, vwave + nwave), yc(y, y + nwave);
+    if (vconv[nconv - 1] > vwave[nwave - 1] - fwhm / 2.0f) {
+        const float x = vconv[nconv - 1] + fwhm;
+        xc.push_back(x);
+        yc.push_back(y[nwave - 1] + ((y[nwave - 1] - y[nwave - 2]) / (vwave[nwave - 1] - vwave[nwave - 2]) *
+                                     (x - vwave[nwave - 1])));
+    }
+    if (vconv[0] < vwave[0] + fwhm / 2.0f) {
+        const float x = vconv[0] - fwhm;
+        xc.insert(xc.begin(), x);
+        yc.insert(yc.begin(), y[0] + ((y[1] - y[0]) / (vwave[1] - vwave[0]) * (x - vwave[0])));
+    }
+    std::vector<float> x1v, y1v;
+    for (size_t i = 0; i < xc.size(); ++i)
+        if (!std::isnan(yc[i])) {
+            x1v.push_back(xc[i]);
+            y1v.push_back(yc[i]);
+        }
+    const int nc = (int)x1v.size();
+    std::vector<float> y2(nc), u;
+    cspline_nat(x1v.data(), y1v.data(), nc, y2.data(), u);
+    const int nstep = 20;
+    for (int i = 0; i < nconv; ++i) {
+        const float x1 = vconv[i] - fwhm / 2.0f, x2 = vconv[i] + fwhm / 2.0f;
+        const float delx = (x2 - x1) / (float)(nstep - 1);
+        double sum = 0.0, yold = 0.0;
+        for (int j = 1; j <= nstep; ++j) {
+            const float xi = x1 + (float)(j - 1) * delx;
+            const double yi = (double)csplint(x1v.data(), y1v.data(), y2.data(), nc, xi);
+            if (j == 1) sum = 0.0;
+            else sum = sum + (yi + yold) * (double)(delx / 2.0f);
+            yold = yi;
+        }
+        yout[i] = (float)(sum / (double)fwhm);
+    }
+    return RTB_OK;
+}

@@ -125,6 +125,10 @@ float orc_calc_phiret_diag(int ny, const float* y, const float* yn,
 /* calc_serr.f with a diagonal se (REAL se_diag[ny]); outputs REAL (ldx, nx) */
 void orc_calc_serr_diag(int nx, int ny, int ldx, const float* sx_in, const float* se_diag, const double* dd_in,
                         const double* aa_in, float* st_out, float* sn_out, float* sm_out);
+/* cirsconv.f for FWHM >= 0 (FWHM > 0: natural cubic spline, 20-point
+ * trapezoid per channel; FWHM = 0: copy) */
+int orc_cirsconv(int nwave, const float* vwave, const float* y, float fwhm, int nconv, const float* vconv,
+                 float* yout);
 /* dinvertm(jmod=2): Cholesky inverse with the A*Ainv check; returns icheck */
 int orc_dinvertm_chol(int n, int lda, const double* a, double* ainv);
 

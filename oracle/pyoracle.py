@@ -268,3 +268,16 @@ def calc_serr(sx, se_diag, dd, aa):
                          _abi.fptr(out[0]), _abi.fptr(out[1]), _abi.fptr(out[2]))
     return tuple(out)
 
+
+def cirsconv(vwave, y, fwhm, vconv):
+    L = lib()
+    vwave = np.ascontiguousarray(vwave, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    vconv = np.ascontiguousarray(vconv, np.float32)
+    yout = np.zeros(len(vconv), np.float32)
+    st = L.orc_cirsconv(len(vwave), _abi.fptr(vwave), _abi.fptr(y), C.c_float(fwhm), len(vconv), _abi.fptr(vconv),
+                        _abi.fptr(yout))
+    if st != 0:
+        raise RuntimeError(f"oracle status {_abi.STATUS_NAMES.get(st, st)}")
+    return yout
+

@@ -101,6 +101,16 @@ class Context:
                                               _abi.fptr(gts)))
         return calcout, grads, gts
 
+    def cirsconv(self, vwave, y, fwhm, vconv):
+        """cirsconv of series y [nser, nwave] to channels vconv: [nser, nconv]."""
+        vwave = np.ascontiguousarray(vwave, np.float32)
+        vconv = np.ascontiguousarray(vconv, np.float32)
+        y = np.ascontiguousarray(np.atleast_2d(y), np.float32)
+        out = np.zeros((y.shape[0], len(vconv)), np.float32)
+        self._check(self._L.rtb_cirsconv(self._h, len(vwave), _abi.fptr(vwave), y.shape[0], _abi.fptr(y),
+                                         float(fwhm), len(vconv), _abi.fptr(vconv), _abi.fptr(out)))
+        return out
+
     def cirsradg_wave(self, job, isw):
         """rtb_cirsradg_wave on a one-wavenumber job: (output [npath],
         gtsurf [npath], doutputdq [npath, nlayer, nparam])."""

@@ -247,3 +247,26 @@ def test_cirsradg_wave_compat_matches_cirsrtfg_wave(ctx):
             per_level = dq[0, :L, k].astype(np.float64) @ M[lay, :]
             Gh += job.xmap[:, k, :].astype(np.float64) @ per_level
         assert np.all(np.abs(Gh - G[:, iw]) <= 1e-5 * scale)
+
+
+def test_cirsconv_fwhm_matches_oracle(ctx, oracle):
+    """cirsconv.f with FWHM > 0 on the device (natural cubic spline, 20-point
+    trapezoid per channel) against the oracle's restatement, on the radiance,
+    d/dtsurf and every Jacobian row of a spectrum computed at FWHM = 0, with
+    channels that need both end extrapolations and a series holding a NaN;
+    1e-6 of each series' largest value."""
+    kt, cia, job = synth.config2(nwave=200, nlayer=40, nbin=200)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c, g, gt = ctx.cirsrtfg_wave(job)
+    series = np.vstack([c[None], gt[None], g.reshape(job.nv, job.nwave)])
+    series[3, 57] = np.nan
+    fwhm = 2.5
+    vconv = (job.vwave[0] + 0.3 + np.arange(0, 78, 1.0)).astype(np.float32)
+    got = ctx.cirsconv(job.vwave, series, fwhm, vconv)
+    for s in range(series.shape[0]):
+        ref = oracle.cirsconv(job.vwave, series[s], fwhm, vconv)
+        scale = max(np.max(np.abs(ref)), 1e-30)
+        assert np.max(np.abs(got[s] - ref)) <= 1e-6 * scale, s
+    same = ctx.cirsconv(job.vwave, series[:1], 0.0, job.vwave)
+    assert np.array_equal(same[0], series[0])

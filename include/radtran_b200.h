@@ -372,11 +372,17 @@ int rtb_spd_inverse_batch(rtb_context* ctx, int nret, int n, const double* a, do
 /* One retrieval of the layer-state model: the state vector is
  *   x[l]          temperature of layer l, l < nlayer (model 0, one level
  *                 per layer: DTE = identity, npro = nlayer)
- *   x[nlayer + a] natural log of a scale factor of gas scale_gas[a]
- *                 (model 3, nemesis/subprofretg.f:735-741): amount, pp and
- *                 the gas's xmap column at state x are those of `atm` times
- *                 exp(x[nlayer + a])
- * so nx = nlayer + nscale.  `atm` is the atmosphere at scale factor 1 (its
+ *   x[nlayer + a] a scale factor of gas scale_gas[a]: model 3 (default,
+ *                 nemesis/subprofretg.f:735-750) the natural log of the
+ *                 factor, amount, pp and the gas's xmap rows those of `atm`
+ *                 times exp(x); model 2 (subprofretg.f:725-733) the factor
+ *                 itself, amount and pp times x, xmap rows unchanged
+ *   x[nlayer + nscale + p*nlayer + l]  natural log of the vmr of gas
+ *                 prof_gas[p] in layer l (model 0 for a gas,
+ *                 subprofretg.f:638-651): vmr = exp(x), the layer's amount
+ *                 and pp those of `atm` times vmr / vmr_atm (vmr_atm = pp /
+ *                 press), xmap row (l, gas, level l) = vmr
+ * so nx = nlayer + nscale + nprof * nlayer.  `atm` is the atmosphere at scale factor 1 (its
  * temp is replaced by x, emtemp follows temp through layinc); it must have
  * one path, and its xmap must hold the matching derivatives (T rows 1, gas
  * rows the gas's vmr per level).  Host pointers; read during the call only. */
@@ -389,6 +395,9 @@ typedef struct rtb_retrieval_spec {
     const double* sa;         /* [nx][nx] a priori covariance */
     const float* xa;          /* [nx] a priori state */
     const float* x0;          /* [nx] first guess; NULL = xa */
+    const int* scale_model;   /* [nscale] 3 or 2; NULL = all 3 */
+    int nprof;                /* gases retrieved as layer profiles */
+    const int* prof_gas;      /* [nprof] 0-based gas index (not also in scale_gas) */
 } rtb_retrieval_spec;
 
 typedef struct rtb_retrieval_opts {
@@ -416,8 +425,9 @@ typedef struct rtb_retrieval_result {
  * round runs one Newton step on the device for every retrieval whose K
  * changed, then one batched forward+Jacobian launch for every trial state,
  * then the cost on the device, and the coreret decision per retrieval
- * (accept: alambda *= 0.3; reject: *= 10, cap 1e10; trial states with T < 1
- * or a NaN are rejected before the forward model, coreret.f:642-790).
+ * (accept: alambda *= 0.3; reject: *= 10, cap 1e10; trial states with a NaN,
+ * a log variable beyond +-85, a negative model-2 scale or T < 1 are rejected
+ * before the forward model, coreret.f:642-790).
  * K, spectra, Se^-1, Sa^-1 and the states stay in device memory between
  * rounds. */
 int rtb_retrieve_batch(rtb_context* ctx, int nret, const rtb_retrieval_spec* specs,

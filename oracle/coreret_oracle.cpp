@@ -23,12 +23,14 @@ struct Work {
     int L = 0, NV = 0, nparam = 0, NW = 0;
     std::vector<float> temp, pp, amount, emtemp, xmap, pp0, amount0, xmap0;
     std::vector<float> press, delh, scale, dte, dam, vwave;
-    std::vector<int> layinc, idgas, isogas, ktab, nlayin, imod, sg;
+    std::vector<int> layinc, idgas, isogas, ktab, nlayin, imod, sg, sm, pg;
+    std::vector<float> vmr0;   /* [nprof][L] pp / press of the profiled gases */
 };
 
 int setup(const rtb_retrieval_spec& s, Work& w) {
     const rtb_atm& t = *s.atm;
-    if (t.npath != 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale || t.ncont != 0) return RTB_ERR_UNSUPPORTED;
+    if (t.npath != 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont != 0)
+        return RTB_ERR_UNSUPPORTED;
     const int L = t.nlayer, G = t.ngas, NV = t.nv, NW = t.nwave;
     const int ldl = t.ld_lay > 0 ? t.ld_lay : RTB_MAXLAY;
     const int ldv = t.ld_v > 0 ? t.ld_v : RTB_MAXV;
@@ -38,6 +40,9 @@ int setup(const rtb_retrieval_spec& s, Work& w) {
     w.NW = NW;
     w.nparam = G + 1;
     w.sg.assign(s.scale_gas, s.scale_gas + s.nscale);
+    w.sm.assign(s.nscale, 3);
+    if (s.scale_model) w.sm.assign(s.scale_model, s.scale_model + s.nscale);
+    w.pg.assign(s.prof_gas, s.prof_gas + s.nprof);
     auto col = [&](const float* p, int n, std::vector<float>& v) {
         v.resize((size_t)L * n);
         for (int j = 0; j < n; ++j)
@@ -62,6 +67,9 @@ int setup(const rtb_retrieval_spec& s, Work& w) {
             for (int i = 0; i < NV; ++i)
                 w.xmap0[i + (size_t)NV * (j + (size_t)w.nparam * k)] = t.xmap[i + (size_t)ldv * (j + (size_t)ldp * k)];
     w.xmap = w.xmap0;
+    w.vmr0.resize((size_t)s.nprof * L);
+    for (int p = 0; p < s.nprof; ++p)
+        for (int l = 0; l < L; ++l) w.vmr0[(size_t)p * L + l] = w.pp0[l + (size_t)L * s.prof_gas[p]] / w.press[l];
     w.vwave.assign(t.vwave, t.vwave + NW);
     w.idgas.assign(t.idgas, t.idgas + G);
     w.isogas.assign(t.isogas, t.isogas + G);
@@ -98,9 +106,11 @@ void at_state(Work& w, const float* x) {
     const int L = w.L;
     for (int l = 0; l < L; ++l) w.temp[l] = x[l];
     for (int j = 0; j < w.nlayin[0]; ++j) w.emtemp[j] = w.temp[w.layinc[j] - 1];
-    for (size_t a = 0; a < w.sg.size(); ++a) {
+    const int ns = (int)w.sg.size();
+    for (int a = 0; a < ns; ++a) {
         const int g = w.sg[a];
-        const float f = expf(x[L + a]);                  /* REAL EXP of subprofretg.f:746 */
+        const bool lin = w.sm[a] == 2;                   /* model 2: X1 = XREF*XN (subprofretg.f:725-733) */
+        const float f = lin ? x[L + a] : expf(x[L + a]); /* model 3: REAL EXP of subprofretg.f:746 */
         for (int l = 0; l < L; ++l) {
             w.amount[l + (size_t)L * g] = w.amount0[l + (size_t)L * g] * f;
             w.pp[l + (size_t)L * g] = w.pp0[l + (size_t)L * g] * f;
@@ -108,8 +118,21 @@ void at_state(Work& w, const float* x) {
         for (int k = 0; k < L; ++k)
             for (int i = 0; i < w.NV; ++i) {
                 const size_t idx = i + (size_t)w.NV * (g + (size_t)w.nparam * k);
-                w.xmap[idx] = w.xmap0[idx] * f;
+                w.xmap[idx] = lin ? w.xmap0[idx] : w.xmap0[idx] * f;
             }
+    }
+    /* model 0 for a gas: X1(I) = EXP(XN(I)), XMAP(I, IPAR, I) = X1(I) (subprofretg.f:638-651) */
+    for (size_t p = 0; p < w.pg.size(); ++p) {
+        const int g = w.pg[p];
+        const int base = L + ns + (int)p * L;
+        for (int l = 0; l < L; ++l) {
+            const float v = expf(x[base + l]);
+            const float f = v / w.vmr0[p * L + l];
+            w.amount[l + (size_t)L * g] = w.amount0[l + (size_t)L * g] * f;
+            w.pp[l + (size_t)L * g] = w.pp0[l + (size_t)L * g] * f;
+            for (int k = 0; k < L; ++k)
+                w.xmap[(base + l) + (size_t)w.NV * (g + (size_t)w.nparam * k)] = k == l ? v : 0.0f;
+        }
     }
 }
 
@@ -175,11 +198,19 @@ int orc_retrieve(const orc_tables* tab, const rtb_retrieval_spec* s, const rtb_r
                 alambda = alambda * 10.0f;
                 if (alambda > 1e10f) alambda = 1e10f;
                 ok = false;
-            } else if (i >= L && (xn1[i] > 85.0f || xn1[i] < -85.0f)) {
+            } else if (i >= L && !(i < L + s->nscale && s->scale_model && s->scale_model[i - L] == 2) &&
+                       (xn1[i] > 85.0f || xn1[i] < -85.0f)) {   /* lx = 1: models 3 and gas model 0 */
                 alambda = 1e10f;
                 ok = false;
             }
         }
+        /* subprofretg ierr = 1: a vmr gone negative (model-2 scale < 0), coreret.f:683-700 */
+        for (int a = 0; a < s->nscale && ok; ++a)
+            if (s->scale_model && s->scale_model[a] == 2 && xn1[L + a] < 0.0f) {
+                alambda = alambda * 10.0f;
+                if (alambda > 1e10f) alambda = 1e10f;
+                ok = false;
+            }
         for (int i = 0; i < L && ok; ++i)
             if (xn1[i] < 1.0f) {
                 alambda = alambda * 10.0f;

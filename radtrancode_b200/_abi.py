@@ -61,6 +61,7 @@ class RtbRetrievalSpec(C.Structure):
         ("atm", C.POINTER(RtbAtm)), ("nscale", C.c_int), ("scale_gas", _ip),
         ("y", _fp), ("sei", C.POINTER(C.c_double)), ("sa", C.POINTER(C.c_double)),
         ("xa", _fp), ("x0", _fp),
+        ("scale_model", _ip), ("nprof", C.c_int), ("prof_gas", _ip),
     ]
 
 

@@ -49,7 +49,8 @@ struct AtmWork {
     std::vector<float> press, temp, delh, pp, amount, cont, scale, emtemp, dte, dam, dco, xmap, vwave, xsec;
     std::vector<int> idgas, isogas, ktab, nlayin, imod, layinc;
     std::vector<float> pp0, amount0, xmap0;   // at scale factor 1
-    std::vector<int> scale_gas;
+    std::vector<int> scale_gas, scale_model, prof_gas;
+    std::vector<float> vmr0;                  // [nprof][L] pp0 / press of the profiled gases
 };
 
 int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
@@ -62,7 +63,9 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     const int nparam = G + 1 + NC;
     if (NP != 1) return fail(c, RTB_ERR_UNSUPPORTED, "retrieval atmosphere must have one path (npath=%d)", NP);
     if (NPRO != L) return fail(c, RTB_ERR_UNSUPPORTED, "layer-state model needs npro == nlayer");
-    if (NV != L + s.nscale) return fail(c, RTB_ERR_ARG, "nv=%d but nlayer + nscale = %d", NV, L + s.nscale);
+    if (s.nprof < 0 || (s.nprof > 0 && !s.prof_gas)) return fail(c, RTB_ERR_ARG, "nprof/prof_gas");
+    if (NV != L + s.nscale + s.nprof * L)
+        return fail(c, RTB_ERR_ARG, "nv=%d but nlayer + nscale + nprof*nlayer = %d", NV, L + s.nscale + s.nprof * L);
     if (NV > kNewtonMaxNx) return fail(c, RTB_ERR_UNSUPPORTED, "state size %d > %d", NV, kNewtonMaxNx);
     if (NV >= NW) return fail(c, RTB_ERR_UNSUPPORTED, "nx=%d >= ny=%d (calc_gain_matrix nx<ny branch only)", NV, NW);
     if (!t.press || !t.temp || !t.delh || !t.pp || !t.amount || !t.idgas || !t.isogas || !t.ktab || !t.nlayin ||
@@ -73,8 +76,19 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     for (int a = 0; a < s.nscale; ++a)
         if (!s.scale_gas || s.scale_gas[a] < 0 || s.scale_gas[a] >= G)
             return fail(c, RTB_ERR_ARG, "scale_gas[%d] outside 0..ngas-1", a);
+    for (int a = 0; a < s.nscale; ++a)
+        if (s.scale_model && !(s.scale_model[a] == 2 || s.scale_model[a] == 3))
+            return fail(c, RTB_ERR_UNSUPPORTED, "scale_model[%d]=%d (models 2 and 3 only)", a, s.scale_model[a]);
+    for (int p = 0; p < s.nprof; ++p) {
+        if (s.prof_gas[p] < 0 || s.prof_gas[p] >= G) return fail(c, RTB_ERR_ARG, "prof_gas[%d] outside gases", p);
+        for (int a = 0; a < s.nscale; ++a)
+            if (s.scale_gas[a] == s.prof_gas[p]) return fail(c, RTB_ERR_ARG, "gas %d both scaled and profiled", s.prof_gas[p]);
+    }
     w.nparam = nparam;
     w.scale_gas.assign(s.scale_gas, s.scale_gas + s.nscale);
+    w.scale_model.assign(s.nscale, 3);
+    if (s.scale_model) w.scale_model.assign(s.scale_model, s.scale_model + s.nscale);
+    w.prof_gas.assign(s.prof_gas, s.prof_gas + s.nprof);
     auto lay1 = [&](const float* p, std::vector<float>& v) { v.assign(p, p + L); };
     auto lay2 = [&](const float* p, int ncols, std::vector<float>& v) {
         v.resize((size_t)L * ncols);
@@ -108,6 +122,9 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
             for (int i = 0; i < NV; ++i)
                 w.xmap0[i + (size_t)NV * (j + (size_t)nparam * k)] = t.xmap[i + (size_t)ldv * (j + (size_t)ldp * k)];
     w.xmap = w.xmap0;
+    w.vmr0.resize((size_t)s.nprof * L);
+    for (int p = 0; p < s.nprof; ++p)
+        for (int l = 0; l < L; ++l) w.vmr0[(size_t)p * L + l] = w.pp0[l + (size_t)L * s.prof_gas[p]] / w.press[l];
     w.vwave.assign(t.vwave, t.vwave + NW);
     w.idgas.assign(t.idgas, t.idgas + G);
     w.isogas.assign(t.isogas, t.isogas + G);
@@ -152,9 +169,11 @@ void set_state(AtmWork& w, const float* x) {
     for (int l = 0; l < L; ++l) w.temp[l] = x[l];
     const int nl = w.nlayin[0];
     for (int j = 0; j < nl; ++j) w.emtemp[j] = w.temp[w.layinc[j] - 1];
-    for (size_t a = 0; a < w.scale_gas.size(); ++a) {
+    const int ns = (int)w.scale_gas.size();
+    for (int a = 0; a < ns; ++a) {
         const int g = w.scale_gas[a];
-        const float f = expf(x[L + a]);
+        const bool lin = w.scale_model[a] == 2;
+        const float f = lin ? x[L + a] : expf(x[L + a]);
         for (int l = 0; l < L; ++l) {
             w.amount[l + (size_t)L * g] = w.amount0[l + (size_t)L * g] * f;
             w.pp[l + (size_t)L * g] = w.pp0[l + (size_t)L * g] * f;
@@ -162,8 +181,20 @@ void set_state(AtmWork& w, const float* x) {
         for (int k = 0; k < NPRO; ++k)
             for (int i = 0; i < NV; ++i) {
                 const size_t idx = i + (size_t)NV * (g + (size_t)nparam * k);
-                w.xmap[idx] = w.xmap0[idx] * f;
+                w.xmap[idx] = lin ? w.xmap0[idx] : w.xmap0[idx] * f;
             }
+    }
+    // model-0 gas profiles: vmr = EXP(XN) per layer, xmap = vmr on its own level
+    for (size_t p = 0; p < w.prof_gas.size(); ++p) {
+        const int g = w.prof_gas[p];
+        const int base = L + ns + (int)p * L;
+        for (int l = 0; l < L; ++l) {
+            const float v = expf(x[base + l]);
+            const float f = v / w.vmr0[p * L + l];
+            w.amount[l + (size_t)L * g] = w.amount0[l + (size_t)L * g] * f;
+            w.pp[l + (size_t)L * g] = w.pp0[l + (size_t)L * g] * f;
+            for (int k = 0; k < NPRO; ++k) w.xmap[(base + l) + (size_t)NV * (g + (size_t)nparam * k)] = k == l ? v : 0.0f;
+        }
     }
 }
 
@@ -175,6 +206,7 @@ void set_state(AtmWork& w, const float* x) {
 struct Slot {
     long long id = 0;
     int nx = 0, ny = 0, nlayer = 0;
+    std::vector<unsigned char> kind;  // per state element: 0 T, 1 log variable (lx = 1), 2 linear scale
     size_t bytes = 0, off = 0;        // arena block
     int xrow = -1;                    // row of the state area
     int phase = 0;                    // 0: first forward model pending; 1: iterating
@@ -209,11 +241,16 @@ bool make_trial(Slot& R) {
             R.alambda = std::min(R.alambda * 10.0f, 1e10f);
             return false;
         }
-        if (i >= R.nlayer && (R.xn1[i] > 85.0f || R.xn1[i] < -85.0f)) {   // :651-666, lx = 1 for model 3
+        if (R.kind[i] == 1 && (R.xn1[i] > 85.0f || R.xn1[i] < -85.0f)) {   // :651-666, log variables (lx = 1)
             R.alambda = 1e10f;
             return false;
         }
     }
+    for (int i = 0; i < nx; ++i)                             // :683-700, a vmr gone negative (model 2)
+        if (R.kind[i] == 2 && R.xn1[i] < 0.0f) {
+            R.alambda = std::min(R.alambda * 10.0f, 1e10f);
+            return false;
+        }
     for (int i = 0; i < R.nlayer; ++i)                       // model-0 temperature
         if (R.xn1[i] < 1.0f) {
             R.alambda = std::min(R.alambda * 10.0f, 1e10f);
@@ -350,6 +387,9 @@ struct Engine {
         }
         s->nlayer = sp.atm->nlayer;
         s->nx = sp.atm->nv;
+        s->kind.assign(s->nx, 1);
+        for (int l = 0; l < s->nlayer; ++l) s->kind[l] = 0;
+        for (int a = 0; a < sp.nscale; ++a) s->kind[s->nlayer + a] = (sp.scale_model && sp.scale_model[a] == 2) ? 2 : 1;
         s->ny = sp.atm->nwave;
         s->bytes = slot_bytes(s->nx, s->ny);
         if (s->bytes > budget) {

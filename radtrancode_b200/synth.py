@@ -311,6 +311,8 @@ class RetrievalCase:
     x_true: np.ndarray         # float32 [nx]
     y: np.ndarray | None = None
     x0: np.ndarray | None = None
+    scale_model: np.ndarray | None = None   # int32 [nscale], 3 (log) or 2 (linear); None = all 3
+    prof_gas: np.ndarray | None = None      # int32 [nprof] gases retrieved as log-vmr layer profiles
 
     @property
     def nx(self):
@@ -331,7 +333,11 @@ class RetrievalCase:
         s.sa = _abi.dptr(self.sa)
         s.xa = _abi.fptr(self.xa)
         s.x0 = _abi.fptr(self.x0)
-        s._keep = (self, atm)
+        s.scale_model = _abi.iptr(self.scale_model)
+        pg = self.prof_gas if self.prof_gas is not None else np.zeros(0, np.int32)
+        s.nprof = len(pg)
+        s.prof_gas = _abi.iptr(pg) if len(pg) else None
+        s._keep = (self, atm, pg)
         return s
 
 
@@ -348,22 +354,49 @@ def prior_covariance(p_lay, n_scale, sig_t=3.0, sig_scale=0.5, clen=1.5):
 
 
 def make_retrieval(tables: KTables, absorbers, *, nlayer, seed, iw0=0, nwave=None, theta_deg=0.0,
-                   noise=1e-9, vmr_perturb=0.3) -> RetrievalCase:
+                   noise=1e-9, vmr_perturb=0.3, scale_model=None, profile=()) -> RetrievalCase:
     """Retrieval case with a priori = smooth T profile and unit gas scales;
     the true state is a seeded draw from Sa.  The measurement y is set by
-    the caller (forward model at x_true plus noise, see `observe`)."""
+    the caller (forward model at x_true plus noise, see `observe`).
+    scale_model: per scaled absorber 3 (log scale, a priori 0) or 2 (linear
+    scale, a priori 1); profile: indices into `absorbers` retrieved as
+    log-vmr layer profiles (a priori the job's vmr, 50 %, correlated over
+    1.5 scale heights) instead of a scale."""
     rng = np.random.default_rng(seed)
     p_lev, p_lay = _levels(nlayer)
     t_prior = temperature_profile(p_lay, rng, noise=0.0)
     job = make_job(tables, absorbers, nlayer=nlayer, seed=seed + 1, iw0=iw0, nwave=nwave, theta_deg=theta_deg,
                    vmr_perturb=vmr_perturb, temp=t_prior)
-    ns = len(absorbers)
-    xa = np.concatenate([t_prior, np.zeros(ns)]).astype(np.float32)
-    sa = prior_covariance(p_lay, ns)
-    x_true = (xa + np.linalg.cholesky(sa) @ rng.standard_normal(len(xa))).astype(np.float32)
+    L = nlayer
+    prof = [int(a) for a in profile]
+    scaled = [a for a in range(len(absorbers)) if a not in prof]
+    ns, npf = len(scaled), len(prof)
+    sm = np.array(scale_model if scale_model is not None else [3] * ns, np.int32)
+    nv = L + ns + npf * L
+    xmap = np.zeros((nv, job.nparam, L), np.float32, order="F")
+    idx = np.arange(L)
+    xmap[idx, job.ngas, idx] = 1.0
+    for k, a in enumerate(scaled):
+        xmap[L + k, 2 + a, :] = job.vmr[:, 2 + a].astype(np.float32)
+    for k, a in enumerate(prof):
+        xmap[L + ns + k * L + idx, 2 + a, idx] = job.vmr[:, 2 + a].astype(np.float32)
+    job = dataclasses.replace(job, nv=nv, ld_v=nv, xmap=xmap)
+    xa = np.concatenate([t_prior, np.where(sm == 2, 1.0, 0.0)] +
+                        [np.log(job.vmr[:, 2 + a]) for a in prof]).astype(np.float32)
+    sa = np.zeros((nv, nv))
+    sa[:L + ns, :L + ns] = prior_covariance(p_lay, ns)
+    lnp = np.log(p_lay)
+    for k in range(npf):
+        o = L + ns + k * L
+        sa[o:o + L, o:o + L] = 0.25 * np.exp(-np.abs(lnp[:, None] - lnp[None, :]) / 1.5)
+    x_true = (xa + np.linalg.cholesky(sa) @ rng.standard_normal(nv)).astype(np.float32)
+    for k in range(ns):
+        if sm[k] == 2:
+            x_true[L + k] = max(x_true[L + k], np.float32(0.05))
     sei = np.full(job.nwave, 1.0 / (noise * noise))
-    return RetrievalCase(job=job, scale_gas=np.arange(2, 2 + ns, dtype=np.int32), xa=xa, sa=sa, sei=sei,
-                         x_true=x_true)
+    return RetrievalCase(job=job, scale_gas=np.array([2 + a for a in scaled], np.int32), xa=xa, sa=sa, sei=sei,
+                         x_true=x_true, scale_model=sm if scale_model is not None else None,
+                         prof_gas=np.array([2 + a for a in prof], np.int32) if npf else None)
 
 
 def observe(case: RetrievalCase, spectrum, seed, noise=1e-9):

@@ -171,6 +171,32 @@ def test_retrieve_batch_matches_oracle(ctx, oracle, c1, hess):
         assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
 
 
+def test_retrieve_scale_model_2_and_gas_profile_match_oracle(ctx, oracle):
+    """A linear (model 2) scale of CH4 and a log-vmr layer profile of NH3
+    (model 0 for a gas) beside the temperatures: same iterations, forward
+    evaluations and stop rule as the oracle's coreret loop, states within
+    1e-3 prior sigma, cost within 1e-3."""
+    kt, cia, _ = synth.config2()
+    case = synth.make_retrieval(kt, [synth.CH4, synth.NH3], nlayer=40, seed=41, nwave=120, scale_model=[2],
+                                profile=[1])
+    y_true, _ = oracle.forward_state(kt, cia, case, case.x_true, nthreads=8)
+    synth.observe(case, y_true, seed=42)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ref, tr = oracle.retrieve(kt, cia, case, kiter=10, phlimit=0.1, nthreads=8)
+    sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
+    for hess in (1, 0):
+        ctx.set_newton_mode(hess, 1)
+        try:
+            g = ctx.retrieve_batch([case], kiter=10, phlimit=0.1)[0]
+        finally:
+            ctx.set_newton_mode(0, 1)
+        assert (g["converged"], g["iterations"], g["forwards"]) == (ref["converged"], ref["iterations"],
+                                                                   ref["forwards"])
+        assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
+        assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
+
+
 def test_retrieve_batch_result_independent_of_batch(ctx, c1):
     kt, cia, cases = c1
     ctx.set_ktables(kt)

@@ -65,6 +65,15 @@ int pindex_f(const float* x, int nx, float& x1) {
     return j;
 }
 
+// PINDEX on an ascending grid: the loop above stops at the first point above
+// x1, so its result is the number of the first nx-1 points <= x1, found here
+// by bisection (the same index)
+int pindex_ascending(const float* x, int nx, float& x1) {
+    if (x1 > x[nx - 1]) x1 = x[nx - 1];
+    if (x1 < x[0]) x1 = x[0];
+    return (int)(std::upper_bound(x, x + nx - 1, x1) - x);
+}
+
 // RAYLEIGHJ (radtran/scatter/rayleighj.f) with faniso(0) = 1
 float rayleighj_f(float v) {
     const float AH2 = 13.58E-5f, BH2 = 7.52E-3f, AHe = 3.48E-5f, BHe = 2.30E-3f;
@@ -322,7 +331,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         W.cia_cv = -1;
         if (c->has_cia && !(vv > vvk1[RTB_CIA_NUMWN - 1] || vv < vvk1[0])) {
             float vvc = vv;
-            const int cv = pindex_f(vvk1.data(), RTB_CIA_NUMWN, vvc);
+            const int cv = pindex_ascending(vvk1.data(), RTB_CIA_NUMWN, vvc);   // vvk1(i) = (i-1)*dnu
             W.cia_cv = cv - 1;
             W.cia_t = (vv - vvk1[cv - 1]) / (vvk1[cv] - vvk1[cv - 1]);
         }
@@ -403,38 +412,74 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
                     if (v != 0.0f) xm[(size_t)k * npro + lev].push_back({iv, v});
                 }
         }
+        // levels with a nonzero d(layer)/d(level) entry, per layer, for each of dam, dte, dco
+        const float* mats[3] = {a.dam, a.dte, a.dco};
+        std::vector<std::pair<int, float>> nzl[3];
+        std::vector<int> nzl_ptr[3];
+        for (int q = 0; q < 3; ++q) {
+            if (!mats[q]) continue;
+            nzl_ptr[q].assign(a.nlayer + 1, 0);
+            for (int lay = 0; lay < a.nlayer; ++lay) {
+                for (int lev = 0; lev < npro; ++lev) {
+                    const float m = mats[q][lay + (size_t)d.ld_lay * lev];
+                    if (m != 0.0f) nzl[q].push_back({lev, m});
+                }
+                nzl_ptr[q][lay + 1] = (int)nzl[q].size();
+            }
+        }
+        // Each (iv, j, s) entry sums m * xmap over levels in ascending order,
+        // as a dense accumulation over (s, j, lev) would; the entries are then
+        // ordered by iv (stable, so rows stay ascending within a column).
+        std::vector<double> acc(nv, 0.0);
+        std::vector<uint8_t> hit(nv, 0);
+        std::vector<int> ivs, trip_iv, trip_r, cnt(nv + 1);
+        std::vector<float> trip_v;
+        ivs.reserve(nv);
         for (int ip = 0; ip < a.npath; ++ip) {
             const int nl = a.nlayin[ip];
-            std::vector<double> T((size_t)nv * nlmax * std::max(nsw, 1), 0.0);
-            std::vector<uint8_t> touched(T.size(), 0);
-            for (int s = 0; s < nsw; ++s) {
-                const int k = isw[s];
-                const float* M = k < a.ngas ? a.dam : (k == a.ngas ? a.dte : a.dco);
-                if (!M) continue;
-                for (int j = 0; j < nl; ++j) {
-                    const int lay = a.layinc[j + (size_t)d.ld_lay * ip] - 1;
-                    for (int lev = 0; lev < npro; ++lev) {
-                        const float m = M[lay + (size_t)d.ld_lay * lev];
-                        if (m == 0.0f) continue;
-                        for (const auto& e : xm[(size_t)k * npro + lev]) {
-                            const size_t idx = (size_t)e.first * nlmax * nsw + (size_t)j * nsw + s;
-                            T[idx] += (double)m * (double)e.second;
-                            touched[idx] = 1;
+            trip_iv.clear();
+            trip_r.clear();
+            trip_v.clear();
+            for (int j = 0; j < nl; ++j) {
+                const int lay = a.layinc[j + (size_t)d.ld_lay * ip] - 1;
+                for (int s = 0; s < nsw; ++s) {
+                    const int k = isw[s];
+                    const int q = k < a.ngas ? 0 : (k == a.ngas ? 1 : 2);
+                    if (!mats[q]) continue;
+                    for (int e = nzl_ptr[q][lay]; e < nzl_ptr[q][lay + 1]; ++e) {
+                        const int lev = nzl[q][e].first;
+                        const double m = (double)nzl[q][e].second;
+                        for (const auto& x : xm[(size_t)k * npro + lev]) {
+                            if (!hit[x.first]) {
+                                hit[x.first] = 1;
+                                ivs.push_back(x.first);
+                            }
+                            acc[x.first] += m * (double)x.second;
                         }
                     }
-                }
-            }
-            for (int iv = 0; iv < nv; ++iv) {
-                st.map_colptr.push_back((int)st.map_row.size());
-                for (int r = 0; r < nlmax * nsw; ++r) {
-                    const size_t idx = (size_t)iv * nlmax * nsw + r;
-                    if (touched[idx]) {
-                        st.map_row.push_back(r);
-                        st.map_val.push_back((float)T[idx]);
+                    for (int iv : ivs) {
+                        trip_iv.push_back(iv);
+                        trip_r.push_back(j * nsw + s);
+                        trip_v.push_back((float)acc[iv]);
+                        acc[iv] = 0.0;
+                        hit[iv] = 0;
                     }
+                    ivs.clear();
                 }
             }
-            st.map_colptr.push_back((int)st.map_row.size());
+            std::fill(cnt.begin(), cnt.end(), 0);
+            for (int iv : trip_iv) ++cnt[iv + 1];
+            for (int iv = 0; iv < nv; ++iv) cnt[iv + 1] += cnt[iv];
+            const int base = (int)st.map_row.size();
+            for (int iv = 0; iv < nv; ++iv) st.map_colptr.push_back(base + cnt[iv]);
+            st.map_colptr.push_back(base + cnt[nv]);
+            st.map_row.resize(base + trip_iv.size());
+            st.map_val.resize(base + trip_iv.size());
+            for (size_t t = 0; t < trip_iv.size(); ++t) {
+                const int at = base + cnt[trip_iv[t]]++;
+                st.map_row[at] = trip_r[t];
+                st.map_val[at] = trip_v[t];
+            }
         }
     }
     S.out_off = st.n_out;

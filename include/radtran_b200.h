@@ -117,6 +117,26 @@ int rtb_load_cia(rtb_context* ctx, const char* path, float dnu);
 /* Forward model + Jacobian (cirsrtfg_wave replacement)                    */
 /* ---------------------------------------------------------------------- */
 
+/* The channels of the instrument convolution, cirsconv (radtran/cirsrad/
+ * cirsconv.f:12-246), as cirsrtfg_wave hands them over (vconv, nconv and the
+ * .fwh / .fil files it reads, cirsrtfg_wave.f:185-198, cirsconv.f:183-196). */
+typedef struct rtb_conv {
+    int nconv;
+    const float* vconv;      /* (nconv) channel centres */
+    /* FWHM > 0 only: the channel-dependent bin width of a .fwh file
+     * (FWHMEXIST), VERINT-interpolated at each channel; nfwhm = 0 for none */
+    int nfwhm;
+    const float* vfwhm;      /* (nfwhm) */
+    const float* xfwhm;      /* (nfwhm) */
+    /* FWHM < 0 only: the filter functions of a .fil file; filter k is centred
+     * at vcen[k] and has nsub[k] points (vfil, fil), filters concatenated */
+    int nfil;
+    const float* vcen;       /* (nfil) */
+    const int* nsub;         /* (nfil) */
+    const float* vfil;       /* (sum nsub) */
+    const float* fil;        /* (sum nsub) */
+} rtb_conv;
+
 /* One call of cirsrtfg_wave after its set-up (subpathg + read_klist): the
  * layer/path arrays of /LAYCOM/ and /PATHCOM/, the gradient matrices of
  * /LGRAD/ and the state mapping xmap, by pointer, in Fortran layout.
@@ -161,13 +181,17 @@ typedef struct rtb_atm {
     int   nem;
     const float* vem;        /* (nem) */
     const float* emissivity; /* (nem) */
+    /* instrument channels; NULL means FWHM = 0 with nconv = nwave (the
+     * outputs are on the calculation grid) */
+    const rtb_conv* conv;
 } rtb_atm;
 
-/* Outputs, packed as cirsrtfg_wave packs them (cirsrtfg_wave.f:425-446,
- * FWHM = 0 so cirsconv is the identity and nconv = nwave):
- *   calcout[nwave*ipath + iwave]
- *   gradients[nwave*nv*ipath + nwave*iv + iwave]
- *   gradtsurf[nwave*ipath + iwave]            (may be NULL)                */
+/* Outputs, convolved by cirsconv with atm->fwhm onto the channels of
+ * atm->conv (nconv = nwave when conv is NULL) and packed as cirsrtfg_wave
+ * packs them (cirsrtfg_wave.f:448-516):
+ *   calcout[nconv*ipath + iconv]
+ *   gradients[nconv*nv*ipath + nconv*iv + iconv]
+ *   gradtsurf[nconv*ipath + iconv]            (may be NULL)                */
 int rtb_cirsrtfg_wave(rtb_context* ctx, const rtb_atm* atm,
                       float* calcout, float* gradients, float* gradtsurf);
 
@@ -178,16 +202,35 @@ int rtb_cirsrtfg_wave_batch(rtb_context* ctx, int nspec, const rtb_atm* atms,
                             float* const* calcout, float* const* gradients,
                             float* const* gradtsurf);
 
-/* Instrument convolution, cirsconv (radtran/cirsrad/cirsconv.f:12-160), of
- * nser series y[nser][nwave] on the calculation grid vwave to nconv channels
- * vconv: FWHM > 0 averages a natural cubic spline of each series over a
- * square bin of width fwhm (20-point trapezoid); FWHM = 0 copies (nconv must
- * equal nwave); FWHM < 0 (filter-file channels) is not implemented.  With
- * rtb_cirsrtfg_wave called at FWHM = 0 this gives cirsrtfg_wave's outputs for
- * FWHM > 0 (cirsrtfg_wave.f:448-516 convolves calcout, gradtsurf and every
- * Jacobian row the same way).  yout[nser][nconv]. */
+/* Instrument convolution, cirsconv (radtran/cirsrad/cirsconv.f:12-246), of
+ * nser series y[nser][nwave] on the calculation grid vwave to the channels
+ * of conv, yout[nser][conv->nconv]:
+ *   FWHM > 0  a natural cubic spline of each series averaged over a square
+ *             bin of width fwhm (or the .fwh width at the channel) by a
+ *             20-point trapezoid, divided by fwhm;
+ *   FWHM = 0  a copy of the first nconv points (nconv <= nwave);
+ *   FWHM < 0  the mean of the series weighted by the channel's filter
+ *             function (the last filter centred within 1e-5 of the channel;
+ *             a channel without one is refused);
+ *   nwave = 1 and FWHM != 0: 1 (cirsconv.f:45-54; nconv must be 1).
+ * rtb_cirsrtfg_wave applies the same convolution to its outputs. */
+int rtb_cirsconv_ex(rtb_context* ctx, float fwhm, int nwave, const float* vwave, int nser, const float* y,
+                    const rtb_conv* conv, float* yout);
+/* The same with channel centres only (FWHM >= 0; FWHM = 0 needs nconv ==
+ * nwave). */
 int rtb_cirsconv(rtb_context* ctx, int nwave, const float* vwave, int nser, const float* y, float fwhm,
                  int nconv, const float* vconv, float* yout);
+
+/* The text files of the convolution, read on the host (no context needed):
+ * rtb_read_fwh reads a .fwh file (cirsrtfg_wave.f:191-196: NFWHM, then NFWHM
+ * lines VFWHM XFWHM); rtb_read_fil reads a .fil file (cirsconv.f:185-196:
+ * NCONV1, then per filter VCENTRAL, NSUB and NSUB lines VFIL FIL).  Called
+ * with NULL arrays they return the counts only (*n, or *nfil and *npts =
+ * sum of nsub); otherwise cap is the capacity of the arrays (points) and a
+ * larger file is refused with RTB_ERR_LIMIT. */
+int rtb_read_fwh(const char* path, int* n, float* v, float* x, int cap);
+int rtb_read_fil(const char* path, int* nfil, int* npts, float* vcen, int* nsub, float* vfil, float* fil,
+                 int cap_fil, int cap_pts);
 
 /* Per-wavenumber compatibility form of cirsradg_wave (radtran/cirsradg/
  * cirsradg_wave.f:1-5, outputs :1240-1267) for A/B checks against the

@@ -266,8 +266,8 @@ float orc_calc_phiret_diag(int ny, const float* y, const float* yn, const double
 
 }  // extern "C"
 
-/* ---- instrument convolution (radtran/cirsrad/cirsconv.f:12-160, FWHM > 0
- * and FWHM = 0) with CSPLINE (rtm_util/cspline.f) and CSPLINT
+/* ---- instrument convolution (radtran/cirsrad/cirsconv.f:12-246: FWHM > 0
+ * with an optional .fwh width table, FWHM = 0, FWHM < 0 filter channels) with CSPLINE (rtm_util/cspline.f) and CSPLINT
  * (rtm_util/csplint.f); REAL arithmetic as the reference, DOUBLE sums. ---- */
 namespace {
 void cspline_nat(const float* X, const float* Y, int N, float* Y2, std::vector<float>& U) {
@@ -306,13 +306,68 @@ float csplint(const float* XA, const float* YA, const float* Y2A, int N, float X
 }
 }  // namespace
 
-extern "C" int orc_cirsconv(int nwave, const float* vwave, const float* y, float fwhm, int nconv,
-                            const float* vconv, float* yout) {
-    if (fwhm == 0.0f) {
+namespace {
+/* INTERP (rtm_util/interp.f:24-37); with verint, VERINT (radtran/path/verint.f:29-46) */
+float interp_f(const float* X, const float* Y, int N, float XIN, bool verint) {
+    int I = N;
+    if (X[0] < X[N - 1]) {
+        for (int k = 1; k <= N; ++k)
+            if (X[k - 1] > XIN) { I = k; break; }
+    } else {
+        for (int k = 1; k <= N; ++k)
+            if (X[k - 1] < XIN) { I = k; break; }
+    }
+    if (I == 1) I = 2;
+    float YOUT = Y[I - 2] + (Y[I - 1] - Y[I - 2]) * (XIN - X[I - 2]) / (X[I - 1] - X[I - 2]);
+    if (verint) {
+        if (X[I - 2] == X[I - 1]) YOUT = Y[I - 1];
+        if (std::isnan(YOUT)) YOUT = Y[I - 1];
+    }
+    return YOUT;
+}
+}  // namespace
+
+extern "C" int orc_cirsconv_ex(float fwhm, int nwave, const float* vwave, const float* y, int nconv,
+                               const float* vconv, int nfwhm, const float* vfwhm, const float* xfwhm, int nfil,
+                               const float* vcen, const int* nsub, const float* vfil, const float* fil,
+                               float* yout) {
+    if (nwave == 1 && fwhm != 0.0f) {          /* cirsconv.f:45-54 */
+        if (nconv != 1) return RTB_ERR_ARG;
+        yout[0] = 1.0f;
+        return RTB_OK;
+    }
+    if (fwhm == 0.0f) {                        /* cirsconv.f:162-169 */
         for (int i = 0; i < nconv; ++i) yout[i] = y[i];
         return RTB_OK;
     }
-    if (fwhm < 0.0f || nwave < 2) return RTB_ERR_UNSUPPORTED;
+    if (fwhm < 0.0f) {                         /* cirsconv.f:171-239 */
+        int off = 0;
+        std::vector<float> ytmp(nwave);
+        for (int k = 0; k < nfil; ++k) {
+            const float* VF = vfil + off;
+            const float* FF = fil + off;
+            const int ns = nsub[k];
+            off += ns;
+            for (int i = 0; i < nconv; ++i) {
+                const float dv = std::fabs(vcen[k] - vconv[i]);
+                if (!(dv < 0.00001f)) continue;
+                for (int j = 0; j < nwave; ++j)
+                    ytmp[j] = (vwave[j] >= VF[0] && vwave[j] <= VF[ns - 1]) ? interp_f(VF, FF, ns, vwave[j], false)
+                                                                             : 0.0f;
+                double sumf = 0.0, sum = 0.0;
+                for (int j = 0; j < nwave - 1; ++j)
+                    if (ytmp[j] != 0.0f) {
+                        const float delv = vwave[j + 1] - vwave[j];
+                        const float a = ytmp[j] * y[j] * delv;
+                        const float b = ytmp[j] * delv;
+                        sum = sum + (double)a;
+                        sumf = sumf + (double)b;
+                    }
+                yout[i] = (float)(sum / sumf);
+            }
+        }
+        return RTB_OK;
+    }
     std::vector<float> xc(vwave, vwave + nwave), yc(y, y + nwave);
     if (vconv[nconv - 1] > vwave[nwave - 1] - fwhm / 2.0f) {
         const float x = vconv[nconv - 1] + fwhm;
@@ -336,7 +391,9 @@ extern "C" int orc_cirsconv(int nwave, const float* vwave, const float* y, float
     cspline_nat(x1v.data(), y1v.data(), nc, y2.data(), u);
     const int nstep = 20;
     for (int i = 0; i < nconv; ++i) {
-        const float x1 = vconv[i] - fwhm / 2.0f, x2 = vconv[i] + fwhm / 2.0f;
+        float yfwhm = fwhm;                    /* cirsconv.f:147-150 */
+        if (nfwhm > 0) yfwhm = interp_f(vfwhm, xfwhm, nfwhm, vconv[i], true);
+        const float x1 = vconv[i] - yfwhm / 2.0f, x2 = vconv[i] + yfwhm / 2.0f;
         const float delx = (x2 - x1) / (float)(nstep - 1);
         double sum = 0.0, yold = 0.0;
         for (int j = 1; j <= nstep; ++j) {
@@ -349,4 +406,11 @@ extern "C" int orc_cirsconv(int nwave, const float* vwave, const float* y, float
         yout[i] = (float)(sum / (double)fwhm);
     }
     return RTB_OK;
+}
+
+extern "C" int orc_cirsconv(int nwave, const float* vwave, const float* y, float fwhm, int nconv,
+                            const float* vconv, float* yout) {
+    if (fwhm < 0.0f || (fwhm > 0.0f && nwave < 2)) return RTB_ERR_UNSUPPORTED;
+    return orc_cirsconv_ex(fwhm, nwave, vwave, y, nconv, vconv, 0, nullptr, nullptr, 0, nullptr, nullptr, nullptr,
+                           nullptr, yout);
 }

@@ -129,6 +129,13 @@ void orc_calc_serr_diag(int nx, int ny, int ldx, const float* sx_in, const float
  * trapezoid per channel; FWHM = 0: copy) */
 int orc_cirsconv(int nwave, const float* vwave, const float* y, float fwhm, int nconv, const float* vconv,
                  float* yout);
+/* cirsconv.f:12-246 in full: FWHM > 0 with an optional width table
+ * (vfwhm, xfwhm; nfwhm = 0 for none), FWHM = 0, FWHM < 0 with nfil filter
+ * functions (filter k: vcen[k], nsub[k] points of vfil/fil, concatenated),
+ * nwave = 1 with FWHM != 0 */
+int orc_cirsconv_ex(float fwhm, int nwave, const float* vwave, const float* y, int nconv, const float* vconv,
+                    int nfwhm, const float* vfwhm, const float* xfwhm, int nfil, const float* vcen, const int* nsub,
+                    const float* vfil, const float* fil, float* yout);
 /* dinvertm(jmod=2): Cholesky inverse with the A*Ainv check; returns icheck */
 int orc_dinvertm_chol(int n, int lda, const double* a, double* ainv);
 

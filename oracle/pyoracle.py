@@ -269,6 +269,24 @@ def calc_serr(sx, se_diag, dd, aa):
     return tuple(out)
 
 
+def cirsconv_ex(vwave, y, fwhm, channels):
+    """cirsconv.f:12-246 of one series onto ``channels`` (synth.Channels)."""
+    L = lib()
+    vwave = np.ascontiguousarray(vwave, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    ch = channels
+    yout = np.zeros(len(ch.vconv), np.float32)
+    nf = 0 if ch.vfwhm is None else len(ch.vfwhm)
+    nfil = 0 if ch.vcen is None else len(ch.vcen)
+    st = L.orc_cirsconv_ex(C.c_float(fwhm), len(vwave), _abi.fptr(vwave), _abi.fptr(y), len(ch.vconv),
+                           _abi.fptr(ch.vconv), nf, _abi.fptr(ch.vfwhm), _abi.fptr(ch.xfwhm), nfil,
+                           _abi.fptr(ch.vcen), _abi.iptr(ch.nsub), _abi.fptr(ch.vfil), _abi.fptr(ch.fil),
+                           _abi.fptr(yout))
+    if st != 0:
+        raise RuntimeError(f"oracle status {_abi.STATUS_NAMES.get(st, st)}")
+    return yout
+
+
 def cirsconv(vwave, y, fwhm, vconv):
     L = lib()
     vwave = np.ascontiguousarray(vwave, np.float32)

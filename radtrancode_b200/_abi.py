@@ -30,6 +30,14 @@ _fp = C.POINTER(C.c_float)
 _ip = C.POINTER(C.c_int)
 
 
+class RtbConv(C.Structure):
+    _fields_ = [
+        ("nconv", C.c_int), ("vconv", _fp),
+        ("nfwhm", C.c_int), ("vfwhm", _fp), ("xfwhm", _fp),
+        ("nfil", C.c_int), ("vcen", _fp), ("nsub", _ip), ("vfil", _fp), ("fil", _fp),
+    ]
+
+
 class RtbAtm(C.Structure):
     _fields_ = [
         ("nlayer", C.c_int), ("ngas", C.c_int), ("ncont", C.c_int), ("npath", C.c_int),
@@ -45,6 +53,7 @@ class RtbAtm(C.Structure):
         ("flagh2p", C.c_int), ("ilbl", C.c_int), ("inlte", C.c_int), ("iform", C.c_int),
         ("tsurf", C.c_float), ("fwhm", C.c_float),
         ("nem", C.c_int), ("vem", _fp), ("emissivity", _fp),
+        ("conv", C.POINTER(RtbConv)),
     ]
 
 

@@ -107,6 +107,12 @@ def lib() -> C.CDLL:
         L.rtb_calc_serr.restype = C.c_int
         L.rtb_cirsconv.argtypes = [vp, C.c_int, fp, C.c_int, fp, C.c_float, C.c_int, fp, fp]
         L.rtb_cirsconv.restype = C.c_int
+        L.rtb_cirsconv_ex.argtypes = [vp, C.c_float, C.c_int, fp, C.c_int, fp, C.POINTER(_abi.RtbConv), fp]
+        L.rtb_cirsconv_ex.restype = C.c_int
+        L.rtb_read_fwh.argtypes = [C.c_char_p, ip, fp, fp, C.c_int]
+        L.rtb_read_fwh.restype = C.c_int
+        L.rtb_read_fil.argtypes = [C.c_char_p, ip, ip, fp, ip, fp, fp, C.c_int, C.c_int]
+        L.rtb_read_fil.restype = C.c_int
         L.rtb_kta_header.argtypes = [C.c_char_p, ip, ip, ip, ip, fp, fp, ip, ip]
         L.rtb_kta_header.restype = C.c_int
         L.rtb_load_ktables.argtypes = [vp, C.c_int, C.POINTER(C.c_char_p), ip, ip]
@@ -130,5 +136,5 @@ EXPORTED = [
     "rtb_fwd_set_schedule", "rtb_fwd_autotune", "rtb_fwd_use_graph", "rtb_server_create", "rtb_server_destroy",
     "rtb_server_submit", "rtb_server_step", "rtb_server_poll", "rtb_calc_gain_matrix", "rtb_calcnextxn",
     "rtb_cirsradg_wave", "rtb_kta_header", "rtb_load_ktables", "rtb_load_cia",
-    "rtb_calc_serr", "rtb_cirsconv",
+    "rtb_calc_serr", "rtb_cirsconv", "rtb_cirsconv_ex", "rtb_read_fwh", "rtb_read_fil",
 ]

@@ -24,6 +24,33 @@ class RtbError(RuntimeError):
         self.status = status
 
 
+def _file_status(st, path):
+    if st != _abi.RTB_OK:
+        raise RtbError(st, f"cannot read {path}")
+
+
+def read_fwh(path):
+    """A .fwh file (cirsrtfg_wave.f:191-196): (vfwhm, xfwhm)."""
+    L = _lib.lib()
+    n = C.c_int(0)
+    _file_status(L.rtb_read_fwh(os.fsencode(path), C.byref(n), None, None, 0), path)
+    v, x = np.zeros(n.value, np.float32), np.zeros(n.value, np.float32)
+    _file_status(L.rtb_read_fwh(os.fsencode(path), C.byref(n), _abi.fptr(v), _abi.fptr(x), len(v)), path)
+    return v, x
+
+
+def read_fil(path):
+    """A .fil file (cirsconv.f:185-196): (vcen, nsub, vfil, fil)."""
+    L = _lib.lib()
+    nf, npt = C.c_int(0), C.c_int(0)
+    _file_status(L.rtb_read_fil(os.fsencode(path), C.byref(nf), C.byref(npt), None, None, None, None, 0, 0), path)
+    vc, ns = np.zeros(nf.value, np.float32), np.zeros(nf.value, np.int32)
+    vf, fl = np.zeros(npt.value, np.float32), np.zeros(npt.value, np.float32)
+    _file_status(L.rtb_read_fil(os.fsencode(path), C.byref(nf), C.byref(npt), _abi.fptr(vc), _abi.iptr(ns),
+                                _abi.fptr(vf), _abi.fptr(fl), len(vc), len(vf)), path)
+    return vc, ns, vf, fl
+
+
 class Context:
     """One device context (one CUDA device, one host thread at a time)."""
 
@@ -109,6 +136,18 @@ class Context:
         out = np.zeros((y.shape[0], len(vconv)), np.float32)
         self._check(self._L.rtb_cirsconv(self._h, len(vwave), _abi.fptr(vwave), y.shape[0], _abi.fptr(y),
                                          float(fwhm), len(vconv), _abi.fptr(vconv), _abi.fptr(out)))
+        return out
+
+    def cirsconv_ex(self, vwave, y, fwhm, channels):
+        """cirsconv of series y [nser, nwave] with any FWHM (> 0 with an
+        optional width table, 0, < 0 with filter functions) onto
+        ``channels`` (a ``synth.Channels``): [nser, nconv]."""
+        vwave = np.ascontiguousarray(vwave, np.float32)
+        y = np.ascontiguousarray(np.atleast_2d(y), np.float32)
+        cs = channels.as_struct()
+        out = np.zeros((y.shape[0], len(channels.vconv)), np.float32)
+        self._check(self._L.rtb_cirsconv_ex(self._h, float(fwhm), len(vwave), _abi.fptr(vwave), y.shape[0],
+                                            _abi.fptr(y), C.byref(cs), _abi.fptr(out)))
         return out
 
     def cirsradg_wave(self, job, isw):

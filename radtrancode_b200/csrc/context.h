@@ -98,6 +98,24 @@ int apply_schedule(rtb_context* c);
 void drop_graph(rtb_context* c);
 cudaStream_t stream_of(rtb_context* c);
 
+// one spectrum's instrument convolution (the cirsconv arguments), copied
+// when the batch is prepared
+struct ConvSpec {
+    float fwhm = 0.0f;
+    std::vector<float> vwave, vconv;          // empty vconv: no convolution (FWHM = 0, nconv = nwave)
+    std::vector<float> vfwhm, xfwhm;          // FWHM > 0: channel-dependent width table
+    std::vector<int> fil_of, fil_off;         // FWHM < 0: filter of each channel; point offsets per filter
+    std::vector<float> vfil, fil;
+};
+// nser device series of nwave values at y, convolved to yout[nser][nconv]
+struct ConvSeg {
+    const float* y;
+    int nser;
+    float* yout;
+};
+int conv_check(rtb_context* c, float fwhm, int nwave, const float* vwave, const rtb_conv* cv, ConvSpec& out);
+int conv_run(rtb_context* c, const ConvSpec& cs, int nseg, const ConvSeg* seg, cudaStream_t st);
+
 }  // namespace rtb
 
 // the context is the opaque handle of the C ABI (global namespace)
@@ -140,6 +158,11 @@ struct rtb_context {
     long long cells = 0;
     rtb::DevBuf d_dbg_perm, d_dbg_split;
     rtb::DevBuf d_dq;                     // per-path-position derivatives (rtb_cirsradg_wave)
+    // instrument convolution of the resident batch's outputs (cirsrtfg_wave.f:448-516)
+    std::vector<rtb::ConvSpec> spec_conv;
+    int any_conv = 0;
+    rtb::DevBuf d_conv, d_convout;
+    std::vector<char> h_conv;
     size_t dbg_perm_n = 0, dbg_split_n = 0;
     rtb_fwd_stats stats{};
     // schedule of the resident batch (rtb_fwd_set_schedule / rtb_fwd_autotune)

@@ -1,16 +1,26 @@
 // conv.cu -- instrument convolution of calculated spectra on the device.
 //
-// Reference: radtran/cirsrad/cirsconv.f:12-160 (FWHM > 0: a natural cubic
-// spline through the calculated points, CSPLINE rtm_util/cspline.f, read by
-// CSPLINT rtm_util/csplint.f at 20 equally spaced points across each
-// channel's square bin, trapezoid sum in DOUBLE PRECISION; FWHM = 0: a copy)
-// as cirsrtfg_wave.f:448-516 applies it to the radiance, d/dtsurf and every
-// Jacobian row.  One block per series: thread 0 builds the extrapolated,
-// NaN-free knot list and solves the spline's tridiagonal system (a sequential
-// recurrence), then the block's threads fill the channels.  REAL arithmetic
-// is written with explicitly rounded intrinsics so that it rounds as the
-// reference's does.
+// Reference: radtran/cirsrad/cirsconv.f:12-246 as cirsrtfg_wave.f:448-516
+// applies it to the radiance, d/dtsurf and every Jacobian row:
+//   * one calculated point and FWHM != 0 (:45-54): the output is 1;
+//   * FWHM > 0 (:64-160): a natural cubic spline through the calculated
+//     points (CSPLINE rtm_util/cspline.f, read by CSPLINT rtm_util/csplint.f)
+//     averaged at 20 equally spaced points across each channel's square bin,
+//     trapezoid sum in DOUBLE PRECISION; the bin width may vary by channel
+//     (the .fwh table read by VERINT radtran/path/verint.f, :147-150);
+//   * FWHM = 0 (:162-169): a copy of the first nconv points;
+//   * FWHM < 0 (:171-239): each channel's filter function from the .fil file,
+//     linearly interpolated (INTERP rtm_util/interp.f) onto the calculated
+//     points, and the filter-weighted mean of the series.
+// One block per series.  For FWHM > 0 thread 0 builds the extrapolated,
+// NaN-free knot list and solves the spline's tridiagonal system (a
+// sequential recurrence), then the block's threads fill the channels.  REAL
+// arithmetic is written with explicitly rounded intrinsics so that it rounds
+// as the reference's does.
 #include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
 
 #include "context.h"
 
@@ -38,9 +48,33 @@ __device__ float csplint_dev(const float* XA, const float* YA, const float* Y2A,
     return fabs(y1) > 1.00E-37 ? __double2float_rn(y1) : 1.00E-37f;
 }
 
+// INTERP (rtm_util/interp.f) and VERINT (radtran/path/verint.f): the first
+// point beyond XIN in the table's direction (the last point if none, the
+// second if it is the first), then the REAL line through it and the point
+// before.  VERINT also returns Y(I) for a vertical segment or a NaN.
+__device__ float interp_dev(const float* X, const float* Y, int N, float XIN, bool verint) {
+    int I = 1;
+    if (X[0] < X[N - 1]) {
+        while (I <= N && !(X[I - 1] > XIN)) ++I;
+    } else {
+        while (I <= N && !(X[I - 1] < XIN)) ++I;
+    }
+    if (I > N) I = N;
+    if (I == 1) I = 2;
+    const float t = __fdiv_rn(__fmul_rn(__fsub_rn(Y[I - 1], Y[I - 2]), __fsub_rn(XIN, X[I - 2])),
+                              __fsub_rn(X[I - 1], X[I - 2]));
+    float y = __fadd_rn(Y[I - 2], t);
+    if (verint) {
+        if (X[I - 2] == X[I - 1]) y = Y[I - 1];
+        if (isnan(y)) y = Y[I - 1];
+    }
+    return y;
+}
+
 __global__ void __launch_bounds__(kConvThreads)
 cirsconv_kernel(int nwave, const float* __restrict__ vwave, const float* __restrict__ y, float fwhm, int nconv,
-                const float* __restrict__ vconv, float* __restrict__ yout, float* __restrict__ scr) {
+                const float* __restrict__ vconv, int nfwhm, const float* __restrict__ vfwhm,
+                const float* __restrict__ xfwhm, float* __restrict__ yout, float* __restrict__ scr) {
     __shared__ int s_nc;
     const int s = blockIdx.x;
     const float* ys = y + (int64_t)s * nwave;
@@ -108,7 +142,9 @@ cirsconv_kernel(int nwave, const float* __restrict__ vwave, const float* __restr
     __syncthreads();
     const int nc = s_nc;
     for (int i = threadIdx.x; i < nconv; i += kConvThreads) {
-        const float half = __fdiv_rn(fwhm, 2.0f);
+        // the channel's bin width: FWHM, or the .fwh table at the channel (cirsconv.f:147-150)
+        const float yfwhm = nfwhm > 0 ? interp_dev(vfwhm, xfwhm, nfwhm, vconv[i], true) : fwhm;
+        const float half = __fdiv_rn(yfwhm, 2.0f);
         const float x1 = __fsub_rn(vconv[i], half), x2 = __fadd_rn(vconv[i], half);
         const float delx = __fdiv_rn(__fsub_rn(x2, x1), (float)(kNstep - 1));
         const double hd = (double)__fdiv_rn(delx, 2.0f);
@@ -119,43 +155,208 @@ cirsconv_kernel(int nwave, const float* __restrict__ vwave, const float* __restr
             if (j > 1) sum = __dadd_rn(sum, __dmul_rn(__dadd_rn(yi, yold), hd));
             yold = yi;
         }
+        // the sum is divided by FWHM itself, not the channel's width (cirsconv.f:159)
         yout[(int64_t)s * nconv + i] = __double2float_rn(__ddiv_rn(sum, (double)fwhm));
     }
 }
 
+// FWHM < 0: ytmp of cirsconv.f:205-213 for every (channel, calculated point),
+// the channel's filter interpolated where the point lies inside it, else 0
+__global__ void __launch_bounds__(kConvThreads)
+filter_weights_kernel(int nwave, const float* __restrict__ vwave, const int* __restrict__ fil_of,
+                      const int* __restrict__ fil_off, const float* __restrict__ vfil, const float* __restrict__ fil,
+                      float* __restrict__ w) {
+    const int i = blockIdx.x;
+    const int k = fil_of[i];
+    const float* X = vfil + fil_off[k];
+    const float* Y = fil + fil_off[k];
+    const int n = fil_off[k + 1] - fil_off[k];
+    for (int j = threadIdx.x; j < nwave; j += kConvThreads) {
+        const float v = vwave[j];
+        w[(int64_t)i * nwave + j] = (v >= X[0] && v <= X[n - 1]) ? interp_dev(X, Y, n, v, false) : 0.0f;
+    }
+}
+
+// FWHM < 0: the filter-weighted mean (cirsconv.f:220-237, xnorm true): DOUBLE
+// sums of the REAL products ytmp*y*delv and ytmp*delv over the points below
+// the last one where ytmp is not zero
+__global__ void __launch_bounds__(kConvThreads)
+filter_conv_kernel(int nwave, int nconv, const float* __restrict__ vwave, const float* __restrict__ y,
+                   const float* __restrict__ w, float* __restrict__ yout) {
+    const int s = blockIdx.x;
+    const float* ys = y + (int64_t)s * nwave;
+    for (int i = threadIdx.x; i < nconv; i += kConvThreads) {
+        const float* wi = w + (int64_t)i * nwave;
+        double sum = 0.0, sumf = 0.0;
+        for (int j = 0; j < nwave - 1; ++j) {
+            const float yt = wi[j];
+            if (yt != 0.0f) {
+                const float delv = __fsub_rn(vwave[j + 1], vwave[j]);
+                sum = __dadd_rn(sum, (double)__fmul_rn(__fmul_rn(yt, ys[j]), delv));
+                sumf = __dadd_rn(sumf, (double)__fmul_rn(yt, delv));
+            }
+        }
+        yout[(int64_t)s * nconv + i] = __double2float_rn(__ddiv_rn(sum, sumf));
+    }
+}
+
+__global__ void fill_kernel(float* p, int64_t n, float v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+size_t align16(size_t n) { return (n + 15) & ~(size_t)15; }
+
 }  // namespace
+
+int conv_check(rtb_context* c, float fwhm, int nwave, const float* vwave, const rtb_conv* cv, ConvSpec& out) {
+    out = ConvSpec();
+    out.fwhm = fwhm;
+    if (!cv) {
+        if (fwhm != 0.0f) return fail(c, RTB_ERR_ARG, "cirsconv: FWHM != 0 needs the channel list (rtb_conv)");
+        return RTB_OK;
+    }
+    if (nwave <= 0 || !vwave) return fail(c, RTB_ERR_ARG, "cirsconv: no calculated points");
+    if (cv->nconv <= 0 || !cv->vconv) return fail(c, RTB_ERR_ARG, "cirsconv: no channels (nconv, vconv)");
+    out.vwave.assign(vwave, vwave + nwave);
+    out.vconv.assign(cv->vconv, cv->vconv + cv->nconv);
+    if (nwave == 1 && fwhm != 0.0f) {   // cirsconv.f:45-54 resets nconv to 1
+        if (cv->nconv != 1) return fail(c, RTB_ERR_ARG, "cirsconv: one calculated point gives one channel (nconv=1)");
+        return RTB_OK;
+    }
+    if (fwhm == 0.0f) {
+        if (cv->nconv > nwave) return fail(c, RTB_ERR_ARG, "cirsconv: FWHM = 0 copies, so nconv <= nwave");
+        return RTB_OK;
+    }
+    if (fwhm > 0.0f) {
+        if (cv->nfwhm != 0) {
+            if (cv->nfwhm < 2 || !cv->vfwhm || !cv->xfwhm)
+                return fail(c, RTB_ERR_ARG, "cirsconv: a FWHM table needs at least two points");
+            out.vfwhm.assign(cv->vfwhm, cv->vfwhm + cv->nfwhm);
+            out.xfwhm.assign(cv->xfwhm, cv->xfwhm + cv->nfwhm);
+        }
+        return RTB_OK;
+    }
+    // FWHM < 0: filter channels
+    if (cv->nfil <= 0 || !cv->vcen || !cv->nsub || !cv->vfil || !cv->fil)
+        return fail(c, RTB_ERR_ARG, "cirsconv: FWHM < 0 needs the filter functions (nfil, vcen, nsub, vfil, fil)");
+    out.fil_off.assign(1, 0);
+    for (int k = 0; k < cv->nfil; ++k) {
+        if (cv->nsub[k] < 2) return fail(c, RTB_ERR_ARG, "cirsconv: filter %d has fewer than two points", k);
+        out.fil_off.push_back(out.fil_off.back() + cv->nsub[k]);
+    }
+    out.vfil.assign(cv->vfil, cv->vfil + out.fil_off.back());
+    out.fil.assign(cv->fil, cv->fil + out.fil_off.back());
+    out.fil_of.assign(cv->nconv, -1);
+    for (int i = 0; i < cv->nconv; ++i) {
+        // the last filter centred within 1e-5 of the channel (cirsconv.f:197-202)
+        for (int k = 0; k < cv->nfil; ++k)
+            if (std::fabs(cv->vcen[k] - cv->vconv[i]) < 0.00001f) out.fil_of[i] = k;
+        if (out.fil_of[i] < 0)
+            return fail(c, RTB_ERR_ARG, "cirsconv: no filter function centred on channel %d (%g)", i,
+                        (double)cv->vconv[i]);
+    }
+    return RTB_OK;
+}
+
+int conv_run(rtb_context* c, const ConvSpec& cs, int nseg, const ConvSeg* seg, cudaStream_t st) {
+    const int nwave = (int)cs.vwave.size(), nconv = (int)cs.vconv.size();
+    int nser_max = 0;
+    for (int q = 0; q < nseg; ++q) nser_max = std::max(nser_max, seg[q].nser);
+    if (nser_max == 0) return RTB_OK;
+    if (nwave == 1 && cs.fwhm != 0.0f) {
+        for (int q = 0; q < nseg; ++q)
+            if (seg[q].nser > 0) {
+                fill_kernel<<<1, 128, 0, st>>>(seg[q].yout, seg[q].nser, 1.0f);
+                CUDA_TRY(c, cudaGetLastError());
+            }
+        return RTB_OK;
+    }
+    if (cs.fwhm == 0.0f) {
+        for (int q = 0; q < nseg; ++q)
+            if (seg[q].nser > 0)
+                CUDA_TRY(c, cudaMemcpy2DAsync(seg[q].yout, (size_t)nconv * 4, seg[q].y, (size_t)nwave * 4,
+                                              (size_t)nconv * 4, seg[q].nser, cudaMemcpyDeviceToDevice, st));
+        return RTB_OK;
+    }
+    // one upload of the channel description, then the scratch
+    std::vector<char>& blob = c->h_conv;
+    blob.clear();
+    auto put = [&](const void* p, size_t n) {
+        const size_t o = align16(blob.size());
+        blob.resize(o + align16(n));
+        if (n) std::memcpy(blob.data() + o, p, n);
+        return o;
+    };
+    const size_t o_vw = put(cs.vwave.data(), nwave * 4), o_vc = put(cs.vconv.data(), nconv * 4);
+    const size_t o_vf = put(cs.vfwhm.data(), cs.vfwhm.size() * 4), o_xf = put(cs.xfwhm.data(), cs.xfwhm.size() * 4);
+    const size_t o_fo = put(cs.fil_of.data(), cs.fil_of.size() * 4), o_ff = put(cs.fil_off.data(), cs.fil_off.size() * 4);
+    const size_t o_pv = put(cs.vfil.data(), cs.vfil.size() * 4), o_pf = put(cs.fil.data(), cs.fil.size() * 4);
+    const size_t o_scr = align16(blob.size());
+    const size_t n_scr = cs.fwhm > 0.0f ? (size_t)nser_max * 4 * (nwave + 2) * 4 : (size_t)nconv * nwave * 4;
+    CUDA_TRY(c, c->d_conv.ensure(o_scr + n_scr + 16));
+    char* d = (char*)c->d_conv.p;
+    CUDA_TRY(c, cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, st));
+    const float* dvw = (const float*)(d + o_vw);
+    const float* dvc = (const float*)(d + o_vc);
+    float* dscr = (float*)(d + o_scr);
+    if (cs.fwhm > 0.0f) {
+        for (int q = 0; q < nseg; ++q)
+            if (seg[q].nser > 0) {
+                cirsconv_kernel<<<seg[q].nser, kConvThreads, 0, st>>>(
+                    nwave, dvw, seg[q].y, cs.fwhm, nconv, dvc, (int)cs.vfwhm.size(), (const float*)(d + o_vf),
+                    (const float*)(d + o_xf), seg[q].yout, dscr);
+                CUDA_TRY(c, cudaGetLastError());
+            }
+        return RTB_OK;
+    }
+    filter_weights_kernel<<<nconv, kConvThreads, 0, st>>>(nwave, dvw, (const int*)(d + o_fo), (const int*)(d + o_ff),
+                                                          (const float*)(d + o_pv), (const float*)(d + o_pf), dscr);
+    CUDA_TRY(c, cudaGetLastError());
+    for (int q = 0; q < nseg; ++q)
+        if (seg[q].nser > 0) {
+            filter_conv_kernel<<<seg[q].nser, kConvThreads, 0, st>>>(nwave, nconv, dvw, seg[q].y, dscr, seg[q].yout);
+            CUDA_TRY(c, cudaGetLastError());
+        }
+    return RTB_OK;
+}
 
 }  // namespace rtb
 
 using namespace rtb;
 
-extern "C" int rtb_cirsconv(rtb_context* c, int nwave, const float* vwave, int nser, const float* y, float fwhm,
-                            int nconv, const float* vconv, float* yout) {
+extern "C" int rtb_cirsconv_ex(rtb_context* c, float fwhm, int nwave, const float* vwave, int nser, const float* y,
+                               const rtb_conv* conv, float* yout) {
     if (!c) return RTB_ERR_ARG;
-    if (nwave <= 0 || nser <= 0 || nconv <= 0 || !vwave || !y || !vconv || !yout)
-        return fail(c, RTB_ERR_ARG, "cirsconv: bad arguments");
-    if (fwhm == 0.0f) {   // cirsconv.f:141-147: the outputs are the inputs
-        if (nconv != nwave) return fail(c, RTB_ERR_ARG, "cirsconv: FWHM = 0 needs nconv == nwave");
-        for (size_t i = 0; i < (size_t)nser * nwave; ++i) yout[i] = y[i];
-        return RTB_OK;
-    }
-    if (fwhm < 0.0f) return fail(c, RTB_ERR_UNSUPPORTED, "cirsconv: FWHM < 0 (filter-file channels) not implemented");
-    if (nwave < 2) return fail(c, RTB_ERR_ARG, "cirsconv: FWHM > 0 needs at least two calculated points");
+    if (nwave <= 0 || nser <= 0 || !vwave || !y || !conv || !yout) return fail(c, RTB_ERR_ARG, "cirsconv: bad arguments");
+    ConvSpec cs;
+    const int r = conv_check(c, fwhm, nwave, vwave, conv, cs);
+    if (r) return r;
     CUDA_TRY(c, cudaSetDevice(c->device));
     const cudaStream_t st = stream_of(c);
-    const size_t ny = (size_t)nser * nwave, no = (size_t)nser * nconv, ns = (size_t)nser * 4 * (nwave + 2);
-    CUDA_TRY(c, c->d_nt32.ensure((nwave + nconv + ny + no + ns) * sizeof(float) + 64));
-    float* dv = (float*)c->d_nt32.p;
-    float* dc = dv + nwave;
-    float* dy = dc + nconv;
-    float* dout = dy + ny;
-    float* dscr = dout + no;
-    CUDA_TRY(c, cudaMemcpyAsync(dv, vwave, (size_t)nwave * 4, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(c, cudaMemcpyAsync(dc, vconv, (size_t)nconv * 4, cudaMemcpyHostToDevice, st));
+    const int nconv = conv->nconv;
+    const size_t ny = (size_t)nser * nwave, no = (size_t)nser * nconv;
+    CUDA_TRY(c, c->d_nt32.ensure((ny + no) * sizeof(float) + 64));
+    float* dy = (float*)c->d_nt32.p;
+    float* dout = dy + ((ny + 3) & ~(size_t)3);
     CUDA_TRY(c, cudaMemcpyAsync(dy, y, ny * 4, cudaMemcpyHostToDevice, st));
-    cirsconv_kernel<<<nser, kConvThreads, 0, st>>>(nwave, dv, dy, fwhm, nconv, dc, dout, dscr);
-    CUDA_TRY(c, cudaGetLastError());
+    const ConvSeg seg{dy, nser, dout};
+    const int r2 = conv_run(c, cs, 1, &seg, st);
+    if (r2) return r2;
     CUDA_TRY(c, cudaMemcpyAsync(yout, dout, no * 4, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(c, cudaStreamSynchronize(st));
     return RTB_OK;
+}
+
+extern "C" int rtb_cirsconv(rtb_context* c, int nwave, const float* vwave, int nser, const float* y, float fwhm,
+                            int nconv, const float* vconv, float* yout) {
+    if (!c) return RTB_ERR_ARG;
+    if (fwhm < 0.0f)
+        return fail(c, RTB_ERR_UNSUPPORTED, "cirsconv: FWHM < 0 takes the filter functions (rtb_cirsconv_ex)");
+    if (fwhm == 0.0f && nconv != nwave) return fail(c, RTB_ERR_ARG, "cirsconv: FWHM = 0 needs nconv == nwave");
+    rtb_conv cv;
+    std::memset(&cv, 0, sizeof cv);
+    cv.nconv = nconv;
+    cv.vconv = vconv;
+    return rtb_cirsconv_ex(c, fwhm, nwave, vwave, nser, y, &cv, yout);
 }

@@ -13,9 +13,14 @@
 // CIA .tab (radtran/radtran/ciaread.f:77-98): a sequential unformatted file
 // with two records, 25 DOUBLE temperatures and REAL kcia(9, 25, 1501), each
 // framed by 4-byte length markers.
+//
+// .fwh and .fil (cirsrtfg_wave.f:185-198, cirsconv.f:183-196): text files
+// read by list-directed READ(u,*), the channel widths and filter functions of
+// the instrument convolution, handed to rtb_cirsconv_ex / rtb_conv.
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -87,6 +92,46 @@ int read_kta_header(FILE* f, Kta& k, std::string& err) {
         return RTB_ERR_ARG;
     }
     return RTB_OK;
+}
+
+// One list-directed READ(u,*) of n values (the Fortran rule the reference's
+// text files rely on): it starts at the next record, takes values separated
+// by blanks or commas across as many records as it needs, and drops the rest
+// of its last record.
+bool list_read(FILE* f, int n, std::vector<std::string>& out) {
+    out.clear();
+    char line[4096];
+    while ((int)out.size() < n) {
+        if (!std::fgets(line, sizeof line, f)) return false;
+        std::string cur;
+        for (const char* p = line;; ++p) {
+            const char ch = *p;
+            if (ch == ' ' || ch == '\t' || ch == ',' || ch == '\n' || ch == '\r' || ch == '\0') {
+                if (!cur.empty() && (int)out.size() < n) out.push_back(cur);
+                cur.clear();
+                if (ch == '\0') break;
+            } else {
+                cur += ch;
+            }
+        }
+    }
+    return true;
+}
+
+bool to_int(const std::string& t, int& v) {
+    char* e = nullptr;
+    const long x = std::strtol(t.c_str(), &e, 10);
+    if (e == t.c_str() || *e) return false;
+    v = (int)x;
+    return true;
+}
+
+bool to_real(std::string t, float& v) {
+    for (char& ch : t)
+        if (ch == 'd' || ch == 'D') ch = 'e';   // DOUBLE PRECISION exponent letter
+    char* e = nullptr;
+    v = std::strtof(t.c_str(), &e);
+    return e != t.c_str() && !*e;
 }
 
 }  // namespace
@@ -167,6 +212,55 @@ int rtb_load_cia(rtb_context* c, const char* path, float dnu) {
         return fail(c, RTB_ERR_ARG, "%s: not a CIA table (two unformatted records: 25 DOUBLE, REAL(9,25,1501))",
                     path);
     return rtb_set_cia(c, dnu, temps, kcia.data());
+}
+
+// .fwh (cirsrtfg_wave.f:191-196): NFWHM, then NFWHM records VFWHM XFWHM
+int rtb_read_fwh(const char* path, int* n, float* v, float* x, int cap) {
+    File fl(path);
+    if (!fl.f || !n) return RTB_ERR_ARG;
+    std::vector<std::string> t;
+    int m = 0;
+    if (!list_read(fl.f, 1, t) || !to_int(t[0], m) || m < 0) return RTB_ERR_ARG;
+    *n = m;
+    if (!v && !x) return RTB_OK;
+    if (!v || !x) return RTB_ERR_ARG;
+    if (m > cap) return RTB_ERR_LIMIT;
+    for (int i = 0; i < m; ++i)
+        if (!list_read(fl.f, 2, t) || !to_real(t[0], v[i]) || !to_real(t[1], x[i])) return RTB_ERR_ARG;
+    return RTB_OK;
+}
+
+// .fil (cirsconv.f:185-196): NCONV1, then per filter VCENTRAL, NSUB and NSUB
+// records VFIL FIL
+int rtb_read_fil(const char* path, int* nfil, int* npts, float* vcen, int* nsub, float* vfil, float* fil,
+                 int cap_fil, int cap_pts) {
+    File fl(path);
+    if (!fl.f || !nfil || !npts) return RTB_ERR_ARG;
+    std::vector<std::string> t;
+    int m = 0;
+    if (!list_read(fl.f, 1, t) || !to_int(t[0], m) || m < 0) return RTB_ERR_ARG;
+    std::vector<float> vc(m), pv, pf;
+    std::vector<int> ns(m);
+    for (int k = 0; k < m; ++k) {
+        if (!list_read(fl.f, 1, t) || !to_real(t[0], vc[k])) return RTB_ERR_ARG;
+        if (!list_read(fl.f, 1, t) || !to_int(t[0], ns[k]) || ns[k] < 0) return RTB_ERR_ARG;
+        for (int j = 0; j < ns[k]; ++j) {
+            float a = 0.0f, b = 0.0f;
+            if (!list_read(fl.f, 2, t) || !to_real(t[0], a) || !to_real(t[1], b)) return RTB_ERR_ARG;
+            pv.push_back(a);
+            pf.push_back(b);
+        }
+    }
+    *nfil = m;
+    *npts = (int)pv.size();
+    if (!vcen && !nsub && !vfil && !fil) return RTB_OK;
+    if (!vcen || !nsub || !vfil || !fil) return RTB_ERR_ARG;
+    if (m > cap_fil || (int)pv.size() > cap_pts) return RTB_ERR_LIMIT;
+    std::copy(vc.begin(), vc.end(), vcen);
+    std::copy(ns.begin(), ns.end(), nsub);
+    std::copy(pv.begin(), pv.end(), vfil);
+    std::copy(pf.begin(), pf.end(), fil);
+    return RTB_OK;
 }
 
 }  // extern "C"

@@ -148,7 +148,6 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     if (a.flagh2p != 0) return fail(c, RTB_ERR_UNSUPPORTED, "flagh2p=1 (nparacon path) not implemented");
     if (a.ilbl != 0) return fail(c, RTB_ERR_UNSUPPORTED, "ILBL != 0 (line-by-line tables) not implemented");
     if (a.inlte != 0) return fail(c, RTB_ERR_UNSUPPORTED, "non-LTE emission temperatures not implemented");
-    if (a.fwhm != 0.0f) return fail(c, RTB_ERR_UNSUPPORTED, "FWHM != 0 convolution not implemented");
     if (!(a.iform == 0 || a.iform == 2)) return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d not implemented", a.iform);
     if (a.iray > 1) return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (only Jovian Rayleigh, iray=1)", a.iray);
     if (a.npath > 4) return fail(c, RTB_ERR_UNSUPPORTED, "more than 4 paths per spectrum");
@@ -589,6 +588,16 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     if (c->ng > 22 || c->ng < 2) return fail(c, RTB_ERR_UNSUPPORTED, "NG=%d outside the device range 2..22", c->ng);
     CUDA_TRY(c, cudaSetDevice(c->device));
     c->prepared = 0;
+    // instrument convolution of each spectrum's outputs (cirsrtfg_wave.f:448-516)
+    std::vector<ConvSpec> convs(nspec);
+    int any_conv = 0;
+    for (int s = 0; s < nspec; ++s) {
+        const int r = conv_check(c, atms[s].fwhm, atms[s].nwave, atms[s].vwave, atms[s].conv, convs[s]);
+        if (r) return r;
+        if (!convs[s].vconv.empty()) any_conv = 1;
+    }
+    if (any_conv && place)
+        return fail(c, RTB_ERR_UNSUPPORTED, "instrument convolution of a batch written to caller arrays");
     Staging st;
     const int r0 = pack_batch(c, nspec, atms, st);
     if (r0) return r0;
@@ -716,6 +725,8 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     c->nlmax_max = st.nlmax_max;
     c->npath_max = st.npath_max;
     c->spec_host = st.spec;
+    c->spec_conv = std::move(convs);
+    c->any_conv = any_conv;
     c->spec_npath.clear();
     c->spec_nv.clear();
     c->spec_nwave.clear();
@@ -816,6 +827,41 @@ int launch(rtb_context* c) {
     return RTB_OK;
 }
 
+// cirsrtfg_wave.f:448-516: the radiance, d/dtsurf and every Jacobian row of a
+// spectrum with channels, convolved on the device from the batch's outputs
+int fetch_convolved(rtb_context* c, cudaStream_t strm, float* const* calcout, float* const* gradients,
+                    float* const* gradtsurf) {
+    size_t need = 0;
+    for (size_t s = 0; s < c->spec_host.size(); ++s)
+        need = std::max(need, (size_t)c->spec_npath[s] * (2 + c->spec_nv[s]) * c->spec_conv[s].vconv.size());
+    CUDA_TRY(c, c->d_convout.ensure(need * sizeof(float) + 16));
+    const float* d = (const float*)c->d_out.p;
+    float* o = (float*)c->d_convout.p;
+    for (size_t s = 0; s < c->spec_host.size(); ++s) {
+        const ConvSpec& cs = c->spec_conv[s];
+        if (cs.vconv.empty()) continue;
+        const SpecDev& S = c->spec_host[s];
+        const int np = c->spec_npath[s], nv = c->spec_nv[s];
+        const size_t nc = cs.vconv.size();
+        const bool want_gt = gradtsurf && gradtsurf[s];
+        const ConvSeg seg[3] = {{d + S.out_off, np, o},
+                                {d + c->n_out + S.out_off, want_gt ? np : 0, o + np * nc},
+                                {d + 2 * c->n_out + S.jac_off, np * nv, o + 2 * np * nc}};
+        const int r = conv_run(c, cs, 3, seg, strm);
+        if (r) return r;
+        if (calcout && calcout[s])
+            CUDA_TRY(c, cudaMemcpyAsync(calcout[s], o, np * nc * sizeof(float), cudaMemcpyDeviceToHost, strm));
+        if (want_gt)
+            CUDA_TRY(c, cudaMemcpyAsync(gradtsurf[s], o + np * nc, np * nc * sizeof(float), cudaMemcpyDeviceToHost,
+                                        strm));
+        if (gradients && gradients[s])
+            CUDA_TRY(c, cudaMemcpyAsync(gradients[s], o + 2 * np * nc, (size_t)np * nv * nc * sizeof(float),
+                                        cudaMemcpyDeviceToHost, strm));
+        CUDA_TRY(c, cudaStreamSynchronize(strm));
+    }
+    return RTB_OK;
+}
+
 int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float* const* gradtsurf) {
     if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
     if (c->placed) return fail(c, RTB_ERR_ARG, "the resident batch belongs to the retrieval engine");
@@ -840,6 +886,7 @@ int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float*
     if (status & kStGord) return fail(c, RTB_ERR_GORD, "g-ordinate walk ran past NG (rankg.f:118-147)");
     const float* h = (const float*)c->h_out.p;
     for (size_t s = 0; s < c->spec_host.size(); ++s) {
+        if (c->any_conv && !c->spec_conv[s].vconv.empty()) continue;
         const SpecDev& S = c->spec_host[s];
         const size_t no = (size_t)c->spec_npath[s] * c->spec_nwave[s];
         const size_t nj = (size_t)c->spec_npath[s] * c->spec_nv[s] * c->spec_nwave[s];
@@ -847,7 +894,7 @@ int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float*
         if (gradtsurf && gradtsurf[s]) memcpy(gradtsurf[s], h + c->n_out + S.out_off, no * sizeof(float));
         if (gradients && gradients[s]) memcpy(gradients[s], h + 2 * c->n_out + S.jac_off, nj * sizeof(float));
     }
-    return RTB_OK;
+    return c->any_conv ? fetch_convolved(c, strm, calcout, gradients, gradtsurf) : RTB_OK;
 }
 
 int run_batch(rtb_context* c, int nspec, const rtb_atm* atms, float* const* calcout, float* const* gradients,
@@ -953,6 +1000,8 @@ void rtb_destroy(rtb_context* c) {
     drop_graph(c);
     c->d_order.release();
     c->d_dq.release();
+    c->d_conv.release();
+    c->d_convout.release();
     c->d_nt32.release();
     c->d_nt64.release();
     c->d_ntsmall.release();
@@ -1167,6 +1216,8 @@ int rtb_cirsradg_wave(rtb_context* c, const rtb_atm* atm, int nsw, const int* is
     std::vector<float> xm(nparam, 0.0f), zl(ldl, 0.0f);
     for (int s = 0; s < nsw; ++s) xm[isw[s]] = 1.0f;
     rtb_atm a = a0;
+    a.fwhm = 0.0f;   // cirsradg_wave returns the calculation-grid values
+    a.conv = nullptr;
     a.nv = 1;
     a.npro = 1;
     a.ld_v = 1;

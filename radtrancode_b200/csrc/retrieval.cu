@@ -62,6 +62,8 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     const int ldp = t.ld_param > 0 ? t.ld_param : (RTB_MAXGAS + 2 + RTB_MAXCON);
     const int nparam = G + 1 + NC;
     if (NP != 1) return fail(c, RTB_ERR_UNSUPPORTED, "retrieval atmosphere must have one path (npath=%d)", NP);
+    if (t.fwhm != 0.0f || t.conv)
+        return fail(c, RTB_ERR_UNSUPPORTED, "retrieval on convolved channels (FWHM != 0) not supported");
     if (NPRO != L) return fail(c, RTB_ERR_UNSUPPORTED, "layer-state model needs npro == nlayer");
     if (s.nprof < 0 || (s.nprof > 0 && !s.prof_gas)) return fail(c, RTB_ERR_ARG, "nprof/prof_gas");
     if (NV != L + s.nscale + s.nprof * L)

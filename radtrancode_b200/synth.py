@@ -112,6 +112,40 @@ def make_cia(seed=0, dnu=1.0) -> CIATable:
 
 
 @dataclasses.dataclass
+class Channels:
+    """Instrument channels of cirsconv (the rtb_conv structure): centres,
+    optionally a channel-dependent width table (.fwh, FWHM > 0) or filter
+    functions (.fil, FWHM < 0; filter k has nsub[k] points)."""
+    vconv: np.ndarray
+    vfwhm: np.ndarray | None = None
+    xfwhm: np.ndarray | None = None
+    vcen: np.ndarray | None = None
+    nsub: np.ndarray | None = None
+    vfil: np.ndarray | None = None
+    fil: np.ndarray | None = None
+
+    def __post_init__(self):
+        self.vconv = np.ascontiguousarray(self.vconv, np.float32)
+        for k in ("vfwhm", "xfwhm", "vcen", "vfil", "fil"):
+            v = getattr(self, k)
+            if v is not None:
+                setattr(self, k, np.ascontiguousarray(v, np.float32))
+        if self.nsub is not None:
+            self.nsub = np.ascontiguousarray(self.nsub, np.int32)
+
+    def as_struct(self) -> _abi.RtbConv:
+        s = _abi.RtbConv()
+        f, i = _abi.fptr, _abi.iptr
+        s.nconv, s.vconv = len(self.vconv), f(self.vconv)
+        if self.vfwhm is not None:
+            s.nfwhm, s.vfwhm, s.xfwhm = len(self.vfwhm), f(self.vfwhm), f(self.xfwhm)
+        if self.vcen is not None:
+            s.nfil, s.vcen, s.nsub, s.vfil, s.fil = len(self.vcen), f(self.vcen), i(self.nsub), f(self.vfil), f(self.fil)
+        s._keep = self
+        return s
+
+
+@dataclasses.dataclass
 class Job:
     """One cirsrtfg_wave call in the reference's Fortran array layout."""
     nlayer: int
@@ -148,6 +182,8 @@ class Job:
     ispace: int = 0
     tsurf: float = 0.0
     iform: int = 0
+    fwhm: float = 0.0
+    conv: "Channels | None" = None   # instrument channels (None: FWHM = 0, nconv = nwave)
     # bookkeeping for the synthetic state vector (not part of the ABI)
     vmr: np.ndarray | None = None
     ncol: np.ndarray | None = None
@@ -173,13 +209,22 @@ class Job:
         s.vwave, s.xsec_ext = f(self.vwave), None
         s.inormal, s.iray, s.itype, s.ispace = self.inormal, self.iray, self.itype, self.ispace
         s.flagh2p, s.ilbl, s.inlte, s.iform = 0, 0, 0, self.iform
-        s.tsurf, s.fwhm = float(self.tsurf), 0.0
+        s.tsurf, s.fwhm = float(self.tsurf), float(self.fwhm)
         s.nem, s.vem, s.emissivity = len(self.vem), f(self.vem), f(self.emissivity)
+        if self.conv is not None:
+            cs = self.conv.as_struct()
+            s.conv = C.pointer(cs)
+            s._keep_conv = cs
         s._keep = self   # keep the arrays alive with the struct
         return s
 
+    @property
+    def nconv(self) -> int:
+        return self.nwave if self.conv is None else len(self.conv.vconv)
+
     def out_shapes(self):
-        return (self.npath * self.nwave,), (self.npath * self.nv * self.nwave,), (self.npath * self.nwave,)
+        nc = self.nconv
+        return (self.npath * nc,), (self.npath * self.nv * nc,), (self.npath * nc,)
 
 
 def _levels(nlayer):

@@ -327,6 +327,77 @@ int rtb_fwd_autotune(rtb_context* ctx, rtb_fwd_tune* out);
 int rtb_fwd_use_graph(rtb_context* ctx, int on);
 
 /* ---------------------------------------------------------------------- */
+/* Layering: profile -> layers and gradient matrices (subpathg set-up)     */
+/* ---------------------------------------------------------------------- */
+
+/* The atmospheric profile LAYERG integrates (the .prf arrays of /PATHCOM/
+ * that subpathg reads: H, P, T, VMR, DUST, with RADIUS and MOLWT), by
+ * pointer, in Fortran layout. */
+typedef struct rtb_profile {
+    int npro, nvmr, ndust;
+    int ld_pro, ld_con;     /* leading dimensions of vmr and dust; 0 = npro, ndust */
+    const float* h;         /* (npro) km, ascending */
+    const float* p;         /* (npro) atm */
+    const float* t;         /* (npro) K */
+    const float* vmr;       /* (ld_pro, nvmr) volume mixing ratios */
+    const float* dust;      /* (ld_con, npro) particles per gram of atmosphere; NULL if ndust == 0 */
+    float molwt;            /* g/mol (AMFORM = 0) */
+    float radius;           /* planet radius, km */
+} rtb_profile;
+
+/* The layering and path keywords of the .pat file (layerg.f:78-126 NLAY,
+ * LAYTYP, LAYINT, LAYHT, LAYANG; atmg.f NADIR angle botlay ipzen, THERM,
+ * BINBB).  laytyp 0 equal pressure, 1 equal log pressure, 2 equal height,
+ * 3 equal path distance, 4 base pressures given (base, nlay values; the
+ * pressure.lay file), 5 base heights given (height.lay); layint 0 layer-
+ * centre values, 1 Curtis-Godson integration (101-point Simpson).  The path
+ * is one nadir thermal-emission path (IMOD 3) through layers botlay..nlay at
+ * `angle` degrees from the nadir (> 90 looks up from the bottom, atmg.f:
+ * 142-147), with ipzen 0 (angle at the bottom layer) or 1 (angle defined at
+ * 0 km, atmg.f:253-257). */
+typedef struct rtb_layer_opts {
+    int nlay, laytyp, layint;
+    float layht, layang;
+    const float* base;      /* laytyp 4 / 5: (nlay) base pressures (atm) / heights (km) */
+    float angle;
+    int botlay;             /* 1-based */
+    int ipzen;
+} rtb_layer_opts;
+
+/* Outputs, in the layout of /LAYCOM/, /LGRAD/ and /PATHCOM/ (caller-owned
+ * host arrays; NULL skips one).  Layer i is the i-th from the bottom. */
+typedef struct rtb_layers {
+    int ld_lay, ld_con;     /* leading dimensions of the 2-D outputs; 0 = nlay, ndust */
+    float* baseh;           /* (nlay) km */
+    float* delh;            /* (nlay) km */
+    float* basep;           /* (nlay) atm */
+    float* baset;           /* (nlay) K */
+    float* press;           /* (nlay) atm, Curtis-Godson */
+    float* temp;            /* (nlay) K */
+    float* totam;           /* (nlay) molecules cm-2 (vertical path) */
+    float* laysf;           /* (nlay) path / vertical length */
+    float* amount;          /* (ld_lay, nvmr) */
+    float* pp;              /* (ld_lay, nvmr) atm */
+    float* cont;            /* (ld_con, nlay) particles cm-2 */
+    float* dte;             /* (ld_lay, npro) d temp / d T(level) */
+    float* dam;             /* (ld_lay, npro) d amount / d vmr(level) */
+    float* dco;             /* (ld_lay, npro) d cont / d dust(level) */
+    /* the path (atmg.f:290-373, 509-560) */
+    int* npath;             /* 1 */
+    int* nlayin;            /* (1) */
+    int* imod;              /* (1) 3 */
+    int* layinc;            /* (nlay) 1-based layers, farthest from the observer last */
+    float* scale;           /* (nlay) */
+    float* emtemp;          /* (nlay) K */
+} rtb_layers;
+
+/* LAYERG (radtran/path/layerg.f:146-458) and the nadir path of ATMG
+ * (radtran/path/atmg.f:290-373) on the device, one warp per layer.  A layer
+ * with a negative pressure, temperature, amount or dust column (the
+ * reference's STOP at layerg.f:460-495) is refused with RTB_ERR_RANGE. */
+int rtb_layerg(rtb_context* ctx, const rtb_profile* prof, const rtb_layer_opts* opts, rtb_layers* out);
+
+/* ---------------------------------------------------------------------- */
 /* Optimal-estimation Newton step (calc_gain_matrix + calcnextxn)          */
 /* ---------------------------------------------------------------------- */
 

@@ -154,6 +154,11 @@ int orc_forward_state(const orc_tables* tab, const rtb_retrieval_spec* s, const 
 int orc_retrieve(const orc_tables* tab, const rtb_retrieval_spec* s, const rtb_retrieval_opts* o, int precision,
                  int nthreads, rtb_retrieval_result* res, orc_retrieval_trace* tr);
 
+/* LAYERG (radtran/path/layerg.f:146-458) and the nadir thermal path of ATMG
+ * (radtran/path/atmg.f:250-373): the same arguments and outputs as
+ * rtb_layerg, in REAL arithmetic */
+int orc_layerg(const rtb_profile* prof, const rtb_layer_opts* opts, rtb_layers* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -269,6 +269,17 @@ def calc_serr(sx, se_diag, dd, aa):
     return tuple(out)
 
 
+def layerg(prof, **opts):
+    """The oracle's LAYERG + nadir ATMG path, same arguments and outputs as
+    Context.layerg."""
+    from radtrancode_b200.cirsradg import layer_call
+    L = lib()
+    st, out = layer_call(lambda p, o, r: L.orc_layerg(p, o, r), prof, **opts)
+    if st != 0:
+        raise RuntimeError(f"oracle status {_abi.STATUS_NAMES.get(st, st)}")
+    return out
+
+
 def cirsconv_ex(vwave, y, fwhm, channels):
     """cirsconv.f:12-246 of one series onto ``channels`` (synth.Channels)."""
     L = lib()

@@ -57,6 +57,32 @@ class RtbAtm(C.Structure):
     ]
 
 
+class RtbProfile(C.Structure):
+    _fields_ = [
+        ("npro", C.c_int), ("nvmr", C.c_int), ("ndust", C.c_int), ("ld_pro", C.c_int), ("ld_con", C.c_int),
+        ("h", _fp), ("p", _fp), ("t", _fp), ("vmr", _fp), ("dust", _fp),
+        ("molwt", C.c_float), ("radius", C.c_float),
+    ]
+
+
+class RtbLayerOpts(C.Structure):
+    _fields_ = [
+        ("nlay", C.c_int), ("laytyp", C.c_int), ("layint", C.c_int),
+        ("layht", C.c_float), ("layang", C.c_float), ("base", _fp),
+        ("angle", C.c_float), ("botlay", C.c_int), ("ipzen", C.c_int),
+    ]
+
+
+class RtbLayers(C.Structure):
+    _fields_ = [
+        ("ld_lay", C.c_int), ("ld_con", C.c_int),
+        ("baseh", _fp), ("delh", _fp), ("basep", _fp), ("baset", _fp), ("press", _fp), ("temp", _fp),
+        ("totam", _fp), ("laysf", _fp), ("amount", _fp), ("pp", _fp), ("cont", _fp),
+        ("dte", _fp), ("dam", _fp), ("dco", _fp),
+        ("npath", _ip), ("nlayin", _ip), ("imod", _ip), ("layinc", _ip), ("scale", _fp), ("emtemp", _fp),
+    ]
+
+
 class RtbFwdStats(C.Structure):
     _fields_ = [
         ("cells", C.c_longlong), ("sort_passes", C.c_longlong), ("tie_passes", C.c_longlong),

@@ -51,6 +51,37 @@ def read_fil(path):
     return vc, ns, vf, fl
 
 
+def layer_call(fn, prof, *, nlay, laytyp=1, layint=1, layht=None, layang=0.0, base=None, angle=0.0, botlay=1,
+               ipzen=0):
+    """Run a layering function with the rtb_layerg arguments (``fn(prof_struct,
+    opts_struct, out_struct) -> status``) and return its outputs as arrays."""
+    o = _abi.RtbLayerOpts()
+    o.nlay, o.laytyp, o.layint = nlay, laytyp, layint
+    o.layht = float(prof.h[0] if layht is None else layht)
+    o.layang = float(layang)
+    b = None if base is None else np.ascontiguousarray(base, np.float32)
+    o.base = _abi.fptr(b)
+    o.angle, o.botlay, o.ipzen = float(angle), botlay, ipzen
+    npro, nvmr = prof.npro, prof.vmr.shape[1]
+    out = {k: np.zeros(nlay, np.float32) for k in ("baseh", "delh", "basep", "baset", "press", "temp", "totam",
+                                                   "laysf", "scale", "emtemp")}
+    out["layinc"] = np.zeros(nlay, np.int32)
+    for k, n in (("amount", nvmr), ("pp", nvmr), ("dte", npro), ("dam", npro), ("dco", npro)):
+        out[k] = np.zeros((nlay, n), np.float32, order="F")
+    ints = {k: np.zeros(1, np.int32) for k in ("npath", "nlayin", "imod")}
+    r = _abi.RtbLayers()
+    r.ld_lay, r.ld_con = nlay, 0
+    for k, v in out.items():
+        setattr(r, k, _abi.iptr(v) if v.dtype == np.int32 else _abi.fptr(v))
+    for k, v in ints.items():
+        setattr(r, k, _abi.iptr(v))
+    ps = prof.as_struct()
+    st = fn(C.byref(ps), C.byref(o), C.byref(r))
+    out.update({k: int(v[0]) for k, v in ints.items()})
+    out["nlay"] = nlay
+    return st, out
+
+
 class Context:
     """One device context (one CUDA device, one host thread at a time)."""
 
@@ -148,6 +179,13 @@ class Context:
         out = np.zeros((y.shape[0], len(channels.vconv)), np.float32)
         self._check(self._L.rtb_cirsconv_ex(self._h, float(fwhm), len(vwave), _abi.fptr(vwave), y.shape[0],
                                             _abi.fptr(y), C.byref(cs), _abi.fptr(out)))
+        return out
+
+    def layerg(self, prof, **opts):
+        """LAYERG + the nadir path of ATMG on the device (rtb_layerg): the
+        layers, gradient matrices and path of a ``synth.Profile``."""
+        st, out = layer_call(lambda p, o, r: self._L.rtb_layerg(self._h, p, o, r), prof, **opts)
+        self._check(st)
         return out
 
     def cirsradg_wave(self, job, isw):

@@ -162,6 +162,7 @@ struct rtb_context {
     std::vector<rtb::ConvSpec> spec_conv;
     int any_conv = 0;
     rtb::DevBuf d_conv, d_convout;
+    rtb::DevBuf d_layer;                  // rtb_layerg inputs, arguments and outputs
     std::vector<char> h_conv;
     size_t dbg_perm_n = 0, dbg_split_n = 0;
     rtb_fwd_stats stats{};

@@ -1002,6 +1002,7 @@ void rtb_destroy(rtb_context* c) {
     c->d_dq.release();
     c->d_conv.release();
     c->d_convout.release();
+    c->d_layer.release();
     c->d_nt32.release();
     c->d_nt64.release();
     c->d_ntsmall.release();

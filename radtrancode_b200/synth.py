@@ -312,6 +312,96 @@ def make_job(tables: KTables, absorbers, *, nlayer, seed, iw0=0, nwave=None, the
                vmr=vmr, ncol=ncol, xscale=xscale)
 
 
+@dataclasses.dataclass
+class Profile:
+    """A .prf-style level profile (the rtb_profile structure): heights (km,
+    ascending), pressures (atm), temperatures (K) and volume mixing ratios
+    [npro, nvmr] of `gases` ([H2, He] + absorbers)."""
+    h: np.ndarray
+    p: np.ndarray
+    t: np.ndarray
+    vmr: np.ndarray
+    gases: list
+    molwt: float = MMW
+    radius: float = 71492.0          # km (Jupiter)
+
+    @property
+    def npro(self):
+        return len(self.h)
+
+    def as_struct(self) -> _abi.RtbProfile:
+        s = _abi.RtbProfile()
+        f = _abi.fptr
+        s.npro, s.nvmr, s.ndust, s.ld_pro, s.ld_con = self.npro, self.vmr.shape[1], 0, self.npro, 0
+        s.h, s.p, s.t, s.vmr, s.dust = f(self.h), f(self.p), f(self.t), f(self.vmr), None
+        s.molwt, s.radius = float(self.molwt), float(self.radius)
+        s._keep = self
+        return s
+
+
+def make_profile(absorbers, *, npro, seed, vmr_perturb=0.3, p_bot_bar=10.0, p_top_bar=1e-4) -> Profile:
+    """Level profile of the synthetic atmosphere: pressures log-spaced from
+    p_bot to p_top, the smooth seeded T(p) of the layer jobs, hydrostatic
+    heights from 0 km at the bottom, and seeded log-normal perturbations of
+    the absorbers' mixing ratios."""
+    rng = np.random.default_rng(seed)
+    p_pa = np.geomspace(p_bot_bar, p_top_bar, npro) * 1e5
+    t = temperature_profile(p_pa, rng)
+    hs = KB * 0.5 * (t[1:] + t[:-1]) / (MMW * AMU * GRAV) / 1e3              # km
+    h = np.concatenate([[0.0], np.cumsum(hs * np.log(p_pa[:-1] / p_pa[1:]))])
+    gases = [H2, HE] + list(absorbers)
+    vmr = np.zeros((npro, len(gases)))
+    for k, g in enumerate(gases):
+        prof = np.full(npro, VMR[g])
+        if vmr_perturb > 0 and k >= 2:
+            prof = prof * np.exp(vmr_perturb * rng.standard_normal(npro))
+        vmr[:, k] = prof
+    return Profile(h=h.astype(np.float32), p=(p_pa / 1e5 * BAR_TO_ATM).astype(np.float32),
+                   t=t.astype(np.float32), vmr=np.asfortranarray(vmr, np.float32), gases=gases)
+
+
+def job_from_layers(tables: KTables, prof: Profile, lay: dict, *, iw0=0, nwave=None) -> Job:
+    """The forward-model job of a layered profile (rtb_layerg / oracle
+    layerg outputs in `lay`): layers, the nadir path and the gradient
+    matrices, with a state of temperature at every profile level (model 0)
+    and one model-3 scale factor per absorber, mapped through DTE / DAM
+    (map2pro.f)."""
+    L = int(lay["nlay"])
+    npro = prof.npro
+    gases = prof.gases
+    ng_ = len(gases)
+    tab_of = {g: i for i, g in enumerate(tables.gases)}
+    ktab = np.array([tab_of.get(g, -1) for g in gases], np.int32)
+    nbin = int(tables.nbin[0])
+    if nwave is None:
+        nwave = nbin - iw0
+    vwave = (tables.vmin[0] + tables.delv[0] * np.arange(iw0, iw0 + nwave, dtype=np.float32)).astype(np.float32)
+    nl = int(lay["nlayin"])
+
+    def col(a, n):
+        out = np.zeros((L, 1), np.float32, order="F")
+        out[:n, 0] = a[:n]
+        return out
+
+    nabs = ng_ - 2
+    nparam = ng_ + 1
+    nv = npro + nabs
+    xmap = np.zeros((nv, nparam, npro), np.float32, order="F")
+    idx = np.arange(npro)
+    xmap[idx, ng_, idx] = 1.0
+    for a in range(nabs):
+        xmap[npro + a, 2 + a, :] = prof.vmr[:, 2 + a]
+    return Job(nlayer=L, ngas=ng_, npath=1, npro=npro, nv=nv, nwave=int(nwave), ld_lay=L, ld_v=nv,
+               ld_param=nparam, press=lay["press"].copy(), temp=lay["temp"].copy(), delh=lay["delh"].copy(),
+               pp=np.asfortranarray(lay["pp"]), amount=np.asfortranarray(lay["amount"]),
+               idgas=np.array([g[0] for g in gases], np.int32), isogas=np.array([g[1] for g in gases], np.int32),
+               ktab=ktab, nlayin=np.array([nl], np.int32), imod=np.array([int(lay["imod"])], np.int32),
+               layinc=col(lay["layinc"].astype(np.int32), nl).astype(np.int32), scale=col(lay["scale"], nl),
+               emtemp=col(lay["emtemp"], nl), dte=np.asfortranarray(lay["dte"]),
+               dam=np.asfortranarray(lay["dam"]), xmap=xmap, vwave=vwave,
+               vem=np.array([0.0, 1e5], np.float32), emissivity=np.array([1.0, 1.0], np.float32))
+
+
 def config1(seed=1001):
     tables = make_ktables([CH4], np_=20, nt=10, ng=20, vmin=1200.0, delv=1.5, nbin=100, seed=seed)
     job = make_job(tables, [CH4], nlayer=40, seed=seed + 1)

@@ -75,13 +75,15 @@ const char* rtb_version(void);
  * READs of get_kg (radtran/cirsradg/get_kg.f:228-304).
  *   ntab            number of tables (one per gas that has a .kta file)
  *   np, nt, ng      table grid (all tables share it, as the /INTERPK/ COMMON
- *                   block of get_kg.f:100-101 does); nt > 0 only
+ *                   block of get_kg.f:100-101 does); nt < 0 selects one
+ *                   temperature grid of |nt| points per pressure (TEMP2)
  *   lnp[np]         log of the table pressures in atm (read_khead.f:81-84)
- *   tk[nt]          table temperatures, K
+ *   tk              table temperatures, K: TEMP(nt), or for nt < 0
+ *                   TEMP2(np, |nt|) column-major (pressure fastest)
  *   delg[ng]        g-ordinate weights (DEL_G)
  *   vmin[ntab], delv[ntab], nbin[ntab]   wavenumber grid of each table
  *                   (delv > 0: regular grid as in get_kg.f:193-208)
- *   data            concatenation over tables of REAL k(ng, nt, np, nbin) in
+ *   data            concatenation over tables of REAL k(ng, |nt|, np, nbin) in
  *                   record order: record = ((ibin*np + ip)*nt + it)*ng + ig,
  *                   i.e. exactly the .kta record order after IREC0, values
  *                   multiplied by 1e20 as stored in the files.

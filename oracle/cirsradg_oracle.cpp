@@ -340,24 +340,55 @@ int noverlapg(const R* delg, int ng, int ngas, const R* amount, const R* k_gn, c
     return RTB_OK;
 }
 
-/* Per-layer position in the k-table grid: get_kg.f:117-141 (NT > 0). */
+/* Per-layer position in the k-table grid: get_kg.f:117-171 (NT > 0, and
+ * NT < 0 with one temperature grid per pressure, TEMP2(NP, |NT|)). */
 template <class R>
 struct LayerK {
     int ioff[4];
     R u, v, dudt;
+    R u2, dudt2;   /* NT < 0: the temperature weight at pressure cp + 1 */
 };
 
 template <class R>
 void layer_prep(const orc_tables& t, const R* p, const R* tt, float press, float temp, LayerK<R>& L) {
     const int np = t.np, nt = t.nt, ng = t.ng;
-    const R pmax = p[np - 1], pmin = p[0], tmax = tt[nt - 1], tmin = tt[0];
     R P1 = Prec<R>::LOG((R)press);
-    if (P1 < pmin) P1 = pmin;
-    if (P1 > pmax) P1 = pmax;
+    if (P1 < p[0]) P1 = p[0];
+    if (P1 > p[np - 1]) P1 = p[np - 1];
     int cp = locate<R>(p, np, P1);
     if (cp < 1) cp = 1;
     if (cp >= np) cp = np - 1;
     L.v = (P1 - p[cp - 1]) / (p[cp] - p[cp - 1]);
+    if (nt < 0) {                                   /* get_kg.f:143-169 */
+        const int nx = -nt;
+        R TN[RTB_MAXK];
+        int ct[2];
+        R u[2], du[2];
+        for (int r = 0; r < 2; ++r) {
+            for (int i = 0; i < nx; ++i) TN[i] = tt[(cp - 1 + r) + (size_t)np * i];
+            R T1 = (R)temp;
+            if (T1 < TN[0]) T1 = TN[0];
+            if (T1 > TN[nx - 1]) T1 = TN[nx - 1];
+            int c = locate<R>(TN, nx, T1);
+            if (c < 1) c = 1;
+            if (c >= nx) c = nx - 1;
+            u[r] = (T1 - TN[c - 1]) / (TN[c] - TN[c - 1]);
+            du[r] = (R)1.0 / (TN[c] - TN[c - 1]);
+            ct[r] = c;
+        }
+        L.u = u[0];
+        L.dudt = du[0];
+        L.u2 = u[1];
+        L.dudt2 = du[1];
+        L.ioff[0] = (nx * ng * (cp - 1)) + (ng * (ct[0] - 1));
+        L.ioff[1] = (nx * ng * cp) + (ng * (ct[1] - 1));
+        L.ioff[2] = (nx * ng * cp) + (ng * ct[1]);
+        L.ioff[3] = (nx * ng * (cp - 1)) + (ng * ct[0]);
+        return;
+    }
+    L.u2 = 0;
+    L.dudt2 = 0;
+    const R tmax = tt[nt - 1], tmin = tt[0];
     R T1 = (R)temp;
     if (T1 < tmin) T1 = tmin;
     if (T1 > tmax) T1 = tmax;
@@ -401,8 +432,8 @@ int select_bin(const orc_tables& t, int itab, float vwave, BinSel& b) {
     if (n1 < 0 || need >= t.nbin[itab]) return RTB_ERR_RANGE;
     /* zero probe over the slice at n1 */
     size_t off = 0;
-    for (int k = 0; k < itab; ++k) off += (size_t)t.nbin[k] * t.np * t.nt * t.ng;
-    const size_t ntab = (size_t)t.np * t.nt * t.ng;
+    for (int k = 0; k < itab; ++k) off += (size_t)t.nbin[k] * t.np * std::abs(t.nt) * t.ng;
+    const size_t ntab = (size_t)t.np * std::abs(t.nt) * t.ng;
     const float* s = t.data + off + (size_t)n1 * ntab;
     bool any = false;
     for (size_t i = 0; i < ntab; ++i) if (s[i] > 0.0f) { any = true; break; }
@@ -412,8 +443,8 @@ int select_bin(const orc_tables& t, int itab, float vwave, BinSel& b) {
 
 const float* table_slice(const orc_tables& t, int itab, int n1) {
     size_t off = 0;
-    for (int k = 0; k < itab; ++k) off += (size_t)t.nbin[k] * t.np * t.nt * t.ng;
-    return t.data + off + (size_t)n1 * t.np * t.nt * t.ng;
+    for (int k = 0; k < itab; ++k) off += (size_t)t.nbin[k] * t.np * std::abs(t.nt) * t.ng;
+    return t.data + off + (size_t)n1 * t.np * std::abs(t.nt) * t.ng;
 }
 
 /* GET_KG interpolation for one layer of one gas: get_kg.f:306-471. */
@@ -422,8 +453,22 @@ void get_kg_layer(const orc_tables& t, const BinSel& b, const float* tab1, const
                   const LayerK<R>& L, const R* delg, R* kout, R* dkout) {
     const int ng = t.ng;
     R k_g[kMaxG], dkdt[kMaxG];
-    const R U = L.u, V = L.v, DUDT = L.dudt;
+    const R U = L.u, V = L.v, DUDT = L.dudt, U2 = L.u2, DUDT2 = L.dudt2;
     const int I1 = L.ioff[0], I2 = L.ioff[1], I3 = L.ioff[2], I4 = L.ioff[3];
+    const bool t2 = t.nt < 0;
+    /* get_kg.f:355-365 / 413-423: X and dX/dT of the four corners */
+    auto interp = [&](R Y1, R Y2, R Y3, R Y4, R& X, R& DXDT) {
+        const R a = (R)1.0 - V, bb = (R)1.0 - U;
+        if (t2) {
+            const R X1 = bb * Y1 + U * Y4;
+            const R X2 = ((R)1.0 - U2) * Y2 + U2 * Y3;
+            X = a * X1 + V * X2;
+            DXDT = a * (-Y1 + Y4) * DUDT + V * (-Y2 + Y3) * DUDT2;
+        } else {
+            X = a * bb * Y1 + V * bb * Y2 + V * U * Y3 + a * U * Y4;
+            DXDT = (-(a * Y1) - V * Y2 + V * Y3 + a * Y4) * DUDT;
+        }
+    };
     if (b.coinc) {
         R Y1 = tab1[I1], Y2 = tab1[I2], Y3 = tab1[I3], Y4 = tab1[I4];
         bool KLOG = !((Y1 <= 0) || (Y2 <= 0) || (Y3 <= 0) || (Y4 <= 0));
@@ -433,9 +478,8 @@ void get_kg_layer(const orc_tables& t, const BinSel& b, const float* tab1, const
                 Y1 = Prec<R>::LOG(Y1); Y2 = Prec<R>::LOG(Y2);
                 Y3 = Prec<R>::LOG(Y3); Y4 = Prec<R>::LOG(Y4);
             }
-            const R a = (R)1.0 - V, bb = (R)1.0 - U;
-            const R X = a * bb * Y1 + V * bb * Y2 + V * U * Y3 + a * U * Y4;
-            const R DXDT = (-(a * Y1) - V * Y2 + V * Y3 + a * Y4) * DUDT;
+            R X, DXDT;
+            interp(Y1, Y2, Y3, Y4, X, DXDT);
             if (KLOG) {
                 k_g[i] = Prec<R>::EXP(X);
                 dkdt[i] = Prec<R>::EXP(X) * DXDT;
@@ -452,9 +496,8 @@ void get_kg_layer(const orc_tables& t, const BinSel& b, const float* tab1, const
             const float* tb = loop == 0 ? tab1 : tab2;
             for (int i = 0; i < ng; ++i) {
                 const R Y1 = tb[I1 + i], Y2 = tb[I2 + i], Y3 = tb[I3 + i], Y4 = tb[I4 + i];
-                const R a = (R)1.0 - V, bb = (R)1.0 - U;
-                const R X = a * bb * Y1 + V * bb * Y2 + V * U * Y3 + a * U * Y4;
-                const R DXDT = (-(a * Y1) - V * Y2 + V * Y3 + a * Y4) * DUDT;
+                R X, DXDT;
+                interp(Y1, Y2, Y3, Y4, X, DXDT);
                 cont[count] = X;
                 dcont[count] = DXDT;
                 fac[count] = delg[i] * w[loop];
@@ -702,8 +745,8 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
     if (a.nlayer > d.ld_lay || a.nlayer > RTB_MAXLAY || a.npath > RTB_MAXPAT ||
         a.ngas > RTB_MAXGAS || a.ncont > RTB_MAXCON || a.npro > RTB_MAXPRO || a.nv > d.ld_v)
         return RTB_ERR_LIMIT;
-    if (t.ng > RTB_MAXG || t.np > RTB_MAXK || t.nt > RTB_MAXK) return RTB_ERR_LIMIT;
-    if (t.ng < 2 || t.nt <= 0) return RTB_ERR_UNSUPPORTED;
+    if (t.ng > RTB_MAXG || t.np > RTB_MAXK || std::abs(t.nt) > RTB_MAXK) return RTB_ERR_LIMIT;
+    if (t.ng < 2 || std::abs(t.nt) < 2) return RTB_ERR_UNSUPPORTED;
     if (a.flagh2p != 0 || a.ilbl != 0 || a.inlte != 0 || a.fwhm != 0.0f) return RTB_ERR_UNSUPPORTED;
     if (!(a.iform == 0 || a.iform == 2)) return RTB_ERR_UNSUPPORTED;
     if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
@@ -1055,9 +1098,10 @@ int run(const orc_tables& t, const rtb_atm& a, double* calcout, double* gradient
                 if (a.xmap[iv + (size_t)d.ld_v * (ip + (size_t)d.ld_param * ipro)] != 0.0f) { on = true; break; }
         if (on) isw.push_back(ip);
     }
-    std::vector<R> p(t.np), tt(t.nt);
+    const size_t ntk = t.nt < 0 ? (size_t)t.np * -t.nt : (size_t)t.nt;   /* TEMP2(NP, |NT|) or TEMP(NT) */
+    std::vector<R> p(t.np), tt(ntk);
     for (int i = 0; i < t.np; ++i) p[i] = (R)t.lnp[i];
-    for (int i = 0; i < t.nt; ++i) tt[i] = (R)t.tk[i];
+    for (size_t i = 0; i < ntk; ++i) tt[i] = (R)t.tk[i];
     std::vector<LayerK<R>> LK(a.nlayer);
     for (int l = 0; l < a.nlayer; ++l) layer_prep<R>(t, p.data(), tt.data(), a.press[l], a.temp[l], LK[l]);
 

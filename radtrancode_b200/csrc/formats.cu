@@ -70,24 +70,30 @@ int read_kta_header(FILE* f, Kta& k, std::string& err) {
         err = "implausible .kta sizes (NP, NT, NG, NPOINT)";
         return RTB_ERR_LIMIT;
     }
-    if (k.nt < 0) {
-        err = ".kta with pressure-dependent temperatures (NT < 0) not supported";
-        return RTB_ERR_UNSUPPORTED;
-    }
     if (!(k.delv > 0.0f)) {
         err = ".kta on an irregular wavenumber grid (DELV <= 0) not supported";
         return RTB_ERR_UNSUPPORTED;
     }
+    // TEMP(NT), or TEMP2(NP, |NT|) stored with the temperature index fastest
+    // (read_khead.f:86-98); kept column-major (pressure fastest) as TEMP2 is
+    const int ntk = k.nt > 0 ? k.nt : k.np * -k.nt;
     k.delg.resize(k.ng);
     k.press.resize(k.np);
-    k.temp.resize(k.nt);
+    std::vector<float> rec(ntk);
     ok = recs4(f, 11 + k.ng, k.ng, k.delg.data()) && recs4(f, 11 + 2 * k.ng + 2, k.np, k.press.data()) &&
-         recs4(f, 11 + 2 * k.ng + 2 + k.np, k.nt, k.temp.data());
+         recs4(f, 11 + 2 * k.ng + 2 + k.np, ntk, rec.data());
     if (!ok) {
         err = "short .kta header arrays";
         return RTB_ERR_ARG;
     }
-    if (k.irec0 < 11 + 2 * k.ng + 2 + k.np + k.nt) {
+    k.temp.resize(ntk);
+    if (k.nt > 0) {
+        k.temp = rec;
+    } else {
+        for (int i = 0; i < k.np; ++i)
+            for (int j = 0; j < -k.nt; ++j) k.temp[i + (size_t)k.np * j] = rec[(size_t)i * -k.nt + j];
+    }
+    if (k.irec0 < 11 + 2 * k.ng + 2 + k.np + ntk) {
         err = "IREC0 points into the .kta header";
         return RTB_ERR_ARG;
     }
@@ -178,7 +184,7 @@ int rtb_load_ktables(rtb_context* c, int ntab, const char* const* paths, int* id
         if (t > 0 && (k.np != hd[0].np || k.nt != hd[0].nt || k.ng != hd[0].ng || k.press != hd[0].press ||
                       k.temp != hd[0].temp || k.delg != hd[0].delg))
             return fail(c, RTB_ERR_UNSUPPORTED, "%s: P/T/g grid differs from %s", paths[t], paths[0]);
-        const size_t n = (size_t)k.npoint * k.np * k.nt * k.ng;
+        const size_t n = (size_t)k.npoint * k.np * std::abs(k.nt) * k.ng;
         const size_t off = data.size();
         data.resize(off + n);
         if (!recs4(fl.f, k.irec0, n, data.data() + off))

@@ -229,13 +229,23 @@ __device__ void rankk_lane(int ng, const float* gw, int nloop, float* cont, floa
     }
 }
 
-// linear bilinear interpolation of one g of one table slice (no logarithms:
-// the non-coincident branch of get_kg.f:396-420)
-__device__ __forceinline__ void interp_lin(const float* t, const LayerDev& L, int g, float& X, float& DXDT) {
-    const float Y1 = __ldg(t + L.ioff[0] + g), Y2 = __ldg(t + L.ioff[1] + g);
-    const float Y3 = __ldg(t + L.ioff[2] + g), Y4 = __ldg(t + L.ioff[3] + g);
+// X and dX/dT of the four (P, T) corners of one g (get_kg.f:355-365 and
+// 413-423): bilinear in (ln p, T) for a table with one temperature grid; for
+// TEMP2 tables (NT < 0) linear in T along each pressure row with its own
+// weight, then linear in ln p
+template <bool t2>
+__device__ __forceinline__ void corners(const LayerDev& L, float Y1, float Y2, float Y3, float Y4, float& X,
+                                        float& DXDT) {
     const float U = L.u, V = L.v;
     const float a = __fsub_rn(1.0f, V), b = __fsub_rn(1.0f, U);
+    if (t2) {
+        const float X1 = __fadd_rn(__fmul_rn(b, Y1), __fmul_rn(U, Y4));
+        const float X2 = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, L.u2), Y2), __fmul_rn(L.u2, Y3));
+        X = __fadd_rn(__fmul_rn(a, X1), __fmul_rn(V, X2));
+        DXDT = __fadd_rn(__fmul_rn(__fmul_rn(a, __fadd_rn(-Y1, Y4)), L.dudt),
+                         __fmul_rn(__fmul_rn(V, __fadd_rn(-Y2, Y3)), L.dudt2));
+        return;
+    }
     X = __fmul_rn(__fmul_rn(a, b), Y1);
     X = __fadd_rn(X, __fmul_rn(__fmul_rn(V, b), Y2));
     X = __fadd_rn(X, __fmul_rn(__fmul_rn(V, U), Y3));
@@ -247,10 +257,20 @@ __device__ __forceinline__ void interp_lin(const float* t, const LayerDev& L, in
     DXDT = __fmul_rn(D, L.dudt);
 }
 
+// linear interpolation of one g of one table slice (no logarithms: the
+// non-coincident branch of get_kg.f:396-420)
+template <bool t2>
+__device__ __forceinline__ void interp_lin(const float* t, const LayerDev& L, int g, float& X, float& DXDT) {
+    const float Y1 = __ldg(t + L.ioff[0] + g), Y2 = __ldg(t + L.ioff[1] + g);
+    const float Y3 = __ldg(t + L.ioff[2] + g), Y4 = __ldg(t + L.ioff[3] + g);
+    corners<t2>(L, Y1, Y2, Y3, Y4, X, DXDT);
+}
+
 // get_kg for a wavenumber between two table points (get_kg.f:380-438):
 // 2 NG linearly interpolated values, weighted (1 - w2) delg and w2 delg,
 // rank-rebinned by rankk on lane 0.  scr: per-warp shared scratch of at least
 // 8 * kMaxNg floats + 2 * kMaxNg shorts.  Called by the whole warp.
+template <bool t2>
 __device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w2, const LayerDev& L, int lane, float* scr,
                                float& k, float& dk) {
     const int ng = B.ng;
@@ -269,7 +289,7 @@ __device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w2, const
         const float w1 = __fsub_rn(1.0f, w2);
         for (int loop = 0; loop < 2; ++loop) {
             float X, D;
-            interp_lin(B.ktab_raw + slice + loop * step, L, lane, X, D);
+            interp_lin<t2>(B.ktab_raw + slice + loop * step, L, lane, X, D);
             cont[loop * ng + lane] = X;
             dcont[loop * ng + lane] = D;
             fac[loop * ng + lane] = __fmul_rn(B.delg[lane], loop ? w2 : w1);
@@ -287,6 +307,7 @@ __device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w2, const
     __syncwarp();
 }
 
+template <bool t2>
 __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, const LayerDev& L, int lane,
                                             float& k, float& dk) {
     k = 0.0f;
@@ -300,17 +321,8 @@ __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, co
     const float* t = klog ? (B.ktab_log + slice) : raw;
     const float Y1 = __ldg(t + L.ioff[0] + lane), Y2 = __ldg(t + L.ioff[1] + lane);
     const float Y3 = __ldg(t + L.ioff[2] + lane), Y4 = __ldg(t + L.ioff[3] + lane);
-    const float U = L.u, V = L.v;
-    const float a = __fsub_rn(1.0f, V), b = __fsub_rn(1.0f, U);
-    float X = __fmul_rn(__fmul_rn(a, b), Y1);
-    X = __fadd_rn(X, __fmul_rn(__fmul_rn(V, b), Y2));
-    X = __fadd_rn(X, __fmul_rn(__fmul_rn(V, U), Y3));
-    X = __fadd_rn(X, __fmul_rn(__fmul_rn(a, U), Y4));
-    float D = -__fmul_rn(a, Y1);
-    D = __fsub_rn(D, __fmul_rn(V, Y2));
-    D = __fadd_rn(D, __fmul_rn(V, Y3));
-    D = __fadd_rn(D, __fmul_rn(a, Y4));
-    const float DXDT = __fmul_rn(D, L.dudt);
+    float X, DXDT;
+    corners<t2>(L, Y1, Y2, Y3, Y4, X, DXDT);
     if (klog) {
         const float e = det_expf(X);
         k = e;
@@ -932,6 +944,10 @@ __device__ __forceinline__ void planck_fp32(int ispace, float vwave, float T, fl
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// t2: the run's k-tables carry one temperature grid per pressure (NT < 0);
+// a template argument so that the usual single-grid kernel carries no trace
+// of the other interpolation
+template <bool t2>
 __global__ void __launch_bounds__(kThreads, 5)
 fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) {
     extern __shared__ __align__(16) char smem[];
@@ -1015,7 +1031,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                 for (int g = 0; g < S.ngas; ++g)
                     if (w2s[g] >= 0.0f) {
                         float kv, dv;
-                        get_kg_lane_nc(B, slices[g], w2s[g], L, lane, (float*)wp.bufA, kv, dv);
+                        get_kg_lane_nc<t2>(B, slices[g], w2s[g], L, lane, (float*)wp.bufA, kv, dv);
                         if (lane < ng) {
                             ncw[(g * kMaxNg + lane) * 2] = kv;
                             ncw[(g * kMaxNg + lane) * 2 + 1] = dv;
@@ -1038,7 +1054,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                     kv = lane < ng ? ncw[(g * kMaxNg + lane) * 2] : 0.0f;
                     dv = lane < ng ? ncw[(g * kMaxNg + lane) * 2 + 1] : 0.0f;
                 } else {
-                    get_kg_lane(B, slices[g], L, lane, kv, dv);
+                    get_kg_lane<t2>(B, slices[g], L, lane, kv, dv);
                 }
             };
             float* colP = colA;
@@ -1289,16 +1305,23 @@ int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath) {
 
 int fwd_blocks_per_sm(int smem) {
     int nb = 0;
-    if (cudaFuncSetAttribute(fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fwd_kernel, kThreads, smem) != cudaSuccess) return 0;
-    return nb;
+    // both instantiations: the smaller residency of the two
+    int nb2 = 0;
+    if (cudaFuncSetAttribute(fwd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+        cudaFuncSetAttribute(fwd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fwd_kernel<false>, kThreads, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, fwd_kernel<true>, kThreads, smem) != cudaSuccess)
+        return 0;
+    return nb < nb2 ? nb : nb2;
 }
 
 cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st) {
     const int smem = fwd_smem_bytes(B.ng, nsw, ncol, nlmax, npath);
-    cudaError_t e = cudaFuncSetAttribute(fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    auto kern = B.t2 ? fwd_kernel<true> : fwd_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    fwd_kernel<<<grid, kThreads, smem, st>>>(B, nsw, ncol, nlmax, npath);
+    kern<<<grid, kThreads, smem, st>>>(B, nsw, ncol, nlmax, npath);
     return cudaGetLastError();
 }
 

@@ -226,7 +226,8 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     S.lg_off = (int64_t)st.amo.size();
     S.lc_off = (int64_t)st.cont.size();
     const int np = c->np, nt = c->nt;
-    const float pmax = c->lnp[np - 1], pmin = c->lnp[0], tmax = c->tk[nt - 1], tmin = c->tk[0];
+    const float pmax = c->lnp[np - 1], pmin = c->lnp[0];
+    const float tmax = nt > 0 ? c->tk[nt - 1] : 0.0f, tmin = nt > 0 ? c->tk[0] : 0.0f;
     for (int l = 0; l < a.nlayer; ++l) {
         LayerDev L;
         memset(&L, 0, sizeof L);
@@ -238,18 +239,47 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         if (cp < 1) cp = 1;
         if (cp >= np) cp = np - 1;
         L.v = (P1 - c->lnp[cp - 1]) / (c->lnp[cp] - c->lnp[cp - 1]);
-        float T1 = a.temp[l];
-        if (T1 < tmin) T1 = tmin;
-        if (T1 > tmax) T1 = tmax;
-        int ct = locate_f(c->tk.data(), nt, T1);
-        if (ct < 1) ct = 1;
-        if (ct >= nt) ct = nt - 1;
-        L.u = (T1 - c->tk[ct - 1]) / (c->tk[ct] - c->tk[ct - 1]);
-        L.dudt = 1.0f / (c->tk[ct] - c->tk[ct - 1]);
-        L.ioff[0] = (nt * ng * (cp - 1)) + (ng * (ct - 1));
-        L.ioff[1] = (nt * ng * cp) + (ng * (ct - 1));
-        L.ioff[2] = (nt * ng * cp) + (ng * ct);
-        L.ioff[3] = (nt * ng * (cp - 1)) + (ng * ct);
+        if (nt < 0) {
+            // one temperature grid per pressure, TEMP2(NP, |NT|) (get_kg.f:143-169): the
+            // bracket and weight at pressure cp, then at cp + 1
+            const int nx = -nt;
+            float TN[RTB_MAXK];
+            int ct[2];
+            float uu[2], du[2];
+            for (int r = 0; r < 2; ++r) {
+                for (int i = 0; i < nx; ++i) TN[i] = c->tk[(cp - 1 + r) + (size_t)np * i];
+                float T1 = a.temp[l];
+                if (T1 < TN[0]) T1 = TN[0];
+                if (T1 > TN[nx - 1]) T1 = TN[nx - 1];
+                int cc = locate_f(TN, nx, T1);
+                if (cc < 1) cc = 1;
+                if (cc >= nx) cc = nx - 1;
+                uu[r] = (T1 - TN[cc - 1]) / (TN[cc] - TN[cc - 1]);
+                du[r] = 1.0f / (TN[cc] - TN[cc - 1]);
+                ct[r] = cc;
+            }
+            L.u = uu[0];
+            L.dudt = du[0];
+            L.u2 = uu[1];
+            L.dudt2 = du[1];
+            L.ioff[0] = (nx * ng * (cp - 1)) + (ng * (ct[0] - 1));
+            L.ioff[1] = (nx * ng * cp) + (ng * (ct[1] - 1));
+            L.ioff[2] = (nx * ng * cp) + (ng * ct[1]);
+            L.ioff[3] = (nx * ng * (cp - 1)) + (ng * ct[0]);
+        } else {
+            float T1 = a.temp[l];
+            if (T1 < tmin) T1 = tmin;
+            if (T1 > tmax) T1 = tmax;
+            int ct = locate_f(c->tk.data(), nt, T1);
+            if (ct < 1) ct = 1;
+            if (ct >= nt) ct = nt - 1;
+            L.u = (T1 - c->tk[ct - 1]) / (c->tk[ct] - c->tk[ct - 1]);
+            L.dudt = 1.0f / (c->tk[ct] - c->tk[ct - 1]);
+            L.ioff[0] = (nt * ng * (cp - 1)) + (ng * (ct - 1));
+            L.ioff[1] = (nt * ng * cp) + (ng * (ct - 1));
+            L.ioff[2] = (nt * ng * cp) + (ng * ct);
+            L.ioff[3] = (nt * ng * (cp - 1)) + (ng * ct);
+        }
         // utotl (cirsradg_wave.f:418-426)
         float u = 0.0f;
         for (int k = 0; k < a.ngas; ++k) u = u + a.amount[l + (size_t)d.ld_lay * k];
@@ -367,7 +397,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
                 if (n1 < 0 || need >= c->nbin[itab])
                     return fail(c, RTB_ERR_RANGE, "wavenumber %g outside k-table %d", vwave, itab);
                 if (c->nonzero[itab][n1])
-                    slice = c->tab_off[itab] + (int64_t)n1 * np * nt * ng;
+                    slice = c->tab_off[itab] + (int64_t)n1 * np * std::abs(nt) * ng;
             }
             st.wg_slice.push_back(slice);
             st.wg_w2.push_back(w2);
@@ -677,7 +707,8 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     B.ktab_raw = (const float*)c->d_raw.p;
     B.ktab_log = (const float*)c->d_log.p;
     B.np = c->np;
-    B.nt = c->nt;
+    B.nt = std::abs(c->nt);
+    B.t2 = c->nt < 0 ? 1 : 0;
     B.ng = c->ng;
     B.delg = (const float*)c->d_delg.p;
     B.g_ord = (const double*)c->d_gord.p;
@@ -1020,9 +1051,10 @@ const char* rtb_last_error(const rtb_context* c) { return c ? c->err.c_str() : "
 int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const float* lnp, const float* tk,
                     const float* delg, const float* vmin, const float* delv, const int* nbin, const float* data) {
     if (!c) return RTB_ERR_ARG;
-    if (ntab <= 0 || np < 2 || nt < 2 || ng < 1 || !lnp || !tk || !delg || !vmin || !delv || !nbin || !data)
+    if (ntab <= 0 || np < 2 || std::abs(nt) < 2 || ng < 1 || !lnp || !tk || !delg || !vmin || !delv || !nbin ||
+        !data)
         return fail(c, RTB_ERR_ARG, "bad k-table arguments");
-    if (np > RTB_MAXK || nt > RTB_MAXK || ng > RTB_MAXG || ntab > RTB_MAXGAS)
+    if (np > RTB_MAXK || std::abs(nt) > RTB_MAXK || ng > RTB_MAXG || ntab > RTB_MAXGAS)
         return fail(c, RTB_ERR_LIMIT, "k-table grid exceeds MAXK/MAXG");
     if (ng > kMaxNg) return fail(c, RTB_ERR_UNSUPPORTED, "NG=%d > %d", ng, kMaxNg);
     // the FP64 cumulative-weight scan is exact in any order when every
@@ -1039,7 +1071,7 @@ int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const floa
     c->nt = nt;
     c->ng = ng;
     c->lnp.assign(lnp, lnp + np);
-    c->tk.assign(tk, tk + nt);
+    c->tk.assign(tk, tk + (nt > 0 ? (size_t)nt : (size_t)np * -nt));   // TEMP(NT) or TEMP2(NP, |NT|)
     c->delg.assign(delg, delg + ng);
     c->g_ord.assign(ng + 1, 0.0);
     for (int i = 0; i < ng; ++i) c->g_ord[i + 1] = c->g_ord[i] + (double)delg[i];
@@ -1049,7 +1081,7 @@ int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const floa
     c->nbin.assign(nbin, nbin + ntab);
     c->tab_off.assign(ntab, 0);
     c->nonzero.assign(ntab, {});
-    const int64_t slice = (int64_t)np * nt * ng;
+    const int64_t slice = (int64_t)np * std::abs(nt) * ng;
     int64_t total = 0;
     for (int t = 0; t < ntab; ++t) {
         if (nbin[t] <= 0) return fail(c, RTB_ERR_ARG, "table %d has no bins", t);

@@ -32,7 +32,7 @@ struct LayerDev {
     float cia_tau;        // height * amagat^2 of nciacon
     float q[5];           // qh2, qhe, qn2, qch4, qco2
     int iabs[5];          // 0-based gas index or -1
-    float taudust;        // unused slot (dust is per wavenumber)
+    float u2, dudt2;      // NT < 0: the temperature weight at pressure cp + 1 (get_kg.f:157-165)
 };
 
 // per-wavenumber constants
@@ -94,7 +94,8 @@ struct BatchDev {
     // tables
     const float* ktab_raw;       // k*1e20, record order
     const float* ktab_log;       // (float)log((double)k)
-    int np, nt, ng;
+    int np, nt, ng;              // nt = |NT|
+    int t2;                      // NT < 0: one temperature grid per pressure (TEMP2)
     const float* delg;           // [ng]
     const double* g_ord;         // [ng+1], g_ord[ng] forced >= 1 (rankg.f:65-67)
     const float* kcia;           // (9,25,1501) Fortran order

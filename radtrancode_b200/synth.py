@@ -49,7 +49,7 @@ class KTables:
     nt: int
     ng: int
     lnp: np.ndarray        # (np,) float32, ln(p / atm)
-    tk: np.ndarray         # (nt,) float32
+    tk: np.ndarray         # (nt,) float32; NT < 0: TEMP2 (np, |nt|) column-major, one grid per pressure
     g_ord: np.ndarray      # (ng,) float32
     delg: np.ndarray       # (ng,) float32
     vmin: np.ndarray       # (ntab,) float32
@@ -63,10 +63,11 @@ class KTables:
         return len(self.gases)
 
     def table(self, i: int) -> np.ndarray:
-        """Table i as an array [nbin, np, nt, ng] (a view)."""
-        n = self.np_ * self.nt * self.ng
+        """Table i as an array [nbin, np, |nt|, ng] (a view)."""
+        nt = abs(self.nt)
+        n = self.np_ * nt * self.ng
         off = int(sum(int(self.nbin[k]) for k in range(i))) * n
-        return self.data[off: off + int(self.nbin[i]) * n].reshape(int(self.nbin[i]), self.np_, self.nt, self.ng)
+        return self.data[off: off + int(self.nbin[i]) * n].reshape(int(self.nbin[i]), self.np_, nt, self.ng)
 
 
 @dataclasses.dataclass
@@ -78,12 +79,20 @@ class CIATable:
 
 def make_ktables(gases, *, np_=20, nt=15, ng=20, vmin=600.0, delv=0.4, nbin=2000, seed=0,
                  p_top_bar=1e-4, p_bot_bar=10.0, t_min=70.0, t_max=200.0, sigma=2.0,
-                 median=1e-22) -> KTables:
-    """Lognormal k-tables, monotone in g, stored x1e20 (cm2 x 1e20)."""
+                 median=1e-22, t2=False) -> KTables:
+    """Lognormal k-tables, monotone in g, stored x1e20 (cm2 x 1e20).  t2:
+    a pressure-dependent temperature grid (NT < 0, TEMP2(NP, |NT|)): row i
+    spans [t_min, t_max] shifted by up to +/-15 K and stretched with
+    pressure."""
     rng = np.random.default_rng(seed)
     p_atm = np.geomspace(p_top_bar, p_bot_bar, np_) * BAR_TO_ATM
     lnp = np.log(p_atm.astype(np.float32).astype(np.float64)).astype(np.float32)
-    tk = np.linspace(t_min, t_max, nt).astype(np.float32)
+    if t2:
+        f = np.linspace(0.0, 1.0, np_)[:, None]
+        grid = t_min - 15.0 + 30.0 * f + (t_max - t_min) * (0.9 + 0.2 * f) * np.linspace(0.0, 1.0, nt)[None, :]
+        tk = np.asfortranarray(grid.astype(np.float32)).ravel(order="F")
+    else:
+        tk = np.linspace(t_min, t_max, nt).astype(np.float32)
     g_ord, delg = gauss_legendre_01(ng)
     mu = np.log(median * 1e20)
     tabs = []
@@ -93,7 +102,7 @@ def make_ktables(gases, *, np_=20, nt=15, ng=20, vmin=600.0, delv=0.4, nbin=2000
         tabs.append(np.exp(mu + sigma * z).astype(np.float32).ravel())
     data = np.concatenate(tabs) if tabs else np.zeros(0, np.float32)
     n = len(gases)
-    return KTables(np_, nt, ng, lnp, tk, g_ord, delg,
+    return KTables(np_, -nt if t2 else nt, ng, lnp, tk, g_ord, delg,
                    np.full(n, vmin, np.float32), np.full(n, delv, np.float32),
                    np.full(n, nbin, np.int32), data, list(gases))
 

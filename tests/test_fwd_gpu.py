@@ -270,3 +270,37 @@ def test_cirsconv_fwhm_matches_oracle(ctx, oracle):
         assert np.max(np.abs(got[s] - ref)) <= 1e-6 * scale, s
     same = ctx.cirsconv(job.vwave, series[:1], 0.0, job.vwave)
     assert np.array_equal(same[0], series[0])
+
+
+@pytest.mark.parametrize("shift", [0.0, 0.13])
+def test_pressure_dependent_temperature_grid(ctx, oracle, shift):
+    """k-tables with one temperature grid per pressure (NT < 0, TEMP2;
+    get_kg.f:143-169, 355-365, 413-423), on table wavenumbers and between
+    them: radiance and Jacobian within tolerance of the FP64 oracle, g-bins
+    bit-exact with the mixed oracle, and the k values differ from those of a
+    single grid."""
+    kt = synth.make_ktables(synth.ABSORBERS_C2, np_=20, nt=15, ng=20, nbin=16, seed=1002, t2=True)
+    assert kt.nt == -15 and kt.tk.shape == (20 * 15,)
+    cia = synth.make_cia(1002)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=40, seed=77, nwave=12, vmr_perturb=0.3)
+    j = _off_grid(job, kt, shift) if shift else job
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_debug(True)
+    try:
+        c, g, gt = ctx.cirsrtfg_wave(j)
+        perm, split = ctx.debug_bins(j)
+    finally:
+        ctx.set_debug(False)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, j.nv) <= JAC_TOL
+    (cm, gm, _), (operm, osplit, _) = oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_MIXED, debug=True)
+    assert np.array_equal(assignment(perm, split, kt.ng), assignment(operm, osplit, kt.ng))
+    assert np.array_equal(split, osplit)
+    # the same k values read through the first pressure row's grid give another spectrum
+    import dataclasses
+    kt1 = dataclasses.replace(kt, nt=15, tk=np.ascontiguousarray(kt.tk[::20]))
+    ctx.set_ktables(kt1)
+    c1, _, _ = ctx.cirsrtfg_wave(j)
+    assert not np.array_equal(c1, c)

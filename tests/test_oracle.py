@@ -175,6 +175,26 @@ def test_mixed_precision_agrees_with_fp64(oracle):
     assert jac_err(g, g64, job.nv) < 1e-4
 
 
+def test_t2_tables_in_both_precisions(oracle):
+    """NT < 0 tables (TEMP2, get_kg.f:143-169): the two precisions agree, and
+    a table whose every pressure row carries the same grid gives the run of
+    the single-grid table (the two interpolations are the same function)."""
+    import dataclasses
+    kt = synth.make_ktables(synth.ABSORBERS_C2, np_=20, nt=15, ng=20, nbin=10, seed=3, t2=True)
+    cia = synth.make_cia(3)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=40, seed=4, nwave=10)
+    c, g, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) < 1e-5
+    assert jac_err(g, g64, job.nv) < 1e-4
+    grid = np.linspace(70.0, 200.0, 15).astype(np.float32)
+    kts = dataclasses.replace(kt, nt=15, tk=grid)
+    ktr = dataclasses.replace(kt, nt=-15, tk=np.repeat(grid, 20))     # TEMP2(i, j) = grid(j)
+    a = oracle.cirsrtfg_wave(kts, cia, job, oracle.ORC_FP64)
+    b = oracle.cirsrtfg_wave(ktr, cia, job, oracle.ORC_FP64)
+    assert rad_err(b[0], a[0]) < 1e-12 and jac_err(b[1], a[1], job.nv) < 1e-11
+
+
 def test_finite_difference_jacobian_fp64(oracle):
     """Analytic dR/dx of the FP64 oracle against central differences of its
     own forward model (temperature of chosen levels, gas scale factors)."""

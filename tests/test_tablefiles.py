@@ -32,12 +32,13 @@ def test_kta_header(tmp_path):
     assert h == (kt.np_, kt.nt, kt.ng, int(kt.nbin[0]), float(kt.vmin[0]), float(kt.delv[0]), 6, 0)
 
 
-def test_kta_unsupported_and_short_files(tmp_path):
+def test_kta_t2_header_and_short_files(tmp_path):
     _lib.build()
-    kt, _, _ = synth.config1()
+    kt = synth.make_ktables([synth.CH4], np_=12, nt=9, ng=10, nbin=4, t2=True)
     p = str(tmp_path / "t2.kta")
-    write_kta(p, kt, 0, 6, 0, nt_sign=-1)           # TEMP2(NP, |NT|) tables
-    assert _header(p)[0] == 3                        # RTB_ERR_UNSUPPORTED
+    write_kta(p, kt, 0, 6, 0)                        # TEMP2(NP, |NT|) tables
+    st, h = _header(p)
+    assert st == 0 and h[:3] == (12, -9, 10)
     q = str(tmp_path / "short.kta")
     open(q, "wb").write(open(p, "rb").read()[:20])
     assert _header(q)[0] == 1                        # RTB_ERR_ARG
@@ -64,3 +65,24 @@ def test_run_from_files_matches_in_memory_tables(ctx, tmp_path):
     assert rad_err(c, c0) <= RAD_TOL
     assert jac_err(g, g0, job.nv) <= JAC_TOL
     ctx.set_ktables(kt)                  # leave the session context as the other tests expect
+
+
+@pytest.mark.gpu
+def test_run_from_t2_files_matches_in_memory_tables(ctx, tmp_path):
+    """.kta files with TEMP2(NP, |NT|) temperatures (read_khead.f:86-93) give
+    the run of the same tables handed over in memory."""
+    kt = synth.make_ktables(synth.ABSORBERS_C2, np_=20, nt=15, ng=20, nbin=12, seed=5, t2=True)
+    cia = synth.make_cia(5)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=40, seed=6, nwave=12)
+    paths = []
+    for i, gas in enumerate(kt.gases):
+        p = str(tmp_path / f"t2gas{i}.kta")
+        write_kta(p, kt, i, gas[0], gas[1])
+        paths.append(p)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c0, g0, _ = ctx.cirsrtfg_wave(job)
+    ctx.load_ktables(paths)
+    c, g, _ = ctx.cirsrtfg_wave(job)
+    assert rad_err(c, c0) <= RAD_TOL
+    assert jac_err(g, g0, job.nv) <= JAC_TOL

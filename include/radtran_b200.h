@@ -82,7 +82,9 @@ const char* rtb_version(void);
  *                   TEMP2(np, |nt|) column-major (pressure fastest)
  *   delg[ng]        g-ordinate weights (DEL_G)
  *   vmin[ntab], delv[ntab], nbin[ntab]   wavenumber grid of each table
- *                   (delv > 0: regular grid as in get_kg.f:193-208)
+ *                   (delv > 0: regular grid as in get_kg.f:193-208; delv <= 0:
+ *                   an irregular grid, the same delv for every table, with
+ *                   the centres given by rtb_set_ktable_centres)
  *   data            concatenation over tables of REAL k(ng, |nt|, np, nbin) in
  *                   record order: record = ((ibin*np + ip)*nt + it)*ng + ig,
  *                   i.e. exactly the .kta record order after IREC0, values
@@ -92,6 +94,14 @@ int rtb_set_ktables(rtb_context* ctx, int ntab, int np, int nt, int ng,
                     const float* lnp, const float* tk, const float* delg,
                     const float* vmin, const float* delv, const int* nbin,
                     const float* data);
+
+/* The centres VCEN(npoint) of irregular k-tables (delv <= 0; read_khead.f:
+ * 100-103), those of the first table as read_klist.f:141-145 keeps them
+ * (npoint = its nbin).  A calculation wavenumber takes the centre nearest in
+ * per cent (delv < 0, coincident) or the nearest at or below it, weighted
+ * with the next by FRACK (delv = 0), read_klist.f:266-310.  Cleared by
+ * rtb_set_ktables. */
+int rtb_set_ktable_centres(rtb_context* ctx, int npoint, const float* vcen);
 
 /* Load a CIA table: replaces the one-time read of ciaread
  * (radtran/radtran/ciaread.f:63-105) into /CIATABLE/.
@@ -104,7 +114,10 @@ int rtb_set_cia(rtb_context* ctx, float dnu, const double* temps, const float* k
  * rtb_load_ktables reads ntab .kta files (read_klist.f / read_khead.f:33-110
  * header, then the records from IREC0 on) and loads them with
  * rtb_set_ktables; the tables must share the P, T and g grid (the /INTERPK/
- * block of get_kg.f:100-101) and a regular wavenumber grid.  idgas/isogas
+ * block of get_kg.f:100-101); irregular tables (DELV <= 0) share DELV and
+ * have their centres (VCEN records) within 1e-4 per cent of the first
+ * table's (read_klist.f:160-176), which are loaded with
+ * rtb_set_ktable_centres.  idgas/isogas
  * (may be NULL) receive each file's gas and isotope ids.
  * rtb_kta_header reads one header (no context needed).
  * rtb_load_cia reads a CIA .tab file (ciaread.f:77-98: sequential

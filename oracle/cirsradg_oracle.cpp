@@ -54,6 +54,37 @@ int locate(const R* xx, int n, R x) {
     return jl;
 }
 
+/* FINDLOC: radtran/cirsrad/findloc.f:13-100.  The 1-based range [I1, I2] of
+ * the grid x inside [y1, y2] (0, 0 when disjoint), the ends snapped to grid
+ * points within 1e-5. */
+void findloc(const float* x, int nx, float y1, float y2, int& I1, int& I2) {
+    const bool up = x[0] < x[nx - 1];
+    const float xbot = up ? x[0] : x[nx - 1], xtop = up ? x[nx - 1] : x[0];
+    const int Ibot = up ? 1 : nx, Itop = up ? nx : 1;
+    if ((y1 < xbot && y2 < xbot) || (y1 > xtop && y2 > xtop)) {
+        I1 = I2 = 0;
+        return;
+    }
+    int I1f, I2f;
+    const float ys[2] = {y1, y2};
+    int* Is[2] = {&I1, &I2};
+    int* fs[2] = {&I1f, &I2f};
+    for (int e = 0; e < 2; ++e) {
+        const float y = ys[e];
+        if (y <= xbot) { *Is[e] = Ibot; *fs[e] = 1; }
+        else if (y >= xtop) { *Is[e] = Itop; *fs[e] = 1; }
+        else {
+            const int it = locate<float>(x, nx, y);
+            *Is[e] = it;
+            *fs[e] = 0;
+            for (int I = it; I <= it + 1; ++I)
+                if (std::fabs(y - x[I - 1]) < 1.e-5f) { *Is[e] = I; *fs[e] = 1; }
+        }
+    }
+    if (y1 < y2) { if (I1f == 0) I1 = I1 + 1; }
+    else { if (I2f == 0) I2 = I2 + 1; }
+}
+
 /* SORT2G: radtran/cirsradg/sort2g.f:1-52, Numerical Recipes heapsort that
  * carries an integer index.  ra/ib are 0-based storage of RA(1..N)/IB(1..N).
  * N < 2 is not reached by the reference path (NG >= 2 checked by caller). */
@@ -412,11 +443,66 @@ struct BinSel {
     bool coinc;
     float w2;
     bool zero;  /* KTEST == 0: all-zero slice (get_kg.f:228-250) */
+    bool irr;   /* irregular grid: the two weights are FRACK and 1 - FRACK */
+    float w1;
 };
+
+/* Irregular grid (delv <= 0, read_klist.f:266-310): the centre nearest in
+ * per cent (delv < 0, snapped, coincident), or nearest at or below the
+ * wavenumber (delv = 0, weighted with the next centre by FRACK). */
+int select_bin_irregular(const orc_tables& t, int itab, float vwave, BinSel& b) {
+    const float delv = t.delv[itab];
+    if (!t.vcen || t.npoint < 1) return RTB_ERR_UNSUPPORTED;
+    const int npoint = t.npoint;
+    int ipo_m = 0;
+    float maxdx1 = 1e10f, frack = 1.0f;
+    for (int ipo = 1; ipo <= npoint; ++ipo) {
+        const float xc = t.vcen[ipo - 1];
+        const float dx = 100.0f * std::fabs((vwave - xc) / xc);
+        if (delv == 0.0f) {
+            if (dx < maxdx1 && xc <= vwave) {
+                ipo_m = ipo;
+                if (ipo < npoint) {
+                    const float dxx = t.vcen[ipo] - xc;
+                    frack = 1.0f - (vwave - xc) / dxx;
+                } else {
+                    frack = 1.0f;
+                }
+                maxdx1 = dx;
+            }
+        } else if (dx < maxdx1) {
+            ipo_m = ipo;
+            frack = 1.0f;
+            maxdx1 = dx;
+        }
+    }
+    if (ipo_m == 0) return RTB_ERR_RANGE;          /* 'Match not found' STOP */
+    b.n1 = ipo_m - 1;
+    b.coinc = delv < 0.0f;                         /* get_kg.f:266-279 */
+    b.irr = true;
+    b.w1 = frack;                                  /* get_kg.f:391-393 */
+    b.w2 = 1.0f - frack;
+    const int need = b.coinc ? b.n1 : b.n1 + 1;
+    if (need >= t.nbin[itab] || (!b.coinc && ipo_m == npoint)) return RTB_ERR_RANGE;
+    return RTB_OK;
+}
 
 int select_bin(const orc_tables& t, int itab, float vwave, BinSel& b) {
     const float vmin = t.vmin[itab], delv = t.delv[itab];
-    if (!(delv > 0.0f)) return RTB_ERR_UNSUPPORTED;  /* irregular tables: not implemented */
+    b.irr = false;
+    b.w1 = 0.0f;
+    if (!(delv > 0.0f)) {
+        const int r = select_bin_irregular(t, itab, vwave, b);
+        if (r) return r;
+        size_t off = 0;
+        for (int k = 0; k < itab; ++k) off += (size_t)t.nbin[k] * t.np * std::abs(t.nt) * t.ng;
+        const size_t ntab = (size_t)t.np * std::abs(t.nt) * t.ng;
+        const float* s = t.data + off + (size_t)b.n1 * ntab;
+        bool any = false;
+        for (size_t i = 0; i < ntab; ++i) if (s[i] > 0.0f) { any = true; break; }
+        b.zero = !any;
+        return RTB_OK;
+    }
     float eps;
     if (delv >= 0.0001f) eps = 0.02f * delv; else eps = 0.25f * delv;
     const int n1 = (int)(((double)vwave + (double)eps - (double)vmin) / (double)delv);
@@ -489,7 +575,7 @@ void get_kg_layer(const orc_tables& t, const BinSel& b, const float* tab1, const
             }
         }
     } else {
-        const R w[2] = {(R)1.0f - (R)b.w2, (R)b.w2};
+        const R w[2] = {b.irr ? (R)b.w1 : (R)1.0f - (R)b.w2, (R)b.w2};
         R cont[2 * kMaxG], dcont[2 * kMaxG], fac[2 * kMaxG];
         int count = 0;
         for (int loop = 0; loop < 2; ++loop) {
@@ -820,6 +906,13 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
         const int itab = a.ktab[k];
         BinSel bs{};
         bool zero = itab < 0;
+        if (!zero && t.delv[itab] > 0.0f) {   /* a wavenumber the table does not cover: no table
+                                                  (read_klist.f:250-265, 341-351) */
+            const float xmax = t.vmin[itab] + (float)(t.nbin[itab] - 1) * t.delv[itab];
+            int i1 = 0, i2 = 0;
+            findloc(a.vwave, a.nwave, t.vmin[itab], xmax, i1, i2);
+            zero = i1 == 0 || i2 == 0 || iw + 1 < i1 || iw + 1 > i2;
+        }
         if (!zero) {
             int st = select_bin(t, itab, vwave, bs);
             if (st) return st;

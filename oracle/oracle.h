@@ -47,6 +47,10 @@ typedef struct orc_tables {
     float dnu;
     const double* cia_temps;
     const float* kcia;
+    /* irregular wavenumber grids (delv <= 0, the same for every table): the
+     * first table's centres VCEN(npoint) (read_klist.f:141-145); else NULL */
+    int npoint;
+    const float* vcen;
 } orc_tables;
 
 /* Debug capture of the g-bin assignment (mixed mode), one record per

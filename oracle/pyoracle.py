@@ -28,6 +28,7 @@ class OrcTables(C.Structure):
         ("data", C.POINTER(C.c_float)),
         ("has_cia", C.c_int), ("dnu", C.c_float), ("cia_temps", C.POINTER(C.c_double)),
         ("kcia", C.POINTER(C.c_float)),
+        ("npoint", C.c_int), ("vcen", C.POINTER(C.c_float)),
     ]
 
 
@@ -72,6 +73,8 @@ def tables_struct(kt, cia=None):
     t.lnp, t.tk, t.delg = _abi.fptr(kt.lnp), _abi.fptr(kt.tk), _abi.fptr(kt.delg)
     t.vmin, t.delv, t.nbin = _abi.fptr(kt.vmin), _abi.fptr(kt.delv), _abi.iptr(kt.nbin)
     t.data = _abi.fptr(kt.data)
+    if kt.vcen is not None:
+        t.npoint, t.vcen = len(kt.vcen), _abi.fptr(kt.vcen)
     if cia is not None:
         t.has_cia, t.dnu = 1, cia.dnu
         t.cia_temps = _abi.dptr(cia.temps)

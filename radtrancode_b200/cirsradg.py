@@ -121,6 +121,8 @@ class Context:
         self._check(self._L.rtb_set_ktables(
             self._h, kt.ntab, kt.np_, kt.nt, kt.ng, _abi.fptr(kt.lnp), _abi.fptr(kt.tk), _abi.fptr(kt.delg),
             _abi.fptr(kt.vmin), _abi.fptr(kt.delv), _abi.iptr(kt.nbin), _abi.fptr(kt.data)))
+        if kt.vcen is not None:     # irregular grid: the first table's centres
+            self._check(self._L.rtb_set_ktable_centres(self._h, len(kt.vcen), _abi.fptr(kt.vcen)))
         self.tables = kt
 
     def load_ktables(self, paths):

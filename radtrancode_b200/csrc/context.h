@@ -70,7 +70,9 @@ struct Staging {
     std::vector<WaveDev> wave;
     std::vector<int64_t> wg_slice;
     std::vector<float> wg_w2;         // [.. nwave][ngas] upper-point weight, < 0 coincident
+    std::vector<float> wg_w1;         // [.. nwave][ngas] lower-point weight of an irregular grid, < 0 none
     bool any_noncoinc = false;
+    bool any_w1 = false;
     std::vector<float> xsec, cont;
     std::vector<int> p_layinc;
     std::vector<float> p_scale, p_emtemp;
@@ -132,6 +134,7 @@ struct rtb_context {
     std::vector<float> vmin, delv;
     std::vector<int> nbin;
     std::vector<int64_t> tab_off;            // element offset of each table
+    std::vector<float> vcen;                 // irregular grids: the first table's centres VCEN(NPOINT)
     std::vector<std::vector<uint8_t>> nonzero;  // [tab][bin]: any value > 0 (get_kg.f:228-250)
     rtb::DevBuf d_raw, d_log, d_delg, d_gord;
     // CIA

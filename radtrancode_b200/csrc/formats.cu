@@ -42,7 +42,7 @@ struct File {
 struct Kta {
     int irec0 = 0, npoint = 0, np = 0, nt = 0, ng = 0, idgas = 0, isogas = 0;
     float vmin = 0, delv = 0, fwhm = 0;
-    std::vector<float> press, temp, delg;
+    std::vector<float> press, temp, delg, vcen;
 };
 
 // 1-based 4-byte record n of a direct-access file
@@ -70,10 +70,6 @@ int read_kta_header(FILE* f, Kta& k, std::string& err) {
         err = "implausible .kta sizes (NP, NT, NG, NPOINT)";
         return RTB_ERR_LIMIT;
     }
-    if (!(k.delv > 0.0f)) {
-        err = ".kta on an irregular wavenumber grid (DELV <= 0) not supported";
-        return RTB_ERR_UNSUPPORTED;
-    }
     // TEMP(NT), or TEMP2(NP, |NT|) stored with the temperature index fastest
     // (read_khead.f:86-98); kept column-major (pressure fastest) as TEMP2 is
     const int ntk = k.nt > 0 ? k.nt : k.np * -k.nt;
@@ -93,7 +89,16 @@ int read_kta_header(FILE* f, Kta& k, std::string& err) {
         for (int i = 0; i < k.np; ++i)
             for (int j = 0; j < -k.nt; ++j) k.temp[i + (size_t)k.np * j] = rec[(size_t)i * -k.nt + j];
     }
-    if (k.irec0 < 11 + 2 * k.ng + 2 + k.np + ntk) {
+    // the centres of an irregular grid (read_khead.f:100-103)
+    const int nvc = k.delv > 0.0f ? 0 : k.npoint;
+    if (nvc) {
+        k.vcen.resize(nvc);
+        if (!recs4(f, 11 + 2 * k.ng + 2 + k.np + ntk, nvc, k.vcen.data())) {
+            err = "short .kta centre records";
+            return RTB_ERR_ARG;
+        }
+    }
+    if (k.irec0 < 11 + 2 * k.ng + 2 + k.np + ntk + nvc) {
         err = "IREC0 points into the .kta header";
         return RTB_ERR_ARG;
     }
@@ -196,10 +201,18 @@ int rtb_load_ktables(rtb_context* c, int ntab, const char* const* paths, int* id
         if (isogas) isogas[t] = k.isogas;
     }
     const Kta& k0 = hd[0];
+    // irregular grids: every table's centres those of the first within MAXDX = 1e-4 per cent (read_klist.f:160-176)
+    for (int t = 1; t < ntab && !k0.vcen.empty(); ++t)
+        for (size_t j = 0; j < hd[t].vcen.size() && j < k0.vcen.size(); ++j) {
+            const float dx = 100.0f * std::fabs((hd[t].vcen[j] - k0.vcen[j]) / hd[t].vcen[j]);
+            if (dx > 1e-4f) return fail(c, RTB_ERR_ARG, "%s: wave centre %zu differs from %s", paths[t], j + 1, paths[0]);
+        }
     std::vector<float> lnp(k0.np);
     for (int i = 0; i < k0.np; ++i) lnp[i] = logf(k0.press[i]);   // PRESS(J) = LOG(PRESS(J)), read_khead.f:83
-    return rtb_set_ktables(c, ntab, k0.np, k0.nt, k0.ng, lnp.data(), k0.temp.data(), k0.delg.data(), vmin.data(),
-                           delv.data(), nbin.data(), data.data());
+    const int r = rtb_set_ktables(c, ntab, k0.np, k0.nt, k0.ng, lnp.data(), k0.temp.data(), k0.delg.data(),
+                                  vmin.data(), delv.data(), nbin.data(), data.data());
+    if (r || k0.vcen.empty()) return r;
+    return rtb_set_ktable_centres(c, k0.npoint, k0.vcen.data());
 }
 
 int rtb_load_cia(rtb_context* c, const char* path, float dnu) {

@@ -271,7 +271,8 @@ __device__ __forceinline__ void interp_lin(const float* t, const LayerDev& L, in
 // rank-rebinned by rankk on lane 0.  scr: per-warp shared scratch of at least
 // 8 * kMaxNg floats + 2 * kMaxNg shorts.  Called by the whole warp.
 template <bool t2>
-__device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w2, const LayerDev& L, int lane, float* scr,
+__device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w1, float w2, const LayerDev& L, int lane,
+                               float* scr,
                                float& k, float& dk) {
     const int ng = B.ng;
     float* cont = scr;
@@ -286,7 +287,6 @@ __device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w2, const
     if (slice < 0) return;
     if (lane < ng) {
         const int64_t step = (int64_t)B.np * B.nt * ng;
-        const float w1 = __fsub_rn(1.0f, w2);
         for (int loop = 0; loop < 2; ++loop) {
             float X, D;
             interp_lin<t2>(B.ktab_raw + slice + loop * step, L, lane, X, D);
@@ -1031,7 +1031,9 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                 for (int g = 0; g < S.ngas; ++g)
                     if (w2s[g] >= 0.0f) {
                         float kv, dv;
-                        get_kg_lane_nc<t2>(B, slices[g], w2s[g], L, lane, (float*)wp.bufA, kv, dv);
+                        const float w1 = B.wg_w1 ? B.wg_w1[S.wg_off + (int64_t)iw * S.ngas + g]
+                                                 : __fsub_rn(1.0f, w2s[g]);
+                        get_kg_lane_nc<t2>(B, slices[g], w1, w2s[g], L, lane, (float*)wp.bufA, kv, dv);
                         if (lane < ng) {
                             ncw[(g * kMaxNg + lane) * 2] = kv;
                             ncw[(g * kMaxNg + lane) * 2 + 1] = dv;

@@ -54,6 +54,56 @@ int locate_f(const float* xx, int n, float x) {
     return jl;
 }
 
+// FINDLOC (radtran/cirsrad/findloc.f:13-100): the 1-based index range
+// [I1, I2] of the calculation grid x that a table spanning [y1, y2] covers;
+// 0, 0 when the table lies wholly outside it
+void findloc_f(const float* x, int nx, float y1, float y2, int& I1, int& I2) {
+    float xbot, xtop;
+    int Ibot, Itop;
+    if (x[0] < x[nx - 1]) {
+        xbot = x[0];
+        xtop = x[nx - 1];
+        Ibot = 1;
+        Itop = nx;
+    } else {
+        xbot = x[nx - 1];
+        xtop = x[0];
+        Ibot = nx;
+        Itop = 1;
+    }
+    if ((y1 < xbot && y2 < xbot) || (y1 > xtop && y2 > xtop)) {
+        I1 = 0;
+        I2 = 0;
+        return;
+    }
+    auto end = [&](float y, int& I, int& exact) {
+        if (y <= xbot) {
+            I = Ibot;
+            exact = 1;
+        } else if (y >= xtop) {
+            I = Itop;
+            exact = 1;
+        } else {
+            const int it = locate_f(x, nx, y);
+            I = it;
+            exact = 0;
+            for (int i = it; i <= it + 1; ++i)
+                if (std::fabs(y - x[i - 1]) < 1.e-5f) {
+                    I = i;
+                    exact = 1;
+                }
+        }
+    };
+    int f1 = 0, f2 = 0;
+    end(y1, I1, f1);
+    end(y2, I2, f2);
+    if (y1 < y2) {
+        if (f1 == 0) I1 = I1 + 1;
+    } else {
+        if (f2 == 0) I2 = I2 + 1;
+    }
+}
+
 // PINDEX (radtran/radtran/read_ktable.f:201-226); clamps x1 in place, 1-based
 int pindex_f(const float* x, int nx, float& x1) {
     if (x1 > x[nx - 1]) x1 = x[nx - 1];
@@ -346,6 +396,25 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         vvk1.resize(RTB_CIA_NUMWN);
         for (int i = 0; i < RTB_CIA_NUMWN; ++i) vvk1[i] = (float)i * c->dnu;
     }
+    // the calculation wavenumbers each gas's table covers (read_klist.f:250-265);
+    // outside them the gas has no table there (lun = -99, read_klist.f:341-351)
+    std::vector<int> cov_lo(a.ngas, 0), cov_hi(a.ngas, -1);
+    for (int k = 0; k < a.ngas; ++k) {
+        const int itab = a.ktab[k];
+        if (itab < 0) continue;
+        if (!(c->delv[itab] > 0.0f)) {   // an irregular grid serves every wavenumber (read_klist.f:266-321)
+            cov_lo[k] = 1;
+            cov_hi[k] = a.nwave;
+            continue;
+        }
+        const float xmax = c->vmin[itab] + (float)(c->nbin[itab] - 1) * c->delv[itab];
+        int i1 = 0, i2 = 0;
+        findloc_f(a.vwave, a.nwave, c->vmin[itab], xmax, i1, i2);
+        if (i1 != 0 && i2 != 0) {
+            cov_lo[k] = i1;
+            cov_hi[k] = i2;
+        }
+    }
     for (int iw = 0; iw < a.nwave; ++iw) {
         WaveDev W;
         memset(&W, 0, sizeof W);
@@ -372,14 +441,56 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
             W.gradground_s = esurf * dB;
         }
         st.wave.push_back(W);
+        // irregular grid (delv <= 0, shared by every table): the centre of this
+        // wavenumber, nearest in per cent (delv < 0) or nearest at or below it
+        // with FRACK (delv = 0), read_klist.f:266-310
+        int irr_ipo = 0;
+        float irr_frack = 1.0f;
+        if (!c->vcen.empty()) {
+            const int npoint = (int)c->vcen.size();
+            const float delv0 = c->delv[0];
+            float maxdx1 = 1e10f;
+            for (int ipo = 1; ipo <= npoint; ++ipo) {
+                const float xc = c->vcen[ipo - 1];
+                const float dx = 100.0f * std::fabs((vwave - xc) / xc);
+                if (delv0 == 0.0f) {
+                    if (dx < maxdx1 && xc <= vwave) {
+                        irr_ipo = ipo;
+                        irr_frack = ipo < npoint ? 1.0f - (vwave - xc) / (c->vcen[ipo] - xc) : 1.0f;
+                        maxdx1 = dx;
+                    }
+                } else if (dx < maxdx1) {
+                    irr_ipo = ipo;
+                    irr_frack = 1.0f;
+                    maxdx1 = dx;
+                }
+            }
+            if (irr_ipo == 0)
+                return fail(c, RTB_ERR_RANGE, "no k-table centre at or below %g (read_klist.f:314-318)", vwave);
+        }
         // table record choice (get_kg.f:189-275)
         for (int k = 0; k < a.ngas; ++k) {
             const int itab = a.ktab[k];
             int64_t slice = -1;
             float w2 = -1.0f;                  // < 0: coincident wavenumber
-            if (itab >= 0) {
+            float w1 = -1.0f;                  // irregular grid: the lower record's weight FRACK
+            if (itab >= 0 && iw + 1 >= cov_lo[k] && iw + 1 <= cov_hi[k] && !(c->delv[itab] > 0.0f)) {
+                if (c->vcen.empty()) return fail(c, RTB_ERR_ARG, "irregular k-tables without centres (rtb_set_ktable_centres)");
+                const int n1 = irr_ipo - 1;
+                const bool coinc = c->delv[itab] < 0.0f;          // get_kg.f:266-279
+                if (!coinc) {
+                    if (irr_ipo == (int)c->vcen.size())
+                        return fail(c, RTB_ERR_RANGE, "wavenumber %g above the last k-table centre", vwave);
+                    w1 = irr_frack;                                // get_kg.f:391-393
+                    w2 = 1.0f - irr_frack;
+                    st.any_noncoinc = true;
+                    st.any_w1 = true;
+                }
+                const int need = coinc ? n1 : n1 + 1;
+                if (need >= c->nbin[itab]) return fail(c, RTB_ERR_RANGE, "k-table %d has no record %d", itab, need);
+                if (c->nonzero[itab][n1]) slice = c->tab_off[itab] + (int64_t)n1 * np * std::abs(nt) * ng;
+            } else if (itab >= 0 && iw + 1 >= cov_lo[k] && iw + 1 <= cov_hi[k]) {
                 const float vmin = c->vmin[itab], delv = c->delv[itab];
-                if (!(delv > 0.0f)) return fail(c, RTB_ERR_UNSUPPORTED, "irregular k-table grid (delv <= 0)");
                 float eps;
                 if (delv >= 0.0001f) eps = 0.02f * delv; else eps = 0.25f * delv;
                 const int n1 = (int)(((double)vwave + (double)eps - (double)vmin) / (double)delv);
@@ -401,6 +512,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
             }
             st.wg_slice.push_back(slice);
             st.wg_w2.push_back(w2);
+            st.wg_w1.push_back(w1);
         }
         for (int k = 0; k < a.ncont; ++k) st.xsec.push_back(a.xsec_ext[k + (size_t)a.ncont * iw]);
     }
@@ -555,6 +667,7 @@ void append_staging(Staging& dst, const Staging& src) {
     append_vec(dst.wave, src.wave);
     append_vec(dst.wg_slice, src.wg_slice);
     append_vec(dst.wg_w2, src.wg_w2);
+    append_vec(dst.wg_w1, src.wg_w1);
     append_vec(dst.xsec, src.xsec);
     append_vec(dst.cont, src.cont);
     append_vec(dst.p_layinc, src.p_layinc);
@@ -570,6 +683,7 @@ void append_staging(Staging& dst, const Staging& src) {
     dst.npath_max = std::max(dst.npath_max, src.npath_max);
     dst.ngas_max = std::max(dst.ngas_max, src.ngas_max);
     dst.any_noncoinc = dst.any_noncoinc || src.any_noncoinc;
+    dst.any_w1 = dst.any_w1 || src.any_w1;
     dst.n_out += src.n_out;
     dst.n_jac += src.n_jac;
 }
@@ -663,6 +777,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     const size_t i_wave = add(st.wave.data(), bytes_of(st.wave));
     const size_t i_wg = add(st.wg_slice.data(), bytes_of(st.wg_slice));
     const size_t i_w2 = add(st.wg_w2.data(), st.any_noncoinc ? bytes_of(st.wg_w2) : 0);
+    const size_t i_w1 = add(st.wg_w1.data(), st.any_w1 ? bytes_of(st.wg_w1) : 0);
     const size_t i_xsec = add(st.xsec.data(), bytes_of(st.xsec));
     const size_t i_cont = add(st.cont.data(), bytes_of(st.cont));
     const size_t i_pl = add(st.p_layinc.data(), bytes_of(st.p_layinc));
@@ -696,6 +811,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     B.wave = (const WaveDev*)dp(i_wave);
     B.wg_slice = (const int64_t*)dp(i_wg);
     B.wg_w2 = st.any_noncoinc ? (const float*)dp(i_w2) : nullptr;
+    B.wg_w1 = st.any_w1 ? (const float*)dp(i_w1) : nullptr;
     B.xsec = (const float*)dp(i_xsec);
     B.cont = (const float*)dp(i_cont);
     B.p_layinc = (const int*)dp(i_pl);
@@ -1048,6 +1164,21 @@ void rtb_destroy(rtb_context* c) {
 
 const char* rtb_last_error(const rtb_context* c) { return c ? c->err.c_str() : "no context"; }
 
+int rtb_set_ktable_centres(rtb_context* c, int npoint, const float* vcen) {
+    if (!c) return RTB_ERR_ARG;
+    if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
+    if (c->delv[0] > 0.0f) return fail(c, RTB_ERR_ARG, "k-table centres are for irregular grids (DELV <= 0)");
+    if (!vcen || npoint != c->nbin[0]) return fail(c, RTB_ERR_ARG, "centres: npoint %d, the first table has %d", npoint, c->nbin[0]);
+    for (int t = 0; t < c->ntab; ++t)
+        if (c->nbin[t] < npoint)
+            return fail(c, RTB_ERR_UNSUPPORTED, "k-table %d has %d records, fewer than the %d centres", t, c->nbin[t],
+                        npoint);
+    for (int i = 0; i < npoint; ++i)
+        if (!(vcen[i] != 0.0f)) return fail(c, RTB_ERR_ARG, "k-table centre %d is zero", i);
+    c->vcen.assign(vcen, vcen + npoint);
+    return RTB_OK;
+}
+
 int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const float* lnp, const float* tk,
                     const float* delg, const float* vmin, const float* delv, const int* nbin, const float* data) {
     if (!c) return RTB_ERR_ARG;
@@ -1065,6 +1196,11 @@ int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const floa
         sdelg += delg[i];
     }
     if (sdelg > 1.5) return fail(c, RTB_ERR_UNSUPPORTED, "sum of delg > 1.5");
+    // an irregular grid (DELV <= 0) is one DELV for every table (read_klist.f:147-158)
+    for (int t = 0; t < ntab; ++t)
+        if ((!(delv[t] > 0.0f) || !(delv[0] > 0.0f)) && delv[t] != delv[0])
+            return fail(c, RTB_ERR_ARG, "k-table %d: DELV %g differs from the first table's %g (read_klist.f:147-158)", t,
+                        (double)delv[t], (double)delv[0]);
     CUDA_TRY(c, cudaSetDevice(c->device));
     c->ntab = 0;
     c->np = np;
@@ -1072,6 +1208,7 @@ int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const floa
     c->ng = ng;
     c->lnp.assign(lnp, lnp + np);
     c->tk.assign(tk, tk + (nt > 0 ? (size_t)nt : (size_t)np * -nt));   // TEMP(NT) or TEMP2(NP, |NT|)
+    c->vcen.clear();
     c->delg.assign(delg, delg + ng);
     c->g_ord.assign(ng + 1, 0.0);
     for (int i = 0; i < ng; ++i) c->g_ord[i + 1] = c->g_ord[i] + (double)delg[i];

@@ -83,6 +83,7 @@ struct BatchDev {
     const WaveDev* wave;
     const int64_t* wg_slice;     // [.. nwave][ngas] element offset of the table slice, -1 = zero
     const float* wg_w2;          // [.. nwave][ngas] non-coincident weight of slice+1 (< 0: coincident); may be null
+    const float* wg_w1;          // [.. nwave][ngas] weight of slice (irregular grids); null: 1 - wg_w2
     const float* xsec;           // [.. nwave][ncont]
     const float* cont;           // [.. nlayer][ncont]
     const int* p_layinc;         // [.. npath][nlmax] 0-based layer

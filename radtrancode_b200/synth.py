@@ -57,6 +57,7 @@ class KTables:
     nbin: np.ndarray       # (ntab,) int32
     data: np.ndarray       # concatenated float32 records
     gases: list            # (id, iso) of each table
+    vcen: np.ndarray | None = None   # irregular grid (delv <= 0): the centres, (nbin,) float32
 
     @property
     def ntab(self) -> int:
@@ -79,7 +80,7 @@ class CIATable:
 
 def make_ktables(gases, *, np_=20, nt=15, ng=20, vmin=600.0, delv=0.4, nbin=2000, seed=0,
                  p_top_bar=1e-4, p_bot_bar=10.0, t_min=70.0, t_max=200.0, sigma=2.0,
-                 median=1e-22, t2=False) -> KTables:
+                 median=1e-22, t2=False, irregular=None) -> KTables:
     """Lognormal k-tables, monotone in g, stored x1e20 (cm2 x 1e20).  t2:
     a pressure-dependent temperature grid (NT < 0, TEMP2(NP, |NT|)): row i
     spans [t_min, t_max] shifted by up to +/-15 K and stretched with
@@ -102,9 +103,14 @@ def make_ktables(gases, *, np_=20, nt=15, ng=20, vmin=600.0, delv=0.4, nbin=2000
         tabs.append(np.exp(mu + sigma * z).astype(np.float32).ravel())
     data = np.concatenate(tabs) if tabs else np.zeros(0, np.float32)
     n = len(gases)
+    vcen = None
+    if irregular is not None:
+        # an irregular grid: DELV = irregular (0 or -1), centres vmin + delv * (i + a seeded jitter of +/-0.3)
+        vcen = (vmin + delv * (np.arange(nbin) + rng.uniform(-0.3, 0.3, nbin))).astype(np.float32)
+        delv = float(irregular)
     return KTables(np_, -nt if t2 else nt, ng, lnp, tk, g_ord, delg,
                    np.full(n, vmin, np.float32), np.full(n, delv, np.float32),
-                   np.full(n, nbin, np.int32), data, list(gases))
+                   np.full(n, nbin, np.int32), data, list(gases), vcen)
 
 
 def make_cia(seed=0, dnu=1.0) -> CIATable:

@@ -4,8 +4,9 @@ write_kta follows the record layout of radtran/radtran/calc_fnktablec.f:
 304-367 (direct access, 4-byte records): IREC0, NPOINT, VMIN, DELV, FWHM,
 NP, NT, NG, IDGAS, ISOGAS, G_ORD(NG), DEL_G(NG), two spare records,
 PRESS(NP) in atm, TEMP(NT) -- or for NT < 0 TEMP2(NP, |NT|) with the
-temperature index fastest (read_khead.f:87-93) -- then the k values (x 1e20)
-from record IREC0, bin by bin with g fastest.  write_cia_tab writes the two sequential
+temperature index fastest (read_khead.f:87-93) -- and VCEN(NPOINT) when
+DELV <= 0, then the k values (x 1e20) from record IREC0, bin by bin with g
+fastest.  write_cia_tab writes the two sequential
 unformatted records that ciaread.f:77-98 reads."""
 import numpy as np
 
@@ -13,7 +14,8 @@ import numpy as np
 def write_kta(path, kt, i, idgas, isogas):
     ng, np_, nt = kt.ng, kt.np_, kt.nt
     ntk = nt if nt > 0 else np_ * -nt
-    irec0 = 11 + 2 * ng + 2 + np_ + ntk + 2
+    nvc = int(kt.nbin[i]) if not kt.delv[i] > 0 else 0      # VCEN(NPOINT) of an irregular grid
+    irec0 = 11 + 2 * ng + 2 + np_ + ntk + nvc + 2
     head = np.zeros(irec0 - 1, np.int32)
     f = head.view(np.float32)
     head[0], head[1] = irec0, int(kt.nbin[i])
@@ -27,6 +29,8 @@ def write_kta(path, kt, i, idgas, isogas):
         f[o + np_:o + np_ + nt] = kt.tk
     else:   # TEMP2(I, J) records, J fastest
         f[o + np_:o + np_ + ntk] = kt.tk.reshape(-nt, np_).T.ravel()
+    if nvc:
+        f[o + np_ + ntk:o + np_ + ntk + nvc] = kt.vcen
     with open(path, "wb") as fh:
         fh.write(head.tobytes())
         fh.write(np.ascontiguousarray(kt.table(i), np.float32).tobytes())

@@ -152,10 +152,6 @@ def test_unsupported_options_raise(ctx):
     with pytest.raises(cirsradg.RtbError, match="UNSUPPORTED"):
         ctx.cirsrtfg_wave(j)
     j = copy.deepcopy(job)
-    j.vwave = j.vwave + np.float32(0.7)        # the last one needs a table point past the grid (get_kg.f:210-226)
-    with pytest.raises(cirsradg.RtbError, match="RANGE"):
-        ctx.cirsrtfg_wave(j)
-    j = copy.deepcopy(job)
     j.vem = np.array([1250.0, 1300.0], np.float32)   # interpem.f range error
     with pytest.raises(cirsradg.RtbError, match="RANGE"):
         ctx.cirsrtfg_wave(j)
@@ -304,3 +300,69 @@ def test_pressure_dependent_temperature_grid(ctx, oracle, shift):
     ctx.set_ktables(kt1)
     c1, _, _ = ctx.cirsrtfg_wave(j)
     assert not np.array_equal(c1, c)
+
+
+def test_tables_covering_part_of_the_spectrum(ctx, oracle):
+    """A table covers the calculation wavenumbers FINDLOC finds inside
+    [VMIN, VMIN + (NPOINT-1) DELV] (read_klist.f:250-265); elsewhere its gas
+    has no table (lun = -99, zero k; read_klist.f:341-351), including the
+    last wavenumber of a grid shifted past the table's end.  Radiance and
+    Jacobian within tolerance of the FP64 oracle; an uncovered gas's scale
+    derivative is zero there and not elsewhere."""
+    import dataclasses
+    kt, cia, _ = synth.config2(nwave=40, nlayer=30, nbin=40)
+    ktc = dataclasses.replace(kt, vmin=np.array([600.0, 604.0, 596.0, 600.0], np.float32))
+    job = synth.make_job(ktc, synth.ABSORBERS_C2, nlayer=30, seed=31, nwave=40)
+    ctx.set_ktables(ktc)
+    ctx.set_cia(cia)
+    c, g, _ = ctx.cirsrtfg_wave(job)
+    c64, g64, _ = oracle.cirsrtfg_wave(ktc, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+    G = g.reshape(job.nv, job.nwave)
+    L = job.nlayer
+    assert np.all(G[L + 1, :10] == 0) and np.all(G[L + 1, 10:] != 0)     # the C2H6 table starts at 604
+    assert np.all(G[L + 2, 30:] == 0) and np.all(G[L + 2, :30] != 0)     # the C2H2 table ends at 611.6
+    j = copy.deepcopy(job)
+    j.vwave = j.vwave + np.float32(0.15)      # the last wavenumber is past the CH4 / NH3 tables' end
+    c, g, _ = ctx.cirsrtfg_wave(j)
+    c64, g64, _ = oracle.cirsrtfg_wave(ktc, cia, j, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, j.nv) <= JAC_TOL
+    assert g.reshape(j.nv, j.nwave)[L + 3, -1] == 0
+
+
+@pytest.mark.parametrize("delv", [-1.0, 0.0])
+def test_irregular_wavenumber_grid(ctx, oracle, delv):
+    """k-tables on an irregular grid (DELV <= 0, centres VCEN): DELV < 0
+    snaps each wavenumber to the centre nearest in per cent (coincident),
+    DELV = 0 weights the centre at or below it and the next by FRACK
+    (read_klist.f:266-310, get_kg.f:209-279, 391-393).  Radiance and
+    Jacobian within tolerance of the FP64 oracle, g-bins bit-exact with the
+    mixed oracle."""
+    kt = synth.make_ktables(synth.ABSORBERS_C2, np_=20, nt=15, ng=20, nbin=24, seed=41, irregular=delv)
+    cia = synth.make_cia(41)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=40, seed=42, nwave=16)
+    job.vwave = (600.0 + 0.4 * (np.arange(16) + 1) + 0.07).astype(np.float32)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_debug(True)
+    try:
+        c, g, gt = ctx.cirsrtfg_wave(job)
+        perm, split = ctx.debug_bins(job)
+    finally:
+        ctx.set_debug(False)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+    (cm, gm, _), (operm, osplit, _) = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED, debug=True)
+    assert np.array_equal(assignment(perm, split, kt.ng), assignment(operm, osplit, kt.ng))
+    assert np.array_equal(split, osplit)
+    # below the first centre there is no record at or below the wavenumber (read_klist.f:314-318)
+    if delv == 0.0:
+        from radtrancode_b200 import cirsradg
+        j = copy.deepcopy(job)
+        j.vwave = (j.vwave - np.float32(2.0)).astype(np.float32)
+        with pytest.raises(cirsradg.RtbError, match="RANGE"):
+            ctx.cirsrtfg_wave(j)
+

@@ -86,3 +86,27 @@ def test_run_from_t2_files_matches_in_memory_tables(ctx, tmp_path):
     c, g, _ = ctx.cirsrtfg_wave(job)
     assert rad_err(c, c0) <= RAD_TOL
     assert jac_err(g, g0, job.nv) <= JAC_TOL
+
+
+@pytest.mark.gpu
+def test_run_from_irregular_files_matches_in_memory_tables(ctx, tmp_path):
+    """.kta files on an irregular grid (DELV = 0, VCEN records,
+    read_khead.f:100-103): the loader hands the first file's centres to
+    rtb_set_ktable_centres and the run is the in-memory one."""
+    kt = synth.make_ktables(synth.ABSORBERS_C2, np_=20, nt=15, ng=20, nbin=14, seed=8, irregular=0.0)
+    cia = synth.make_cia(8)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=40, seed=9, nwave=8)
+    job.vwave = (600.0 + 0.4 * (np.arange(8) + 1) + 0.11).astype(np.float32)
+    paths = []
+    for i, gas in enumerate(kt.gases):
+        p = str(tmp_path / f"irr{i}.kta")
+        write_kta(p, kt, i, gas[0], gas[1])
+        paths.append(p)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c0, g0, _ = ctx.cirsrtfg_wave(job)
+    ctx.load_ktables(paths)
+    c, g, _ = ctx.cirsrtfg_wave(job)
+    assert rad_err(c, c0) <= RAD_TOL
+    assert jac_err(g, g0, job.nv) <= JAC_TOL
+

@@ -95,6 +95,17 @@ int rtb_set_ktables(rtb_context* ctx, int ntab, int np, int nt, int ng,
                     const float* vmin, const float* delv, const int* nbin,
                     const float* data);
 
+/* The gas and isotope ids of the loaded tables (the .kta header's IDGAS,
+ * ISOGAS; rtb_load_ktables sets them).  With them a gas's ktab may be
+ * RTB_KTAB_BY_ID: its tables are every table of its ids, in load order, and
+ * each calculation wavenumber takes the first regular table whose range
+ * covers it (FINDLOC, read_klist.f:247-265) -- or, on an irregular grid, the
+ * last of them (read_klist.f:266-310); a wavenumber no table covers gives
+ * the gas zero k (lun = -99, read_klist.f:341-351).  Cleared by
+ * rtb_set_ktables. */
+#define RTB_KTAB_BY_ID (-2)
+int rtb_set_ktable_ids(rtb_context* ctx, int ntab, const int* idgas, const int* isogas);
+
 /* The centres VCEN(npoint) of irregular k-tables (delv <= 0; read_khead.f:
  * 100-103), those of the first table as read_klist.f:141-145 keeps them
  * (npoint = its nbin).  A calculation wavenumber takes the centre nearest in
@@ -172,7 +183,9 @@ typedef struct rtb_atm {
     const float* cont;     /* (ld_con, nlayer) particles cm-2 (ncont > 0) */
     const int*   idgas;    /* (ngas) */
     const int*   isogas;   /* (ngas) */
-    /* gas -> k-table index loaded by rtb_set_ktables; -1 = no table (lun < 0) */
+    /* gas -> k-table index loaded by rtb_set_ktables; -1 = no table (lun < 0);
+     * RTB_KTAB_BY_ID = every loaded table of the gas's (idgas, isogas), in
+     * load order, as read_klist assigns them per wavenumber */
     const int*   ktab;     /* (ngas) */
     /* /PATHCOM/ */
     const int*   nlayin;   /* (npath) */

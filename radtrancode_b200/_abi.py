@@ -23,6 +23,8 @@ STATUS_NAMES = {
     8: "RTB_ERR_GORD", 9: "RTB_ERR_BUDGET",
 }
 
+KTAB_BY_ID = -2
+
 MAXLAY, MAXPAT, MAXGAS, MAXCON, MAXG, MAXK, MAXV, MAXPRO = 400, 200, 30, 10, 51, 30, 401, 200
 CIA_NUMPAIRS, CIA_NUMT, CIA_NUMWN = 9, 25, 1501
 

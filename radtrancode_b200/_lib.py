@@ -113,6 +113,8 @@ def lib() -> C.CDLL:
         L.rtb_read_fwh.restype = C.c_int
         L.rtb_read_fil.argtypes = [C.c_char_p, ip, ip, fp, ip, fp, fp, C.c_int, C.c_int]
         L.rtb_read_fil.restype = C.c_int
+        L.rtb_set_ktable_ids.argtypes = [vp, C.c_int, ip, ip]
+        L.rtb_set_ktable_ids.restype = C.c_int
         L.rtb_set_ktable_centres.argtypes = [vp, C.c_int, fp]
         L.rtb_set_ktable_centres.restype = C.c_int
         L.rtb_layerg.argtypes = [vp, C.POINTER(_abi.RtbProfile), C.POINTER(_abi.RtbLayerOpts),
@@ -142,5 +144,5 @@ EXPORTED = [
     "rtb_server_submit", "rtb_server_step", "rtb_server_poll", "rtb_calc_gain_matrix", "rtb_calcnextxn",
     "rtb_cirsradg_wave", "rtb_kta_header", "rtb_load_ktables", "rtb_load_cia",
     "rtb_calc_serr", "rtb_cirsconv", "rtb_cirsconv_ex", "rtb_read_fwh", "rtb_read_fil",
-    "rtb_layerg", "rtb_set_ktable_centres",
+    "rtb_layerg", "rtb_set_ktable_centres", "rtb_set_ktable_ids",
 ]

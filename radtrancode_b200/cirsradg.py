@@ -121,6 +121,9 @@ class Context:
         self._check(self._L.rtb_set_ktables(
             self._h, kt.ntab, kt.np_, kt.nt, kt.ng, _abi.fptr(kt.lnp), _abi.fptr(kt.tk), _abi.fptr(kt.delg),
             _abi.fptr(kt.vmin), _abi.fptr(kt.delv), _abi.iptr(kt.nbin), _abi.fptr(kt.data)))
+        ids = np.array([g[0] for g in kt.gases], np.int32)
+        isos = np.array([g[1] for g in kt.gases], np.int32)
+        self._check(self._L.rtb_set_ktable_ids(self._h, kt.ntab, _abi.iptr(ids), _abi.iptr(isos)))
         if kt.vcen is not None:     # irregular grid: the first table's centres
             self._check(self._L.rtb_set_ktable_centres(self._h, len(kt.vcen), _abi.fptr(kt.vcen)))
         self.tables = kt

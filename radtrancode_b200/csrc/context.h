@@ -135,6 +135,7 @@ struct rtb_context {
     std::vector<int> nbin;
     std::vector<int64_t> tab_off;            // element offset of each table
     std::vector<float> vcen;                 // irregular grids: the first table's centres VCEN(NPOINT)
+    std::vector<int> tab_id, tab_iso;        // the tables' gas and isotope ids (RTB_KTAB_BY_ID), empty: unknown
     std::vector<std::vector<uint8_t>> nonzero;  // [tab][bin]: any value > 0 (get_kg.f:228-250)
     rtb::DevBuf d_raw, d_log, d_delg, d_gord;
     // CIA

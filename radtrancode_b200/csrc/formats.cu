@@ -209,8 +209,15 @@ int rtb_load_ktables(rtb_context* c, int ntab, const char* const* paths, int* id
         }
     std::vector<float> lnp(k0.np);
     for (int i = 0; i < k0.np; ++i) lnp[i] = logf(k0.press[i]);   // PRESS(J) = LOG(PRESS(J)), read_khead.f:83
-    const int r = rtb_set_ktables(c, ntab, k0.np, k0.nt, k0.ng, lnp.data(), k0.temp.data(), k0.delg.data(),
-                                  vmin.data(), delv.data(), nbin.data(), data.data());
+    int r = rtb_set_ktables(c, ntab, k0.np, k0.nt, k0.ng, lnp.data(), k0.temp.data(), k0.delg.data(), vmin.data(),
+                            delv.data(), nbin.data(), data.data());
+    if (r) return r;
+    std::vector<int> ids(ntab), isos(ntab);
+    for (int t = 0; t < ntab; ++t) {
+        ids[t] = hd[t].idgas;
+        isos[t] = hd[t].isogas;
+    }
+    r = rtb_set_ktable_ids(c, ntab, ids.data(), isos.data());
     if (r || k0.vcen.empty()) return r;
     return rtb_set_ktable_centres(c, k0.npoint, k0.vcen.data());
 }

@@ -210,6 +210,8 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         if (id == 91 || id == 48 || id == 80)
             return fail(c, RTB_ERR_UNSUPPORTED, "gas id %d needs the H-/electron continuum", id);
         if (a.ktab[k] >= c->ntab) return fail(c, RTB_ERR_ARG, "ktab[%d]=%d >= ntab", k, a.ktab[k]);
+        if (a.ktab[k] == RTB_KTAB_BY_ID && c->tab_id.empty())
+            return fail(c, RTB_ERR_ARG, "ktab[%d] = RTB_KTAB_BY_ID but the tables' gas ids are unknown", k);
         if (id == 22 || id == 2) n2co2 = true;
     }
     int nlmax = 0;
@@ -396,23 +398,29 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         vvk1.resize(RTB_CIA_NUMWN);
         for (int i = 0; i < RTB_CIA_NUMWN; ++i) vvk1[i] = (float)i * c->dnu;
     }
-    // the calculation wavenumbers each gas's table covers (read_klist.f:250-265);
-    // outside them the gas has no table there (lun = -99, read_klist.f:341-351)
-    std::vector<int> cov_lo(a.ngas, 0), cov_hi(a.ngas, -1);
+    // the table of every (gas, calculation wavenumber), read_klist.f:247-351: the
+    // gas's tables in load order (its own ktab, or with RTB_KTAB_BY_ID every table
+    // of its gas and isotope ids); a regular table takes the wavenumbers FINDLOC
+    // places inside its range that no earlier table took, an irregular one every
+    // wavenumber; what no table takes has none (lun = -99, zero k)
+    std::vector<int> wtab((size_t)a.ngas * a.nwave, -1);
     for (int k = 0; k < a.ngas; ++k) {
-        const int itab = a.ktab[k];
-        if (itab < 0) continue;
-        if (!(c->delv[itab] > 0.0f)) {   // an irregular grid serves every wavenumber (read_klist.f:266-321)
-            cov_lo[k] = 1;
-            cov_hi[k] = a.nwave;
-            continue;
-        }
-        const float xmax = c->vmin[itab] + (float)(c->nbin[itab] - 1) * c->delv[itab];
-        int i1 = 0, i2 = 0;
-        findloc_f(a.vwave, a.nwave, c->vmin[itab], xmax, i1, i2);
-        if (i1 != 0 && i2 != 0) {
-            cov_lo[k] = i1;
-            cov_hi[k] = i2;
+        int* wt = wtab.data() + (size_t)k * a.nwave;
+        for (int t = 0; t < c->ntab; ++t) {
+            const bool serves = a.ktab[k] == RTB_KTAB_BY_ID
+                                    ? (c->tab_id[t] == a.idgas[k] && c->tab_iso[t] == a.isogas[k])
+                                    : t == a.ktab[k];
+            if (!serves) continue;
+            if (!(c->delv[t] > 0.0f)) {
+                for (int iw = 0; iw < a.nwave; ++iw) wt[iw] = t;
+                continue;
+            }
+            const float xmax = c->vmin[t] + (float)(c->nbin[t] - 1) * c->delv[t];
+            int i1 = 0, i2 = 0;
+            findloc_f(a.vwave, a.nwave, c->vmin[t], xmax, i1, i2);
+            if (i1 == 0 || i2 == 0) continue;
+            for (int iw = i1 - 1; iw <= i2 - 1 && iw < a.nwave; ++iw)
+                if (wt[iw] < 0) wt[iw] = t;
         }
     }
     for (int iw = 0; iw < a.nwave; ++iw) {
@@ -470,11 +478,11 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         }
         // table record choice (get_kg.f:189-275)
         for (int k = 0; k < a.ngas; ++k) {
-            const int itab = a.ktab[k];
+            const int itab = wtab[(size_t)k * a.nwave + iw];
             int64_t slice = -1;
             float w2 = -1.0f;                  // < 0: coincident wavenumber
             float w1 = -1.0f;                  // irregular grid: the lower record's weight FRACK
-            if (itab >= 0 && iw + 1 >= cov_lo[k] && iw + 1 <= cov_hi[k] && !(c->delv[itab] > 0.0f)) {
+            if (itab >= 0 && !(c->delv[itab] > 0.0f)) {
                 if (c->vcen.empty()) return fail(c, RTB_ERR_ARG, "irregular k-tables without centres (rtb_set_ktable_centres)");
                 const int n1 = irr_ipo - 1;
                 const bool coinc = c->delv[itab] < 0.0f;          // get_kg.f:266-279
@@ -489,7 +497,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
                 const int need = coinc ? n1 : n1 + 1;
                 if (need >= c->nbin[itab]) return fail(c, RTB_ERR_RANGE, "k-table %d has no record %d", itab, need);
                 if (c->nonzero[itab][n1]) slice = c->tab_off[itab] + (int64_t)n1 * np * std::abs(nt) * ng;
-            } else if (itab >= 0 && iw + 1 >= cov_lo[k] && iw + 1 <= cov_hi[k]) {
+            } else if (itab >= 0) {
                 const float vmin = c->vmin[itab], delv = c->delv[itab];
                 float eps;
                 if (delv >= 0.0001f) eps = 0.02f * delv; else eps = 0.25f * delv;
@@ -888,7 +896,8 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
         c->cells += (long long)atms[s].nlayer * atms[s].nwave;
         // cost model of one item (wavenumber): layers x (1 + sorting overlap passes) x gradient columns
         int nabs = 0;
-        for (int k = 0; k < atms[s].ngas; ++k) nabs += atms[s].ktab[k] >= 0 ? 1 : 0;
+        for (int k = 0; k < atms[s].ngas; ++k)
+            nabs += (atms[s].ktab[k] >= 0 || atms[s].ktab[k] == RTB_KTAB_BY_ID) ? 1 : 0;
         c->spec_cost.push_back((float)atms[s].nlayer * (1.0f + 4.0f * std::max(nabs - 1, 0)) *
                                (2.0f + st.spec[s].nsw));
     }
@@ -1164,6 +1173,15 @@ void rtb_destroy(rtb_context* c) {
 
 const char* rtb_last_error(const rtb_context* c) { return c ? c->err.c_str() : "no context"; }
 
+int rtb_set_ktable_ids(rtb_context* c, int ntab, const int* idgas, const int* isogas) {
+    if (!c) return RTB_ERR_ARG;
+    if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
+    if (ntab != c->ntab || !idgas || !isogas) return fail(c, RTB_ERR_ARG, "ids of %d tables, %d loaded", ntab, c->ntab);
+    c->tab_id.assign(idgas, idgas + ntab);
+    c->tab_iso.assign(isogas, isogas + ntab);
+    return RTB_OK;
+}
+
 int rtb_set_ktable_centres(rtb_context* c, int npoint, const float* vcen) {
     if (!c) return RTB_ERR_ARG;
     if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
@@ -1209,6 +1227,8 @@ int rtb_set_ktables(rtb_context* c, int ntab, int np, int nt, int ng, const floa
     c->lnp.assign(lnp, lnp + np);
     c->tk.assign(tk, tk + (nt > 0 ? (size_t)nt : (size_t)np * -nt));   // TEMP(NT) or TEMP2(NP, |NT|)
     c->vcen.clear();
+    c->tab_id.clear();
+    c->tab_iso.clear();
     c->delg.assign(delg, delg + ng);
     c->g_ord.assign(ng + 1, 0.0);
     for (int i = 0; i < ng; ++i) c->g_ord[i + 1] = c->g_ord[i] + (double)delg[i];

@@ -366,3 +366,50 @@ def test_irregular_wavenumber_grid(ctx, oracle, delv):
         with pytest.raises(cirsradg.RtbError, match="RANGE"):
             ctx.cirsrtfg_wave(j)
 
+
+
+def test_several_tables_per_gas(ctx):
+    """RTB_KTAB_BY_ID (read_klist.f:247-351): a gas served by several tables
+    takes, per wavenumber, the first listed table covering it.  Every table
+    split into two overlapping halves gives the run of the whole tables bit
+    for bit; of two tables covering the same wavenumbers the first listed
+    wins."""
+    import dataclasses
+    kt, cia, _ = synth.config2(nwave=40, nlayer=30, nbin=40)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=30, seed=51, nwave=40)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c0, g0, gt0 = ctx.cirsrtfg_wave(job)
+    n = kt.ntab
+    lo = [kt.table(i)[:22] for i in range(n)]
+    hi = [kt.table(i)[18:] for i in range(n)]
+    split = dataclasses.replace(
+        kt, vmin=np.concatenate([kt.vmin, kt.vmin + np.float32(18) * kt.delv]).astype(np.float32),
+        delv=np.concatenate([kt.delv, kt.delv]), nbin=np.full(2 * n, 22, np.int32),
+        data=np.concatenate([a.ravel() for a in lo + hi]), gases=list(kt.gases) * 2)
+    jb = copy.deepcopy(job)
+    jb.ktab = np.full(job.ngas, -1, np.int32)
+    jb.ktab[2:] = -2                                   # RTB_KTAB_BY_ID
+    ctx.set_ktables(split)
+    c, g, gt = ctx.cirsrtfg_wave(jb)
+    assert np.array_equal(c, c0) and np.array_equal(g, g0) and np.array_equal(gt, gt0)
+    # two whole tables for CH4: the first listed serves it
+    twice = dataclasses.replace(
+        kt, vmin=np.concatenate([kt.vmin, kt.vmin[:1]]), delv=np.concatenate([kt.delv, kt.delv[:1]]),
+        nbin=np.concatenate([kt.nbin, kt.nbin[:1]]),
+        data=np.concatenate([kt.data, (kt.table(0) * np.float32(3.0)).ravel()]), gases=list(kt.gases) + [kt.gases[0]])
+    ctx.set_ktables(twice)
+    c1, _, _ = ctx.cirsrtfg_wave(jb)
+    assert np.array_equal(c1, c0)
+    j3 = copy.deepcopy(job)
+    j3.ktab = job.ktab.copy()
+    j3.ktab[2] = n                                     # the tripled CH4 table
+    c3, _, _ = ctx.cirsrtfg_wave(j3)
+    assert not np.array_equal(c3, c0)
+    flipped = dataclasses.replace(
+        twice, vmin=twice.vmin[::-1].copy(), delv=twice.delv[::-1].copy(), nbin=twice.nbin[::-1].copy(),
+        data=np.concatenate([twice.table(i).ravel() for i in range(n, -1, -1)]), gases=twice.gases[::-1])
+    ctx.set_ktables(flipped)
+    c4, _, _ = ctx.cirsrtfg_wave(jb)
+    assert np.array_equal(c4, c3)
+    ctx.set_ktables(kt)

@@ -540,6 +540,21 @@ typedef struct rtb_retrieval_spec {
     const int* scale_model;   /* [nscale] 3 or 2; NULL = all 3 */
     int nprof;                /* gases retrieved as layer profiles */
     const int* prof_gas;      /* [nprof] 0-based gas index (not also in scale_gas) */
+    /* The level-state model (NULL: the layer-state model above).  The state
+     * is that of the profile's npro levels: x[lev] the temperature of level
+     * lev, x[npro + a] the scale factor of gas scale_gas[a] (models 3 / 2 on
+     * every level's vmr, subprofretg.f:725-750), x[npro + nscale + p*npro +
+     * lev] the log vmr of gas prof_gas[p] at level lev (model 0); nx = npro +
+     * nscale + nprof*npro.  Every state the loop evaluates rewrites the
+     * profile and re-layers it on the device (rtb_layerg with lopts: layers,
+     * DTE/DAM and the nadir path), the step gsetrad + subpathg take through
+     * the .prf file each iteration; the Jacobian reaches the levels through
+     * DTE/DAM and xmap (map2pro, map2xvec).  `atm` then supplies the gases
+     * (ngas = prof->nvmr, idgas, isogas, ktab), the spectral grid and the
+     * flags; its layer, path and gradient arrays and xmap are not read (may
+     * be NULL); prof->ndust must be 0. */
+    const rtb_profile* prof;
+    const rtb_layer_opts* lopts;
 } rtb_retrieval_spec;
 
 typedef struct rtb_retrieval_opts {

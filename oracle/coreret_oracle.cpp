@@ -25,9 +25,142 @@ struct Work {
     std::vector<float> press, delh, scale, dte, dam, vwave;
     std::vector<int> layinc, idgas, isogas, ktab, nlayin, imod, sg, sm, pg;
     std::vector<float> vmr0;   /* [nprof][L] pp / press of the profiled gases */
+    /* level-state model: L counts the profile's levels (the state's temperatures) */
+    bool level = false;
+    rtb_profile pr{};
+    rtb_layer_opts lo{};
+    std::vector<float> ph, pp_atm, pt, pvmr0, pvmr, lbase;
 };
 
+int setup_level(const rtb_retrieval_spec& s, Work& w) {
+    const rtb_atm& t = *s.atm;
+    const rtb_profile& P = *s.prof;
+    const int G = t.ngas, NPRO = P.npro, NV = t.nv, NW = t.nwave, NL = s.lopts->nlay;
+    if (P.nvmr != G || P.ndust != 0 || NV != NPRO + s.nscale + s.nprof * NPRO) return RTB_ERR_UNSUPPORTED;
+    w.level = true;
+    w.L = NPRO;
+    w.NV = NV;
+    w.NW = NW;
+    w.nparam = G + 1;
+    w.sg.assign(s.scale_gas, s.scale_gas + s.nscale);
+    w.sm.assign(s.nscale, 3);
+    if (s.scale_model) w.sm.assign(s.scale_model, s.scale_model + s.nscale);
+    w.pg.assign(s.prof_gas, s.prof_gas + s.nprof);
+    const int ldp = P.ld_pro > 0 ? P.ld_pro : NPRO;
+    w.ph.assign(P.h, P.h + NPRO);
+    w.pp_atm.assign(P.p, P.p + NPRO);
+    w.pt.assign(P.t, P.t + NPRO);
+    w.pvmr0.resize((size_t)G * NPRO);
+    for (int g = 0; g < G; ++g)
+        for (int l = 0; l < NPRO; ++l) w.pvmr0[l + (size_t)NPRO * g] = P.vmr[l + (size_t)ldp * g];
+    w.pvmr = w.pvmr0;
+    w.pr = P;
+    w.pr.ld_pro = NPRO;
+    w.pr.h = w.ph.data();
+    w.pr.p = w.pp_atm.data();
+    w.pr.t = w.pt.data();
+    w.pr.vmr = w.pvmr.data();
+    w.lo = *s.lopts;
+    if (w.lo.laytyp >= 4 && w.lo.base) w.lbase.assign(w.lo.base, w.lo.base + NL);
+    w.lo.base = w.lbase.empty() ? nullptr : w.lbase.data();
+    w.press.assign(NL, 0.0f);
+    w.temp.assign(NL, 0.0f);
+    w.delh.assign(NL, 0.0f);
+    w.pp.assign((size_t)NL * G, 0.0f);
+    w.amount.assign((size_t)NL * G, 0.0f);
+    w.dte.assign((size_t)NL * NPRO, 0.0f);
+    w.dam.assign((size_t)NL * NPRO, 0.0f);
+    w.scale.assign(NL, 0.0f);
+    w.emtemp.assign(NL, 0.0f);
+    w.layinc.assign(NL, 0);
+    w.nlayin.assign(1, 0);
+    w.imod.assign(1, 3);
+    w.xmap.assign((size_t)NV * w.nparam * NPRO, 0.0f);
+    w.vwave.assign(t.vwave, t.vwave + NW);
+    w.idgas.assign(t.idgas, t.idgas + G);
+    w.isogas.assign(t.isogas, t.isogas + G);
+    w.ktab.assign(t.ktab, t.ktab + G);
+    w.a = t;
+    w.a.nlayer = NL;
+    w.a.npath = 1;
+    w.a.npro = NPRO;
+    w.a.ld_lay = NL;
+    w.a.ld_v = NV;
+    w.a.ld_param = w.nparam;
+    w.a.press = w.press.data();
+    w.a.temp = w.temp.data();
+    w.a.delh = w.delh.data();
+    w.a.pp = w.pp.data();
+    w.a.amount = w.amount.data();
+    w.a.idgas = w.idgas.data();
+    w.a.isogas = w.isogas.data();
+    w.a.ktab = w.ktab.data();
+    w.a.nlayin = w.nlayin.data();
+    w.a.imod = w.imod.data();
+    w.a.layinc = w.layinc.data();
+    w.a.scale = w.scale.data();
+    w.a.emtemp = w.emtemp.data();
+    w.a.dte = w.dte.data();
+    w.a.dam = w.dam.data();
+    w.a.dco = nullptr;
+    w.a.dfp = nullptr;
+    w.a.xmap = w.xmap.data();
+    w.a.vwave = w.vwave.data();
+    w.a.conv = nullptr;
+    return RTB_OK;
+}
+
+/* subprofretg.f models 0 / 2 / 3 on every level of the profile, then
+ * LAYERG + ATMG (the oracle's own, orc_layerg) */
+int at_level_state(Work& w, const float* x) {
+    const int NPRO = w.L, NV = w.NV, np_ = w.nparam, G = w.a.ngas;
+    for (int l = 0; l < NPRO; ++l) w.pt[l] = x[l];
+    w.pvmr = w.pvmr0;
+    std::fill(w.xmap.begin(), w.xmap.end(), 0.0f);
+    for (int l = 0; l < NPRO; ++l) w.xmap[l + (size_t)NV * (G + (size_t)np_ * l)] = 1.0f;     /* XMAP = 1.0 */
+    const int ns = (int)w.sg.size();
+    for (int a = 0; a < ns; ++a) {
+        const int g = w.sg[a];
+        const bool lin = w.sm[a] == 2;
+        const float f = lin ? x[NPRO + a] : expf(x[NPRO + a]);
+        for (int l = 0; l < NPRO; ++l) {
+            const float xref = w.pvmr0[l + (size_t)NPRO * g];
+            const float x1 = xref * f;                     /* X1(J) = XREF(J)*EXP(XN) or XREF(J)*XN */
+            w.pvmr[l + (size_t)NPRO * g] = x1;
+            w.xmap[(NPRO + a) + (size_t)NV * (g + (size_t)np_ * l)] = lin ? xref : x1;
+        }
+    }
+    for (size_t p = 0; p < w.pg.size(); ++p) {
+        const int g = w.pg[p];
+        const int base = NPRO + ns + (int)p * NPRO;
+        for (int l = 0; l < NPRO; ++l) {
+            const float v = expf(x[base + l]);
+            w.pvmr[l + (size_t)NPRO * g] = v;
+            w.xmap[(base + l) + (size_t)NV * (g + (size_t)np_ * l)] = v;
+        }
+    }
+    rtb_layers out;
+    std::memset(&out, 0, sizeof out);
+    int npath = 0;
+    out.ld_lay = w.a.nlayer;
+    out.delh = w.delh.data();
+    out.press = w.press.data();
+    out.temp = w.temp.data();
+    out.amount = w.amount.data();
+    out.pp = w.pp.data();
+    out.dte = w.dte.data();
+    out.dam = w.dam.data();
+    out.npath = &npath;
+    out.nlayin = w.nlayin.data();
+    out.imod = w.imod.data();
+    out.layinc = w.layinc.data();
+    out.scale = w.scale.data();
+    out.emtemp = w.emtemp.data();
+    return orc_layerg(&w.pr, &w.lo, &out);
+}
+
 int setup(const rtb_retrieval_spec& s, Work& w) {
+    if (s.prof) return setup_level(s, w);
     const rtb_atm& t = *s.atm;
     if (t.npath != 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont != 0)
         return RTB_ERR_UNSUPPORTED;
@@ -103,6 +236,7 @@ int setup(const rtb_retrieval_spec& s, Work& w) {
 }
 
 void at_state(Work& w, const float* x) {
+    if (w.level) return;   /* forward() re-layers through at_level_state */
     const int L = w.L;
     for (int l = 0; l < L; ++l) w.temp[l] = x[l];
     for (int j = 0; j < w.nlayin[0]; ++j) w.emtemp[j] = w.temp[w.layinc[j] - 1];
@@ -139,7 +273,12 @@ void at_state(Work& w, const float* x) {
 /* forwardavfovX stand-in: spectrum and kk (ny, nx) REAL at state x */
 int forward(const orc_tables* tab, Work& w, const float* x, int precision, int nthreads, std::vector<float>& yn,
             std::vector<float>& kk) {
-    at_state(w, x);
+    if (w.level) {
+        const int r = at_level_state(w, x);
+        if (r) return r;
+    } else {
+        at_state(w, x);
+    }
     std::vector<double> c(w.NW), g((size_t)w.NV * w.NW);
     const int r = orc_cirsrtfg_wave_mt(tab, &w.a, precision, c.data(), g.data(), nullptr, nthreads);
     if (r) return r;

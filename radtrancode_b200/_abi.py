@@ -99,6 +99,7 @@ class RtbRetrievalSpec(C.Structure):
         ("y", _fp), ("sei", C.POINTER(C.c_double)), ("sa", C.POINTER(C.c_double)),
         ("xa", _fp), ("x0", _fp),
         ("scale_model", _ip), ("nprof", C.c_int), ("prof_gas", _ip),
+        ("prof", C.POINTER(RtbProfile)), ("lopts", C.POINTER(RtbLayerOpts)),
     ]
 
 

@@ -51,9 +51,18 @@ struct AtmWork {
     std::vector<float> pp0, amount0, xmap0;   // at scale factor 1
     std::vector<int> scale_gas, scale_model, prof_gas;
     std::vector<float> vmr0;                  // [nprof][L] pp0 / press of the profiled gases
+    // the level-state model: the profile (levels) and its layering
+    bool level = false;
+    int npro = 0;
+    rtb_profile pr{};
+    rtb_layer_opts lo{};
+    std::vector<float> ph, pp_atm, pt, pvmr0, pvmr, lbase;   // h, p, t [npro]; vmr [ngas][npro]
 };
 
+int build_level_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w);
+
 int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
+    if (s.prof) return build_level_work(c, s, w);
     const rtb_atm& t = *s.atm;
     const int L = t.nlayer, G = t.ngas, NC = t.ncont, NP = t.npath, NPRO = t.npro, NV = t.nv, NW = t.nwave;
     const int ldl = t.ld_lay > 0 ? t.ld_lay : RTB_MAXLAY;
@@ -166,7 +175,10 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
 // lay the atmosphere out at state x: temp = x[l]; amount, pp and the gas's
 // xmap entries scaled by exp(x[L + a]) in REAL arithmetic (subprofretg.f:
 // 746-750 computes X1 = XREF*EXP(XN)); emtemp follows temp along the path
-void set_state(AtmWork& w, const float* x) {
+int set_level_state(rtb_context* c, AtmWork& w, const float* x);
+
+int set_state(rtb_context* c, AtmWork& w, const float* x) {
+    if (w.level) return set_level_state(c, w, x);
     const int L = w.a.nlayer, NV = w.a.nv, NPRO = w.a.npro, nparam = w.nparam;
     for (int l = 0; l < L; ++l) w.temp[l] = x[l];
     const int nl = w.nlayin[0];
@@ -198,6 +210,165 @@ void set_state(AtmWork& w, const float* x) {
             for (int k = 0; k < NPRO; ++k) w.xmap[(base + l) + (size_t)NV * (g + (size_t)nparam * k)] = k == l ? v : 0.0f;
         }
     }
+    return RTB_OK;
+}
+
+// ---------------------------------------------------------------- the level-state model
+int build_level_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
+    const rtb_atm& t = *s.atm;
+    const rtb_profile& P = *s.prof;
+    const int G = t.ngas, NPRO = P.npro, NV = t.nv, NW = t.nwave;
+    if (!s.lopts) return fail(c, RTB_ERR_ARG, "level-state retrieval without layering options");
+    const rtb_layer_opts& o = *s.lopts;
+    if (P.nvmr != G) return fail(c, RTB_ERR_ARG, "profile has %d gases, the atmosphere %d", P.nvmr, G);
+    if (P.ndust != 0 || t.ncont != 0) return fail(c, RTB_ERR_UNSUPPORTED, "level-state retrieval with dust");
+    if (NPRO < 2 || NPRO > RTB_MAXPRO || !P.h || !P.p || !P.t || (G > 0 && !P.vmr))
+        return fail(c, RTB_ERR_ARG, "level profile arrays");
+    if (s.nprof < 0 || (s.nprof > 0 && !s.prof_gas)) return fail(c, RTB_ERR_ARG, "nprof/prof_gas");
+    if (NV != NPRO + s.nscale + s.nprof * NPRO)
+        return fail(c, RTB_ERR_ARG, "nv=%d but npro + nscale + nprof*npro = %d", NV, NPRO + s.nscale + s.nprof * NPRO);
+    if (NV > kNewtonMaxNx) return fail(c, RTB_ERR_UNSUPPORTED, "state size %d > %d", NV, kNewtonMaxNx);
+    if (NV >= NW) return fail(c, RTB_ERR_UNSUPPORTED, "nx=%d >= ny=%d (calc_gain_matrix nx<ny branch only)", NV, NW);
+    if (o.nlay < 1 || o.nlay > RTB_MAXLAY) return fail(c, RTB_ERR_LIMIT, "layering: nlay %d", o.nlay);
+    if (!t.idgas || !t.isogas || !t.ktab || !t.vwave) return fail(c, RTB_ERR_ARG, "NULL input array in retrieval atmosphere");
+    for (int a = 0; a < s.nscale; ++a) {
+        if (!s.scale_gas || s.scale_gas[a] < 0 || s.scale_gas[a] >= G)
+            return fail(c, RTB_ERR_ARG, "scale_gas[%d] outside 0..ngas-1", a);
+        if (s.scale_model && !(s.scale_model[a] == 2 || s.scale_model[a] == 3))
+            return fail(c, RTB_ERR_UNSUPPORTED, "scale_model[%d]=%d (models 2 and 3 only)", a, s.scale_model[a]);
+    }
+    for (int p = 0; p < s.nprof; ++p) {
+        if (s.prof_gas[p] < 0 || s.prof_gas[p] >= G) return fail(c, RTB_ERR_ARG, "prof_gas[%d] outside gases", p);
+        for (int a = 0; a < s.nscale; ++a)
+            if (s.scale_gas[a] == s.prof_gas[p]) return fail(c, RTB_ERR_ARG, "gas %d both scaled and profiled", s.prof_gas[p]);
+    }
+    const int L = o.nlay, nparam = G + 1;
+    w.level = true;
+    w.npro = NPRO;
+    w.nparam = nparam;
+    w.scale_gas.assign(s.scale_gas, s.scale_gas + s.nscale);
+    w.scale_model.assign(s.nscale, 3);
+    if (s.scale_model) w.scale_model.assign(s.scale_model, s.scale_model + s.nscale);
+    w.prof_gas.assign(s.prof_gas, s.prof_gas + s.nprof);
+    const int ldp = P.ld_pro > 0 ? P.ld_pro : NPRO;
+    w.ph.assign(P.h, P.h + NPRO);
+    w.pp_atm.assign(P.p, P.p + NPRO);
+    w.pt.assign(P.t, P.t + NPRO);
+    w.pvmr0.resize((size_t)G * NPRO);
+    for (int g = 0; g < G; ++g)
+        for (int l = 0; l < NPRO; ++l) w.pvmr0[l + (size_t)NPRO * g] = P.vmr[l + (size_t)ldp * g];
+    w.pvmr = w.pvmr0;
+    w.pr = P;
+    w.pr.ld_pro = NPRO;
+    w.pr.ld_con = 0;
+    w.pr.h = w.ph.data();
+    w.pr.p = w.pp_atm.data();
+    w.pr.t = w.pt.data();
+    w.pr.vmr = w.pvmr.data();
+    w.pr.dust = nullptr;
+    w.lo = o;
+    if (o.laytyp >= 4 && o.base) w.lbase.assign(o.base, o.base + L);
+    w.lo.base = w.lbase.empty() ? nullptr : w.lbase.data();
+    // layer, path and gradient arrays, written by every re-layering
+    w.press.assign(L, 0.0f);
+    w.temp.assign(L, 0.0f);
+    w.delh.assign(L, 0.0f);
+    w.pp.assign((size_t)L * G, 0.0f);
+    w.amount.assign((size_t)L * G, 0.0f);
+    w.dte.assign((size_t)L * NPRO, 0.0f);
+    w.dam.assign((size_t)L * NPRO, 0.0f);
+    w.scale.assign(L, 0.0f);
+    w.emtemp.assign(L, 0.0f);
+    w.layinc.assign(L, 0);
+    w.nlayin.assign(1, 0);
+    w.imod.assign(1, 3);
+    w.xmap.assign((size_t)NV * nparam * NPRO, 0.0f);
+    w.vwave.assign(t.vwave, t.vwave + NW);
+    w.idgas.assign(t.idgas, t.idgas + G);
+    w.isogas.assign(t.isogas, t.isogas + G);
+    w.ktab.assign(t.ktab, t.ktab + G);
+    rtb_atm& a = w.a;
+    a = t;
+    a.nlayer = L;
+    a.ncont = 0;
+    a.npath = 1;
+    a.npro = NPRO;
+    a.ld_lay = L;
+    a.ld_con = 1;
+    a.ld_v = NV;
+    a.ld_param = nparam;
+    a.press = w.press.data();
+    a.temp = w.temp.data();
+    a.delh = w.delh.data();
+    a.pp = w.pp.data();
+    a.amount = w.amount.data();
+    a.cont = nullptr;
+    a.idgas = w.idgas.data();
+    a.isogas = w.isogas.data();
+    a.ktab = w.ktab.data();
+    a.nlayin = w.nlayin.data();
+    a.imod = w.imod.data();
+    a.layinc = w.layinc.data();
+    a.scale = w.scale.data();
+    a.emtemp = w.emtemp.data();
+    a.dte = w.dte.data();
+    a.dam = w.dam.data();
+    a.dco = nullptr;
+    a.dfp = nullptr;
+    a.xmap = w.xmap.data();
+    a.vwave = w.vwave.data();
+    a.xsec_ext = nullptr;
+    a.conv = nullptr;
+    return RTB_OK;
+}
+
+// the profile at state x (subprofretg.f:638-651, 725-750 on every level), then
+// its layers, gradient matrices and path (layerg + atmg on the device)
+int set_level_state(rtb_context* c, AtmWork& w, const float* x) {
+    const int NPRO = w.npro, NV = w.a.nv, nparam = w.nparam, G = w.a.ngas;
+    for (int l = 0; l < NPRO; ++l) w.pt[l] = x[l];
+    w.pvmr = w.pvmr0;
+    std::fill(w.xmap.begin(), w.xmap.end(), 0.0f);
+    for (int l = 0; l < NPRO; ++l) w.xmap[l + (size_t)NV * (G + (size_t)nparam * l)] = 1.0f;
+    const int ns = (int)w.scale_gas.size();
+    for (int a = 0; a < ns; ++a) {
+        const int g = w.scale_gas[a];
+        const bool lin = w.scale_model[a] == 2;
+        const float f = lin ? x[NPRO + a] : expf(x[NPRO + a]);
+        for (int l = 0; l < NPRO; ++l) {
+            const float ref = w.pvmr0[l + (size_t)NPRO * g];
+            const float v = ref * f;
+            w.pvmr[l + (size_t)NPRO * g] = v;
+            w.xmap[(NPRO + a) + (size_t)NV * (g + (size_t)nparam * l)] = lin ? ref : v;
+        }
+    }
+    for (size_t p = 0; p < w.prof_gas.size(); ++p) {
+        const int g = w.prof_gas[p];
+        const int base = NPRO + ns + (int)p * NPRO;
+        for (int l = 0; l < NPRO; ++l) {
+            const float v = expf(x[base + l]);
+            w.pvmr[l + (size_t)NPRO * g] = v;
+            w.xmap[(base + l) + (size_t)NV * (g + (size_t)nparam * l)] = v;
+        }
+    }
+    rtb_layers out;
+    std::memset(&out, 0, sizeof out);
+    int npath = 0;
+    out.ld_lay = w.a.nlayer;
+    out.delh = w.delh.data();
+    out.press = w.press.data();
+    out.temp = w.temp.data();
+    out.amount = w.amount.data();
+    out.pp = w.pp.data();
+    out.dte = w.dte.data();
+    out.dam = w.dam.data();
+    out.npath = &npath;
+    out.nlayin = w.nlayin.data();
+    out.imod = w.imod.data();
+    out.layinc = w.layinc.data();
+    out.scale = w.scale.data();
+    out.emtemp = w.emtemp.data();
+    return rtb_layerg(c, &w.pr, &w.lo, &out);
 }
 
 // ---------------------------------------------------------------- the retrieval engine
@@ -387,7 +558,7 @@ struct Engine {
             delete s;
             return e;
         }
-        s->nlayer = sp.atm->nlayer;
+        s->nlayer = sp.prof ? sp.prof->npro : sp.atm->nlayer;   // the temperature elements of x
         s->nx = sp.atm->nv;
         s->kind.assign(s->nx, 1);
         for (int l = 0; l < s->nlayer; ++l) s->kind[l] = 0;
@@ -501,7 +672,8 @@ struct Engine {
         std::vector<int64_t> oo, jo;
         for (Slot* s : v) {
             const bool first = s->phase == 0;
-            set_state(s->w, first ? s->xn.data() : s->xn1.data());
+            const int rs = set_state(c, s->w, first ? s->xn.data() : s->xn1.data());
+            if (rs) return rs;
             atms.push_back(s->w.a);
             const int b = first ? s->cur : 1 - s->cur;
             oo.push_back(Yn(*s, b) - F());

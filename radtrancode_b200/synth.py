@@ -463,6 +463,8 @@ class RetrievalCase:
     x0: np.ndarray | None = None
     scale_model: np.ndarray | None = None   # int32 [nscale], 3 (log) or 2 (linear); None = all 3
     prof_gas: np.ndarray | None = None      # int32 [nprof] gases retrieved as log-vmr layer profiles
+    prof: "Profile | None" = None           # level-state model: the profile re-layered every state
+    lopts: dict | None = None               # its layering (rtb_layer_opts fields)
 
     @property
     def nx(self):
@@ -487,7 +489,21 @@ class RetrievalCase:
         pg = self.prof_gas if self.prof_gas is not None else np.zeros(0, np.int32)
         s.nprof = len(pg)
         s.prof_gas = _abi.iptr(pg) if len(pg) else None
-        s._keep = (self, atm, pg)
+        keep = [self, atm, pg]
+        if self.prof is not None:
+            ps = self.prof.as_struct()
+            o = _abi.RtbLayerOpts()
+            lo = dict(laytyp=1, layint=1, layht=float(self.prof.h[0]), layang=0.0, angle=0.0, botlay=1, ipzen=0)
+            lo.update(self.lopts or {})
+            base = lo.pop("base", None)
+            for k, v in lo.items():
+                setattr(o, k, v)
+            if base is not None:
+                base = np.ascontiguousarray(base, np.float32)
+                o.base = _abi.fptr(base)
+            s.prof, s.lopts = C.pointer(ps), C.pointer(o)
+            keep += [ps, o, base]
+        s._keep = keep
         return s
 
 
@@ -547,6 +563,37 @@ def make_retrieval(tables: KTables, absorbers, *, nlayer, seed, iw0=0, nwave=Non
     return RetrievalCase(job=job, scale_gas=np.array([2 + a for a in scaled], np.int32), xa=xa, sa=sa, sei=sei,
                          x_true=x_true, scale_model=sm if scale_model is not None else None,
                          prof_gas=np.array([2 + a for a in prof], np.int32) if npf else None)
+
+
+def make_level_retrieval(tables: KTables, absorbers, *, npro, nlay, seed, iw0=0, nwave=None, angle=0.0,
+                         noise=1e-9, scale_model=None) -> RetrievalCase:
+    """Retrieval case of the level-state model: the state is the temperature
+    of each of the npro profile levels plus one scale factor per absorber
+    (model 3, or 2 where scale_model says so); every state is re-layered
+    into nlay equal-log-pressure Curtis-Godson layers viewed at `angle`.  A
+    priori: the smooth T(p) and unit scales; the true state a seeded draw
+    from Sa.  The profile's heights stay those of the a priori (the
+    reference re-integrates them only when hydrostatic adjustment is on)."""
+    rng = np.random.default_rng(seed)
+    prof = make_profile(absorbers, npro=npro, seed=seed + 1)
+    p_pa = prof.p.astype(np.float64) / BAR_TO_ATM * 1e5
+    t_prior = temperature_profile(p_pa, rng, noise=0.0)
+    prior = dataclasses.replace(prof, t=t_prior.astype(np.float32))
+    ns = len(absorbers)
+    sm = np.array(scale_model if scale_model is not None else [3] * ns, np.int32)
+    nv = npro + ns
+    job = make_job(tables, absorbers, nlayer=nlay, seed=seed + 2, iw0=iw0, nwave=nwave)
+    job = dataclasses.replace(job, nv=nv, ld_v=nv, npro=1, xmap=np.zeros((nv, job.nparam, 1), np.float32, order="F"))
+    xa = np.concatenate([t_prior, np.where(sm == 2, 1.0, 0.0)]).astype(np.float32)
+    sa = prior_covariance(p_pa, ns)
+    x_true = (xa + np.linalg.cholesky(sa) @ rng.standard_normal(nv)).astype(np.float32)
+    for k in range(ns):
+        if sm[k] == 2:
+            x_true[npro + k] = max(x_true[npro + k], np.float32(0.05))
+    sei = np.full(job.nwave, 1.0 / (noise * noise))
+    return RetrievalCase(job=job, scale_gas=np.arange(2, 2 + ns, dtype=np.int32), xa=xa, sa=sa, sei=sei,
+                         x_true=x_true, scale_model=sm if scale_model is not None else None, prof=prior,
+                         lopts=dict(nlay=nlay, laytyp=1, layint=1, angle=float(angle)))
 
 
 def observe(case: RetrievalCase, spectrum, seed, noise=1e-9):

@@ -197,6 +197,36 @@ def test_retrieve_scale_model_2_and_gas_profile_match_oracle(ctx, oracle):
         assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
 
 
+def test_level_state_retrieval_relayers_every_state(ctx, oracle):
+    """The level-state model: the temperatures of 41 profile levels and two
+    log gas scales, every evaluated state re-layered into 40 Curtis-Godson
+    layers on a 20-degree path (rtb_layerg inside the loop, as gsetrad +
+    subpathg re-layer the .prf each iteration).  Same iterations, forward
+    evaluations and stop rule as the oracle's coreret loop over its own
+    layering, states within 1e-3 prior sigma, cost within 1e-3; the same
+    result alone and beside a second retrieval."""
+    kt, cia, _ = synth.config2()
+    cases = []
+    for seed in (61, 71):
+        case = synth.make_level_retrieval(kt, [synth.CH4, synth.NH3], npro=41, nlay=40, seed=seed, nwave=120,
+                                          angle=20.0)
+        y_true, _ = oracle.forward_state(kt, cia, case, case.x_true, nthreads=8)
+        synth.observe(case, y_true, seed=seed + 1)
+        cases.append(case)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    both = ctx.retrieve_batch(cases, kiter=10, phlimit=0.1)
+    alone = ctx.retrieve_batch(cases[:1], kiter=10, phlimit=0.1)[0]
+    for case, g in zip(cases, both):
+        ref, _ = oracle.retrieve(kt, cia, case, kiter=10, phlimit=0.1, nthreads=8)
+        assert (g["converged"], g["iterations"], g["forwards"]) == (ref["converged"], ref["iterations"],
+                                                                   ref["forwards"])
+        sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
+        assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
+        assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
+    assert np.array_equal(alone["x"], both[0]["x"]) and alone["phi"] == both[0]["phi"]
+
+
 def test_retrieve_batch_result_independent_of_batch(ctx, c1):
     kt, cia, cases = c1
     ctx.set_ktables(kt)

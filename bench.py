@@ -488,6 +488,47 @@ def profile_aux(args):
             print(json.dumps({"profile_aux": n, "phi0": float(phi[0]), "x0": float(x[0])}))
 
 
+def profile_layers(args):
+    """Reduced case for ncu captures of the layering kernel: `--profile-layers`
+    calls of rtb_layerg on a 121-level, 6-gas profile into 120 Curtis-Godson
+    layers on a 30-degree path (the full-size atmosphere), after warm-up."""
+    from radtrancode_b200 import cirsradg, synth
+    prof = synth.make_profile(synth.ABSORBERS_C2, npro=121, seed=1005)
+    with cirsradg.Context(0) as ctx:
+        for i in range(args.warmup + args.profile_layers):
+            t0 = time.perf_counter()
+            lay = ctx.layerg(prof, nlay=120, laytyp=1, layint=1, angle=30.0)
+            print(json.dumps({"profile_layers": i, "call_ms": 1e3 * (time.perf_counter() - t0),
+                              "totam0": float(lay["totam"][0])}))
+
+
+def profile_conv(args):
+    """Reduced case for ncu captures of the convolution kernels: the
+    full-size spectrum's radiance, d/dtsurf and 124 Jacobian rows (126 series
+    of 2000 points) convolved `--profile-conv` times onto 600 square-bin
+    channels (FWHM 1.2 cm-1) and onto 200 filter channels (FWHM < 0)."""
+    from radtrancode_b200 import cirsradg, synth
+    kt, cia, _ = synth.config2()
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, nwave=2000, vmr_perturb=0.3)
+    vw = job.vwave
+    vc = (vw[0] + 5.0 + np.arange(600) * 1.3).astype(np.float32)
+    vf = (vw[0] + 10.0 + np.arange(200) * 3.9).astype(np.float32)
+    tri = np.array([-1.5, -0.5, 0.0, 0.5, 1.5], np.float32)
+    fil = synth.Channels(vconv=vf, vcen=vf, nsub=np.full(200, 5, np.int32), vfil=(vf[:, None] + tri).ravel(),
+                         fil=np.tile(np.array([0.0, 0.6, 1.0, 0.6, 0.0], np.float32), 200))
+    with cirsradg.Context(0) as ctx:
+        ctx.set_ktables(kt)
+        ctx.set_cia(cia)
+        c, g, gt = ctx.cirsrtfg_wave(job)
+        series = np.vstack([c[None], gt[None], g.reshape(job.nv, job.nwave)])
+        for i in range(args.warmup + args.profile_conv):
+            t0 = time.perf_counter()
+            a = ctx.cirsconv_ex(vw, series, 1.2, synth.Channels(vconv=vc))
+            b = ctx.cirsconv_ex(vw, series, -1.0, fil)
+            print(json.dumps({"profile_conv": i, "call_ms": 1e3 * (time.perf_counter() - t0),
+                              "a0": float(a[0, 0]), "b0": float(b[0, 0])}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -506,7 +547,17 @@ def main():
                     help="profiling case: only the Newton-step kernel on N full-size retrievals")
     ap.add_argument("--profile-aux", type=int, default=0,
                     help="profiling case: the small kernels of the Newton-step interface on N retrievals")
+    ap.add_argument("--profile-layers", type=int, default=0,
+                    help="profiling case: N calls of the layering kernel on the full-size profile")
+    ap.add_argument("--profile-conv", type=int, default=0,
+                    help="profiling case: N convolutions of a full-size spectrum's outputs")
     args = ap.parse_args()
+    if args.profile_layers:
+        profile_layers(args)
+        return
+    if args.profile_conv:
+        profile_conv(args)
+        return
     if args.profile_aux:
         profile_aux(args)
         return

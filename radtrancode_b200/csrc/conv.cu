@@ -12,9 +12,11 @@
 //   * FWHM < 0 (:171-239): each channel's filter function from the .fil file,
 //     linearly interpolated (INTERP rtm_util/interp.f) onto the calculated
 //     points, and the filter-weighted mean of the series.
-// One block per series.  For FWHM > 0 thread 0 builds the extrapolated,
-// NaN-free knot list and solves the spline's tridiagonal system (a
-// sequential recurrence), then the block's threads fill the channels.  REAL
+// One block per series.  For FWHM > 0 the first warp compacts the
+// extrapolated, NaN-free knot list (ballots), the block computes each row's
+// terms of the spline's tridiagonal system side by side, one thread runs the
+// recurrence and the back substitution (sequential by nature), and the
+// block's threads fill the channels; the knots sit in shared memory.  REAL
 // arithmetic is written with explicitly rounded intrinsics so that it rounds
 // as the reference's does.
 #include <cuda_runtime.h>
@@ -30,6 +32,7 @@ namespace {
 
 constexpr int kConvThreads = 128;
 constexpr int kNstep = 20;   // cirsconv.f: PARAMETER (nstep=20)
+constexpr size_t kConvSmemMax = 200 * 1024;
 
 __device__ float csplint_dev(const float* XA, const float* YA, const float* Y2A, int N, float X) {
     int klo = 1, khi = N;
@@ -71,81 +74,117 @@ __device__ float interp_dev(const float* X, const float* Y, int N, float XIN, bo
     return y;
 }
 
+// Scratch of one series: knots xc, yc, then y2 and u (which first hold each
+// knot's sig and right-hand side, cirsspline's terms that do not depend on
+// the recurrence), and a flag per knot for a repeated abscissa.
+__host__ __device__ inline size_t conv_scratch_floats(int nwave) { return (size_t)4 * (nwave + 2) + (nwave + 2 + 3) / 4; }
+
+template <bool kShared>
 __global__ void __launch_bounds__(kConvThreads)
 cirsconv_kernel(int nwave, const float* __restrict__ vwave, const float* __restrict__ y, float fwhm, int nconv,
                 const float* __restrict__ vconv, int nfwhm, const float* __restrict__ vfwhm,
                 const float* __restrict__ xfwhm, float* __restrict__ yout, float* __restrict__ scr) {
+    extern __shared__ __align__(16) float csm[];
     __shared__ int s_nc;
     const int s = blockIdx.x;
     const float* ys = y + (int64_t)s * nwave;
     const int cap = nwave + 2;
-    float* xc = scr + (int64_t)s * 4 * cap;
+    float* xc = kShared ? csm : scr + (int64_t)s * conv_scratch_floats(nwave);
     float* yc = xc + cap;
     float* y2 = yc + cap;
     float* u = y2 + cap;
-    if (threadIdx.x == 0) {
-        const float half = __fdiv_rn(fwhm, 2.0f);
+    unsigned char* dup = (unsigned char*)(u + cap);
+    const float half = __fdiv_rn(fwhm, 2.0f);
+    if (threadIdx.x < 32) {
+        // the knots: extrapolated end points (cirsconv.f:77-104) around the
+        // calculated points, NaNs dropped (:107-132); warp 0 compacts them
+        const int lane = threadIdx.x;
         int nc = 0;
-        // extrapolated end points (cirsconv.f:77-104), then the points, NaNs dropped (:107-132)
-        const bool lo = vconv[0] < __fadd_rn(vwave[0], half);
-        const bool hi = vconv[nconv - 1] > __fsub_rn(vwave[nwave - 1], half);
-        if (lo) {
+        if (vconv[0] < __fadd_rn(vwave[0], half)) {
             const float x = __fsub_rn(vconv[0], fwhm);
             const float sl = __fdiv_rn(__fsub_rn(ys[1], ys[0]), __fsub_rn(vwave[1], vwave[0]));
             const float v = __fadd_rn(ys[0], __fmul_rn(sl, __fsub_rn(x, vwave[0])));
             if (!isnan(v)) {
-                xc[nc] = x;
-                yc[nc] = v;
-                ++nc;
+                if (lane == 0) {
+                    xc[0] = x;
+                    yc[0] = v;
+                }
+                nc = 1;
             }
         }
-        for (int i = 0; i < nwave; ++i)
-            if (!isnan(ys[i])) {
-                xc[nc] = vwave[i];
-                yc[nc] = ys[i];
-                ++nc;
+        for (int b = 0; b < nwave; b += 32) {
+            const int i = b + lane;
+            const float yi = i < nwave ? ys[i] : 0.0f;
+            const bool ok = i < nwave && !isnan(yi);
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int at = nc + __popc(m & ((1u << lane) - 1u));
+                xc[at] = vwave[i];
+                yc[at] = yi;
             }
-        if (hi) {
+            nc += __popc(m);
+        }
+        if (vconv[nconv - 1] > __fsub_rn(vwave[nwave - 1], half)) {
             const float x = __fadd_rn(vconv[nconv - 1], fwhm);
             const float sl = __fdiv_rn(__fsub_rn(ys[nwave - 1], ys[nwave - 2]),
                                        __fsub_rn(vwave[nwave - 1], vwave[nwave - 2]));
             const float v = __fadd_rn(ys[nwave - 1], __fmul_rn(sl, __fsub_rn(x, vwave[nwave - 1])));
             if (!isnan(v)) {
-                xc[nc] = x;
-                yc[nc] = v;
+                if (lane == 0) {
+                    xc[nc] = x;
+                    yc[nc] = v;
+                }
                 ++nc;
             }
         }
-        // CSPLINE with natural ends (YP1, YPN > .99E30)
-        y2[0] = 0.0f;
-        u[0] = 0.0f;
-        for (int i = 1; i < nc - 1; ++i) {
-            const float sig = __fdiv_rn(__fsub_rn(xc[i], xc[i - 1]), __fsub_rn(xc[i + 1], xc[i - 1]));
-            const float p = __fadd_rn(__fmul_rn(sig, y2[i - 1]), 2.0f);
-            y2[i] = __fdiv_rn(__fsub_rn(sig, 1.0f), p);
-            if (xc[i - 1] == xc[i] || xc[i] == xc[i + 1]) {
-                u[i] = u[i - 1];
-                continue;
-            }
-            const float d1 = __fdiv_rn(__fsub_rn(yc[i + 1], yc[i]), __fsub_rn(xc[i + 1], xc[i]));
-            const float d0 = __fdiv_rn(__fsub_rn(yc[i], yc[i - 1]), __fsub_rn(xc[i], xc[i - 1]));
-            const float t = __fdiv_rn(__fmul_rn(6.0f, __fsub_rn(d1, d0)), __fsub_rn(xc[i + 1], xc[i - 1]));
-            u[i] = __fdiv_rn(__fsub_rn(t, __fmul_rn(sig, u[i - 1])), p);
-        }
-        if (nc >= 2) {
-            y2[nc - 1] = __fdiv_rn(__fsub_rn(0.0f, __fmul_rn(0.0f, u[nc - 2])),
-                                   __fadd_rn(__fmul_rn(0.0f, y2[nc - 2]), 1.0f));
-            for (int k = nc - 2; k >= 0; --k) y2[k] = __fadd_rn(__fmul_rn(y2[k], y2[k + 1]), u[k]);
-        }
-        s_nc = nc;
+        if (lane == 0) s_nc = nc;
     }
     __syncthreads();
     const int nc = s_nc;
+    // CSPLINE with natural ends (YP1, YPN > .99E30): the terms of each row
+    // that do not depend on the recurrence, side by side
+    for (int i = 1 + threadIdx.x; i < nc - 1; i += kConvThreads) {
+        const float sig = __fdiv_rn(__fsub_rn(xc[i], xc[i - 1]), __fsub_rn(xc[i + 1], xc[i - 1]));
+        y2[i] = sig;
+        if (xc[i - 1] == xc[i] || xc[i] == xc[i + 1]) {
+            dup[i] = 1;
+            u[i] = 0.0f;
+        } else {
+            dup[i] = 0;
+            const float d1 = __fdiv_rn(__fsub_rn(yc[i + 1], yc[i]), __fsub_rn(xc[i + 1], xc[i]));
+            const float d0 = __fdiv_rn(__fsub_rn(yc[i], yc[i - 1]), __fsub_rn(xc[i], xc[i - 1]));
+            u[i] = __fdiv_rn(__fmul_rn(6.0f, __fsub_rn(d1, d0)), __fsub_rn(xc[i + 1], xc[i - 1]));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // the recurrence and the back substitution (cspline.f), one thread
+        float y2p = 0.0f, up = 0.0f;
+        y2[0] = 0.0f;
+        u[0] = 0.0f;
+        for (int i = 1; i < nc - 1; ++i) {
+            const float sig = y2[i], t = u[i];
+            const float p = __fadd_rn(__fmul_rn(sig, y2p), 2.0f);
+            y2p = __fdiv_rn(__fsub_rn(sig, 1.0f), p);
+            up = dup[i] ? up : __fdiv_rn(__fsub_rn(t, __fmul_rn(sig, up)), p);
+            y2[i] = y2p;
+            u[i] = up;
+        }
+        if (nc >= 2) {
+            float nxt = __fdiv_rn(__fsub_rn(0.0f, __fmul_rn(0.0f, u[nc - 2])), __fadd_rn(__fmul_rn(0.0f, y2[nc - 2]), 1.0f));
+            y2[nc - 1] = nxt;
+            for (int k = nc - 2; k >= 0; --k) {
+                nxt = __fadd_rn(__fmul_rn(y2[k], nxt), u[k]);
+                y2[k] = nxt;
+            }
+        }
+    }
+    __syncthreads();
     for (int i = threadIdx.x; i < nconv; i += kConvThreads) {
         // the channel's bin width: FWHM, or the .fwh table at the channel (cirsconv.f:147-150)
         const float yfwhm = nfwhm > 0 ? interp_dev(vfwhm, xfwhm, nfwhm, vconv[i], true) : fwhm;
-        const float half = __fdiv_rn(yfwhm, 2.0f);
-        const float x1 = __fsub_rn(vconv[i], half), x2 = __fadd_rn(vconv[i], half);
+        const float hw = __fdiv_rn(yfwhm, 2.0f);
+        const float x1 = __fsub_rn(vconv[i], hw), x2 = __fadd_rn(vconv[i], hw);
         const float delx = __fdiv_rn(__fsub_rn(x2, x1), (float)(kNstep - 1));
         const double hd = (double)__fdiv_rn(delx, 2.0f);
         double sum = 0.0, yold = 0.0;
@@ -165,15 +204,34 @@ cirsconv_kernel(int nwave, const float* __restrict__ vwave, const float* __restr
 __global__ void __launch_bounds__(kConvThreads)
 filter_weights_kernel(int nwave, const float* __restrict__ vwave, const int* __restrict__ fil_of,
                       const int* __restrict__ fil_off, const float* __restrict__ vfil, const float* __restrict__ fil,
-                      float* __restrict__ w) {
+                      float* __restrict__ w, int* __restrict__ span) {
+    __shared__ int s_lo, s_hi;
     const int i = blockIdx.x;
     const int k = fil_of[i];
     const float* X = vfil + fil_off[k];
     const float* Y = fil + fil_off[k];
     const int n = fil_off[k + 1] - fil_off[k];
+    if (threadIdx.x == 0) {
+        s_lo = nwave;
+        s_hi = -1;
+    }
+    __syncthreads();
+    int lo = nwave, hi = -1;
     for (int j = threadIdx.x; j < nwave; j += kConvThreads) {
         const float v = vwave[j];
-        w[(int64_t)i * nwave + j] = (v >= X[0] && v <= X[n - 1]) ? interp_dev(X, Y, n, v, false) : 0.0f;
+        const float yt = (v >= X[0] && v <= X[n - 1]) ? interp_dev(X, Y, n, v, false) : 0.0f;
+        w[(int64_t)i * nwave + j] = yt;
+        if (yt != 0.0f) {
+            lo = min(lo, j);
+            hi = max(hi, j);
+        }
+    }
+    atomicMin(&s_lo, lo);
+    atomicMax(&s_hi, hi);
+    __syncthreads();
+    if (threadIdx.x == 0) {   // the points where the channel's weight is not zero
+        span[2 * i] = s_lo;
+        span[2 * i + 1] = s_hi;
     }
 }
 
@@ -182,13 +240,15 @@ filter_weights_kernel(int nwave, const float* __restrict__ vwave, const int* __r
 // the last one where ytmp is not zero
 __global__ void __launch_bounds__(kConvThreads)
 filter_conv_kernel(int nwave, int nconv, const float* __restrict__ vwave, const float* __restrict__ y,
-                   const float* __restrict__ w, float* __restrict__ yout) {
+                   const float* __restrict__ w, const int* __restrict__ span, float* __restrict__ yout) {
     const int s = blockIdx.x;
     const float* ys = y + (int64_t)s * nwave;
     for (int i = threadIdx.x; i < nconv; i += kConvThreads) {
         const float* wi = w + (int64_t)i * nwave;
         double sum = 0.0, sumf = 0.0;
-        for (int j = 0; j < nwave - 1; ++j) {
+        // outside [lo, hi] every weight is zero and adds nothing
+        const int lo = span[2 * i], hi = min(span[2 * i + 1], nwave - 2);
+        for (int j = lo; j <= hi; ++j) {
             const float yt = wi[j];
             if (yt != 0.0f) {
                 const float delv = __fsub_rn(vwave[j + 1], vwave[j]);
@@ -293,7 +353,11 @@ int conv_run(rtb_context* c, const ConvSpec& cs, int nseg, const ConvSeg* seg, c
     const size_t o_fo = put(cs.fil_of.data(), cs.fil_of.size() * 4), o_ff = put(cs.fil_off.data(), cs.fil_off.size() * 4);
     const size_t o_pv = put(cs.vfil.data(), cs.vfil.size() * 4), o_pf = put(cs.fil.data(), cs.fil.size() * 4);
     const size_t o_scr = align16(blob.size());
-    const size_t n_scr = cs.fwhm > 0.0f ? (size_t)nser_max * 4 * (nwave + 2) * 4 : (size_t)nconv * nwave * 4;
+    // FWHM > 0: spline knots in shared memory when they fit, else in this scratch
+    const size_t knot_bytes = conv_scratch_floats(nwave) * 4;
+    const bool knots_shared = knot_bytes <= kConvSmemMax;
+    const size_t n_scr = cs.fwhm > 0.0f ? (knots_shared ? 0 : (size_t)nser_max * knot_bytes)
+                                        : (size_t)nconv * nwave * 4 + (size_t)nconv * 8;
     CUDA_TRY(c, c->d_conv.ensure(o_scr + n_scr + 16));
     char* d = (char*)c->d_conv.p;
     CUDA_TRY(c, cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, st));
@@ -301,21 +365,32 @@ int conv_run(rtb_context* c, const ConvSpec& cs, int nseg, const ConvSeg* seg, c
     const float* dvc = (const float*)(d + o_vc);
     float* dscr = (float*)(d + o_scr);
     if (cs.fwhm > 0.0f) {
+        if (knots_shared)
+            CUDA_TRY(c, cudaFuncSetAttribute(cirsconv_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)knot_bytes));
         for (int q = 0; q < nseg; ++q)
             if (seg[q].nser > 0) {
-                cirsconv_kernel<<<seg[q].nser, kConvThreads, 0, st>>>(
-                    nwave, dvw, seg[q].y, cs.fwhm, nconv, dvc, (int)cs.vfwhm.size(), (const float*)(d + o_vf),
-                    (const float*)(d + o_xf), seg[q].yout, dscr);
+                if (knots_shared)
+                    cirsconv_kernel<true><<<seg[q].nser, kConvThreads, knot_bytes, st>>>(
+                        nwave, dvw, seg[q].y, cs.fwhm, nconv, dvc, (int)cs.vfwhm.size(), (const float*)(d + o_vf),
+                        (const float*)(d + o_xf), seg[q].yout, dscr);
+                else
+                    cirsconv_kernel<false><<<seg[q].nser, kConvThreads, 0, st>>>(
+                        nwave, dvw, seg[q].y, cs.fwhm, nconv, dvc, (int)cs.vfwhm.size(), (const float*)(d + o_vf),
+                        (const float*)(d + o_xf), seg[q].yout, dscr);
                 CUDA_TRY(c, cudaGetLastError());
             }
         return RTB_OK;
     }
+    int* dspan = (int*)(dscr + (size_t)nconv * nwave);
     filter_weights_kernel<<<nconv, kConvThreads, 0, st>>>(nwave, dvw, (const int*)(d + o_fo), (const int*)(d + o_ff),
-                                                          (const float*)(d + o_pv), (const float*)(d + o_pf), dscr);
+                                                          (const float*)(d + o_pv), (const float*)(d + o_pf), dscr,
+                                                          dspan);
     CUDA_TRY(c, cudaGetLastError());
     for (int q = 0; q < nseg; ++q)
         if (seg[q].nser > 0) {
-            filter_conv_kernel<<<seg[q].nser, kConvThreads, 0, st>>>(nwave, nconv, dvw, seg[q].y, dscr, seg[q].yout);
+            filter_conv_kernel<<<seg[q].nser, kConvThreads, 0, st>>>(nwave, nconv, dvw, seg[q].y, dscr, dspan,
+                                                                     seg[q].yout);
             CUDA_TRY(c, cudaGetLastError());
         }
     return RTB_OK;

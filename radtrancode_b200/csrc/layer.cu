@@ -3,11 +3,14 @@
 // (radtran/path/atmg.f:250-373, 509-560), the set-up subpathg runs before
 // every forward call of a retrieval (the .prf -> layers step).
 //
-// One warp per layer.  The warp's lanes share the layer's accumulators: lane
-// role 0 the layer totals (TOTAM, TEMP, PRESS) and the gradient rows DTE,
-// DAM, DCO; roles 1..nvmr the amount and partial pressure of one gas; the
-// rest one dust type each.  Every role walks the 101 Simpson points itself,
-// so each accumulator is summed in the reference's order; the REAL
+// One warp (block) per layer.  For a Curtis-Godson layer the lanes first
+// evaluate the 101 Simpson points side by side into shared memory (the
+// bracket search and every interpolation); then each lane owns one
+// accumulator -- lane 0 the layer totals (TOTAM, TEMP, PRESS) and the
+// gradient rows DTE, DAM, DCO, the next lanes the amount and partial
+// pressure of one gas each, the rest one dust type each -- and sums it over
+// the points in the reference's order, so every sum rounds as the
+// reference's does; the REAL
 // arithmetic is written with explicitly rounded intrinsics (no contraction
 // into FMA) so that it rounds as the reference's does.  The few
 // transcendental scalars of the set-up (SIN/COS of the two angles, ASIN of
@@ -29,7 +32,6 @@ namespace rtb {
 
 namespace {
 
-constexpr int kLayWarps = 4;
 constexpr int kNint = 101;                              // layerg.f:44
 
 __device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
@@ -48,6 +50,19 @@ __device__ int above_dev(const float* X, int N, float XIN) {
         for (int k = 1; k <= N; ++k)
             if (X[k - 1] < XIN) { I = k; break; }
     }
+    return I == 1 ? 2 : I;
+}
+
+// the same bracket on a non-decreasing grid with x[0] < x[N-1], by bisection:
+// the first point above XIN is the upper bound
+__device__ int above_sorted(const float* X, int N, float XIN) {
+    int lo = 0, hi = N;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (X[mid] > XIN) hi = mid; else lo = mid + 1;
+    }
+    int I = lo + 1;
+    if (I > N) I = N;
     return I == 1 ? 2 : I;
 }
 
@@ -77,7 +92,9 @@ struct LayGeom {
 
 struct LayArgs {
     int npro, nvmr, ndust, nlay, laytyp, layint, botlay, surface;
-    const float *h, *p, *t, *vmr, *dust, *base;   // vmr [nvmr][npro], dust [ndust][npro]
+    int hsorted;                                   // h ascending: the height bracket by bisection
+    const float *h, *p, *t, *vmr, *dust;          // vmr [nvmr][npro], dust [ndust][npro]
+    const float* bases_h;                          // [nlay] layer base heights (layerg.f:164-224, on the host)
     float molwt, radius;
     LayGeom g;
     float sin2, cosz, zpath;                       // the path's geometry (atmg.f:290-292)
@@ -89,30 +106,6 @@ struct LayArgs {
     int* status;
 };
 
-// base height of layer I (1-based), layerg.f:164-224
-__device__ float base_height(const LayArgs& A, int I) {
-    const int NPRO = A.npro;
-    const float* H = A.h;
-    const float* P = A.p;
-    const LayGeom& g = A.g;
-    const float fi = (float)(I - 1), fn = (float)A.nlay;
-    switch (A.laytyp) {
-        case 0: {
-            const float pnow = fa(g.pbot, fd(fm(fi, fs(P[NPRO - 1], g.pbot)), fn));
-            return verint_dev(P, H, NPRO, pnow);
-        }
-        case 2: return fa(g.layht, fd(fm(fi, fs(H[NPRO - 1], g.layht)), fn));
-        case 3: {
-            const float s = fd(fm(fi, g.smax), fn);
-            const float u = fa(s, fm(g.cosa, g.z0));
-            return fs(__fsqrt_rn(fa(fm(g.sin2a, fm(g.z0, g.z0)), fm(u, u))), A.radius);
-        }
-        case 1:   // base pressures exp(ln p) from the host (layerg.f:174-181)
-        case 4: return verint_dev(P, H, NPRO, A.base[I - 1]);
-        default: return A.base[I - 1];
-    }
-}
-
 // distance along a path from its start to height b (atmg.f:357-362 / layerg.f:236-240)
 __device__ float path_s(float radius, float b, float sin2, float z, float cosz) {
     float stmp = fs(fm(fa(radius, b), fa(radius, b)), fm(sin2, fm(z, z)));
@@ -120,9 +113,139 @@ __device__ float path_s(float radius, float b, float sin2, float z, float cosz) 
     return fs(__fsqrt_rn(stmp), fm(z, cosz));
 }
 
-__global__ void __launch_bounds__(32 * kLayWarps) layerg_kernel(LayArgs A) {
-    const int lane = threadIdx.x & 31;
-    const int L = blockIdx.x * kLayWarps + (threadIdx.x >> 5) + 1;   // 1-based layer
+// shared memory of one layer's Curtis-Godson pass: the 101 points' bracket,
+// P, T, DUDS and F, every gas's and dust's value at them, and the layer's
+// three gradient rows
+constexpr int kPointArrays = 8;   // per point: bracket, DUDS*W, T*DUDS*W, P*DUDS*W, the two DTE/DAM and DCO terms
+
+size_t layer_smem_bytes(int nvmr, int ndust, int npro) {
+    const int nq = 1 + nvmr + ndust;
+    return (size_t)(kPointArrays + 2 * nvmr + ndust) * kNint * 4 + (size_t)3 * npro * 4 + (size_t)(2 + nq) * npro * 4;
+}
+
+// the Curtis-Godson layer (layerg.f:315-422) in three phases: the lanes
+// evaluate the 101 points side by side (bracket search and interpolations,
+// the costly part); then each lane sums its own quantity over the points in
+// the reference's order, reading them from shared memory; then the lanes
+// normalise the gradient rows together
+__device__ void curtis_godson(const LayArgs& A, int i, float S0, float S1, float laysf, float* sm, float& PRESS_o,
+                              float& TEMP_o, float& TOTAM_o, bool& bad) {
+    const int lane = threadIdx.x, NPRO = A.npro, NLAY = A.nlay, NV = A.nvmr, ND = A.ndust;
+    const int nq = 1 + NV + ND;
+    const LayGeom& g = A.g;
+    int* pI = (int*)sm;
+    float* dw = sm + kNint;                 // DUDS*W(K)
+    float* tw = dw + kNint;                 // TNOW*DUDS*W(K)
+    float* pw = tw + kNint;                 // PNOW*DUDS*W(K)
+    float* a0 = pw + kNint;                 // (1-F)*DUDS*W(K), F*DUDS*W(K): DTE and DAM
+    float* a1 = a0 + kNint;
+    float* c0 = a1 + kNint;                 // the same times XMOLWT / AVOGAD: DCO
+    float* c1 = c0 + kNint;
+    float* gw = c1 + kNint;                 // per gas VMR1*DUDS*W(K) [NV][kNint], VMR1*PNOW*DUDS*W(K) [NV][kNint]
+    float* gw2 = gw + (size_t)NV * kNint;
+    float* dwc = gw2 + (size_t)NV * kNint;  // per dust DNOW*(XMOLWT/AVOGAD)*DUDS*W(K) [ND][kNint]
+    float* rows = dwc + (size_t)ND * kNint; // dte, dam, dco [NPRO] each
+    float* prof = rows + (size_t)3 * NPRO;  // h, p, t, every gas, every dust [NPRO] each
+    for (int k = lane; k < (2 + nq) * NPRO; k += 32) prof[k] = A.h[k];
+    for (int jj = lane; jj < 3 * NPRO; jj += 32) rows[jj] = 0.0f;
+    __syncwarp();
+    const float* H = prof;
+    const float* Pp = prof + NPRO;
+    const float* Tp = prof + 2 * NPRO;
+    const float* Yp = prof + 3 * NPRO;
+    const float modboltz = 1.013E4f / 1.37947E-23f;  // constdef.f:8-9
+    const float mw_av = fd(A.molwt, 6.022045E23f);   // XMOLWT / AVOGAD
+    const float DELS = fd(fs(S1, S0), (float)(kNint - 1));
+    // every point's terms, side by side (layerg.f:335-400 less the sums)
+    for (int K = lane + 1; K <= kNint; K += 32) {
+        const float S = fa(S0, fm((float)(K - 1), DELS));
+        const float u = fa(S, fm(g.z0, g.cosa));
+        const float HEIGHT = fs(__fsqrt_rn(fa(fm(u, u), fm(g.sin2a, fm(g.z0, g.z0)))), A.radius);
+        const int I = A.hsorted ? above_sorted(H, NPRO, HEIGHT) : above_dev(H, NPRO, HEIGHT);
+        const float PNOW = verint_at(H, Pp, I, HEIGHT);
+        const float TNOW = verint_at(H, Tp, I, HEIGHT);
+        const float DUDS = fd(fm(modboltz, PNOW), TNOW);
+        const float F = verintg_f(H, I, HEIGHT);
+        const float WK = (K == 1 || K == kNint) ? 1.0f : ((K & 1) == 0 ? 4.0f : 2.0f);
+        const int k = K - 1;
+        pI[k] = I;
+        dw[k] = fm(DUDS, WK);
+        tw[k] = fm(fm(TNOW, DUDS), WK);
+        pw[k] = fm(fm(PNOW, DUDS), WK);
+        const float b0 = fm(fm(fs(1.0f, F), DUDS), WK), b1 = fm(fm(F, DUDS), WK);
+        a0[k] = b0;
+        a1[k] = b1;
+        c0[k] = fd(fm(b0, A.molwt), 6.022045E23f);
+        c1[k] = fd(fm(b1, A.molwt), 6.022045E23f);
+        for (int q = 0; q < NV; ++q) {
+            const float v = verint_at(H, Yp + (size_t)q * NPRO, I, HEIGHT);
+            gw[(size_t)q * kNint + k] = fm(fm(v, DUDS), WK);
+            gw2[(size_t)q * kNint + k] = fm(fm(fm(v, PNOW), DUDS), WK);
+        }
+        for (int q = 0; q < ND; ++q) {
+            const float d = verint_at(H, Yp + (size_t)(NV + q) * NPRO, I, HEIGHT);
+            dwc[(size_t)q * kNint + k] = fm(fm(fm(d, mw_av), DUDS), WK);
+        }
+    }
+    __syncwarp();
+    // the sums, each on one lane in the reference's order; TOTAM on every lane
+    float TOTAM = 0.0f;
+    for (int k = 0; k < kNint; ++k) TOTAM = fa(TOTAM, dw[k]);
+    float* dte = rows;
+    float* dam = rows + NPRO;
+    float* dco = rows + 2 * NPRO;
+    for (int q = lane; q < nq; q += 32) {
+        if (q == 0) {
+            float TEMP = 0.0f, PRESS = 0.0f;
+            for (int k = 0; k < kNint; ++k) {
+                const int JJ = pI[k] - 1;
+                TEMP = fa(TEMP, tw[k]);
+                dte[JJ - 1] = fa(dte[JJ - 1], a0[k]);
+                dte[JJ] = fa(dte[JJ], a1[k]);
+                PRESS = fa(PRESS, pw[k]);
+                dco[JJ - 1] = fa(dco[JJ - 1], c0[k]);
+                dco[JJ] = fa(dco[JJ], c1[k]);
+                dam[JJ - 1] = fa(dam[JJ - 1], a0[k]);
+                dam[JJ] = fa(dam[JJ], a1[k]);
+            }
+            // normalisation (layerg.f:403-422) and the vertical path (:430-447)
+            TEMP_o = fd(TEMP, TOTAM);
+            PRESS_o = fd(PRESS, TOTAM);
+            TOTAM_o = fd(fd(fm(TOTAM, DELS), 3.0f), laysf);
+            bad = bad || PRESS_o < 0.0f || TEMP_o < 0.0f || TOTAM_o < 0.0f;
+        } else if (q - 1 < NV) {
+            const int gas = q - 1;
+            float ACC = 0.0f, ACC2 = 0.0f;
+            for (int k = 0; k < kNint; ++k) {
+                ACC = fa(ACC, gw[(size_t)gas * kNint + k]);
+                ACC2 = fa(ACC2, gw2[(size_t)gas * kNint + k]);
+            }
+            const float amount = fd(fd(fm(ACC, DELS), 3.0f), laysf);
+            const float pp = fd(ACC2, TOTAM);
+            A.amount[(size_t)gas * NLAY + i] = amount;
+            A.pp[(size_t)gas * NLAY + i] = pp;
+            bad = bad || amount < 0.0f || pp < 0.0f;
+        } else {
+            const int dst = q - 1 - NV;
+            float ACC = 0.0f;
+            for (int k = 0; k < kNint; ++k) ACC = fa(ACC, dwc[(size_t)dst * kNint + k]);
+            const float cont = fd(fd(fm(ACC, DELS), 3.0f), laysf);
+            A.cont[(size_t)i * ND + dst] = cont;
+            bad = bad || cont < 0.0f;
+        }
+    }
+    __syncwarp();
+    for (int jj = lane; jj < NPRO; jj += 32) {
+        A.dte[(size_t)jj * NLAY + i] = fd(dte[jj], TOTAM);
+        A.dam[(size_t)jj * NLAY + i] = fd(fd(fm(dam[jj], DELS), 3.0f), laysf);
+        A.dco[(size_t)jj * NLAY + i] = fd(fd(fm(dco[jj], DELS), 3.0f), laysf);
+    }
+}
+
+__global__ void __launch_bounds__(32) layerg_kernel(LayArgs A) {
+    extern __shared__ __align__(16) float lsm[];
+    const int lane = threadIdx.x;
+    const int L = blockIdx.x + 1;   // 1-based layer
     if (L > A.nlay) return;
     const int i = L - 1, NPRO = A.npro, NLAY = A.nlay;
     const float* H = A.h;
@@ -130,136 +253,83 @@ __global__ void __launch_bounds__(32 * kLayWarps) layerg_kernel(LayArgs A) {
     const float* T = A.t;
     const LayGeom& g = A.g;
     const float radius = A.radius;
-    const float bh = base_height(A, L);
-    const float bh1 = L < NLAY ? base_height(A, L + 1) : 0.0f;
+    const float bh = A.bases_h[L - 1];
+    const float bh1 = L < NLAY ? A.bases_h[L] : 0.0f;
     const float htop = H[NPRO - 1];
     const float S0 = path_s(radius, bh, g.sin2a, g.z0, g.cosa);
     const float S1 = L < NLAY ? path_s(radius, bh1, g.sin2a, g.z0, g.cosa) : g.smax;
     const float laysf = fd(fs(S1, S0), L < NLAY ? fs(bh1, bh) : fs(htop, bh));
-    // zero this layer's gradient rows
-    for (int jj = lane; jj < NPRO; jj += 32) {
-        A.dte[(size_t)jj * NLAY + i] = 0.0f;
-        A.dam[(size_t)jj * NLAY + i] = 0.0f;
-        A.dco[(size_t)jj * NLAY + i] = 0.0f;
-    }
-    __syncwarp();
-    const int nq = 1 + A.nvmr + A.ndust;
-    const float mw_av = fd(A.molwt, 6.022045E23f);   // XMOLWT / AVOGAD
-    const float modboltz = 1.013E4f / 1.37947E-23f;  // constdef.f:8-9
     bool bad = false;
     float temp_layer = 0.0f;
-    for (int q = lane; q < nq; q += 32) {
-        const int gas = q - 1, dst = q - 1 - A.nvmr;
-        const float* Y = q == 0 ? T : (gas < A.nvmr ? A.vmr + (size_t)gas * NPRO : A.dust + (size_t)dst * NPRO);
-        float TOTAM = 0.0f, TEMP = 0.0f, PRESS = 0.0f, ACC = 0.0f, ACC2 = 0.0f;
-        float* dte = A.dte + i;
-        float* dam = A.dam + i;
-        float* dco = A.dco + i;
-        if (A.layint == 0) {
-            // layer-centre values (layerg.f:264-313)
-            const float S = fm(0.5f, fa(S0, S1));
-            const float u = fa(S, fm(g.z0, g.cosa));
-            const float HEIGHT = fs(__fsqrt_rn(fa(fm(u, u), fm(g.sin2a, fm(g.z0, g.z0)))), radius);
-            const int I = above_dev(H, NPRO, HEIGHT);
-            const float F = verintg_f(H, I, HEIGHT);
-            PRESS = verint_at(H, P, I, HEIGHT);
-            TEMP = verintg_y(T, I, F);
-            TOTAM = fm(fd(fm(modboltz, PRESS), TEMP), fs(S1, S0));
-            if (q == 0) {
-                const int JJ = I - 1;
-                dte[(size_t)(JJ - 1) * NLAY] = fa(dte[(size_t)(JJ - 1) * NLAY], fs(1.0f, F));
-                dte[(size_t)JJ * NLAY] = fa(dte[(size_t)JJ * NLAY], F);
-                // DCO(I,JJ) = (1-F) * TOTAM * XMOLWT / AVOGAD, likewise F
-                dco[(size_t)(JJ - 1) * NLAY] = fd(fm(fm(fs(1.0f, F), TOTAM), A.molwt), 6.022045E23f);
-                dco[(size_t)JJ * NLAY] = fd(fm(fm(F, TOTAM), A.molwt), 6.022045E23f);
-                dam[(size_t)(JJ - 1) * NLAY] = fm(fs(1.0f, F), TOTAM);
-                dam[(size_t)JJ * NLAY] = fm(F, TOTAM);
-            } else if (gas < A.nvmr) {
-                const float v = verintg_y(Y, I, F);
-                ACC = fm(v, TOTAM);
-                ACC2 = fm(v, PRESS);
-            } else {
-                ACC = fd(fm(fm(verintg_y(Y, I, F), TOTAM), A.molwt), 6.022045E23f);
-            }
-        } else {
-            // Curtis-Godson path (layerg.f:315-402)
-            const float DELS = fd(fs(S1, S0), (float)(kNint - 1));
-            for (int K = 1; K <= kNint; ++K) {
-                const float S = fa(S0, fm((float)(K - 1), DELS));
-                const float u = fa(S, fm(g.z0, g.cosa));
-                const float HEIGHT = fs(__fsqrt_rn(fa(fm(u, u), fm(g.sin2a, fm(g.z0, g.z0)))), radius);
-                const int I = above_dev(H, NPRO, HEIGHT);
-                const float PNOW = verint_at(H, P, I, HEIGHT);
-                const float TNOW = verint_at(H, T, I, HEIGHT);
-                const float DUDS = fd(fm(modboltz, PNOW), TNOW);
-                const float WK = (K == 1 || K == kNint) ? 1.0f : ((K & 1) == 0 ? 4.0f : 2.0f);
-                const float dw = fm(DUDS, WK);
-                TOTAM = fa(TOTAM, dw);
-                if (q == 0) {
-                    const float F = verintg_f(H, I, HEIGHT);
-                    const int JJ = I - 1;
-                    const float a0 = fm(fm(fs(1.0f, F), DUDS), WK), a1 = fm(fm(F, DUDS), WK);
-                    TEMP = fa(TEMP, fm(fm(TNOW, DUDS), WK));
-                    dte[(size_t)(JJ - 1) * NLAY] = fa(dte[(size_t)(JJ - 1) * NLAY], a0);
-                    dte[(size_t)JJ * NLAY] = fa(dte[(size_t)JJ * NLAY], a1);
-                    PRESS = fa(PRESS, fm(fm(PNOW, DUDS), WK));
-                    dco[(size_t)(JJ - 1) * NLAY] = fa(dco[(size_t)(JJ - 1) * NLAY], fd(fm(a0, A.molwt), 6.022045E23f));
-                    dco[(size_t)JJ * NLAY] = fa(dco[(size_t)JJ * NLAY], fd(fm(a1, A.molwt), 6.022045E23f));
-                    dam[(size_t)(JJ - 1) * NLAY] = fa(dam[(size_t)(JJ - 1) * NLAY], a0);
-                    dam[(size_t)JJ * NLAY] = fa(dam[(size_t)JJ * NLAY], a1);
-                } else if (gas < A.nvmr) {
-                    const float v = verint_at(H, Y, I, HEIGHT);
-                    ACC = fa(ACC, fm(fm(v, DUDS), WK));
-                    ACC2 = fa(ACC2, fm(fm(fm(v, PNOW), DUDS), WK));
-                } else {
-                    const float d = verint_at(H, Y, I, HEIGHT);
-                    ACC = fa(ACC, fm(fm(fm(d, mw_av), DUDS), WK));
-                }
-            }
-            // normalisation (layerg.f:403-422)
-            if (q == 0) {
-                TEMP = fd(TEMP, TOTAM);
-                PRESS = fd(PRESS, TOTAM);
-                for (int jj = 0; jj < NPRO; ++jj) {
-                    dte[(size_t)jj * NLAY] = fd(dte[(size_t)jj * NLAY], TOTAM);
-                    dam[(size_t)jj * NLAY] = fd(fm(dam[(size_t)jj * NLAY], DELS), 3.0f);
-                    dco[(size_t)jj * NLAY] = fd(fm(dco[(size_t)jj * NLAY], DELS), 3.0f);
-                }
-            } else if (gas < A.nvmr) {
-                ACC = fd(fm(ACC, DELS), 3.0f);
-                ACC2 = fd(ACC2, TOTAM);
-            } else {
-                ACC = fd(fm(ACC, DELS), 3.0f);
-            }
-            TOTAM = fd(fm(TOTAM, DELS), 3.0f);
-        }
-        // back to a vertical path (layerg.f:430-447) and the range check (:449-495)
-        TOTAM = fd(TOTAM, laysf);
-        if (q == 0) {
-            for (int jj = 0; jj < NPRO; ++jj) {
-                dam[(size_t)jj * NLAY] = fd(dam[(size_t)jj * NLAY], laysf);
-                dco[(size_t)jj * NLAY] = fd(dco[(size_t)jj * NLAY], laysf);
-            }
+    if (A.layint == 1) {
+        float PRESS = 0.0f, TEMP = 0.0f, TOTAM = 0.0f;
+        curtis_godson(A, i, S0, S1, laysf, lsm, PRESS, TEMP, TOTAM, bad);
+        if (lane == 0) {
             A.press[i] = PRESS;
             A.temp[i] = TEMP;
             A.totam[i] = TOTAM;
-            A.laysf[i] = laysf;
-            A.baseh[i] = bh;
-            A.delh[i] = L < NLAY ? fs(bh1, bh) : fs(htop, bh);
-            A.basep[i] = verint_dev(H, P, NPRO, bh);
-            A.baset[i] = verint_dev(H, T, NPRO, bh);
-            bad = bad || PRESS < 0.0f || TEMP < 0.0f || TOTAM < 0.0f;
             temp_layer = TEMP;
-        } else if (gas < A.nvmr) {
-            ACC = fd(ACC, laysf);
-            A.amount[(size_t)gas * NLAY + i] = ACC;
-            A.pp[(size_t)gas * NLAY + i] = ACC2;
-            bad = bad || ACC < 0.0f || ACC2 < 0.0f;
-        } else {
-            ACC = fd(ACC, laysf);
-            A.cont[(size_t)i * A.ndust + dst] = ACC;
-            bad = bad || ACC < 0.0f;
         }
+    } else {
+        // layer-centre values (layerg.f:264-313): one point, every lane one quantity
+        const int nq = 1 + A.nvmr + A.ndust;
+        const float modboltz = 1.013E4f / 1.37947E-23f;  // constdef.f:8-9
+        for (int jj = lane; jj < NPRO; jj += 32) {
+            A.dte[(size_t)jj * NLAY + i] = 0.0f;
+            A.dam[(size_t)jj * NLAY + i] = 0.0f;
+            A.dco[(size_t)jj * NLAY + i] = 0.0f;
+        }
+        __syncwarp();
+        const float S = fm(0.5f, fa(S0, S1));
+        const float u = fa(S, fm(g.z0, g.cosa));
+        const float HEIGHT = fs(__fsqrt_rn(fa(fm(u, u), fm(g.sin2a, fm(g.z0, g.z0)))), radius);
+        const int I = A.hsorted ? above_sorted(H, NPRO, HEIGHT) : above_dev(H, NPRO, HEIGHT);
+        const float F = verintg_f(H, I, HEIGHT);
+        const float PRESS = verint_at(H, P, I, HEIGHT);
+        const float TEMP = verintg_y(T, I, F);
+        const float TOTAM = fm(fd(fm(modboltz, PRESS), TEMP), fs(S1, S0));
+        for (int q = lane; q < nq; q += 32) {
+            const int gas = q - 1, dst = q - 1 - A.nvmr;
+            if (q == 0) {
+                const int JJ = I - 1;
+                float* dte = A.dte + i;
+                float* dam = A.dam + i;
+                float* dco = A.dco + i;
+                dte[(size_t)(JJ - 1) * NLAY] = fs(1.0f, F);
+                dte[(size_t)JJ * NLAY] = F;
+                // DCO(I,JJ) = (1-F) * TOTAM * XMOLWT / AVOGAD, likewise F; then / LAYSF
+                dco[(size_t)(JJ - 1) * NLAY] = fd(fd(fm(fm(fs(1.0f, F), TOTAM), A.molwt), 6.022045E23f), laysf);
+                dco[(size_t)JJ * NLAY] = fd(fd(fm(fm(F, TOTAM), A.molwt), 6.022045E23f), laysf);
+                dam[(size_t)(JJ - 1) * NLAY] = fd(fm(fs(1.0f, F), TOTAM), laysf);
+                dam[(size_t)JJ * NLAY] = fd(fm(F, TOTAM), laysf);
+                const float tot = fd(TOTAM, laysf);
+                A.press[i] = PRESS;
+                A.temp[i] = TEMP;
+                A.totam[i] = tot;
+                temp_layer = TEMP;
+                bad = bad || PRESS < 0.0f || TEMP < 0.0f || tot < 0.0f;
+            } else if (gas < A.nvmr) {
+                const float v = verintg_y(A.vmr + (size_t)gas * NPRO, I, F);
+                const float amount = fd(fm(v, TOTAM), laysf);
+                const float pp = fm(v, PRESS);
+                A.amount[(size_t)gas * NLAY + i] = amount;
+                A.pp[(size_t)gas * NLAY + i] = pp;
+                bad = bad || amount < 0.0f || pp < 0.0f;
+            } else {
+                const float v = verintg_y(A.dust + (size_t)dst * NPRO, I, F);
+                const float cont = fd(fd(fm(fm(v, TOTAM), A.molwt), 6.022045E23f), laysf);
+                A.cont[(size_t)i * A.ndust + dst] = cont;
+                bad = bad || cont < 0.0f;
+            }
+        }
+    }
+    if (lane == 0) {
+        A.laysf[i] = laysf;
+        A.baseh[i] = bh;
+        A.delh[i] = L < NLAY ? fs(bh1, bh) : fs(htop, bh);
+        const int Ib = A.hsorted ? above_sorted(H, NPRO, bh) : above_dev(H, NPRO, bh);
+        A.basep[i] = verint_at(H, P, Ib, bh);
+        A.baset[i] = verint_at(H, T, Ib, bh);
     }
     if (bad) atomicOr(A.status, 1);
     // the path entry of this layer (atmg.f:328-373): position I holds layer LOC
@@ -350,30 +420,30 @@ extern "C" int rtb_layerg(rtb_context* c, const rtb_profile* pr, const rtb_layer
     g.pbot = verint_host(H, P, npro, g.layht);
     g.lnpbot = std::log(g.pbot);
     g.smax = std::sqrt((radius + htop) * (radius + htop) - (g.sin2a * (g.z0 * g.z0))) - g.cosa * g.z0;
-    std::vector<float> bases;
-    if (o->laytyp == 1) {   // equal log pressure (layerg.f:174-181): the base pressures
-        const float lnptop = std::log(P[npro - 1]);
-        for (int I = 1; I <= nlay; ++I)
-            bases.push_back(std::exp(g.lnpbot + (float)(I - 1) * (lnptop - g.lnpbot) / (float)nlay));
-    } else if (o->laytyp >= 4) {
-        bases.assign(o->base, o->base + nlay);
-    }
-    in.insert(in.end(), bases.begin(), bases.end());
-    // the path (atmg.f:142-147, 250-292): the bottom layer's base height, the angle
-    const int bl = o->botlay;
-    float bb = 0.0f;
-    switch (o->laytyp) {
-        case 0: bb = verint_host(P, H, npro, g.pbot + (float)(bl - 1) * (P[npro - 1] - g.pbot) / (float)nlay); break;
-        case 1:
-        case 4: bb = verint_host(P, H, npro, bases[bl - 1]); break;
-        case 2: bb = g.layht + (float)(bl - 1) * (htop - g.layht) / (float)nlay; break;
-        case 3: {
-            const float s = (float)(bl - 1) * g.smax / (float)nlay;
-            bb = std::sqrt(g.sin2a * (g.z0 * g.z0) + (s + g.cosa * g.z0) * (s + g.cosa * g.z0)) - radius;
-            break;
+    // the layers' base heights (layerg.f:164-224): nlay scalars of the set-up
+    std::vector<float> bases_h(nlay);
+    const float lnptop = std::log(P[npro - 1]);
+    for (int I = 1; I <= nlay; ++I) {
+        float v = 0.0f;
+        switch (o->laytyp) {
+            case 0: v = verint_host(P, H, npro, g.pbot + (float)(I - 1) * (P[npro - 1] - g.pbot) / (float)nlay); break;
+            case 1:
+                v = verint_host(P, H, npro, std::exp(g.lnpbot + (float)(I - 1) * (lnptop - g.lnpbot) / (float)nlay));
+                break;
+            case 2: v = g.layht + (float)(I - 1) * (htop - g.layht) / (float)nlay; break;
+            case 3: {
+                const float s = (float)(I - 1) * g.smax / (float)nlay;
+                v = std::sqrt(g.sin2a * (g.z0 * g.z0) + (s + g.cosa * g.z0) * (s + g.cosa * g.z0)) - radius;
+                break;
+            }
+            case 4: v = verint_host(P, H, npro, o->base[I - 1]); break;
+            default: v = o->base[I - 1];
         }
-        default: bb = bases[bl - 1];
+        bases_h[I - 1] = v;
     }
+    in.insert(in.end(), bases_h.begin(), bases_h.end());
+    // the path (atmg.f:142-147, 250-292): the bottom layer's base height, the angle
+    const float bb = bases_h[o->botlay - 1];
     const bool surface = o->angle > 90.0f;
     float angle = surface ? 180 - o->angle : o->angle;
     if (o->ipzen == 1) angle = (1.0f / dtr) * std::asin(radius * std::sin(dtr * angle) / (radius + bb));
@@ -399,12 +469,15 @@ extern "C" int rtb_layerg(rtb_context* c, const rtb_profile* pr, const rtb_layer
     A.layint = o->layint;
     A.botlay = o->botlay;
     A.surface = surface ? 1 : 0;
+    A.hsorted = pr->h[0] < pr->h[npro - 1] ? 1 : 0;
+    for (int k = 1; k < npro && A.hsorted; ++k)
+        if (!(pr->h[k] >= pr->h[k - 1])) A.hsorted = 0;
     A.h = din;
     A.p = din + npro;
     A.t = din + 2 * npro;
     A.vmr = din + 3 * npro;
     A.dust = A.vmr + (size_t)nvmr * npro;
-    A.base = A.dust + (size_t)ndust * npro;
+    A.bases_h = A.dust + (size_t)ndust * npro;
     A.molwt = pr->molwt;
     A.radius = pr->radius;
     A.g = g;
@@ -436,7 +509,9 @@ extern "C" int rtb_layerg(rtb_context* c, const rtb_profile* pr, const rtb_layer
     CUDA_TRY(c, cudaMemcpyAsync(din, in.data(), in.size() * 4, cudaMemcpyHostToDevice, st));
     CUDA_TRY(c, cudaMemsetAsync(A.status, 0, 4, st));
     CUDA_TRY(c, cudaMemsetAsync(A.layinc, 0, (size_t)nlay * 3 * 4, st));
-    layerg_kernel<<<(nlay + kLayWarps - 1) / kLayWarps, 32 * kLayWarps, 0, st>>>(A);
+    const size_t lsm = layer_smem_bytes(nvmr, ndust, npro);
+    CUDA_TRY(c, cudaFuncSetAttribute(layerg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm));
+    layerg_kernel<<<nlay, 32, lsm, st>>>(A);
     CUDA_TRY(c, cudaGetLastError());
     std::vector<float> h(n_out);
     int status = 0;

@@ -159,22 +159,42 @@ cirsconv_kernel(int nwave, const float* __restrict__ vwave, const float* __restr
     __syncthreads();
     if (threadIdx.x == 0) {
         // the recurrence and the back substitution (cspline.f), one thread
+        // (each row's precomputed terms are read one step ahead, off the chain)
         float y2p = 0.0f, up = 0.0f;
         y2[0] = 0.0f;
         u[0] = 0.0f;
+        float sig_n = 0.0f, t_n = 0.0f;
+        unsigned char d_n = 0;
+        if (nc > 2) {
+            sig_n = y2[1];
+            t_n = u[1];
+            d_n = dup[1];
+        }
         for (int i = 1; i < nc - 1; ++i) {
-            const float sig = y2[i], t = u[i];
+            const float sig = sig_n, t = t_n;
+            const unsigned char dd = d_n;
+            if (i + 1 < nc - 1) {
+                sig_n = y2[i + 1];
+                t_n = u[i + 1];
+                d_n = dup[i + 1];
+            }
             const float p = __fadd_rn(__fmul_rn(sig, y2p), 2.0f);
             y2p = __fdiv_rn(__fsub_rn(sig, 1.0f), p);
-            up = dup[i] ? up : __fdiv_rn(__fsub_rn(t, __fmul_rn(sig, up)), p);
+            up = dd ? up : __fdiv_rn(__fsub_rn(t, __fmul_rn(sig, up)), p);
             y2[i] = y2p;
             u[i] = up;
         }
         if (nc >= 2) {
             float nxt = __fdiv_rn(__fsub_rn(0.0f, __fmul_rn(0.0f, u[nc - 2])), __fadd_rn(__fmul_rn(0.0f, y2[nc - 2]), 1.0f));
             y2[nc - 1] = nxt;
+            float yk = y2[nc - 2], uk = u[nc - 2];
             for (int k = nc - 2; k >= 0; --k) {
-                nxt = __fadd_rn(__fmul_rn(y2[k], nxt), u[k]);
+                const float ycur = yk, ucur = uk;
+                if (k > 0) {
+                    yk = y2[k - 1];
+                    uk = u[k - 1];
+                }
+                nxt = __fadd_rn(__fmul_rn(ycur, nxt), ucur);
                 y2[k] = nxt;
             }
         }

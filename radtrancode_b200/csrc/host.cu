@@ -722,6 +722,28 @@ int pack_batch(rtb_context* c, int nspec, const rtb_atm* atms, Staging& st) {
     for (auto& x : th) x.join();
     for (int t = 0; t < nthr; ++t)
         if (status[t]) return status[t];
+    // room for every part first, so that the concatenation copies each byte once
+    auto total = [&](auto member) {
+        size_t n = 0;
+        for (const Staging& p : part) n += (p.*member).size();
+        return n;
+    };
+    st.spec.reserve(total(&Staging::spec));
+    st.item_start.reserve(total(&Staging::item_start) + 1);
+    st.lay.reserve(total(&Staging::lay));
+    st.amo.reserve(total(&Staging::amo));
+    st.wave.reserve(total(&Staging::wave));
+    st.wg_slice.reserve(total(&Staging::wg_slice));
+    st.wg_w2.reserve(total(&Staging::wg_w2));
+    st.wg_w1.reserve(total(&Staging::wg_w1));
+    st.xsec.reserve(total(&Staging::xsec));
+    st.cont.reserve(total(&Staging::cont));
+    st.p_layinc.reserve(total(&Staging::p_layinc));
+    st.p_scale.reserve(total(&Staging::p_scale));
+    st.p_emtemp.reserve(total(&Staging::p_emtemp));
+    st.map_row.reserve(total(&Staging::map_row));
+    st.map_val.reserve(total(&Staging::map_val));
+    st.map_colptr.reserve(total(&Staging::map_colptr));
     for (int t = 0; t < nthr; ++t) append_staging(st, part[t]);
     return RTB_OK;
 }
@@ -1041,14 +1063,28 @@ int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float*
     c->stats.d2h_bytes = (long long)c->out_bytes;
     if (status & kStGord) return fail(c, RTB_ERR_GORD, "g-ordinate walk ran past NG (rankg.f:118-147)");
     const float* h = (const float*)c->h_out.p;
-    for (size_t s = 0; s < c->spec_host.size(); ++s) {
-        if (c->any_conv && !c->spec_conv[s].vconv.empty()) continue;
-        const SpecDev& S = c->spec_host[s];
-        const size_t no = (size_t)c->spec_npath[s] * c->spec_nwave[s];
-        const size_t nj = (size_t)c->spec_npath[s] * c->spec_nv[s] * c->spec_nwave[s];
-        if (calcout && calcout[s]) memcpy(calcout[s], h + S.out_off, no * sizeof(float));
-        if (gradtsurf && gradtsurf[s]) memcpy(gradtsurf[s], h + c->n_out + S.out_off, no * sizeof(float));
-        if (gradients && gradients[s]) memcpy(gradients[s], h + 2 * c->n_out + S.jac_off, nj * sizeof(float));
+    auto copy_out = [&](size_t s0, size_t s1) {
+        for (size_t s = s0; s < s1; ++s) {
+            if (c->any_conv && !c->spec_conv[s].vconv.empty()) continue;
+            const SpecDev& S = c->spec_host[s];
+            const size_t no = (size_t)c->spec_npath[s] * c->spec_nwave[s];
+            const size_t nj = (size_t)c->spec_npath[s] * c->spec_nv[s] * c->spec_nwave[s];
+            if (calcout && calcout[s]) memcpy(calcout[s], h + S.out_off, no * sizeof(float));
+            if (gradtsurf && gradtsurf[s]) memcpy(gradtsurf[s], h + c->n_out + S.out_off, no * sizeof(float));
+            if (gradients && gradients[s]) memcpy(gradients[s], h + 2 * c->n_out + S.jac_off, nj * sizeof(float));
+        }
+    };
+    // a large batch is copied out by several host threads (spectrum ranges)
+    const size_t nspec = c->spec_host.size();
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nthr = (int)std::min<size_t>(std::min<unsigned>(hw, 16u), nspec / 8);
+    if (nthr <= 1 || c->out_bytes < ((size_t)64 << 20)) {
+        copy_out(0, nspec);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nthr; ++t)
+            th.emplace_back(copy_out, nspec * t / nthr, nspec * (t + 1) / nthr);
+        for (auto& x : th) x.join();
     }
     return c->any_conv ? fetch_convolved(c, strm, calcout, gradients, gradtsurf) : RTB_OK;
 }

@@ -228,15 +228,23 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         nlmax = std::max(nlmax, nl);
     }
     const int nparam = a.ngas + 1 + a.ncont;
-    // ---- isw (cirsrtfg_wave.f:301-313) ----
+    // ---- the nonzero xmap entries per (parameter, level), and isw: the
+    // parameters that have any (cirsrtfg_wave.f:301-313), in one pass ----
     std::vector<int> isw;
+    std::vector<int> xm_off((size_t)nparam * a.npro + 1);
+    std::vector<std::pair<int, float>> xm_e;
+    xm_e.reserve((size_t)4 * a.nv);
     for (int ip = 0; ip < nparam; ++ip) {
-        bool on = false;
-        for (int ipro = 0; ipro < a.npro && !on; ++ipro)
+        const size_t e0 = xm_e.size();
+        for (int lev = 0; lev < a.npro; ++lev) {
+            xm_off[(size_t)ip * a.npro + lev] = (int)xm_e.size();
+            const float* col = a.xmap + (size_t)d.ld_v * (ip + (size_t)d.ld_param * lev);
             for (int iv = 0; iv < a.nv; ++iv)
-                if (a.xmap[iv + (size_t)d.ld_v * (ip + (size_t)d.ld_param * ipro)] != 0.0f) { on = true; break; }
-        if (on) isw.push_back(ip);
+                if (col[iv] != 0.0f) xm_e.push_back({iv, col[iv]});
+        }
+        if (xm_e.size() > e0) isw.push_back(ip);
     }
+    xm_off[(size_t)nparam * a.npro] = (int)xm_e.size();
     if ((int)isw.size() > kMaxSw)
         return fail(c, RTB_ERR_UNSUPPORTED, "%d active gradient parameters (device limit %d)", (int)isw.size(), kMaxSw);
     SpecDev S;
@@ -423,6 +431,14 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
                 if (wt[iw] < 0) wt[iw] = t;
         }
     }
+    auto grow = [](auto& v, size_t extra) {
+        if (v.capacity() < v.size() + extra) v.reserve(std::max(v.size() + extra, 2 * v.capacity()));
+    };
+    grow(st.wave, a.nwave);
+    grow(st.wg_slice, (size_t)a.nwave * a.ngas);
+    grow(st.wg_w2, (size_t)a.nwave * a.ngas);
+    grow(st.wg_w1, (size_t)a.nwave * a.ngas);
+    grow(st.xsec, (size_t)a.nwave * a.ncont);
     for (int iw = 0; iw < a.nwave; ++iw) {
         WaveDev W;
         memset(&W, 0, sizeof W);
@@ -551,29 +567,27 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     S.map_off = (int64_t)st.map_colptr.size();
     {
         const int nsw = S.nsw, nv = a.nv, npro = a.npro;
-        // nonzero xmap entries per (param, level)
-        std::vector<std::vector<std::pair<int, float>>> xm((size_t)nparam * npro);
-        for (int s = 0; s < nsw; ++s) {
-            const int k = isw[s];
-            for (int lev = 0; lev < npro; ++lev)
-                for (int iv = 0; iv < nv; ++iv) {
-                    const float v = a.xmap[iv + (size_t)d.ld_v * (k + (size_t)d.ld_param * lev)];
-                    if (v != 0.0f) xm[(size_t)k * npro + lev].push_back({iv, v});
-                }
-        }
-        // levels with a nonzero d(layer)/d(level) entry, per layer, for each of dam, dte, dco
+        // levels with a nonzero d(layer)/d(level) entry, per layer, in level
+        // order, for each of dam, dte, dco (two passes down the columns)
         const float* mats[3] = {a.dam, a.dte, a.dco};
         std::vector<std::pair<int, float>> nzl[3];
         std::vector<int> nzl_ptr[3];
         for (int q = 0; q < 3; ++q) {
             if (!mats[q]) continue;
-            nzl_ptr[q].assign(a.nlayer + 1, 0);
-            for (int lay = 0; lay < a.nlayer; ++lay) {
-                for (int lev = 0; lev < npro; ++lev) {
-                    const float m = mats[q][lay + (size_t)d.ld_lay * lev];
-                    if (m != 0.0f) nzl[q].push_back({lev, m});
-                }
-                nzl_ptr[q][lay + 1] = (int)nzl[q].size();
+            std::vector<int>& ptr = nzl_ptr[q];
+            ptr.assign(a.nlayer + 1, 0);
+            for (int lev = 0; lev < npro; ++lev) {
+                const float* col = mats[q] + (size_t)d.ld_lay * lev;
+                for (int lay = 0; lay < a.nlayer; ++lay)
+                    if (col[lay] != 0.0f) ++ptr[lay + 1];
+            }
+            for (int lay = 0; lay < a.nlayer; ++lay) ptr[lay + 1] += ptr[lay];
+            nzl[q].resize(ptr[a.nlayer]);
+            std::vector<int> at(ptr.begin(), ptr.end() - 1);
+            for (int lev = 0; lev < npro; ++lev) {
+                const float* col = mats[q] + (size_t)d.ld_lay * lev;
+                for (int lay = 0; lay < a.nlayer; ++lay)
+                    if (col[lay] != 0.0f) nzl[q][at[lay]++] = {lev, col[lay]};
             }
         }
         // Each (iv, j, s) entry sums m * xmap over levels in ascending order,
@@ -598,7 +612,9 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
                     for (int e = nzl_ptr[q][lay]; e < nzl_ptr[q][lay + 1]; ++e) {
                         const int lev = nzl[q][e].first;
                         const double m = (double)nzl[q][e].second;
-                        for (const auto& x : xm[(size_t)k * npro + lev]) {
+                        const size_t key = (size_t)k * npro + lev;
+                        for (int xe = xm_off[key]; xe < xm_off[key + 1]; ++xe) {
+                            const auto& x = xm_e[xe];
                             if (!hit[x.first]) {
                                 hit[x.first] = 1;
                                 ivs.push_back(x.first);

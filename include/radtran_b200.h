@@ -121,6 +121,22 @@ int rtb_set_ktable_centres(rtb_context* ctx, int npoint, const float* vcen);
  *   kcia         REAL kcia(9, 25, 1501), Fortran order (pair fastest). */
 int rtb_set_cia(rtb_context* ctx, float dnu, const double* temps, const float* kcia);
 
+/* Load the para-H2 CIA table of fpread_all (radtran/radtran/fpread_all.f,
+ * the /FPTABLE/ block of ciacom.f), used instead of the CIA table for an
+ * atmosphere with flagh2p = 1 (cirsradg_wave.f:634-640 calls NPARACON_ALL):
+ *   dnu2           wavenumber step of the grid vvk2(i) = (i-1)*dnu2
+ *   ipara          number of tabulated para-H2 fractions (12 or 24)
+ *   temps[25]      REAL temperatures
+ *   fp[ipara]      para-H2 fractions (nparacon_all.f assumes fp(1) = 0.25 and
+ *                  an even spacing fp(2) - fp(1))
+ *   kh2h2, kh2he   REAL (ipara, 25, 1501), Fortran order: H2-H2 and H2-He
+ *   kcia5          REAL (5, 25, 1501): H2-N2, N2-CH4, N2-N2, CH4-CH4, H2-CH4
+ * rtb_load_para_cia reads the same from the unformatted sequential file
+ * fpread_all.f:45-97 reads (records: temps, fp, kh2h2, kh2he, kcia5). */
+int rtb_set_para_cia(rtb_context* ctx, float dnu2, int ipara, const float* temps, const float* fp,
+                     const float* kh2h2, const float* kh2he, const float* kcia5);
+int rtb_load_para_cia(rtb_context* ctx, const char* path, float dnu2, int ipara);
+
 /* The reference's table files, read on the host (no device work):
  * rtb_load_ktables reads ntab .kta files (read_klist.f / read_khead.f:33-110
  * header, then the records from IREC0 on) and loads them with
@@ -197,7 +213,7 @@ typedef struct rtb_atm {
     const float* dte;      /* (ld_lay, npro) */
     const float* dam;      /* (ld_lay, npro) */
     const float* dco;      /* (ld_lay, npro), may be NULL when ncont == 0 */
-    const float* dfp;      /* (ld_lay, npro), unused (flagh2p must be 0) */
+    const float* dfp;      /* (ld_lay, npro), the para-H2 fraction's d(layer)/d(level), flagh2p = 1 only */
     /* state-vector mapping (cirsrtfg_wave.f argument) */
     const float* xmap;     /* (ld_v, ld_param, npro) */
     /* spectral grid and per-wavenumber dust cross sections */
@@ -212,6 +228,10 @@ typedef struct rtb_atm {
     /* instrument channels; NULL means FWHM = 0 with nconv = nwave (the
      * outputs are on the calculation grid) */
     const rtb_conv* conv;
+    /* flagh2p = 1 (para-H2 CIA through the table of rtb_set_para_cia): the
+     * para-H2 fraction of every layer (HFP, /LAYCOM/); its gradient
+     * parameter is the last, ngas + 1 + ncont, mapped to levels by dfp */
+    const float* hfp;      /* (nlayer) */
 } rtb_atm;
 
 /* Outputs, convolved by cirsconv with atm->fwhm onto the channels of

@@ -642,6 +642,148 @@ void ciaread(const orc_tables& t, R vv, R temp, R* alpha, R* dalpha) {
     }
 }
 
+/* FPREAD_ALL: radtran/radtran/fpread_all.f:160-266, the table held in t:
+ * every para fraction's H2-H2 and H2-He coefficient and d/dT, and the five
+ * further pairs, at (vv, temp).  Returns false outside the wavenumber range,
+ * where the reference computes nothing. */
+template <class R>
+bool fpread_all(const orc_tables& t, R vv, R temp, R* absh2, R* abshe, R* dah2dT, R* dahedT, R& deltaf, R* abs5,
+                R* dabs5dT) {
+    const int NWN = RTB_CIA_NUMWN, NT = RTB_CIA_NUMT, KP = t.ipara;
+    std::vector<R> vvk2(NWN);
+    for (int i = 0; i < NWN; ++i) vvk2[i] = (R)((float)i * t.dnu2);
+    if (vv > vvk2[NWN - 1] || vv < vvk2[0]) return false;
+    R tempk2[RTB_CIA_NUMT];
+    for (int i = 0; i < NT; ++i) tempk2[i] = (R)t.para_temps[i];
+    R temp1;
+    if (temp > tempk2[NT - 1]) temp1 = tempk2[NT - 1]; else temp1 = temp;
+    if (temp < tempk2[0]) temp1 = tempk2[0]; else temp1 = temp;    /* overwrites (fpread_all.f:178-195) */
+    deltaf = (R)t.para_fp[1] - (R)t.para_fp[0];
+    R vvc = vv;
+    const int cv = pindex<R>(vvk2.data(), NWN, vvc);
+    const int ct = pindex<R>(tempk2, NT, temp1);
+    const R tt = (vv - vvk2[cv - 1]) / (vvk2[cv] - vvk2[cv - 1]);
+    const R u = (temp1 - tempk2[ct - 1]) / (tempk2[ct] - tempk2[ct - 1]);
+    const R dudt = (R)1.0 / (tempk2[ct] - tempk2[ct - 1]);
+    auto at = [&](const float* k, int n, int i, int c_t, int c_v) {
+        return (R)k[i + (size_t)n * ((c_t - 1) + (size_t)NT * (c_v - 1))];
+    };
+    for (int i = 0; i < KP; ++i) {
+        const float* tabs[2] = {t.kh2h2, t.kh2he};
+        R* outv[2] = {absh2, abshe};
+        R* outd[2] = {dah2dT, dahedT};
+        for (int q = 0; q < 2; ++q) {
+            const R a11 = at(tabs[q], KP, i, ct, cv), a12 = at(tabs[q], KP, i, ct, cv + 1);
+            const R a22 = at(tabs[q], KP, i, ct + 1, cv + 1), a21 = at(tabs[q], KP, i, ct + 1, cv);
+            outv[q][i] = ((R)1.0 - tt) * ((R)1.0 - u) * a11 + tt * ((R)1.0 - u) * a12 + tt * u * a22 +
+                         ((R)1.0 - tt) * u * a21;
+            const R d = -((R)1.0 - tt) * a11 - tt * a12 + tt * a22 + ((R)1.0 - tt) * a21;
+            outd[q][i] = d * dudt;
+        }
+    }
+    for (int i = 0; i < 5; ++i) {
+        const R a11 = at(t.kcia5, 5, i, ct, cv), a12 = at(t.kcia5, 5, i, ct, cv + 1);
+        const R a22 = at(t.kcia5, 5, i, ct + 1, cv + 1), a21 = at(t.kcia5, 5, i, ct + 1, cv);
+        abs5[i] = ((R)1.0 - tt) * ((R)1.0 - u) * a11 + tt * ((R)1.0 - u) * a12 + tt * u * a22 + ((R)1.0 - tt) * u * a21;
+        dabs5dT[i] = (-((R)1.0 - tt) * a11 - tt * a12 + tt * a22 + ((R)1.0 - tt) * a21) * dudt;
+    }
+    return true;
+}
+
+/* NPARACON_ALL: radtran/radtran/nparacon_all.f:88-336.  dabsorb[6] is the
+ * derivative with the para-H2 fraction.  Returns false outside the table. */
+template <class R>
+bool nparacon_all(const orc_tables& t, R v0, R p, R temp, int ngas, const int* idgas, const int* isogas,
+                  const R* amount, const R* pp, R fpara, R xlen, R& absorb, int* iabs, R* dabsorb) {
+    R qh2 = 0, qhe = 0, qn2 = 0, qch4 = 0, qco2 = 0;
+    for (int i = 0; i < 5; ++i) { iabs[i] = 0; dabsorb[i] = 0; }
+    dabsorb[5] = 0; dabsorb[6] = 0;
+    for (int i = 0; i < ngas; ++i) {
+        const int id = idgas[i], iso = isogas[i];
+        if (id == 39 && (iso == 0 || iso == 1)) { qh2 = pp[i] / p; iabs[0] = i + 1; }
+        if (id == 40) { qhe = pp[i] / p; iabs[1] = i + 1; }
+        if (id == 22) { qn2 = pp[i] / p; iabs[2] = i + 1; }
+        if (id == 6 && (iso == 0 || iso == 1)) { qch4 = (pp[i] / p); iabs[3] = i + 1; }
+        if (id == 2) { qco2 = pp[i] / p; iabs[4] = i + 1; }
+    }
+    const R AMAGAT = (R)2.68675E19f;
+    const R MODBOLTZA = (R)(10.0f * 1.37947E-23f / 1.013f);
+    R tau;
+    if (xlen == 0) {
+        R XP1 = 0, height = 0;
+        for (int i = 0; i < ngas; ++i)
+            if (pp[i] > XP1) { height = amount[i] * MODBOLTZA * temp / pp[i]; XP1 = pp[i]; }
+        const R a = p / (R)1.0, b = (R)273.15f / temp;
+        tau = (a * a) * (b * b) * height;
+    } else {
+        const R height = xlen * (R)1e5f;
+        R XP1 = -1, TOTAM = 0;
+        for (int i = 0; i < ngas; ++i)
+            if (pp[i] > XP1 && pp[i] > 0) { TOTAM = amount[i] * p / pp[i]; XP1 = pp[i]; }
+        const R amag1 = (TOTAM / height) / AMAGAT;
+        tau = height * (amag1 * amag1);
+    }
+    const int KP = t.ipara;
+    std::vector<R> h2(KP), he(KP), dh2(KP), dhe(KP);
+    R deltaf = 0, alpha[5], dalpha[5];
+    if (!fpread_all<R>(t, v0, temp, h2.data(), he.data(), dh2.data(), dhe.data(), deltaf, alpha, dalpha)) return false;
+    R AH2H2, AH2HE, DH2DT, DHEDT, DH2DFP, DHEDFP;
+    if (fpara < 0) {
+        AH2H2 = h2[KP - 1];
+        AH2HE = he[KP - 1];
+        DH2DT = dh2[KP - 1];
+        DHEDT = dhe[KP - 1];
+        DH2DFP = 0;
+        DHEDFP = 0;
+    } else {
+        const R x1 = (R)1.0 + (fpara - (R)0.25) / deltaf;
+        int j = (int)x1;
+        R f = x1 - (R)j;
+        if (j < 1) { j = 1; f = 0; }
+        else if (j > KP - 2) { j = KP - 2; f = 1; }
+        AH2H2 = ((R)1.0 - f) * h2[j - 1] + f * h2[j];
+        AH2HE = ((R)1.0 - f) * he[j - 1] + f * he[j];
+        DH2DT = ((R)1.0 - f) * dh2[j - 1] + f * dh2[j];
+        DHEDT = ((R)1.0 - f) * dhe[j - 1] + f * dhe[j];
+        DH2DFP = (h2[j] - h2[j - 1]) / deltaf;
+        DHEDFP = (he[j] - he[j - 1]) / deltaf;
+    }
+    R sum = AH2H2 * qh2 * qh2 + AH2HE * qh2 * qhe;
+    dabsorb[0] = ((R)2 * qh2 * AH2H2 + qhe * AH2HE);
+    dabsorb[1] = qh2 * AH2HE;
+    dabsorb[5] = (DH2DT * qh2 * qh2 + DHEDT * qh2 * qhe);
+    dabsorb[6] = (DH2DFP * qh2 * qh2 + DHEDFP * qh2 * qhe);
+    sum = sum + (alpha[0] * qh2 * qn2);
+    dabsorb[0] = dabsorb[0] + qn2 * alpha[0];
+    dabsorb[2] = dabsorb[2] + qh2 * alpha[0];
+    dabsorb[5] = dabsorb[5] + qh2 * qn2 * dalpha[0];
+    sum = sum + (alpha[1] * qn2 * qch4);
+    dabsorb[2] = dabsorb[2] + qch4 * alpha[1];
+    dabsorb[3] = dabsorb[3] + qn2 * alpha[1];
+    dabsorb[5] = dabsorb[5] + qn2 * qch4 * dalpha[1];
+    sum = sum + (alpha[2] * qn2 * qn2);
+    dabsorb[2] = dabsorb[2] + (R)2 * qn2 * alpha[2];
+    dabsorb[5] = dabsorb[5] + qn2 * qn2 * dalpha[2];
+    sum = sum + (alpha[3] * qch4 * qch4);
+    dabsorb[3] = dabsorb[3] + (R)2 * qch4 * alpha[3];
+    dabsorb[5] = dabsorb[5] + qch4 * qch4 * dalpha[3];
+    sum = sum + (alpha[4] * qh2 * qch4);
+    dabsorb[0] = dabsorb[0] + qch4 * alpha[4];
+    dabsorb[3] = dabsorb[3] + qh2 * alpha[4];
+    dabsorb[5] = dabsorb[5] + qh2 * qch4 * dalpha[4];
+    const R z = 0;   /* co2cia, n2n2cia, n2h2cia: zero below 3900 cm-1 */
+    sum = sum + z * qco2 * qco2;
+    dabsorb[4] = dabsorb[4] + (R)2 * qco2 * z;
+    sum = sum + z * qn2 * qn2;
+    dabsorb[2] = dabsorb[2] + (R)2 * qn2 * z;
+    sum = sum + z * qn2 * qh2;
+    dabsorb[2] = dabsorb[2] + qh2 * z;
+    dabsorb[0] = dabsorb[0] + qn2 * z;
+    absorb = sum * tau;
+    for (int i = 0; i < 7; ++i) dabsorb[i] = dabsorb[i] * tau;
+    return true;
+}
+
 /* NCIACON: radtran/radtran/nciacon.f:84-310 (the three NIR add-ons co2cia,
  * n2n2cia, n2h2cia are zero below 3900 cm-1; the caller rejects N2/CO2
  * runs above that). iabs[5] are 1-based gas numbers (0 = absent). */
@@ -833,7 +975,9 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
         return RTB_ERR_LIMIT;
     if (t.ng > RTB_MAXG || t.np > RTB_MAXK || std::abs(t.nt) > RTB_MAXK) return RTB_ERR_LIMIT;
     if (t.ng < 2 || std::abs(t.nt) < 2) return RTB_ERR_UNSUPPORTED;
-    if (a.flagh2p != 0 || a.ilbl != 0 || a.inlte != 0 || a.fwhm != 0.0f) return RTB_ERR_UNSUPPORTED;
+    if ((a.flagh2p == 1 && (!t.has_para || !a.hfp)) || (a.flagh2p != 0 && a.flagh2p != 1) || a.ilbl != 0 ||
+        a.inlte != 0 || a.fwhm != 0.0f)
+        return RTB_ERR_UNSUPPORTED;
     if (!(a.iform == 0 || a.iform == 2)) return RTB_ERR_UNSUPPORTED;
     if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
     for (int k = 0; k < a.ngas; ++k) {
@@ -882,7 +1026,7 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
              const std::vector<int>& isw, int iw, Work<R>& W, double* calcout, double* gradients,
              double* gradtsurf, const orc_debug* dbg) {
     const int nlayer = a.nlayer, ngas = a.ngas, ng = t.ng, ncont = a.ncont, npath = a.npath;
-    const int nparam = ngas + 1 + ncont;
+    const int nparam = ngas + 1 + ncont + (a.flagh2p == 1 ? 1 : 0);   /* cirsradg_wave.f:375-376 */
     const int nsw = (int)isw.size();
     const float vwave = a.vwave[iw];
     float vv = vwave;
@@ -951,7 +1095,11 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
         R avgcontmp = 0;
         int iabs[5];
         R dabs[7];
-        if (t.has_cia) {
+        if (a.flagh2p == 1) {                                    /* :634-637 */
+            if (!nparacon_all<R>(t, (R)vv, p, tt, ngas, a.idgas, a.isogas, aam.data(), ppp.data(), (R)a.hfp[j],
+                                 (R)a.delh[j], avgcontmp, iabs, dabs))
+                return RTB_ERR_RANGE;
+        } else if (t.has_cia) {
             nciacon<R>(t, (R)vv, p, tt, a.inormal, ngas, a.idgas, a.isogas, aam.data(), ppp.data(),
                        (R)a.delh[j], avgcontmp, iabs, dabs);
         } else {
@@ -965,6 +1113,7 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
             if (k > 0) dtc[k - 1] = dtc[k - 1] + dabs[ii] / (W.utotl[j] * (R)1.0e20f);
         }
         dtc[ngas] = dtc[ngas] + dabs[5];
+        if (a.flagh2p == 1) dtc[nparam - 1] = dtc[nparam - 1] + dabs[6];   /* :659-661 */
         if (a.iray > 0 && a.itype != 0) {                        /* :663-691 (IRAY=1) */
             const R av = W.utotl[j] * (R)xray;
             taucon = taucon + av;
@@ -1152,7 +1301,8 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                     const float* M;
                     if (k < ngas) M = a.dam;
                     else if (k == ngas) M = a.dte;
-                    else M = a.dco;
+                    else if (k < ngas + 1 + ncont) M = a.dco;
+                    else M = a.dfp;                                   /* para-H2 fraction */
                     if (!M) continue;
                     s = s + dq * (R)M[lay + (size_t)d.ld_lay * jj];
                 }
@@ -1181,7 +1331,7 @@ int run(const orc_tables& t, const rtb_atm& a, double* calcout, double* gradient
     const Dims d = dims_of(a);
     int st = validate(t, a, d);
     if (st) return st;
-    const int nparam = a.ngas + 1 + a.ncont;
+    const int nparam = a.ngas + 1 + a.ncont + (a.flagh2p == 1 ? 1 : 0);
     /* nsw / isw: cirsrtfg_wave.f:301-313 */
     std::vector<int> isw;
     for (int ip = 0; ip < nparam; ++ip) {

@@ -51,6 +51,14 @@ typedef struct orc_tables {
      * first table's centres VCEN(npoint) (read_klist.f:141-145); else NULL */
     int npoint;
     const float* vcen;
+    /* para-H2 CIA (fpread_all): same meaning as rtb_set_para_cia; has_para = 0 -> none */
+    int has_para, ipara;
+    float dnu2;
+    const float* para_temps;
+    const float* para_fp;
+    const float* kh2h2;
+    const float* kh2he;
+    const float* kcia5;
 } orc_tables;
 
 /* Debug capture of the g-bin assignment (mixed mode), one record per

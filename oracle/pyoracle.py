@@ -29,6 +29,9 @@ class OrcTables(C.Structure):
         ("has_cia", C.c_int), ("dnu", C.c_float), ("cia_temps", C.POINTER(C.c_double)),
         ("kcia", C.POINTER(C.c_float)),
         ("npoint", C.c_int), ("vcen", C.POINTER(C.c_float)),
+        ("has_para", C.c_int), ("ipara", C.c_int), ("dnu2", C.c_float),
+        ("para_temps", C.POINTER(C.c_float)), ("para_fp", C.POINTER(C.c_float)),
+        ("kh2h2", C.POINTER(C.c_float)), ("kh2he", C.POINTER(C.c_float)), ("kcia5", C.POINTER(C.c_float)),
     ]
 
 
@@ -67,8 +70,14 @@ def lib():
     return _lib
 
 
-def tables_struct(kt, cia=None):
+def tables_struct(kt, cia=None, para=None):
     t = OrcTables()
+    if para is None and cia is not None:
+        para = getattr(cia, "para", None)
+    if para is not None:
+        t.has_para, t.ipara, t.dnu2 = 1, para.ipara, para.dnu2
+        t.para_temps, t.para_fp = _abi.fptr(para.temps), _abi.fptr(para.fp)
+        t.kh2h2, t.kh2he, t.kcia5 = _abi.fptr(para.kh2h2), _abi.fptr(para.kh2he), _abi.fptr(para.kcia5)
     t.ntab, t.np, t.nt, t.ng = kt.ntab, kt.np_, kt.nt, kt.ng
     t.lnp, t.tk, t.delg = _abi.fptr(kt.lnp), _abi.fptr(kt.tk), _abi.fptr(kt.delg)
     t.vmin, t.delv, t.nbin = _abi.fptr(kt.vmin), _abi.fptr(kt.delv), _abi.iptr(kt.nbin)
@@ -79,7 +88,7 @@ def tables_struct(kt, cia=None):
         t.has_cia, t.dnu = 1, cia.dnu
         t.cia_temps = _abi.dptr(cia.temps)
         t.kcia = _abi.fptr(cia.kcia)
-    t._keep = (kt, cia)
+    t._keep = (kt, cia, para)
     return t
 
 

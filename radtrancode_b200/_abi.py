@@ -56,6 +56,7 @@ class RtbAtm(C.Structure):
         ("tsurf", C.c_float), ("fwhm", C.c_float),
         ("nem", C.c_int), ("vem", _fp), ("emissivity", _fp),
         ("conv", C.POINTER(RtbConv)),
+        ("hfp", _fp),
     ]
 
 

@@ -113,6 +113,10 @@ def lib() -> C.CDLL:
         L.rtb_read_fwh.restype = C.c_int
         L.rtb_read_fil.argtypes = [C.c_char_p, ip, ip, fp, ip, fp, fp, C.c_int, C.c_int]
         L.rtb_read_fil.restype = C.c_int
+        L.rtb_set_para_cia.argtypes = [vp, C.c_float, C.c_int, fp, fp, fp, fp, fp]
+        L.rtb_set_para_cia.restype = C.c_int
+        L.rtb_load_para_cia.argtypes = [vp, C.c_char_p, C.c_float, C.c_int]
+        L.rtb_load_para_cia.restype = C.c_int
         L.rtb_set_ktable_ids.argtypes = [vp, C.c_int, ip, ip]
         L.rtb_set_ktable_ids.restype = C.c_int
         L.rtb_set_ktable_centres.argtypes = [vp, C.c_int, fp]
@@ -145,4 +149,5 @@ EXPORTED = [
     "rtb_cirsradg_wave", "rtb_kta_header", "rtb_load_ktables", "rtb_load_cia",
     "rtb_calc_serr", "rtb_cirsconv", "rtb_cirsconv_ex", "rtb_read_fwh", "rtb_read_fil",
     "rtb_layerg", "rtb_set_ktable_centres", "rtb_set_ktable_ids",
+    "rtb_set_para_cia", "rtb_load_para_cia",
 ]

@@ -141,6 +141,16 @@ class Context:
         """ciaread equivalent from a CIA .tab file."""
         self._check(self._L.rtb_load_cia(self._h, os.fsencode(path), float(dnu)))
 
+    def set_para_cia(self, para):
+        """fpread_all's one-time table read (a synth.ParaCIATable)."""
+        self._check(self._L.rtb_set_para_cia(self._h, float(para.dnu2), int(para.ipara), _abi.fptr(para.temps),
+                                             _abi.fptr(para.fp), _abi.fptr(para.kh2h2), _abi.fptr(para.kh2he),
+                                             _abi.fptr(para.kcia5)))
+
+    def load_para_cia(self, path, dnu2=1.0, ipara=24):
+        """fpread_all equivalent from the table file."""
+        self._check(self._L.rtb_load_para_cia(self._h, os.fsencode(path), float(dnu2), int(ipara)))
+
     def set_cia(self, cia):
         """ciaread's one-time table read."""
         self._check(self._L.rtb_set_cia(self._h, float(cia.dnu), _abi.dptr(cia.temps), _abi.fptr(cia.kcia)))

@@ -73,11 +73,14 @@ struct Staging {
     std::vector<float> wg_w1;         // [.. nwave][ngas] lower-point weight of an irregular grid, < 0 none
     bool any_noncoinc = false;
     bool any_w1 = false;
+    bool any_para = false;
     std::vector<float> xsec, cont;
     std::vector<int> p_layinc;
     std::vector<float> p_scale, p_emtemp;
     std::vector<int> map_colptr, map_row;
     std::vector<float> map_val;
+    std::vector<ParaLayDev> para_lay;
+    std::vector<ParaWaveDev> para_wave;
     int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, ngas_max = 1;
     int64_t n_out = 0, n_jac = 0;
 };
@@ -141,6 +144,11 @@ struct rtb_context {
     // CIA
     int has_cia = 0;
     float dnu = 0.0f;
+    // para-H2 CIA (fpread_all)
+    int has_para = 0, ipara = 0;
+    float dnu2 = 0.0f, para_deltaf = 0.0f;
+    std::vector<float> para_tk, para_fp, para_vk;
+    rtb::DevBuf d_kpara;                     // kh2h2 | kh2he | kcia5
     std::vector<float> cia_tk;               // sngl(temps)
     rtb::DevBuf d_kcia;
     // per-call arena

@@ -240,6 +240,27 @@ int rtb_load_cia(rtb_context* c, const char* path, float dnu) {
     return rtb_set_cia(c, dnu, temps, kcia.data());
 }
 
+// the para-H2 CIA table (fpread_all.f:45-97): five sequential unformatted
+// records, REAL TEMPK2(25), FP(IPARA), KH2H2(IPARA,25,1501),
+// KH2HE(IPARA,25,1501), KCIA5(5,25,1501), each framed by 4-byte lengths
+int rtb_load_para_cia(rtb_context* c, const char* path, float dnu2, int ipara) {
+    if (!c) return RTB_ERR_ARG;
+    if (ipara != 12 && ipara != 24) return fail(c, RTB_ERR_ARG, "para-H2 CIA: ipara %d (12 or 24)", ipara);
+    File fl(path);
+    if (!fl.f) return fail(c, RTB_ERR_ARG, "cannot open %s", path ? path : "(null)");
+    const size_t nk = (size_t)ipara * RTB_CIA_NUMT * RTB_CIA_NUMWN, n5 = (size_t)5 * RTB_CIA_NUMT * RTB_CIA_NUMWN;
+    std::vector<float> temps(RTB_CIA_NUMT), fp(ipara), kh2h2(nk), kh2he(nk), k5(n5);
+    auto rec = [&](float* dst, size_t n) {
+        int32_t m1 = 0, m2 = 0;
+        return std::fread(&m1, 4, 1, fl.f) == 1 && m1 == (int32_t)(n * 4) && std::fread(dst, 4, n, fl.f) == n &&
+               std::fread(&m2, 4, 1, fl.f) == 1 && m2 == m1;
+    };
+    if (!(rec(temps.data(), temps.size()) && rec(fp.data(), fp.size()) && rec(kh2h2.data(), nk) &&
+          rec(kh2he.data(), nk) && rec(k5.data(), n5)))
+        return fail(c, RTB_ERR_ARG, "%s: not a para-H2 CIA table of %d fractions (fpread_all.f:45-97)", path, ipara);
+    return rtb_set_para_cia(c, dnu2, ipara, temps.data(), fp.data(), kh2h2.data(), kh2he.data(), k5.data());
+}
+
 // .fwh (cirsrtfg_wave.f:191-196): NFWHM, then NFWHM records VFWHM XFWHM
 int rtb_read_fwh(const char* path, int* n, float* v, float* x, int cap) {
     File fl(path);

@@ -335,9 +335,32 @@ __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, co
     if (dk != dk) dk = 1e-37f;
 }
 
+// bilinear (wavenumber, temperature) value of one CIA table entry and its
+// d/dT (ciaread.f:178-196, fpread_all.f:220-266): REAL, in the reference's
+// order; the four corners are at b + stride * (ct + 25 cv) and neighbours
+__device__ __forceinline__ void cia_bilinear(const float* kc, int64_t e, int64_t stride, int ct, int cv, float t,
+                                             float u, float dudt, float& x, float& dx) {
+    const float omt = __fsub_rn(1.0f, t), omu = __fsub_rn(1.0f, u);
+    const float a11 = __ldg(kc + e + stride * ((int64_t)ct + 25 * (int64_t)cv));
+    const float a12 = __ldg(kc + e + stride * ((int64_t)ct + 25 * ((int64_t)cv + 1)));
+    const float a22 = __ldg(kc + e + stride * ((int64_t)ct + 1 + 25 * ((int64_t)cv + 1)));
+    const float a21 = __ldg(kc + e + stride * ((int64_t)ct + 1 + 25 * (int64_t)cv));
+    x = __fmul_rn(__fmul_rn(omt, omu), a11);
+    x = __fadd_rn(x, __fmul_rn(__fmul_rn(t, omu), a12));
+    x = __fadd_rn(x, __fmul_rn(__fmul_rn(t, u), a22));
+    x = __fadd_rn(x, __fmul_rn(__fmul_rn(omt, u), a21));
+    float d = -__fmul_rn(omt, a11);
+    d = __fsub_rn(d, __fmul_rn(t, a12));
+    d = __fadd_rn(d, __fmul_rn(t, a22));
+    d = __fadd_rn(d, __fmul_rn(omt, a21));
+    dx = __fmul_rn(d, dudt);
+}
+
 // continuum optical depth of one layer and its active derivatives
-// (cirsradg_wave.f:526-691 with nciacon.f:84-310 / ciaread.f:108-198).
-// Lanes 0..8 interpolate one CIA pair each; the sums run on every lane.
+// (cirsradg_wave.f:526-691 with nciacon.f:84-310 / ciaread.f:108-198, or for
+// flagh2p = 1 nparacon_all.f:160-336 / fpread_all.f:195-266).  Lanes 0..8
+// interpolate one CIA table entry each; the sums run on every lane.
+template <bool para>
 __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, const LayerDev& L, const WaveDev& W,
                                            int64_t iw_glob, int64_t il_glob, int lane, float (&dtc)[kMaxSw]) {
 #pragma unroll
@@ -351,7 +374,74 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
             if (s < S.nsw && S.isw[s] == S.ngas + 1 + k) dtc[s] = tau;
     }
     float absorb = 0.0f, dab[7] = {0, 0, 0, 0, 0, 0, 0};
-    if (S.has_cia) {
+    if (para && S.para) {
+        // lanes 0, 1: H2-H2 at the para entries j0, j0+1; 2, 3: H2-He; 4..8: the
+        // five further pairs of kcia5
+        const ParaLayDev PL = B.para_lay[S.para_off + (il_glob - S.lay_off)];
+        const ParaWaveDev PW = B.para_wave[S.paraw_off + (iw_glob - S.wave_off)];
+        float my_a = 0.0f, my_d = 0.0f;
+        if (lane < 9) {
+            if (lane < 4) {
+                const int e = PL.j0 + ((lane & 1) && !PL.neg ? 1 : 0);
+                cia_bilinear(lane < 2 ? B.kh2h2 : B.kh2he, e, B.ipara, PL.ct, PW.cv, PW.t, PL.u, PL.dudt, my_a, my_d);
+            } else {
+                cia_bilinear(B.kcia5, lane - 4, 5, PL.ct, PW.cv, PW.t, PL.u, PL.dudt, my_a, my_d);
+            }
+        }
+        float v[9], dv[9];
+#pragma unroll
+        for (int p = 0; p < 9; ++p) {
+            v[p] = __shfl_sync(kFull, my_a, p);
+            dv[p] = __shfl_sync(kFull, my_d, p);
+        }
+        float ah2h2, ah2he, dh2dt, dhedt, dh2dfp = 0.0f, dhedfp = 0.0f;
+        if (PL.neg) {
+            ah2h2 = v[0];
+            ah2he = v[2];
+            dh2dt = dv[0];
+            dhedt = dv[2];
+        } else {
+            const float f = PL.f, omf = __fsub_rn(1.0f, PL.f);
+            ah2h2 = __fadd_rn(__fmul_rn(omf, v[0]), __fmul_rn(f, v[1]));
+            ah2he = __fadd_rn(__fmul_rn(omf, v[2]), __fmul_rn(f, v[3]));
+            dh2dt = __fadd_rn(__fmul_rn(omf, dv[0]), __fmul_rn(f, dv[1]));
+            dhedt = __fadd_rn(__fmul_rn(omf, dv[2]), __fmul_rn(f, dv[3]));
+            dh2dfp = __fdiv_rn(__fsub_rn(v[1], v[0]), B.para_deltaf);
+            dhedfp = __fdiv_rn(__fsub_rn(v[3], v[2]), B.para_deltaf);
+        }
+        const float qh2 = L.q[0], qhe = L.q[1], qn2 = L.q[2], qch4 = L.q[3], qco2 = L.q[4];
+        float sum = __fadd_rn(__fmul_rn(__fmul_rn(ah2h2, qh2), qh2), __fmul_rn(__fmul_rn(ah2he, qh2), qhe));
+        dab[0] = __fadd_rn(__fmul_rn(__fmul_rn(2.0f, qh2), ah2h2), __fmul_rn(qhe, ah2he));
+        dab[1] = __fmul_rn(qh2, ah2he);
+        dab[5] = __fadd_rn(__fmul_rn(__fmul_rn(dh2dt, qh2), qh2), __fmul_rn(__fmul_rn(dhedt, qh2), qhe));
+        dab[6] = __fadd_rn(__fmul_rn(__fmul_rn(dh2dfp, qh2), qh2), __fmul_rn(__fmul_rn(dhedfp, qh2), qhe));
+        // H2-N2, N2-CH4, N2-N2, CH4-CH4, H2-CH4 (nparacon_all.f:262-318)
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(v[4], qh2), qn2));
+        dab[0] = __fadd_rn(dab[0], __fmul_rn(qn2, v[4]));
+        dab[2] = __fadd_rn(dab[2], __fmul_rn(qh2, v[4]));
+        dab[5] = __fadd_rn(dab[5], __fmul_rn(__fmul_rn(qh2, qn2), dv[4]));
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(v[5], qn2), qch4));
+        dab[2] = __fadd_rn(dab[2], __fmul_rn(qch4, v[5]));
+        dab[3] = __fadd_rn(dab[3], __fmul_rn(qn2, v[5]));
+        dab[5] = __fadd_rn(dab[5], __fmul_rn(__fmul_rn(qn2, qch4), dv[5]));
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(v[6], qn2), qn2));
+        dab[2] = __fadd_rn(dab[2], __fmul_rn(__fmul_rn(2.0f, qn2), v[6]));
+        dab[5] = __fadd_rn(dab[5], __fmul_rn(__fmul_rn(qn2, qn2), dv[6]));
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(v[7], qch4), qch4));
+        dab[3] = __fadd_rn(dab[3], __fmul_rn(__fmul_rn(2.0f, qch4), v[7]));
+        dab[5] = __fadd_rn(dab[5], __fmul_rn(__fmul_rn(qch4, qch4), dv[7]));
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(v[8], qh2), qch4));
+        dab[0] = __fadd_rn(dab[0], __fmul_rn(qch4, v[8]));
+        dab[3] = __fadd_rn(dab[3], __fmul_rn(qh2, v[8]));
+        dab[5] = __fadd_rn(dab[5], __fmul_rn(__fmul_rn(qh2, qch4), dv[8]));
+        // co2cia / n2n2cia / n2h2cia are zero below 3900 cm-1 (host-checked)
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(0.0f, qco2), qco2));
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(0.0f, qn2), qn2));
+        sum = __fadd_rn(sum, __fmul_rn(__fmul_rn(0.0f, qn2), qh2));
+        absorb = __fmul_rn(sum, L.cia_tau);
+#pragma unroll
+        for (int i = 0; i < 7; ++i) dab[i] = __fmul_rn(dab[i], L.cia_tau);
+    } else if (S.has_cia) {
         float my_a = 0.0f, my_d = 0.0f;
         if (W.cia_cv >= 0 && lane < 9) {
             const int p = lane;
@@ -430,6 +520,11 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
 #pragma unroll
     for (int s = 0; s < kMaxSw; ++s)
         if (s == S.sw_T) dtc[s] = __fadd_rn(dtc[s], dab[5]);
+    if (para) {   // the para-H2 fraction (cirsradg_wave.f:659-661)
+#pragma unroll
+        for (int s = 0; s < kMaxSw; ++s)
+            if (s == S.sw_para) dtc[s] = __fadd_rn(dtc[s], dab[6]);
+    }
     if (S.iray) {
         const float av = __fmul_rn(L.utotl, W.xray);
         taucon = __fadd_rn(taucon, av);
@@ -945,9 +1040,9 @@ __device__ __forceinline__ void planck_fp32(int ispace, float vwave, float T, fl
 
 // ---------------------------------------------------------------------------
 // t2: the run's k-tables carry one temperature grid per pressure (NT < 0);
-// a template argument so that the usual single-grid kernel carries no trace
-// of the other interpolation
-template <bool t2>
+// para: some spectrum takes the para-H2 CIA (flagh2p = 1).  Template
+// arguments, so that the usual kernel carries no trace of either
+template <bool t2, bool para>
 __global__ void __launch_bounds__(kThreads, 5)
 fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) {
     extern __shared__ __align__(16) char smem[];
@@ -1046,7 +1141,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
             const int64_t il_glob = S.lay_off + l;
             const LayerDev L = B.lay[il_glob];
             float dtc[kMaxSw];
-            const float taucon = continuum(B, S, L, W, iw_glob, il_glob, lane, dtc);
+            const float taucon = continuum<para>(B, S, L, W, iw_glob, il_glob, lane, dtc);
             const float* amo = B.amo + S.lg_off + (int64_t)l * S.ngas;
             const int64_t* slices = B.wg_slice + S.wg_off + (int64_t)iw * S.ngas;
             const float* w2s = B.wg_w2 ? B.wg_w2 + S.wg_off + (int64_t)iw * S.ngas : nullptr;
@@ -1307,20 +1402,24 @@ int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath) {
 
 int fwd_blocks_per_sm(int smem) {
     int nb = 0;
-    // both instantiations: the smaller residency of the two
-    int nb2 = 0;
-    if (cudaFuncSetAttribute(fwd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-        cudaFuncSetAttribute(fwd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-        return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fwd_kernel<false>, kThreads, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, fwd_kernel<true>, kThreads, smem) != cudaSuccess)
-        return 0;
-    return nb < nb2 ? nb : nb2;
+    // every instantiation: the smallest residency of them
+    void (*const kerns[4])(BatchDev, int, int, int, int) = {fwd_kernel<false, false>, fwd_kernel<true, false>,
+                                                            fwd_kernel<false, true>, fwd_kernel<true, true>};
+    nb = 1 << 30;
+    for (auto k : kerns) {
+        int n = 0;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kThreads, smem) != cudaSuccess)
+            return 0;
+        nb = n < nb ? n : nb;
+    }
+    return nb;
 }
 
 cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st) {
     const int smem = fwd_smem_bytes(B.ng, nsw, ncol, nlmax, npath);
-    auto kern = B.t2 ? fwd_kernel<true> : fwd_kernel<false>;
+    auto kern = B.para ? (B.t2 ? fwd_kernel<true, true> : fwd_kernel<false, true>)
+                       : (B.t2 ? fwd_kernel<true, false> : fwd_kernel<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     kern<<<grid, kThreads, smem, st>>>(B, nsw, ncol, nlmax, npath);

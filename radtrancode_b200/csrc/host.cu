@@ -195,7 +195,9 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     if (a.nlayer > d.ld_lay || a.nlayer > RTB_MAXLAY || a.npath > RTB_MAXPAT || a.ngas > RTB_MAXGAS ||
         a.ncont > RTB_MAXCON || a.npro > RTB_MAXPRO || a.nv > d.ld_v || a.nv > RTB_MAXV)
         return fail(c, RTB_ERR_LIMIT, "array limit exceeded (check_limits.f)");
-    if (a.flagh2p != 0) return fail(c, RTB_ERR_UNSUPPORTED, "flagh2p=1 (nparacon path) not implemented");
+    if (a.flagh2p != 0 && a.flagh2p != 1) return fail(c, RTB_ERR_ARG, "flagh2p=%d", a.flagh2p);
+    if (a.flagh2p == 1 && (!c->has_para || !a.hfp))
+        return fail(c, RTB_ERR_ARG, "flagh2p=1 needs the para-H2 CIA table (rtb_set_para_cia) and hfp");
     if (a.ilbl != 0) return fail(c, RTB_ERR_UNSUPPORTED, "ILBL != 0 (line-by-line tables) not implemented");
     if (a.inlte != 0) return fail(c, RTB_ERR_UNSUPPORTED, "non-LTE emission temperatures not implemented");
     if (!(a.iform == 0 || a.iform == 2)) return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d not implemented", a.iform);
@@ -227,7 +229,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         }
         nlmax = std::max(nlmax, nl);
     }
-    const int nparam = a.ngas + 1 + a.ncont;
+    const int nparam = a.ngas + 1 + a.ncont + (a.flagh2p == 1 ? 1 : 0);   // cirsradg_wave.f:375-376
     // ---- the nonzero xmap entries per (parameter, level), and isw: the
     // parameters that have any (cirsrtfg_wave.f:301-313), in one pass ----
     std::vector<int> isw;
@@ -277,6 +279,13 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         if (isw[s] == a.ngas) S.sw_T = s;
     }
     S.ncol = ncol;
+    S.para = a.flagh2p == 1 ? 1 : 0;
+    S.sw_para = -1;
+    for (int s = 0; s < S.nsw; ++s)
+        if (S.para && isw[s] == a.ngas + 1 + a.ncont) S.sw_para = s;
+    if (S.sw_para >= 0 && !a.dfp) return fail(c, RTB_ERR_ARG, "para-H2 fraction in xmap without dfp");
+    S.para_off = (int64_t)st.para_lay.size();
+    S.paraw_off = (int64_t)st.para_wave.size();
     for (int ip = 0; ip < a.npath; ++ip) {
         S.nlayin[ip] = a.nlayin[ip];
         S.imod[ip] = a.imod[ip];
@@ -380,6 +389,42 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
             tau = height * (amag1 * amag1);
         }
         L.cia_tau = tau;
+        if (S.para) {
+            // fpread_all.f:178-219 (PINDEX clamps the temperature) and the para
+            // fraction bracket of nparacon_all.f:234-253
+            ParaLayDev PL;
+            const float* tk2 = c->para_tk.data();
+            float temp1;
+            if (T > tk2[RTB_CIA_NUMT - 1]) temp1 = tk2[RTB_CIA_NUMT - 1]; else temp1 = T;
+            if (T < tk2[0]) temp1 = tk2[0]; else temp1 = T;
+            const int ct = pindex_f(tk2, RTB_CIA_NUMT, temp1);
+            PL.ct = ct - 1;
+            PL.u = (temp1 - tk2[ct - 1]) / (tk2[ct] - tk2[ct - 1]);
+            PL.dudt = 1.0f / (tk2[ct] - tk2[ct - 1]);
+            const float fpara = a.hfp[l];
+            const int kpara = c->ipara;
+            if (fpara < 0.0f) {
+                PL.neg = 1;
+                PL.j0 = kpara - 1;
+                PL.f = 0.0f;
+            } else {
+                PL.neg = 0;
+                const float x1 = 1.0f + (fpara - 0.25f) / c->para_deltaf;
+                int j = (int)x1;
+                float f = x1 - (float)j;
+                if (j < 1) {
+                    j = 1;
+                    f = 0.0f;
+                } else if (j > kpara - 2) {
+                    j = kpara - 2;
+                    f = 1.0f;
+                }
+                PL.j0 = j - 1;
+                PL.f = f;
+            }
+            st.para_lay.push_back(PL);
+            st.any_para = true;
+        }
         if (c->has_cia) {
             // ciaread.f:133-157 (the second test overwrites the first; pindex clamps)
             const float* tk1 = c->cia_tk.data();
@@ -456,6 +501,20 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
             const int cv = pindex_ascending(vvk1.data(), RTB_CIA_NUMWN, vvc);   // vvk1(i) = (i-1)*dnu
             W.cia_cv = cv - 1;
             W.cia_t = (vv - vvk1[cv - 1]) / (vvk1[cv] - vvk1[cv - 1]);
+        }
+        if (S.para) {
+            // fpread_all.f:160-205: the wavenumber bracket on vvk2(i) = (i-1)*dnu2; the
+            // reference reads no table outside it (its outputs are then undefined)
+            const float top = (float)(RTB_CIA_NUMWN - 1) * c->dnu2;
+            if (vv > top || vv < 0.0f)
+                return fail(c, RTB_ERR_RANGE, "wavenumber %g outside the para-H2 CIA table (0..%g)", vv, top);
+            std::vector<float>& vk2 = c->para_vk;
+            float vvc = vv;
+            const int cv = pindex_ascending(vk2.data(), RTB_CIA_NUMWN, vvc);
+            ParaWaveDev PW;
+            PW.cv = cv - 1;
+            PW.t = (vv - vk2[cv - 1]) / (vk2[cv] - vk2[cv - 1]);
+            st.para_wave.push_back(PW);
         }
         W.xray = S.iray ? rayleighj_f(vv) * 1E20f : 0.0f;
         if (a.tsurf > 0.0f) {
@@ -569,10 +628,10 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         const int nsw = S.nsw, nv = a.nv, npro = a.npro;
         // levels with a nonzero d(layer)/d(level) entry, per layer, in level
         // order, for each of dam, dte, dco (two passes down the columns)
-        const float* mats[3] = {a.dam, a.dte, a.dco};
-        std::vector<std::pair<int, float>> nzl[3];
-        std::vector<int> nzl_ptr[3];
-        for (int q = 0; q < 3; ++q) {
+        const float* mats[4] = {a.dam, a.dte, a.dco, a.flagh2p == 1 ? a.dfp : nullptr};
+        std::vector<std::pair<int, float>> nzl[4];
+        std::vector<int> nzl_ptr[4];
+        for (int q = 0; q < 4; ++q) {
             if (!mats[q]) continue;
             std::vector<int>& ptr = nzl_ptr[q];
             ptr.assign(a.nlayer + 1, 0);
@@ -607,7 +666,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
                 const int lay = a.layinc[j + (size_t)d.ld_lay * ip] - 1;
                 for (int s = 0; s < nsw; ++s) {
                     const int k = isw[s];
-                    const int q = k < a.ngas ? 0 : (k == a.ngas ? 1 : 2);
+                    const int q = k < a.ngas ? 0 : (k == a.ngas ? 1 : (k < a.ngas + 1 + a.ncont ? 2 : 3));
                     if (!mats[q]) continue;
                     for (int e = nzl_ptr[q][lay]; e < nzl_ptr[q][lay + 1]; ++e) {
                         const int lev = nzl[q][e].first;
@@ -681,6 +740,8 @@ void append_staging(Staging& dst, const Staging& src) {
         S.wc_off += xsec;
         S.path_off += path;
         S.map_off += colptr;
+        S.para_off += (int64_t)dst.para_lay.size();
+        S.paraw_off += (int64_t)dst.para_wave.size();
         S.out_off += dst.n_out;
         S.jac_off += dst.n_jac;
         dst.spec.push_back(S);
@@ -700,6 +761,8 @@ void append_staging(Staging& dst, const Staging& src) {
     append_vec(dst.map_row, src.map_row);
     append_vec(dst.map_val, src.map_val);
     for (int v : src.map_colptr) dst.map_colptr.push_back(v + (int)rows);
+    append_vec(dst.para_lay, src.para_lay);
+    append_vec(dst.para_wave, src.para_wave);
     dst.Lmax = std::max(dst.Lmax, src.Lmax);
     dst.nsw_max = std::max(dst.nsw_max, src.nsw_max);
     dst.ncol_max = std::max(dst.ncol_max, src.ncol_max);
@@ -708,6 +771,7 @@ void append_staging(Staging& dst, const Staging& src) {
     dst.ngas_max = std::max(dst.ngas_max, src.ngas_max);
     dst.any_noncoinc = dst.any_noncoinc || src.any_noncoinc;
     dst.any_w1 = dst.any_w1 || src.any_w1;
+    dst.any_para = dst.any_para || src.any_para;
     dst.n_out += src.n_out;
     dst.n_jac += src.n_jac;
 }
@@ -760,6 +824,8 @@ int pack_batch(rtb_context* c, int nspec, const rtb_atm* atms, Staging& st) {
     st.map_row.reserve(total(&Staging::map_row));
     st.map_val.reserve(total(&Staging::map_val));
     st.map_colptr.reserve(total(&Staging::map_colptr));
+    st.para_lay.reserve(total(&Staging::para_lay));
+    st.para_wave.reserve(total(&Staging::para_wave));
     for (int t = 0; t < nthr; ++t) append_staging(st, part[t]);
     return RTB_OK;
 }
@@ -832,6 +898,8 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     const size_t i_mc = add(st.map_colptr.data(), bytes_of(st.map_colptr));
     const size_t i_mr = add(st.map_row.data(), bytes_of(st.map_row));
     const size_t i_mv = add(st.map_val.data(), bytes_of(st.map_val));
+    const size_t i_parl = add(st.para_lay.data(), bytes_of(st.para_lay));
+    const size_t i_parw = add(st.para_wave.data(), bytes_of(st.para_wave));
     const size_t in_bytes = off + 256;
     CUDA_TRY(c, c->h_in.ensure(in_bytes));
     CUDA_TRY(c, c->d_in.ensure(in_bytes));
@@ -875,6 +943,17 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     B.delg = (const float*)c->d_delg.p;
     B.g_ord = (const double*)c->d_gord.p;
     B.kcia = (const float*)c->d_kcia.p;
+    B.para = st.any_para ? 1 : 0;
+    if (st.any_para) {
+        const size_t nk = (size_t)c->ipara * RTB_CIA_NUMT * RTB_CIA_NUMWN;
+        B.ipara = c->ipara;
+        B.para_deltaf = c->para_deltaf;
+        B.kh2h2 = (const float*)c->d_kpara.p;
+        B.kh2he = B.kh2h2 + nk;
+        B.kcia5 = B.kh2he + nk;
+        B.para_lay = (const ParaLayDev*)dp(i_parl);
+        B.para_wave = (const ParaWaveDev*)dp(i_parw);
+    }
     if (place) {
         B.calcout = place->calcout;
         B.gradtsurf = place->gradtsurf;
@@ -1211,6 +1290,7 @@ void rtb_destroy(rtb_context* c) {
     c->d_conv.release();
     c->d_convout.release();
     c->d_layer.release();
+    c->d_kpara.release();
     c->d_nt32.release();
     c->d_nt64.release();
     c->d_ntsmall.release();
@@ -1332,6 +1412,29 @@ int rtb_set_cia(rtb_context* c, float dnu, const double* temps, const float* kci
     CUDA_TRY(c, c->d_kcia.ensure(n * 4));
     CUDA_TRY(c, cudaMemcpy(c->d_kcia.p, kcia, n * 4, cudaMemcpyHostToDevice));
     c->has_cia = 1;
+    return RTB_OK;
+}
+
+int rtb_set_para_cia(rtb_context* c, float dnu2, int ipara, const float* temps, const float* fp, const float* kh2h2,
+                     const float* kh2he, const float* kcia5) {
+    if (!c) return RTB_ERR_ARG;
+    if (!(dnu2 > 0.0f) || (ipara != 12 && ipara != 24) || !temps || !fp || !kh2h2 || !kh2he || !kcia5)
+        return fail(c, RTB_ERR_ARG, "bad para-H2 CIA arguments (ipara 12 or 24)");
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    const size_t nk = (size_t)ipara * RTB_CIA_NUMT * RTB_CIA_NUMWN, n5 = (size_t)5 * RTB_CIA_NUMT * RTB_CIA_NUMWN;
+    CUDA_TRY(c, c->d_kpara.ensure((2 * nk + n5) * 4));
+    float* d = (float*)c->d_kpara.p;
+    CUDA_TRY(c, cudaMemcpy(d, kh2h2, nk * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(d + nk, kh2he, nk * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(d + 2 * nk, kcia5, n5 * 4, cudaMemcpyHostToDevice));
+    c->para_tk.assign(temps, temps + RTB_CIA_NUMT);
+    c->para_fp.assign(fp, fp + ipara);
+    c->para_deltaf = fp[1] - fp[0];   // fpread_all.f:197
+    c->para_vk.resize(RTB_CIA_NUMWN);
+    for (int i = 0; i < RTB_CIA_NUMWN; ++i) c->para_vk[i] = (float)i * dnu2;
+    c->ipara = ipara;
+    c->dnu2 = dnu2;
+    c->has_para = 1;
     return RTB_OK;
 }
 

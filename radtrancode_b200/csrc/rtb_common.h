@@ -45,6 +45,22 @@ struct WaveDev {
     float gradground_s;   // esurf*dB/dT(tsurf)
 };
 
+// para-H2 CIA (flagh2p = 1, nparacon_all.f / fpread_all.f): per layer the
+// table temperature bracket and the para-fraction bracket, per wavenumber the
+// table wavenumber bracket
+struct ParaLayDev {
+    int ct;               // 0-based temperature index of fpread_all's PINDEX
+    float u, dudt;
+    int j0;               // 0-based lower para-fraction entry used
+    float f;              // weight of the entry above it
+    int neg;              // fpara < 0: entry j0 = KPARA alone, no para derivative
+};
+
+struct ParaWaveDev {
+    int cv;               // 0-based wavenumber index
+    float t;
+};
+
 // per-spectrum descriptor
 struct SpecDev {
     int nlayer, ngas, npath, nwave, nv, ncont, nsw, nlmax;
@@ -71,6 +87,10 @@ struct SpecDev {
     int col_of_param[kMaxSw]; // tracked overlap column of isw[s] (-1: continuum only)
     int col_gas[kMaxCols];    // gas index of tracked column c (ngas = temperature)
     int sw_T;             // s index of the temperature column, -1 if inactive
+    int para;             // flagh2p = 1: the para-H2 CIA replaces the CIA table
+    int sw_para;          // s index of the para-H2 fraction column, -1 if inactive
+    int64_t para_off;     // ParaLayDev index of layer 0 / ParaWaveDev index of wavenumber 0
+    int64_t paraw_off;
 };
 
 struct BatchDev {
@@ -100,6 +120,15 @@ struct BatchDev {
     const float* delg;           // [ng]
     const double* g_ord;         // [ng+1], g_ord[ng] forced >= 1 (rankg.f:65-67)
     const float* kcia;           // (9,25,1501) Fortran order
+    // para-H2 CIA (spectra with flagh2p = 1)
+    int para;                    // any spectrum of the batch uses it
+    int ipara;                   // tabulated para fractions
+    float para_deltaf;           // fp(2) - fp(1)
+    const float* kh2h2;          // (ipara,25,1501) Fortran order
+    const float* kh2he;
+    const float* kcia5;          // (5,25,1501)
+    const ParaLayDev* para_lay;
+    const ParaWaveDev* para_wave;
     // per-CTA scratch slots (tau, dtau/dq of every layer of the current item)
     float* cell_scratch;
     int64_t cell_slot;             // floats per slot

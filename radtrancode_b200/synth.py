@@ -78,6 +78,46 @@ class CIATable:
     kcia: np.ndarray       # float32, Fortran (9, 25, 1501) flattened in Fortran order
 
 
+@dataclasses.dataclass
+class ParaCIATable:
+    """The para-H2 CIA table of fpread_all (rtb_set_para_cia layout)."""
+    dnu2: float
+    ipara: int
+    temps: np.ndarray      # (25,) float32
+    fp: np.ndarray         # (ipara,) float32
+    kh2h2: np.ndarray      # float32, Fortran (ipara, 25, 1501) flattened
+    kh2he: np.ndarray
+    kcia5: np.ndarray      # float32, Fortran (5, 25, 1501) flattened
+
+
+def make_para_cia(seed=0, dnu2=1.0, ipara=24) -> ParaCIATable:
+    """Smooth lognormal H2-H2 / H2-He coefficients that grow with the para-H2
+    fraction (fp = 0.25 .. 1.0 evenly, as nparacon_all.f assumes), plus
+    H2-CH4 and CH4-CH4 among the five further pairs (the N2 pairs zero)."""
+    rng = np.random.default_rng(seed)
+    temps = np.linspace(40.0, 400.0, _abi.CIA_NUMT)
+    fp = np.linspace(0.25, 1.0, ipara)
+    v = np.arange(_abi.CIA_NUMWN, dtype=np.float64) * dnu2
+    vv = np.maximum(v, 1.0)
+
+    def band(amp, v0, s, gam):
+        shape = np.exp(-0.5 * (np.log(vv / v0) / s) ** 2)
+        shape[v == 0] = 0.0
+        return amp * shape[None, :] * (temps[:, None] / 150.0) ** gam
+
+    h2 = band(2e-8, 500.0, 0.6, -0.5)
+    he = band(0.8e-8, 700.0, 0.7, -0.3)
+    tilt = 1.0 + 0.05 * rng.standard_normal()
+    kh2h2 = np.stack([h2 * (0.7 + 0.9 * f * tilt) for f in fp])          # (ipara, 25, 1501)
+    kh2he = np.stack([he * (0.9 + 0.3 * f) for f in fp])
+    k5 = np.zeros((5, _abi.CIA_NUMT, _abi.CIA_NUMWN))
+    k5[3] = band(3e-9, 900.0, 0.5, -0.4)          # CH4-CH4
+    k5[4] = band(5e-9, 650.0, 0.6, -0.2)          # H2-CH4
+    f32 = lambda a: np.asarray(a, np.float32).ravel(order="F")
+    return ParaCIATable(float(dnu2), int(ipara), temps.astype(np.float32), fp.astype(np.float32),
+                        f32(np.transpose(kh2h2, (0, 1, 2))), f32(kh2he), f32(k5))
+
+
 def make_ktables(gases, *, np_=20, nt=15, ng=20, vmin=600.0, delv=0.4, nbin=2000, seed=0,
                  p_top_bar=1e-4, p_bot_bar=10.0, t_min=70.0, t_max=200.0, sigma=2.0,
                  median=1e-22, t2=False, irregular=None) -> KTables:
@@ -197,6 +237,9 @@ class Job:
     ispace: int = 0
     tsurf: float = 0.0
     iform: int = 0
+    flagh2p: int = 0
+    hfp: np.ndarray | None = None    # (nlayer) para-H2 fractions, flagh2p = 1
+    dfp: np.ndarray | None = None    # (ld_lay, npro) F
     fwhm: float = 0.0
     conv: "Channels | None" = None   # instrument channels (None: FWHM = 0, nconv = nwave)
     # bookkeeping for the synthetic state vector (not part of the ABI)
@@ -206,7 +249,7 @@ class Job:
 
     @property
     def nparam(self) -> int:
-        return self.ngas + 1
+        return self.ngas + 1 + (1 if self.flagh2p else 0)
 
     def as_struct(self) -> _abi.RtbAtm:
         s = _abi.RtbAtm()
@@ -223,7 +266,9 @@ class Job:
         s.xmap = f(self.xmap)
         s.vwave, s.xsec_ext = f(self.vwave), None
         s.inormal, s.iray, s.itype, s.ispace = self.inormal, self.iray, self.itype, self.ispace
-        s.flagh2p, s.ilbl, s.inlte, s.iform = 0, 0, 0, self.iform
+        s.flagh2p, s.ilbl, s.inlte, s.iform = self.flagh2p, 0, 0, self.iform
+        if self.flagh2p:
+            s.hfp, s.dfp = f(self.hfp), f(self.dfp)
         s.tsurf, s.fwhm = float(self.tsurf), float(self.fwhm)
         s.nem, s.vem, s.emissivity = len(self.vem), f(self.vem), f(self.emissivity)
         if self.conv is not None:
@@ -415,6 +460,23 @@ def job_from_layers(tables: KTables, prof: Profile, lay: dict, *, iw0=0, nwave=N
                emtemp=col(lay["emtemp"], nl), dte=np.asfortranarray(lay["dte"]),
                dam=np.asfortranarray(lay["dam"]), xmap=xmap, vwave=vwave,
                vem=np.array([0.0, 1e5], np.float32), emissivity=np.array([1.0, 1.0], np.float32))
+
+
+def with_para_h2(job: Job, hfp) -> Job:
+    """The job with the para-H2 CIA (flagh2p = 1): layer para fractions hfp,
+    DFP the identity on the layers, and one more state element per layer,
+    the para fraction of that level (model 0: xmap 1), after the others."""
+    L, npro, nv0 = job.nlayer, job.npro, job.nv
+    nparam = job.ngas + 2
+    nv = nv0 + npro
+    xmap = np.zeros((nv, nparam, npro), np.float32, order="F")
+    xmap[:nv0, :job.ngas + 1, :] = job.xmap[:nv0, :job.ngas + 1, :]
+    idx = np.arange(npro)
+    xmap[nv0 + idx, job.ngas + 1, idx] = 1.0
+    dfp = np.zeros((job.ld_lay, npro), np.float32, order="F")
+    dfp[np.arange(L), np.arange(L)] = 1.0
+    return dataclasses.replace(job, nv=nv, ld_v=nv, ld_param=nparam, xmap=xmap, flagh2p=1,
+                               hfp=np.ascontiguousarray(hfp, np.float32), dfp=dfp)
 
 
 def config1(seed=1001):

@@ -4,6 +4,7 @@ Every comparison runs the CUDA kernels through the C ABI (radtrancode_b200
 Context -> libradtran_b200.so) and the oracle on the same seeded inputs.
 Tolerances: tests/helpers.py."""
 import copy
+import dataclasses
 import os
 
 import numpy as np
@@ -413,3 +414,67 @@ def test_several_tables_per_gas(ctx):
     c4, _, _ = ctx.cirsrtfg_wave(jb)
     assert np.array_equal(c4, c3)
     ctx.set_ktables(kt)
+
+
+def _para_case(nlayer=30, nwave=12):
+    kt, cia, _ = synth.config2(nwave=nwave, nlayer=nlayer, nbin=nwave)
+    para = synth.make_para_cia(7)
+    job0 = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=nlayer, seed=81, nwave=nwave)
+    rng = np.random.default_rng(3)
+    hfp = rng.uniform(0.3, 0.9, nlayer)
+    hfp[[3, 17]] = -1.0         # fpara < 0: the last tabulated fraction, no para derivative
+    hfp[5] = 1.2                # above the table: the last bracket with f = 1
+    hfp[8] = 0.1                # below it: the first bracket with f = 0
+    return kt, cia, para, synth.with_para_h2(job0, hfp)
+
+
+def test_para_h2_cia(ctx, oracle):
+    """flagh2p = 1 (cirsradg_wave.f:634-661): the para-H2 CIA of
+    nparacon_all / fpread_all replaces nciacon, and the para-H2 fraction of
+    every level is a state element (DFP).  Radiance and Jacobian within
+    tolerance of the FP64 oracle, the g-bins bit-exact with the mixed oracle;
+    the para columns vanish for the fpara < 0 layers and not elsewhere."""
+    kt, cia, para, job = _para_case()
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_para_cia(para)
+    ctx.set_debug(True)
+    try:
+        c, g, gt = ctx.cirsrtfg_wave(job)
+        perm, split = ctx.debug_bins(job)
+    finally:
+        ctx.set_debug(False)
+    cia.para = para
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+    (cm, gm, _), (operm, osplit, _) = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED, debug=True)
+    assert np.array_equal(assignment(perm, split, kt.ng), assignment(operm, osplit, kt.ng))
+    G = g.reshape(job.nv, job.nwave)
+    rows = G[job.nv - job.npro:]
+    zero = np.all(rows == 0, axis=1)
+    assert zero[3] and zero[17] and not zero[[0, 1, 5, 8, 20]].any()
+    del cia.para
+    c0, _, _ = ctx.cirsrtfg_wave(dataclasses.replace(job, flagh2p=0, ld_param=job.ngas + 1,
+                                                     xmap=np.asfortranarray(job.xmap[:, :job.ngas + 1, :]),
+                                                     nv=job.nv, ld_v=job.nv))
+    assert not np.array_equal(c0, c)
+
+
+def test_para_h2_table_file(ctx, tmp_path):
+    """The para-H2 table read from the unformatted file fpread_all reads
+    (five framed records) gives the in-memory table's run bit for bit."""
+    kt, cia, para, job = _para_case(nlayer=20, nwave=6)
+    path = tmp_path / "para.tab"
+    with open(path, "wb") as fh:
+        for rec in (para.temps, para.fp, para.kh2h2, para.kh2he, para.kcia5):
+            b = np.asarray(rec, np.float32).tobytes()
+            n = np.array([len(b)], np.int32).tobytes()
+            fh.write(n + b + n)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_para_cia(para)
+    a = ctx.cirsrtfg_wave(job)
+    ctx.load_para_cia(str(path), para.dnu2, para.ipara)
+    b = ctx.cirsrtfg_wave(job)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))

@@ -270,3 +270,29 @@ def test_real_cia_table_isotest(oracle):
     c0, _, _ = oracle.cirsrtfg_wave(kt, None, job, oracle.ORC_FP64)
     assert np.all(np.isfinite(c)) and np.all(c > 0)
     assert np.any(c != c0)     # the H2-H2/H2-He continuum changes the spectrum
+
+
+def test_para_h2_jacobian_by_finite_differences(oracle):
+    """The FP64 oracle's para-H2 fraction derivative (nparacon_all.f DH2DFP,
+    DHEDFP through DFP and xmap) against central differences of its own
+    radiance in the layer's para fraction; the coefficients are linear in the
+    fraction within a bracket, so the two agree closely away from the
+    bracket edges."""
+    kt, cia, _ = synth.config2(nwave=4, nlayer=20, nbin=4)
+    cia.para = synth.make_para_cia(7)
+    job0 = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=20, seed=82, nwave=4)
+    fp = cia.para.fp
+    mid = 0.5 * (fp[4:15] + fp[5:16])                    # bracket centres
+    hfp = np.resize(mid, 20).astype(np.float32)
+    job = synth.with_para_h2(job0, hfp)
+    c, g, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    G = g.reshape(job.nv, job.nwave)
+    h = 1e-3
+    for lay in (2, 9, 15):
+        jp = synth.with_para_h2(job0, hfp + h * (np.arange(20) == lay))
+        jm = synth.with_para_h2(job0, hfp - h * (np.arange(20) == lay))
+        cp, _, _ = oracle.cirsrtfg_wave(kt, cia, jp, oracle.ORC_FP64)
+        cm, _, _ = oracle.cirsrtfg_wave(kt, cia, jm, oracle.ORC_FP64)
+        fd = (cp - cm) / (2 * h)
+        an = G[job.nv - job.npro + lay]
+        assert np.max(np.abs(fd - an)) <= 2e-3 * np.max(np.abs(an)) + 1e-30, lay

@@ -133,6 +133,15 @@ int rtb_set_cia(rtb_context* ctx, float dnu, const double* temps, const float* k
  *   kcia5          REAL (5, 25, 1501): H2-N2, N2-CH4, N2-N2, CH4-CH4, H2-CH4
  * rtb_load_para_cia reads the same from the unformatted sequential file
  * fpread_all.f:45-97 reads (records: temps, fp, kh2h2, kh2he, kcia5). */
+/* Load the exponential-integral table of e3interp (radtran/radtran/
+ * e3interp.f:1-79; the e3tab.dat file it reads): n = 1001 transmissions
+ * 0, 0.001, .., 1 and E3 at each (DOUBLE).  Needed by IMOD 18 paths
+ * (hemispherically integrated emission, cirsradg_wave.f:1116-1225).
+ * rtb_load_e3_table reads the text file (n, a header line, then n lines
+ * tau tran e3). */
+int rtb_set_e3_table(rtb_context* ctx, int n, const double* tran, const double* e3);
+int rtb_load_e3_table(rtb_context* ctx, const char* path);
+
 int rtb_set_para_cia(rtb_context* ctx, float dnu2, int ipara, const float* temps, const float* fp,
                      const float* kh2h2, const float* kh2he, const float* kcia5);
 int rtb_load_para_cia(rtb_context* ctx, const char* path, float dnu2, int ipara);
@@ -232,6 +241,10 @@ typedef struct rtb_atm {
      * para-H2 fraction of every layer (HFP, /LAYCOM/); its gradient
      * parameter is the last, ngas + 1 + ncont, mapped to levels by dfp */
     const float* hfp;      /* (nlayer) */
+    /* iform = 3 (total spectral flux of the planet, x 1e-18): the planet's
+     * radius RADIUS1 and the height added above it, radextra, in km
+     * (cirsradg_wave.f:913-929, 1136-1152) */
+    float radius1, radextra;
 } rtb_atm;
 
 /* Outputs, convolved by cirsconv with atm->fwhm onto the channels of

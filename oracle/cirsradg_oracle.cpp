@@ -642,6 +642,29 @@ void ciaread(const orc_tables& t, R vv, R temp, R* alpha, R* dalpha) {
     }
 }
 
+/* E3INTERP: radtran/radtran/e3interp.f:14-75 on the table held in t (1001
+ * points; egrad formed as the reference forms it at its read) */
+void e3interp(const orc_tables& t, double xtrans, double& e3out, double& de3out) {
+    const int mtab = 1001;
+    const double dtrans = 1.0f / (float)(mtab - 1);
+    auto egrad = [&](int i) {   /* 1-based */
+        if (i == 1) return (t.e3_e3[1] - t.e3_e3[0]) / dtrans;
+        if (i == mtab) return (t.e3_e3[mtab - 1] - t.e3_e3[mtab - 2]) / dtrans;
+        return 0.5 * (t.e3_e3[i] - t.e3_e3[i - 2]) / dtrans;
+    };
+    if (xtrans < 0 || std::isnan(xtrans)) {
+        e3out = 0.;
+        de3out = 0.;
+        return;
+    }
+    int j = 1 + (int)(xtrans / dtrans);
+    if (j >= mtab) j = mtab - 1;
+    double f = (xtrans - t.e3_tran[j - 1]) / dtrans;
+    if (f > 1.0) f = 1.0;
+    e3out = (1.0 - f) * t.e3_e3[j - 1] + f * t.e3_e3[j];
+    de3out = (1.0 - f) * egrad(j) + f * egrad(j + 1);
+}
+
 /* FPREAD_ALL: radtran/radtran/fpread_all.f:160-266, the table held in t:
  * every para fraction's H2-H2 and H2-He coefficient and d/dT, and the five
  * further pairs, at (vv, temp).  Returns false outside the wavenumber range,
@@ -978,7 +1001,7 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
     if ((a.flagh2p == 1 && (!t.has_para || !a.hfp)) || (a.flagh2p != 0 && a.flagh2p != 1) || a.ilbl != 0 ||
         a.inlte != 0 || a.fwhm != 0.0f)
         return RTB_ERR_UNSUPPORTED;
-    if (!(a.iform == 0 || a.iform == 2)) return RTB_ERR_UNSUPPORTED;
+    if (!(a.iform == 0 || a.iform == 2 || a.iform == 3)) return RTB_ERR_UNSUPPORTED;
     if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
     for (int k = 0; k < a.ngas; ++k) {
         if (a.idgas[k] == 91 || a.idgas[k] == 48 || a.idgas[k] == 80) return RTB_ERR_UNSUPPORTED;
@@ -986,7 +1009,8 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
     }
     for (int ip = 0; ip < a.npath; ++ip) {
         const int m = a.imod[ip];
-        if (!(m == 0 || m == 1 || m == 3)) return RTB_ERR_UNSUPPORTED;
+        if (!(m == 0 || m == 1 || m == 3 || m == 18)) return RTB_ERR_UNSUPPORTED;
+        if (m == 18 && (!t.e3_tran || !t.e3_e3 || a.tsurf < 0.0f)) return RTB_ERR_UNSUPPORTED;
         if (a.nlayin[ip] > d.ld_lay || a.nlayin[ip] > 2 * RTB_MAXPAT) return RTB_ERR_LIMIT;
         if (a.nlayin[ip] < (m == 3 ? 2 : 1)) return RTB_ERR_UNSUPPORTED;
         for (int j = 0; j < a.nlayin[ip]; ++j) {
@@ -1207,6 +1231,61 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                             DC(ip, ig, j, k) = tmp * ((R)1 - cork) * dtaudq[(size_t)j * nparam + k];
                         }
                 }
+            } else if (im == 18) {  /* hemispherically integrated emission: :1116-1225 */
+                const R PI = (R)3.1415927f;
+                R xfac = 1;
+                if (a.iform == 3) {
+                    const R rr = ((R)a.radius1 + (R)a.radextra) * (R)1e5f;
+                    xfac = xfac * (R)4. * PI * (rr * rr);
+                    xfac = xfac * (R)1e-18f;
+                }
+                double trold = 1., e3old = 0.5;
+                std::vector<R> de3olddq((size_t)nlays * nparam, 0), de3dq((size_t)nlays * nparam, 0);
+                for (int j = 0; j < nlays; ++j)
+                    for (int k = 0; k < nparam; ++k) {
+                        dtolddq[(size_t)j * nparam + k] = 0;
+                        dtrdq[(size_t)j * nparam + k] = 0;
+                    }
+                const R bsurf = a.tsurf > 0.0f ? planck_wave<R>(a.ispace, (R)vwave, (R)a.tsurf) : (R)0;
+                const R gsurf = a.tsurf > 0.0f ? planckg_wave<R>(a.ispace, (R)vwave, (R)a.tsurf) : (R)0;
+                for (int j = 0; j < nlays; ++j) {
+                    if (ig == 0) {
+                        const R Tn = (R)a.emtemp[j + (size_t)d.ld_lay * ip];
+                        W.bb[(size_t)ip * nlmax + j] = planck_wave<R>(a.ispace, (R)vwave, Tn);
+                        W.dbdt[(size_t)ip * nlmax + j] = planckg_wave<R>(a.ispace, (R)vwave, Tn);
+                    }
+                    const R bbj = W.bb[(size_t)ip * nlmax + j];
+                    const double tlayer = std::exp(-(double)taus[j]);
+                    const double tr = trold * tlayer;
+                    double e3new, e3grad;
+                    e3interp(t, tr, e3new, e3grad);
+                    cork = cork + xfac * (R)2.0 * PI * (R)(e3old - e3new) * bbj;
+                    for (int k1 = 0; k1 < nsw; ++k1) {
+                        const int k = isw[k1];
+                        for (int j1 = 0; j1 <= j; ++j1) {
+                            R& dtr = dtrdq[(size_t)j1 * nparam + k];
+                            if (j1 < j) dtr = dtolddq[(size_t)j1 * nparam + k] * (R)tlayer;
+                            else dtr = -dtaudq[(size_t)j1 * nparam + k] * (R)tr;
+                            de3dq[(size_t)j1 * nparam + k] = (R)e3grad * dtr;
+                            DC(ip, ig, j1, k) = DC(ip, ig, j1, k) + bbj * xfac * (R)2.0 * PI *
+                                                (de3olddq[(size_t)j1 * nparam + k] - de3dq[(size_t)j1 * nparam + k]);
+                        }
+                        if (k == ngas)
+                            DC(ip, ig, j, k) = DC(ip, ig, j, k) + xfac * (R)2.0 * PI * (R)(e3old - e3new) *
+                                                                      W.dbdt[(size_t)ip * nlmax + j];
+                    }
+                    e3old = e3new;
+                    trold = tr;
+                    for (int j1 = 0; j1 <= j; ++j1)
+                        for (int k1 = 0; k1 < nsw; ++k1) {
+                            const int k = isw[k1];
+                            dtolddq[(size_t)j1 * nparam + k] = dtrdq[(size_t)j1 * nparam + k];
+                            de3olddq[(size_t)j1 * nparam + k] = de3dq[(size_t)j1 * nparam + k];
+                        }
+                }
+                /* the surface, without its derivative (:1196-1205) */
+                cork = cork + xfac * (R)2.0 * PI * (R)e3old * ((R)esurf * bsurf);
+                W.tempgtsurf[(size_t)ip * ng + ig] = xfac * (R)2.0 * PI * (R)e3old * (R)esurf * gsurf;
             } else {  /* IMOD = 3: :896-1035 */
                 double trold = 1., taud = 0.0;
                 for (int j = 0; j < nlays; ++j)
@@ -1214,7 +1293,13 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                         dtolddq[(size_t)j * nparam + k] = 0;
                         dtrdq[(size_t)j * nparam + k] = 0;
                     }
-                const R xfac = 1.;
+                R xfac = 1.;
+                if (a.iform == 3) {   /* :913-929: the total flux of the planet, x 1e-18 */
+                    const R PI = (R)3.1415927f;
+                    const R rr = ((R)a.radius1 + (R)a.radextra) * (R)1e5f;
+                    xfac = xfac * PI * (R)4. * PI * (rr * rr);
+                    xfac = xfac * (R)1e-18f;
+                }
                 for (int j = 0; j < nlays; ++j) {
                     if (ig == 0) {
                         const R Tn = (R)a.emtemp[j + (size_t)d.ld_lay * ip];

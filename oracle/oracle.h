@@ -59,6 +59,9 @@ typedef struct orc_tables {
     const float* kh2h2;
     const float* kh2he;
     const float* kcia5;
+    /* e3interp's table (IMOD 18): 1001 transmissions and E3; NULL -> none */
+    const double* e3_tran;
+    const double* e3_e3;
 } orc_tables;
 
 /* Debug capture of the g-bin assignment (mixed mode), one record per

@@ -32,6 +32,7 @@ class OrcTables(C.Structure):
         ("has_para", C.c_int), ("ipara", C.c_int), ("dnu2", C.c_float),
         ("para_temps", C.POINTER(C.c_float)), ("para_fp", C.POINTER(C.c_float)),
         ("kh2h2", C.POINTER(C.c_float)), ("kh2he", C.POINTER(C.c_float)), ("kcia5", C.POINTER(C.c_float)),
+        ("e3_tran", C.POINTER(C.c_double)), ("e3_e3", C.POINTER(C.c_double)),
     ]
 
 
@@ -70,8 +71,10 @@ def lib():
     return _lib
 
 
-def tables_struct(kt, cia=None, para=None):
+def tables_struct(kt, cia=None, para=None, e3=None):
     t = OrcTables()
+    if e3 is not None:
+        t.e3_tran, t.e3_e3 = _abi.dptr(e3.tran), _abi.dptr(e3.e3)
     if para is None and cia is not None:
         para = getattr(cia, "para", None)
     if para is not None:
@@ -88,15 +91,16 @@ def tables_struct(kt, cia=None, para=None):
         t.has_cia, t.dnu = 1, cia.dnu
         t.cia_temps = _abi.dptr(cia.temps)
         t.kcia = _abi.fptr(cia.kcia)
-    t._keep = (kt, cia, para)
+    t._keep = (kt, cia, para, e3)
     return t
 
 
-def cirsrtfg_wave(kt, cia, job, precision=ORC_MIXED, debug=False, nthreads=1):
+def cirsrtfg_wave(kt, cia, job, precision=ORC_MIXED, debug=False, nthreads=1, e3=None):
     """Run the oracle forward model.  Returns (calcout, gradients, gradtsurf)
-    as float64 arrays, plus (perm, split) debug arrays when requested."""
+    as float64 arrays, plus (perm, split) debug arrays when requested.  e3 is
+    e3interp's table (a synth.E3Table), needed by IMOD 18 paths."""
     L = lib()
-    t = tables_struct(kt, cia)
+    t = tables_struct(kt, cia, e3=e3)
     s = job.as_struct()
     n1, n2, n3 = job.out_shapes()
     out = np.zeros(n1), np.zeros(n2), np.zeros(n3)

@@ -57,6 +57,7 @@ class RtbAtm(C.Structure):
         ("nem", C.c_int), ("vem", _fp), ("emissivity", _fp),
         ("conv", C.POINTER(RtbConv)),
         ("hfp", _fp),
+        ("radius1", C.c_float), ("radextra", C.c_float),
     ]
 
 

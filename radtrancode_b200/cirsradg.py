@@ -151,6 +151,15 @@ class Context:
         """fpread_all equivalent from the table file."""
         self._check(self._L.rtb_load_para_cia(self._h, os.fsencode(path), float(dnu2), int(ipara)))
 
+    def set_e3_table(self, e3):
+        """e3interp's one-time table read (a synth.E3Table: 1001 transmissions
+        and E3 values), needed by IMOD 18 paths."""
+        self._check(self._L.rtb_set_e3_table(self._h, len(e3.tran), _abi.dptr(e3.tran), _abi.dptr(e3.e3)))
+
+    def load_e3_table(self, path):
+        """e3interp's read of the e3tab.dat text file."""
+        self._check(self._L.rtb_load_e3_table(self._h, os.fsencode(path)))
+
     def set_cia(self, cia):
         """ciaread's one-time table read."""
         self._check(self._L.rtb_set_cia(self._h, float(cia.dnu), _abi.dptr(cia.temps), _abi.fptr(cia.kcia)))

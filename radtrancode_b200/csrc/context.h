@@ -74,6 +74,8 @@ struct Staging {
     bool any_noncoinc = false;
     bool any_w1 = false;
     bool any_para = false;
+    bool any_ext = false;        // an IMOD 18 path or iform = 3
+
     std::vector<float> xsec, cont;
     std::vector<int> p_layinc;
     std::vector<float> p_scale, p_emtemp;
@@ -149,6 +151,8 @@ struct rtb_context {
     float dnu2 = 0.0f, para_deltaf = 0.0f;
     std::vector<float> para_tk, para_fp, para_vk;
     rtb::DevBuf d_kpara;                     // kh2h2 | kh2he | kcia5
+    int has_e3 = 0;
+    rtb::DevBuf d_e3;                        // tabtran | tabe3 | egrad (e3interp)
     std::vector<float> cia_tk;               // sngl(temps)
     rtb::DevBuf d_kcia;
     // per-call arena

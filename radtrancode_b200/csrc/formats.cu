@@ -261,6 +261,31 @@ int rtb_load_para_cia(rtb_context* c, const char* path, float dnu2, int ipara) {
     return rtb_set_para_cia(c, dnu2, ipara, temps.data(), fp.data(), kh2h2.data(), kh2he.data(), k5.data());
 }
 
+// e3tab.dat (e3interp.f:22-32): N, a header line, then N records TAU TRAN E3
+int rtb_load_e3_table(rtb_context* c, const char* path) {
+    if (!c) return RTB_ERR_ARG;
+    File fl(path);
+    if (!fl.f) return fail(c, RTB_ERR_ARG, "cannot open %s", path ? path : "(null)");
+    std::vector<std::string> t;
+    int n = 0;
+    if (!list_read(fl.f, 1, t) || !to_int(t[0], n) || n <= 0 || n > 100000)
+        return fail(c, RTB_ERR_ARG, "%s: no point count", path);
+    char line[4096];
+    if (!std::fgets(line, sizeof line, fl.f)) return fail(c, RTB_ERR_ARG, "%s: no header line", path);
+    std::vector<double> tran(n), e3(n);
+    for (int i = 0; i < n; ++i) {
+        if (!list_read(fl.f, 3, t)) return fail(c, RTB_ERR_ARG, "%s: short table", path);
+        for (std::string& x : t)
+            for (char& ch : x)
+                if (ch == 'd' || ch == 'D') ch = 'e';
+        char *e1 = nullptr, *e2 = nullptr;
+        tran[i] = std::strtod(t[1].c_str(), &e1);
+        e3[i] = std::strtod(t[2].c_str(), &e2);
+        if (*e1 || *e2) return fail(c, RTB_ERR_ARG, "%s: record %d is not TAU TRAN E3", path, i + 1);
+    }
+    return rtb_set_e3_table(c, n, tran.data(), e3.data());
+}
+
 // .fwh (cirsrtfg_wave.f:191-196): NFWHM, then NFWHM records VFWHM XFWHM
 int rtb_read_fwh(const char* path, int* n, float* v, float* x, int cap) {
     File fl(path);

@@ -335,6 +335,76 @@ __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, co
     if (dk != dk) dk = 1e-37f;
 }
 
+// E3INTERP (radtran/radtran/e3interp.f:42-75) on the table tabtran | tabe3 |
+// egrad (1001 points each): E3 and dE3/dtrans of a transmission, DOUBLE
+__device__ __forceinline__ void e3interp_dev(const double* tab, double x, double& e3, double& de3) {
+    constexpr int mtab = 1001;
+    if (x < 0.0 || x != x) {
+        e3 = 0.0;
+        de3 = 0.0;
+        return;
+    }
+    const double dtrans = (double)(1.0f / 1000.0f);
+    int j = 1 + (int)(x / dtrans);
+    if (j >= mtab) j = mtab - 1;
+    double f = (x - tab[j - 1]) / dtrans;
+    if (f > 1.0) f = 1.0;
+    const double* te3 = tab + mtab;
+    const double* eg = tab + 2 * mtab;
+    e3 = __dadd_rn(__dmul_rn(1.0 - f, te3[j - 1]), __dmul_rn(f, te3[j]));
+    de3 = __dadd_rn(__dmul_rn(1.0 - f, eg[j - 1]), __dmul_rn(f, eg[j]));
+}
+
+// iform = 3 on an IMOD 3 path (cirsradg_wave.f:913-929): the total flux of the
+// planet, every term of lane g's radiance and derivatives times x.  Out of
+// line, as is path_imod18: the common paths' code stays as compact as it was.
+__device__ __noinline__ void scale_path(float x, int nlays, int ng, int g, float* drdt, float* trd, float* rad,
+                                        float* gts) {
+    rad[g] *= x;
+    gts[g] *= x;
+    for (int j = 0; j < nlays; ++j) {
+        drdt[j * ng + g] *= x;
+        trd[j * ng + g] *= x;
+    }
+}
+
+// IMOD 18, hemispherically integrated emission (cirsradg_wave.f:1116-1225), on
+// g-ordinate g of one path:
+// R = c sum_j B_j (E3(T_{j-1}) - E3(T_j)) + c E3(T_N) e_s B_s with the vertical
+// transmissions T_j in DOUBLE and E3 from e3interp's table, c = 2 pi xfac;
+// dR/dtau_j = c (B_j G_j + sum_{m>j} B_m (G_m - G_{m-1})), G_m = E3'(T_m) T_m
+// (the reference leaves the surface term out of the derivative).  drdt
+// receives dR/dtau_j, trd the factor of dB/dT in the temperature column.
+__device__ __noinline__ void path_imod18(const double* e3tab, float xfac18, int nlays, int ng, int g,
+                                         const int* layinc, const float* scale, const float* tau_s,
+                                         const float* bb, float radground_s, float gradground_s, float* drdt,
+                                         float* trd, float* rad, float* gts) {
+    const float c = __fmul_rn(__fmul_rn(xfac18, 2.0f), 3.1415927f);
+    double tr = 1.0, e3o = 0.5;
+    float R = 0.0f;
+    for (int j = 0; j < nlays; ++j) {
+        const float tau = tau_s[layinc[j] * ng + g] * scale[j];
+        tr = tr * exp(-(double)tau);
+        double e3n, e3g;
+        e3interp_dev(e3tab, tr, e3n, e3g);
+        const float d = __double2float_rn(e3o - e3n);
+        R = __fadd_rn(R, __fmul_rn(__fmul_rn(c, d), bb[j]));
+        trd[j * ng + g] = __fmul_rn(c, d);
+        drdt[j * ng + g] = __double2float_rn(e3g) * __double2float_rn(tr);   // G_j
+        e3o = e3n;
+    }
+    const float e3l = __double2float_rn(e3o);
+    R = __fadd_rn(R, __fmul_rn(__fmul_rn(c, e3l), radground_s));
+    float Ssum = 0.0f;
+    for (int j = nlays - 1; j >= 0; --j) {
+        const float Gj = drdt[j * ng + g];
+        drdt[j * ng + g] = c * fmaf(bb[j], Gj, Ssum);
+        if (j > 0) Ssum = fmaf(bb[j], Gj - drdt[(j - 1) * ng + g], Ssum);
+    }
+    rad[g] = R;
+    gts[g] = __fmul_rn(__fmul_rn(c, e3l), gradground_s);
+}
+
 // bilinear (wavenumber, temperature) value of one CIA table entry and its
 // d/dT (ciaread.f:178-196, fpread_all.f:220-266): REAL, in the reference's
 // order; the four corners are at b + stride * (ct + 25 cv) and neighbours
@@ -1040,9 +1110,10 @@ __device__ __forceinline__ void planck_fp32(int ispace, float vwave, float T, fl
 
 // ---------------------------------------------------------------------------
 // t2: the run's k-tables carry one temperature grid per pressure (NT < 0);
-// para: some spectrum takes the para-H2 CIA (flagh2p = 1).  Template
-// arguments, so that the usual kernel carries no trace of either
-template <bool t2, bool para>
+// ext: some spectrum takes the para-H2 CIA (flagh2p = 1), an IMOD 18 path or
+// iform = 3.  Template arguments, so that the usual kernel carries no trace
+// of either
+template <bool t2, bool ext>
 __global__ void __launch_bounds__(kThreads, 5)
 fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) {
     extern __shared__ __align__(16) char smem[];
@@ -1141,7 +1212,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
             const int64_t il_glob = S.lay_off + l;
             const LayerDev L = B.lay[il_glob];
             float dtc[kMaxSw];
-            const float taucon = continuum<para>(B, S, L, W, iw_glob, il_glob, lane, dtc);
+            const float taucon = continuum<ext>(B, S, L, W, iw_glob, il_glob, lane, dtc);
             const float* amo = B.amo + S.lg_off + (int64_t)l * S.ngas;
             const int64_t* slices = B.wg_slice + S.wg_off + (int64_t)iw * S.ngas;
             const float* w2s = B.wg_w2 ? B.wg_w2 + S.wg_off + (int64_t)iw * S.ngas : nullptr;
@@ -1276,7 +1347,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
             const int* layinc = B.p_layinc + S.path_off + (int64_t)p * S.nlmax;
             const float* scale = B.p_scale + S.path_off + (int64_t)p * S.nlmax;
             const float* emt = B.p_emtemp + S.path_off + (int64_t)p * S.nlmax;
-            if (im == 3) {
+            if (im == 3 || (ext && im == 18)) {
                 for (int j = lane; j < nlays; j += 32) planck_fp32(S.ispace, W.vwave, emt[j], bb[j], dbdt[j]);
             }
             __syncwarp();
@@ -1309,6 +1380,10 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                     }
                     rad[g] = R;
                     gts[g] = gt;
+                    if (ext && S.xfac3 != 1.0f) scale_path(S.xfac3, nlays, ng, g, drdt, trd, rad, gts);   // iform 3
+                } else if (ext && im == 18) {
+                    path_imod18(B.e3tab, S.xfac18, nlays, ng, g, layinc, scale, tau_s, bb, W.radground_s,
+                                W.gradground_s, drdt, trd, rad, gts);
                 } else {
                     float tsum = 0.0f;
                     for (int j = 0; j < nlays; ++j) tsum = tsum + tau_s[layinc[j] * ng + g] * scale[j];
@@ -1338,7 +1413,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
             const int nlays = S.nlayin[p];
             const int* layinc = B.p_layinc + S.path_off + (int64_t)p * S.nlmax;
             const float* scale = B.p_scale + S.path_off + (int64_t)p * S.nlmax;
-            const bool em = S.imod[p] == 3;
+            const bool em = S.imod[p] == 3 || (ext && S.imod[p] == 18);
             for (int t = tid; t < nlays * nsw; t += kThreads) {
                 const int j = t / nsw, s = t - (t / nsw) * nsw;
                 const int l = layinc[j];
@@ -1418,7 +1493,7 @@ int fwd_blocks_per_sm(int smem) {
 
 cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st) {
     const int smem = fwd_smem_bytes(B.ng, nsw, ncol, nlmax, npath);
-    auto kern = B.para ? (B.t2 ? fwd_kernel<true, true> : fwd_kernel<false, true>)
+    auto kern = B.ext ? (B.t2 ? fwd_kernel<true, true> : fwd_kernel<false, true>)
                        : (B.t2 ? fwd_kernel<true, false> : fwd_kernel<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;

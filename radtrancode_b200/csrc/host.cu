@@ -200,7 +200,8 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         return fail(c, RTB_ERR_ARG, "flagh2p=1 needs the para-H2 CIA table (rtb_set_para_cia) and hfp");
     if (a.ilbl != 0) return fail(c, RTB_ERR_UNSUPPORTED, "ILBL != 0 (line-by-line tables) not implemented");
     if (a.inlte != 0) return fail(c, RTB_ERR_UNSUPPORTED, "non-LTE emission temperatures not implemented");
-    if (!(a.iform == 0 || a.iform == 2)) return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d not implemented", a.iform);
+    if (!(a.iform == 0 || a.iform == 2 || a.iform == 3))
+        return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d (a stellar spectrum) not implemented", a.iform);
     if (a.iray > 1) return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (only Jovian Rayleigh, iray=1)", a.iray);
     if (a.npath > 4) return fail(c, RTB_ERR_UNSUPPORTED, "more than 4 paths per spectrum");
     if (a.ncont > 0 && (!a.cont || !a.xsec_ext || !a.dco)) return fail(c, RTB_ERR_ARG, "dust arrays missing");
@@ -219,7 +220,10 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     int nlmax = 0;
     for (int ip = 0; ip < a.npath; ++ip) {
         const int m = a.imod[ip];
-        if (!(m == 0 || m == 1 || m == 3)) return fail(c, RTB_ERR_UNSUPPORTED, "IMOD=%d not implemented", m);
+        if (!(m == 0 || m == 1 || m == 3 || m == 18))
+            return fail(c, RTB_ERR_UNSUPPORTED, "IMOD=%d not implemented", m);
+        if (m == 18 && !c->has_e3) return fail(c, RTB_ERR_ARG, "IMOD 18 needs the E3 table (rtb_set_e3_table)");
+        if (m == 18 && a.tsurf < 0.0f) return fail(c, RTB_ERR_UNSUPPORTED, "IMOD 18 with TSURF < 0");
         const int nl = a.nlayin[ip];
         if (nl > d.ld_lay || nl > 2 * RTB_MAXPAT) return fail(c, RTB_ERR_LIMIT, "nlayin exceeds maxinc");
         if (nl < (m == 3 ? 2 : 1)) return fail(c, RTB_ERR_UNSUPPORTED, "path with %d layers", nl);
@@ -265,6 +269,18 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     S.iray = (a.iray > 0 && a.itype != 0) ? 1 : 0;
     S.has_cia = c->has_cia;
     S.tsurf_pos = a.tsurf > 0.0f ? 1 : 0;
+    // iform 3: total spectral flux of the planet, x 1e-18 (cirsradg_wave.f:913-929, 1136-1152)
+    S.xfac3 = 1.0f;
+    S.xfac18 = 1.0f;
+    if (a.iform == 3) {
+        const float PI = 3.1415927f;   // constdef.f:11
+        const float r = (a.radius1 + a.radextra) * 1e5f;
+        S.xfac3 = 1.0f * PI * 4.0f * PI * (r * r) * 1e-18f;
+        S.xfac18 = 1.0f * 4.0f * PI * (r * r) * 1e-18f;
+        st.any_ext = true;
+    }
+    for (int ip = 0; ip < a.npath; ++ip)
+        if (a.imod[ip] == 18) st.any_ext = true;
     for (int s = 0; s < kMaxSw; ++s) { S.isw[s] = -1; S.col_of_param[s] = -1; }
     for (int cc = 0; cc < kMaxCols; ++cc) S.col_gas[cc] = -1;
     int ncol = 0;
@@ -772,6 +788,7 @@ void append_staging(Staging& dst, const Staging& src) {
     dst.any_noncoinc = dst.any_noncoinc || src.any_noncoinc;
     dst.any_w1 = dst.any_w1 || src.any_w1;
     dst.any_para = dst.any_para || src.any_para;
+    dst.any_ext = dst.any_ext || src.any_ext;
     dst.n_out += src.n_out;
     dst.n_jac += src.n_jac;
 }
@@ -943,7 +960,9 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     B.delg = (const float*)c->d_delg.p;
     B.g_ord = (const double*)c->d_gord.p;
     B.kcia = (const float*)c->d_kcia.p;
+    B.e3tab = c->has_e3 ? (const double*)c->d_e3.p : nullptr;
     B.para = st.any_para ? 1 : 0;
+    B.ext = (st.any_para || st.any_ext) ? 1 : 0;
     if (st.any_para) {
         const size_t nk = (size_t)c->ipara * RTB_CIA_NUMT * RTB_CIA_NUMWN;
         B.ipara = c->ipara;
@@ -1291,6 +1310,7 @@ void rtb_destroy(rtb_context* c) {
     c->d_convout.release();
     c->d_layer.release();
     c->d_kpara.release();
+    c->d_e3.release();
     c->d_nt32.release();
     c->d_nt64.release();
     c->d_ntsmall.release();
@@ -1412,6 +1432,28 @@ int rtb_set_cia(rtb_context* c, float dnu, const double* temps, const float* kci
     CUDA_TRY(c, c->d_kcia.ensure(n * 4));
     CUDA_TRY(c, cudaMemcpy(c->d_kcia.p, kcia, n * 4, cudaMemcpyHostToDevice));
     c->has_cia = 1;
+    return RTB_OK;
+}
+
+int rtb_set_e3_table(rtb_context* c, int n, const double* tran, const double* e3) {
+    if (!c) return RTB_ERR_ARG;
+    constexpr int kMtab = 1001;   // e3interp.f: PARAMETER (mtab=1001)
+    if (n != kMtab || !tran || !e3) return fail(c, RTB_ERR_ARG, "E3 table: %d points (e3interp.f holds 1001)", n);
+    if (tran[kMtab - 1] != 1.0) return fail(c, RTB_ERR_ARG, "E3 table: the last transmission must be 1");
+    std::vector<double> t(3 * kMtab);
+    const double dtrans = (double)(1.0f / (float)(kMtab - 1));   // REAL 1.0/float(mtab-1) into DOUBLE
+    for (int i = 0; i < kMtab; ++i) {
+        t[i] = tran[i];
+        t[kMtab + i] = e3[i];
+    }
+    double* eg = t.data() + 2 * kMtab;   // egrad (e3interp.f:36-40)
+    eg[0] = (e3[1] - e3[0]) / dtrans;
+    eg[kMtab - 1] = (e3[kMtab - 1] - e3[kMtab - 2]) / dtrans;
+    for (int i = 1; i < kMtab - 1; ++i) eg[i] = 0.5 * (e3[i + 1] - e3[i - 1]) / dtrans;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    CUDA_TRY(c, c->d_e3.ensure(t.size() * 8));
+    CUDA_TRY(c, cudaMemcpy(c->d_e3.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
+    c->has_e3 = 1;
     return RTB_OK;
 }
 

@@ -66,6 +66,7 @@ struct SpecDev {
     int nlayer, ngas, npath, nwave, nv, ncont, nsw, nlmax;
     int ncol;             // tracked overlap columns
     int tsurf_pos;        // tsurf > 0
+    float xfac3, xfac18;  // iform factor of the IMOD 3 and IMOD 18 paths (1 unless iform = 3)
     int nonlimb_mask;     // bit p: path p adds the surface term (cirsradg_wave.f:985-1000)
     int ispace;
     int inormal;
@@ -120,8 +121,11 @@ struct BatchDev {
     const float* delg;           // [ng]
     const double* g_ord;         // [ng+1], g_ord[ng] forced >= 1 (rankg.f:65-67)
     const float* kcia;           // (9,25,1501) Fortran order
+    // E3 table of e3interp (IMOD 18): tabtran | tabe3 | egrad, 1001 each
+    const double* e3tab;
     // para-H2 CIA (spectra with flagh2p = 1)
     int para;                    // any spectrum of the batch uses it
+    int ext;                     // para, an IMOD 18 path or iform = 3 somewhere in the batch
     int ipara;                   // tabulated para fractions
     float para_deltaf;           // fp(2) - fp(1)
     const float* kh2h2;          // (ipara,25,1501) Fortran order

@@ -90,6 +90,39 @@ class ParaCIATable:
     kcia5: np.ndarray      # float32, Fortran (5, 25, 1501) flattened
 
 
+@dataclasses.dataclass
+class E3Table:
+    """e3interp's table (rtb_set_e3_table layout): the third exponential
+    integral E3(tau) at the 1001 transmissions tran = i/1000, tau = -ln(tran)."""
+    tau: np.ndarray        # (1001,) float64
+    tran: np.ndarray
+    e3: np.ndarray
+
+
+def make_e3_table() -> E3Table:
+    """E3 of the e3tab.dat layout: tran(i) = REAL(i/1000), tau = -ln(tran)
+    (1e36 standing for tran = 0, where E3 = 0), E3(0) = 1/2."""
+    from scipy.special import expn
+    tran = (np.arange(1001) / 1000.0).astype(np.float32).astype(np.float64)
+    pos = tran > 0
+    tau = np.full(1001, 1e36)
+    tau[pos] = -np.log(tran[pos])
+    e3 = np.zeros(1001)
+    e3[pos] = expn(3, tau[pos])
+    e3[-1], tau[-1] = 0.5, 0.0
+    return E3Table(tau, tran, e3)
+
+
+def write_e3_table(path, e3: E3Table):
+    """The text file e3interp.f reads: the count, a header line, then one
+    TAU TRAN E3 record per line (17 significant digits: the doubles read
+    back exactly)."""
+    with open(path, "w") as fh:
+        fh.write(f"{len(e3.tran):8d}\n      tau        trans        e3\n")
+        for a, b, c in zip(e3.tau, e3.tran, e3.e3):
+            fh.write(f" {a:.16e} {b:.16e} {c:.16e}\n")
+
+
 def make_para_cia(seed=0, dnu2=1.0, ipara=24) -> ParaCIATable:
     """Smooth lognormal H2-H2 / H2-He coefficients that grow with the para-H2
     fraction (fp = 0.25 .. 1.0 evenly, as nparacon_all.f assumes), plus
@@ -241,6 +274,8 @@ class Job:
     hfp: np.ndarray | None = None    # (nlayer) para-H2 fractions, flagh2p = 1
     dfp: np.ndarray | None = None    # (ld_lay, npro) F
     fwhm: float = 0.0
+    radius1: float = 0.0             # km, planet radius (iform = 3 total flux)
+    radextra: float = 0.0            # km, correction to radius1
     conv: "Channels | None" = None   # instrument channels (None: FWHM = 0, nconv = nwave)
     # bookkeeping for the synthetic state vector (not part of the ABI)
     vmr: np.ndarray | None = None
@@ -270,6 +305,7 @@ class Job:
         if self.flagh2p:
             s.hfp, s.dfp = f(self.hfp), f(self.dfp)
         s.tsurf, s.fwhm = float(self.tsurf), float(self.fwhm)
+        s.radius1, s.radextra = float(self.radius1), float(self.radextra)
         s.nem, s.vem, s.emissivity = len(self.vem), f(self.vem), f(self.emissivity)
         if self.conv is not None:
             cs = self.conv.as_struct()

@@ -478,3 +478,70 @@ def test_para_h2_table_file(ctx, tmp_path):
     ctx.load_para_cia(str(path), para.dnu2, para.ipara)
     b = ctx.cirsrtfg_wave(job)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def _emission_case(case):
+    kt, cia, _ = synth.config2(nwave=5, nlayer=24, nbin=5)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=24, seed=23, nwave=5)
+    job.vem = np.array([500.0, 1500.0], np.float32)
+    job.emissivity = np.array([0.9, 0.7], np.float32)
+    if case.startswith("imod18"):
+        job.imod[:] = 18
+    if case in ("imod18_surface", "imod18_iform3", "imod3_iform3"):
+        job.tsurf = 175.0
+    if case.endswith("iform3"):
+        job.iform, job.radius1, job.radextra = 3, 71492.0, 40.0
+    if case == "paths_18_and_3":
+        L = job.nlayer
+        lay = np.zeros((L, 2), np.int32, order="F")
+        lay[:, 0] = lay[:, 1] = job.layinc[:L, 0]
+        sc = np.ones((L, 2), np.float32, order="F")
+        sc[:, 1] = 1.5
+        em = np.zeros((L, 2), np.float32, order="F")
+        em[:, 0] = em[:, 1] = job.emtemp[:L, 0]
+        job = dataclasses.replace(job, npath=2, layinc=lay, scale=sc, emtemp=em, nlayin=np.array([L, L], np.int32),
+                                  imod=np.array([18, 3], np.int32), tsurf=160.0)
+    return kt, cia, job
+
+
+@pytest.mark.parametrize("case", ["imod18", "imod18_surface", "imod18_iform3", "imod3_iform3", "paths_18_and_3"])
+def test_hemispherical_emission_and_total_flux(ctx, oracle, case):
+    """IMOD 18 (cirsradg_wave.f:1116-1225: the flux integrated over the
+    hemisphere through e3interp's E3 table; the Jacobian by the E3-gradient
+    recurrence, evaluated on the device as one backward sum) and iform = 3
+    (the total flux of the planet, cirsradg_wave.f:913-929 and 1136-1152):
+    radiance, Jacobian and surface-temperature gradient within tolerance of
+    the FP64 oracle."""
+    e3 = synth.make_e3_table()
+    kt, cia, job = _emission_case(case)
+    ctx.set_e3_table(e3)
+    c, g, gt = _run(ctx, kt, cia, job)
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=e3)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.npath * job.nv) <= JAC_TOL
+    if job.tsurf > 0:
+        assert np.max(np.abs(gt - gt64)) <= RAD_TOL * np.max(np.abs(gt64))
+    if case.endswith("iform3"):
+        base = dataclasses.replace(job, iform=0)
+        c0, _, _ = ctx.cirsrtfg_wave(base)
+        assert np.max(c / c0) > 100.0
+
+
+def test_e3_table_file_and_missing_table(tmp_path):
+    """The E3 table read from e3interp's text file gives the in-memory
+    table's run bit for bit; an IMOD 18 path without a table is refused."""
+    from radtrancode_b200 import cirsradg
+    e3 = synth.make_e3_table()
+    path = tmp_path / "e3tab.dat"
+    synth.write_e3_table(path, e3)
+    kt, cia, job = _emission_case("imod18_surface")
+    with cirsradg.Context(0) as c2:
+        c2.set_ktables(kt)
+        c2.set_cia(cia)
+        with pytest.raises(cirsradg.RtbError, match="E3"):
+            c2.cirsrtfg_wave(job)
+        c2.set_e3_table(e3)
+        a = c2.cirsrtfg_wave(job)
+        c2.load_e3_table(str(path))
+        b = c2.cirsrtfg_wave(job)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))

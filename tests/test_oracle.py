@@ -296,3 +296,101 @@ def test_para_h2_jacobian_by_finite_differences(oracle):
         fd = (cp - cm) / (2 * h)
         an = G[job.nv - job.npro + lay]
         assert np.max(np.abs(fd - an)) <= 2e-3 * np.max(np.abs(an)) + 1e-30, lay
+
+
+def _imod18(job, tsurf=0.0, emissivity=1.0):
+    job.imod[:] = 18
+    job.tsurf = tsurf
+    job.vem = np.array([1.0, 1e4], np.float32)
+    job.emissivity = np.array([emissivity, emissivity], np.float32)
+    return job
+
+
+def test_imod18_isothermal_hemisphere_radiates_pi_planck(oracle):
+    """IMOD 18 (cirsradg_wave.f:1116-1225): over a black surface at the
+    atmosphere's temperature the E3 differences telescope to E3(0) = 1/2, so
+    the hemispherical flux is pi B(T) whatever the optical depths; with
+    iform = 3 it is that flux times 4 pi ((radius1 + radextra) 1e5)^2 1e-18
+    (cirsradg_wave.f:1136-1152)."""
+    import dataclasses
+    e3 = synth.make_e3_table()
+    kt, cia, job = synth.config2(nwave=6, nlayer=24, nbin=6)
+    job = _imod18(_isothermal(job, 150.0), tsurf=150.0)
+    c64, _, gt = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=e3)
+    v = job.vwave.astype(np.float64)
+    c1, c2 = float(np.float32(1.1911e-12)), float(np.float32(1.439))
+    pi = float(np.float32(np.pi))
+    B = c1 * v ** 3 / np.expm1(c2 * v / 150.0) * float(np.sum(kt.delg.astype(np.float64)))
+    assert np.max(np.abs(c64 - pi * B) / B) < 1e-12
+    assert np.all(gt > 0)
+    j3 = dataclasses.replace(job, iform=3, radius1=71492.0, radextra=25.0)
+    c3, _, _ = oracle.cirsrtfg_wave(kt, cia, j3, oracle.ORC_FP64, e3=e3)
+    r = (71492.0 + 25.0) * 1e5           # the FP64 oracle forms the factor in double
+    xfac = 4.0 * pi * r * r * float(np.float32(1e-18))
+    assert np.max(np.abs(c3 / c64 - xfac)) < 1e-12 * xfac
+
+
+def test_imod18_jacobian_by_finite_differences(oracle):
+    """The FP64 oracle's IMOD 18 Jacobian (the E3-gradient recurrence of
+    cirsradg_wave.f:1176-1195) against central differences of its own
+    hemispherical flux, with no surface term (TSURF = 0).  The analytic
+    E3 gradient interpolates e3interp's central-difference table, not the
+    slope of the interpolant, hence the looser bound than the IMOD 3 check."""
+    e3 = synth.make_e3_table()
+    kt, cia, job = synth.config2(nwave=4, nlayer=20, nbin=4)
+    absorbers = synth.ABSORBERS_C2
+    base_T = job.temp.astype(np.float64).copy()
+    job = _imod18(job)
+    _, g0, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=e3)
+    G = g0.reshape(job.nv, -1)
+    L = job.nlayer
+
+    def run(T=None, xscale=None):
+        j = synth.make_job(kt, absorbers, nlayer=L, seed=1003, nwave=4, vmr_perturb=0.3,
+                           temp=base_T if T is None else T, xscale=xscale)
+        j.delh[:] = job.delh
+        return oracle.cirsrtfg_wave(kt, cia, _imod18(j), oracle.ORC_FP64, e3=e3)[0]
+
+    for lev in (0, 7, 19):
+        Tp = base_T.copy(); Tp[lev] += 2e-3
+        Tm = base_T.copy(); Tm[lev] -= 2e-3
+        h2 = float(np.float32(Tp[lev])) - float(np.float32(Tm[lev]))
+        fd = (run(T=Tp) - run(T=Tm)) / h2
+        assert np.max(np.abs(fd - G[lev])) / np.max(np.abs(G[lev])) < 5e-3, lev
+    for a in range(len(absorbers)):
+        xp = np.zeros(len(absorbers)); xp[a] = 1e-4
+        fd = (run(xscale=xp) - run(xscale=-xp)) / 2e-4
+        assert np.max(np.abs(fd - G[L + a])) / np.max(np.abs(G[L + a])) < 5e-3, a
+
+
+def test_imod18_needs_the_e3_table(oracle):
+    kt, cia, job = synth.config2(nwave=2, nlayer=10, nbin=2)
+    job = _imod18(job)
+    with pytest.raises(RuntimeError, match="UNSUPPORTED"):
+        oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+
+
+E3TAB = "/root/reference/raddata/e3tab.dat"
+
+
+@pytest.mark.skipif(not os.path.exists(E3TAB), reason="reference data not mounted")
+def test_real_e3_table(oracle):
+    """The reference's own e3tab.dat (read as e3interp.f:36-45 reads it): the
+    synthetic table the GPU tests use agrees with it to 5e-5 at transmissions
+    >= 0.1 (below that the file's entries drift from E3 by up to a few tens
+    of per cent), and the oracle's IMOD 18 run on it keeps the
+    pi B identity of a black isothermal hemisphere."""
+    lines = open(E3TAB).read().splitlines()
+    n = int(lines[0])
+    rec = np.array([[float(x) for x in ln.split()] for ln in lines[2:2 + n]])
+    real = synth.E3Table(rec[:, 0].copy(), rec[:, 1].copy(), rec[:, 2].copy())
+    syn = synth.make_e3_table()
+    assert n == 1001 and real.tran[-1] == 1.0 and real.e3[-1] == 0.5
+    assert np.max(np.abs(real.tran - syn.tran)) < 1e-9
+    ok = syn.tran >= 0.1
+    assert np.max(np.abs(real.e3[ok] - syn.e3[ok]) / syn.e3[ok]) < 5e-5
+    kt, cia, job = synth.config2(nwave=4, nlayer=20, nbin=4)
+    job = _imod18(_isothermal(job, 150.0), tsurf=150.0)
+    c_real, _, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=real)
+    c_syn, _, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=syn)
+    assert np.max(np.abs(c_real - c_syn) / c_syn) < 1e-12

@@ -565,7 +565,9 @@ typedef struct rtb_retrieval_spec {
     const rtb_atm* atm;
     int nscale;
     const int* scale_gas;     /* [nscale] 0-based gas index into atm */
-    const float* y;           /* [ny] measurement, ny = atm->nwave */
+    const float* y;           /* [ny] measurement, ny = atm->nwave; with channels
+                                 (atm->conv, any FWHM) ny = atm->conv->nconv: every
+                                 spectrum and Jacobian row is convolved onto them */
     const double* sei;        /* [ny] diagonal of Se^-1 */
     const double* sa;         /* [nx][nx] a priori covariance */
     const float* xa;          /* [nx] a priori state */

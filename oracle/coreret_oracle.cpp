@@ -21,6 +21,11 @@ namespace {
 struct Work {
     rtb_atm a{};
     int L = 0, NV = 0, nparam = 0, NW = 0;
+    /* the measurement's channels (cirsrtfg_wave.f:520-560 convolves the
+     * spectrum and every Jacobian row onto them); NY = nconv, or NW */
+    int NY = 0;
+    float fwhm = 0.0f;
+    const rtb_conv* cv = nullptr;
     std::vector<float> temp, pp, amount, emtemp, xmap, pp0, amount0, xmap0;
     std::vector<float> press, delh, scale, dte, dam, vwave;
     std::vector<int> layinc, idgas, isogas, ktab, nlayin, imod, sg, sm, pg;
@@ -159,8 +164,7 @@ int at_level_state(Work& w, const float* x) {
     return orc_layerg(&w.pr, &w.lo, &out);
 }
 
-int setup(const rtb_retrieval_spec& s, Work& w) {
-    if (s.prof) return setup_level(s, w);
+int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     const rtb_atm& t = *s.atm;
     if (t.npath != 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont != 0)
         return RTB_ERR_UNSUPPORTED;
@@ -270,6 +274,23 @@ void at_state(Work& w, const float* x) {
     }
 }
 
+int setup(const rtb_retrieval_spec& s, Work& w) {
+    const int r = s.prof ? setup_level(s, w) : setup_layers(s, w);
+    if (r) return r;
+    const rtb_atm& t = *s.atm;
+    w.NY = w.NW;
+    if (t.conv && t.conv->nconv > 0) {
+        w.fwhm = t.fwhm;
+        w.cv = t.conv;
+        w.NY = t.conv->nconv;
+    } else if (t.fwhm != 0.0f) {
+        return RTB_ERR_ARG;
+    }
+    w.a.fwhm = 0.0f;
+    w.a.conv = nullptr;
+    return w.NV < w.NY ? RTB_OK : RTB_ERR_UNSUPPORTED;
+}
+
 /* forwardavfovX stand-in: spectrum and kk (ny, nx) REAL at state x */
 int forward(const orc_tables* tab, Work& w, const float* x, int precision, int nthreads, std::vector<float>& yn,
             std::vector<float>& kk) {
@@ -286,6 +307,19 @@ int forward(const orc_tables* tab, Work& w, const float* x, int precision, int n
     kk.resize((size_t)w.NV * w.NW);
     for (int i = 0; i < w.NW; ++i) yn[i] = (float)c[i];
     for (size_t i = 0; i < g.size(); ++i) kk[i] = (float)g[i];   /* gradients(iv*ny + iw) = kk(iw, iv) */
+    if (w.cv) {   /* cirsconv of the spectrum and of each Jacobian row onto the channels */
+        const rtb_conv& v = *w.cv;
+        std::vector<float> yc(w.NY), kc((size_t)w.NV * w.NY);
+        int e = orc_cirsconv_ex(w.fwhm, w.NW, w.vwave.data(), yn.data(), v.nconv, v.vconv, v.nfwhm, v.vfwhm,
+                                v.xfwhm, v.nfil, v.vcen, v.nsub, v.vfil, v.fil, yc.data());
+        for (int iv = 0; iv < w.NV && !e; ++iv)
+            e = orc_cirsconv_ex(w.fwhm, w.NW, w.vwave.data(), kk.data() + (size_t)iv * w.NW, v.nconv, v.vconv,
+                                v.nfwhm, v.vfwhm, v.xfwhm, v.nfil, v.vcen, v.nsub, v.vfil, v.fil,
+                                kc.data() + (size_t)iv * w.NY);
+        if (e) return e;
+        yn.swap(yc);
+        kk.swap(kc);
+    }
     return RTB_OK;
 }
 
@@ -311,7 +345,7 @@ int orc_retrieve(const orc_tables* tab, const rtb_retrieval_spec* s, const rtb_r
     Work w;
     int r = setup(*s, w);
     if (r) return r;
-    const int nx = w.NV, ny = w.NW, L = w.L;
+    const int nx = w.NV, ny = w.NY, L = w.L;
     std::vector<float> xa(s->xa, s->xa + nx), xn(nx), xn1(nx), x_out(nx);
     for (int i = 0; i < nx; ++i) xn[i] = s->x0 ? s->x0[i] : s->xa[i];
     std::vector<double> sai((size_t)nx * nx), dd((size_t)nx * ny), aa((size_t)nx * nx);

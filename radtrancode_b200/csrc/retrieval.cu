@@ -57,7 +57,27 @@ struct AtmWork {
     rtb_profile pr{};
     rtb_layer_opts lo{};
     std::vector<float> ph, pp_atm, pt, pvmr0, pvmr, lbase;   // h, p, t [npro]; vmr [ngas][npro]
+    // the measurement's channels: the forward model's spectrum and Jacobian
+    // rows convolved by cirsconv onto them (cirsrtfg_wave.f:520-560)
+    ConvSpec conv;
+    bool has_conv = false;
+    int ny = 0;                 // measurement points: nconv, or nwave without channels
 };
+
+// the channels of a retrieval's atmosphere (FWHM and rtb_conv as
+// rtb_cirsrtfg_wave takes them) and the size of its measurement vector
+int work_channels(rtb_context* c, const rtb_atm& t, AtmWork& w) {
+    w.has_conv = false;
+    w.ny = t.nwave;
+    if (t.fwhm == 0.0f && !t.conv) return RTB_OK;
+    const int r = conv_check(c, t.fwhm, t.nwave, t.vwave, t.conv, w.conv);
+    if (r) return r;
+    if (!w.conv.vconv.empty()) {
+        w.has_conv = true;
+        w.ny = (int)w.conv.vconv.size();
+    }
+    return RTB_OK;
+}
 
 int build_level_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w);
 
@@ -71,14 +91,14 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     const int ldp = t.ld_param > 0 ? t.ld_param : (RTB_MAXGAS + 2 + RTB_MAXCON);
     const int nparam = G + 1 + NC;
     if (NP != 1) return fail(c, RTB_ERR_UNSUPPORTED, "retrieval atmosphere must have one path (npath=%d)", NP);
-    if (t.fwhm != 0.0f || t.conv)
-        return fail(c, RTB_ERR_UNSUPPORTED, "retrieval on convolved channels (FWHM != 0) not supported");
+    if (!t.vwave) return fail(c, RTB_ERR_ARG, "NULL input array in retrieval atmosphere");
+    if (const int r = work_channels(c, t, w)) return r;
     if (NPRO != L) return fail(c, RTB_ERR_UNSUPPORTED, "layer-state model needs npro == nlayer");
     if (s.nprof < 0 || (s.nprof > 0 && !s.prof_gas)) return fail(c, RTB_ERR_ARG, "nprof/prof_gas");
     if (NV != L + s.nscale + s.nprof * L)
         return fail(c, RTB_ERR_ARG, "nv=%d but nlayer + nscale + nprof*nlayer = %d", NV, L + s.nscale + s.nprof * L);
     if (NV > kNewtonMaxNx) return fail(c, RTB_ERR_UNSUPPORTED, "state size %d > %d", NV, kNewtonMaxNx);
-    if (NV >= NW) return fail(c, RTB_ERR_UNSUPPORTED, "nx=%d >= ny=%d (calc_gain_matrix nx<ny branch only)", NV, NW);
+    if (NV >= w.ny) return fail(c, RTB_ERR_UNSUPPORTED, "nx=%d >= ny=%d (calc_gain_matrix nx<ny branch only)", NV, w.ny);
     if (!t.press || !t.temp || !t.delh || !t.pp || !t.amount || !t.idgas || !t.isogas || !t.ktab || !t.nlayin ||
         !t.imod || !t.layinc || !t.scale || !t.emtemp || !t.dte || !t.dam || !t.xmap || !t.vwave)
         return fail(c, RTB_ERR_ARG, "NULL input array in retrieval atmosphere");
@@ -144,6 +164,8 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     w.imod.assign(t.imod, t.imod + NP);
     rtb_atm& a = w.a;
     a = t;
+    a.fwhm = 0.0f;      // the engine convolves the raw outputs itself
+    a.conv = nullptr;
     a.ld_lay = L;
     a.ld_con = NC > 0 ? NC : 1;
     a.ld_v = NV;
@@ -228,7 +250,9 @@ int build_level_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     if (NV != NPRO + s.nscale + s.nprof * NPRO)
         return fail(c, RTB_ERR_ARG, "nv=%d but npro + nscale + nprof*npro = %d", NV, NPRO + s.nscale + s.nprof * NPRO);
     if (NV > kNewtonMaxNx) return fail(c, RTB_ERR_UNSUPPORTED, "state size %d > %d", NV, kNewtonMaxNx);
-    if (NV >= NW) return fail(c, RTB_ERR_UNSUPPORTED, "nx=%d >= ny=%d (calc_gain_matrix nx<ny branch only)", NV, NW);
+    if (!t.vwave) return fail(c, RTB_ERR_ARG, "NULL input array in retrieval atmosphere");
+    if (const int r = work_channels(c, t, w)) return r;
+    if (NV >= w.ny) return fail(c, RTB_ERR_UNSUPPORTED, "nx=%d >= ny=%d (calc_gain_matrix nx<ny branch only)", NV, w.ny);
     if (o.nlay < 1 || o.nlay > RTB_MAXLAY) return fail(c, RTB_ERR_LIMIT, "layering: nlay %d", o.nlay);
     if (!t.idgas || !t.isogas || !t.ktab || !t.vwave) return fail(c, RTB_ERR_ARG, "NULL input array in retrieval atmosphere");
     for (int a = 0; a < s.nscale; ++a) {
@@ -289,6 +313,8 @@ int build_level_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     w.ktab.assign(t.ktab, t.ktab + G);
     rtb_atm& a = w.a;
     a = t;
+    a.fwhm = 0.0f;      // the engine convolves the raw outputs itself
+    a.conv = nullptr;
     a.nlayer = L;
     a.ncont = 0;
     a.npath = 1;
@@ -391,15 +417,23 @@ struct Slot {
     double t_submit = 0, t_done = 0;
     rtb_retrieval_result res{};
     AtmWork w;
+    int nraw = 0;                     // calculation points of the raw outputs when the spectrum is convolved
     // arena layout (element offsets from the block start)
     int64_t k_elems() const { return 2 * (int64_t)nx * ny; }
     int64_t y_elems() const { return 3 * al4(ny); }
 };
 
-size_t slot_bytes(int nx, int ny) {
+size_t slot_core_bytes(int nx, int ny) {
     const size_t f = (size_t)(2 * (int64_t)nx * ny + 3 * al4(ny)) * 4;
     const size_t d = (size_t)(2 * al4(ny) + 2 * (int64_t)nx * nx) * 8;
     return (((f + 7) & ~(size_t)7) + d + 255) & ~(size_t)255;
+}
+
+// K and the spectra of two states, y, Se^-1, the Newton work, Sa^-1 and Sa;
+// with channels, after them the unconvolved spectrum and Jacobian of the
+// state being evaluated, [nraw] then [nx][nraw]
+size_t slot_bytes(int nx, int ny, int nraw) {
+    return slot_core_bytes(nx, ny) + (((size_t)(al4(nraw) + (int64_t)nx * nraw) * 4 + 255) & ~(size_t)255);
 }
 
 // coreret.f:621-700 and :757-766: the next trial state, or its rejection
@@ -509,6 +543,7 @@ struct Engine {
     double* Work(const Slot& s) const { return Db(s) + al4(s.ny); }
     double* Sai(const Slot& s) const { return Db(s) + 2 * al4(s.ny); }
     double* Sa(const Slot& s) const { return Sai(s) + (int64_t)s.nx * s.nx; }
+    float* Raw(const Slot& s) const { return F() + (s.off + slot_core_bytes(s.nx, s.ny)) / 4; }
     float* X(const Slot& s, int part) const { return (float*)xarea.p + (int64_t)s.xrow * kXRow + part * kNewtonMaxNx; }
 
     int init(rtb_context* ctx, const rtb_retrieval_opts& opts, size_t bytes) {
@@ -563,12 +598,13 @@ struct Engine {
         s->kind.assign(s->nx, 1);
         for (int l = 0; l < s->nlayer; ++l) s->kind[l] = 0;
         for (int a = 0; a < sp.nscale; ++a) s->kind[s->nlayer + a] = (sp.scale_model && sp.scale_model[a] == 2) ? 2 : 1;
-        s->ny = sp.atm->nwave;
-        s->bytes = slot_bytes(s->nx, s->ny);
+        s->ny = s->w.ny;
+        s->nraw = s->w.has_conv ? sp.atm->nwave : 0;
+        s->bytes = s->w.has_conv ? slot_bytes(s->nx, s->ny, s->nraw) : slot_core_bytes(s->nx, s->ny);
         if (s->bytes > budget) {
+            const size_t need = s->bytes;
             delete s;
-            return fail(c, RTB_ERR_BUDGET, "retrieval needs %zu B, budget %zu B", slot_bytes(sp.atm->nv, sp.atm->nwave),
-                        budget);
+            return fail(c, RTB_ERR_BUDGET, "retrieval needs %zu B, budget %zu B", need, budget);
         }
         s->xa.assign(sp.xa, sp.xa + s->nx);
         const float* x0 = sp.x0 ? sp.x0 : sp.xa;
@@ -676,8 +712,13 @@ struct Engine {
             if (rs) return rs;
             atms.push_back(s->w.a);
             const int b = first ? s->cur : 1 - s->cur;
-            oo.push_back(Yn(*s, b) - F());
-            jo.push_back(K(*s, b) - F());
+            if (s->w.has_conv) {   // raw outputs, convolved below into Yn and K
+                oo.push_back(Raw(*s) - F());
+                jo.push_back(Raw(*s) + al4(s->nraw) - F());
+            } else {
+                oo.push_back(Yn(*s, b) - F());
+                jo.push_back(K(*s, b) - F());
+            }
             s->forwards++;
         }
         OutPlace pl;
@@ -690,6 +731,13 @@ struct Engine {
         if (r) return r;
         r = launch(c);
         if (r) return r;
+        for (const Slot* s : v)
+            if (s->w.has_conv) {
+                const int b = s->phase == 0 ? s->cur : 1 - s->cur;
+                const ConvSeg seg[2] = {{Raw(*s), 1, Yn(*s, b)}, {Raw(*s) + al4(s->nraw), s->nx, K(*s, b)}};
+                r = conv_run(c, s->w.conv, 2, seg, st);
+                if (r) return r;
+            }
         CUDA_TRY(c, cudaStreamSynchronize(st));
         unsigned long long diag[8];
         CUDA_TRY(c, cudaMemcpy(diag, c->d_diag.p, 64, cudaMemcpyDeviceToHost));
@@ -986,7 +1034,9 @@ int rtb_retrieve_batch(rtb_context* c, int nret, const rtb_retrieval_spec* specs
     std::vector<size_t> sz(nret);
     for (int i = 0; i < nret; ++i) {
         if (!specs[i].atm) return fail(c, RTB_ERR_ARG, "retrieval %d: NULL atmosphere", i);
-        sz[i] = slot_bytes(specs[i].atm->nv, specs[i].atm->nwave);
+        const rtb_atm& t = *specs[i].atm;
+        sz[i] = (t.conv && t.conv->nconv > 0) ? slot_bytes(t.nv, t.conv->nconv, t.nwave)
+                                              : slot_core_bytes(t.nv, t.nwave);
     }
     std::sort(sz.begin(), sz.end(), std::greater<size_t>());
     const int m = o.max_batch > 0 ? std::min(o.max_batch, nret) : nret;

@@ -570,7 +570,7 @@ class RetrievalCase:
 
     @property
     def ny(self):
-        return self.job.nwave
+        return self.job.nconv
 
     def as_struct(self):
         s = _abi.RtbRetrievalSpec()
@@ -692,6 +692,14 @@ def make_level_retrieval(tables: KTables, absorbers, *, npro, nlay, seed, iw0=0,
     return RetrievalCase(job=job, scale_gas=np.arange(2, 2 + ns, dtype=np.int32), xa=xa, sa=sa, sei=sei,
                          x_true=x_true, scale_model=sm if scale_model is not None else None, prof=prior,
                          lopts=dict(nlay=nlay, laytyp=1, layint=1, angle=float(angle)))
+
+
+def with_channels(case: RetrievalCase, fwhm, channels: Channels, noise=1e-9) -> RetrievalCase:
+    """The case measured on instrument channels: the atmosphere convolves
+    its spectrum and Jacobian with cirsconv (FWHM, channels), and y, Se are
+    on the channels."""
+    job = dataclasses.replace(case.job, fwhm=float(fwhm), conv=channels)
+    return dataclasses.replace(case, job=job, y=None, sei=np.full(job.nconv, 1.0 / (noise * noise)))
 
 
 def observe(case: RetrievalCase, spectrum, seed, noise=1e-9):

@@ -1002,6 +1002,7 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
         a.inlte != 0 || a.fwhm != 0.0f)
         return RTB_ERR_UNSUPPORTED;
     if (!(a.iform == 0 || a.iform == 2 || a.iform == 3)) return RTB_ERR_UNSUPPORTED;
+    if (a.ncont < 0 || (a.ncont > 0 && (!a.cont || !a.xsec_ext))) return RTB_ERR_ARG;
     if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
     for (int k = 0; k < a.ngas; ++k) {
         if (a.idgas[k] == 91 || a.idgas[k] == 48 || a.idgas[k] == 80) return RTB_ERR_UNSUPPORTED;

@@ -27,7 +27,7 @@ struct Work {
     float fwhm = 0.0f;
     const rtb_conv* cv = nullptr;
     std::vector<float> temp, pp, amount, emtemp, xmap, pp0, amount0, xmap0;
-    std::vector<float> press, delh, scale, dte, dam, vwave;
+    std::vector<float> press, delh, scale, dte, dam, dco, vwave;
     std::vector<int> layinc, idgas, isogas, ktab, nlayin, imod, sg, sm, pg;
     std::vector<float> vmr0;   /* [nprof][L] pp / press of the profiled gases */
     /* level-state model: L counts the profile's levels (the state's temperatures) */
@@ -166,7 +166,7 @@ int at_level_state(Work& w, const float* x) {
 
 int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     const rtb_atm& t = *s.atm;
-    if (t.npath != 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont != 0)
+    if (t.npath != 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont < 0)
         return RTB_ERR_UNSUPPORTED;
     const int L = t.nlayer, G = t.ngas, NV = t.nv, NW = t.nwave;
     const int ldl = t.ld_lay > 0 ? t.ld_lay : RTB_MAXLAY;
@@ -175,7 +175,7 @@ int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     w.L = L;
     w.NV = NV;
     w.NW = NW;
-    w.nparam = G + 1;
+    w.nparam = G + 1 + t.ncont;   /* dust: a fixed background, its columns of xmap zero */
     w.sg.assign(s.scale_gas, s.scale_gas + s.nscale);
     w.sm.assign(s.nscale, 3);
     if (s.scale_model) w.sm.assign(s.scale_model, s.scale_model + s.nscale);
@@ -194,6 +194,7 @@ int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     col(t.emtemp, 1, w.emtemp);
     col(t.dte, L, w.dte);
     col(t.dam, L, w.dam);
+    if (t.ncont > 0 && t.dco) col(t.dco, L, w.dco);
     w.pp = w.pp0;
     w.amount = w.amount0;
     w.layinc.resize(L);
@@ -232,7 +233,7 @@ int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     w.a.emtemp = w.emtemp.data();
     w.a.dte = w.dte.data();
     w.a.dam = w.dam.data();
-    w.a.dco = nullptr;
+    w.a.dco = w.dco.empty() ? nullptr : w.dco.data();   /* cont and xsec_ext: the caller's arrays */
     w.a.dfp = nullptr;
     w.a.xmap = w.xmap.data();
     w.a.vwave = w.vwave.data();

@@ -277,6 +277,10 @@ class Job:
     radius1: float = 0.0             # km, planet radius (iform = 3 total flux)
     radextra: float = 0.0            # km, correction to radius1
     conv: "Channels | None" = None   # instrument channels (None: FWHM = 0, nconv = nwave)
+    ncont: int = 0                   # dust types
+    cont: np.ndarray | None = None   # (ncont, nlayer) F, dust particles / cm2 per layer
+    xsec_ext: np.ndarray | None = None   # (ncont, nwave) F, extinction x-section at vwave (cm2)
+    dco: np.ndarray | None = None    # (ld_lay, npro) F, d(layer dust)/d(level dust)
     # bookkeeping for the synthetic state vector (not part of the ABI)
     vmr: np.ndarray | None = None
     ncol: np.ndarray | None = None
@@ -284,13 +288,13 @@ class Job:
 
     @property
     def nparam(self) -> int:
-        return self.ngas + 1 + (1 if self.flagh2p else 0)
+        return self.ngas + 1 + self.ncont + (1 if self.flagh2p else 0)
 
     def as_struct(self) -> _abi.RtbAtm:
         s = _abi.RtbAtm()
-        s.nlayer, s.ngas, s.ncont, s.npath = self.nlayer, self.ngas, 0, self.npath
+        s.nlayer, s.ngas, s.ncont, s.npath = self.nlayer, self.ngas, self.ncont, self.npath
         s.npro, s.nv, s.nwave = self.npro, self.nv, self.nwave
-        s.ld_lay, s.ld_con, s.ld_v, s.ld_param = self.ld_lay, 1, self.ld_v, self.ld_param
+        s.ld_lay, s.ld_con, s.ld_v, s.ld_param = self.ld_lay, max(self.ncont, 1), self.ld_v, self.ld_param
         f, i = _abi.fptr, _abi.iptr
         s.press, s.temp, s.delh = f(self.press), f(self.temp), f(self.delh)
         s.pp, s.amount, s.cont = f(self.pp), f(self.amount), None
@@ -300,6 +304,8 @@ class Job:
         s.dte, s.dam, s.dco, s.dfp = f(self.dte), f(self.dam), None, None
         s.xmap = f(self.xmap)
         s.vwave, s.xsec_ext = f(self.vwave), None
+        if self.ncont:
+            s.cont, s.xsec_ext, s.dco = f(self.cont), f(self.xsec_ext), f(self.dco)
         s.inormal, s.iray, s.itype, s.ispace = self.inormal, self.iray, self.itype, self.ispace
         s.flagh2p, s.ilbl, s.inlte, s.iform = self.flagh2p, 0, 0, self.iform
         if self.flagh2p:
@@ -513,6 +519,39 @@ def with_para_h2(job: Job, hfp) -> Job:
     dfp[np.arange(L), np.arange(L)] = 1.0
     return dataclasses.replace(job, nv=nv, ld_v=nv, ld_param=nparam, xmap=xmap, flagh2p=1,
                                hfp=np.ascontiguousarray(hfp, np.float32), dfp=dfp)
+
+
+def with_dust(job: Job, ncont=2, seed=0, tau=0.4, state=True) -> Job:
+    """The job with ncont dust types (cirsradg_wave.f:550-575): layer
+    columns cont(k, l) following a Gaussian in ln p around a seeded level,
+    scaled to a total vertical optical depth near `tau`; smooth extinction
+    cross sections at vwave; DCO the identity on the layers; and (state)
+    one state element per dust type, the scale of its whole profile (xmap =
+    the column of each level), after the others.  state=False: a fixed
+    dust background, its xmap columns zero."""
+    assert not job.flagh2p
+    rng = np.random.default_rng(seed)
+    L, npro, nv0 = job.nlayer, job.npro, job.nv
+    lnp = np.log(job.press[:L].astype(np.float64))
+    v = job.vwave.astype(np.float64)
+    xs = np.zeros((ncont, job.nwave))
+    cont = np.zeros((ncont, L))
+    for k in range(ncont):
+        x0 = 1e-12 * (1.0 + k) * (1.0 + 0.3 * np.sin(v / (40.0 + 25.0 * k) + rng.uniform(0, 6)))
+        xs[k] = x0
+        shape = np.exp(-0.5 * ((lnp - rng.uniform(lnp.min() + 1, lnp.max() - 1)) / 0.8) ** 2)
+        cont[k] = shape / shape.sum() * tau / float(np.mean(x0)) / ncont
+    nparam = job.ngas + 1 + ncont
+    nv = nv0 + (ncont if state else 0)
+    xmap = np.zeros((nv, nparam, npro), np.float32, order="F")
+    xmap[:nv0, :job.ngas + 1, :] = job.xmap[:nv0, :job.ngas + 1, :]
+    for k in range(ncont if state else 0):
+        xmap[nv0 + k, job.ngas + 1 + k, :L] = cont[k].astype(np.float32)
+    dco = np.zeros((job.ld_lay, npro), np.float32, order="F")
+    dco[np.arange(L), np.arange(L)] = 1.0
+    return dataclasses.replace(job, nv=nv, ld_v=nv, ld_param=nparam, xmap=xmap, ncont=ncont,
+                               cont=np.asfortranarray(cont.astype(np.float32)),
+                               xsec_ext=np.asfortranarray(xs.astype(np.float32)), dco=dco)
 
 
 def config1(seed=1001):

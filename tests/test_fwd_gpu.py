@@ -545,3 +545,21 @@ def test_e3_table_file_and_missing_table(tmp_path):
         c2.load_e3_table(str(path))
         b = c2.cirsrtfg_wave(job)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def test_dust_continuum(ctx, oracle):
+    """Dust (cirsradg_wave.f:550-575) with two types whose profile scales are
+    state elements (DCO): radiance and Jacobian within tolerance of the FP64
+    oracle; in a batch beside dust-free spectra each gets its own result."""
+    kt, cia, _ = synth.config2(nwave=6, nlayer=30, nbin=6)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=30, seed=31, nwave=6)
+    jd = synth.with_dust(job, 2, seed=4)
+    c, g, gt = _run(ctx, kt, cia, jd)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, jd, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, jd.nv) <= JAC_TOL
+    assert np.all(g.reshape(jd.nv, -1)[job.nv:] != 0)
+    c0, g0, _ = ctx.cirsrtfg_wave(job)
+    outs = ctx.cirsrtfg_wave_batch([job, jd, job])
+    assert np.array_equal(outs[1][0], c) and np.array_equal(outs[1][1], g)
+    assert np.array_equal(outs[0][0], c0) and np.array_equal(outs[2][1], g0)

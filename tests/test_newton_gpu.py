@@ -283,3 +283,24 @@ def test_retrieval_on_convolved_channels(ctx, oracle, mode):
     assert np.array_equal(alone["x"], g["x"]) and alone["phi"] == g["phi"]
     ref_b, _ = oracle.retrieve(kt, cia, base, kiter=10, phlimit=0.1, nthreads=8)
     assert np.all(np.abs(both[1]["x"] - ref_b["x"]) <= 1e-3 * np.sqrt(np.diag(base.sa)).astype(np.float32))
+
+
+def test_retrieval_with_dust_background(ctx, oracle):
+    """A layer-state retrieval through a fixed dust background (two dust
+    types, their xmap columns zero): same iterations, forward evaluations
+    and stop rule as the oracle's coreret loop, states within 1e-3 prior
+    sigma, cost within 1e-3."""
+    import dataclasses
+    kt, cia, _ = synth.config2()
+    case = synth.make_retrieval(kt, [synth.CH4, synth.NH3], nlayer=30, seed=95, nwave=150)
+    case = dataclasses.replace(case, job=synth.with_dust(case.job, 2, seed=5, state=False))
+    y_true, _ = oracle.forward_state(kt, cia, case, case.x_true, nthreads=8)
+    synth.observe(case, y_true, seed=96)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    g = ctx.retrieve_batch([case], kiter=10, phlimit=0.1)[0]
+    ref, _ = oracle.retrieve(kt, cia, case, kiter=10, phlimit=0.1, nthreads=8)
+    assert (g["converged"], g["iterations"], g["forwards"]) == (ref["converged"], ref["iterations"], ref["forwards"])
+    sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
+    assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
+    assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]

@@ -394,3 +394,27 @@ def test_real_e3_table(oracle):
     c_real, _, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=real)
     c_syn, _, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=syn)
     assert np.max(np.abs(c_real - c_syn) / c_syn) < 1e-12
+
+
+def test_dust_jacobian_by_finite_differences(oracle):
+    """Dust continuum (cirsradg_wave.f:550-575: taucon += xsec * cont,
+    dtaucondq(ngas+1+k) = xsec; DCO maps it to the levels): the FP64
+    oracle's derivative in the scale of each dust profile against central
+    differences of its own radiance, and a dusty spectrum darker than the
+    clear one."""
+    kt, cia, job = synth.config2(nwave=4, nlayer=30, nbin=4)
+    jd = synth.with_dust(job, 2, seed=3)
+    c, g, _ = oracle.cirsrtfg_wave(kt, cia, jd, oracle.ORC_FP64)
+    c0, _, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert np.all(c < c0)
+    G = g.reshape(jd.nv, -1)
+    h = 1e-3
+    for k in range(2):
+        jp = synth.with_dust(job, 2, seed=3)
+        jp.cont[k] *= 1 + h
+        jm = synth.with_dust(job, 2, seed=3)
+        jm.cont[k] *= 1 - h
+        fd = (oracle.cirsrtfg_wave(kt, cia, jp, oracle.ORC_FP64)[0] -
+              oracle.cirsrtfg_wave(kt, cia, jm, oracle.ORC_FP64)[0]) / (2 * h)
+        an = G[job.nv + k]
+        assert np.max(np.abs(fd - an)) <= 1e-4 * np.max(np.abs(an)), k

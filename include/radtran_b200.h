@@ -245,6 +245,10 @@ typedef struct rtb_atm {
      * radius RADIUS1 and the height added above it, radextra, in km
      * (cirsradg_wave.f:913-929, 1136-1152) */
     float radius1, radextra;
+    /* inlte = 1 (/nlte_flags/ of the .nlte file, cirsrtfg_wave.f:200-214):
+     * collisional rate k1 (1e-20 .. 1e-3, else RTB_ERR_ARG) and the
+     * Einstein A of calc_nlte_t.f; unused for inlte = 0 and 2 */
+    float nlte_k1, nlte_A;
 } rtb_atm;
 
 /* Outputs, convolved by cirsconv with atm->fwhm onto the channels of

@@ -936,6 +936,37 @@ template <> double planckg_wave<double>(int ispace, double v, double T) {
     return std::exp(tmp) * A / (em1 * em1);
 }
 
+/* INVPLANCK_WAVE: radtran/radtran/invplanck_wave.f:1-30 (DOUBLE inside,
+ * REAL result) */
+template <class R> R invplanck_wave(int iwave, R v, R B) {
+    double t;
+    if (B == (R)0 || v == (R)0) t = 0.0;
+    else {
+        const double dv = (double)v, v2 = dv * dv, v4 = v2 * v2;   /* dble(v)**3, **5 as products */
+        if (iwave == 0) t = kC2 * dv / std::log((kC1 * (v2 * dv)) / (double)B + 1.0);
+        else t = kC2 * (double)1.0e4f / dv / std::log((kC1 * (double)1.0e16f) / ((double)B * (v4 * dv)) + 1.0);
+    }
+    return (R)t;
+}
+
+/* CALC_NLTE_T: radtran/radtran/calc_nlte_t.f:1-45.  cirsradg_wave.f:933-935
+ * passes the wavenumber index as its IWAVE, so planck_wave and
+ * invplanck_wave there always take their IWAVE != 0 branch */
+template <class R> R calc_nlte_t(R T, R p, R v, int inlte, R k1, R A) {
+    R f;
+    if (inlte == 1) {
+        const R kboltz = (R)1.380658e-23f;
+        const R ntot = (p * (R)101325.f / (kboltz * T)) * (R)1.0e-6f;
+        f = (k1 * ntot) / (A + k1 * ntot);
+    } else if (inlte == 2) {
+        f = p * (R)1.0e6f / ((R)1.0 + p * (R)1.0e6f);
+    } else {
+        return T;
+    }
+    const R B = planck_wave<R>(1, v, T);
+    return invplanck_wave<R>(1, v, B * f);
+}
+
 /* DPEXP: radtran/radtran/dpexp.f */
 template <class R>
 R dpexp(R x) {
@@ -999,9 +1030,10 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
     if (t.ng > RTB_MAXG || t.np > RTB_MAXK || std::abs(t.nt) > RTB_MAXK) return RTB_ERR_LIMIT;
     if (t.ng < 2 || std::abs(t.nt) < 2) return RTB_ERR_UNSUPPORTED;
     if ((a.flagh2p == 1 && (!t.has_para || !a.hfp)) || (a.flagh2p != 0 && a.flagh2p != 1) || a.ilbl != 0 ||
-        a.inlte != 0 || a.fwhm != 0.0f)
+        !(a.inlte == 0 || a.inlte == 1 || a.inlte == 2) || a.fwhm != 0.0f)
         return RTB_ERR_UNSUPPORTED;
     if (!(a.iform == 0 || a.iform == 2 || a.iform == 3)) return RTB_ERR_UNSUPPORTED;
+    if (a.inlte == 1 && !(a.nlte_k1 >= 1.0e-20f && a.nlte_k1 <= 1.0e-3f)) return RTB_ERR_ARG;   /* calc_nlte_t.f:17-20 */
     if (a.ncont < 0 || (a.ncont > 0 && (!a.cont || !a.xsec_ext))) return RTB_ERR_ARG;
     if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
     for (int k = 0; k < a.ngas; ++k) {
@@ -1250,8 +1282,10 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                 const R bsurf = a.tsurf > 0.0f ? planck_wave<R>(a.ispace, (R)vwave, (R)a.tsurf) : (R)0;
                 const R gsurf = a.tsurf > 0.0f ? planckg_wave<R>(a.ispace, (R)vwave, (R)a.tsurf) : (R)0;
                 for (int j = 0; j < nlays; ++j) {
-                    if (ig == 0) {
-                        const R Tn = (R)a.emtemp[j + (size_t)d.ld_lay * ip];
+                    if (ig == 0) {   /* calc_nlte_t at the layer's pressure (:933-935, :1156-1158) */
+                        const R Tn = calc_nlte_t<R>((R)a.emtemp[j + (size_t)d.ld_lay * ip],
+                                                    (R)a.press[a.layinc[j + (size_t)d.ld_lay * ip] - 1], (R)vwave,
+                                                    a.inlte, (R)a.nlte_k1, (R)a.nlte_A);
                         W.bb[(size_t)ip * nlmax + j] = planck_wave<R>(a.ispace, (R)vwave, Tn);
                         W.dbdt[(size_t)ip * nlmax + j] = planckg_wave<R>(a.ispace, (R)vwave, Tn);
                     }
@@ -1302,8 +1336,10 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                     xfac = xfac * (R)1e-18f;
                 }
                 for (int j = 0; j < nlays; ++j) {
-                    if (ig == 0) {
-                        const R Tn = (R)a.emtemp[j + (size_t)d.ld_lay * ip];
+                    if (ig == 0) {   /* calc_nlte_t at the layer's pressure (:933-935, :1156-1158) */
+                        const R Tn = calc_nlte_t<R>((R)a.emtemp[j + (size_t)d.ld_lay * ip],
+                                                    (R)a.press[a.layinc[j + (size_t)d.ld_lay * ip] - 1], (R)vwave,
+                                                    a.inlte, (R)a.nlte_k1, (R)a.nlte_A);
                         W.bb[(size_t)ip * nlmax + j] = planck_wave<R>(a.ispace, (R)vwave, Tn);
                         W.dbdt[(size_t)ip * nlmax + j] = planckg_wave<R>(a.ispace, (R)vwave, Tn);
                     }

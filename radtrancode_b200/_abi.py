@@ -58,6 +58,7 @@ class RtbAtm(C.Structure):
         ("conv", C.POINTER(RtbConv)),
         ("hfp", _fp),
         ("radius1", C.c_float), ("radextra", C.c_float),
+        ("nlte_k1", C.c_float), ("nlte_A", C.c_float),
     ]
 
 

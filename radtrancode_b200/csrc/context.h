@@ -83,6 +83,7 @@ struct Staging {
     std::vector<float> map_val;
     std::vector<ParaLayDev> para_lay;
     std::vector<ParaWaveDev> para_wave;
+    std::vector<float> lpress;   // layer pressures (atm) of the spectra with non-LTE emission
     int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, ngas_max = 1;
     int64_t n_out = 0, n_jac = 0;
 };

@@ -355,6 +355,35 @@ __device__ __forceinline__ void e3interp_dev(const double* tab, double x, double
     de3 = __dadd_rn(__dmul_rn(1.0 - f, eg[j - 1]), __dmul_rn(f, eg[j]));
 }
 
+// calc_nlte_t.f:1-45, the emission temperature of a layer at pressure p (atm)
+// outside LTE: B(T_nlte) = f B(T) with f = k1 N / (A + k1 N), N the number
+// density (inlte = 1), or f = 1e6 p / (1 + 1e6 p) (inlte = 2).  Its IWAVE is
+// the wavenumber index in cirsradg_wave.f:933-935, never 0, so planck_wave
+// and invplanck_wave take their wavelength branch (y = 1e4 / v) there.
+// DOUBLE inside as those two are; REAL factors as calc_nlte_t forms them.
+__device__ __noinline__ float nlte_temp(int inlte, float T, float p, float v, float k1, float A) {
+    float f;
+    if (inlte == 1) {
+        const float ntot = __fmul_rn(__fdiv_rn(__fmul_rn(p, 101325.0f), __fmul_rn(1.380658e-23f, T)), 1.0e-6f);
+        f = __fdiv_rn(__fmul_rn(k1, ntot), __fadd_rn(A, __fmul_rn(k1, ntot)));
+    } else if (inlte == 2) {
+        const float x = __fmul_rn(p, 1.0e6f);
+        f = __fdiv_rn(x, __fadd_rn(1.0f, x));
+    } else {
+        return T;
+    }
+    const double c1 = (double)1.1911e-12f, c2 = (double)1.439f;
+    const float y = __fdiv_rn(1e4f, v);
+    if (y == 0.0f) return 0.0f;                  // planck_wave = 0, then invplanck_wave(B = 0) = 0
+    const float y2 = __fmul_rn(y, y), y4 = __fmul_rn(y2, y2);
+    const double a = c1 * (double)__fmul_rn(y4, y) / 1e4;
+    const float Bt = __double2float_rn(a / (exp(c2 * (double)y / (double)T) - 1.0));
+    const float Bf = __fmul_rn(Bt, f);
+    if (Bf == 0.0f || v == 0.0f) return 0.0f;
+    const double dv = (double)v, v2 = dv * dv, v4 = v2 * v2;
+    return __double2float_rn(c2 * (double)1.0e4f / dv / log((c1 * (double)1.0e16f) / ((double)Bf * (v4 * dv)) + 1.0));
+}
+
 // iform = 3 on an IMOD 3 path (cirsradg_wave.f:913-929): the total flux of the
 // planet, every term of lane g's radiance and derivatives times x.  Out of
 // line, as is path_imod18: the common paths' code stays as compact as it was.
@@ -437,8 +466,10 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
     for (int s = 0; s < kMaxSw; ++s) dtc[s] = 0.0f;
     float taucon = 0.0f;
     for (int k = 0; k < S.ncont; ++k) {
-        const float tau = B.xsec[iw_glob * S.ncont + k];
-        taucon = __fadd_rn(taucon, __fmul_rn(tau, B.cont[il_glob * S.ncont + k]));
+        // this spectrum's [nwave][ncont] and [nlayer][ncont] blocks: the
+        // batch's spectra need not share ncont
+        const float tau = B.xsec[S.wc_off + (iw_glob - S.wave_off) * S.ncont + k];
+        taucon = __fadd_rn(taucon, __fmul_rn(tau, B.cont[S.lc_off + (il_glob - S.lay_off) * S.ncont + k]));
 #pragma unroll
         for (int s = 0; s < kMaxSw; ++s)
             if (s < S.nsw && S.isw[s] == S.ngas + 1 + k) dtc[s] = tau;
@@ -1348,7 +1379,12 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
             const float* scale = B.p_scale + S.path_off + (int64_t)p * S.nlmax;
             const float* emt = B.p_emtemp + S.path_off + (int64_t)p * S.nlmax;
             if (im == 3 || (ext && im == 18)) {
-                for (int j = lane; j < nlays; j += 32) planck_fp32(S.ispace, W.vwave, emt[j], bb[j], dbdt[j]);
+                for (int j = lane; j < nlays; j += 32) {
+                    float Tn = emt[j];
+                    if (ext && S.inlte)
+                        Tn = nlte_temp(S.inlte, Tn, B.lay_press[S.lp_off + layinc[j]], W.vwave, S.nlte_k1, S.nlte_A);
+                    planck_fp32(S.ispace, W.vwave, Tn, bb[j], dbdt[j]);
+                }
             }
             __syncwarp();
             if (lane < ng) {

@@ -199,7 +199,10 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     if (a.flagh2p == 1 && (!c->has_para || !a.hfp))
         return fail(c, RTB_ERR_ARG, "flagh2p=1 needs the para-H2 CIA table (rtb_set_para_cia) and hfp");
     if (a.ilbl != 0) return fail(c, RTB_ERR_UNSUPPORTED, "ILBL != 0 (line-by-line tables) not implemented");
-    if (a.inlte != 0) return fail(c, RTB_ERR_UNSUPPORTED, "non-LTE emission temperatures not implemented");
+    if (!(a.inlte == 0 || a.inlte == 1 || a.inlte == 2))
+        return fail(c, RTB_ERR_UNSUPPORTED, "inlte=%d (calc_nlte_t.f knows 0, 1, 2)", a.inlte);
+    if (a.inlte == 1 && !(a.nlte_k1 >= 1.0e-20f && a.nlte_k1 <= 1.0e-3f))   // calc_nlte_t.f:17-20
+        return fail(c, RTB_ERR_ARG, "calc_nlte_t: k1=%g out of range", (double)a.nlte_k1);
     if (!(a.iform == 0 || a.iform == 2 || a.iform == 3))
         return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d (a stellar spectrum) not implemented", a.iform);
     if (a.iray > 1) return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (only Jovian Rayleigh, iray=1)", a.iray);
@@ -302,6 +305,15 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     if (S.sw_para >= 0 && !a.dfp) return fail(c, RTB_ERR_ARG, "para-H2 fraction in xmap without dfp");
     S.para_off = (int64_t)st.para_lay.size();
     S.paraw_off = (int64_t)st.para_wave.size();
+    // non-LTE emission temperatures (cirsradg_wave.f:933-935): the layer pressures
+    S.inlte = a.inlte;
+    S.nlte_k1 = a.nlte_k1;
+    S.nlte_A = a.nlte_A;
+    S.lp_off = (int64_t)st.lpress.size();
+    if (a.inlte != 0) {
+        st.lpress.insert(st.lpress.end(), a.press, a.press + a.nlayer);
+        st.any_ext = true;
+    }
     for (int ip = 0; ip < a.npath; ++ip) {
         S.nlayin[ip] = a.nlayin[ip];
         S.imod[ip] = a.imod[ip];
@@ -758,6 +770,7 @@ void append_staging(Staging& dst, const Staging& src) {
         S.map_off += colptr;
         S.para_off += (int64_t)dst.para_lay.size();
         S.paraw_off += (int64_t)dst.para_wave.size();
+        S.lp_off += (int64_t)dst.lpress.size();
         S.out_off += dst.n_out;
         S.jac_off += dst.n_jac;
         dst.spec.push_back(S);
@@ -778,6 +791,7 @@ void append_staging(Staging& dst, const Staging& src) {
     append_vec(dst.map_val, src.map_val);
     for (int v : src.map_colptr) dst.map_colptr.push_back(v + (int)rows);
     append_vec(dst.para_lay, src.para_lay);
+    append_vec(dst.lpress, src.lpress);
     append_vec(dst.para_wave, src.para_wave);
     dst.Lmax = std::max(dst.Lmax, src.Lmax);
     dst.nsw_max = std::max(dst.nsw_max, src.nsw_max);
@@ -842,6 +856,7 @@ int pack_batch(rtb_context* c, int nspec, const rtb_atm* atms, Staging& st) {
     st.map_val.reserve(total(&Staging::map_val));
     st.map_colptr.reserve(total(&Staging::map_colptr));
     st.para_lay.reserve(total(&Staging::para_lay));
+    st.lpress.reserve(total(&Staging::lpress));
     st.para_wave.reserve(total(&Staging::para_wave));
     for (int t = 0; t < nthr; ++t) append_staging(st, part[t]);
     return RTB_OK;
@@ -917,6 +932,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     const size_t i_mv = add(st.map_val.data(), bytes_of(st.map_val));
     const size_t i_parl = add(st.para_lay.data(), bytes_of(st.para_lay));
     const size_t i_parw = add(st.para_wave.data(), bytes_of(st.para_wave));
+    const size_t i_lp = add(st.lpress.data(), bytes_of(st.lpress));
     const size_t in_bytes = off + 256;
     CUDA_TRY(c, c->h_in.ensure(in_bytes));
     CUDA_TRY(c, c->d_in.ensure(in_bytes));
@@ -973,6 +989,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
         B.para_lay = (const ParaLayDev*)dp(i_parl);
         B.para_wave = (const ParaWaveDev*)dp(i_parw);
     }
+    B.lay_press = st.lpress.empty() ? nullptr : (const float*)dp(i_lp);
     if (place) {
         B.calcout = place->calcout;
         B.gradtsurf = place->gradtsurf;

@@ -67,6 +67,9 @@ struct SpecDev {
     int ncol;             // tracked overlap columns
     int tsurf_pos;        // tsurf > 0
     float xfac3, xfac18;  // iform factor of the IMOD 3 and IMOD 18 paths (1 unless iform = 3)
+    int inlte;            // non-LTE emission temperatures (calc_nlte_t.f): 0, 1 or 2
+    float nlte_k1, nlte_A;
+    int64_t lp_off;       // lay_press index of layer 0 (inlte != 0)
     int nonlimb_mask;     // bit p: path p adds the surface term (cirsradg_wave.f:985-1000)
     int ispace;
     int inormal;
@@ -133,6 +136,7 @@ struct BatchDev {
     const float* kcia5;          // (5,25,1501)
     const ParaLayDev* para_lay;
     const ParaWaveDev* para_wave;
+    const float* lay_press;      // [.. nlayer] layer pressures (atm) of non-LTE spectra
     // per-CTA scratch slots (tau, dtau/dq of every layer of the current item)
     float* cell_scratch;
     int64_t cell_slot;             // floats per slot

@@ -276,6 +276,9 @@ class Job:
     fwhm: float = 0.0
     radius1: float = 0.0             # km, planet radius (iform = 3 total flux)
     radextra: float = 0.0            # km, correction to radius1
+    inlte: int = 0                   # non-LTE emission temperatures (calc_nlte_t.f): 0, 1 or 2
+    nlte_k1: float = 0.0             # inlte = 1: collisional rate and Einstein A
+    nlte_A: float = 0.0
     conv: "Channels | None" = None   # instrument channels (None: FWHM = 0, nconv = nwave)
     ncont: int = 0                   # dust types
     cont: np.ndarray | None = None   # (ncont, nlayer) F, dust particles / cm2 per layer
@@ -307,7 +310,8 @@ class Job:
         if self.ncont:
             s.cont, s.xsec_ext, s.dco = f(self.cont), f(self.xsec_ext), f(self.dco)
         s.inormal, s.iray, s.itype, s.ispace = self.inormal, self.iray, self.itype, self.ispace
-        s.flagh2p, s.ilbl, s.inlte, s.iform = self.flagh2p, 0, 0, self.iform
+        s.flagh2p, s.ilbl, s.inlte, s.iform = self.flagh2p, 0, self.inlte, self.iform
+        s.nlte_k1, s.nlte_A = float(self.nlte_k1), float(self.nlte_A)
         if self.flagh2p:
             s.hfp, s.dfp = f(self.hfp), f(self.dfp)
         s.tsurf, s.fwhm = float(self.tsurf), float(self.fwhm)

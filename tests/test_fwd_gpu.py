@@ -563,3 +563,26 @@ def test_dust_continuum(ctx, oracle):
     outs = ctx.cirsrtfg_wave_batch([job, jd, job])
     assert np.array_equal(outs[1][0], c) and np.array_equal(outs[1][1], g)
     assert np.array_equal(outs[0][0], c0) and np.array_equal(outs[2][1], g0)
+
+
+@pytest.mark.parametrize("case", ["inlte1", "inlte2", "inlte1_imod18"])
+def test_nlte_emission_temperatures(ctx, oracle, case):
+    """Non-LTE emission temperatures (calc_nlte_t.f, cirsradg_wave.f:933-935
+    and 1156-1158) on IMOD 3 and IMOD 18 paths: radiance, Jacobian and
+    surface gradient within tolerance of the FP64 oracle."""
+    e3 = synth.make_e3_table()
+    kt, cia, _ = synth.config2(nwave=5, nlayer=30, nbin=5)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=30, seed=37, nwave=5)
+    job.tsurf = 170.0
+    if case.startswith("inlte1"):
+        job = dataclasses.replace(job, inlte=1, nlte_k1=1e-10, nlte_A=5e5)
+    else:
+        job = dataclasses.replace(job, inlte=2)
+    if case.endswith("imod18"):
+        job.imod[:] = 18
+    ctx.set_e3_table(e3)
+    c, g, gt = _run(ctx, kt, cia, job)
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=e3)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+    assert np.max(np.abs(gt - gt64)) <= RAD_TOL * np.max(np.abs(gt64))

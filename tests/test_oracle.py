@@ -418,3 +418,24 @@ def test_dust_jacobian_by_finite_differences(oracle):
               oracle.cirsrtfg_wave(kt, cia, jm, oracle.ORC_FP64)[0]) / (2 * h)
         an = G[job.nv + k]
         assert np.max(np.abs(fd - an)) <= 1e-4 * np.max(np.abs(an)), k
+
+
+def test_nlte_emission_temperatures(oracle):
+    """calc_nlte_t (inlte 1, 2): with A = 0 the source function is B(T)
+    itself (T_nlte = invplanck(planck(T)) to rounding), so the spectrum is
+    the LTE one; a finite A lowers the upper layers' source function and
+    the spectrum darkens; inlte = 2 at these pressures (f >= 0.99) changes
+    it by under 1 %.  k1 outside 1e-20 .. 1e-3 is refused."""
+    import dataclasses
+    kt, cia, job = synth.config2(nwave=4, nlayer=30, nbin=4)
+    c0, g0, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    ca, ga, _ = oracle.cirsrtfg_wave(kt, cia, dataclasses.replace(job, inlte=1, nlte_k1=1e-10, nlte_A=0.0),
+                                     oracle.ORC_FP64)
+    assert rad_err(ca, c0) < 1e-6 and jac_err(ga, g0, job.nv) < 1e-5
+    cb, _, _ = oracle.cirsrtfg_wave(kt, cia, dataclasses.replace(job, inlte=1, nlte_k1=1e-10, nlte_A=5e5),
+                                    oracle.ORC_FP64)
+    assert np.all(cb < c0)
+    cc, _, _ = oracle.cirsrtfg_wave(kt, cia, dataclasses.replace(job, inlte=2), oracle.ORC_FP64)
+    assert np.all(cc <= c0) and np.max(np.abs(cc - c0) / c0) < 1e-2
+    with pytest.raises(RuntimeError, match="ARG"):
+        oracle.cirsrtfg_wave(kt, cia, dataclasses.replace(job, inlte=1, nlte_k1=1e-2, nlte_A=1.0), oracle.ORC_FP64)

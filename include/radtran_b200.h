@@ -142,6 +142,20 @@ int rtb_set_cia(rtb_context* ctx, float dnu, const double* temps, const float* k
 int rtb_set_e3_table(rtb_context* ctx, int n, const double* tran, const double* e3);
 int rtb_load_e3_table(rtb_context* ctx, const char* path);
 
+/* The stellar spectrum of /solardat/ (radtran/cirsrad/init_solar_wave.f:
+ * 1-93; its presence is the reference's iread = 999): npt points wave[]
+ * (the calculation's wavespace, monotonic) and rad[] (the star's total
+ * power spectrum).  With it, iform = 1 divides the total planet flux of
+ * IMOD 3 and 18 paths by get_solar_wave(v, -1) (cirsradg_wave.f:919-926,
+ * 1142-1149) and iform = 4 multiplies IMOD 0 transmissions by
+ * get_solar_wave(v, atm->dist) (:861-879); get_solar_wave.f:17-39 takes the
+ * linear interpolation of interp.f, zero outside the table.  Without it both
+ * factors are left out, as there.  rtb_load_stellar_spectrum reads the
+ * text file (comment lines starting '#', the wavespace, which must equal
+ * ispace, the stellar radius, then wave rad pairs). */
+int rtb_set_stellar_spectrum(rtb_context* ctx, int npt, const float* wave, const float* rad);
+int rtb_load_stellar_spectrum(rtb_context* ctx, const char* path, int ispace);
+
 int rtb_set_para_cia(rtb_context* ctx, float dnu2, int ipara, const float* temps, const float* fp,
                      const float* kh2h2, const float* kh2he, const float* kcia5);
 int rtb_load_para_cia(rtb_context* ctx, const char* path, float dnu2, int ipara);
@@ -249,6 +263,9 @@ typedef struct rtb_atm {
      * collisional rate k1 (1e-20 .. 1e-3, else RTB_ERR_ARG) and the
      * Einstein A of calc_nlte_t.f; unused for inlte = 0 and 2 */
     float nlte_k1, nlte_A;
+    /* distance from the star in AU (cirsrtfg_wave.f argument DIST): iform = 4
+     * scales the star's spectrum by 1 / (4 pi (dist AU)^2) when dist > 0 */
+    float dist;
 } rtb_atm;
 
 /* Outputs, convolved by cirsconv with atm->fwhm onto the channels of

@@ -642,6 +642,41 @@ void ciaread(const orc_tables& t, R vv, R temp, R* alpha, R* dalpha) {
     }
 }
 
+/* INTERP: radtran/rtm_util/interp.f:1-17 (the first point past xin, then
+ * the segment before it) */
+float interp_f(const float* x, const float* y, int n, float xin) {
+    int i = 1;
+    if (x[0] < x[n - 1]) {
+        while (i <= n && !(x[i - 1] > xin)) ++i;
+    } else {
+        while (i <= n && !(x[i - 1] < xin)) ++i;
+    }
+    if (i > n) i = n;
+    if (i == 1) i = 2;
+    return y[i - 2] + (y[i - 1] - y[i - 2]) * (xin - x[i - 2]) / (x[i - 1] - x[i - 2]);
+}
+
+/* GET_SOLAR_WAVE: radtran/cirsrad/get_solar_wave.f:17-39 */
+float get_solar_wave(const orc_tables& t, float x, float dist) {
+    const float* w = t.solar_wave;
+    const int n = t.solar_npt;
+    float y = interp_f(w, t.solar_rad, n, x);
+    if (w[0] < w[n - 1]) {
+        if (x < w[0]) y = 0.0f;
+        if (x > w[n - 1]) y = 0.0f;
+    } else {
+        if (x > w[0]) y = 0.0f;
+        if (x < w[n - 1]) y = 0.0f;
+    }
+    if (dist > 0.0f) {
+        const float PI = 3.1415927f, AU = 1.49598e13f;   /* constdef.f:11 */
+        const float d = dist * AU;
+        const float area = 4.0f * PI * (d * d);
+        return y / area;
+    }
+    return y;
+}
+
 /* E3INTERP: radtran/radtran/e3interp.f:14-75 on the table held in t (1001
  * points; egrad formed as the reference forms it at its read) */
 void e3interp(const orc_tables& t, double xtrans, double& e3out, double& de3out) {
@@ -1032,7 +1067,8 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
     if ((a.flagh2p == 1 && (!t.has_para || !a.hfp)) || (a.flagh2p != 0 && a.flagh2p != 1) || a.ilbl != 0 ||
         !(a.inlte == 0 || a.inlte == 1 || a.inlte == 2) || a.fwhm != 0.0f)
         return RTB_ERR_UNSUPPORTED;
-    if (!(a.iform == 0 || a.iform == 2 || a.iform == 3)) return RTB_ERR_UNSUPPORTED;
+    if (a.iform < 0 || a.iform > 4) return RTB_ERR_UNSUPPORTED;
+    if (t.solar_npt == 1 || (t.solar_npt > 1 && (!t.solar_wave || !t.solar_rad))) return RTB_ERR_ARG;
     if (a.inlte == 1 && !(a.nlte_k1 >= 1.0e-20f && a.nlte_k1 <= 1.0e-3f)) return RTB_ERR_ARG;   /* calc_nlte_t.f:17-20 */
     if (a.ncont < 0 || (a.ncont > 0 && (!a.cont || !a.xsec_ext))) return RTB_ERR_ARG;
     if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
@@ -1249,7 +1285,8 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                 const R tmp = cork;
                 if (im == 0) {
                     cork = dpexp<R>(-tmp);
-                    const R xfac = 1;
+                    R xfac = 1;   /* iform 4 with a stellar spectrum: x the star's flux (:861-867) */
+                    if (t.solar_npt > 0 && a.iform == 4) xfac = (R)get_solar_wave(t, vwave, a.dist);
                     for (int j = 0; j < nlays; ++j)
                         for (int k1 = 0; k1 < nsw; ++k1) {
                             const int k = isw[k1];
@@ -1266,12 +1303,13 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                 }
             } else if (im == 18) {  /* hemispherically integrated emission: :1116-1225 */
                 const R PI = (R)3.1415927f;
-                R xfac = 1;
-                if (a.iform == 3) {
+                R xfac = 1;   /* :1136-1152 */
+                if (a.iform == 1 || a.iform == 3) {
                     const R rr = ((R)a.radius1 + (R)a.radextra) * (R)1e5f;
                     xfac = xfac * (R)4. * PI * (rr * rr);
-                    xfac = xfac * (R)1e-18f;
                 }
+                if (t.solar_npt > 0 && a.iform == 1) xfac = xfac / (R)get_solar_wave(t, vwave, -1.0f);
+                if (a.iform == 3) xfac = xfac * (R)1e-18f;
                 double trold = 1., e3old = 0.5;
                 std::vector<R> de3olddq((size_t)nlays * nparam, 0), de3dq((size_t)nlays * nparam, 0);
                 for (int j = 0; j < nlays; ++j)
@@ -1328,13 +1366,14 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
                         dtolddq[(size_t)j * nparam + k] = 0;
                         dtrdq[(size_t)j * nparam + k] = 0;
                     }
-                R xfac = 1.;
-                if (a.iform == 3) {   /* :913-929: the total flux of the planet, x 1e-18 */
+                R xfac = 1.;   /* :913-929: the total flux of the planet, over the star's (iform 1), x 1e-18 (iform 3) */
+                if (a.iform == 1 || a.iform == 3) {
                     const R PI = (R)3.1415927f;
                     const R rr = ((R)a.radius1 + (R)a.radextra) * (R)1e5f;
                     xfac = xfac * PI * (R)4. * PI * (rr * rr);
-                    xfac = xfac * (R)1e-18f;
                 }
+                if (t.solar_npt > 0 && a.iform == 1) xfac = xfac / (R)get_solar_wave(t, vwave, -1.0f);
+                if (a.iform == 3) xfac = xfac * (R)1e-18f;
                 for (int j = 0; j < nlays; ++j) {
                     if (ig == 0) {   /* calc_nlte_t at the layer's pressure (:933-935, :1156-1158) */
                         const R Tn = calc_nlte_t<R>((R)a.emtemp[j + (size_t)d.ld_lay * ip],

@@ -62,6 +62,10 @@ typedef struct orc_tables {
     /* e3interp's table (IMOD 18): 1001 transmissions and E3; NULL -> none */
     const double* e3_tran;
     const double* e3_e3;
+    /* /solardat/ of init_solar_wave (iform 1, 4): npt = 0 -> none */
+    int solar_npt;
+    const float* solar_wave;
+    const float* solar_rad;
 } orc_tables;
 
 /* Debug capture of the g-bin assignment (mixed mode), one record per

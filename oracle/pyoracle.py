@@ -33,6 +33,7 @@ class OrcTables(C.Structure):
         ("para_temps", C.POINTER(C.c_float)), ("para_fp", C.POINTER(C.c_float)),
         ("kh2h2", C.POINTER(C.c_float)), ("kh2he", C.POINTER(C.c_float)), ("kcia5", C.POINTER(C.c_float)),
         ("e3_tran", C.POINTER(C.c_double)), ("e3_e3", C.POINTER(C.c_double)),
+        ("solar_npt", C.c_int), ("solar_wave", C.POINTER(C.c_float)), ("solar_rad", C.POINTER(C.c_float)),
     ]
 
 
@@ -71,8 +72,11 @@ def lib():
     return _lib
 
 
-def tables_struct(kt, cia=None, para=None, e3=None):
+def tables_struct(kt, cia=None, para=None, e3=None, solar=None):
     t = OrcTables()
+    if solar is not None:
+        t.solar_npt = len(solar.wave)
+        t.solar_wave, t.solar_rad = _abi.fptr(solar.wave), _abi.fptr(solar.rad)
     if e3 is not None:
         t.e3_tran, t.e3_e3 = _abi.dptr(e3.tran), _abi.dptr(e3.e3)
     if para is None and cia is not None:
@@ -91,16 +95,17 @@ def tables_struct(kt, cia=None, para=None, e3=None):
         t.has_cia, t.dnu = 1, cia.dnu
         t.cia_temps = _abi.dptr(cia.temps)
         t.kcia = _abi.fptr(cia.kcia)
-    t._keep = (kt, cia, para, e3)
+    t._keep = (kt, cia, para, e3, solar)
     return t
 
 
-def cirsrtfg_wave(kt, cia, job, precision=ORC_MIXED, debug=False, nthreads=1, e3=None):
+def cirsrtfg_wave(kt, cia, job, precision=ORC_MIXED, debug=False, nthreads=1, e3=None, solar=None):
     """Run the oracle forward model.  Returns (calcout, gradients, gradtsurf)
     as float64 arrays, plus (perm, split) debug arrays when requested.  e3 is
-    e3interp's table (a synth.E3Table), needed by IMOD 18 paths."""
+    e3interp's table (a synth.E3Table), needed by IMOD 18 paths; solar the
+    stellar spectrum (a synth.StellarSpectrum) of iform 1 and 4."""
     L = lib()
-    t = tables_struct(kt, cia, e3=e3)
+    t = tables_struct(kt, cia, e3=e3, solar=solar)
     s = job.as_struct()
     n1, n2, n3 = job.out_shapes()
     out = np.zeros(n1), np.zeros(n2), np.zeros(n3)

@@ -59,6 +59,7 @@ class RtbAtm(C.Structure):
         ("hfp", _fp),
         ("radius1", C.c_float), ("radextra", C.c_float),
         ("nlte_k1", C.c_float), ("nlte_A", C.c_float),
+        ("dist", C.c_float),
     ]
 
 

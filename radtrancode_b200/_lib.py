@@ -121,6 +121,10 @@ def lib() -> C.CDLL:
         L.rtb_set_e3_table.restype = C.c_int
         L.rtb_load_e3_table.argtypes = [vp, C.c_char_p]
         L.rtb_load_e3_table.restype = C.c_int
+        L.rtb_set_stellar_spectrum.argtypes = [vp, C.c_int, fp, fp]
+        L.rtb_set_stellar_spectrum.restype = C.c_int
+        L.rtb_load_stellar_spectrum.argtypes = [vp, C.c_char_p, C.c_int]
+        L.rtb_load_stellar_spectrum.restype = C.c_int
         L.rtb_set_ktable_ids.argtypes = [vp, C.c_int, ip, ip]
         L.rtb_set_ktable_ids.restype = C.c_int
         L.rtb_set_ktable_centres.argtypes = [vp, C.c_int, fp]
@@ -154,4 +158,5 @@ EXPORTED = [
     "rtb_calc_serr", "rtb_cirsconv", "rtb_cirsconv_ex", "rtb_read_fwh", "rtb_read_fil",
     "rtb_layerg", "rtb_set_ktable_centres", "rtb_set_ktable_ids",
     "rtb_set_para_cia", "rtb_load_para_cia", "rtb_set_e3_table", "rtb_load_e3_table",
+    "rtb_set_stellar_spectrum", "rtb_load_stellar_spectrum",
 ]

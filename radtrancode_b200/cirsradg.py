@@ -160,6 +160,15 @@ class Context:
         """e3interp's read of the e3tab.dat text file."""
         self._check(self._L.rtb_load_e3_table(self._h, os.fsencode(path)))
 
+    def set_stellar_spectrum(self, ss):
+        """init_solar_wave's table (a synth.StellarSpectrum), used by iform 1
+        and 4."""
+        self._check(self._L.rtb_set_stellar_spectrum(self._h, len(ss.wave), _abi.fptr(ss.wave), _abi.fptr(ss.rad)))
+
+    def load_stellar_spectrum(self, path, ispace=0):
+        """init_solar_wave's read of the stellar spectrum file."""
+        self._check(self._L.rtb_load_stellar_spectrum(self._h, os.fsencode(path), int(ispace)))
+
     def set_cia(self, cia):
         """ciaread's one-time table read."""
         self._check(self._L.rtb_set_cia(self._h, float(cia.dnu), _abi.dptr(cia.temps), _abi.fptr(cia.kcia)))

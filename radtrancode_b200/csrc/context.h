@@ -84,6 +84,7 @@ struct Staging {
     std::vector<ParaLayDev> para_lay;
     std::vector<ParaWaveDev> para_wave;
     std::vector<float> lpress;   // layer pressures (atm) of the spectra with non-LTE emission
+    std::vector<float> wfac;     // get_solar_wave at each wavenumber of iform 1 / 4 spectra
     int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, ngas_max = 1;
     int64_t n_out = 0, n_jac = 0;
 };
@@ -153,6 +154,8 @@ struct rtb_context {
     std::vector<float> para_tk, para_fp, para_vk;
     rtb::DevBuf d_kpara;                     // kh2h2 | kh2he | kcia5
     int has_e3 = 0;
+    // /solardat/ (init_solar_wave): the stellar spectrum, used on the host only
+    std::vector<float> solar_wave, solar_rad;
     rtb::DevBuf d_e3;                        // tabtran | tabe3 | egrad (e3interp)
     std::vector<float> cia_tk;               // sngl(temps)
     rtb::DevBuf d_kcia;

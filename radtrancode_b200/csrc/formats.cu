@@ -261,6 +261,51 @@ int rtb_load_para_cia(rtb_context* c, const char* path, float dnu2, int ipara) {
     return rtb_set_para_cia(c, dnu2, ipara, temps.data(), fp.data(), kh2h2.data(), kh2he.data(), k5.data());
 }
 
+// the stellar spectrum file of init_solar_wave.f:22-78: comment lines
+// starting '#', the wavespace, the stellar radius, then records WAVE RAD up
+// to the end of the file (at most MAXBIN = 16000, arrdef.f:19)
+int rtb_load_stellar_spectrum(rtb_context* c, const char* path, int ispace) {
+    if (!c) return RTB_ERR_ARG;
+    File fl(path);
+    if (!fl.f) return fail(c, RTB_ERR_ARG, "cannot open %s", path ? path : "(null)");
+    char line[4096];
+    std::string first;
+    while (std::fgets(line, sizeof line, fl.f)) {
+        if (line[0] == '#') continue;
+        first = line;
+        break;
+    }
+    int ispace1 = 0;
+    {
+        std::string tok;
+        for (char ch : first) {
+            if (ch == ' ' || ch == '\t' || ch == ',' || ch == '\n' || ch == '\r') {
+                if (!tok.empty()) break;
+            } else {
+                tok += ch;
+            }
+        }
+        if (!to_int(tok, ispace1)) return fail(c, RTB_ERR_ARG, "%s: no wavespace line", path);
+    }
+    if (ispace1 != ispace)
+        return fail(c, RTB_ERR_ARG, "%s: wavespace %d of the stellar file is not the calculation's %d", path, ispace1,
+                    ispace);
+    std::vector<std::string> t;
+    float solrad = 0.0f;
+    if (!list_read(fl.f, 1, t) || !to_real(t[0], solrad)) return fail(c, RTB_ERR_ARG, "%s: no stellar radius", path);
+    std::vector<float> wave, rad;
+    constexpr int kMaxBin = 16000;
+    while (list_read(fl.f, 2, t)) {
+        float w, r;
+        if (!to_real(t[0], w) || !to_real(t[1], r)) return fail(c, RTB_ERR_ARG, "%s: record %zu is not WAVE RAD", path,
+                                                                wave.size() + 1);
+        if ((int)wave.size() == kMaxBin) return fail(c, RTB_ERR_LIMIT, "%s: more than MAXBIN = %d points", path, kMaxBin);
+        wave.push_back(w);
+        rad.push_back(r);
+    }
+    return rtb_set_stellar_spectrum(c, (int)wave.size(), wave.data(), rad.data());
+}
+
 // e3tab.dat (e3interp.f:22-32): N, a header line, then N records TAU TRAN E3
 int rtb_load_e3_table(rtb_context* c, const char* path) {
     if (!c) return RTB_ERR_ARG;

@@ -1416,9 +1416,14 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                     }
                     rad[g] = R;
                     gts[g] = gt;
-                    if (ext && S.xfac3 != 1.0f) scale_path(S.xfac3, nlays, ng, g, drdt, trd, rad, gts);   // iform 3
+                    if (ext) {   // iform 1 (over the star's flux at v) and 3 (cirsradg_wave.f:913-929)
+                        float x = S.xfac3;
+                        if (S.wmode == 1) x = __fdiv_rn(x, B.wave_fac[S.wf_off + iw]);
+                        if (x != 1.0f) scale_path(x, nlays, ng, g, drdt, trd, rad, gts);
+                    }
                 } else if (ext && im == 18) {
-                    path_imod18(B.e3tab, S.xfac18, nlays, ng, g, layinc, scale, tau_s, bb, W.radground_s,
+                    const float x18 = S.wmode == 1 ? __fdiv_rn(S.xfac18, B.wave_fac[S.wf_off + iw]) : S.xfac18;
+                    path_imod18(B.e3tab, x18, nlays, ng, g, layinc, scale, tau_s, bb, W.radground_s,
                                 W.gradground_s, drdt, trd, rad, gts);
                 } else {
                     float tsum = 0.0f;
@@ -1431,6 +1436,11 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                     float out, dr;
                     if (im == 0) { out = e; dr = -tsum * e; }
                     else { out = 1.0f - e; dr = tsum * e; }
+                    if (ext && im == 0 && S.wmode == 2) {   // iform 4: times the star's flux (cirsradg_wave.f:861-879)
+                        const float x = B.wave_fac[S.wf_off + iw];
+                        out = out * x;
+                        dr = dr * x;
+                    }
                     for (int j = 0; j < nlays; ++j) { drdt[j * ng + g] = dr; trd[j * ng + g] = 0.0f; }
                     rad[g] = out;
                     gts[g] = 0.0f;

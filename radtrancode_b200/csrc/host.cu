@@ -179,6 +179,42 @@ struct Dims {
 
 namespace rtb {
 
+// INTERP (radtran/rtm_util/interp.f:1-17): the first point past xin (the
+// order of the table either way), then the segment before it
+float interp_f(const float* x, const float* y, int n, float xin) {
+    int i = 1;
+    if (x[0] < x[n - 1]) {
+        while (i <= n && !(x[i - 1] > xin)) ++i;
+    } else {
+        while (i <= n && !(x[i - 1] < xin)) ++i;
+    }
+    if (i > n) i = n;
+    if (i == 1) i = 2;
+    return y[i - 2] + (y[i - 1] - y[i - 2]) * (xin - x[i - 2]) / (x[i - 1] - x[i - 2]);
+}
+
+// GET_SOLAR_WAVE (radtran/cirsrad/get_solar_wave.f:17-39): zero outside the
+// table; dist > 0 spreads the star's power over the sphere of radius dist AU
+float get_solar_wave_f(const rtb_context* c, float x, float dist) {
+    const float* w = c->solar_wave.data();
+    const int n = (int)c->solar_wave.size();
+    float y = interp_f(w, c->solar_rad.data(), n, x);
+    if (w[0] < w[n - 1]) {
+        if (x < w[0]) y = 0.0f;
+        if (x > w[n - 1]) y = 0.0f;
+    } else {
+        if (x > w[0]) y = 0.0f;
+        if (x < w[n - 1]) y = 0.0f;
+    }
+    if (dist > 0.0f) {
+        const float PI = 3.1415927f, AU = 1.49598e13f;   // constdef.f:11
+        const float d = dist * AU;
+        const float area = 4.0f * PI * (d * d);
+        return y / area;
+    }
+    return y;
+}
+
 int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     Dims d;
     d.ld_lay = a.ld_lay > 0 ? a.ld_lay : RTB_MAXLAY;
@@ -203,8 +239,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         return fail(c, RTB_ERR_UNSUPPORTED, "inlte=%d (calc_nlte_t.f knows 0, 1, 2)", a.inlte);
     if (a.inlte == 1 && !(a.nlte_k1 >= 1.0e-20f && a.nlte_k1 <= 1.0e-3f))   // calc_nlte_t.f:17-20
         return fail(c, RTB_ERR_ARG, "calc_nlte_t: k1=%g out of range", (double)a.nlte_k1);
-    if (!(a.iform == 0 || a.iform == 2 || a.iform == 3))
-        return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d (a stellar spectrum) not implemented", a.iform);
+    if (a.iform < 0 || a.iform > 4) return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d", a.iform);
     if (a.iray > 1) return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (only Jovian Rayleigh, iray=1)", a.iray);
     if (a.npath > 4) return fail(c, RTB_ERR_UNSUPPORTED, "more than 4 paths per spectrum");
     if (a.ncont > 0 && (!a.cont || !a.xsec_ext || !a.dco)) return fail(c, RTB_ERR_ARG, "dust arrays missing");
@@ -275,11 +310,25 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     // iform 3: total spectral flux of the planet, x 1e-18 (cirsradg_wave.f:913-929, 1136-1152)
     S.xfac3 = 1.0f;
     S.xfac18 = 1.0f;
-    if (a.iform == 3) {
+    if (a.iform == 1 || a.iform == 3) {
         const float PI = 3.1415927f;   // constdef.f:11
         const float r = (a.radius1 + a.radextra) * 1e5f;
-        S.xfac3 = 1.0f * PI * 4.0f * PI * (r * r) * 1e-18f;
-        S.xfac18 = 1.0f * 4.0f * PI * (r * r) * 1e-18f;
+        S.xfac3 = 1.0f * PI * 4.0f * PI * (r * r);
+        S.xfac18 = 1.0f * 4.0f * PI * (r * r);
+        if (a.iform == 3) {
+            S.xfac3 = S.xfac3 * 1e-18f;
+            S.xfac18 = S.xfac18 * 1e-18f;
+        }
+        st.any_ext = true;
+    }
+    // a stellar spectrum (iread = 999): iform 1 divides the planet's flux by
+    // get_solar_wave(v, -1), iform 4 multiplies IMOD 0 by get_solar_wave(v, dist)
+    S.wmode = 0;
+    S.wf_off = (int64_t)st.wfac.size();
+    if (!c->solar_wave.empty() && (a.iform == 1 || a.iform == 4)) {
+        S.wmode = a.iform == 1 ? 1 : 2;
+        const float dist = a.iform == 1 ? -1.0f : a.dist;
+        for (int iw = 0; iw < a.nwave; ++iw) st.wfac.push_back(get_solar_wave_f(c, a.vwave[iw], dist));
         st.any_ext = true;
     }
     for (int ip = 0; ip < a.npath; ++ip)
@@ -771,6 +820,7 @@ void append_staging(Staging& dst, const Staging& src) {
         S.para_off += (int64_t)dst.para_lay.size();
         S.paraw_off += (int64_t)dst.para_wave.size();
         S.lp_off += (int64_t)dst.lpress.size();
+        S.wf_off += (int64_t)dst.wfac.size();
         S.out_off += dst.n_out;
         S.jac_off += dst.n_jac;
         dst.spec.push_back(S);
@@ -792,6 +842,7 @@ void append_staging(Staging& dst, const Staging& src) {
     for (int v : src.map_colptr) dst.map_colptr.push_back(v + (int)rows);
     append_vec(dst.para_lay, src.para_lay);
     append_vec(dst.lpress, src.lpress);
+    append_vec(dst.wfac, src.wfac);
     append_vec(dst.para_wave, src.para_wave);
     dst.Lmax = std::max(dst.Lmax, src.Lmax);
     dst.nsw_max = std::max(dst.nsw_max, src.nsw_max);
@@ -857,6 +908,7 @@ int pack_batch(rtb_context* c, int nspec, const rtb_atm* atms, Staging& st) {
     st.map_colptr.reserve(total(&Staging::map_colptr));
     st.para_lay.reserve(total(&Staging::para_lay));
     st.lpress.reserve(total(&Staging::lpress));
+    st.wfac.reserve(total(&Staging::wfac));
     st.para_wave.reserve(total(&Staging::para_wave));
     for (int t = 0; t < nthr; ++t) append_staging(st, part[t]);
     return RTB_OK;
@@ -933,6 +985,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     const size_t i_parl = add(st.para_lay.data(), bytes_of(st.para_lay));
     const size_t i_parw = add(st.para_wave.data(), bytes_of(st.para_wave));
     const size_t i_lp = add(st.lpress.data(), bytes_of(st.lpress));
+    const size_t i_wf = add(st.wfac.data(), bytes_of(st.wfac));
     const size_t in_bytes = off + 256;
     CUDA_TRY(c, c->h_in.ensure(in_bytes));
     CUDA_TRY(c, c->d_in.ensure(in_bytes));
@@ -990,6 +1043,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
         B.para_wave = (const ParaWaveDev*)dp(i_parw);
     }
     B.lay_press = st.lpress.empty() ? nullptr : (const float*)dp(i_lp);
+    B.wave_fac = st.wfac.empty() ? nullptr : (const float*)dp(i_wf);
     if (place) {
         B.calcout = place->calcout;
         B.gradtsurf = place->gradtsurf;
@@ -1471,6 +1525,17 @@ int rtb_set_e3_table(rtb_context* c, int n, const double* tran, const double* e3
     CUDA_TRY(c, c->d_e3.ensure(t.size() * 8));
     CUDA_TRY(c, cudaMemcpy(c->d_e3.p, t.data(), t.size() * 8, cudaMemcpyHostToDevice));
     c->has_e3 = 1;
+    return RTB_OK;
+}
+
+int rtb_set_stellar_spectrum(rtb_context* c, int npt, const float* wave, const float* rad) {
+    if (!c) return RTB_ERR_ARG;
+    if (npt < 2 || !wave || !rad) return fail(c, RTB_ERR_ARG, "stellar spectrum: %d points", npt);
+    for (int i = 0; i < npt; ++i)
+        if (!std::isfinite(wave[i]) || !std::isfinite(rad[i]))
+            return fail(c, RTB_ERR_ARG, "stellar spectrum: point %d not finite", i);
+    c->solar_wave.assign(wave, wave + npt);
+    c->solar_rad.assign(rad, rad + npt);
     return RTB_OK;
 }
 

@@ -70,6 +70,8 @@ struct SpecDev {
     int inlte;            // non-LTE emission temperatures (calc_nlte_t.f): 0, 1 or 2
     float nlte_k1, nlte_A;
     int64_t lp_off;       // lay_press index of layer 0 (inlte != 0)
+    int wmode;            // stellar factor per wavenumber: 0 none, 1 divides (iform 1), 2 multiplies IMOD 0 (iform 4)
+    int64_t wf_off;       // wave_fac index of wavenumber 0 (wmode != 0)
     int nonlimb_mask;     // bit p: path p adds the surface term (cirsradg_wave.f:985-1000)
     int ispace;
     int inormal;
@@ -137,6 +139,7 @@ struct BatchDev {
     const ParaLayDev* para_lay;
     const ParaWaveDev* para_wave;
     const float* lay_press;      // [.. nlayer] layer pressures (atm) of non-LTE spectra
+    const float* wave_fac;       // [.. nwave] get_solar_wave of iform 1 / 4 spectra
     // per-CTA scratch slots (tau, dtau/dq of every layer of the current item)
     float* cell_scratch;
     int64_t cell_slot;             // floats per slot

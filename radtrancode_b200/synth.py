@@ -99,6 +99,38 @@ class E3Table:
     e3: np.ndarray
 
 
+@dataclasses.dataclass
+class StellarSpectrum:
+    """The stellar spectrum of init_solar_wave (/solardat/): the star's
+    radius and its total power spectrum rad at the points wave."""
+    solrad: float
+    wave: np.ndarray       # float32, monotonic
+    rad: np.ndarray        # float32
+
+
+def make_stellar_spectrum(v0, v1, npt=400, teff=5800.0, solrad=6.96e10, descending=False) -> StellarSpectrum:
+    """A blackbody star of temperature teff and radius solrad (cm): total
+    power 4 pi^2 R^2 B(v, teff) at npt wavenumbers spanning [v0, v1],
+    in descending order if asked (interp.f handles both)."""
+    v = np.linspace(v0, v1, npt)
+    b = 1.1911e-12 * v ** 3 / np.expm1(1.439 * v / teff)
+    rad = 4.0 * np.pi ** 2 * solrad ** 2 * b
+    if descending:
+        v, rad = v[::-1].copy(), rad[::-1].copy()
+    return StellarSpectrum(float(solrad), v.astype(np.float32), rad.astype(np.float32))
+
+
+def write_stellar_file(path, ss: StellarSpectrum, ispace=0):
+    """The text file init_solar_wave.f reads: comment lines, the wavespace,
+    the stellar radius, then WAVE RAD records (9 significant digits: the
+    REAL values read back exactly)."""
+    with open(path, "w") as fh:
+        fh.write("# synthetic stellar spectrum\n# wavespace, radius, then wave rad\n")
+        fh.write(f"{ispace}\n{ss.solrad:.9e}\n")
+        for w, r in zip(ss.wave, ss.rad):
+            fh.write(f"{float(w):.9e} {float(r):.9e}\n")
+
+
 def make_e3_table() -> E3Table:
     """E3 of the e3tab.dat layout: tran(i) = REAL(i/1000), tau = -ln(tran)
     (1e36 standing for tran = 0, where E3 = 0), E3(0) = 1/2."""
@@ -279,6 +311,7 @@ class Job:
     inlte: int = 0                   # non-LTE emission temperatures (calc_nlte_t.f): 0, 1 or 2
     nlte_k1: float = 0.0             # inlte = 1: collisional rate and Einstein A
     nlte_A: float = 0.0
+    dist: float = 0.0                # AU, distance from the star (iform = 4)
     conv: "Channels | None" = None   # instrument channels (None: FWHM = 0, nconv = nwave)
     ncont: int = 0                   # dust types
     cont: np.ndarray | None = None   # (ncont, nlayer) F, dust particles / cm2 per layer
@@ -312,6 +345,7 @@ class Job:
         s.inormal, s.iray, s.itype, s.ispace = self.inormal, self.iray, self.itype, self.ispace
         s.flagh2p, s.ilbl, s.inlte, s.iform = self.flagh2p, 0, self.inlte, self.iform
         s.nlte_k1, s.nlte_A = float(self.nlte_k1), float(self.nlte_A)
+        s.dist = float(self.dist)
         if self.flagh2p:
             s.hfp, s.dfp = f(self.hfp), f(self.dfp)
         s.tsurf, s.fwhm = float(self.tsurf), float(self.fwhm)

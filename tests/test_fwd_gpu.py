@@ -586,3 +586,57 @@ def test_nlte_emission_temperatures(ctx, oracle, case):
     assert rad_err(c, c64) <= RAD_TOL
     assert jac_err(g, g64, job.nv) <= JAC_TOL
     assert np.max(np.abs(gt - gt64)) <= RAD_TOL * np.max(np.abs(gt64))
+
+
+@pytest.mark.parametrize("case", ["iform1_imod3", "iform1_imod18", "iform4_imod0", "iform1_no_star"])
+def test_stellar_spectrum_forms(ctx, oracle, case):
+    """iform 1 (planet flux over the star's, cirsradg_wave.f:913-929 and
+    1136-1152) and iform 4 (IMOD 0 transmission times the star's flux at
+    dist, :861-879) with init_solar_wave's table, and iform 1 without one:
+    radiance and Jacobian within tolerance of the FP64 oracle."""
+    from radtrancode_b200 import cirsradg
+    e3 = synth.make_e3_table()
+    ss = synth.make_stellar_spectrum(550.0, 700.0, npt=301, descending=case == "iform4_imod0")
+    kt, cia, _ = synth.config2(nwave=5, nlayer=30, nbin=5)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=30, seed=41, nwave=5)
+    job.tsurf = 165.0
+    if case.startswith("iform1"):
+        job = dataclasses.replace(job, iform=1, radius1=71492.0, radextra=20.0)
+    else:
+        job = dataclasses.replace(job, iform=4, dist=5.2, imod=np.zeros_like(job.imod))
+    if case == "iform1_imod18":
+        job.imod[:] = 18
+    with cirsradg.Context(0) as c2:
+        c2.set_ktables(kt)
+        c2.set_cia(cia)
+        c2.set_e3_table(e3)
+        if case != "iform1_no_star":
+            c2.set_stellar_spectrum(ss)
+        c, g, gt = c2.cirsrtfg_wave(job)
+    star = None if case == "iform1_no_star" else ss
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, e3=e3, solar=star)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+
+
+def test_stellar_spectrum_file(tmp_path):
+    """The stellar spectrum read from init_solar_wave's text file gives the
+    in-memory table's run bit for bit; a file in the other wavespace is
+    refused."""
+    from radtrancode_b200 import cirsradg
+    ss = synth.make_stellar_spectrum(550.0, 700.0, npt=301)
+    path = tmp_path / "star.dat"
+    synth.write_stellar_file(path, ss, ispace=0)
+    kt, cia, _ = synth.config2(nwave=5, nlayer=30, nbin=5)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=30, seed=43, nwave=5)
+    job = dataclasses.replace(job, iform=1, radius1=71492.0)
+    with cirsradg.Context(0) as c2:
+        c2.set_ktables(kt)
+        c2.set_cia(cia)
+        c2.set_stellar_spectrum(ss)
+        a = c2.cirsrtfg_wave(job)
+        c2.load_stellar_spectrum(str(path), 0)
+        b = c2.cirsrtfg_wave(job)
+        with pytest.raises(cirsradg.RtbError, match="wavespace"):
+            c2.load_stellar_spectrum(str(path), 1)
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))

@@ -439,3 +439,70 @@ def test_nlte_emission_temperatures(oracle):
     assert np.all(cc <= c0) and np.max(np.abs(cc - c0) / c0) < 1e-2
     with pytest.raises(RuntimeError, match="ARG"):
         oracle.cirsrtfg_wave(kt, cia, dataclasses.replace(job, inlte=1, nlte_k1=1e-2, nlte_A=1.0), oracle.ORC_FP64)
+
+
+def _read_stellar(path):
+    """init_solar_wave.f:22-78: '#' comment lines, the wavespace, the
+    stellar radius, then WAVE RAD records."""
+    rows = [ln.split() for ln in open(path).read().splitlines() if ln.strip() and not ln.startswith("#")]
+    ispace, solrad = int(rows[0][0]), float(rows[1][0])
+    rec = np.array([[float(a), float(b)] for a, b in rows[2:]], np.float32)
+    return ispace, synth.StellarSpectrum(solrad, rec[:, 0].copy(), rec[:, 1].copy())
+
+
+def test_stellar_flux_ratio_and_transmission(oracle):
+    """iform 1 (cirsradg_wave.f:913-929): the IMOD 3 flux times
+    pi 4 pi (R 1e5)^2, over get_solar_wave(v, -1); iform 4 (:861-879): the
+    IMOD 0 transmission times get_solar_wave(v, dist), the star's power
+    over 4 pi (dist AU)^2; without a stellar spectrum iform 1 keeps the
+    total flux and iform 4 the transmission.  Checked against numpy's
+    linear interpolation of the table."""
+    import dataclasses
+    kt, cia, job = synth.config2(nwave=4, nlayer=30, nbin=4)
+    ss = synth.make_stellar_spectrum(500.0, 800.0, descending=True)
+    v = job.vwave.astype(np.float64)
+    xs = np.interp(v, ss.wave[::-1].astype(np.float64), ss.rad[::-1].astype(np.float64))
+    pi = float(np.float32(np.pi))
+    c0, g0, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    j1 = dataclasses.replace(job, iform=1, radius1=71492.0, radextra=10.0)
+    c1, g1, _ = oracle.cirsrtfg_wave(kt, cia, j1, oracle.ORC_FP64, solar=ss)
+    area = pi * 4.0 * pi * ((71492.0 + 10.0) * 1e5) ** 2
+    assert np.max(np.abs(c1 * xs / area / c0 - 1.0)) < 1e-6
+    assert jac_err(g1 * np.tile(xs, job.nv) / area, g0, job.nv) < 1e-6
+    c1n, _, _ = oracle.cirsrtfg_wave(kt, cia, j1, oracle.ORC_FP64)
+    assert np.max(np.abs(c1n / area / c0 - 1.0)) < 1e-6
+    j4 = dataclasses.replace(job, iform=4, dist=5.2)
+    j4.imod[:] = 0
+    j0 = dataclasses.replace(job)
+    j0.imod = np.zeros_like(job.imod)
+    t0, _, _ = oracle.cirsrtfg_wave(kt, cia, j0, oracle.ORC_FP64)
+    t4, _, _ = oracle.cirsrtfg_wave(kt, cia, j4, oracle.ORC_FP64, solar=ss)
+    sph = 4.0 * pi * (5.2 * 1.49598e13) ** 2
+    assert np.max(np.abs(t4 * sph / xs / t0 - 1.0)) < 1e-5
+
+
+STELLAR = "/root/reference/raddata/upsAnd.dat"
+
+
+@pytest.mark.skipif(not os.path.exists(STELLAR), reason="reference data not mounted")
+def test_real_stellar_spectrum_file(oracle):
+    """The reference's upsAnd.dat (wavelength space, 0.465-0.97 um) read as
+    init_solar_wave reads it; the oracle's iform 4 transmission at 0.8 um
+    is the IMOD 0 transmission times the file's interpolated luminosity
+    over 4 pi (dist AU)^2."""
+    import dataclasses
+    ispace, ss = _read_stellar(STELLAR)
+    assert ispace == 1 and ss.solrad > 0 and len(ss.wave) > 10 and np.all(ss.rad > 0)
+    kt = synth.make_ktables(synth.ABSORBERS_C2, np_=20, nt=15, ng=20, vmin=12500.0, delv=0.4, nbin=4, seed=2)
+    cia = synth.make_cia(2)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=30, seed=3, nwave=4)
+    lam = (1e4 / job.vwave.astype(np.float64)).astype(np.float32)
+    assert ss.wave.min() < lam.min() and lam.max() < ss.wave.max()
+    j0 = dataclasses.replace(job, ispace=1, vwave=lam, imod=np.zeros_like(job.imod))
+    j4 = dataclasses.replace(j0, iform=4, dist=3.0)
+    t0, _, _ = oracle.cirsrtfg_wave(kt, None, j0, oracle.ORC_FP64)
+    t4, _, _ = oracle.cirsrtfg_wave(kt, None, j4, oracle.ORC_FP64, solar=ss)
+    xs = np.interp(lam.astype(np.float64), ss.wave.astype(np.float64), ss.rad.astype(np.float64))
+    pi = float(np.float32(np.pi))
+    sph = 4.0 * pi * (3.0 * 1.49598e13) ** 2
+    assert np.all(t0 > 0) and np.max(np.abs(t4 * sph / xs / t0 - 1.0)) < 1e-5

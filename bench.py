@@ -651,7 +651,8 @@ def main():
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "peak_source": f"{how} (MEASURED_PEAKS.json hbm_gbs, burst)",
+                         "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst)" if how == "measured" else
+                                         "fallback: the pool's earlier copy measurement (MEASURED_PEAKS.json absent)"),
                          "algorithmic_bytes_per_launch": ab, "kernel": "fwd_kernel"},
             "overlap_passes": {"sorted": st["sort_passes"], "with_ties": st["tie_passes"],
                                "reference_heapsort": st["exact_passes"], "irregular": st["irregular_passes"]},

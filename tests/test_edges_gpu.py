@@ -89,3 +89,21 @@ def test_empty_and_malformed_calls(ctx):
     j.layinc[0, 0] = job.nlayer + 1                      # a path through a layer that does not exist
     with pytest.raises(cirsradg.RtbError, match="LIMIT"):
         ctx.cirsrtfg_wave(j)
+
+
+def test_largest_profile_and_its_limit(ctx, oracle):
+    """200 layers, each its own profile level: NPRO = MAXPRO of arrdef.f,
+    the largest profile the reference holds, against the FP64 oracle; one
+    level more is refused with RTB_ERR_LIMIT (check_limits.f)."""
+    kt, cia, _ = synth.config2(nwave=2, nlayer=20, nbin=2)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=200, seed=88, nwave=2)
+    assert job.npro == 200
+    c, g, _ = ctx.cirsrtfg_wave(job)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64, nthreads=2)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+    big = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=201, seed=89, nwave=1)
+    with pytest.raises(cirsradg.RtbError, match="LIMIT"):
+        ctx.cirsrtfg_wave(big)

@@ -319,7 +319,8 @@ int rtb_read_fil(const char* path, int* nfil, int* npts, float* vcen, int* nsub,
  * reference one wavenumber at a time: the layer and path arrays as for
  * rtb_cirsrtfg_wave with atm->nwave == 1 (xmap, dte, dam, dco, npro and nv are
  * ignored), the active parameters isw[nsw] (0-based parameter ids: gases
- * 0..ngas-1, temperature ngas, dust ngas+1..; increasing, nsw <= 8) and:
+ * 0..ngas-1, temperature ngas, dust ngas+1..; increasing, nsw <= 8; at
+ * most 4 paths, RTB_ERR_UNSUPPORTED beyond) and:
  *   output[npath]           radiance of every path
  *   gtsurf[npath]           d output / d tsurf (may be NULL)
  *   doutputdq(ld_pat, ld_lay, ld_param)  d output(ipath) / d q(layer j of the

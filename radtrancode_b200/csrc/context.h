@@ -84,6 +84,7 @@ struct Staging {
     std::vector<ParaLayDev> para_lay;
     std::vector<ParaWaveDev> para_wave;
     std::vector<float> lpress;   // layer pressures (atm) of the spectra with non-LTE emission
+    std::vector<int> nsub;       // device spectra (path groups) of each caller spectrum, in order
     std::vector<float> wfac;     // get_solar_wave at each wavenumber of iform 1 / 4 spectra
     int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, ngas_max = 1;
     int64_t n_out = 0, n_jac = 0;

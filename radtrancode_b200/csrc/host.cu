@@ -241,7 +241,6 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
         return fail(c, RTB_ERR_ARG, "calc_nlte_t: k1=%g out of range", (double)a.nlte_k1);
     if (a.iform < 0 || a.iform > 4) return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d", a.iform);
     if (a.iray > 1) return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (only Jovian Rayleigh, iray=1)", a.iray);
-    if (a.npath > 4) return fail(c, RTB_ERR_UNSUPPORTED, "more than 4 paths per spectrum");
     if (a.ncont > 0 && (!a.cont || !a.xsec_ext || !a.dco)) return fail(c, RTB_ERR_ARG, "dust arrays missing");
     const int ng = c->ng;
     if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
@@ -362,10 +361,6 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     if (a.inlte != 0) {
         st.lpress.insert(st.lpress.end(), a.press, a.press + a.nlayer);
         st.any_ext = true;
-    }
-    for (int ip = 0; ip < a.npath; ++ip) {
-        S.nlayin[ip] = a.nlayin[ip];
-        S.imod[ip] = a.imod[ip];
     }
     // ---- per-layer set-up ----
     S.lay_off = (int64_t)st.lay.size();
@@ -678,7 +673,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     }
     // ---- paths ----
     S.path_off = (int64_t)st.p_layinc.size();
-    S.nonlimb_mask = 0;
+    std::vector<char> nonlimb(a.npath, 0);
     for (int ip = 0; ip < a.npath; ++ip) {
         const int nl = a.nlayin[ip];
         for (int j = 0; j < nlmax; ++j) {
@@ -696,7 +691,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
             const int j1 = (int)(0.5f * (float)nl);
             const float p1 = a.press[a.layinc[(j1 - 1) + (size_t)d.ld_lay * ip] - 1];
             const float p2 = a.press[a.layinc[(nl - 1) + (size_t)d.ld_lay * ip] - 1];
-            if (p2 > p1) S.nonlimb_mask |= 1 << ip;
+            if (p2 > p1) nonlimb[ip] = 1;
         }
     }
     // ---- map2pro o map2xvec: sparse (s, j) -> iv per path ----
@@ -787,13 +782,35 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     S.jac_off = st.n_jac;
     st.n_out += (int64_t)a.npath * a.nwave;
     st.n_jac += (int64_t)a.npath * a.nv * a.nwave;
-    st.item_start.push_back(st.item_start.back() + a.nwave);
-    st.spec.push_back(S);
+    // The device takes up to kMaxPathDev paths per spectrum.  A spectrum with
+    // more (limb sets of many tangent paths, up to MAXPAT) is launched as
+    // groups of kMaxPathDev paths over the same layers, wavenumbers and
+    // state map; each group writes its paths' slots of the spectrum's
+    // outputs, which stay contiguous in path order.
+    const int ngrp = (a.npath + kMaxPathDev - 1) / kMaxPathDev;
+    for (int gi = 0; gi < ngrp; ++gi) {
+        SpecDev G = S;
+        const int p0 = gi * kMaxPathDev;
+        G.npath = std::min(kMaxPathDev, a.npath - p0);
+        G.nonlimb_mask = 0;
+        for (int ip = 0; ip < kMaxPathDev; ++ip) {
+            G.nlayin[ip] = ip < G.npath ? a.nlayin[p0 + ip] : 0;
+            G.imod[ip] = ip < G.npath ? a.imod[p0 + ip] : 0;
+            if (ip < G.npath && nonlimb[p0 + ip]) G.nonlimb_mask |= 1 << ip;
+        }
+        G.path_off = S.path_off + (int64_t)p0 * nlmax;
+        G.map_off = S.map_off + (int64_t)p0 * (a.nv + 1);
+        G.out_off = S.out_off + (int64_t)p0 * a.nwave;
+        G.jac_off = S.jac_off + (int64_t)p0 * a.nv * a.nwave;
+        st.item_start.push_back(st.item_start.back() + a.nwave);
+        st.spec.push_back(G);
+    }
+    st.nsub.push_back(ngrp);
     st.Lmax = std::max(st.Lmax, a.nlayer);
     st.nsw_max = std::max(st.nsw_max, S.nsw);
     st.ncol_max = std::max(st.ncol_max, S.ncol);
     st.nlmax_max = std::max(st.nlmax_max, nlmax);
-    st.npath_max = std::max(st.npath_max, a.npath);
+    st.npath_max = std::max(st.npath_max, std::min(a.npath, kMaxPathDev));
     st.ngas_max = std::max(st.ngas_max, a.ngas);
     return RTB_OK;
 }
@@ -842,6 +859,7 @@ void append_staging(Staging& dst, const Staging& src) {
     for (int v : src.map_colptr) dst.map_colptr.push_back(v + (int)rows);
     append_vec(dst.para_lay, src.para_lay);
     append_vec(dst.lpress, src.lpress);
+    append_vec(dst.nsub, src.nsub);
     append_vec(dst.wfac, src.wfac);
     append_vec(dst.para_wave, src.para_wave);
     dst.Lmax = std::max(dst.Lmax, src.Lmax);
@@ -948,11 +966,16 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
         return fail(c, RTB_ERR_UNSUPPORTED, "spectrum needs %d B of shared memory (device %d)", smem, smem_max);
     const int bpsm = fwd_blocks_per_sm(smem);
     if (bpsm <= 0) return fail(c, RTB_ERR_CUDA, "forward kernel cannot be resident (smem %d B)", smem);
+    // first device spectrum of each caller spectrum (path groups follow it)
+    std::vector<int> first(nspec + 1, 0);
+    for (int sp = 0; sp < nspec; ++sp) first[sp + 1] = first[sp] + st.nsub[sp];
     if (place)
-        for (int sp = 0; sp < nspec; ++sp) {
-            st.spec[sp].out_off = place->out_off[sp];
-            st.spec[sp].jac_off = place->jac_off[sp];
-        }
+        for (int sp = 0; sp < nspec; ++sp)
+            for (int k = first[sp]; k < first[sp + 1]; ++k) {
+                const int p0 = (k - first[sp]) * kMaxPathDev;
+                st.spec[k].out_off = place->out_off[sp] + (int64_t)p0 * atms[sp].nwave;
+                st.spec[k].jac_off = place->jac_off[sp] + (int64_t)p0 * atms[sp].nv * atms[sp].nwave;
+            }
     struct Seg {
         const void* src;
         size_t n;
@@ -1002,7 +1025,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     auto dp = [&](size_t i) { return (const void*)((const char*)c->d_in.p + segs[i].off); };
     BatchDev& B = c->B;
     memset(&B, 0, sizeof B);
-    B.nspec = nspec;
+    B.nspec = (int)st.spec.size();   // device spectra: path groups of the caller's spectra
     B.nitems = st.item_start.back();
     B.item_start = (const int64_t*)dp(i_item);
     B.spec = (const SpecDev*)dp(i_spec);
@@ -1086,7 +1109,8 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     c->ncol_max = st.ncol_max;
     c->nlmax_max = st.nlmax_max;
     c->npath_max = st.npath_max;
-    c->spec_host = st.spec;
+    c->spec_host.clear();
+    for (int s = 0; s < nspec; ++s) c->spec_host.push_back(st.spec[first[s]]);   // outputs start at path 0
     c->spec_conv = std::move(convs);
     c->any_conv = any_conv;
     c->spec_npath.clear();
@@ -1105,8 +1129,9 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
         int nabs = 0;
         for (int k = 0; k < atms[s].ngas; ++k)
             nabs += (atms[s].ktab[k] >= 0 || atms[s].ktab[k] == RTB_KTAB_BY_ID) ? 1 : 0;
-        c->spec_cost.push_back((float)atms[s].nlayer * (1.0f + 4.0f * std::max(nabs - 1, 0)) *
-                               (2.0f + st.spec[s].nsw));
+        for (int k = first[s]; k < first[s + 1]; ++k)   // per device spectrum, as item_start_host
+            c->spec_cost.push_back((float)atms[s].nlayer * (1.0f + 4.0f * std::max(nabs - 1, 0)) *
+                                   (2.0f + st.spec[k].nsw));
     }
     c->item_start_host = st.item_start;
     c->order_ready = 0;
@@ -1675,6 +1700,8 @@ int rtb_cirsradg_wave(rtb_context* c, const rtb_atm* atm, int nsw, const int* is
     const int nparam = a0.ngas + 1 + a0.ncont;
     if (ld_pat < a0.npath || ld_lay < a0.nlayer || ld_param < nparam)
         return fail(c, RTB_ERR_ARG, "cirsradg_wave: doutputdq leading dimensions too small");
+    if (a0.npath > kMaxPathDev)   // its per-path derivatives are captured for one path group only
+        return fail(c, RTB_ERR_UNSUPPORTED, "cirsradg_wave: more than %d paths", kMaxPathDev);
     for (int s = 0; s < nsw; ++s)
         if (isw[s] < 0 || isw[s] >= nparam || (s > 0 && isw[s] <= isw[s - 1]))
             return fail(c, RTB_ERR_ARG, "cirsradg_wave: isw must increase within 0..%d", nparam - 1);

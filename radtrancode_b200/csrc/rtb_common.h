@@ -13,6 +13,7 @@ constexpr int kMaxNg = 32;        // one lane per g-ordinate
 constexpr int kMaxCols = 8;       // tracked gradient columns in the overlap (active gases + T)
 constexpr int kMaxSw = 8;         // active Jacobian columns (isw) per spectrum
 constexpr int kMaxGasDev = 30;    // MAXGAS
+constexpr int kMaxPathDev = 4;    // paths of one spectrum per device work item (more: path groups)
 constexpr int kWarps = 4;         // warps per CTA of the forward kernel
 constexpr int kThreads = kWarps * 32;
 
@@ -87,8 +88,8 @@ struct SpecDev {
     int64_t map_off;      // map CSC: colptr index of (path 0, iv 0); [npath][nv+1]
     int64_t out_off;      // calcout/gradtsurf index of (path 0, wave 0)
     int64_t jac_off;      // gradients index of (path 0, iv 0, wave 0)
-    int nlayin[4];        // up to 4 paths per spectrum on the device path
-    int imod[4];
+    int nlayin[kMaxPathDev];  // the spectrum's paths in this group
+    int imod[kMaxPathDev];
     int isw[kMaxSw];      // active parameters (0-based param ids)
     int col_of_param[kMaxSw]; // tracked overlap column of isw[s] (-1: continuum only)
     int col_gas[kMaxCols];    // gas index of tracked column c (ngas = temperature)

@@ -640,3 +640,62 @@ def test_stellar_spectrum_file(tmp_path):
         with pytest.raises(cirsradg.RtbError, match="wavespace"):
             c2.load_stellar_spectrum(str(path), 1)
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def _many_paths(npath=10, nlayer=24, nwave=5):
+    """npath paths over one atmosphere: nadir-like paths at growing air
+    masses (IMOD 3 through the column, 0 and 1 through its upper half, in
+    turn) and every fourth a limb path down to
+    a tangent layer and up again (cirsradg_wave.f:983-988 skips its
+    surface term)."""
+    kt, cia, _ = synth.config2(nwave=nwave, nlayer=nlayer, nbin=nwave)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=nlayer, seed=51, nwave=nwave)
+    L = nlayer
+    ld = 2 * L
+    lay = np.zeros((ld, npath), np.int32, order="F")
+    sc = np.zeros((ld, npath), np.float32, order="F")
+    em = np.ones((ld, npath), np.float32, order="F")
+    nl = np.zeros(npath, np.int32)
+    imod = np.zeros(npath, np.int32)
+    for p in range(npath):
+        if p % 4 == 3:
+            tang = 4 + p // 4
+            half = np.arange(L, tang - 1, -1)
+            path = np.concatenate([half, half[::-1]])
+            imod[p] = 3
+        else:
+            imod[p] = (3, 0, 1)[p % 3]
+            # transmission and absorption paths through the upper half only: over
+            # the whole column 1 - A falls below 1e-13, where even the FP64
+            # oracle's 1 - (1 - T) loses digits
+            path = job.layinc[:L, 0].copy() if imod[p] == 3 else job.layinc[:L // 2, 0].copy()
+        n = path.size
+        lay[:n, p] = path
+        sc[:n, p] = 1.0 + 0.15 * p
+        em[:n, p] = job.temp[path - 1]
+        nl[p] = n
+    pad = lambda a, fill: np.asfortranarray(np.concatenate([a[:L], np.full((ld - L,) + a.shape[1:], fill, a.dtype)]))
+    job = dataclasses.replace(job, npath=npath, ld_lay=ld, layinc=lay, scale=sc, emtemp=em, nlayin=nl, imod=imod,
+                              press=job.press, temp=job.temp, delh=job.delh, pp=pad(job.pp, 0),
+                              amount=pad(job.amount, 0), dte=pad(job.dte, 0), dam=pad(job.dam, 0))
+    job.tsurf = 160.0
+    return kt, cia, job
+
+
+def test_many_paths_in_groups(ctx, oracle):
+    """A spectrum of 10 paths (limb sets run many tangent paths per
+    spectrum; the device takes them in groups of four): every path's
+    radiance, Jacobian and surface gradient within tolerance of the FP64
+    oracle, and the same result alone and in a batch beside a one-path
+    spectrum."""
+    kt, cia, job = _many_paths()
+    c, g, gt = _run(ctx, kt, cia, job)
+    c64, g64, gt64 = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.npath * job.nv) <= JAC_TOL
+    assert np.max(np.abs(gt - gt64)) <= RAD_TOL * np.max(np.abs(gt64))
+    one = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=24, seed=52, nwave=5)
+    c1, g1, _ = ctx.cirsrtfg_wave(one)
+    outs = ctx.cirsrtfg_wave_batch([one, job, one])
+    assert np.array_equal(outs[1][0], c) and np.array_equal(outs[1][1], g) and np.array_equal(outs[1][2], gt)
+    assert np.array_equal(outs[0][0], c1) and np.array_equal(outs[2][1], g1)

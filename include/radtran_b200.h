@@ -580,16 +580,19 @@ int rtb_spd_inverse_batch(rtb_context* ctx, int nret, int n, const double* a, do
  *                 and pp those of `atm` times vmr / vmr_atm (vmr_atm = pp /
  *                 press), xmap row (l, gas, level l) = vmr
  * so nx = nlayer + nscale + nprof * nlayer.  `atm` is the atmosphere at scale factor 1 (its
- * temp is replaced by x, emtemp follows temp through layinc); it must have
- * one path, and its xmap must hold the matching derivatives (T rows 1, gas
- * rows the gas's vmr per level).  Host pointers; read during the call only. */
+ * temp is replaced by x, emtemp follows temp through layinc of every path);
+ * each of its paths has at most nlayer positions, and its xmap must hold the
+ * matching derivatives (T rows 1, gas rows the gas's vmr per level).  Host
+ * pointers; read during the call only. */
 typedef struct rtb_retrieval_spec {
     const rtb_atm* atm;
     int nscale;
     const int* scale_gas;     /* [nscale] 0-based gas index into atm */
-    const float* y;           /* [ny] measurement, ny = atm->nwave; with channels
-                                 (atm->conv, any FWHM) ny = atm->conv->nconv: every
-                                 spectrum and Jacobian row is convolved onto them */
+    const float* y;           /* [ny] measurement: ny = npath x nwave, one spectrum per
+                                 path, path after path (the level-state model has one
+                                 path); with channels (atm->conv, any FWHM) nconv in
+                                 place of nwave: every spectrum and Jacobian row is
+                                 convolved onto them */
     const double* sei;        /* [ny] diagonal of Se^-1 */
     const double* sa;         /* [nx][nx] a priori covariance */
     const float* xa;          /* [nx] a priori state */

@@ -20,7 +20,7 @@ namespace {
 // compact copy of the atmosphere at scale factor 1 and its state layout
 struct Work {
     rtb_atm a{};
-    int L = 0, NV = 0, nparam = 0, NW = 0;
+    int L = 0, NV = 0, nparam = 0, NW = 0, NP = 1;   /* NP paths: y and K hold them path after path */
     /* the measurement's channels (cirsrtfg_wave.f:520-560 convolves the
      * spectrum and every Jacobian row onto them); NY = nconv, or NW */
     int NY = 0;
@@ -166,8 +166,10 @@ int at_level_state(Work& w, const float* x) {
 
 int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     const rtb_atm& t = *s.atm;
-    if (t.npath != 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont < 0)
+    if (t.npath < 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont < 0)
         return RTB_ERR_UNSUPPORTED;
+    for (int p = 0; p < t.npath; ++p)
+        if (t.nlayin[p] > t.nlayer) return RTB_ERR_UNSUPPORTED;
     const int L = t.nlayer, G = t.ngas, NV = t.nv, NW = t.nwave;
     const int ldl = t.ld_lay > 0 ? t.ld_lay : RTB_MAXLAY;
     const int ldv = t.ld_v > 0 ? t.ld_v : RTB_MAXV;
@@ -190,15 +192,17 @@ int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     col(t.delh, 1, w.delh);
     col(t.pp, G, w.pp0);
     col(t.amount, G, w.amount0);
-    col(t.scale, 1, w.scale);
-    col(t.emtemp, 1, w.emtemp);
+    w.NP = t.npath;
+    col(t.scale, w.NP, w.scale);
+    col(t.emtemp, w.NP, w.emtemp);
     col(t.dte, L, w.dte);
     col(t.dam, L, w.dam);
     if (t.ncont > 0 && t.dco) col(t.dco, L, w.dco);
     w.pp = w.pp0;
     w.amount = w.amount0;
-    w.layinc.resize(L);
-    for (int i = 0; i < L; ++i) w.layinc[i] = t.layinc[i];
+    w.layinc.resize((size_t)L * w.NP);
+    for (int p = 0; p < w.NP; ++p)
+        for (int i = 0; i < L; ++i) w.layinc[i + (size_t)L * p] = t.layinc[i + (size_t)ldl * p];
     w.xmap0.resize((size_t)NV * w.nparam * L);
     for (int k = 0; k < L; ++k)
         for (int j = 0; j < w.nparam; ++j)
@@ -212,8 +216,8 @@ int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     w.idgas.assign(t.idgas, t.idgas + G);
     w.isogas.assign(t.isogas, t.isogas + G);
     w.ktab.assign(t.ktab, t.ktab + G);
-    w.nlayin.assign(t.nlayin, t.nlayin + 1);
-    w.imod.assign(t.imod, t.imod + 1);
+    w.nlayin.assign(t.nlayin, t.nlayin + w.NP);
+    w.imod.assign(t.imod, t.imod + w.NP);
     w.a = t;
     w.a.ld_lay = L;
     w.a.ld_v = NV;
@@ -244,7 +248,8 @@ void at_state(Work& w, const float* x) {
     if (w.level) return;   /* forward() re-layers through at_level_state */
     const int L = w.L;
     for (int l = 0; l < L; ++l) w.temp[l] = x[l];
-    for (int j = 0; j < w.nlayin[0]; ++j) w.emtemp[j] = w.temp[w.layinc[j] - 1];
+    for (int p = 0; p < w.NP; ++p)
+        for (int j = 0; j < w.nlayin[p]; ++j) w.emtemp[j + (size_t)L * p] = w.temp[w.layinc[j + (size_t)L * p] - 1];
     const int ns = (int)w.sg.size();
     for (int a = 0; a < ns; ++a) {
         const int g = w.sg[a];
@@ -287,6 +292,7 @@ int setup(const rtb_retrieval_spec& s, Work& w) {
     } else if (t.fwhm != 0.0f) {
         return RTB_ERR_ARG;
     }
+    w.NY *= w.NP;   /* the measurement: every path's spectrum, path after path */
     w.a.fwhm = 0.0f;
     w.a.conv = nullptr;
     return w.NV < w.NY ? RTB_OK : RTB_ERR_UNSUPPORTED;
@@ -301,25 +307,35 @@ int forward(const orc_tables* tab, Work& w, const float* x, int precision, int n
     } else {
         at_state(w, x);
     }
-    std::vector<double> c(w.NW), g((size_t)w.NV * w.NW);
+    const int NP = w.NP, NW = w.NW, NV = w.NV;
+    std::vector<double> c((size_t)NP * NW), g((size_t)NP * NV * NW);   /* [path][wave], [path][iv][wave] */
     const int r = orc_cirsrtfg_wave_mt(tab, &w.a, precision, c.data(), g.data(), nullptr, nthreads);
     if (r) return r;
-    yn.resize(w.NW);
-    kk.resize((size_t)w.NV * w.NW);
-    for (int i = 0; i < w.NW; ++i) yn[i] = (float)c[i];
-    for (size_t i = 0; i < g.size(); ++i) kk[i] = (float)g[i];   /* gradients(iv*ny + iw) = kk(iw, iv) */
-    if (w.cv) {   /* cirsconv of the spectrum and of each Jacobian row onto the channels */
+    /* per path: the spectrum and the Jacobian rows, cirsconv'd onto the channels when there are any */
+    const int ny1 = w.NY / NP;
+    yn.resize(w.NY);
+    kk.resize((size_t)NV * w.NY);   /* kk[iv * NY + p * ny1 + i] */
+    std::vector<float> src(NW), dst(ny1);
+    auto conv1 = [&](const std::vector<float>& in, std::vector<float>& out) {
+        if (!w.cv) {
+            std::copy(in.begin(), in.begin() + ny1, out.begin());
+            return 0;
+        }
         const rtb_conv& v = *w.cv;
-        std::vector<float> yc(w.NY), kc((size_t)w.NV * w.NY);
-        int e = orc_cirsconv_ex(w.fwhm, w.NW, w.vwave.data(), yn.data(), v.nconv, v.vconv, v.nfwhm, v.vfwhm,
-                                v.xfwhm, v.nfil, v.vcen, v.nsub, v.vfil, v.fil, yc.data());
-        for (int iv = 0; iv < w.NV && !e; ++iv)
-            e = orc_cirsconv_ex(w.fwhm, w.NW, w.vwave.data(), kk.data() + (size_t)iv * w.NW, v.nconv, v.vconv,
-                                v.nfwhm, v.vfwhm, v.xfwhm, v.nfil, v.vcen, v.nsub, v.vfil, v.fil,
-                                kc.data() + (size_t)iv * w.NY);
+        return orc_cirsconv_ex(w.fwhm, NW, w.vwave.data(), in.data(), v.nconv, v.vconv, v.nfwhm, v.vfwhm, v.xfwhm,
+                               v.nfil, v.vcen, v.nsub, v.vfil, v.fil, out.data());
+    };
+    for (int p = 0; p < NP; ++p) {
+        for (int i = 0; i < NW; ++i) src[i] = (float)c[(size_t)p * NW + i];
+        int e = conv1(src, dst);
         if (e) return e;
-        yn.swap(yc);
-        kk.swap(kc);
+        std::copy(dst.begin(), dst.end(), yn.begin() + (size_t)p * ny1);
+        for (int iv = 0; iv < NV; ++iv) {
+            for (int i = 0; i < NW; ++i) src[i] = (float)g[((size_t)p * NV + iv) * NW + i];
+            e = conv1(src, dst);
+            if (e) return e;
+            std::copy(dst.begin(), dst.end(), kk.begin() + (size_t)iv * w.NY + (size_t)p * ny1);
+        }
     }
     return RTB_OK;
 }

@@ -61,7 +61,8 @@ struct AtmWork {
     // rows convolved by cirsconv onto them (cirsrtfg_wave.f:520-560)
     ConvSpec conv;
     bool has_conv = false;
-    int ny = 0;                 // measurement points: nconv, or nwave without channels
+    int ny = 0;                 // measurement points: npath x (nconv, or nwave without channels)
+    int npath = 1;              // paths of the layer-state model, measured one after the other
 };
 
 // the channels of a retrieval's atmosphere (FWHM and rtb_conv as
@@ -90,9 +91,14 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     const int ldv = t.ld_v > 0 ? t.ld_v : RTB_MAXV;
     const int ldp = t.ld_param > 0 ? t.ld_param : (RTB_MAXGAS + 2 + RTB_MAXCON);
     const int nparam = G + 1 + NC;
-    if (NP != 1) return fail(c, RTB_ERR_UNSUPPORTED, "retrieval atmosphere must have one path (npath=%d)", NP);
+    if (NP < 1 || NP > RTB_MAXPAT || !t.nlayin) return fail(c, RTB_ERR_ARG, "retrieval atmosphere: npath=%d", NP);
+    for (int p = 0; p < NP; ++p)
+        if (t.nlayin[p] < 1 || t.nlayin[p] > L)
+            return fail(c, RTB_ERR_UNSUPPORTED, "retrieval path %d has %d positions (1..nlayer=%d)", p, t.nlayin[p], L);
     if (!t.vwave) return fail(c, RTB_ERR_ARG, "NULL input array in retrieval atmosphere");
     if (const int r = work_channels(c, t, w)) return r;
+    w.npath = NP;
+    w.ny *= NP;   // y: every path's spectrum, path after path
     if (NPRO != L) return fail(c, RTB_ERR_UNSUPPORTED, "layer-state model needs npro == nlayer");
     if (s.nprof < 0 || (s.nprof > 0 && !s.prof_gas)) return fail(c, RTB_ERR_ARG, "nprof/prof_gas");
     if (NV != L + s.nscale + s.nprof * L)
@@ -203,8 +209,8 @@ int set_state(rtb_context* c, AtmWork& w, const float* x) {
     if (w.level) return set_level_state(c, w, x);
     const int L = w.a.nlayer, NV = w.a.nv, NPRO = w.a.npro, nparam = w.nparam;
     for (int l = 0; l < L; ++l) w.temp[l] = x[l];
-    const int nl = w.nlayin[0];
-    for (int j = 0; j < nl; ++j) w.emtemp[j] = w.temp[w.layinc[j] - 1];
+    for (int p = 0; p < w.npath; ++p)
+        for (int j = 0; j < w.nlayin[p]; ++j) w.emtemp[j + (size_t)L * p] = w.temp[w.layinc[j + (size_t)L * p] - 1];
     const int ns = (int)w.scale_gas.size();
     for (int a = 0; a < ns; ++a) {
         const int g = w.scale_gas[a];
@@ -417,7 +423,8 @@ struct Slot {
     double t_submit = 0, t_done = 0;
     rtb_retrieval_result res{};
     AtmWork w;
-    int nraw = 0;                     // calculation points of the raw outputs when the spectrum is convolved
+    int nraw = 0;                     // calculation points of the raw outputs (channels or several paths)
+    int np = 1;                       // paths measured one after the other
     // arena layout (element offsets from the block start)
     int64_t k_elems() const { return 2 * (int64_t)nx * ny; }
     int64_t y_elems() const { return 3 * al4(ny); }
@@ -430,10 +437,27 @@ size_t slot_core_bytes(int nx, int ny) {
 }
 
 // K and the spectra of two states, y, Se^-1, the Newton work, Sa^-1 and Sa;
-// with channels, after them the unconvolved spectrum and Jacobian of the
-// state being evaluated, [nraw] then [nx][nraw]
-size_t slot_bytes(int nx, int ny, int nraw) {
-    return slot_core_bytes(nx, ny) + (((size_t)(al4(nraw) + (int64_t)nx * nraw) * 4 + 255) & ~(size_t)255);
+// with channels or several paths, after them the forward model's own
+// outputs for the state being evaluated, [np][nraw] then [np][nx][nraw],
+// and with both, the convolved Jacobian [np][nx][ny / np] before its rows
+// are laid into K
+int64_t raw_floats(int nx, int ny, int nraw, int np, bool conv) {
+    int64_t f = al4((int64_t)np * nraw) + (int64_t)np * nx * nraw;
+    if (conv && np > 1) f = al4(f) + (int64_t)nx * ny;
+    return f;
+}
+
+size_t slot_bytes(int nx, int ny, int nraw, int np, bool conv) {
+    return slot_core_bytes(nx, ny) + (((size_t)raw_floats(nx, ny, nraw, np, conv) * 4 + 255) & ~(size_t)255);
+}
+
+// the arena block of one retrieval, from its specification alone
+size_t spec_bytes(const rtb_retrieval_spec& sp) {
+    const rtb_atm& t = *sp.atm;
+    const int np = sp.prof ? 1 : std::max(t.npath, 1);
+    const bool conv = t.conv && t.conv->nconv > 0;
+    const int ny = np * (conv ? t.conv->nconv : t.nwave);
+    return (conv || np > 1) ? slot_bytes(t.nv, ny, t.nwave, np, conv) : slot_core_bytes(t.nv, ny);
 }
 
 // coreret.f:621-700 and :757-766: the next trial state, or its rejection
@@ -599,8 +623,10 @@ struct Engine {
         for (int l = 0; l < s->nlayer; ++l) s->kind[l] = 0;
         for (int a = 0; a < sp.nscale; ++a) s->kind[s->nlayer + a] = (sp.scale_model && sp.scale_model[a] == 2) ? 2 : 1;
         s->ny = s->w.ny;
-        s->nraw = s->w.has_conv ? sp.atm->nwave : 0;
-        s->bytes = s->w.has_conv ? slot_bytes(s->nx, s->ny, s->nraw) : slot_core_bytes(s->nx, s->ny);
+        s->np = s->w.level ? 1 : s->w.npath;
+        const bool raw = s->w.has_conv || s->np > 1;
+        s->nraw = raw ? sp.atm->nwave : 0;
+        s->bytes = raw ? slot_bytes(s->nx, s->ny, s->nraw, s->np, s->w.has_conv) : slot_core_bytes(s->nx, s->ny);
         if (s->bytes > budget) {
             const size_t need = s->bytes;
             delete s;
@@ -712,9 +738,9 @@ struct Engine {
             if (rs) return rs;
             atms.push_back(s->w.a);
             const int b = first ? s->cur : 1 - s->cur;
-            if (s->w.has_conv) {   // raw outputs, convolved below into Yn and K
+            if (s->nraw) {   // own outputs, convolved and / or laid out below into Yn and K
                 oo.push_back(Raw(*s) - F());
-                jo.push_back(Raw(*s) + al4(s->nraw) - F());
+                jo.push_back(Raw(*s) + al4((int64_t)s->np * s->nraw) - F());
             } else {
                 oo.push_back(Yn(*s, b) - F());
                 jo.push_back(K(*s, b) - F());
@@ -731,13 +757,34 @@ struct Engine {
         if (r) return r;
         r = launch(c);
         if (r) return r;
-        for (const Slot* s : v)
-            if (s->w.has_conv) {
-                const int b = s->phase == 0 ? s->cur : 1 - s->cur;
-                const ConvSeg seg[2] = {{Raw(*s), 1, Yn(*s, b)}, {Raw(*s) + al4(s->nraw), s->nx, K(*s, b)}};
+        for (const Slot* s : v) {
+            if (!s->nraw) continue;
+            const int b = s->phase == 0 ? s->cur : 1 - s->cur;
+            const int np = s->np, ny1 = s->ny / np;
+            float* ro = Raw(*s);
+            float* rj = ro + al4((int64_t)np * s->nraw);
+            float* kb = K(*s, b);
+            if (s->w.has_conv && np == 1) {   // straight onto the channels: K's rows are the series
+                const ConvSeg seg[2] = {{ro, 1, Yn(*s, b)}, {rj, s->nx, kb}};
                 r = conv_run(c, s->w.conv, 2, seg, st);
                 if (r) return r;
+                continue;
             }
+            // y_p follows y_{p-1}; K's row iv holds path 0's ny1 points, then path 1's, ...
+            const float* jrow = rj;   // [np][nx][ny1] after the convolution, else the raw [np][nx][nraw]
+            if (s->w.has_conv) {
+                float* tmp = rj + al4((int64_t)np * s->nx * s->nraw);
+                const ConvSeg seg[2] = {{ro, np, Yn(*s, b)}, {rj, np * s->nx, tmp}};
+                r = conv_run(c, s->w.conv, 2, seg, st);
+                if (r) return r;
+                jrow = tmp;
+            } else {
+                CUDA_TRY(c, cudaMemcpyAsync(Yn(*s, b), ro, (size_t)np * s->nraw * 4, cudaMemcpyDeviceToDevice, st));
+            }
+            for (int p = 0; p < np; ++p)
+                CUDA_TRY(c, cudaMemcpy2DAsync(kb + (size_t)p * ny1, (size_t)s->ny * 4, jrow + (size_t)p * s->nx * ny1,
+                                              (size_t)ny1 * 4, (size_t)ny1 * 4, s->nx, cudaMemcpyDeviceToDevice, st));
+        }
         CUDA_TRY(c, cudaStreamSynchronize(st));
         unsigned long long diag[8];
         CUDA_TRY(c, cudaMemcpy(diag, c->d_diag.p, 64, cudaMemcpyDeviceToHost));
@@ -1034,9 +1081,7 @@ int rtb_retrieve_batch(rtb_context* c, int nret, const rtb_retrieval_spec* specs
     std::vector<size_t> sz(nret);
     for (int i = 0; i < nret; ++i) {
         if (!specs[i].atm) return fail(c, RTB_ERR_ARG, "retrieval %d: NULL atmosphere", i);
-        const rtb_atm& t = *specs[i].atm;
-        sz[i] = (t.conv && t.conv->nconv > 0) ? slot_bytes(t.nv, t.conv->nconv, t.nwave)
-                                              : slot_core_bytes(t.nv, t.nwave);
+        sz[i] = spec_bytes(specs[i]);
     }
     std::sort(sz.begin(), sz.end(), std::greater<size_t>());
     const int m = o.max_batch > 0 ? std::min(o.max_batch, nret) : nret;

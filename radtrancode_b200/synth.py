@@ -647,7 +647,7 @@ class RetrievalCase:
 
     @property
     def ny(self):
-        return self.job.nconv
+        return self.job.npath * self.job.nconv
 
     def as_struct(self):
         s = _abi.RtbRetrievalSpec()
@@ -777,6 +777,24 @@ def with_channels(case: RetrievalCase, fwhm, channels: Channels, noise=1e-9) -> 
     on the channels."""
     job = dataclasses.replace(case.job, fwhm=float(fwhm), conv=channels)
     return dataclasses.replace(case, job=job, y=None, sei=np.full(job.nconv, 1.0 / (noise * noise)))
+
+
+def with_paths(case: RetrievalCase, airmass, noise=1e-9) -> RetrievalCase:
+    """The case measured along several paths at once (emission angles of one
+    footprint): the job's path repeated with its scale factors times each
+    airmass; y holds one spectrum per path, path after path."""
+    j = case.job
+    npth = len(airmass)
+    lay = np.zeros((j.ld_lay, npth), np.int32, order="F")
+    sc = np.zeros((j.ld_lay, npth), np.float32, order="F")
+    em = np.zeros((j.ld_lay, npth), np.float32, order="F")
+    for p, f in enumerate(airmass):
+        lay[:, p] = j.layinc[:, 0]
+        sc[:, p] = j.scale[:, 0] * np.float32(f)
+        em[:, p] = j.emtemp[:, 0]
+    job = dataclasses.replace(j, npath=npth, layinc=lay, scale=sc, emtemp=em,
+                              nlayin=np.full(npth, j.nlayin[0], np.int32), imod=np.full(npth, j.imod[0], np.int32))
+    return dataclasses.replace(case, job=job, y=None, sei=np.full(npth * job.nconv, 1.0 / (noise * noise)))
 
 
 def observe(case: RetrievalCase, spectrum, seed, noise=1e-9):

@@ -304,3 +304,32 @@ def test_retrieval_with_dust_background(ctx, oracle):
     sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
     assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
     assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
+
+
+@pytest.mark.parametrize("mode", ["three_paths", "two_paths_channels"])
+def test_retrieval_over_several_paths(ctx, oracle, mode):
+    """One footprint seen along several paths at once (air masses 1, 1.4,
+    2; y holds one spectrum per path, path after path, as cirsrtfg_wave
+    packs them), on the calculation grid or on channels: same iterations,
+    forward evaluations and stop rule as the oracle's coreret loop, states
+    within 1e-3 prior sigma, cost within 1e-3."""
+    kt, cia, _ = synth.config2()
+    case = synth.make_retrieval(kt, [synth.CH4, synth.NH3], nlayer=30, seed=61, nwave=150)
+    if mode == "two_paths_channels":
+        vc = (case.job.vwave[0] + 2.1 + np.arange(0, 55, 0.8)).astype(np.float32)
+        case = synth.with_channels(case, 1.6, synth.Channels(vconv=vc))
+        case = synth.with_paths(case, [1.0, 1.8])
+    else:
+        case = synth.with_paths(case, [1.0, 1.4, 2.0])
+    assert case.ny == case.job.npath * case.job.nconv
+    y_true, _ = oracle.forward_state(kt, cia, case, case.x_true, nthreads=8)
+    synth.observe(case, y_true, seed=62)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    g = ctx.retrieve_batch([case], kiter=10, phlimit=0.1)[0]
+    ref, _ = oracle.retrieve(kt, cia, case, kiter=10, phlimit=0.1, nthreads=8)
+    assert (g["converged"], g["iterations"], g["forwards"]) == (ref["converged"], ref["iterations"], ref["forwards"])
+    sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
+    assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
+    assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
+    assert g["yn"].shape == (case.ny,)

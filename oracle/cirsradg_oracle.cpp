@@ -1026,6 +1026,34 @@ float interpem(int nem, const float* vem, const float* em, float v, int* err) {
 
 /* RAYLEIGHJ: radtran/scatter/rayleighj.f:1-35 with faniso(0) = 1
  * (radtran/scatter/rayleigha.f:55-63). */
+/* RAYLEIGHV: radtran/scatter/rayleighv.f:1-12 (Venus, C / lambda^4) */
+float rayleighv(float v) {
+    const float C = 8.8E-28f;
+    float lambda = 10000.0f / v;
+    const float l2 = lambda * lambda;   /* lambda**4 as gfortran expands it */
+    lambda = l2 * l2;
+    return C / lambda;
+}
+
+/* RAYLEIGHA: radtran/scatter/rayleigha.f:1-38 (air at the layer's P, T) */
+float rayleigha(float v, float P, float T) {
+    const float c1 = 8342.12f, c2 = 2406030.0f, c3 = 15997.0f, delta = 0.035f, pi = 3.1415927f, k = 1.37971e-23f;
+    float lambda = 1e4f / v;
+    const float nu2 = 1.0f / (lambda * lambda);
+    float m1 = c1 + c2 / (130.0f - nu2) + c3 / (38.9f - nu2);
+    m1 = m1 * 1e-8f;
+    const float P1 = P * 1.013e5f, T1 = T - 273.15f;
+    const float xcorr = P1 * (1.0f + P1 * (61.3f - T1) * 1E-10f) / (96095.4f * (1.0f + 0.003661f * T1));
+    m1 = m1 * xcorr;
+    const float Ns = P1 / (k * T);
+    lambda = lambda * 1e-6f;
+    const float x = Ns * lambda * lambda;
+    const float mm = m1 * (m1 + 2.0f);
+    const float temp = 8.0f * (pi * pi * pi) * (mm * mm);
+    const float faniso = (6.0f + 3.0f * delta) / (6.0f - 7.0f * delta);
+    return temp * 1e4f * faniso / (3.0f * (x * x));
+}
+
 float rayleighj(float v) {
     const float AH2 = 13.58E-5f, BH2 = 7.52E-3f, AHe = 3.48E-5f, BHe = 2.30E-3f;
     const float pi = 3.1415927f, fH2 = 0.864f, k = 1.37971e-23f, P0 = 1.013e5f, T0 = 273.15f;
@@ -1071,7 +1099,7 @@ int validate(const orc_tables& t, const rtb_atm& a, const Dims& d) {
     if (t.solar_npt == 1 || (t.solar_npt > 1 && (!t.solar_wave || !t.solar_rad))) return RTB_ERR_ARG;
     if (a.inlte == 1 && !(a.nlte_k1 >= 1.0e-20f && a.nlte_k1 <= 1.0e-3f)) return RTB_ERR_ARG;   /* calc_nlte_t.f:17-20 */
     if (a.ncont < 0 || (a.ncont > 0 && (!a.cont || !a.xsec_ext))) return RTB_ERR_ARG;
-    if (a.iray > 1) return RTB_ERR_UNSUPPORTED;
+    if (a.iray > 3) return RTB_ERR_UNSUPPORTED;   /* rayleighls reads FRAC of gases it may not have */
     for (int k = 0; k < a.ngas; ++k) {
         if (a.idgas[k] == 91 || a.idgas[k] == 48 || a.idgas[k] == 80) return RTB_ERR_UNSUPPORTED;
         if (a.ktab[k] >= t.ntab) return RTB_ERR_ARG;
@@ -1165,7 +1193,8 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
         for (int l = 0; l < nlayer; ++l)
             get_kg_layer<R>(t, bs, tab1, tab2, LK[l], delg.data(), ko + (size_t)l * ng, dko + (size_t)l * ng);
     }
-    const float xray = (a.iray > 0 && a.itype != 0) ? rayleighj(vv) * 1E20f : 0.0f;
+    /* :663-680: Jovian (1) or Venus (2) per wavenumber; air (3) per layer below */
+    const float xray = (a.iray > 0 && a.itype != 0) ? (a.iray == 2 ? rayleighv(vv) : rayleighj(vv)) * 1E20f : 0.0f;
     std::vector<R> amo(ngas), kgn((size_t)ngas * ng), dkgn((size_t)ngas * ng), aam(ngas), ppp(ngas);
     std::vector<R> k_g(ng), dkdq((size_t)(ngas + 1) * ng);
     /* layer loop: cirsradg_wave.f:510-760 */
@@ -1207,10 +1236,11 @@ int one_wave(const orc_tables& t, const rtb_atm& a, const Dims& d, const std::ve
         }
         dtc[ngas] = dtc[ngas] + dabs[5];
         if (a.flagh2p == 1) dtc[nparam - 1] = dtc[nparam - 1] + dabs[6];   /* :659-661 */
-        if (a.iray > 0 && a.itype != 0) {                        /* :663-691 (IRAY=1) */
-            const R av = W.utotl[j] * (R)xray;
+        if (a.iray > 0 && a.itype != 0) {                        /* :663-691 */
+            const float xr = a.iray == 3 ? rayleigha(vv, a.press[j], a.temp[j]) * 1E20f : xray;
+            const R av = W.utotl[j] * (R)xr;
             taucon = taucon + av;
-            for (int k = 0; k < ngas; ++k) dtc[k] = dtc[k] + (R)xray * (R)1.0e-20f;
+            for (int k = 0; k < ngas; ++k) dtc[k] = dtc[k] + (R)xr * (R)1.0e-20f;
         }
         W.taucon[j] = taucon;
         /* gather and overlap: :703-753 */

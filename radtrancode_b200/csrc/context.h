@@ -83,7 +83,8 @@ struct Staging {
     std::vector<float> map_val;
     std::vector<ParaLayDev> para_lay;
     std::vector<ParaWaveDev> para_wave;
-    std::vector<float> lpress;   // layer pressures (atm) of the spectra with non-LTE emission
+    std::vector<float> lpress;   // layer pressures (atm) of the spectra with non-LTE emission or air Rayleigh
+    std::vector<float> ltemp;    // layer temperatures (K) of the spectra with air Rayleigh
     std::vector<int> nsub;       // device spectra (path groups) of each caller spectrum, in order
     std::vector<float> wfac;     // get_solar_wave at each wavenumber of iform 1 / 4 spectra
     int Lmax = 0, nsw_max = 1, ncol_max = 1, nlmax_max = 1, npath_max = 1, ngas_max = 1;

@@ -455,6 +455,27 @@ __device__ __forceinline__ void cia_bilinear(const float* kc, int64_t e, int64_t
     dx = __fmul_rn(d, dudt);
 }
 
+// RAYLEIGHA (radtran/scatter/rayleigha.f:1-38): the Rayleigh cross section of
+// air at pressure P (atm) and temperature T, REAL arithmetic in its order
+__device__ __noinline__ float rayleigha_dev(float v, float P, float T) {
+    const float c1 = 8342.12f, c2 = 2406030.0f, c3 = 15997.0f, delta = 0.035f, pi = 3.1415927f, k = 1.37971e-23f;
+    float lambda = __fdiv_rn(1e4f, v);
+    const float nu2 = __fdiv_rn(1.0f, __fmul_rn(lambda, lambda));
+    float m1 = __fadd_rn(__fadd_rn(c1, __fdiv_rn(c2, __fsub_rn(130.0f, nu2))), __fdiv_rn(c3, __fsub_rn(38.9f, nu2)));
+    m1 = __fmul_rn(m1, 1e-8f);
+    const float P1 = __fmul_rn(P, 1.013e5f), T1 = __fsub_rn(T, 273.15f);
+    const float num = __fmul_rn(P1, __fadd_rn(1.0f, __fmul_rn(__fmul_rn(P1, __fsub_rn(61.3f, T1)), 1E-10f)));
+    const float xcorr = __fdiv_rn(num, __fmul_rn(96095.4f, __fadd_rn(1.0f, __fmul_rn(0.003661f, T1))));
+    m1 = __fmul_rn(m1, xcorr);
+    const float Ns = __fdiv_rn(P1, __fmul_rn(k, T));
+    lambda = __fmul_rn(lambda, 1e-6f);
+    const float x = __fmul_rn(__fmul_rn(Ns, lambda), lambda);
+    const float mm = __fmul_rn(m1, __fadd_rn(m1, 2.0f));
+    const float temp = __fmul_rn(__fmul_rn(8.0f, __fmul_rn(__fmul_rn(pi, pi), pi)), __fmul_rn(mm, mm));
+    const float faniso = __fdiv_rn(__fadd_rn(6.0f, __fmul_rn(3.0f, delta)), __fsub_rn(6.0f, __fmul_rn(7.0f, delta)));
+    return __fdiv_rn(__fmul_rn(__fmul_rn(temp, 1e4f), faniso), __fmul_rn(3.0f, __fmul_rn(x, x)));
+}
+
 // continuum optical depth of one layer and its active derivatives
 // (cirsradg_wave.f:526-691 with nciacon.f:84-310 / ciaread.f:108-198, or for
 // flagh2p = 1 nparacon_all.f:160-336 / fpread_all.f:195-266).  Lanes 0..8
@@ -627,9 +648,15 @@ __device__ __forceinline__ float continuum(const BatchDev& B, const SpecDev& S, 
             if (s == S.sw_para) dtc[s] = __fadd_rn(dtc[s], dab[6]);
     }
     if (S.iray) {
-        const float av = __fmul_rn(L.utotl, W.xray);
+        float xr = W.xray;
+        if (para && S.iray == 3) {   // air: rayleigha at this layer's P and T (cirsradg_wave.f:668-669)
+            const int64_t l = il_glob - S.lay_off;
+            const float vv = S.ispace ? __fdiv_rn(1e4f, W.vwave) : W.vwave;
+            xr = __fmul_rn(rayleigha_dev(vv, B.lay_press[S.lp_off + l], B.lay_temp[S.lt_off + l]), 1E20f);
+        }
+        const float av = __fmul_rn(L.utotl, xr);
         taucon = __fadd_rn(taucon, av);
-        const float add = __fmul_rn(W.xray, 1.0e-20f);
+        const float add = __fmul_rn(xr, 1.0e-20f);
 #pragma unroll
         for (int s = 0; s < kMaxSw; ++s)
             if (s < S.nsw && S.isw[s] < S.ngas) dtc[s] = __fadd_rn(dtc[s], add);

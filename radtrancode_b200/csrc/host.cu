@@ -125,6 +125,15 @@ int pindex_ascending(const float* x, int nx, float& x1) {
 }
 
 // RAYLEIGHJ (radtran/scatter/rayleighj.f) with faniso(0) = 1
+// RAYLEIGHV (radtran/scatter/rayleighv.f:1-12): Venus, C / lambda^4
+float rayleighv_f(float v) {
+    const float C = 8.8E-28f;
+    float lambda = 10000.0f / v;
+    const float l2 = lambda * lambda;
+    lambda = l2 * l2;
+    return C / lambda;
+}
+
 float rayleighj_f(float v) {
     const float AH2 = 13.58E-5f, BH2 = 7.52E-3f, AHe = 3.48E-5f, BHe = 2.30E-3f;
     const float pi = 3.1415927f, fH2 = 0.864f, k = 1.37971e-23f, P0 = 1.013e5f, T0 = 273.15f;
@@ -240,7 +249,8 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     if (a.inlte == 1 && !(a.nlte_k1 >= 1.0e-20f && a.nlte_k1 <= 1.0e-3f))   // calc_nlte_t.f:17-20
         return fail(c, RTB_ERR_ARG, "calc_nlte_t: k1=%g out of range", (double)a.nlte_k1);
     if (a.iform < 0 || a.iform > 4) return fail(c, RTB_ERR_UNSUPPORTED, "iform=%d", a.iform);
-    if (a.iray > 1) return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (only Jovian Rayleigh, iray=1)", a.iray);
+    if (a.iray > 3)   // rayleighls reads the layer fractions of gases the atmosphere may not hold
+        return fail(c, RTB_ERR_UNSUPPORTED, "iray=%d (Jovian 1, Venus 2 and air 3 only)", a.iray);
     if (a.ncont > 0 && (!a.cont || !a.xsec_ext || !a.dco)) return fail(c, RTB_ERR_ARG, "dust arrays missing");
     const int ng = c->ng;
     if (c->ntab <= 0) return fail(c, RTB_ERR_NOTABLE, "no k-tables loaded");
@@ -303,7 +313,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     S.sw_T = -1;
     S.ispace = a.ispace;
     S.inormal = a.inormal;
-    S.iray = (a.iray > 0 && a.itype != 0) ? 1 : 0;
+    S.iray = (a.iray > 0 && a.itype != 0) ? a.iray : 0;   // 1 Jovian, 2 Venus, 3 air (cirsradg_wave.f:663-680)
     S.has_cia = c->has_cia;
     S.tsurf_pos = a.tsurf > 0.0f ? 1 : 0;
     // iform 3: total spectral flux of the planet, x 1e-18 (cirsradg_wave.f:913-929, 1136-1152)
@@ -358,10 +368,12 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     S.nlte_k1 = a.nlte_k1;
     S.nlte_A = a.nlte_A;
     S.lp_off = (int64_t)st.lpress.size();
-    if (a.inlte != 0) {
+    if (a.inlte != 0 || S.iray == 3) {   // also rayleigha's P of each layer
         st.lpress.insert(st.lpress.end(), a.press, a.press + a.nlayer);
         st.any_ext = true;
     }
+    S.lt_off = (int64_t)st.ltemp.size();
+    if (S.iray == 3) st.ltemp.insert(st.ltemp.end(), a.temp, a.temp + a.nlayer);
     // ---- per-layer set-up ----
     S.lay_off = (int64_t)st.lay.size();
     S.lg_off = (int64_t)st.amo.size();
@@ -588,7 +600,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
             PW.t = (vv - vk2[cv - 1]) / (vk2[cv] - vk2[cv - 1]);
             st.para_wave.push_back(PW);
         }
-        W.xray = S.iray ? rayleighj_f(vv) * 1E20f : 0.0f;
+        W.xray = S.iray ? (S.iray == 2 ? rayleighv_f(vv) : rayleighj_f(vv)) * 1E20f : 0.0f;   // air (3): per layer
         if (a.tsurf > 0.0f) {
             float B, dB;
             planck_host(a.ispace, vwave, a.tsurf, B, dB);
@@ -837,6 +849,7 @@ void append_staging(Staging& dst, const Staging& src) {
         S.para_off += (int64_t)dst.para_lay.size();
         S.paraw_off += (int64_t)dst.para_wave.size();
         S.lp_off += (int64_t)dst.lpress.size();
+        S.lt_off += (int64_t)dst.ltemp.size();
         S.wf_off += (int64_t)dst.wfac.size();
         S.out_off += dst.n_out;
         S.jac_off += dst.n_jac;
@@ -859,6 +872,7 @@ void append_staging(Staging& dst, const Staging& src) {
     for (int v : src.map_colptr) dst.map_colptr.push_back(v + (int)rows);
     append_vec(dst.para_lay, src.para_lay);
     append_vec(dst.lpress, src.lpress);
+    append_vec(dst.ltemp, src.ltemp);
     append_vec(dst.nsub, src.nsub);
     append_vec(dst.wfac, src.wfac);
     append_vec(dst.para_wave, src.para_wave);
@@ -926,6 +940,7 @@ int pack_batch(rtb_context* c, int nspec, const rtb_atm* atms, Staging& st) {
     st.map_colptr.reserve(total(&Staging::map_colptr));
     st.para_lay.reserve(total(&Staging::para_lay));
     st.lpress.reserve(total(&Staging::lpress));
+    st.ltemp.reserve(total(&Staging::ltemp));
     st.wfac.reserve(total(&Staging::wfac));
     st.para_wave.reserve(total(&Staging::para_wave));
     for (int t = 0; t < nthr; ++t) append_staging(st, part[t]);
@@ -1008,6 +1023,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     const size_t i_parl = add(st.para_lay.data(), bytes_of(st.para_lay));
     const size_t i_parw = add(st.para_wave.data(), bytes_of(st.para_wave));
     const size_t i_lp = add(st.lpress.data(), bytes_of(st.lpress));
+    const size_t i_lt = add(st.ltemp.data(), bytes_of(st.ltemp));
     const size_t i_wf = add(st.wfac.data(), bytes_of(st.wfac));
     const size_t in_bytes = off + 256;
     CUDA_TRY(c, c->h_in.ensure(in_bytes));
@@ -1066,6 +1082,7 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
         B.para_wave = (const ParaWaveDev*)dp(i_parw);
     }
     B.lay_press = st.lpress.empty() ? nullptr : (const float*)dp(i_lp);
+    B.lay_temp = st.ltemp.empty() ? nullptr : (const float*)dp(i_lt);
     B.wave_fac = st.wfac.empty() ? nullptr : (const float*)dp(i_wf);
     if (place) {
         B.calcout = place->calcout;

@@ -70,13 +70,14 @@ struct SpecDev {
     float xfac3, xfac18;  // iform factor of the IMOD 3 and IMOD 18 paths (1 unless iform = 3)
     int inlte;            // non-LTE emission temperatures (calc_nlte_t.f): 0, 1 or 2
     float nlte_k1, nlte_A;
-    int64_t lp_off;       // lay_press index of layer 0 (inlte != 0)
+    int64_t lp_off;       // lay_press index of layer 0 (inlte != 0 or iray = 3)
+    int64_t lt_off;       // lay_temp index of layer 0 (iray = 3)
     int wmode;            // stellar factor per wavenumber: 0 none, 1 divides (iform 1), 2 multiplies IMOD 0 (iform 4)
     int64_t wf_off;       // wave_fac index of wavenumber 0 (wmode != 0)
     int nonlimb_mask;     // bit p: path p adds the surface term (cirsradg_wave.f:985-1000)
     int ispace;
     int inormal;
-    int iray;             // IRAY > 0 and ITYPE != 0
+    int iray;             // IRAY (1 Jovian, 2 Venus, 3 air) when ITYPE != 0, else 0
     int has_cia;
     int64_t lay_off;      // LayerDev index of layer 0
     int64_t lg_off;       // (layer, gas) arrays: index of (0,0); [nlayer][ngas]
@@ -139,7 +140,8 @@ struct BatchDev {
     const float* kcia5;          // (5,25,1501)
     const ParaLayDev* para_lay;
     const ParaWaveDev* para_wave;
-    const float* lay_press;      // [.. nlayer] layer pressures (atm) of non-LTE spectra
+    const float* lay_press;      // [.. nlayer] layer pressures (atm) of non-LTE / air-Rayleigh spectra
+    const float* lay_temp;       // [.. nlayer] layer temperatures (K) of air-Rayleigh spectra
     const float* wave_fac;       // [.. nwave] get_solar_wave of iform 1 / 4 spectra
     // per-CTA scratch slots (tau, dtau/dq of every layer of the current item)
     float* cell_scratch;

@@ -699,3 +699,22 @@ def test_many_paths_in_groups(ctx, oracle):
     outs = ctx.cirsrtfg_wave_batch([one, job, one])
     assert np.array_equal(outs[1][0], c) and np.array_equal(outs[1][1], g) and np.array_equal(outs[1][2], gt)
     assert np.array_equal(outs[0][0], c1) and np.array_equal(outs[2][1], g1)
+
+
+@pytest.mark.parametrize("iray", [2, 3])
+def test_rayleigh_venus_and_air(ctx, oracle, iray):
+    """IRAY 2 (Venus, per wavenumber on the host) and 3 (air at each
+    layer's P and T, on the device): radiance and Jacobian within tolerance
+    of the FP64 oracle, and in a batch beside IRAY 1 and 0 spectra each gets
+    its own result."""
+    kt, cia, _ = synth.config2(nwave=6, nlayer=30, nbin=6)
+    job = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=30, seed=61, nwave=6)
+    j = dataclasses.replace(job, iray=iray)
+    c, g, _ = _run(ctx, kt, cia, j)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, j.nv) <= JAC_TOL
+    j1 = dataclasses.replace(job, iray=1)
+    outs = ctx.cirsrtfg_wave_batch([j1, j, job])
+    assert np.array_equal(outs[1][0], c) and np.array_equal(outs[1][1], g)
+    assert np.array_equal(outs[0][0], ctx.cirsrtfg_wave(j1)[0]) and np.array_equal(outs[2][0], ctx.cirsrtfg_wave(job)[0])

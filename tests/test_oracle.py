@@ -506,3 +506,22 @@ def test_real_stellar_spectrum_file(oracle):
     pi = float(np.float32(np.pi))
     sph = 4.0 * pi * (3.0 * 1.49598e13) ** 2
     assert np.all(t0 > 0) and np.max(np.abs(t4 * sph / xs / t0 - 1.0)) < 1e-5
+
+
+def test_rayleigh_venus_and_air(oracle):
+    """IRAY 2 (rayleighv.f, C / lambda^4 per wavenumber) and 3 (rayleigha.f,
+    air at each layer's P and T): the two precisions agree, the scattering
+    optical depth dims the spectrum against IRAY 0, and IRAY 4 (rayleighls,
+    whose layer fractions the reference leaves unset for absent gases) is
+    refused."""
+    import dataclasses
+    kt, cia, job = synth.config2(nwave=4, nlayer=30, nbin=4)
+    c0, _, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    for iray in (2, 3):
+        j = dataclasses.replace(job, iray=iray)
+        cm, gm, _ = oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_MIXED)
+        c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, j, oracle.ORC_FP64)
+        assert rad_err(cm, c64) < 1e-5 and jac_err(gm, g64, j.nv) < 1e-4
+        assert np.all(c64 <= c0) and np.any(c64 < c0)
+    with pytest.raises(RuntimeError, match="UNSUPPORTED"):
+        oracle.cirsrtfg_wave(kt, cia, dataclasses.replace(job, iray=4), oracle.ORC_FP64)

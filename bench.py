@@ -92,7 +92,9 @@ def algorithmic_bytes(kt, job, in_bytes, out_bytes):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """Clock and throttle-reason samples during the timed region: NVML read
+    in-process every 20 ms (the timed region lasts a fraction of a second),
+    else nvidia-smi every 200 ms.  Reads only; no GPU setting is changed."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -102,7 +104,40 @@ class ClockSampler:
         self.proc = None
         self.f = None
 
+    # clocks-event reason bits of NVML (nvml.h): sw power cap, hw slowdown,
+    # sw thermal, hw thermal
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
+
+    def _nvml_start(self):
+        import threading
+
+        import pynvml
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+        self.nv_max = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        self.nv_rows = []
+        self.nv_stop = threading.Event()
+
+        def loop():
+            while not self.nv_stop.is_set():
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                    self.nv_rows.append((sm, rs))
+                except Exception:
+                    pass
+                self.nv_stop.wait(0.02)
+
+        self.nv_thread = threading.Thread(target=loop, daemon=True)
+        self.nv_thread.start()
+
     def start(self):
+        self.nv_thread = None
+        try:
+            self._nvml_start()
+            return
+        except Exception:
+            self.nv_thread = None
         try:
             self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
@@ -112,6 +147,15 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.nv_thread is not None:
+            self.nv_stop.set()
+            self.nv_thread.join(timeout=2)
+            rows = list(self.nv_rows)
+            if not rows:
+                return None
+            reasons = sorted(n for n, b in self.BITS.items() if any(r & b for _, r in rows))
+            return {"sm_mhz": statistics.median(s for s, _ in rows), "sm_max_mhz": float(self.nv_max),
+                    "reasons": reasons, "samples": len(rows), "source": "NVML, 20 ms"}
         if self.proc is None:
             return None
         self.proc.terminate()

@@ -150,6 +150,11 @@ class ClockSampler:
         if self.nv_thread is not None:
             self.nv_stop.set()
             self.nv_thread.join(timeout=2)
+            try:
+                import pynvml
+                pynvml.nvmlShutdown()
+            except Exception:
+                pass
             rows = list(self.nv_rows)
             if not rows:
                 return None

@@ -168,10 +168,10 @@ class OrcTrace(C.Structure):
     _fields_ = [("n", C.c_int), ("phi", C.c_float * 64), ("verdict", C.c_int * 64), ("alambda", C.c_float * 64)]
 
 
-def forward_state(kt, cia, case, x, precision=ORC_MIXED, nthreads=1):
+def forward_state(kt, cia, case, x, precision=ORC_MIXED, nthreads=1, e3=None, solar=None):
     """Spectrum yn[ny] and K^T [nx, ny] of a retrieval case at state x."""
     L = lib()
-    t = tables_struct(kt, cia)
+    t = tables_struct(kt, cia, e3=e3, solar=solar)
     s = case.as_struct()
     x = np.ascontiguousarray(x, np.float32)
     yn = np.zeros(case.ny, np.float32)
@@ -183,10 +183,11 @@ def forward_state(kt, cia, case, x, precision=ORC_MIXED, nthreads=1):
     return yn, kk
 
 
-def retrieve(kt, cia, case, kiter=10, phlimit=0.1, dchisq_stop=0.0, precision=ORC_MIXED, nthreads=1):
+def retrieve(kt, cia, case, kiter=10, phlimit=0.1, dchisq_stop=0.0, precision=ORC_MIXED, nthreads=1, e3=None,
+             solar=None):
     """coreret restatement on one case: (result dict, trace dict)."""
     L = lib()
-    t = tables_struct(kt, cia)
+    t = tables_struct(kt, cia, e3=e3, solar=solar)
     s = case.as_struct()
     o = _abi.RtbRetrievalOpts(kiter, phlimit, dchisq_stop, 0)
     x = np.zeros(case.nx, np.float32)

@@ -333,3 +333,28 @@ def test_retrieval_over_several_paths(ctx, oracle, mode):
     assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
     assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
     assert g["yn"].shape == (case.ny,)
+
+
+def test_retrieval_of_total_planet_flux(ctx, oracle):
+    """A retrieval on the hemispherically integrated total flux of the planet
+    (IMOD 18 with iform 3, the extended kernel in the loop): same
+    iterations, forward evaluations and stop rule as the oracle's coreret
+    loop, states within 1e-3 prior sigma, cost within 1e-3."""
+    import dataclasses
+    kt, cia, _ = synth.config2()
+    e3 = synth.make_e3_table()
+    case = synth.make_retrieval(kt, [synth.CH4, synth.NH3], nlayer=30, seed=61, nwave=150)
+    job = dataclasses.replace(case.job, imod=np.full_like(case.job.imod, 18), iform=3, radius1=71492.0)
+    noise = 2e-7                       # fluxes near 5e-4 (x 1e-18 of W (cm-1)-1)
+    case = dataclasses.replace(case, job=job, sei=np.full(case.ny, 1.0 / noise ** 2))
+    y_true, _ = oracle.forward_state(kt, cia, case, case.x_true, nthreads=8, e3=e3)
+    synth.observe(case, y_true, seed=62, noise=noise)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_e3_table(e3)
+    g = ctx.retrieve_batch([case], kiter=10, phlimit=0.1)[0]
+    ref, _ = oracle.retrieve(kt, cia, case, kiter=10, phlimit=0.1, nthreads=8, e3=e3)
+    assert (g["converged"], g["iterations"], g["forwards"]) == (ref["converged"], ref["iterations"], ref["forwards"])
+    sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
+    assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
+    assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]

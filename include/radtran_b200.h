@@ -615,6 +615,14 @@ typedef struct rtb_retrieval_spec {
      * be NULL); prof->ndust must be 0. */
     const rtb_profile* prof;
     const rtb_layer_opts* lopts;
+    /* layer-state model: dust types whose column profile is scaled (model 3
+     * on an aerosol, subprofretg.f:735-750): x[nlayer + nscale + nprof*nlayer
+     * + d] is the log scale of dust type dust_type[d] (0-based, < ncont):
+     * cont = cont_atm * exp(x); atm->xmap holds the matching rows (row d,
+     * parameter ngas+1+type, level l: the type's column in layer l at scale
+     * 1) and atm->dco maps layers to levels; nx grows by ndust */
+    int ndust;
+    const int* dust_type;
 } rtb_retrieval_spec;
 
 typedef struct rtb_retrieval_opts {

@@ -28,6 +28,8 @@ struct Work {
     const rtb_conv* cv = nullptr;
     std::vector<float> temp, pp, amount, emtemp, xmap, pp0, amount0, xmap0;
     std::vector<float> press, delh, scale, dte, dam, dco, vwave;
+    std::vector<int> dust;              /* dust types whose column is scaled (model 3 on an aerosol) */
+    std::vector<float> cont, cont0;     /* [nlayer][ncont] */
     std::vector<int> layinc, idgas, isogas, ktab, nlayin, imod, sg, sm, pg;
     std::vector<float> vmr0;   /* [nprof][L] pp / press of the profiled gases */
     /* level-state model: L counts the profile's levels (the state's temperatures) */
@@ -166,7 +168,8 @@ int at_level_state(Work& w, const float* x) {
 
 int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     const rtb_atm& t = *s.atm;
-    if (t.npath < 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer || t.ncont < 0)
+    if (t.npath < 1 || t.npro != t.nlayer || t.nv != t.nlayer + s.nscale + s.nprof * t.nlayer + s.ndust ||
+        t.ncont < 0 || s.ndust < 0 || (s.ndust > 0 && (!s.dust_type || t.ncont == 0 || !t.dco)))
         return RTB_ERR_UNSUPPORTED;
     for (int p = 0; p < t.npath; ++p)
         if (t.nlayin[p] > t.nlayer) return RTB_ERR_UNSUPPORTED;
@@ -198,6 +201,14 @@ int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     col(t.dte, L, w.dte);
     col(t.dam, L, w.dam);
     if (t.ncont > 0 && t.dco) col(t.dco, L, w.dco);
+    if (t.ncont > 0) {   /* a working copy of the dust columns, scaled per state */
+        const int ldc = t.ld_con > 0 ? t.ld_con : RTB_MAXCON;
+        w.cont0.resize((size_t)t.ncont * L);
+        for (int l = 0; l < L; ++l)
+            for (int k = 0; k < t.ncont; ++k) w.cont0[k + (size_t)t.ncont * l] = t.cont[k + (size_t)ldc * l];
+        w.cont = w.cont0;
+        w.dust.assign(s.dust_type, s.dust_type + s.ndust);
+    }
     w.pp = w.pp0;
     w.amount = w.amount0;
     w.layinc.resize((size_t)L * w.NP);
@@ -237,7 +248,11 @@ int setup_layers(const rtb_retrieval_spec& s, Work& w) {
     w.a.emtemp = w.emtemp.data();
     w.a.dte = w.dte.data();
     w.a.dam = w.dam.data();
-    w.a.dco = w.dco.empty() ? nullptr : w.dco.data();   /* cont and xsec_ext: the caller's arrays */
+    w.a.dco = w.dco.empty() ? nullptr : w.dco.data();   /* xsec_ext: the caller's array */
+    if (t.ncont > 0) {
+        w.a.cont = w.cont.data();
+        w.a.ld_con = t.ncont;
+    }
     w.a.dfp = nullptr;
     w.a.xmap = w.xmap.data();
     w.a.vwave = w.vwave.data();
@@ -277,6 +292,20 @@ void at_state(Work& w, const float* x) {
             for (int k = 0; k < L; ++k)
                 w.xmap[(base + l) + (size_t)w.NV * (g + (size_t)w.nparam * k)] = k == l ? v : 0.0f;
         }
+    }
+    /* dust scales: model 3 on the type's column profile (subprofretg.f:735-750) */
+    const int NC = w.a.ncont;
+    const int dbase = L + ns + (int)w.pg.size() * L;
+    for (size_t d = 0; d < w.dust.size(); ++d) {
+        const int k = w.dust[d];
+        const float f = expf(x[dbase + (int)d]);
+        for (int l = 0; l < L; ++l) w.cont[k + (size_t)NC * l] = w.cont0[k + (size_t)NC * l] * f;
+        const int q = w.a.ngas + 1 + k;
+        for (int lev = 0; lev < L; ++lev)
+            for (int i = 0; i < w.NV; ++i) {
+                const size_t idx = i + (size_t)w.NV * (q + (size_t)w.nparam * lev);
+                w.xmap[idx] = w.xmap0[idx] * f;
+            }
     }
 }
 

@@ -104,6 +104,7 @@ class RtbRetrievalSpec(C.Structure):
         ("xa", _fp), ("x0", _fp),
         ("scale_model", _ip), ("nprof", C.c_int), ("prof_gas", _ip),
         ("prof", C.POINTER(RtbProfile)), ("lopts", C.POINTER(RtbLayerOpts)),
+        ("ndust", C.c_int), ("dust_type", _ip),
     ]
 
 

@@ -49,7 +49,8 @@ struct AtmWork {
     std::vector<float> press, temp, delh, pp, amount, cont, scale, emtemp, dte, dam, dco, xmap, vwave, xsec;
     std::vector<int> idgas, isogas, ktab, nlayin, imod, layinc;
     std::vector<float> pp0, amount0, xmap0;   // at scale factor 1
-    std::vector<int> scale_gas, scale_model, prof_gas;
+    std::vector<int> scale_gas, scale_model, prof_gas, dust_type;
+    std::vector<float> cont0;                 // dust columns at scale 1 [nlayer][ncont]
     std::vector<float> vmr0;                  // [nprof][L] pp0 / press of the profiled gases
     // the level-state model: the profile (levels) and its layering
     bool level = false;
@@ -101,8 +102,13 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
     w.ny *= NP;   // y: every path's spectrum, path after path
     if (NPRO != L) return fail(c, RTB_ERR_UNSUPPORTED, "layer-state model needs npro == nlayer");
     if (s.nprof < 0 || (s.nprof > 0 && !s.prof_gas)) return fail(c, RTB_ERR_ARG, "nprof/prof_gas");
-    if (NV != L + s.nscale + s.nprof * L)
-        return fail(c, RTB_ERR_ARG, "nv=%d but nlayer + nscale + nprof*nlayer = %d", NV, L + s.nscale + s.nprof * L);
+    if (s.ndust < 0 || (s.ndust > 0 && (!s.dust_type || NC == 0 || !t.dco)))
+        return fail(c, RTB_ERR_ARG, "ndust/dust_type (dust scales need ncont > 0 and dco)");
+    for (int d = 0; d < s.ndust; ++d)
+        if (s.dust_type[d] < 0 || s.dust_type[d] >= NC) return fail(c, RTB_ERR_ARG, "dust_type[%d] outside 0..ncont-1", d);
+    if (NV != L + s.nscale + s.nprof * L + s.ndust)
+        return fail(c, RTB_ERR_ARG, "nv=%d but nlayer + nscale + nprof*nlayer + ndust = %d", NV,
+                    L + s.nscale + s.nprof * L + s.ndust);
     if (NV > kNewtonMaxNx) return fail(c, RTB_ERR_UNSUPPORTED, "state size %d > %d", NV, kNewtonMaxNx);
     if (NV >= w.ny) return fail(c, RTB_ERR_UNSUPPORTED, "nx=%d >= ny=%d (calc_gain_matrix nx<ny branch only)", NV, w.ny);
     if (!t.press || !t.temp || !t.delh || !t.pp || !t.amount || !t.idgas || !t.isogas || !t.ktab || !t.nlayin ||
@@ -143,6 +149,8 @@ int build_work(rtb_context* c, const rtb_retrieval_spec& s, AtmWork& w) {
         w.cont.resize((size_t)NC * L);
         for (int j = 0; j < L; ++j)
             for (int i = 0; i < NC; ++i) w.cont[i + (size_t)NC * j] = t.cont[i + (size_t)ldc * j];
+        w.cont0 = w.cont;
+        w.dust_type.assign(s.dust_type, s.dust_type + s.ndust);
         lay2(t.dco, NPRO, w.dco);
         w.xsec.assign(t.xsec_ext, t.xsec_ext + (size_t)NC * NW);
     }
@@ -237,6 +245,20 @@ int set_state(rtb_context* c, AtmWork& w, const float* x) {
             w.pp[l + (size_t)L * g] = w.pp0[l + (size_t)L * g] * f;
             for (int k = 0; k < NPRO; ++k) w.xmap[(base + l) + (size_t)NV * (g + (size_t)nparam * k)] = k == l ? v : 0.0f;
         }
+    }
+    // dust scales: model 3 on the type's column profile (subprofretg.f:735-750)
+    const int NC = w.a.ncont;
+    const int dbase = L + ns + (int)w.prof_gas.size() * L;
+    for (size_t d = 0; d < w.dust_type.size(); ++d) {
+        const int k = w.dust_type[d];
+        const float f = expf(x[dbase + (int)d]);
+        for (int l = 0; l < L; ++l) w.cont[k + (size_t)NC * l] = w.cont0[k + (size_t)NC * l] * f;
+        const int q = w.a.ngas + 1 + k;
+        for (int lev = 0; lev < NPRO; ++lev)
+            for (int i = 0; i < NV; ++i) {
+                const size_t idx = i + (size_t)NV * (q + (size_t)nparam * lev);
+                w.xmap[idx] = w.xmap0[idx] * f;
+            }
     }
     return RTB_OK;
 }

@@ -640,6 +640,7 @@ class RetrievalCase:
     prof_gas: np.ndarray | None = None      # int32 [nprof] gases retrieved as log-vmr layer profiles
     prof: "Profile | None" = None           # level-state model: the profile re-layered every state
     lopts: dict | None = None               # its layering (rtb_layer_opts fields)
+    dust_type: np.ndarray | None = None     # int32 [ndust] dust types whose column is scaled (log), last in x
 
     @property
     def nx(self):
@@ -678,8 +679,34 @@ class RetrievalCase:
                 o.base = _abi.fptr(base)
             s.prof, s.lopts = C.pointer(ps), C.pointer(o)
             keep += [ps, o, base]
+        if self.dust_type is not None and len(self.dust_type):
+            dt = np.ascontiguousarray(self.dust_type, np.int32)
+            s.ndust, s.dust_type = len(dt), _abi.iptr(dt)
+            keep.append(dt)
         s._keep = keep
         return s
+
+
+def with_dust_scales(case: RetrievalCase, ncont=2, seed=0, sig=0.5) -> RetrievalCase:
+    """The layer-state case through ncont dust types (with_dust) whose column
+    profiles are scaled, log scale a priori 0 with sigma `sig` each, last in
+    the state vector; the true scales a seeded draw."""
+    rng = np.random.default_rng(seed)
+    j = with_dust(case.job, ncont, seed=seed, state=False)
+    nv0, L = j.nv, j.nlayer
+    nv = nv0 + ncont
+    xmap = np.zeros((nv, j.nparam, j.npro), np.float32, order="F")
+    xmap[:nv0] = j.xmap
+    for k in range(ncont):
+        xmap[nv0 + k, j.ngas + 1 + k, :L] = j.cont[k]
+    job = dataclasses.replace(j, nv=nv, ld_v=nv, xmap=xmap)
+    sa = np.zeros((nv, nv))
+    sa[:nv0, :nv0] = case.sa
+    sa[nv0:, nv0:] = np.eye(ncont) * sig * sig
+    xa = np.concatenate([case.xa, np.zeros(ncont, np.float32)]).astype(np.float32)
+    x_true = np.concatenate([case.x_true, rng.normal(0.0, sig, ncont)]).astype(np.float32)
+    return dataclasses.replace(case, job=job, sa=sa, xa=xa, x_true=x_true, y=None,
+                               dust_type=np.arange(ncont, dtype=np.int32))
 
 
 def prior_covariance(p_lay, n_scale, sig_t=3.0, sig_scale=0.5, clen=1.5):

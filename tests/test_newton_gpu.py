@@ -358,3 +358,24 @@ def test_retrieval_of_total_planet_flux(ctx, oracle):
     sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
     assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
     assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]
+
+
+def test_retrieval_of_dust_scales(ctx, oracle):
+    """Two dust types whose column profiles are retrieved as log scales
+    beside the temperatures and gas scales (model 3 on an aerosol,
+    subprofretg.f:735-750; their Jacobian through DCO): same iterations,
+    forward evaluations and stop rule as the oracle's coreret loop, states
+    within 1e-3 prior sigma, cost within 1e-3."""
+    kt, cia, _ = synth.config2()
+    base = synth.make_retrieval(kt, [synth.CH4, synth.NH3], nlayer=30, seed=61, nwave=150)
+    case = synth.with_dust_scales(base, 2, seed=7)
+    y_true, _ = oracle.forward_state(kt, cia, case, case.x_true, nthreads=8)
+    synth.observe(case, y_true, seed=62)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    g = ctx.retrieve_batch([case], kiter=10, phlimit=0.1)[0]
+    ref, _ = oracle.retrieve(kt, cia, case, kiter=10, phlimit=0.1, nthreads=8)
+    assert (g["converged"], g["iterations"], g["forwards"]) == (ref["converged"], ref["iterations"], ref["forwards"])
+    sig = np.sqrt(np.diag(case.sa)).astype(np.float32)
+    assert np.all(np.abs(g["x"] - ref["x"]) <= 1e-3 * sig)
+    assert abs(g["phi"] - ref["phi"]) <= 1e-3 * ref["phi"]

@@ -266,6 +266,19 @@ typedef struct rtb_atm {
     /* distance from the star in AU (cirsrtfg_wave.f argument DIST): iform = 4
      * scales the star's spectrum by 1 / (4 pi (dist AU)^2) when dist > 0 */
     float dist;
+    /* The gas-continuum switches of /GASCONDEF/ (radtran/includes/gascom.f,
+     * read from the .fla file by READFLAGS) that NGASCON tests per layer and
+     * gas (radtran/radtran/ngascon.f:132-318, called from cirsradg_wave.f:
+     * 590-611): IH2O (H2O id 1, any isotope), ICH4 (CH4 id 6), INH3 (NH3
+     * id 11), IO3 (O3 id 3) -- the last three for isotope 0 or 1 -- and the
+     * iuvscat bitmask of UV cross sections (bit 1 NH3 11, 2 PH3 28, 4 C2H2
+     * 26, 8 C2H6 27, 16 C4H2 30, 32 CH4 6, 64 CO 5, 128 GeH4 33, 256 H2O 1,
+     * 512 C3H8 34).  A switch whose gas is absent contributes nothing, as in
+     * the reference.  A switch whose gas is present would add a continuum
+     * from data tables this library does not hold, so the call is refused
+     * with RTB_ERR_UNSUPPORTED naming the switch and the gas; zero (the
+     * reference's default) for all five is the computed path. */
+    int ih2o, ich4, inh3, io3, iuvscat;
 } rtb_atm;
 
 /* Outputs, convolved by cirsconv with atm->fwhm onto the channels of

@@ -60,6 +60,7 @@ class RtbAtm(C.Structure):
         ("radius1", C.c_float), ("radextra", C.c_float),
         ("nlte_k1", C.c_float), ("nlte_A", C.c_float),
         ("dist", C.c_float),
+        ("ih2o", C.c_int), ("ich4", C.c_int), ("inh3", C.c_int), ("io3", C.c_int), ("iuvscat", C.c_int),
     ]
 
 

@@ -224,6 +224,39 @@ float get_solar_wave_f(const rtb_context* c, float x, float dist) {
     return y;
 }
 
+// The NGASCON gate (radtran/radtran/ngascon.f:132-318): the first switch of
+// /GASCONDEF/ that would give a gas of the atmosphere a continuum, as a
+// message, or null when every gas's NGASCON term is the reference's zero.
+// IH2O = 2 is refused too: that branch leaves ABSORB unassigned.
+const char* gascon_refusal(const rtb_atm& a) {
+    static thread_local char msg[160];
+    struct Uv { int bit, id; const char* name; };
+    static const Uv uv[] = {{1, 11, "NH3"}, {2, 28, "PH3"}, {4, 26, "C2H2"}, {8, 27, "C2H6"}, {16, 30, "C4H2"},
+                            {32, 6, "CH4"}, {64, 5, "CO"}, {128, 33, "GeH4"}, {256, 1, "H2O"}, {512, 34, "C3H8"}};
+    for (int k = 0; k < a.ngas; ++k) {
+        const int id = a.idgas[k], iso = a.isogas[k];
+        const bool iso01 = iso == 0 || iso == 1;
+        const char* sw = nullptr;
+        if (id == 1 && a.ih2o != 0) sw = a.ih2o == 1 ? "IH2O=1 (CKD H2O continuum)" : "IH2O!=0,1";
+        else if (id == 6 && iso01 && a.ich4 != 0) sw = "ICH4 (Karkoschka CH4 continuum)";
+        else if (id == 11 && iso01 && a.inh3 != 0) sw = "INH3 (Lutz-Owen NH3 continuum)";
+        else if (id == 3 && iso01 && a.io3 != 0) sw = "IO3 (Serdyuchenko O3 cross sections)";
+        if (!sw && a.iuvscat > 0)
+            for (const Uv& u : uv)
+                if (id == u.id && (a.iuvscat & u.bit)) {
+                    snprintf(msg, sizeof msg, "ngascon: iuvscat bit %d (%s UV cross sections) for gas %d (id %d): "
+                             "gas continua are not implemented", u.bit, u.name, k + 1, id);
+                    return msg;
+                }
+        if (sw) {
+            snprintf(msg, sizeof msg, "ngascon: %s for gas %d (id %d, iso %d): gas continua are not implemented",
+                     sw, k + 1, id, iso);
+            return msg;
+        }
+    }
+    return nullptr;
+}
+
 int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
     Dims d;
     d.ld_lay = a.ld_lay > 0 ? a.ld_lay : RTB_MAXLAY;
@@ -264,6 +297,7 @@ int pack_spectrum(rtb_context* c, const rtb_atm& a, Staging& st) {
             return fail(c, RTB_ERR_ARG, "ktab[%d] = RTB_KTAB_BY_ID but the tables' gas ids are unknown", k);
         if (id == 22 || id == 2) n2co2 = true;
     }
+    if (const char* why = gascon_refusal(a)) return fail(c, RTB_ERR_UNSUPPORTED, "%s", why);
     int nlmax = 0;
     for (int ip = 0; ip < a.npath; ++ip) {
         const int m = a.imod[ip];

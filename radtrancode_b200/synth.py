@@ -312,6 +312,7 @@ class Job:
     nlte_k1: float = 0.0             # inlte = 1: collisional rate and Einstein A
     nlte_A: float = 0.0
     dist: float = 0.0                # AU, distance from the star (iform = 4)
+    gascon: tuple = (0, 0, 0, 0, 0)  # /GASCONDEF/ switches IH2O, ICH4, INH3, IO3, iuvscat (ngascon.f)
     conv: "Channels | None" = None   # instrument channels (None: FWHM = 0, nconv = nwave)
     ncont: int = 0                   # dust types
     cont: np.ndarray | None = None   # (ncont, nlayer) F, dust particles / cm2 per layer
@@ -346,6 +347,7 @@ class Job:
         s.flagh2p, s.ilbl, s.inlte, s.iform = self.flagh2p, 0, self.inlte, self.iform
         s.nlte_k1, s.nlte_A = float(self.nlte_k1), float(self.nlte_A)
         s.dist = float(self.dist)
+        s.ih2o, s.ich4, s.inh3, s.io3, s.iuvscat = (int(x) for x in self.gascon)
         if self.flagh2p:
             s.hfp, s.dfp = f(self.hfp), f(self.dfp)
         s.tsurf, s.fwhm = float(self.tsurf), float(self.fwhm)

@@ -107,3 +107,37 @@ def test_largest_profile_and_its_limit(ctx, oracle):
     big = synth.make_job(kt, [synth.CH4, synth.NH3], nlayer=201, seed=89, nwave=1)
     with pytest.raises(cirsradg.RtbError, match="LIMIT"):
         ctx.cirsrtfg_wave(big)
+
+
+def test_ngascon_switches_refused_or_zero(ctx):
+    """The NGASCON gate (ngascon.f:132-318 via cirsradg_wave.f:590-611).
+    A /GASCONDEF/ switch whose gas is in the atmosphere would add a gas
+    continuum the library does not compute: refused, naming the switch.  A
+    switch whose gas is absent contributes nothing in the reference either:
+    the spectrum is bit-identical to the all-off run."""
+    kt, cia, job = synth.config2(nwave=4, nlayer=20, nbin=4)   # CH4 (6), C2H6 (27), C2H2 (26), NH3 (11)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    c0, g0, t0 = ctx.cirsrtfg_wave(job)
+    refused = {(0, 1, 0, 0, 0): "ICH4", (0, 0, 1, 0, 0): "INH3", (0, 0, 0, 0, 1): "iuvscat bit 1",
+               (0, 0, 0, 0, 4): "iuvscat bit 4", (0, 0, 0, 0, 8): "iuvscat bit 8", (0, 0, 0, 0, 32): "iuvscat bit 32"}
+    for sw, name in refused.items():
+        j = copy.deepcopy(job)
+        j.gascon = sw
+        with pytest.raises(cirsradg.RtbError, match="UNSUPPORTED") as e:
+            ctx.cirsrtfg_wave(j)
+        assert name in str(e.value)
+    # switches of absent gases (H2O, O3, PH3, C4H2, CO, GeH4, H2O UV, C3H8), and CH4 of another isotope
+    for sw in ((1, 0, 0, 0, 0), (2, 0, 0, 0, 0), (0, 0, 0, 1, 0), (0, 0, 0, 0, 2 | 16 | 64 | 128 | 256 | 512)):
+        j = copy.deepcopy(job)
+        j.gascon = sw
+        c, g, t = ctx.cirsrtfg_wave(j)
+        assert np.array_equal(c, c0) and np.array_equal(g, g0) and np.array_equal(t, t0)
+    j = copy.deepcopy(job)
+    j.isogas = job.isogas.copy()
+    j.isogas[0] = 2                                   # 13CH4: ICH4 applies to isotopes 0 and 1 only
+    j.gascon = (0, 1, 0, 0, 0)
+    c, g, t = ctx.cirsrtfg_wave(j)
+    j.gascon = (0, 0, 0, 0, 0)
+    c2, g2, t2 = ctx.cirsrtfg_wave(j)
+    assert np.array_equal(c, c2) and np.array_equal(g, g2)

@@ -1573,7 +1573,8 @@ int run(const orc_tables& t, const rtb_atm& a, double* calcout, double* gradient
             Work<R> W;
             make_work(W);
             for (int iw = tid; iw < a.nwave; iw += nthreads) {
-                int s = one_wave<R>(t, a, d, LK, isw, iw, W, calcout, gradients, gradtsurf, nullptr);
+                // debug records are per (wavenumber, layer, pass): the threads write disjoint ones
+                int s = one_wave<R>(t, a, d, LK, isw, iw, W, calcout, gradients, gradtsurf, dbg);
                 if (s) { stat[tid] = s; return; }
             }
         });
@@ -1594,9 +1595,9 @@ int orc_cirsrtfg_wave(const orc_tables* tab, const rtb_atm* atm, int precision, 
 }
 
 int orc_cirsrtfg_wave_mt(const orc_tables* tab, const rtb_atm* atm, int precision, double* calcout,
-                         double* gradients, double* gradtsurf, int nthreads) {
+                         double* gradients, double* gradtsurf, int nthreads, const orc_debug* dbg) {
     if (!tab || !atm || !calcout || !gradients) return RTB_ERR_ARG;
-    if (precision == ORC_MIXED) return run<float>(*tab, *atm, calcout, gradients, gradtsurf, nullptr, nthreads);
+    if (precision == ORC_MIXED) return run<float>(*tab, *atm, calcout, gradients, gradtsurf, dbg, nthreads);
     return run<double>(*tab, *atm, calcout, gradients, gradtsurf, nullptr, nthreads);
 }
 

@@ -338,7 +338,7 @@ int forward(const orc_tables* tab, Work& w, const float* x, int precision, int n
     }
     const int NP = w.NP, NW = w.NW, NV = w.NV;
     std::vector<double> c((size_t)NP * NW), g((size_t)NP * NV * NW);   /* [path][wave], [path][iv][wave] */
-    const int r = orc_cirsrtfg_wave_mt(tab, &w.a, precision, c.data(), g.data(), nullptr, nthreads);
+    const int r = orc_cirsrtfg_wave_mt(tab, &w.a, precision, c.data(), g.data(), nullptr, nthreads, nullptr);
     if (r) return r;
     /* per path: the spectrum and the Jacobian rows, cirsconv'd onto the channels when there are any */
     const int ny1 = w.NY / NP;

@@ -91,10 +91,11 @@ int orc_cirsrtfg_wave(const orc_tables* tab, const rtb_atm* atm, int precision,
                       const orc_debug* dbg);
 
 /* Same, running independent wavenumbers on `nthreads` host threads (the
- * reference loop over wavenumbers has no carried state). */
+ * reference loop over wavenumbers has no carried state); dbg (may be NULL)
+ * as above, each thread writing the records of its own wavenumbers. */
 int orc_cirsrtfg_wave_mt(const orc_tables* tab, const rtb_atm* atm, int precision,
                          double* calcout, double* gradients, double* gradtsurf,
-                         int nthreads);
+                         int nthreads, const orc_debug* dbg);
 
 /* --- unit-level entry points used by the oracle's own tests ----------- */
 /* 0 = reference heapsort (default); 1 = stable sort (tie-order experiments) */

@@ -42,8 +42,22 @@ class OrcDebug(C.Structure):
                 ("ties", C.POINTER(C.c_int16))]
 
 
+NATIVE_PATH = os.path.join(HERE, "_build", "liboracle_native.so")
+
+
 def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def use_native():
+    """Load the -O3 -march=native build (made here, on the host that runs
+    it) instead of the portable one: the timed CPU baseline.  Call before
+    any other use of the oracle in the process."""
+    global LIB_PATH
+    if _lib is not None:
+        raise RuntimeError("oracle already loaded")
+    subprocess.run(["make", "-s", "-C", HERE, "native"], check=True)
+    LIB_PATH = NATIVE_PATH
 
 
 _lib = None
@@ -120,7 +134,8 @@ def cirsrtfg_wave(kt, cia, job, precision=ORC_MIXED, debug=False, nthreads=1, e3
         dbg = OrcDebug(perm.ctypes.data_as(p16), split.ctypes.data_as(p16), ties.ctypes.data_as(p16))
     dp = [a.ctypes.data_as(C.POINTER(C.c_double)) for a in out]
     if nthreads > 1:
-        st = L.orc_cirsrtfg_wave_mt(C.byref(t), C.byref(s), precision, dp[0], dp[1], dp[2], nthreads)
+        st = L.orc_cirsrtfg_wave_mt(C.byref(t), C.byref(s), precision, dp[0], dp[1], dp[2], nthreads,
+                                    C.byref(dbg) if dbg is not None else None)
     else:
         st = L.orc_cirsrtfg_wave(C.byref(t), C.byref(s), precision, dp[0], dp[1], dp[2],
                                  C.byref(dbg) if dbg is not None else None)

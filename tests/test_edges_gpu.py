@@ -135,7 +135,7 @@ def test_ngascon_switches_refused_or_zero(ctx):
         assert np.array_equal(c, c0) and np.array_equal(g, g0) and np.array_equal(t, t0)
     j = copy.deepcopy(job)
     j.isogas = job.isogas.copy()
-    j.isogas[0] = 2                                   # 13CH4: ICH4 applies to isotopes 0 and 1 only
+    j.isogas[list(job.idgas).index(6)] = 2            # 13CH4: ICH4 applies to isotopes 0 and 1 only
     j.gascon = (0, 1, 0, 0, 0)
     c, g, t = ctx.cirsrtfg_wave(j)
     j.gascon = (0, 0, 0, 0, 0)

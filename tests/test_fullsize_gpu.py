@@ -27,7 +27,8 @@ NTHR = os.cpu_count() or 1
 @pytest.fixture(scope="module")
 def full(oracle):
     kt, cia, job = synth.config2()
-    assert (job.nlayer, job.ngas, job.nwave, job.nv) == (120, 4, 2000, 124)
+    # H2, He (continuum only) and the four absorbers
+    assert (job.nlayer, job.ngas, job.nwave, job.nv) == (120, 6, 2000, 124)
     return kt, cia, job
 
 

@@ -1,15 +1,23 @@
-"""Benchmark of the B200 CIRSRADG forward model + analytic Jacobian.
+"""Benchmark of the B200 CIRSRADG forward model + analytic Jacobian and the
+optimal-estimation retrieval built on it.
 
-Workload (one step): one nadir thermal-emission spectrum of 120 layers,
-H2/He + CH4, C2H6, C2H2, NH3 random-overlapped (NG = 20), 2000 wavenumbers,
-Jacobian over NX = 124 state elements -- the full-size single-spectrum
-configuration.  Inputs are the seeded synthetic workload of
-radtrancode_b200/synth.py (the reference measures on no public data set).
+Headline workload (one step): one nadir thermal-emission spectrum of 120
+layers, H2/He + CH4, C2H6, C2H2, NH3 random-overlapped (NG = 20), 2000
+wavenumbers, Jacobian over NX = 124 state elements -- the full-size
+single-spectrum configuration.  Beside it, each at its stated size:
+  batch      4096 uneven spectra in one persistent launch (autotuned tile and
+             schedule, CUDA graph)
+  retrieval  1024 full-size retrievals, up to 10 Newton iterations
+  serving    Poisson arrivals at 2000 req/s into the continuous-batching
+             server under an HBM budget that caps the requests in flight,
+             and a sub-saturation point (40 req/s for 30 s)
+Inputs are the seeded synthetic workloads of radtrancode_b200/synth.py (the
+reference measures on no public data set).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 `value`: spectra/s with inputs resident in HBM (CUDA events on the launching
-stream around K launches; the k-tables, 384 MB of raw + log k, exceed the
+stream around K launches; the k-tables, 384 MB of raw + ln k, exceed the
 126 MB L2, so no flush is needed between steps).  `e2e`: the same metric
 through the public C ABI call (rtb_cirsrtfg_wave) with host buffers, the
 host->device copy of the inputs and the device->host copy of the radiance
@@ -22,7 +30,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -37,36 +44,39 @@ sys.path.insert(0, ROOT)
 METRIC = "fwd+Jacobian spectra/s & retrievals/s at ≤1e-4 rel err; retrieval p50/p99 ms"
 WORKLOAD = ("single spectrum, full size: 120 layers, H2/He + CH4/C2H6/C2H2/NH3 random overlap (NG=20), "
             "2000 wavenumbers 600-1400 cm-1, k-tables 20P x 15T x 20g, Jacobian NX=124")
-CPU_SAMPLE_WAVES = 1000       # bounded CPU-baseline sample (half the spectrum)
-ACC_SAMPLE_WAVES = 48         # FP64-oracle accuracy sample
+PROFILE_DATA = os.path.join(ROOT, "profiles", "fwd_kernel_config2.json")
 
 
-def peaks():
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def measured_peaks():
+    """HBM GB/s and bf16 TFLOP/s of MEASURED_PEAKS.json (driver-written on
+    this pool's B200s), else the pool's earlier fallback figures."""
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return 6650.0, 1590.0, "fallback"
 
 
-def tensor_peak():
+def profile_data():
+    """Per-launch figures of one ncu capture of the forward kernel on this
+    workload (DRAM bytes, warp instructions), committed beside the summary."""
     try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            return float(json.load(f)["bf16_tflops"])
-    except Exception:
-        return 1590.0
-
-
-def profile_traffic():
-    """DRAM bytes per launch of the forward kernel from the committed ncu
-    summary (profiles/fwd_kernel_config2.md, line 'dram_bytes_per_launch:')."""
-    path = os.path.join(ROOT, "profiles", "fwd_kernel_config2.md")
-    try:
-        m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-        return float(m.group(1)) if m else None
-    except OSError:
-        return None
+        with open(PROFILE_DATA) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
 
 
 def algorithmic_bytes(kt, job, in_bytes, out_bytes):
@@ -190,92 +200,98 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ---------------------------------------------------------------- accuracy against the FP64 oracle
+def _jac_errors(g, g64, nv):
+    G = np.asarray(g, np.float64).reshape(nv, -1)
+    R = np.asarray(g64, np.float64).reshape(nv, -1)
+    scale = np.max(np.abs(R), axis=1, keepdims=True)
+    colnorm = float(np.max(np.abs(G - R) / np.where(scale > 0, scale, 1.0)))
+    big = (np.abs(R) >= 1e-3 * scale) & (scale > 0)
+    elem = float(np.max(np.abs(G - R)[big] / np.abs(R)[big])) if big.any() else 0.0
+    return colnorm, elem
+
+
+def accuracy(kt, cia, pairs, nthr, what):
+    """Per-result errors of device outputs against the FP64 oracle: the
+    largest radiance relative error, the largest column-normalised Jacobian
+    error (each state element's row scaled by its largest magnitude) and the
+    element-wise relative Jacobian error over entries of at least 1e-3 of
+    their row's largest magnitude, over the (job, (calcout, gradients, _))
+    pairs given."""
+    from oracle import pyoracle as po
+    r = jc = je = 0.0
+    for job, (c, g, _) in pairs:
+        c64, g64, _ = po.cirsrtfg_wave(kt, cia, job, po.ORC_FP64, nthreads=nthr)
+        r = max(r, float(np.max(np.abs(np.asarray(c, np.float64) - c64) / np.abs(c64))))
+        a, b = _jac_errors(g, g64, job.nv)
+        jc, je = max(jc, a), max(je, b)
+    return {"radiance_max_rel_err": r, "jacobian_max_rel_err": jc, "jacobian_elementwise_max_rel_err": je,
+            "results": len(pairs), "of": what, "vs": "FP64 oracle",
+            "gates": {"radiance": 1e-4, "jacobian": 1e-3}}
+
+
+# ---------------------------------------------------------------- reference arm
 def reference_arm(args, rank):
     """The reference's CPU path on the host cores.  No Fortran compiler exists
     here or on the GPU host, so the reference Fortran cannot be built; the
     arm runs the oracle (the C++ restatement of the reference Fortran,
-    oracle/) on all host threads, each step a bounded sample of the same
-    workload."""
+    oracle/, built -O3 -march=native on this host) on all host threads over
+    the whole spectrum every step."""
     if rank != 0:
         return
     from oracle import pyoracle as po
+    po.use_native()
     from radtrancode_b200 import synth
     kt, cia, job = synth.config2()
-    sample = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0, nwave=CPU_SAMPLE_WAVES,
-                            vmr_perturb=0.3)
     nthr = os.cpu_count() or 1
+    warm = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0, nwave=4 * nthr, vmr_perturb=0.3)
     for _ in range(args.warmup):
-        po.cirsrtfg_wave(kt, cia, synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0,
-                                                 nwave=nthr, vmr_perturb=0.3), po.ORC_MIXED, nthreads=nthr)
+        po.cirsrtfg_wave(kt, cia, warm, po.ORC_MIXED, nthreads=nthr)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        po.cirsrtfg_wave(kt, cia, sample, po.ORC_MIXED, nthreads=nthr)
+        po.cirsrtfg_wave(kt, cia, job, po.ORC_MIXED, nthreads=nthr)
         times.append(time.perf_counter() - t)
     t_step = statistics.mean(times)
-    frac = CPU_SAMPLE_WAVES / job.nwave
-    value = frac / t_step
+    value = 1.0 / t_step
+    sample = (f"the whole spectrum (2000 wavenumbers) per step, {nthr} threads on {cpu_model()}; C++ restatement "
+              "of the reference Fortran, -O3 -march=native (no Fortran compiler on the host)")
     out = {
         "metric": METRIC, "value": value, "unit": "spectra/s", "impl": "reference", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3 / frac,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 transmissions)",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"{CPU_SAMPLE_WAVES} of 2000 wavenumbers per step"},
-        "cpu_baseline": {"value": value, "unit": "spectra/s", "cores": nthr, "kind": "port",
-                         "sample": f"{CPU_SAMPLE_WAVES} of 2000 wavenumbers per step, {nthr} threads; "
-                                   "C++ restatement of the reference Fortran (no Fortran compiler on the host)"},
+        "config": {"workload": WORKLOAD, "sample": "whole spectrum per step"},
+        "cpu_baseline": {"value": value, "unit": "spectra/s", "cores": nthr, "kind": "port", "sample": sample,
+                         "cpu": cpu_model()},
         "e2e": {"value": value, "unit": "spectra/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
     print(json.dumps(out))
 
 
-def cpu_baseline_and_accuracy(kt, cia, job, gpu_out):
-    """Rank-0 CPU baseline (oracle port on all host threads, bounded sample)
-    and the accuracy of the measured GPU result against the FP64 oracle on a
-    sample of the same spectrum."""
+def cpu_baseline(kt, cia, job, nthr):
+    """Rank-0 CPU baseline: the oracle port on all host threads over the whole
+    spectrum (about 1.5 s)."""
     from oracle import pyoracle as po
-    from radtrancode_b200 import synth
-    nthr = os.cpu_count() or 1
-    sample = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=0, nwave=CPU_SAMPLE_WAVES,
-                            vmr_perturb=0.3)
     t = time.perf_counter()
-    po.cirsrtfg_wave(kt, cia, sample, po.ORC_MIXED, nthreads=nthr)
+    po.cirsrtfg_wave(kt, cia, job, po.ORC_MIXED, nthreads=nthr)
     dt = time.perf_counter() - t
-    base = {"value": (CPU_SAMPLE_WAVES / job.nwave) / dt, "unit": "spectra/s", "cores": nthr, "kind": "port",
-            "sample": f"{CPU_SAMPLE_WAVES} of 2000 wavenumbers of the same spectrum, {nthr} threads, "
-                      "C++ restatement of the reference Fortran (no Fortran compiler on the host)"}
-    stride = job.nwave // ACC_SAMPLE_WAVES
-    acc_rad, acc_jac = 0.0, 0.0
-    c, g, _ = gpu_out
-    G = g.reshape(job.nv, job.nwave)
-    for iw0 in range(0, job.nwave, stride * 8):
-        sj = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, iw0=iw0, nwave=8, vmr_perturb=0.3)
-        c64, g64, _ = po.cirsrtfg_wave(kt, cia, sj, po.ORC_FP64, nthreads=min(nthr, 8))
-        acc_rad = max(acc_rad, float(np.max(np.abs(c[iw0:iw0 + 8] - c64) / np.abs(c64))))
-        R = g64.reshape(job.nv, 8)
-        scale = np.maximum(np.max(np.abs(G), axis=1, keepdims=True), 1e-300)
-        acc_jac = max(acc_jac, float(np.max(np.abs(G[:, iw0:iw0 + 8] - R) / scale)))
-    return base, {"radiance_max_rel_err": acc_rad, "jacobian_max_rel_err": acc_jac,
-                  "sample_wavenumbers": len(range(0, job.nwave, stride * 8)) * 8, "vs": "FP64 oracle"}
+    return {"value": 1.0 / dt, "unit": "spectra/s", "cores": nthr, "kind": "port", "cpu": cpu_model(),
+            "sample": f"the whole spectrum (2000 wavenumbers), {nthr} threads, C++ restatement of the reference "
+                      "Fortran built -O3 -march=native (no Fortran compiler on the host)"}
 
 
-RET_SAMPLE = 64               # full-size retrievals timed in the default run
-RET_FP64_SAMPLE = 16          # of those, re-run with the all-FP64 Newton step
-NEWTON_BATCH = 296            # retrievals per timed Newton-step launch (2 per SM)
-RET_WORKLOAD = ("optimal-estimation retrievals, full size: NX=124 (120 layer T + 4 log gas scales), NY=2000, "
-                "10 Newton iterations max, phlimit 0.1 %, Sa exponential correlation 1.5 scale heights "
-                "3 K / 50 %, Se diagonal (1e-9)^2, y = F(x_true) + N(0, 1e-9), x_true ~ N(xa, Sa)")
-
-
-BATCH_SPECTRA = 1024          # uneven spectra in the batched leg (the 4096 of the batching workload: --batch-spectra)
+# ---------------------------------------------------------------- batch leg
+BATCH_SPECTRA = 4096          # the batching workload: 4096 uneven spectra
 BATCH_TUNE = 256              # sub-batch the autotuner times
+BATCH_ACC = 8                 # spectra of the batch checked against the FP64 oracle
 
 
-def batch_leg(ctx, kt, nspec):
-    """Uneven-spectra batch in one persistent launch: default schedule vs
-    the autotuned schedule replayed through a CUDA graph, and the batched
-    C-ABI call end to end."""
+def batch_leg(ctx, kt, cia, nspec, nthr):
+    """Uneven-spectra batch in one persistent launch: default tile and
+    schedule vs the autotuned ones replayed through a CUDA graph, the batched
+    C-ABI call end to end, and the accuracy of a sample of its spectra."""
     from radtrancode_b200 import synth
     jobs = synth.config3_jobs(kt, nspec, seed=1003)
     nwave = sum(j.nwave for j in jobs)
@@ -284,21 +300,25 @@ def batch_leg(ctx, kt, nspec):
     t = time.perf_counter()
     ctx.prepare(jobs)
     t_prep = time.perf_counter() - t
-
-    def timed(n):
-        ms = []
-        for _ in range(n):
-            ctx.launch()
-            ctx.fetch()
-            ms.append(ctx.stats()["ms_kernel"])
-        return ms[-1]
+    ctx.set_tile(0)
     ctx.set_schedule(0, 0)
-    ms_default = timed(2)
+    ctx.launch()
+    ctx.fetch()
+    ms_default = ctx.stats()["ms_kernel"]
+    ctx.set_tile(tune["warps"])
     ctx.set_schedule(tune["schedule"], tune["blocks_per_sm"])
     ctx.use_graph(True)
-    ms_tuned = timed(3)
+    ms = []
+    for _ in range(2):                     # capture, then a replay
+        ctx.launch()
+        outs = ctx.fetch()
+        ms.append(ctx.stats()["ms_kernel"])
+    ms_tuned = ms[-1]
     ctx.use_graph(False)
+    ctx.set_tile(0)
     ctx.set_schedule(0, 0)
+    pick = np.linspace(0, nspec - 1, BATCH_ACC).astype(int)
+    acc = accuracy(kt, cia, [(jobs[i], outs[i]) for i in pick], nthr, f"{BATCH_ACC} spectra of the batch")
     t = time.perf_counter()
     ctx.cirsrtfg_wave_batch(jobs)
     t_e2e = time.perf_counter() - t
@@ -309,19 +329,113 @@ def batch_leg(ctx, kt, nspec):
         "spectra": nspec, "wavenumbers": nwave,
         "value": nspec / (ms_tuned * 1e-3), "unit": "spectra/s",
         "ms_launch_tuned_graph": ms_tuned, "ms_launch_default": ms_default,
-        "tuned": {"schedule": ["static", "dynamic", "dynamic longest-first"][tune["schedule"]],
-                  "blocks_per_sm": tune["blocks_per_sm"], "candidates": tune["candidates"],
-                  "tuned_on_spectra": BATCH_TUNE},
+        "tuned": tune | {"schedule": ["static", "dynamic", "dynamic longest-first"][tune["schedule"]],
+                         "tile": f"{tune['warps']} warps per block (one layer per warp, one g-ordinate per lane, "
+                                 "one (spectrum, wavenumber) item per block)",
+                         "tuned_on_spectra": BATCH_TUNE},
         "prepare_s": t_prep,
         "e2e": {"value": nspec / t_e2e, "unit": "spectra/s", "h2d_bytes": st["h2d_bytes"],
-                "d2h_bytes": st["d2h_bytes"], "note": "rtb_cirsrtfg_wave_batch with host buffers, default schedule"},
+                "d2h_bytes": st["d2h_bytes"], "note": "rtb_cirsrtfg_wave_batch with host buffers, default tile"},
+        "accuracy": acc,
     }
 
 
-SERVE_RATE = 2000.0           # offered requests/s, Poisson
-SERVE_WINDOW = 0.25           # s of arrivals in the default run (the serving workload's 60 s: --serve-window 60)
+# ---------------------------------------------------------------- retrieval leg
+RET_N = 1024                  # the retrieval workload: 1024 full-size retrievals
+RET_FP64 = 16                 # of those, re-run with the all-FP64 Newton step
+RET_ACC = 4                   # final states whose forward model is checked against the FP64 oracle
+NEWTON_BATCH = 296            # retrievals per timed Newton-step launch (2 per SM)
+RET_WORKLOAD = ("optimal-estimation retrievals, full size: NX=124 (120 layer T + 4 log gas scales), NY=2000, "
+                "10 Newton iterations max, phlimit 0.1 %, Sa exponential correlation 1.5 scale heights "
+                "3 K / 50 %, Se diagonal (1e-9)^2, y = F(x_true) + N(0, 1e-9), x_true ~ N(xa, Sa)")
+
+
+def retrieval_cases(ctx, kt, n, seed0=4000):
+    """Full-size retrieval cases; observations from the device forward model
+    at the true states (batched launches) plus seeded noise."""
+    from radtrancode_b200 import synth
+    cases = [synth.make_retrieval(kt, synth.ABSORBERS_C2, nlayer=120, seed=seed0 + 17 * i, nwave=2000)
+             for i in range(n)]
+    outs = []
+    for b in range(0, n, 256):
+        outs += ctx.cirsrtfg_wave_batch([synth.job_at_state(c, c.x_true) for c in cases[b:b + 256]])
+    for i, c in enumerate(cases):
+        synth.observe(c, outs[i][0], seed=seed0 + 17 * i + 1)
+    return cases, outs
+
+
+def retrieval_leg(ctx, kt, cia, nret, bf16_peak, hbm_peak, nthr):
+    """Retrievals/s and completion-time percentiles of the batched engine
+    (rtb_retrieve_batch), the mixed-precision result against the all-FP64
+    device solve, the forward model at the retrieved states against the FP64
+    oracle, the Newton kernel against the tensor and HBM peaks, and the
+    oracle's retrieval on the host cores."""
+    from oracle import pyoracle as po
+    from radtrancode_b200 import synth
+    cases, outs = retrieval_cases(ctx, kt, nret)
+    ctx.set_newton_mode(0, 1)
+    t = time.perf_counter()
+    res = ctx.retrieve_batch(cases, kiter=10, phlimit=0.1)
+    dt = time.perf_counter() - t
+    lat = np.array([r["ms"] for r in res])
+    ctx.set_newton_mode(1, 0)
+    try:
+        res64 = ctx.retrieve_batch(cases[:RET_FP64], kiter=10, phlimit=0.1)
+    finally:
+        ctx.set_newton_mode(0, 1)
+    dx, same = 0.0, 0
+    for c, a, b in zip(cases, res, res64):
+        sig = np.sqrt(np.diag(c.sa))
+        dx = max(dx, float(np.max(np.abs(a["x"] - b["x"]) / sig)))
+        same += int(a["iterations"] == b["iterations"] and a["converged"] == b["converged"])
+    # the forward model at retrieved states, device vs FP64 oracle
+    jobs = [synth.job_at_state(cases[i], res[i]["x"]) for i in range(RET_ACC)]
+    acc = accuracy(kt, cia, list(zip(jobs, ctx.cirsrtfg_wave_batch(jobs))), nthr,
+                   f"the forward model at {RET_ACC} retrieved states")
+    # Newton-step kernel alone: NEWTON_BATCH retrievals of K at the true states
+    pick = [i % nret for i in range(NEWTON_BATCH)]
+    kk = np.stack([outs[i][1].reshape(124, 2000) for i in pick])
+    sai = np.stack([np.linalg.inv(cases[i].sa) for i in pick])
+    sei = np.stack([cases[i].sei for i in pick])
+    xa = np.stack([cases[i].xa for i in pick])
+    y = np.stack([cases[i].y for i in pick])
+    yn = np.stack([outs[i][0] for i in pick])
+    ms_newton = []
+    for _ in range(4):
+        ctx.newton_step_batch(kk, sei, sai, xa, xa, y, yn)
+        ms_newton.append(ctx.newton_stats()["ms_kernel"])
+    ms_n = statistics.median(ms_newton[1:])
+    flops = NEWTON_BATCH * (2.0 * 124 * 124 * 2000 + 2.0 * 124 * 2000)
+    tflops = flops / (ms_n * 1e-3) / 1e12
+    kbytes = NEWTON_BATCH * 124 * 2000 * 4 * 2        # K read by the product pass and the refinement pass
+    t = time.perf_counter()
+    po.retrieve(kt, cia, cases[0], kiter=10, phlimit=0.1, nthreads=nthr)
+    t_cpu = time.perf_counter() - t
+    return {
+        "workload": RET_WORKLOAD, "retrievals": nret, "value": nret / dt, "unit": "retrievals/s",
+        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+        "latency_note": "completion time from the start of the batched call (all admitted at once)",
+        "iterations_mean": float(np.mean([r["iterations"] for r in res])),
+        "forwards_mean": float(np.mean([r["forwards"] for r in res])),
+        "converged": int(sum(r["converged"] > 0 for r in res)),
+        "accuracy": acc,
+        "newton": {"hessian": "K~ = Se^-1/2 K as bf16 hi + lo, hi*hi + hi*lo + lo*hi by tcgen05.mma (M=N=128, K=16) "
+                              "into an FP32 accumulator in tensor memory; 1 FP64 refinement step; FP64 Cholesky",
+                   "vs_fp64_solve": {"retrievals": RET_FP64, "max_dx_over_prior_sigma": dx,
+                                     "same_iterations_and_stop_rule": same}},
+        "newton_kernel": {"batch": NEWTON_BATCH, "ms": ms_n, "achieved_tflops": tflops, "peak_tflops": bf16_peak,
+                          "frac": tflops / bf16_peak, "flops_per_retrieval": "2 NX^2 NY + 2 NX NY",
+                          "k_read_gbs": kbytes / (ms_n * 1e-3) / 1e9,
+                          "k_read_frac_of_hbm": kbytes / (ms_n * 1e-3) / 1e9 / hbm_peak},
+        "cpu_baseline": {"value": 1.0 / t_cpu, "unit": "retrievals/s", "cores": nthr, "kind": "port",
+                         "sample": f"1 retrieval of the same workload, oracle coreret restatement, {nthr} threads"},
+    }
+
+
+# ---------------------------------------------------------------- serving leg
+SERVE_POINTS = ((2000.0, 0.5, 256 << 20), (40.0, 30.0, 16 << 30))   # (req/s, s of arrivals, HBM budget)
 SERVE_PLAIN = 24              # requests run one at a time for the plain per-request form
-SERVE_BUDGET = 16 << 30       # HBM arena of the server
+SERVE_CHECK = 4               # served results re-run alone: bit-identical
 
 
 def serving_cases(ctx, kt, n, seed=5000):
@@ -339,45 +453,81 @@ def serving_cases(ctx, kt, n, seed=5000):
         ab = [synth.ABSORBERS_C2[k] for k in sorted(rng.choice(4, size=na, replace=False))]
         cases.append(synth.make_retrieval(kt, ab, nlayer=L, seed=seed + 7 * i + 1, nwave=w, iw0=iw0,
                                           theta_deg=float(rng.uniform(0.0, 70.0))))
-    outs = ctx.cirsrtfg_wave_batch([synth.job_at_state(c, c.x_true) for c in cases])
+    outs = []
+    for b in range(0, n, 512):
+        outs += ctx.cirsrtfg_wave_batch([synth.job_at_state(c, c.x_true) for c in cases[b:b + 512]])
     for i, c in enumerate(cases):
         synth.observe(c, outs[i][0], seed=seed + 7 * i + 2)
     return cases
 
 
-def serving_leg(ctx, kt, window, rate):
+def serve_point(ctx, kt, rate, window, budget, seed):
     """Poisson arrivals into the continuous-batching server; latency from
-    each request's arrival time to its completion.  Beside it the plain
-    per-request GPU form (one retrieval at a time through
-    rtb_retrieve_batch)."""
+    each request's arrival time to its completion; a few served results
+    re-run alone (bit-identical expected)."""
     from radtrancode_b200 import cirsradg
-    rng = np.random.default_rng(77)
+    rng = np.random.default_rng(seed)
     arr = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * window * 1.5) + 16))
     arr = arr[arr < window]
     n = len(arr)
-    cases = serving_cases(ctx, kt, n)
-    lat, its, rounds, peak_active = [], [], 0, 0
+    cases = serving_cases(ctx, kt, n, seed=5000 + seed)
+    lat, its, rounds, peak, queued_rounds, step_s = [], [], 0, 0, 0, 0.0
+    results = {}
     i, pending = 0, {}
     t0 = time.perf_counter()
-    with cirsradg.Server(ctx, SERVE_BUDGET, kiter=15, phlimit=0.1, dchisq_stop=0.1) as srv:
+    with cirsradg.Server(ctx, budget, kiter=15, phlimit=0.1, dchisq_stop=0.1) as srv:
         while i < n or pending:
             now = time.perf_counter() - t0
             while i < n and arr[i] <= now:
-                pending[srv.submit(cases[i])] = arr[i]
+                pending[srv.submit(cases[i])] = (i, arr[i])
                 i += 1
             if not pending:
                 time.sleep(max(0.0, arr[i] - now))
                 continue
-            active, _ = srv.step()
+            t1 = time.perf_counter()
+            active, queued = srv.step()
+            step_s += time.perf_counter() - t1
             rounds += 1
-            peak_active = max(peak_active, active)
+            peak = max(peak, active)
+            queued_rounds += int(queued > 0)
             t = time.perf_counter() - t0
             for rid in list(pending):
                 r = srv.poll(rid)
                 if r is not None:
-                    lat.append((t - pending.pop(rid)) * 1e3)
+                    k, a = pending.pop(rid)
+                    lat.append((t - a) * 1e3)
                     its.append(r["iterations"])
+                    results[k] = r
     t_total = time.perf_counter() - t0
+    same = 0
+    for k in sorted(results)[:SERVE_CHECK]:
+        alone = ctx.retrieve_batch([cases[k]], kiter=15, phlimit=0.1, dchisq_stop=0.1)[0]
+        same += int(np.array_equal(alone["x"], results[k]["x"]) and alone["iterations"] == results[k]["iterations"])
+    lat = np.array(lat)
+    return cases, {
+        "offered_rate": rate, "window_s": window, "hbm_budget_bytes": budget, "requests": n,
+        "value": n / t_total, "unit": "retrievals/s", "wall_s": t_total, "rounds": rounds,
+        "peak_in_flight": peak, "rounds_with_requests_waiting_for_memory": queued_rounds,
+        "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
+        "p99_ms": float(np.percentile(lat, 99)), "iterations_mean": float(np.mean(its)),
+        "server_step_s": step_s,
+        "alone_vs_mix": {"checked": min(SERVE_CHECK, len(results)), "bit_identical": same},
+    }
+
+
+def serving_leg(ctx, kt, cia, nthr, points=SERVE_POINTS):
+    """The server at each (rate, window, budget) point, the plain per-request
+    GPU form beside it, and the forward model at served states against the
+    FP64 oracle."""
+    from radtrancode_b200 import synth
+    out = {"workload": "Poisson arrivals, sizes of the uneven batch (W~U[200,2000], L~U[40,120], 1-4 absorbers), "
+                       "up to 15 Newton iterations, early exit at |delta chi2| < 0.1, continuous batching under an "
+                       "HBM budget; latency from each request's arrival", "points": []}
+    cases = None
+    for k, (rate, window, budget) in enumerate(points):
+        cs, pt = serve_point(ctx, kt, rate, window, budget, seed=77 + k)
+        out["points"].append(pt)
+        cases = cases or cs
     plain = []
     t = time.perf_counter()
     for c in cases[:SERVE_PLAIN]:
@@ -385,236 +535,108 @@ def serving_leg(ctx, kt, window, rate):
         ctx.retrieve_batch([c], kiter=15, phlimit=0.1, dchisq_stop=0.1)
         plain.append((time.perf_counter() - t1) * 1e3)
     t_plain = time.perf_counter() - t
-    lat = np.array(lat)
-    return {
-        "workload": f"Poisson arrivals at {rate:.0f} req/s for {window} s ({n} requests), sizes of the uneven batch, "
-                    "up to 15 Newton iterations, early exit at |delta chi2| < 0.1, HBM budget "
-                    f"{SERVE_BUDGET >> 30} GiB",
-        "requests": n, "value": n / t_total, "unit": "retrievals/s", "wall_s": t_total, "rounds": rounds,
-        "peak_in_flight": peak_active,
-        "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
-        "p99_ms": float(np.percentile(lat, 99)), "iterations_mean": float(np.mean(its)),
-        "latency_note": "from the request's arrival time; the offered rate is above the service rate, so "
-                        "latency includes the wait for the backlog",
-        "plain_per_request": {"requests": SERVE_PLAIN, "value": SERVE_PLAIN / t_plain, "unit": "retrievals/s",
-                              "p50_ms": float(np.percentile(plain, 50)), "p99_ms": float(np.percentile(plain, 99)),
-                              "note": "one request at a time, rtb_retrieve_batch of one, service time only"},
-    }
+    out["plain_per_request"] = {"requests": SERVE_PLAIN, "value": SERVE_PLAIN / t_plain, "unit": "retrievals/s",
+                                "p50_ms": float(np.percentile(plain, 50)), "p99_ms": float(np.percentile(plain, 99)),
+                                "note": "one request at a time, rtb_retrieve_batch of one, service time only"}
+    sel = cases[:4]
+    res = ctx.retrieve_batch(sel, kiter=15, phlimit=0.1, dchisq_stop=0.1)
+    jobs = [synth.job_at_state(c, r["x"]) for c, r in zip(sel, res)]
+    out["accuracy"] = accuracy(kt, cia, list(zip(jobs, ctx.cirsrtfg_wave_batch(jobs))), nthr,
+                               "the forward model at 4 served states")
+    out["value"] = out["points"][0]["value"]
+    out["unit"] = "retrievals/s"
+    return out
 
 
-def retrieval_cases(ctx, kt, n, seed0=4000):
-    """Full-size retrieval cases; observations from the device forward model
-    at the true states (one batched launch) plus seeded noise."""
-    from radtrancode_b200 import synth
-    cases = [synth.make_retrieval(kt, synth.ABSORBERS_C2, nlayer=120, seed=seed0 + 17 * i, nwave=2000)
-             for i in range(n)]
-    outs = ctx.cirsrtfg_wave_batch([synth.job_at_state(c, c.x_true) for c in cases])
-    for i, c in enumerate(cases):
-        synth.observe(c, outs[i][0], seed=seed0 + 17 * i + 1)
-    return cases, outs
-
-
-def retrieval_leg(ctx, kt, cia, bf16_peak):
-    """Retrievals/s and completion-time percentiles of the batched engine
-    (rtb_retrieve_batch), the mixed-precision result against the all-FP64
-    device solve, the Newton kernel against the tensor peak, and the oracle
-    retrieval on the host cores."""
-    from oracle import pyoracle as po
-    cases, outs = retrieval_cases(ctx, kt, RET_SAMPLE)
-    ctx.set_newton_mode(0, 1)
-    t = time.perf_counter()
-    res = ctx.retrieve_batch(cases, kiter=10, phlimit=0.1)
-    dt = time.perf_counter() - t
-    lat = np.array([r["ms"] for r in res])
-    ctx.set_newton_mode(1, 0)
-    try:
-        res64 = ctx.retrieve_batch(cases[:RET_FP64_SAMPLE], kiter=10, phlimit=0.1)
-    finally:
-        ctx.set_newton_mode(0, 1)
-    dx, same = 0.0, 0
-    for c, a, b in zip(cases, res, res64):
-        sig = np.sqrt(np.diag(c.sa))
-        dx = max(dx, float(np.max(np.abs(a["x"] - b["x"]) / sig)))
-        same += int(a["iterations"] == b["iterations"] and a["converged"] == b["converged"])
-    # Newton-step kernel alone: NEWTON_BATCH retrievals of K at the true states
-    pick = [i % RET_SAMPLE for i in range(NEWTON_BATCH)]
-    kk = np.stack([outs[i][1].reshape(124, 2000) for i in pick])
-    sai = np.stack([np.linalg.inv(cases[i].sa) for i in pick])
-    sei = np.stack([cases[i].sei for i in pick])
-    xa = np.stack([cases[i].xa for i in pick])
-    y = np.stack([cases[i].y for i in pick])
-    yn = np.stack([outs[i][0] for i in pick])
-    ms_newton = []
-    for _ in range(4):
-        ctx.newton_step_batch(kk, sei, sai, xa, xa, y, yn)
-        ms_newton.append(ctx.newton_stats()["ms_kernel"])
-    ms_n = statistics.median(ms_newton[1:])
-    flops = NEWTON_BATCH * (2.0 * 124 * 124 * 2000 + 2.0 * 124 * 2000)
-    tflops = flops / (ms_n * 1e-3) / 1e12
-    # the oracle's retrieval on the host cores: one case, all threads
-    nthr = os.cpu_count() or 1
-    t = time.perf_counter()
-    po.retrieve(kt, cia, cases[0], kiter=10, phlimit=0.1, nthreads=nthr)
-    t_cpu = time.perf_counter() - t
-    return {
-        "workload": RET_WORKLOAD, "retrievals": RET_SAMPLE, "value": RET_SAMPLE / dt, "unit": "retrievals/s",
-        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-        "latency_note": "completion time from the start of the batched call (all admitted at once)",
-        "iterations_mean": float(np.mean([r["iterations"] for r in res])),
-        "forwards_mean": float(np.mean([r["forwards"] for r in res])),
-        "converged": int(sum(r["converged"] > 0 for r in res)),
-        "newton": {"hessian": "bf16 hi/lo split on tensor cores (mma.sync m16n8k16), FP32 accumulation, "
-                              "1 FP64 refinement step; FP64 Cholesky",
-                   "vs_fp64_solve": {"retrievals": RET_FP64_SAMPLE, "max_dx_over_prior_sigma": dx,
-                                     "same_iterations_and_stop_rule": same}},
-        "newton_kernel": {"batch": NEWTON_BATCH, "ms": ms_n, "achieved_tflops": tflops, "peak_tflops": bf16_peak,
-                          "frac": tflops / bf16_peak, "flops_per_retrieval": "2 NX^2 NY + 2 NX NY"},
-        "cpu_baseline": {"value": 1.0 / t_cpu, "unit": "retrievals/s", "cores": nthr, "kind": "port",
-                         "sample": f"1 retrieval of the same workload, oracle coreret restatement, {nthr} threads"},
-    }
-
-
+# ---------------------------------------------------------------- profiling cases
 def profile_case(args):
-    """Reduced case for ncu captures: the same spectrum cut to its first
-    `--profile-waves` wavenumbers, warm-up + `--steps` launches."""
+    """Reduced cases for ncu captures (warm-up + --steps launches each):
+      forward  the full-size spectrum cut to its first --profile-size wavenumbers
+      newton   --profile-size full-size Newton steps (NX=124, NY=2000)
+      aux      calc_phiret, the Sa inverse, calc_gain_matrix + calcnextxn on --profile-size retrievals
+      layers   --profile-size calls of rtb_layerg on the full-size profile (121 levels, 6 gases, 30 deg)
+      conv     --profile-size convolutions of a full-size spectrum's 126 series onto 600 square-bin
+               channels (FWHM 1.2 cm-1) and 200 filter channels"""
     from radtrancode_b200 import cirsradg, synth
-    kt, cia, _ = synth.config2()
-    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, nwave=args.profile_waves, vmr_perturb=0.3)
-    with cirsradg.Context(0) as ctx:
-        ctx.set_ktables(kt)
-        ctx.set_cia(cia)
-        ctx.prepare([job])
-        for _ in range(args.warmup + args.steps):
-            ctx.launch()
-            ctx.fetch()
-            print(json.dumps({"profile_waves": args.profile_waves, "ms_kernel": ctx.stats()["ms_kernel"]}))
-
-
-def profile_newton(args):
-    """Reduced case for ncu captures of the Newton-step kernel:
-    `--profile-newton` full-size retrievals (NX=124, NY=2000) with seeded
-    K of the forward model's magnitude, warm-up + `--steps` launches."""
-    from radtrancode_b200 import cirsradg, synth
-    n, nx, ny = args.profile_newton, 124, 2000
+    n, what = args.profile_size, args.profile
     rng = np.random.default_rng(11)
-    p_lev, p_lay = synth._levels(120)
-    sa = synth.prior_covariance(p_lay, 4)
-    sai = np.broadcast_to(np.linalg.inv(sa), (n, nx, nx))
-    kk = (rng.standard_normal((n, nx, ny)) * 1e-9).astype(np.float32)
-    sei = np.full((n, ny), 1e18)
-    xa = np.full((n, nx), 150.0, np.float32)
-    y = (rng.standard_normal((n, ny)) * 1e-8).astype(np.float32)
-    yn = np.zeros((n, ny), np.float32)
     with cirsradg.Context(0) as ctx:
-        for _ in range(args.warmup + args.steps):
-            ctx.newton_step_batch(kk, sei, sai, xa, xa, y, yn)
-            print(json.dumps({"profile_newton": n, "ms_kernel": ctx.newton_stats()["ms_kernel"]}))
+        if what == "forward":
+            kt, cia, _ = synth.config2()
+            job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, nwave=n, vmr_perturb=0.3)
+            ctx.set_ktables(kt)
+            ctx.set_cia(cia)
+            ctx.prepare([job])
+            for _ in range(args.warmup + args.steps):
+                ctx.launch()
+                ctx.fetch()
+                print(json.dumps({"profile": what, "ms_kernel": ctx.stats()["ms_kernel"]}))
+        elif what in ("newton", "aux"):
+            nx, ny = 124, 2000
+            _, p_lay = synth._levels(120)
+            sa = synth.prior_covariance(p_lay, 4)
+            sai = np.broadcast_to(np.linalg.inv(sa), (n, nx, nx))
+            sei = np.full((n, ny), 1e18)
+            xa = np.full((n, nx), 150.0, np.float32)
+            xn = xa + rng.standard_normal((n, nx)).astype(np.float32)
+            y = (rng.standard_normal((n, ny)) * 1e-8).astype(np.float32)
+            yn = np.zeros((n, ny), np.float32)
+            for _ in range(args.warmup + args.steps):
+                if what == "newton":
+                    kk = (rng.standard_normal((n, nx, ny)) * 1e-9).astype(np.float32)
+                    ctx.newton_step_batch(kk, sei, sai, xa, xa, y, yn)
+                    print(json.dumps({"profile": what, "ms_kernel": ctx.newton_stats()["ms_kernel"]}))
+                else:
+                    kk = (rng.standard_normal((nx, ny)) * 1e-9).astype(np.float32)
+                    phi, _ = ctx.calc_phiret_batch(y, yn, sei, xn, xa, sai)
+                    ctx.spd_inverse_batch(np.broadcast_to(sa, (n, nx, nx)))
+                    dd, aa, _ = ctx.calc_gain_matrix(kk, sai[0], sei[0])
+                    x = ctx.calcnextxn(xa[0], xn[0], y[0], yn[0], dd, aa)
+                    print(json.dumps({"profile": what, "phi0": float(phi[0]), "x0": float(x[0])}))
+        elif what == "layers":
+            prof = synth.make_profile(synth.ABSORBERS_C2, npro=121, seed=1005)
+            for i in range(args.warmup + n):
+                t0 = time.perf_counter()
+                lay = ctx.layerg(prof, nlay=120, laytyp=1, layint=1, angle=30.0)
+                print(json.dumps({"profile": what, "call_ms": 1e3 * (time.perf_counter() - t0),
+                                  "totam0": float(lay["totam"][0])}))
+        elif what == "conv":
+            kt, cia, _ = synth.config2()
+            job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, nwave=2000, vmr_perturb=0.3)
+            vw = job.vwave
+            vc = (vw[0] + 5.0 + np.arange(600) * 1.3).astype(np.float32)
+            vf = (vw[0] + 10.0 + np.arange(200) * 3.9).astype(np.float32)
+            tri = np.array([-1.5, -0.5, 0.0, 0.5, 1.5], np.float32)
+            fil = synth.Channels(vconv=vf, vcen=vf, nsub=np.full(200, 5, np.int32), vfil=(vf[:, None] + tri).ravel(),
+                                 fil=np.tile(np.array([0.0, 0.6, 1.0, 0.6, 0.0], np.float32), 200))
+            ctx.set_ktables(kt)
+            ctx.set_cia(cia)
+            c, g, gt = ctx.cirsrtfg_wave(job)
+            series = np.vstack([c[None], gt[None], g.reshape(job.nv, job.nwave)])
+            for i in range(args.warmup + n):
+                t0 = time.perf_counter()
+                a = ctx.cirsconv_ex(vw, series, 1.2, synth.Channels(vconv=vc))
+                b = ctx.cirsconv_ex(vw, series, -1.0, fil)
+                print(json.dumps({"profile": what, "call_ms": 1e3 * (time.perf_counter() - t0),
+                                  "a0": float(a[0, 0]), "b0": float(b[0, 0])}))
 
 
-def profile_aux(args):
-    """Reduced case for ncu captures of the small kernels of the Newton-step
-    interface: `--profile-aux` retrievals (NX=124, NY=2000) through
-    calc_phiret, the Sa inverse, then one calc_gain_matrix + calcnextxn."""
-    from radtrancode_b200 import cirsradg, synth
-    n, nx, ny = args.profile_aux, 124, 2000
-    rng = np.random.default_rng(12)
-    p_lev, p_lay = synth._levels(120)
-    sa = synth.prior_covariance(p_lay, 4)
-    sai1 = np.linalg.inv(sa)
-    sai = np.broadcast_to(sai1, (n, nx, nx))
-    sei = np.full((n, ny), 1e18)
-    xa = np.full((n, nx), 150.0, np.float32)
-    xn = xa + rng.standard_normal((n, nx)).astype(np.float32)
-    y = (rng.standard_normal((n, ny)) * 1e-8).astype(np.float32)
-    yn = np.zeros((n, ny), np.float32)
-    kk = (rng.standard_normal((nx, ny)) * 1e-9).astype(np.float32)
-    with cirsradg.Context(0) as ctx:
-        for _ in range(args.warmup + args.steps):
-            phi, _ = ctx.calc_phiret_batch(y, yn, sei, xn, xa, sai)
-            ctx.spd_inverse_batch(np.broadcast_to(sa, (n, nx, nx)))
-            dd, aa, _ = ctx.calc_gain_matrix(kk, sai1, sei[0])
-            x = ctx.calcnextxn(xa[0], xn[0], y[0], yn[0], dd, aa)
-            print(json.dumps({"profile_aux": n, "phi0": float(phi[0]), "x0": float(x[0])}))
-
-
-def profile_layers(args):
-    """Reduced case for ncu captures of the layering kernel: `--profile-layers`
-    calls of rtb_layerg on a 121-level, 6-gas profile into 120 Curtis-Godson
-    layers on a 30-degree path (the full-size atmosphere), after warm-up."""
-    from radtrancode_b200 import cirsradg, synth
-    prof = synth.make_profile(synth.ABSORBERS_C2, npro=121, seed=1005)
-    with cirsradg.Context(0) as ctx:
-        for i in range(args.warmup + args.profile_layers):
-            t0 = time.perf_counter()
-            lay = ctx.layerg(prof, nlay=120, laytyp=1, layint=1, angle=30.0)
-            print(json.dumps({"profile_layers": i, "call_ms": 1e3 * (time.perf_counter() - t0),
-                              "totam0": float(lay["totam"][0])}))
-
-
-def profile_conv(args):
-    """Reduced case for ncu captures of the convolution kernels: the
-    full-size spectrum's radiance, d/dtsurf and 124 Jacobian rows (126 series
-    of 2000 points) convolved `--profile-conv` times onto 600 square-bin
-    channels (FWHM 1.2 cm-1) and onto 200 filter channels (FWHM < 0)."""
-    from radtrancode_b200 import cirsradg, synth
-    kt, cia, _ = synth.config2()
-    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=120, seed=1003, nwave=2000, vmr_perturb=0.3)
-    vw = job.vwave
-    vc = (vw[0] + 5.0 + np.arange(600) * 1.3).astype(np.float32)
-    vf = (vw[0] + 10.0 + np.arange(200) * 3.9).astype(np.float32)
-    tri = np.array([-1.5, -0.5, 0.0, 0.5, 1.5], np.float32)
-    fil = synth.Channels(vconv=vf, vcen=vf, nsub=np.full(200, 5, np.int32), vfil=(vf[:, None] + tri).ravel(),
-                         fil=np.tile(np.array([0.0, 0.6, 1.0, 0.6, 0.0], np.float32), 200))
-    with cirsradg.Context(0) as ctx:
-        ctx.set_ktables(kt)
-        ctx.set_cia(cia)
-        c, g, gt = ctx.cirsrtfg_wave(job)
-        series = np.vstack([c[None], gt[None], g.reshape(job.nv, job.nwave)])
-        for i in range(args.warmup + args.profile_conv):
-            t0 = time.perf_counter()
-            a = ctx.cirsconv_ex(vw, series, 1.2, synth.Channels(vconv=vc))
-            b = ctx.cirsconv_ex(vw, series, -1.0, fil)
-            print(json.dumps({"profile_conv": i, "call_ms": 1e3 * (time.perf_counter() - t0),
-                              "a0": float(a[0, 0]), "b0": float(b[0, 0])}))
-
-
+# ---------------------------------------------------------------- main
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--profile-waves", type=int, default=0,
-                    help="profiling case: only launch the forward kernel on the first N wavenumbers of the "
-                         "workload (steps launches after warmup), print the kernel time, skip e2e and baselines")
-    ap.add_argument("--no-retrieval", action="store_true", help="skip the retrieval leg")
-    ap.add_argument("--serve-window", type=float, default=SERVE_WINDOW,
-                    help="seconds of Poisson arrivals in the serving leg (0 skips it)")
-    ap.add_argument("--batch-spectra", type=int, default=BATCH_SPECTRA,
-                    help="uneven spectra in the batched leg (0 skips it)")
-    ap.add_argument("--profile-newton", type=int, default=0,
-                    help="profiling case: only the Newton-step kernel on N full-size retrievals")
-    ap.add_argument("--profile-aux", type=int, default=0,
-                    help="profiling case: the small kernels of the Newton-step interface on N retrievals")
-    ap.add_argument("--profile-layers", type=int, default=0,
-                    help="profiling case: N calls of the layering kernel on the full-size profile")
-    ap.add_argument("--profile-conv", type=int, default=0,
-                    help="profiling case: N convolutions of a full-size spectrum's outputs")
+    ap.add_argument("--batch-spectra", type=int, default=BATCH_SPECTRA, help="uneven spectra of the batch leg (0 skips)")
+    ap.add_argument("--retrievals", type=int, default=RET_N, help="retrievals of the retrieval leg (0 skips)")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--profile", choices=["forward", "newton", "aux", "layers", "conv"], default=None,
+                    help="run one reduced profiling case instead of the benchmark")
+    ap.add_argument("--profile-size", type=int, default=16)
     args = ap.parse_args()
-    if args.profile_layers:
-        profile_layers(args)
-        return
-    if args.profile_conv:
-        profile_conv(args)
-        return
-    if args.profile_aux:
-        profile_aux(args)
-        return
-    if args.profile_waves:
+    if args.profile:
         profile_case(args)
-        return
-    if args.profile_newton:
-        profile_newton(args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -623,6 +645,9 @@ def main():
         reference_arm(args, rank)
         return
 
+    if rank == 0 and world == 1:
+        from oracle import pyoracle as po
+        po.use_native()        # the CPU baseline, built here for this host's CPU, before any GPU work
     import torch
     import torch.distributed as dist
 
@@ -684,10 +709,20 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms_step, t_e2e = float(tt[0]), float(tt[1])
     if rank == 0:
-        hbm, how = peaks()
+        hbm, bf16, how = measured_peaks()
         ab = algorithmic_bytes(kt, job, st_e2e["h2d_bytes"], st_e2e["d2h_bytes"])
         achieved = ab / (ms_step * 1e-3) / 1e9
-        traffic = profile_traffic()
+        prof = profile_data()
+        nthr = os.cpu_count() or 1
+        elems = st["sort_passes"] * kt.ng * kt.ng
+        issue = None
+        if prof.get("warp_instructions_per_launch") and clk and clk.get("sm_mhz"):
+            ceiling = 148 * 4 * clk["sm_mhz"] * 1e6               # warp instructions/s at 4 per SM per cycle
+            got = prof["warp_instructions_per_launch"] / (ms_step * 1e-3)
+            issue = {"achieved_warp_inst_per_s": got, "ceiling": ceiling, "frac": got / ceiling,
+                     "warp_inst_per_sorted_pass": prof["warp_instructions_per_launch"] / max(1, st["sort_passes"]),
+                     "source": "ncu warp instructions of one launch (profiles/fwd_kernel_config2.json), "
+                               "ceiling 148 SMs x 4 issues x the sampled SM clock"}
         out = {
             "metric": METRIC, "value": world * 1000.0 / ms_step, "unit": "spectra/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -699,24 +734,26 @@ def main():
                     "d2h_bytes_per_step": st_e2e["d2h_bytes"]},
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic,
+                         "frac": achieved / hbm, "traffic": prof.get("dram_bytes_per_launch"),
                          "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs, burst)" if how == "measured" else
                                          "fallback: the pool's earlier copy measurement (MEASURED_PEAKS.json absent)"),
                          "algorithmic_bytes_per_launch": ab, "kernel": "fwd_kernel"},
+            "issue_roofline": issue,
+            "sorted_elements_per_s": elems / (ms_step * 1e-3),
             "overlap_passes": {"sorted": st["sort_passes"], "with_ties": st["tie_passes"],
-                               "reference_heapsort": st["exact_passes"], "irregular": st["irregular_passes"]},
+                               "reference_heapsort": st["exact_passes"], "irregular": st["irregular_passes"],
+                               "rows_already_sorted": st["block_passes"]},
             "clocks": clk,
         }
         if world == 1:
-            base, acc = cpu_baseline_and_accuracy(kt, cia, job, gpu_out)
-            out["cpu_baseline"] = base
-            out["accuracy"] = acc
+            out["cpu_baseline"] = cpu_baseline(kt, cia, job, nthr)
+            out["accuracy"] = accuracy(kt, cia, [(job, gpu_out)], nthr, "the whole measured spectrum")
             if args.batch_spectra > 0:
-                out["batch"] = batch_leg(ctx, kt, args.batch_spectra)
-            if not args.no_retrieval:
-                out["retrieval"] = retrieval_leg(ctx, kt, cia, tensor_peak())
-            if args.serve_window > 0:
-                out["serving"] = serving_leg(ctx, kt, args.serve_window, SERVE_RATE)
+                out["batch"] = batch_leg(ctx, kt, cia, args.batch_spectra, nthr)
+            if args.retrievals > 0:
+                out["retrieval"] = retrieval_leg(ctx, kt, cia, args.retrievals, bf16, hbm, nthr)
+            if not args.no_serving:
+                out["serving"] = serving_leg(ctx, kt, cia, nthr)
         print(json.dumps(out))
     ctx.close()
     if world > 1:

@@ -371,6 +371,7 @@ typedef struct rtb_fwd_stats {
     long long block_passes;           /* passes sorted by row-block ranks (no merge) */
     long long h2d_bytes, d2h_bytes;   /* host<->device bytes of the call */
     float ms_kernel;
+    int grid;                         /* blocks of the last forward launch */
 } rtb_fwd_stats;
 int rtb_get_fwd_stats(const rtb_context* ctx, rtb_fwd_stats* out);
 
@@ -404,16 +405,28 @@ int rtb_set_strict_ties(rtb_context* ctx, int on);
  * schedule (each item is computed by one block, in the same order). */
 int rtb_fwd_set_schedule(rtb_context* ctx, int schedule, int blocks_per_sm);
 
-/* Time the resident batch under every schedule and the three highest
- * occupancies (two launches each, the second timed), keep the fastest and
- * report it.  Every candidate runs the whole batch: tune on a
- * representative batch and carry the result to larger ones with
- * rtb_fwd_set_schedule. */
+/* Tile shape of the resident batch's launches: warps per block, i.e. the
+ * layers of one (spectrum, wavenumber) item worked on at once (one warp per
+ * layer, one lane per g-ordinate): 2, 4 or 8; 0 = the default 4.  Tiles
+ * other than 4 exist for the usual kernel instance (one temperature grid, no
+ * para-H2 / IMOD 18 / iform / non-LTE / air-Rayleigh option); other batches
+ * run 4.  Results do not depend on the tile. */
+int rtb_fwd_set_tile(rtb_context* ctx, int warps);
+
+/* Time the resident batch under every tile (2, 4, 8 warps per block) x
+ * schedule x the three highest occupancies of the tile (two launches each,
+ * the second timed), keep the fastest and report it.  The result is also
+ * kept in the context under the batch's shape (its largest layer count in
+ * buckets of 20 layers, and its largest gas count): a later rtb_fwd_prepare
+ * of a batch of the same shape starts with it (tune on a representative
+ * batch, run the large one).  rtb_fwd_set_schedule / rtb_fwd_set_tile after
+ * the prepare override it. */
 typedef struct rtb_fwd_tune {
     int schedule;
     int blocks_per_sm;
     float ms;          /* launch time of the chosen configuration */
     int candidates;    /* configurations timed */
+    int warps;         /* warps per block of the chosen tile */
 } rtb_fwd_tune;
 int rtb_fwd_autotune(rtb_context* ctx, rtb_fwd_tune* out);
 
@@ -712,13 +725,20 @@ int  rtb_server_poll(rtb_server* srv, long long id, int* done, rtb_retrieval_res
  * RTB_STATIC_SCRATCH_BYTES per device, instead of the context's scratch.
  * Outputs, status and statistics are read with rtb_fwd_fetch as usual.
  *
+ * Only the launch is allocation-free: rtb_fwd_prepare, which runs at set-up,
+ * still sizes and allocates the context's buffers (the packed batch, the
+ * outputs and the ordinary per-block scratch), as for rtb_fwd_launch.
  * First call: the first call on each device looks up the array's device
  * address (cudaGetSymbolAddress, with that device current) and keeps it for
  * the process; make that first call before any stream capture is started.
+ * The address is not looked up again: after cudaDeviceReset (or with another
+ * CUDA context made current on the device) it is stale, so a process that
+ * resets a device must not call this entry point on it again.
  * Limit: a batch whose per-block slot (layers x NG x (1 + gradient columns)
- * floats) does not fit in RTB_STATIC_SCRATCH_BYTES is refused with
+ * floats, plus the parked k-distributions of wavenumbers between two table
+ * points) does not fit in RTB_STATIC_SCRATCH_BYTES is refused with
  * RTB_ERR_LIMIT; a batch whose slots fit fewer blocks than rtb_fwd_launch
- * would use runs on that many blocks.  Nothing in the array needs to start at
+ * would use runs on that many blocks (rtb_fwd_stats.grid).  Nothing in the array needs to start at
  * zero; the status and counter words that do are cleared on the stream by
  * every call.
  * Races: the array is one per device, shared by every context of the process

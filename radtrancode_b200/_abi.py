@@ -94,7 +94,7 @@ class RtbFwdStats(C.Structure):
     _fields_ = [
         ("cells", C.c_longlong), ("sort_passes", C.c_longlong), ("tie_passes", C.c_longlong),
         ("exact_passes", C.c_longlong), ("irregular_passes", C.c_longlong), ("block_passes", C.c_longlong),
-        ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong), ("ms_kernel", C.c_float),
+        ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong), ("ms_kernel", C.c_float), ("grid", C.c_int),
     ]
 
 
@@ -122,7 +122,8 @@ class RtbRetrievalResult(C.Structure):
 
 
 class RtbFwdTune(C.Structure):
-    _fields_ = [("schedule", C.c_int), ("blocks_per_sm", C.c_int), ("ms", C.c_float), ("candidates", C.c_int)]
+    _fields_ = [("schedule", C.c_int), ("blocks_per_sm", C.c_int), ("ms", C.c_float), ("candidates", C.c_int),
+                ("warps", C.c_int)]
 
 
 class RtbNewtonStats(C.Structure):

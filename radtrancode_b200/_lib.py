@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
         L.rtb_get_newton_stats.restype = C.c_int
         L.rtb_fwd_set_schedule.argtypes = [vp, C.c_int, C.c_int]
         L.rtb_fwd_set_schedule.restype = C.c_int
+        L.rtb_fwd_set_tile.argtypes = [vp, C.c_int]
+        L.rtb_fwd_set_tile.restype = C.c_int
         L.rtb_fwd_autotune.argtypes = [vp, C.POINTER(_abi.RtbFwdTune)]
         L.rtb_fwd_autotune.restype = C.c_int
         L.rtb_fwd_use_graph.argtypes = [vp, C.c_int]
@@ -152,7 +154,7 @@ EXPORTED = [
     "rtb_get_debug_bins", "rtb_set_strict_ties", "rtb_fwd_prepare", "rtb_fwd_launch", "rtb_fwd_fetch",
     "rtb_set_stream", "rtb_fwd_launch_static", "rtb_set_newton_mode", "rtb_newton_step_batch",
     "rtb_calc_phiret_batch", "rtb_spd_inverse_batch", "rtb_retrieve_batch", "rtb_get_newton_stats",
-    "rtb_fwd_set_schedule", "rtb_fwd_autotune", "rtb_fwd_use_graph", "rtb_server_create", "rtb_server_destroy",
+    "rtb_fwd_set_schedule", "rtb_fwd_set_tile", "rtb_fwd_autotune", "rtb_fwd_use_graph", "rtb_server_create", "rtb_server_destroy",
     "rtb_server_submit", "rtb_server_step", "rtb_server_poll", "rtb_calc_gain_matrix", "rtb_calcnextxn",
     "rtb_cirsradg_wave", "rtb_kta_header", "rtb_load_ktables", "rtb_load_cia",
     "rtb_calc_serr", "rtb_cirsconv", "rtb_cirsconv_ex", "rtb_read_fwh", "rtb_read_fil",

@@ -274,6 +274,10 @@ class Context:
     def set_schedule(self, schedule, blocks_per_sm=0):
         self._check(self._L.rtb_fwd_set_schedule(self._h, schedule, blocks_per_sm))
 
+    def set_tile(self, warps=0):
+        """Warps per block of the resident batch's launches (2, 4, 8; 0 = 4)."""
+        self._check(self._L.rtb_fwd_set_tile(self._h, warps))
+
     def autotune(self) -> dict:
         t = _abi.RtbFwdTune()
         self._check(self._L.rtb_fwd_autotune(self._h, C.byref(t)))

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -13,9 +15,13 @@
 #include "rtb_common.h"
 
 namespace rtb {
-int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath);
-int fwd_blocks_per_sm(int smem);
-cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st);
+int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath, int warps);
+// warps per CTA a launch uses for a requested tile (tiles other than kWarps
+// exist for the usual instance only), and the blocks per SM it can hold
+int fwd_tile_warps(bool t2, bool ext, int warps);
+int fwd_blocks_per_sm(int smem, bool t2, bool ext, int warps, int ng);
+cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, int warps,
+                       cudaStream_t st);
 
 // growable device buffer / pinned host buffer (grow-only, freed by release)
 // growable device buffer
@@ -188,10 +194,17 @@ struct rtb_context {
     std::vector<char> h_conv;
     size_t dbg_perm_n = 0, dbg_split_n = 0;
     rtb_fwd_stats stats{};
+    int launched_grid = 0;                // blocks of the last forward launch
     // schedule of the resident batch (rtb_fwd_set_schedule / rtb_fwd_autotune)
     int sched = 0;                        // 0 static, 1 dynamic, 2 dynamic cost-ordered
     int occ = 0;                          // blocks per SM (0 = the occupancy maximum)
-    int bpsm_max = 1;
+    int tile = rtb::kWarps;               // requested warps per CTA (rtb_fwd_set_tile / rtb_fwd_autotune)
+    int tile_eff = rtb::kWarps;           // warps per CTA of the resident batch's launches
+    int bpsm_w[9] = {};                   // blocks per SM of the batch at 2, 4, 8 warps per CTA (0: not resident)
+    int bpsm_max = 1;                     // blocks per SM of the current tile
+    // rtb_fwd_autotune results by batch shape (layer bucket of 20, gas count): tile, schedule, occupancy
+    std::map<std::pair<int, int>, std::array<int, 3>> tuned;
+    std::pair<int, int> shape{0, 0};      // shape of the resident batch
     std::vector<int64_t> item_start_host;
     std::vector<float> spec_cost;
     int order_ready = 0;

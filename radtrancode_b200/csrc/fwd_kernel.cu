@@ -95,14 +95,67 @@ __device__ __noinline__ void heapsort_sort2g(int n, float* ra0, unsigned short* 
     }
 }
 
+// The same heapsort on 64-bit words (float bits of RA << 32 | IB), one thread:
+// the comparisons are the float comparisons of sort2g.f (RA(J) < RA(J+1),
+// RRA < RA(J)), so the words end in exactly the order of heapsort_sort2g.
+// RA and IB move as one word, and the sift-down loads the four grandchildren
+// while it compares the two children, so that no shared-memory load is on
+// the critical path of a level.
+__device__ __forceinline__ float wkey(unsigned long long w) { return __uint_as_float((unsigned)(w >> 32)); }
+__device__ __noinline__ void heapsort_words(int n, unsigned long long* W0) {
+    if (n < 2) return;
+    unsigned long long* W = W0 - 1;            // W[1..n]
+    int L = n / 2 + 1, IR = n;
+    for (;;) {
+        unsigned long long R;
+        if (L > 1) {
+            L = L - 1;
+            R = W[L];
+        } else {
+            R = W[IR];
+            W[IR] = W[1];
+            IR = IR - 1;
+            if (IR == 1) {
+                W[1] = R;
+                return;
+            }
+        }
+        const float kR = wkey(R);
+        int I = L, J = L + L;
+        if (J <= IR) {
+            unsigned long long c0 = W[J], c1 = W[J < IR ? J + 1 : J];
+            for (;;) {
+                // grandchildren of J and J + 1 (clamped into 1..IR; used only when in range)
+                const int G = J + J;
+                const unsigned long long g0 = W[G <= IR ? G : IR], g1 = W[G + 1 <= IR ? G + 1 : IR];
+                const unsigned long long g2 = W[G + 2 <= IR ? G + 2 : IR], g3 = W[G + 3 <= IR ? G + 3 : IR];
+                int Jc = J;
+                unsigned long long c = c0;
+                if (J < IR && wkey(c0) < wkey(c1)) {
+                    Jc = J + 1;
+                    c = c1;
+                }
+                if (!(kR < wkey(c))) break;
+                W[I] = c;
+                I = Jc;
+                J = Jc + Jc;
+                if (J > IR) break;
+                c0 = Jc == G / 2 ? g0 : g2;
+                c1 = Jc == G / 2 ? g1 : g3;
+            }
+        }
+        W[I] = R;
+    }
+}
+
 __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 
-// bytes of one element buffer: NG^2 64-bit words, or the gradient-column
-// scratch of sort_pass (U/V tables 4 NG float4, first/last partials
-// 2 x kMaxCols x 32 floats, inside-chunk bins kMaxCols x NG floats, 2 x 32
-// shorts), whichever is larger, for NG up to 22
+// bytes of one element buffer: NG^2 64-bit words, or the scratch of
+// grad_columns (U/V tables 4 NG float4, the closing-split partials 8 x NG
+// floats, the chunk-end partials 8 x 32 floats and 32 shorts), whichever is
+// larger, for NG up to 22
 constexpr int kNgDev = 22;
-constexpr int kGradScratch = 64 * kNgDev + 8 * kMaxCols * 32 + 4 * kMaxCols * kNgDev + 128;
+constexpr int kGradScratch = 64 * kNgDev + 32 * kNgDev + 32 * 32 + 2 * 32;
 constexpr int kElemBuf = ((8 * kN > kGradScratch ? 8 * kN : kGradScratch) + 15) & ~15;
 // per-warp scratch sub-offsets (bytes).  bufA holds the sorted (key, element)
 // words of a pass; bufB is the merge's second buffer, then the per-bin row and
@@ -152,7 +205,7 @@ __host__ __device__ inline PathOff path_off(int nlmax, int ng, int nsw) {
 struct Layout {
     int warp_bytes, path_bytes, off_gord, off_delg, off_region, total;
 };
-__host__ __device__ inline Layout make_layout(int ng, int nsw, int ncol, int nlmax, int npath) {
+__host__ __device__ inline Layout make_layout(int ng, int nsw, int ncol, int nlmax, int npath, int warps) {
     Layout Lo;
     Lo.warp_bytes = warp_off(ncol).total;
     Lo.path_bytes = path_off(nlmax, ng, nsw).total;
@@ -161,7 +214,7 @@ __host__ __device__ inline Layout make_layout(int ng, int nsw, int ncol, int nlm
     Lo.off_delg = o; o += 4 * kMaxNg;
     o = align16(o);
     Lo.off_region = o;
-    const int a = kWarps * Lo.warp_bytes, b = npath * Lo.path_bytes;
+    const int a = warps * Lo.warp_bytes, b = npath * Lo.path_bytes;
     o += a > b ? a : b;
     Lo.total = o;
     return Lo;
@@ -307,7 +360,7 @@ __device__ void get_kg_lane_nc(const BatchDev& B, int64_t slice, float w1, float
     __syncwarp();
 }
 
-template <bool t2>
+template <bool t2, int NGC>
 __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, const LayerDev& L, int lane,
                                             float& k, float& dk) {
     k = 0.0f;
@@ -317,7 +370,7 @@ __device__ __forceinline__ void get_kg_lane(const BatchDev& B, int64_t slice, co
     const float y10 = __ldg(raw + L.ioff[0]), y20 = __ldg(raw + L.ioff[1]);
     const float y30 = __ldg(raw + L.ioff[2]), y40 = __ldg(raw + L.ioff[3]);
     const bool klog = !((y10 <= 0.0f) || (y20 <= 0.0f) || (y30 <= 0.0f) || (y40 <= 0.0f));
-    if (lane >= B.ng) return;
+    if (lane >= (NGC ? NGC : B.ng)) return;
     const float* t = klog ? (B.ktab_log + slice) : raw;
     const float Y1 = __ldg(t + L.ioff[0] + lane), Y2 = __ldg(t + L.ioff[1] + lane);
     const float Y3 = __ldg(t + L.ioff[2] + lane), Y4 = __ldg(t + L.ioff[3] + lane);
@@ -698,7 +751,9 @@ __device__ __forceinline__ unsigned long long pack(float key, int i, int j) {
 // from one merge-path search.  Within a merge every word of the left run
 // has a smaller element part than every word of the right run, so comparing
 // whole words is the stable merge.
-__device__ int merge_rows(const WarpPtr& wp, int ng, int lane, int start) {
+template <int NGC>
+__device__ int merge_rows(const WarpPtr& wp, int ng_run, int lane, int start) {
+    const int ng = NGC ? NGC : ng_run;
     const int n = ng * ng;
     const int ch = (n + 31) >> 5;
     int cur = start;
@@ -762,10 +817,145 @@ __device__ __forceinline__ float elem_grad(const PassCtx& P, int gcol, int c, in
     return colP[c * kMaxNg + i];
 }
 
+// Gradient columns of one sorted pass.  They feed the Jacobian alone (never a
+// sort key), so they need not follow the reference's summation order.  Every
+// column is v_c(i, j) = U[i][c] + V[j][c] (T: dk1(i)[a1] + dk2(j) a2; earlier
+// gas: u(i); added gas: k2(j)).  Bin b of column c is the sum over its sorted
+// positions of w * v_c (split elements shared f : 1 - f), divided by the
+// bin's normalisation.  Each lane sums its chunk of positions; at a split it
+// writes the closing bin's partial to Eb[b] (one lane holds each split) and
+// restarts; its chunk-end partial goes to Lp with its bin in BL.  One lane
+// per bin then adds Eb[b] and the chunk-end partials of the lanes between
+// the bin's two boundaries that belong to it, in lane order (deterministic,
+// no atomics).  NCV: the columns computed per element (4, 5 or 8, at least
+// P.ncol).  scratch: the free element buffer (kGradScratch bytes).
+template <int NCV>
+__device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
+                                             const unsigned long long* A, void* scratch, const float* delg,
+                                             const float* colP, float* colN, int ng, int nloop, int c_last, int p0,
+                                             int p1, int ch, int lane) {
+    const int ncol = P.ncol;
+    float4* UV = (float4*)scratch;             // U rows [ng][2 float4], then V rows [ng][2 float4]
+    float* Eb = (float*)(UV + 4 * ng);         // [ng][8] partial of bin b up to its closing split
+    float4* Lp = (float4*)(Eb + 8 * ng);       // [32][2] chunk-end partial of each lane
+    short* BL = (short*)(Lp + 2 * 32);         // [32] its bin (-1: empty chunk)
+    if (lane < ng) {
+        const int x = lane;
+        float u[kMaxCols], v[kMaxCols];
+#pragma unroll
+        for (int c = 0; c < kMaxCols; ++c) {
+            u[c] = 0.0f;
+            v[c] = 0.0f;
+            if (c < ncol) {
+                const int gcol = S.col_gas[c];
+                if (gcol == S.ngas) {                  // temperature: dk1(i)[*a1] + dk2(j)*a2
+                    u[c] = P.first ? wp.dk1[x] * P.a1 : wp.dk1[x];
+                    v[c] = wp.dk2[x] * P.a2;
+                } else if (gcol == P.igas) {           // the gas being added: k2(j)
+                    v[c] = wp.k2[x];
+                } else if (gcol < P.igas) {            // an earlier gas
+                    if (!P.first) u[c] = colP[c * kMaxNg + x];
+                    else if (gcol == 0) u[c] = wp.k1[x];
+                }
+            }
+        }
+        UV[2 * x] = make_float4(u[0], u[1], u[2], u[3]);
+        UV[2 * x + 1] = make_float4(u[4], u[5], u[6], u[7]);
+        UV[2 * ng + 2 * x] = make_float4(v[0], v[1], v[2], v[3]);
+        UV[2 * ng + 2 * x + 1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+    __syncwarp();
+    int b = 0;
+    {
+        int lo = 0, hi = c_last;                // first boundary at or after p0
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (wp.splitpos[mid] < p0) lo = mid + 1; else hi = mid;
+        }
+        b = lo;
+    }
+    int nsp = b < c_last ? wp.splitpos[b] : nloop;
+    float acc[NCV];
+#pragma unroll
+    for (int c = 0; c < NCV; ++c) acc[c] = 0.0f;
+#pragma unroll 1
+    for (int p = p0; p < p1; ++p) {
+        const unsigned q = (unsigned)A[p] & 0xffffu;
+        const int i = q >> 5, j = q & 31;
+        const float w = __fmul_rn(delg[i], delg[j]);
+        float uu[8], vv[8];
+        {
+            const float4 u0 = UV[2 * i], v0 = UV[2 * ng + 2 * j];
+            uu[0] = u0.x; uu[1] = u0.y; uu[2] = u0.z; uu[3] = u0.w;
+            vv[0] = v0.x; vv[1] = v0.y; vv[2] = v0.z; vv[3] = v0.w;
+            if (NCV == 5) {
+                uu[4] = ((const float*)(UV + 2 * i + 1))[0];
+                vv[4] = ((const float*)(UV + 2 * ng + 2 * j + 1))[0];
+            } else if (NCV == 8) {
+                const float4 u1 = UV[2 * i + 1], v1 = UV[2 * ng + 2 * j + 1];
+                uu[4] = u1.x; uu[5] = u1.y; uu[6] = u1.z; uu[7] = u1.w;
+                vv[4] = v1.x; vv[5] = v1.y; vv[6] = v1.z; vv[7] = v1.w;
+            }
+        }
+        float val[NCV];
+#pragma unroll
+        for (int c = 0; c < NCV; ++c) val[c] = w * (uu[c] + vv[c]);
+        if (p == nsp) {                         // the split element closes bin b
+            const float f = (float)wp.splitfrac[b];
+#pragma unroll
+            for (int c = 0; c < NCV; ++c) {
+                Eb[b * 8 + c] = fmaf(f, val[c], acc[c]);
+                acc[c] = (1.0f - f) * val[c];
+            }
+            ++b;
+            nsp = b < c_last ? wp.splitpos[b] : nloop;
+        } else {
+#pragma unroll
+            for (int c = 0; c < NCV; ++c) acc[c] += val[c];
+        }
+    }
+    {
+        float a8[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) a8[c] = c < NCV ? acc[c < NCV ? c : 0] : 0.0f;
+        Lp[2 * lane] = make_float4(a8[0], a8[1], a8[2], a8[3]);
+        Lp[2 * lane + 1] = make_float4(a8[4], a8[5], a8[6], a8[7]);
+    }
+    BL[lane] = (short)(p0 < p1 ? b : -1);
+    __syncwarp();
+    if (lane < ng) {
+        const int bb = lane;
+        const float nf = wp.normf[bb];
+        float tot[NCV];
+#pragma unroll
+        for (int c = 0; c < NCV; ++c) tot[c] = 0.0f;
+        if (nf != 0.0f && bb <= c_last) {
+            const int Lfrom = bb == 0 ? 0 : wp.splitpos[bb - 1] / ch;
+            const int Lto = bb < c_last ? wp.splitpos[bb] / ch : (nloop - 1) / ch;
+#pragma unroll 1
+            for (int L = Lfrom; L <= Lto; ++L)
+                if (BL[L] == bb) {
+                    const float* src = (const float*)(Lp + 2 * L);
+#pragma unroll
+                    for (int c = 0; c < NCV; ++c) tot[c] += src[c];
+                }
+            if (bb < c_last) {
+#pragma unroll
+                for (int c = 0; c < NCV; ++c) tot[c] += Eb[bb * 8 + c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NCV; ++c)
+            if (c < ncol) colN[c * kMaxNg + bb] = nf != 0.0f ? tot[c] / nf : 0.0f;
+    }
+}
+
+template <int NGC>
 __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
                           const double* g_ord, const float* delg, int lane, Diag& dg, const float* colP,
                           float* colN, int16_t* dbg_perm, int16_t* dbg_split) {
-    const int ng = P.ng, nloop = P.nloop;
+    // NGC > 0: the run's NG as a compile-time constant (NGC = P.ng)
+    const int ng = NGC ? NGC : P.ng, nloop = NGC ? NGC * NGC : P.nloop;
     // ---- sort --------------------------------------------------------------
     // The words of row i, k1(i)[*a1] + k2(j)*a2 over j, are sorted when k2 is
     // monotone and a2 >= 0.  If every row's first word exceeds the last word
@@ -793,7 +983,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         if (disjoint) {
             A = W;
             dg.block_passes += (lane == 0);
-        } else if (merge_rows(wp, ng, lane, 1) != 0) {
+        } else if (merge_rows<NGC>(wp, ng, lane, 1) != 0) {
             A = W;
         }
     }
@@ -816,20 +1006,18 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     auto heapsort_pass = [&]() {
         __syncwarp();
         unsigned long long* Aw = (A == wp.bufA) ? wp.bufA : wp.bufB;
-        float* hk = (float*)((A == wp.bufA) ? wp.bufB : wp.bufA);
-        unsigned short* hi_ = (unsigned short*)(hk + nloop);
         for (int e = lane; e < nloop; e += 32) {
             const int i = e / ng, j = e - i * ng;
-            hk[e] = key_of(P, wp, i, j);
-            hi_[e] = (unsigned short)(e + 1);
+            Aw[e] = ((unsigned long long)__float_as_uint(key_of(P, wp, i, j)) << 32) | (unsigned)e;
         }
         __syncwarp();
-        if (lane == 0) heapsort_sort2g(nloop, hk, hi_);
+        if (lane == 0) heapsort_words(nloop, Aw);
         __syncwarp();
         for (int p = lane; p < nloop; p += 32) {
-            const int e = (int)hi_[p] - 1;
+            const unsigned long long w = Aw[p];
+            const int e = (int)(unsigned)w;
             const int i = e / ng, j = e - i * ng;
-            Aw[p] = pack(hk[p], i, j);
+            Aw[p] = pack(wkey(w), i, j);
         }
         __syncwarp();
         A = Aw;
@@ -1024,129 +1212,10 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         wp.normf[bb] = nf;
     }
     // ---- gradient columns ----------------------------------------------------
-    // They feed the Jacobian alone (never a sort key), so they need not follow
-    // the reference's summation order.  Every column is v_c(i, j) = U[i][c] +
-    // V[j][c] (T: dk1(i)[a1] + dk2(j) a2; earlier gas: u(i); added gas: k2(j)).
-    // Bin b of column c is the sum over its sorted positions of w * v_c (split
-    // elements shared f : 1 - f).  Each lane sums its chunk of positions per
-    // bin: the first and the last bin of the chunk as partials, bins wholly
-    // inside directly; one lane per bin then adds the partials of the lanes it
-    // spans, in lane order (deterministic, no atomics).
-    {
-        const int ncol = P.ncol;
-        float4* UV = (float4*)gd;                  // U rows [ng][2 float4], then V rows [ng][2 float4]
-        float* Fp = (float*)(UV + 4 * ng);         // [kMaxCols][32] first-bin partial
-        float* Lp = Fp + kMaxCols * 32;            // [kMaxCols][32] last-bin partial
-        float* Mid = Lp + kMaxCols * 32;           // [kMaxCols][ng] bins inside one chunk
-        short* B0 = (short*)(Mid + kMaxCols * ng); // [32] first bin of each lane's chunk
-        short* BL = B0 + 32;                       // [32] last bin of each lane's chunk
-        if (lane < ng) {
-            const int x = lane;
-            float u[kMaxCols], v[kMaxCols];
-#pragma unroll
-            for (int c = 0; c < kMaxCols; ++c) {
-                u[c] = 0.0f;
-                v[c] = 0.0f;
-                if (c < ncol) {
-                    const int gcol = S.col_gas[c];
-                    if (gcol == S.ngas) {                  // temperature: dk1(i)[*a1] + dk2(j)*a2
-                        u[c] = P.first ? wp.dk1[x] * P.a1 : wp.dk1[x];
-                        v[c] = wp.dk2[x] * P.a2;
-                    } else if (gcol == P.igas) {           // the gas being added: k2(j)
-                        v[c] = wp.k2[x];
-                    } else if (gcol < P.igas) {            // an earlier gas
-                        if (!P.first) u[c] = colP[c * kMaxNg + x];
-                        else if (gcol == 0) u[c] = wp.k1[x];
-                    }
-                }
-            }
-            UV[2 * x] = make_float4(u[0], u[1], u[2], u[3]);
-            UV[2 * x + 1] = make_float4(u[4], u[5], u[6], u[7]);
-            UV[2 * ng + 2 * x] = make_float4(v[0], v[1], v[2], v[3]);
-            UV[2 * ng + 2 * x + 1] = make_float4(v[4], v[5], v[6], v[7]);
-        }
-        __syncwarp();
-        int b = 0;
-        {
-            int lo = 0, hi = c_last;                // first boundary at or after p0
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (wp.splitpos[mid] < p0) lo = mid + 1; else hi = mid;
-            }
-            b = lo;
-        }
-        const int b0 = b;
-        int nsp = b < c_last ? wp.splitpos[b] : nloop;
-        float acc[kMaxCols], first[kMaxCols];
-        bool in_first = true;
-#pragma unroll
-        for (int c = 0; c < kMaxCols; ++c) {
-            acc[c] = 0.0f;
-            first[c] = 0.0f;
-        }
-#pragma unroll 1
-        for (int p = p0; p < p1; ++p) {
-            const unsigned q = (unsigned)A[p] & 0xffffu;
-            const int i = q >> 5, j = q & 31;
-            const float w = __fmul_rn(delg[i], delg[j]);
-            const float4 u0 = UV[2 * i], u1 = UV[2 * i + 1];
-            const float4 v0 = UV[2 * ng + 2 * j], v1 = UV[2 * ng + 2 * j + 1];
-            const float val[kMaxCols] = {w * (u0.x + v0.x), w * (u0.y + v0.y), w * (u0.z + v0.z),
-                                         w * (u0.w + v0.w), w * (u1.x + v1.x), w * (u1.y + v1.y),
-                                         w * (u1.z + v1.z), w * (u1.w + v1.w)};
-            if (p == nsp) {                         // the split element closes bin b
-                const float f = (float)wp.splitfrac[b];
-#pragma unroll
-                for (int c = 0; c < kMaxCols; ++c) {
-                    const float t = fmaf(f, val[c], acc[c]);
-                    if (in_first) first[c] = t;
-                    else if (c < ncol) Mid[c * ng + b] = t;
-                    acc[c] = (1.0f - f) * val[c];
-                }
-                in_first = false;
-                ++b;
-                nsp = b < c_last ? wp.splitpos[b] : nloop;
-            } else {
-#pragma unroll
-                for (int c = 0; c < kMaxCols; ++c) acc[c] += val[c];
-            }
-        }
-        if (p0 < p1) {
-#pragma unroll
-            for (int c = 0; c < kMaxCols; ++c)
-                if (c < ncol) {
-                    Fp[c * 32 + lane] = in_first ? acc[c] : first[c];
-                    Lp[c * 32 + lane] = in_first ? 0.0f : acc[c];
-                }
-        }
-        B0[lane] = (short)(p0 < p1 ? b0 : -1);
-        BL[lane] = (short)(p0 < p1 ? b : -1);
-        __syncwarp();
-        if (lane < ng) {
-            const int bb = lane;
-            const float nf = wp.normf[bb];
-            float tot[kMaxCols];
-#pragma unroll
-            for (int c = 0; c < kMaxCols; ++c) tot[c] = 0.0f;
-            if (nf != 0.0f && bb <= c_last) {
-                const int sp0 = bb == 0 ? 0 : wp.splitpos[bb - 1];
-                const int sp1 = bb < c_last ? wp.splitpos[bb] : nloop - 1;
-                const int L0 = sp0 / ch, L1 = sp1 / ch;
-#pragma unroll 1
-                for (int L = L0; L <= L1; ++L) {
-                    const int lb0 = B0[L], lbl = BL[L];
-                    const float* src = lb0 == bb ? Fp + L : (lbl == bb ? Lp + L : Mid + bb);
-                    const int stride = (lb0 == bb || lbl == bb) ? 32 : ng;
-#pragma unroll
-                    for (int c = 0; c < kMaxCols; ++c)
-                        if (c < ncol) tot[c] += src[c * stride];
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < kMaxCols; ++c)
-                if (c < ncol) colN[c * kMaxNg + bb] = nf != 0.0f ? tot[c] / nf : 0.0f;
-        }
-    }
+    // the columns' own arithmetic, specialised on how many there are
+    if (P.ncol <= 4) grad_columns<4>(S, P, wp, A, gd, delg, colP, colN, ng, nloop, c_last, p0, p1, ch, lane);
+    else if (P.ncol == 5) grad_columns<5>(S, P, wp, A, gd, delg, colP, colN, ng, nloop, c_last, p0, p1, ch, lane);
+    else grad_columns<8>(S, P, wp, A, gd, delg, colP, colN, ng, nloop, c_last, p0, p1, ch, lane);
     __syncwarp();
 }
 
@@ -1170,20 +1239,26 @@ __device__ __forceinline__ void planck_fp32(int ispace, float vwave, float T, fl
 // t2: the run's k-tables carry one temperature grid per pressure (NT < 0);
 // ext: some spectrum takes the para-H2 CIA (flagh2p = 1), an IMOD 18 path or
 // iform = 3.  Template arguments, so that the usual kernel carries no trace
-// of either
-template <bool t2, bool ext>
-__global__ void __launch_bounds__(kThreads, 5)
+// of either.  WARPS: warps per CTA, the layers of one (spectrum, wavenumber)
+// item worked on at once -- the tile shape the autotuner chooses; the
+// residency bound keeps 20 warps per SM at 96 registers.  NGC: NG as a
+// compile-time constant (the overlap's sizes, offsets and loop bounds fold),
+// or 0 for an NG read at run time
+template <bool t2, bool ext, int WARPS, int NGC>
+__global__ void __launch_bounds__(WARPS * 32, 20 / WARPS)
 fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) {
+    constexpr int kThreads = WARPS * 32;
+    constexpr int kWarps = WARPS;
     extern __shared__ __align__(16) char smem[];
     __shared__ SpecDev S_sh;
-    const Layout Lo = make_layout(B.ng, nsw_max, ncol_max, nlmax_max, npath_max);
+    const Layout Lo = make_layout(B.ng, nsw_max, ncol_max, nlmax_max, npath_max, WARPS);
     const WarpOff wo = warp_off(ncol_max);
     const PathOff po = path_off(nlmax_max, B.ng, nsw_max);
     double* g_ord = (double*)(smem + Lo.off_gord);
     float* delg = (float*)(smem + Lo.off_delg);
     char* region = smem + Lo.off_region;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int ng = B.ng;
+    const int ng = NGC ? NGC : B.ng;   // NGC > 0: the instance for NG = NGC (== B.ng)
     // per-CTA scratch slot in global memory (L2-resident): tau[l][g], dtau[l][s][g]
     float* tau_s = B.cell_scratch + (int64_t)blockIdx.x * B.cell_slot;
     float* dtau_s = tau_s + (int64_t)B.cell_Lmax * ng;
@@ -1280,7 +1355,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                     kv = lane < ng ? ncw[(g * kMaxNg + lane) * 2] : 0.0f;
                     dv = lane < ng ? ncw[(g * kMaxNg + lane) * 2 + 1] : 0.0f;
                 } else {
-                    get_kg_lane<t2>(B, slices[g], L, lane, kv, dv);
+                    get_kg_lane<t2, NGC>(B, slices[g], L, lane, kv, dv);
                 }
             };
             float* colP = colA;
@@ -1364,7 +1439,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                         PassCtx P;
                         P.ng = ng; P.nloop = ng * ng; P.ncol = ncol; P.first = first; P.igas = ig;
                         P.a1 = a1; P.a2 = a2;
-                        sort_pass(B, S, P, wp, g_ord, delg, lane, dg, colP, colN, dp, dsp);
+                        sort_pass<NGC>(B, S, P, wp, g_ord, delg, lane, dg, colP, colN, dp, dsp);
                         kgv = lane < ng ? wp.kg[lane] : 0.0f;
                     }
                     __syncwarp();
@@ -1544,33 +1619,50 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
 }
 
 // host-side helpers exported to host.cu
-int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath) {
-    return make_layout(ng, nsw, ncol, nlmax, npath).total;
+int fwd_smem_bytes(int ng, int nsw, int ncol, int nlmax, int npath, int warps) {
+    return make_layout(ng, nsw, ncol, nlmax, npath, warps).total;
 }
 
-int fwd_blocks_per_sm(int smem) {
-    int nb = 0;
-    // every instantiation: the smallest residency of them
-    void (*const kerns[4])(BatchDev, int, int, int, int) = {fwd_kernel<false, false>, fwd_kernel<true, false>,
-                                                            fwd_kernel<false, true>, fwd_kernel<true, true>};
-    nb = 1 << 30;
-    for (auto k : kerns) {
-        int n = 0;
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kThreads, smem) != cudaSuccess)
-            return 0;
-        nb = n < nb ? n : nb;
+namespace {
+using FwdKern = void (*)(BatchDev, int, int, int, int);
+// the instance of a launch: t2 and ext as the batch needs them; a tile other
+// than kWarps, and NG = 20 as a constant, exist for the usual instance only
+// (one temperature grid, no extended options)
+constexpr int kNgConst = 20;
+FwdKern fwd_instance(bool t2, bool ext, int warps, int ng) {
+    if (ext) return t2 ? fwd_kernel<true, true, kWarps, 0> : fwd_kernel<false, true, kWarps, 0>;
+    if (t2) return fwd_kernel<true, false, kWarps, 0>;
+    const bool c20 = ng == kNgConst;
+    switch (warps) {
+    case 2: return c20 ? fwd_kernel<false, false, 2, kNgConst> : fwd_kernel<false, false, 2, 0>;
+    case 8: return c20 ? fwd_kernel<false, false, 8, kNgConst> : fwd_kernel<false, false, 8, 0>;
+    default: return c20 ? fwd_kernel<false, false, kWarps, kNgConst> : fwd_kernel<false, false, kWarps, 0>;
     }
-    return nb;
+}
+}  // namespace
+
+int fwd_tile_warps(bool t2, bool ext, int warps) {
+    return (ext || t2 || (warps != 2 && warps != 8)) ? kWarps : warps;
 }
 
-cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, cudaStream_t st) {
-    const int smem = fwd_smem_bytes(B.ng, nsw, ncol, nlmax, npath);
-    auto kern = B.ext ? (B.t2 ? fwd_kernel<true, true> : fwd_kernel<false, true>)
-                       : (B.t2 ? fwd_kernel<true, false> : fwd_kernel<false, false>);
+int fwd_blocks_per_sm(int smem, bool t2, bool ext, int warps, int ng) {
+    const int w = fwd_tile_warps(t2, ext, warps);
+    const FwdKern k = fwd_instance(t2, ext, w, ng);
+    int n = 0;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, w * 32, smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+cudaError_t launch_fwd(const BatchDev& B, int nsw, int ncol, int nlmax, int npath, int grid, int warps,
+                       cudaStream_t st) {
+    const int w = fwd_tile_warps(B.t2, B.ext, warps);
+    const int smem = fwd_smem_bytes(B.ng, nsw, ncol, nlmax, npath, w);
+    const FwdKern kern = fwd_instance(B.t2, B.ext, w, B.ng);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, kThreads, smem, st>>>(B, nsw, ncol, nlmax, npath);
+    kern<<<grid, w * 32, smem, st>>>(B, nsw, ncol, nlmax, npath);
     return cudaGetLastError();
 }
 

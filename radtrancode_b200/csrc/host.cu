@@ -1008,13 +1008,20 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     Staging st;
     const int r0 = pack_batch(c, nspec, atms, st);
     if (r0) return r0;
-    const int smem = fwd_smem_bytes(c->ng, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max);
     int smem_max = 0;
     CUDA_TRY(c, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    const bool t2 = c->nt < 0, ext = st.any_para || st.any_ext;
+    int bpsm_all = 0;
+    for (int w : {2, 4, 8}) {
+        const int sm_w = fwd_smem_bytes(c->ng, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max, w);
+        c->bpsm_w[w] =
+            (sm_w <= smem_max && fwd_tile_warps(t2, ext, w) == w) ? fwd_blocks_per_sm(sm_w, t2, ext, w, c->ng) : 0;
+        bpsm_all = std::max(bpsm_all, c->bpsm_w[w]);
+    }
+    const int smem = fwd_smem_bytes(c->ng, st.nsw_max, st.ncol_max, st.nlmax_max, st.npath_max, kWarps);
     if (smem > smem_max)
         return fail(c, RTB_ERR_UNSUPPORTED, "spectrum needs %d B of shared memory (device %d)", smem, smem_max);
-    const int bpsm = fwd_blocks_per_sm(smem);
-    if (bpsm <= 0) return fail(c, RTB_ERR_CUDA, "forward kernel cannot be resident (smem %d B)", smem);
+    if (c->bpsm_w[kWarps] <= 0) return fail(c, RTB_ERR_CUDA, "forward kernel cannot be resident (smem %d B)", smem);
     // first device spectrum of each caller spectrum (path groups follow it)
     std::vector<int> first(nspec + 1, 0);
     for (int sp = 0; sp < nspec; ++sp) first[sp + 1] = first[sp] + st.nsub[sp];
@@ -1143,10 +1150,12 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
         B.dbg_perm = (int16_t*)c->d_dbg_perm.p;
         B.dbg_split = (int16_t*)c->d_dbg_split.p;
     }
-    int64_t grid = (int64_t)c->nsm * bpsm;
+    // the scratch holds a slot for every block of the largest grid any tile launches
+    int64_t grid = (int64_t)c->nsm * bpsm_all;
     if (grid > B.nitems) grid = B.nitems;
     c->grid = (int)grid;
-    c->bpsm_max = bpsm;
+    c->tile_eff = kWarps;
+    c->bpsm_max = c->bpsm_w[kWarps];
     // one scratch slot per CTA: tau[Lmax][ng] + dtau[Lmax][nsw][ng]
     B.cell_Lmax = st.Lmax;
     B.cell_slot = (int64_t)st.Lmax * c->ng * (1 + st.nsw_max);
@@ -1192,6 +1201,14 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     c->out_bytes = out_bytes;
     c->placed = place ? 1 : 0;
     c->prepared = 1;
+    // a batch of a shape tuned before starts with that tile and schedule
+    c->shape = {(st.Lmax + 19) / 20, st.ngas_max};
+    const auto tn = c->tuned.find(c->shape);
+    if (tn != c->tuned.end()) {
+        c->tile = tn->second[0];
+        c->sched = tn->second[1];
+        c->occ = tn->second[2];
+    }
     return apply_schedule(c);
 }
 
@@ -1206,6 +1223,9 @@ void drop_graph(rtb_context* c) {
 int apply_schedule(rtb_context* c) {
     drop_graph(c);
     BatchDev& B = c->B;
+    const int w = fwd_tile_warps(B.t2, B.ext, c->tile);
+    c->tile_eff = c->bpsm_w[w] > 0 ? w : kWarps;
+    c->bpsm_max = c->bpsm_w[c->tile_eff];
     const int b = c->occ > 0 ? std::min(c->occ, c->bpsm_max) : c->bpsm_max;
     int64_t grid = (int64_t)c->nsm * b;
     if (grid > B.nitems) grid = B.nitems;
@@ -1244,7 +1264,8 @@ int launch(rtb_context* c) {
             cudaGraph_t g = nullptr;
             CUDA_TRY(c, cudaStreamBeginCapture(strm, cudaStreamCaptureModeRelaxed));
             cudaError_t e = cudaMemsetAsync(c->d_diag.p, 0, 64, strm);
-            if (e == cudaSuccess) e = launch_fwd(c->B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, strm);
+            if (e == cudaSuccess)
+                e = launch_fwd(c->B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, c->tile_eff, strm);
             const cudaError_t e2 = cudaStreamEndCapture(strm, &g);
             if (e != cudaSuccess || e2 != cudaSuccess) {
                 if (g) cudaGraphDestroy(g);
@@ -1257,12 +1278,14 @@ int launch(rtb_context* c) {
         CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
         CUDA_TRY(c, cudaGraphLaunch(c->gexec, strm));
         CUDA_TRY(c, cudaEventRecord(c->ev1, strm));
+        c->launched_grid = c->grid;
         return RTB_OK;
     }
     CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, strm));
     CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
-    CUDA_TRY(c, launch_fwd(c->B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, strm));
+    CUDA_TRY(c, launch_fwd(c->B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, c->grid, c->tile_eff, strm));
     CUDA_TRY(c, cudaEventRecord(c->ev1, strm));
+    c->launched_grid = c->grid;
     return RTB_OK;
 }
 
@@ -1320,6 +1343,7 @@ int fetch(rtb_context* c, float* const* calcout, float* const* gradients, float*
     c->stats.irregular_passes = (long long)diag[4];
     c->stats.block_passes = (long long)diag[5];
     c->stats.ms_kernel = ms;
+    c->stats.grid = c->launched_grid;
     c->stats.h2d_bytes = (long long)c->in_bytes;
     c->stats.d2h_bytes = (long long)c->out_bytes;
     if (status & kStGord) return fail(c, RTB_ERR_GORD, "g-ordinate walk ran past NG (rankg.f:118-147)");
@@ -1397,16 +1421,18 @@ int launch_static(rtb_context* c) {
     const size_t nslot = (size_t)RTB_STATIC_SCRATCH_BYTES / slot_bytes;
     if (nslot < 1)
         return fail(c, RTB_ERR_LIMIT,
-                    "forward scratch slot of %zu B (%d layers x NG %d x %d columns) exceeds the static scratch of %u B",
-                    slot_bytes, c->Lmax, c->ng, 1 + c->nsw_max, (unsigned)RTB_STATIC_SCRATCH_BYTES);
+                    "forward scratch slot of %zu B (tau and dtau/dq of %d layers x NG %d, and the parked k of "
+                    "off-grid wavenumbers) exceeds the static scratch of %u B",
+                    slot_bytes, c->Lmax, c->ng, (unsigned)RTB_STATIC_SCRATCH_BYTES);
     const int grid = nslot < (size_t)c->grid ? (int)nslot : c->grid;
     BatchDev B = c->B;
     B.cell_scratch = base;
     const cudaStream_t strm = stream_of(c);
     CUDA_TRY(c, cudaMemsetAsync(c->d_diag.p, 0, 64, strm));
     CUDA_TRY(c, cudaEventRecord(c->ev0, strm));
-    CUDA_TRY(c, launch_fwd(B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, grid, strm));
+    CUDA_TRY(c, launch_fwd(B, c->nsw_max, c->ncol_max, c->nlmax_max, c->npath_max, grid, c->tile_eff, strm));
     CUDA_TRY(c, cudaEventRecord(c->ev1, strm));
+    c->launched_grid = grid;
     return RTB_OK;
 }
 
@@ -1693,6 +1719,16 @@ int rtb_fwd_set_schedule(rtb_context* c, int schedule, int blocks_per_sm) {
     return apply_schedule(c);
 }
 
+int rtb_fwd_set_tile(rtb_context* c, int warps) {
+    if (!c) return RTB_ERR_ARG;
+    if (!(warps == 0 || warps == 2 || warps == 4 || warps == 8))
+        return fail(c, RTB_ERR_ARG, "tile of %d warps per block (2, 4 or 8)", warps);
+    c->tile = warps ? warps : kWarps;
+    if (!c->prepared) return RTB_OK;
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    return apply_schedule(c);
+}
+
 int rtb_fwd_autotune(rtb_context* c, rtb_fwd_tune* out) {
     if (!c || !c->prepared) return fail(c, RTB_ERR_ARG, "no prepared batch (rtb_fwd_prepare)");
     CUDA_TRY(c, cudaSetDevice(c->device));
@@ -1700,30 +1736,38 @@ int rtb_fwd_autotune(rtb_context* c, rtb_fwd_tune* out) {
     const int keep_graph = c->use_graph;
     c->use_graph = 0;
     float best = 3.4e38f;
-    int best_s = 0, best_b = c->bpsm_max, n = 0;
-    for (int sch = 0; sch <= 2; ++sch)
-        for (int b = c->bpsm_max; b >= 1 && b >= c->bpsm_max - 2; --b) {
-            c->sched = sch;
-            c->occ = b;
-            int r = apply_schedule(c);
-            if (r) return r;
-            float ms = 0.0f;
-            for (int rep = 0; rep < 2; ++rep) {   // the second launch is timed
-                r = launch(c);
+    int best_w = kWarps, best_s = 0, best_b = c->bpsm_w[kWarps], n = 0;
+    for (int w : {4, 8, 2}) {
+        if (fwd_tile_warps(c->B.t2, c->B.ext, w) != w || c->bpsm_w[w] <= 0) continue;
+        const int bmax = c->bpsm_w[w];
+        for (int sch = 0; sch <= 2; ++sch)
+            for (int b = bmax; b >= 1 && b >= bmax - 2; --b) {
+                c->tile = w;
+                c->sched = sch;
+                c->occ = b;
+                int r = apply_schedule(c);
                 if (r) return r;
-                CUDA_TRY(c, cudaStreamSynchronize(strm));
-                CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+                float ms = 0.0f;
+                for (int rep = 0; rep < 2; ++rep) {   // the second launch is timed
+                    r = launch(c);
+                    if (r) return r;
+                    CUDA_TRY(c, cudaStreamSynchronize(strm));
+                    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+                }
+                ++n;
+                if (ms < best) {
+                    best = ms;
+                    best_w = w;
+                    best_s = sch;
+                    best_b = b;
+                }
             }
-            ++n;
-            if (ms < best) {
-                best = ms;
-                best_s = sch;
-                best_b = b;
-            }
-        }
+    }
+    c->tile = best_w;
     c->sched = best_s;
     c->occ = best_b;
     c->use_graph = keep_graph;
+    c->tuned[c->shape] = {best_w, best_s, best_b};
     const int r = apply_schedule(c);
     if (r) return r;
     if (out) {
@@ -1731,6 +1775,7 @@ int rtb_fwd_autotune(rtb_context* c, rtb_fwd_tune* out) {
         out->blocks_per_sm = best_b;
         out->ms = best;
         out->candidates = n;
+        out->warps = best_w;
     }
     return RTB_OK;
 }

@@ -10,6 +10,7 @@ constexpr int kNewtonMaxNx = 128;   // state size handled by one block (NX=124 a
 
 // status bits of one retrieval's step
 constexpr unsigned kNtNonPd = 1u;   // a Cholesky pivot was <= 0 and was replaced by 1 (dcholdc.f:69-84)
+constexpr unsigned kNtTimeout = 2u; // a wait on the tensor-core pipeline gave up: x_out was not written
 
 // one retrieval's Newton step: every pointer is device memory
 struct NewtonDev {
@@ -22,7 +23,6 @@ struct NewtonDev {
     const float* xa;      // [nx] a priori
     const float* xn;      // [nx] current state
     float* x_out;         // [nx] out: xa + C^-1 K^T Se^-1 (y - yn + K (xn - xa))
-    double* work;         // [ny] scratch
 };
 
 // chi^2 and cost of one retrieval (calc_phiret.f), every pointer device memory

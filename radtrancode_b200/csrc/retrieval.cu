@@ -454,11 +454,11 @@ struct Slot {
 
 size_t slot_core_bytes(int nx, int ny) {
     const size_t f = (size_t)(2 * (int64_t)nx * ny + 3 * al4(ny)) * 4;
-    const size_t d = (size_t)(2 * al4(ny) + 2 * (int64_t)nx * nx) * 8;
+    const size_t d = (size_t)(al4(ny) + 2 * (int64_t)nx * nx) * 8;
     return (((f + 7) & ~(size_t)7) + d + 255) & ~(size_t)255;
 }
 
-// K and the spectra of two states, y, Se^-1, the Newton work, Sa^-1 and Sa;
+// K and the spectra of two states, y, Se^-1, Sa^-1 and Sa;
 // with channels or several paths, after them the forward model's own
 // outputs for the state being evaluated, [np][nraw] then [np][nx][nraw],
 // and with both, the convolved Jacobian [np][nx][ny / np] before its rows
@@ -586,8 +586,7 @@ struct Engine {
         return (double*)((char*)arena.p + s.off + ((f + 7) & ~(size_t)7));
     }
     double* Sei(const Slot& s) const { return Db(s); }
-    double* Work(const Slot& s) const { return Db(s) + al4(s.ny); }
-    double* Sai(const Slot& s) const { return Db(s) + 2 * al4(s.ny); }
+    double* Sai(const Slot& s) const { return Db(s) + al4(s.ny); }
     double* Sa(const Slot& s) const { return Sai(s) + (int64_t)s.nx * s.nx; }
     float* Raw(const Slot& s) const { return F() + (s.off + slot_core_bytes(s.nx, s.ny)) / 4; }
     float* X(const Slot& s, int part) const { return (float*)xarea.p + (int64_t)s.xrow * kXRow + part * kNewtonMaxNx; }
@@ -727,7 +726,6 @@ struct Engine {
             d.xa = X(*s, 0);
             d.xn = X(*s, 1);
             d.x_out = X(*s, 3);
-            d.work = Work(*s);
             desc.push_back(d);
         }
         CUDA_TRY(c, h2d(nt_desc, desc, st));
@@ -739,6 +737,8 @@ struct Engine {
         CUDA_TRY(c, cudaMemcpyAsync(xs.data(), xarea.p, xs.size() * 4, cudaMemcpyDeviceToHost, st));
         CUDA_TRY(c, cudaMemcpyAsync(sts.data(), small.p, 4 * v.size(), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(c, cudaStreamSynchronize(st));
+        for (size_t k = 0; k < v.size(); ++k)
+            if (sts[k] & kNtTimeout) return fail(c, RTB_ERR_CUDA, "Newton step: the tensor-core pipeline timed out");
         for (size_t k = 0; k < v.size(); ++k) {
             Slot& s = *v[k];
             const float* xo = xs.data() + (size_t)s.xrow * kXRow + 3 * kNewtonMaxNx;
@@ -969,7 +969,7 @@ int rtb_newton_step_batch(rtb_context* c, int nret, int nx, int ny, const float*
     // f32: kk | y | yn | xa | xn | x_out ; f64: sei | sai | work
     const int64_t o_y = (int64_t)nret * nx * ny, o_yn = o_y + nret * nya, o_xa = o_yn + nret * nya;
     const int64_t o_xn = o_xa + nret * nxa, o_xo = o_xn + nret * nxa, n32 = o_xo + nret * nxa;
-    const int64_t o_sai = nret * nya, o_w = o_sai + (int64_t)nret * nx * nx, n64 = o_w + nret * nya;
+    const int64_t o_sai = nret * nya, n64 = o_sai + (int64_t)nret * nx * nx;
     CUDA_TRY(c, c->d_nt32.ensure((size_t)n32 * 4));
     CUDA_TRY(c, c->d_nt64.ensure((size_t)n64 * 8));
     CUDA_TRY(c, c->d_ntsmall.ensure((size_t)12 * nret + 64));
@@ -995,7 +995,6 @@ int rtb_newton_step_batch(rtb_context* c, int nret, int nx, int ny, const float*
         d.x_out = F + o_xo + r * nxa;
         d.sei = D + r * nya;
         d.sai = D + o_sai + (int64_t)r * nx * nx;
-        d.work = D + o_w + r * nya;
     }
     CUDA_TRY(c, h2d(c->d_ntdesc, desc, st));
     unsigned* status = (unsigned*)c->d_ntsmall.p;
@@ -1009,6 +1008,8 @@ int rtb_newton_step_batch(rtb_context* c, int nret, int nx, int ny, const float*
     CUDA_TRY(c, cudaMemcpyAsync(sts.data(), status, 4 * (size_t)nret, cudaMemcpyDeviceToHost, st));
     if (resid) CUDA_TRY(c, cudaMemcpyAsync(resid, dres, 8 * (size_t)nret, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(c, cudaStreamSynchronize(st));
+    for (int r = 0; r < nret; ++r)
+        if (sts[r] & kNtTimeout) return fail(c, RTB_ERR_CUDA, "Newton step: the tensor-core pipeline timed out");
     if (nonpd)
         for (int r = 0; r < nret; ++r) nonpd[r] = (sts[r] & kNtNonPd) ? 1 : 0;
     float ms = 0.0f;

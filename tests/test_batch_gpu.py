@@ -1,7 +1,9 @@
 """GPU tests of the batched forward model on uneven spectra (the
-persistent-launch form): every schedule, the autotuner and the CUDA-graph
-replay give the same bits as one rtb_cirsrtfg_wave call per spectrum, and
-the batch agrees with the FP64 oracle within the parity tolerances."""
+persistent-launch form): every tile (warps per block), schedule and
+occupancy, the autotuner and the CUDA-graph replay give the same bits as one
+rtb_cirsrtfg_wave call per spectrum, a re-prepared batch of the tuned shape
+starts with the tuned configuration, and the batch agrees with the FP64
+oracle within the parity tolerances."""
 import os
 
 import numpy as np
@@ -32,22 +34,33 @@ def test_schedules_graph_and_autotune_are_bit_identical(ctx, uneven):
     singles = [ctx.cirsrtfg_wave(j) for j in jobs]
     ctx.prepare(jobs)
     try:
-        for sched in (0, 1, 2):
-            for occ in (0, 1):
-                ctx.set_schedule(sched, occ)
-                ctx.launch()
-                _same(ctx.fetch(), singles)
+        for tile in (4, 2, 8):
+            ctx.set_tile(tile)
+            for sched in (0, 1, 2):
+                for occ in (0, 1):
+                    ctx.set_schedule(sched, occ)
+                    ctx.launch()
+                    _same(ctx.fetch(), singles)
+        ctx.set_tile(0)
         ctx.use_graph(True)
         for _ in range(3):                       # capture, then two replays
             ctx.launch()
             _same(ctx.fetch(), singles)
         tune = ctx.autotune()
-        assert tune["candidates"] >= 3 and tune["ms"] > 0
+        assert tune["candidates"] >= 9 and tune["ms"] > 0 and tune["warps"] in (2, 4, 8)
         ctx.launch()
         _same(ctx.fetch(), singles)
         assert ctx.stats()["cells"] == sum(j.nlayer * j.nwave for j in jobs)
+        # a batch of the same shape starts with the tuned tile: the launch's grid is the tuned one
+        grid_tuned = ctx.stats()["grid"]
+        ctx.use_graph(False)
+        ctx.prepare(jobs[::-1])
+        ctx.launch()
+        _same(ctx.fetch()[::-1], singles)
+        assert ctx.stats()["grid"] == grid_tuned
     finally:
         ctx.use_graph(False)
+        ctx.set_tile(0)
         ctx.set_schedule(0, 0)
 
 

@@ -3,8 +3,10 @@ from the library's fixed per-device array instead of the context.
 
 Checked against the ordinary entry point (rtb_cirsrtfg_wave) on the same
 batch, on two calls in a row, within the parity tolerances of
-tests/helpers.py.  The 200-layer case has more wavenumbers than the static
-array holds block slots, so it also runs the reduced grid."""
+tests/helpers.py.  The 200-layer case has more blocks than the static array
+holds slots: the test checks that it runs on fewer blocks than the ordinary
+launch (the reduced grid), under the static schedule and the two dynamic
+ones (which pull items from a counter and, longest first, from an order)."""
 import numpy as np
 import pytest
 
@@ -14,20 +16,30 @@ from tests.helpers import JAC_TOL, RAD_TOL, jac_err, rad_err
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("nwave,nlayer", [(64, 120), (1000, 200)])
-def test_static_scratch_matches_rtb_cirsrtfg_wave(ctx, nwave, nlayer):
+@pytest.mark.parametrize("nwave,nlayer,reduced", [(64, 120, False), (1000, 200, True)])
+def test_static_scratch_matches_rtb_cirsrtfg_wave(ctx, nwave, nlayer, reduced):
     kt, cia, job = synth.config2(nwave=nwave, nlayer=nlayer, nbin=nwave)
     ctx.set_ktables(kt)
     ctx.set_cia(cia)
     c_ref, g_ref, gt_ref = ctx.cirsrtfg_wave(job)
     ctx.prepare([job])
-    for _ in range(2):
-        ctx.launch_static()
-        (c, g, gt), = ctx.fetch()
-        assert rad_err(c, c_ref) <= RAD_TOL
-        assert jac_err(g, g_ref, job.nv) <= JAC_TOL
-        assert np.max(np.abs(gt - gt_ref)) <= RAD_TOL * np.max(np.abs(gt_ref))
-        assert ctx.stats()["cells"] == nwave * nlayer
+    ctx.launch()
+    ctx.fetch()
+    full_grid = ctx.stats()["grid"]
+    try:
+        for sched in ((0, 1, 2) if reduced else (0,)):
+            ctx.set_schedule(sched, 0)
+            for _ in range(2):
+                ctx.launch_static()
+                (c, g, gt), = ctx.fetch()
+                st = ctx.stats()
+                assert rad_err(c, c_ref) <= RAD_TOL
+                assert jac_err(g, g_ref, job.nv) <= JAC_TOL
+                assert np.max(np.abs(gt - gt_ref)) <= RAD_TOL * np.max(np.abs(gt_ref))
+                assert st["cells"] == nwave * nlayer
+                assert (0 < st["grid"] < full_grid) if reduced else (st["grid"] == full_grid)
+    finally:
+        ctx.set_schedule(0, 0)
 
 
 def test_static_scratch_needs_a_prepared_batch():

@@ -10,6 +10,9 @@ from radtrancode_b200 import synth
 from tests.helpers import jac_err, rad_err
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+# the reference's data directory (raddata/): the checkout named by RADTRAN_REFERENCE,
+# else /root/reference; the tests that read it skip where it is absent (on a GPU host)
+RADDATA = os.path.join(os.environ.get("RADTRAN_REFERENCE", "/root/reference"), "raddata")
 
 
 def _golden_input_digest(kt, cia, job):
@@ -244,7 +247,7 @@ def test_unsupported_options_are_reported(oracle):
 
 
 # ---------------------------------------------------------------- real CIA data
-ISOTEST = "/root/reference/raddata/isotest.tab"
+ISOTEST = os.path.join(RADDATA, "isotest.tab")
 
 
 def read_cia_tab(path):
@@ -370,7 +373,7 @@ def test_imod18_needs_the_e3_table(oracle):
         oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
 
 
-E3TAB = "/root/reference/raddata/e3tab.dat"
+E3TAB = os.path.join(RADDATA, "e3tab.dat")
 
 
 @pytest.mark.skipif(not os.path.exists(E3TAB), reason="reference data not mounted")
@@ -481,7 +484,7 @@ def test_stellar_flux_ratio_and_transmission(oracle):
     assert np.max(np.abs(t4 * sph / xs / t0 - 1.0)) < 1e-5
 
 
-STELLAR = "/root/reference/raddata/upsAnd.dat"
+STELLAR = os.path.join(RADDATA, "upsAnd.dat")
 
 
 @pytest.mark.skipif(not os.path.exists(STELLAR), reason="reference data not mounted")

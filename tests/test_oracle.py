@@ -10,8 +10,8 @@ from radtrancode_b200 import synth
 from tests.helpers import jac_err, rad_err
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-# the reference's data directory (raddata/): the checkout named by RADTRAN_REFERENCE,
-# else /root/reference; the tests that read it skip where it is absent (on a GPU host)
+# the reference's data directory (raddata/) of the checkout named by RADTRAN_REFERENCE,
+# else of the default checkout; the tests that read it skip where it is absent
 RADDATA = os.path.join(os.environ.get("RADTRAN_REFERENCE", "/root/reference"), "raddata")
 
 

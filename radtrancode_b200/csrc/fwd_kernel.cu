@@ -827,13 +827,15 @@ __device__ __forceinline__ float elem_grad(const PassCtx& P, int gcol, int c, in
 // restarts; its chunk-end partial goes to Lp with its bin in BL.  One lane
 // per bin then adds Eb[b] and the chunk-end partials of the lanes between
 // the bin's two boundaries that belong to it, in lane order (deterministic,
-// no atomics).  NCV: the columns computed per element (4, 5 or 8, at least
-// P.ncol).  scratch: the free element buffer (kGradScratch bytes).
+// no atomics).  cmap[0..nz): the columns computed (slot k holds column
+// cmap[k]); every other column is zero in this pass.  NCV: the slots computed
+// per element (4, 5 or 8, at least nz).  scratch: the free element buffer
+// (kGradScratch bytes).
 template <int NCV>
 __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
                                              const unsigned long long* A, void* scratch, const float* delg,
-                                             const float* colP, float* colN, int ng, int nloop, int c_last, int p0,
-                                             int p1, int ch, int lane) {
+                                             const float* colP, float* colN, const int (&cmap)[kMaxCols], int nz,
+                                             int ng, int nloop, int c_last, int p0, int p1, int ch, int lane) {
     const int ncol = P.ncol;
     float4* UV = (float4*)scratch;             // U rows [ng][2 float4], then V rows [ng][2 float4]
     float* Eb = (float*)(UV + 4 * ng);         // [ng][8] partial of bin b up to its closing split
@@ -843,19 +845,20 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
         const int x = lane;
         float u[kMaxCols], v[kMaxCols];
 #pragma unroll
-        for (int c = 0; c < kMaxCols; ++c) {
-            u[c] = 0.0f;
-            v[c] = 0.0f;
-            if (c < ncol) {
+        for (int k = 0; k < kMaxCols; ++k) {
+            u[k] = 0.0f;
+            v[k] = 0.0f;
+            if (k < nz) {
+                const int c = cmap[k];
                 const int gcol = S.col_gas[c];
                 if (gcol == S.ngas) {                  // temperature: dk1(i)[*a1] + dk2(j)*a2
-                    u[c] = P.first ? wp.dk1[x] * P.a1 : wp.dk1[x];
-                    v[c] = wp.dk2[x] * P.a2;
+                    u[k] = P.first ? wp.dk1[x] * P.a1 : wp.dk1[x];
+                    v[k] = wp.dk2[x] * P.a2;
                 } else if (gcol == P.igas) {           // the gas being added: k2(j)
-                    v[c] = wp.k2[x];
+                    v[k] = wp.k2[x];
                 } else if (gcol < P.igas) {            // an earlier gas
-                    if (!P.first) u[c] = colP[c * kMaxNg + x];
-                    else if (gcol == 0) u[c] = wp.k1[x];
+                    if (!P.first) u[k] = colP[c * kMaxNg + x];
+                    else if (gcol == 0) u[k] = wp.k1[x];
                 }
             }
         }
@@ -945,8 +948,11 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
             }
         }
 #pragma unroll
-        for (int c = 0; c < NCV; ++c)
-            if (c < ncol) colN[c * kMaxNg + bb] = nf != 0.0f ? tot[c] / nf : 0.0f;
+        for (int c = 0; c < kMaxCols; ++c)
+            if (c < ncol) colN[c * kMaxNg + bb] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < NCV; ++k)
+            if (k < nz) colN[cmap[k] * kMaxNg + bb] = nf != 0.0f ? tot[k] / nf : 0.0f;
     }
 }
 
@@ -1212,10 +1218,21 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         wp.normf[bb] = nf;
     }
     // ---- gradient columns ----------------------------------------------------
-    // the columns' own arithmetic, specialised on how many there are
-    if (P.ncol <= 4) grad_columns<4>(S, P, wp, A, gd, delg, colP, colN, ng, nloop, c_last, p0, p1, ch, lane);
-    else if (P.ncol == 5) grad_columns<5>(S, P, wp, A, gd, delg, colP, colN, ng, nloop, c_last, p0, p1, ch, lane);
-    else grad_columns<8>(S, P, wp, A, gd, delg, colP, colN, ng, nloop, c_last, p0, p1, ch, lane);
+    // A column of a gas not yet added (gas index above igas) is zero in this
+    // pass; the others are computed, their arithmetic specialised on how many
+    // there are
+    int cmap[kMaxCols], nz = 0;
+#pragma unroll
+    for (int c = 0; c < kMaxCols; ++c) {
+        cmap[c] = 0;
+        if (c < P.ncol) {
+            const int g = S.col_gas[c];
+            if (g == S.ngas || g <= P.igas) cmap[nz++] = c;
+        }
+    }
+    if (nz <= 4) grad_columns<4>(S, P, wp, A, gd, delg, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
+    else if (nz == 5) grad_columns<5>(S, P, wp, A, gd, delg, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
+    else grad_columns<8>(S, P, wp, A, gd, delg, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
     __syncwarp();
 }
 

@@ -37,7 +37,7 @@ def test_static_scratch_matches_rtb_cirsrtfg_wave(ctx, nwave, nlayer, reduced):
                 assert jac_err(g, g_ref, job.nv) <= JAC_TOL
                 assert np.max(np.abs(gt - gt_ref)) <= RAD_TOL * np.max(np.abs(gt_ref))
                 assert st["cells"] == nwave * nlayer
-                assert (0 < st["grid"] < full_grid) if reduced else (st["grid"] == full_grid)
+                assert ((0 < st["grid"] < full_grid) if reduced else (st["grid"] == full_grid)), (st["grid"], full_grid)
     finally:
         ctx.set_schedule(0, 0)
 

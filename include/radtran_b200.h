@@ -420,7 +420,8 @@ int rtb_fwd_set_tile(rtb_context* ctx, int warps);
  * buckets of 20 layers, and its largest gas count): a later rtb_fwd_prepare
  * of a batch of the same shape starts with it (tune on a representative
  * batch, run the large one).  rtb_fwd_set_schedule / rtb_fwd_set_tile after
- * the prepare override it. */
+ * the prepare override it; a batch of a shape not tuned in the context runs
+ * the values last set with them (or the defaults). */
 typedef struct rtb_fwd_tune {
     int schedule;
     int blocks_per_sm;

@@ -1201,13 +1201,18 @@ int prepare_ex(rtb_context* c, int nspec, const rtb_atm* atms, const OutPlace* p
     c->out_bytes = out_bytes;
     c->placed = place ? 1 : 0;
     c->prepared = 1;
-    // a batch of a shape tuned before starts with that tile and schedule
+    // a batch of a shape tuned before starts with that tile and schedule;
+    // any other batch with the caller's own choices (or the defaults)
     c->shape = {(st.Lmax + 19) / 20, st.ngas_max};
     const auto tn = c->tuned.find(c->shape);
     if (tn != c->tuned.end()) {
         c->tile = tn->second[0];
         c->sched = tn->second[1];
         c->occ = tn->second[2];
+    } else {
+        c->tile = c->tile_user;
+        c->sched = c->sched_user;
+        c->occ = c->occ_user;
     }
     return apply_schedule(c);
 }
@@ -1712,8 +1717,8 @@ int rtb_fwd_set_schedule(rtb_context* c, int schedule, int blocks_per_sm) {
     if (!c) return RTB_ERR_ARG;
     if (schedule < 0 || schedule > 2 || blocks_per_sm < 0)
         return fail(c, RTB_ERR_ARG, "schedule %d, blocks_per_sm %d", schedule, blocks_per_sm);
-    c->sched = schedule;
-    c->occ = blocks_per_sm;
+    c->sched = c->sched_user = schedule;
+    c->occ = c->occ_user = blocks_per_sm;
     if (!c->prepared) return RTB_OK;
     CUDA_TRY(c, cudaSetDevice(c->device));
     return apply_schedule(c);
@@ -1723,7 +1728,7 @@ int rtb_fwd_set_tile(rtb_context* c, int warps) {
     if (!c) return RTB_ERR_ARG;
     if (!(warps == 0 || warps == 2 || warps == 4 || warps == 8))
         return fail(c, RTB_ERR_ARG, "tile of %d warps per block (2, 4 or 8)", warps);
-    c->tile = warps ? warps : kWarps;
+    c->tile = c->tile_user = warps ? warps : kWarps;
     if (!c->prepared) return RTB_OK;
     CUDA_TRY(c, cudaSetDevice(c->device));
     return apply_schedule(c);

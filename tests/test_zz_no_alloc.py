@@ -23,6 +23,7 @@ def test_static_scratch_matches_rtb_cirsrtfg_wave(ctx, nwave, nlayer, reduced):
     ctx.set_cia(cia)
     c_ref, g_ref, gt_ref = ctx.cirsrtfg_wave(job)
     ctx.prepare([job])
+    ctx.set_tile(4)          # 740 blocks of the ordinary launch against the static array's 349 slots of 96 KB
     ctx.launch()
     ctx.fetch()
     full_grid = ctx.stats()["grid"]
@@ -39,6 +40,7 @@ def test_static_scratch_matches_rtb_cirsrtfg_wave(ctx, nwave, nlayer, reduced):
                 assert st["cells"] == nwave * nlayer
                 assert ((0 < st["grid"] < full_grid) if reduced else (st["grid"] == full_grid)), (st["grid"], full_grid)
     finally:
+        ctx.set_tile(0)
         ctx.set_schedule(0, 0)
 
 

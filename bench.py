@@ -200,6 +200,47 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+class BusySampler:
+    """Fraction of time the GPU was running a kernel, from NVML's utilization
+    counter read every 20 ms in a thread (reads only)."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.samples = []
+        self.thread = None
+
+    def start(self):
+        import threading
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+        except Exception:
+            return
+        self.stop_ev = threading.Event()
+
+        def loop():
+            while not self.stop_ev.is_set():
+                try:
+                    self.samples.append(pynvml.nvmlDeviceGetUtilizationRates(h).gpu)
+                except Exception:
+                    pass
+                self.stop_ev.wait(0.02)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if self.thread is None:
+            return None
+        self.stop_ev.set()
+        self.thread.join(timeout=2)
+        if not self.samples:
+            return None
+        return {"mean_pct": float(np.mean(self.samples)), "samples": len(self.samples),
+                "source": "NVML utilization.gpu every 20 ms"}
+
+
 # ---------------------------------------------------------------- accuracy against the FP64 oracle
 def _jac_errors(g, g64, nv):
     G = np.asarray(g, np.float64).reshape(nv, -1)
@@ -474,6 +515,8 @@ def serve_point(ctx, kt, rate, window, budget, seed):
     lat, its, rounds, peak, queued_rounds, step_s = [], [], 0, 0, 0, 0.0
     results = {}
     i, pending = 0, {}
+    busy = BusySampler(ctx.device)
+    busy.start()
     t0 = time.perf_counter()
     with cirsradg.Server(ctx, budget, kiter=15, phlimit=0.1, dchisq_stop=0.1) as srv:
         while i < n or pending:
@@ -499,6 +542,7 @@ def serve_point(ctx, kt, rate, window, budget, seed):
                     its.append(r["iterations"])
                     results[k] = r
     t_total = time.perf_counter() - t0
+    gpu_busy = busy.stop()
     same = 0
     for k in sorted(results)[:SERVE_CHECK]:
         alone = ctx.retrieve_batch([cases[k]], kiter=15, phlimit=0.1, dchisq_stop=0.1)[0]
@@ -510,7 +554,7 @@ def serve_point(ctx, kt, rate, window, budget, seed):
         "peak_in_flight": peak, "rounds_with_requests_waiting_for_memory": queued_rounds,
         "p50_ms": float(np.percentile(lat, 50)), "p95_ms": float(np.percentile(lat, 95)),
         "p99_ms": float(np.percentile(lat, 99)), "iterations_mean": float(np.mean(its)),
-        "server_step_s": step_s,
+        "server_step_s": step_s, "gpu_busy": gpu_busy,
         "alone_vs_mix": {"checked": min(SERVE_CHECK, len(results)), "bit_identical": same},
     }
 

@@ -92,6 +92,7 @@ class Context:
         if st != 0:
             raise RtbError(st, f"rtb_create(device={device}) failed: no usable CUDA device")
         self._h = h
+        self.device = device
         self.tables = None
 
     def close(self):

@@ -745,57 +745,99 @@ __device__ __forceinline__ unsigned long long pack(float key, int i, int j) {
     return ((unsigned long long)fkey(key) << 32) | (unsigned)((i << 5) | j);
 }
 
+__device__ __forceinline__ unsigned hi32(unsigned long long w) { return (unsigned)(w >> 32); }
+
+// Merge of A = ki[a0, a1) and B = ki[b0, b1) into ko[s, e) (e - s elements):
+// the front half smallest-first from the start, the back half largest-first
+// from the end, as two independent chains.  Only the key halves are
+// compared: every element of A precedes every element of B, so on equal keys
+// A's word comes first (the stable order).  Branch-free steps; an exhausted
+// side reads as ~0 (front) or 0 (back), keys no word can hold (NaN keys never
+// reach the merge).
+__device__ __forceinline__ void merge_seg(const unsigned long long* ki, unsigned long long* ko, int s, int e,
+                                          int a0, int a1, int b0, int b1) {
+    const int len = e - s, nb = len >> 1;
+    int fa = a0, fb = b0, ba = a1, bb = b1;
+    unsigned long long xa = fa < a1 ? ki[fa] : ~0ull, yb = fb < b1 ? ki[fb] : ~0ull;
+    unsigned long long xA = ba > a0 ? ki[ba - 1] : 0ull, yB = bb > b0 ? ki[bb - 1] : 0ull;
+#pragma unroll 1
+    for (int t = 0; t < nb; ++t) {
+        const bool ta = hi32(xa) <= hi32(yb), tA = hi32(xA) > hi32(yB);
+        ko[s + t] = ta ? xa : yb;
+        ko[e - 1 - t] = tA ? xA : yB;
+        fa += ta;
+        fb += !ta;
+        ba -= tA;
+        bb -= !tA;
+        const bool ok = ta ? fa < a1 : fb < b1;
+        const bool ok2 = tA ? ba > a0 : bb > b0;
+        const unsigned long long nv = ok ? ki[ta ? fa : fb] : ~0ull;
+        const unsigned long long nv2 = ok2 ? ki[tA ? ba - 1 : bb - 1] : 0ull;
+        xa = ta ? nv : xa;
+        yb = ta ? yb : nv;
+        xA = tA ? nv2 : xA;
+        yB = tA ? yB : nv2;
+    }
+    if (len & 1) ko[s + nb] = hi32(xa) <= hi32(yb) ? xa : yb;   // the middle word
+}
+
 // Stable merge sort of ng sorted rows of ng words (row i = elements i*ng ..
 // i*ng+ng-1).  The rows start in buffer `start`; returns the buffer holding
-// the result.  Each lane produces a contiguous chunk of every level's output
-// from one merge-path search.  Within a merge every word of the left run
-// has a smaller element part than every word of the right run, so comparing
-// whole words is the stable merge.
+// the result.  Each lane produces a contiguous chunk of every level's output:
+// one merge-path search finds the split of its first position, the next
+// lane's search gives the split of its last (a chunk is never longer than a
+// pair of runs, so it touches at most two pairs; a pair's end needs no
+// search).  A level whose every pair is already in order (left run's last
+// word below the right run's first) is skipped; in the overlap passes of
+// typical k-distributions that holds for about one level in four.  Within a
+// merge every word of the left run has a smaller element part than every word
+// of the right run, so comparing whole words is the stable merge.
 template <int NGC>
 __device__ int merge_rows(const WarpPtr& wp, int ng_run, int lane, int start) {
     const int ng = NGC ? NGC : ng_run;
     const int n = ng * ng;
     const int ch = (n + 31) >> 5;
+    const int k0 = min(lane * ch, n), k1 = min(k0 + ch, n);
     int cur = start;
     for (int run = ng; run < n; run <<= 1) {
         const unsigned long long* ki = cur ? wp.bufB : wp.bufA;
         unsigned long long* ko = cur ? wp.bufA : wp.bufB;
-        const int k0 = lane * ch;
-        const int k1 = min(k0 + ch, n);
-        if (k0 < k1) {
-            const int two = run << 1;
-            int ms = (k0 / two) * two;
-            int m = min(run, n - ms);
-            int ny = max(0, min(run, n - ms - run));
+        const int two = run << 1;
+        {   // every pair of runs already in order (one lane per pair): the level is the identity
+            const int ms = lane * two;
+            bool inorder = true;
+            if (ms + run < n) inorder = ki[ms + run - 1] < ki[ms + run];
+            if (__all_sync(kFull, inorder)) continue;
+        }
+        int as = 0;                             // split of k0: words taken from its pair's left run
+        if (k0 < n) {
+            const unsigned* kh = (const unsigned*)ki + 1;   // the key halves
+            const int ms = (k0 / two) * two;
+            const int m = min(run, n - ms), ny = max(0, min(run, n - ms - run));
             const int kk = k0 - ms;
             int lo = max(0, kk - ny), hi = min(kk, m);
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
-                if (ki[ms + mid] < ki[ms + run + kk - mid - 1]) lo = mid + 1; else hi = mid;
+                if (kh[2 * (ms + mid)] <= kh[2 * (ms + run + kk - mid - 1)]) lo = mid + 1; else hi = mid;
             }
-            int a = lo, b = kk - lo;
-            unsigned long long xa = a < m ? ki[ms + a] : ~0ull;
-            unsigned long long yb = b < ny ? ki[ms + run + b] : ~0ull;
-            for (int k = k0; k < k1; ++k) {
-                if (k == ms + m + ny) {       // next pair of runs starts here
-                    ms = k;
-                    m = min(run, n - ms);
-                    ny = max(0, min(run, n - ms - run));
-                    a = 0;
-                    b = 0;
-                    xa = m > 0 ? ki[ms] : ~0ull;
-                    yb = ny > 0 ? ki[ms + run] : ~0ull;
-                }
-                if (xa < yb) {
-                    ko[k] = xa;
-                    ++a;
-                    xa = a < m ? ki[ms + a] : ~0ull;
-                } else {
-                    ko[k] = yb;
-                    ++b;
-                    yb = b < ny ? ki[ms + run + b] : ~0ull;
-                }
+            as = lo;
+        }
+        const int as_next = __shfl_down_sync(kFull, as, 1);
+        int s = k0, a = as;
+        while (s < k1) {
+            const int ms = (s / two) * two;
+            const int m = min(run, n - ms), ny = max(0, min(run, n - ms - run));
+            const int pe = ms + m + ny;
+            const int e = min(k1, pe);
+            const int b = (s - ms) - a;
+            int ae = m, be = ny;
+            if (e < pe) {                       // ends inside the pair: the next lane's split
+                ae = as_next;
+                be = (e - ms) - as_next;
             }
+            merge_seg(ki, ko, s, e, ms + a, ms + ae, ms + run + b, ms + run + be);
+            s = e;
+            a = 0;
         }
         __syncwarp();
         cur ^= 1;
@@ -967,34 +1009,38 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     // monotone and a2 >= 0.  If every row's first word exceeds the last word
     // of the row before it (and the rows are in order), row-major order is
     // already the sorted order; otherwise the rows are merged.  Other inputs
-    // take the bitonic network.
+    // (and any NaN key) take the reference heapsort.
     bool monoB = P.a2 >= 0.0f && (!P.first || P.a1 >= 0.0f);
     if (lane + 1 < ng) monoB = monoB && (wp.k2[lane] <= wp.k2[lane + 1]);
     monoB = __all_sync(kFull, monoB);
     const unsigned long long* A = wp.bufA;
     if (monoB) {
         unsigned long long* W = wp.bufB;            // row-major words
+        bool finite = true;                         // no NaN key
         {
             int i = lane / ng, j = lane - (lane / ng) * ng;
             for (int e = lane; e < nloop; e += 32) {
-                W[e] = pack(key_of(P, wp, i, j), i, j);
+                const float kv = key_of(P, wp, i, j);
+                finite = finite && kv == kv;
+                W[e] = pack(kv, i, j);
                 j += 32;
                 while (j >= ng) { j -= ng; ++i; }
             }
         }
+        monoB = __all_sync(kFull, finite);
         __syncwarp();
         bool disjoint = true;
         if (lane + 1 < ng) disjoint = W[(lane + 1) * ng] > W[lane * ng + ng - 1];
         disjoint = __all_sync(kFull, disjoint);
-        if (disjoint) {
+        if (monoB && disjoint) {
             A = W;
             dg.block_passes += (lane == 0);
-        } else if (merge_rows<NGC>(wp, ng, lane, 1) != 0) {
+        } else if (monoB && merge_rows<NGC>(wp, ng, lane, 1) != 0) {
             A = W;
         }
     }
     // inputs whose rows are not sorted (a k-distribution not monotone in g)
-    // take the reference heapsort below
+    // or that hold a NaN key take the reference heapsort below
     const bool need_exact = !monoB;
 
     // ---- cumulative weights, bin boundaries, tie checks --------------------
@@ -1036,7 +1082,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         gd = (double*)((A == wp.bufA) ? wp.bufB : wp.bufA);   // free buffer
         double run = 0.0;
         unsigned kbp = p0 >= 1 && p0 < p1 ? (unsigned)(A[p0 - 1] >> 32) : 0u;
-        bool anytie = false, nan = false;
+        bool anytie = false;
         for (int p = p0; p < p1; ++p) {
             const unsigned long long word = A[p];
             const unsigned q = (unsigned)word & 0xffffu;
@@ -1044,8 +1090,6 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             run = __dadd_rn(run, (double)__fmul_rn(delg[q >> 5], delg[q & 31]));
             gd[p] = run;
             anytie |= (p >= 1 && kb == kbp);         // fkey folds -0 onto +0
-            const float kp = funkey(kb);
-            nan |= (kp != kp);
             kbp = kb;
         }
         double incl = run;
@@ -1089,12 +1133,11 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         gerr = c_last == ng && sp_last < nloop - 1;    // elements left after the last boundary
         risky = __any_sync(kFull, risky);
         anytie = __any_sync(kFull, anytie);
-        nan = __any_sync(kFull, nan);
         if (attempt == 0) {
             dg.sort_passes += (lane == 0);
             dg.tie_passes += (lane == 0 && anytie);
         }
-        if (exact || !(risky || nan || (B.strict_ties && anytie))) break;
+        if (exact || !(risky || (B.strict_ties && anytie))) break;
         heapsort_pass();
     }
     if (gerr) atomicOr(B.status, kStGord);

@@ -407,7 +407,7 @@ int rtb_fwd_set_schedule(rtb_context* ctx, int schedule, int blocks_per_sm);
 
 /* Tile shape of the resident batch's launches: warps per block, i.e. the
  * layers of one (spectrum, wavenumber) item worked on at once (one warp per
- * layer, one lane per g-ordinate): 2, 4 or 8; 0 = the default 4.  Tiles
+ * layer, one lane per g-ordinate): 2, 4 or 8; 0 = the default 8.  Tiles
  * other than 4 exist for the usual kernel instance (one temperature grid, no
  * para-H2 / IMOD 18 / iform / non-LTE / air-Rayleigh option); other batches
  * run 4.  Results do not depend on the tile. */

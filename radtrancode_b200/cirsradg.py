@@ -276,7 +276,7 @@ class Context:
         self._check(self._L.rtb_fwd_set_schedule(self._h, schedule, blocks_per_sm))
 
     def set_tile(self, warps=0):
-        """Warps per block of the resident batch's launches (2, 4, 8; 0 = 4)."""
+        """Warps per block of the resident batch's launches (2, 4, 8; 0 = the default 8)."""
         self._check(self._L.rtb_fwd_set_tile(self._h, warps))
 
     def autotune(self) -> dict:

@@ -200,7 +200,7 @@ struct rtb_context {
     int occ = 0;                          // blocks per SM (0 = the occupancy maximum)
     int tile = rtb::kWarps;               // requested warps per CTA (rtb_fwd_set_tile / rtb_fwd_autotune)
     // the caller's own choices (rtb_fwd_set_tile / rtb_fwd_set_schedule), which a batch of an untuned shape uses
-    int tile_user = rtb::kWarps, sched_user = 0, occ_user = 0;
+    int tile_user = rtb::kTileDefault, sched_user = 0, occ_user = 0;
     int tile_eff = rtb::kWarps;           // warps per CTA of the resident batch's launches
     int bpsm_w[9] = {};                   // blocks per SM of the batch at 2, 4, 8 warps per CTA (0: not resident)
     int bpsm_max = 1;                     // blocks per SM of the current tile

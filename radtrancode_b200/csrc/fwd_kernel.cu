@@ -202,8 +202,10 @@ __host__ __device__ inline PathOff path_off(int nlmax, int ng, int nsw) {
     return p;
 }
 
+constexpr int kMergeLevels = 5;   // merge levels of NG <= 32 rows
+
 struct Layout {
-    int warp_bytes, path_bytes, off_gord, off_delg, off_region, total;
+    int warp_bytes, path_bytes, off_gord, off_delg, off_wtab, off_mtab, off_region, total;
 };
 __host__ __device__ inline Layout make_layout(int ng, int nsw, int ncol, int nlmax, int npath, int warps) {
     Layout Lo;
@@ -212,6 +214,8 @@ __host__ __device__ inline Layout make_layout(int ng, int nsw, int ncol, int nlm
     int o = 0;
     Lo.off_gord = o; o += 8 * (kMaxNg + 3);
     Lo.off_delg = o; o += 4 * kMaxNg;
+    Lo.off_wtab = o; o += 4 * 32 * kNgDev;       // element weights by (i << 5 | j)
+    Lo.off_mtab = o; o += 2 * kMergeLevels * 33;  // lanes' merge ranges
     o = align16(o);
     Lo.off_region = o;
     const int a = warps * Lo.warp_bytes, b = npath * Lo.path_bytes;
@@ -731,6 +735,7 @@ struct PassCtx {
 
 struct WarpPtr {
     unsigned long long *bufA, *bufB;
+    const short* mtab;       // lanes' merge output ranges (merge_lane_start), per CTA
     float *k1, *k2, *dk1, *dk2, *kg, *normf;
     double* splitfrac;
     int* splitpos;
@@ -781,25 +786,41 @@ __device__ __forceinline__ void merge_seg(const unsigned long long* ki, unsigned
     if (len & 1) ko[s + nb] = hi32(xa) <= hi32(yb) ? xa : yb;   // the middle word
 }
 
+// Output ranges of the lanes at each merge level, for NG rows (run = NG <<
+// level): pair p of runs (start st_p) is served by lanes [L_p, L_p+1),
+// L_p = floor(32 st_p / n), which split it evenly.  No lane's range crosses
+// a pair boundary, so every lane runs a single two-ended merge per level (7
+// steps for NG = 20).  The table mtab[level * 33 + lane] holds the lane's
+// first output position (n past the last level, and at lane 32).
+__device__ __forceinline__ int merge_lane_start(int ng, int level, int l) {
+    const int n = ng * ng, run = ng << level;
+    if (run >= n || l >= 32) return n;
+    const int two = run << 1, npairs = (n + two - 1) / two;
+    int p = 0;
+    while (p + 1 < npairs && (32 * (p + 1) * two) / n <= l) ++p;
+    const int st = p * two, sz = min(two, n - st);
+    const int lp = (32 * st) / n, lq = p + 1 < npairs ? (32 * (p + 1) * two) / n : 32;
+    return st + ((l - lp) * sz) / (lq - lp);
+}
+
 // Stable merge sort of ng sorted rows of ng words (row i = elements i*ng ..
 // i*ng+ng-1).  The rows start in buffer `start`; returns the buffer holding
-// the result.  Each lane produces a contiguous chunk of every level's output:
-// one merge-path search finds the split of its first position, the next
-// lane's search gives the split of its last (a chunk is never longer than a
-// pair of runs, so it touches at most two pairs; a pair's end needs no
-// search).  A level whose every pair is already in order (left run's last
-// word below the right run's first) is skipped; in the overlap passes of
-// typical k-distributions that holds for about one level in four.  Within a
-// merge every word of the left run has a smaller element part than every word
-// of the right run, so comparing whole words is the stable merge.
+// the result.  At each level every lane merges the output range mtab gives it
+// (inside one pair of runs): one merge-path search finds the split of its
+// first position, the next lane's search gives the split of its last (a
+// pair's end needs none).  A level whose every pair is already in order
+// (left run's last word below the right run's first) is skipped; in the
+// overlap passes of typical k-distributions that holds for about one level
+// in four.  Within a merge every word of the left run has a smaller element
+// part than every word of the right run, so comparing whole words is the
+// stable merge.
 template <int NGC>
-__device__ int merge_rows(const WarpPtr& wp, int ng_run, int lane, int start) {
+__device__ int merge_rows(const WarpPtr& wp, const short* mtab, int ng_run, int lane, int start) {
     const int ng = NGC ? NGC : ng_run;
     const int n = ng * ng;
-    const int ch = (n + 31) >> 5;
-    const int k0 = min(lane * ch, n), k1 = min(k0 + ch, n);
     int cur = start;
-    for (int run = ng; run < n; run <<= 1) {
+    int level = 0;
+    for (int run = ng; run < n; run <<= 1, ++level) {
         const unsigned long long* ki = cur ? wp.bufB : wp.bufA;
         unsigned long long* ko = cur ? wp.bufA : wp.bufB;
         const int two = run << 1;
@@ -809,12 +830,13 @@ __device__ int merge_rows(const WarpPtr& wp, int ng_run, int lane, int start) {
             if (ms + run < n) inorder = ki[ms + run - 1] < ki[ms + run];
             if (__all_sync(kFull, inorder)) continue;
         }
-        int as = 0;                             // split of k0: words taken from its pair's left run
-        if (k0 < n) {
+        const int s = mtab[level * 33 + lane], e = mtab[level * 33 + lane + 1];
+        const int ms = (s / two) * two;
+        const int m = min(run, n - ms), ny = max(0, min(run, n - ms - run));
+        const int kk = s - ms;
+        int as = 0;                             // split of s: words taken from the pair's left run
+        if (s < n) {
             const unsigned* kh = (const unsigned*)ki + 1;   // the key halves
-            const int ms = (k0 / two) * two;
-            const int m = min(run, n - ms), ny = max(0, min(run, n - ms - run));
-            const int kk = k0 - ms;
             int lo = max(0, kk - ny), hi = min(kk, m);
             while (lo < hi) {
                 const int mid = (lo + hi) >> 1;
@@ -823,21 +845,13 @@ __device__ int merge_rows(const WarpPtr& wp, int ng_run, int lane, int start) {
             as = lo;
         }
         const int as_next = __shfl_down_sync(kFull, as, 1);
-        int s = k0, a = as;
-        while (s < k1) {
-            const int ms = (s / two) * two;
-            const int m = min(run, n - ms), ny = max(0, min(run, n - ms - run));
-            const int pe = ms + m + ny;
-            const int e = min(k1, pe);
-            const int b = (s - ms) - a;
+        if (s < e) {
             int ae = m, be = ny;
-            if (e < pe) {                       // ends inside the pair: the next lane's split
+            if (e < ms + m + ny) {              // ends inside the pair: the next lane's split
                 ae = as_next;
                 be = (e - ms) - as_next;
             }
-            merge_seg(ki, ko, s, e, ms + a, ms + ae, ms + run + b, ms + run + be);
-            s = e;
-            a = 0;
+            merge_seg(ki, ko, s, e, ms + as, ms + ae, ms + run + (kk - as), ms + run + be);
         }
         __syncwarp();
         cur ^= 1;
@@ -875,7 +889,7 @@ __device__ __forceinline__ float elem_grad(const PassCtx& P, int gcol, int c, in
 // (kGradScratch bytes).
 template <int NCV>
 __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
-                                             const unsigned long long* A, void* scratch, const float* delg,
+                                             const unsigned long long* A, void* scratch, const float* wtab,
                                              const float* colP, float* colN, const int (&cmap)[kMaxCols], int nz,
                                              int ng, int nloop, int c_last, int p0, int p1, int ch, int lane) {
     const int ncol = P.ncol;
@@ -927,7 +941,7 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
     for (int p = p0; p < p1; ++p) {
         const unsigned q = (unsigned)A[p] & 0xffffu;
         const int i = q >> 5, j = q & 31;
-        const float w = __fmul_rn(delg[i], delg[j]);
+        const float w = wtab[q];
         float uu[8], vv[8];
         {
             const float4 u0 = UV[2 * i], v0 = UV[2 * ng + 2 * j];
@@ -1000,7 +1014,7 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
 
 template <int NGC>
 __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
-                          const double* g_ord, const float* delg, int lane, Diag& dg, const float* colP,
+                          const double* g_ord, const float* wtab, int lane, Diag& dg, const float* colP,
                           float* colN, int16_t* dbg_perm, int16_t* dbg_split) {
     // NGC > 0: the run's NG as a compile-time constant (NGC = P.ng)
     const int ng = NGC ? NGC : P.ng, nloop = NGC ? NGC * NGC : P.nloop;
@@ -1035,7 +1049,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         if (monoB && disjoint) {
             A = W;
             dg.block_passes += (lane == 0);
-        } else if (monoB && merge_rows<NGC>(wp, ng, lane, 1) != 0) {
+        } else if (monoB && merge_rows<NGC>(wp, wp.mtab, ng, lane, 1) != 0) {
             A = W;
         }
     }
@@ -1087,7 +1101,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             const unsigned long long word = A[p];
             const unsigned q = (unsigned)word & 0xffffu;
             const unsigned kb = (unsigned)(word >> 32);
-            run = __dadd_rn(run, (double)__fmul_rn(delg[q >> 5], delg[q & 31]));
+            run = __dadd_rn(run, (double)wtab[q]);
             gd[p] = run;
             anytie |= (p >= 1 && kb == kbp);         // fkey folds -0 onto +0
             kbp = kb;
@@ -1117,7 +1131,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
                 const unsigned kb = (unsigned)(word >> 32);
                 const double gprev = sp > 0 ? gd[sp - 1] : 0.0;
                 wp.splitpos[lane] = sp;
-                wp.splitfrac[lane] = __ddiv_rn(__dsub_rn(gb, gprev), (double)__fmul_rn(delg[q >> 5], delg[q & 31]));
+                wp.splitfrac[lane] = __ddiv_rn(__dsub_rn(gb, gprev), (double)wtab[q]);
                 const bool tl = sp >= 1 && kb == (unsigned)(A[sp - 1] >> 32);
                 const bool tr = sp + 1 < nloop && kb == (unsigned)(A[sp + 1] >> 32);
                 risky = tl || tr;
@@ -1166,7 +1180,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
                 const unsigned q = (unsigned)word & 0xffffu;
                 const int i = q >> 5, j = q & 31;
                 const float cval = funkey((unsigned)(word >> 32));
-                const float w = __fmul_rn(delg[i], delg[j]);
+                const float w = wtab[q];
                 const double gcur = __dadd_rn(gprev, (double)w);
                 if (ig >= ng) { atomicOr(B.status, kStGord); break; }
                 if (gcur < g_ord[ig + 1]) {
@@ -1224,7 +1238,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
                 const double frac = wp.splitfrac[bb - 1];
                 const unsigned long long word = A[s];
                 const unsigned q = (unsigned)word & 0xffffu;
-                const float w = __fmul_rn(delg[q >> 5], delg[q & 31]);
+                const float w = wtab[q];
                 const float sr = __double2float_rn(__dsub_rn(1.0, frac));
                 acc = __fmul_rn(__fmul_rn(sr, funkey((unsigned)(word >> 32))), w);
                 sum = __dmul_rn(__dsub_rn(1.0, frac), (double)w);
@@ -1236,7 +1250,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             for (; p < pend; ++p) {
                 const unsigned long long word = A[p];
                 const unsigned q = (unsigned)word & 0xffffu;
-                const float w = __fmul_rn(delg[q >> 5], delg[q & 31]);
+                const float w = wtab[q];
                 acc = __fadd_rn(acc, __fmul_rn(funkey((unsigned)(word >> 32)), w));
                 sum = __dadd_rn(sum, (double)w);
             }
@@ -1246,7 +1260,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
                 const double frac = wp.splitfrac[bb];
                 const unsigned long long word = A[s];
                 const unsigned q = (unsigned)word & 0xffffu;
-                const float w = __fmul_rn(delg[q >> 5], delg[q & 31]);
+                const float w = wtab[q];
                 const float sf = __double2float_rn(frac);
                 acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(sf, funkey((unsigned)(word >> 32))), w));
                 sum = __dadd_rn(sum, __dmul_rn(frac, (double)w));
@@ -1273,9 +1287,9 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             if (g == S.ngas || g <= P.igas) cmap[nz++] = c;
         }
     }
-    if (nz <= 4) grad_columns<4>(S, P, wp, A, gd, delg, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
-    else if (nz == 5) grad_columns<5>(S, P, wp, A, gd, delg, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
-    else grad_columns<8>(S, P, wp, A, gd, delg, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
+    if (nz <= 4) grad_columns<4>(S, P, wp, A, gd, wtab, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
+    else if (nz == 5) grad_columns<5>(S, P, wp, A, gd, wtab, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
+    else grad_columns<8>(S, P, wp, A, gd, wtab, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
     __syncwarp();
 }
 
@@ -1316,6 +1330,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
     const PathOff po = path_off(nlmax_max, B.ng, nsw_max);
     double* g_ord = (double*)(smem + Lo.off_gord);
     float* delg = (float*)(smem + Lo.off_delg);
+    float* wtab = (float*)(smem + Lo.off_wtab);   // w(i, j) = delg(i) delg(j), the overlap's element weights
     char* region = smem + Lo.off_region;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ng = NGC ? NGC : B.ng;   // NGC > 0: the instance for NG = NGC (== B.ng)
@@ -1324,6 +1339,12 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
     float* dtau_s = tau_s + (int64_t)B.cell_Lmax * ng;
     for (int i = tid; i <= ng + 2; i += kThreads) g_ord[i] = i <= ng ? B.g_ord[i] : __longlong_as_double(0x7ff0000000000000ll);
     for (int i = tid; i < ng; i += kThreads) delg[i] = B.delg[i];
+    for (int q = tid; q < ng * 32; q += kThreads) {
+        const int j = q & 31;
+        wtab[q] = j < ng ? __fmul_rn(B.delg[q >> 5], B.delg[j]) : 0.0f;
+    }
+    short* mtab = (short*)(smem + Lo.off_mtab);
+    for (int i = tid; i < kMergeLevels * 33; i += kThreads) mtab[i] = (short)merge_lane_start(ng, i / 33, i % 33);
     Diag dg{0, 0, 0, 0, 0};
     __syncthreads();
 
@@ -1331,6 +1352,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
     WarpPtr wp;
     wp.bufA = (unsigned long long*)(wsm + wo.bufA);
     wp.bufB = (unsigned long long*)(wsm + wo.bufB);
+    wp.mtab = mtab;
     wp.k1 = (float*)(wsm + wo.k1);
     wp.k2 = (float*)(wsm + wo.k2);
     wp.dk1 = (float*)(wsm + wo.dk1);
@@ -1499,7 +1521,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
                         PassCtx P;
                         P.ng = ng; P.nloop = ng * ng; P.ncol = ncol; P.first = first; P.igas = ig;
                         P.a1 = a1; P.a2 = a2;
-                        sort_pass<NGC>(B, S, P, wp, g_ord, delg, lane, dg, colP, colN, dp, dsp);
+                        sort_pass<NGC>(B, S, P, wp, g_ord, wtab, lane, dg, colP, colN, dp, dsp);
                         kgv = lane < ng ? wp.kg[lane] : 0.0f;
                     }
                     __syncwarp();

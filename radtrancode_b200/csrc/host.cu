@@ -1728,7 +1728,7 @@ int rtb_fwd_set_tile(rtb_context* c, int warps) {
     if (!c) return RTB_ERR_ARG;
     if (!(warps == 0 || warps == 2 || warps == 4 || warps == 8))
         return fail(c, RTB_ERR_ARG, "tile of %d warps per block (2, 4 or 8)", warps);
-    c->tile = c->tile_user = warps ? warps : kWarps;
+    c->tile = c->tile_user = warps ? warps : kTileDefault;
     if (!c->prepared) return RTB_OK;
     CUDA_TRY(c, cudaSetDevice(c->device));
     return apply_schedule(c);

@@ -14,7 +14,8 @@ constexpr int kMaxCols = 8;       // tracked gradient columns in the overlap (ac
 constexpr int kMaxSw = 8;         // active Jacobian columns (isw) per spectrum
 constexpr int kMaxGasDev = 30;    // MAXGAS
 constexpr int kMaxPathDev = 4;    // paths of one spectrum per device work item (more: path groups)
-constexpr int kWarps = 4;         // warps per CTA of the forward kernel
+constexpr int kWarps = 4;         // warps per CTA of the forward kernel (every instance has this tile)
+constexpr int kTileDefault = 8;   // the tile a batch runs unless tuned or set (where its instance has it)
 constexpr int kThreads = kWarps * 32;
 
 // status bits accumulated by the kernel (OR-ed into a device word)

@@ -150,16 +150,19 @@ __device__ __noinline__ void heapsort_words(int n, unsigned long long* W0) {
 
 __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 
-// bytes of one element buffer: NG^2 64-bit words, or the scratch of
-// grad_columns (U/V tables 4 NG float4, the closing-split partials 8 x NG
-// floats, the chunk-end partials 8 x 32 floats and 32 shorts), whichever is
-// larger, for NG up to 22
+// bytes of one element buffer: the NG rows of 64-bit words with a sentinel
+// word on either side of each and one sentinel pair after the last (the
+// merge's layout), or the scratch of grad_columns (U/V tables 4 NG float4, the
+// closing-split partials 8 x NG floats, the chunk-end partials 8 x 32 floats
+// and 32 shorts), whichever is larger, for NG up to 22
 constexpr int kNgDev = 22;
 constexpr int kGradScratch = 64 * kNgDev + 32 * kNgDev + 32 * 32 + 2 * 32;
-constexpr int kElemBuf = ((8 * kN > kGradScratch ? 8 * kN : kGradScratch) + 15) & ~15;
-// per-warp scratch sub-offsets (bytes).  bufA holds the sorted (key, element)
-// words of a pass; bufB is the merge's second buffer, then the per-bin row and
-// column weight sums R[b][i], C[b][j] (2*ng*ng floats <= 4096 B for ng <= 22).
+constexpr int kMergeWords = kN + 2 * kNgDev + 2;
+constexpr int kElemBuf = ((8 * kMergeWords > kGradScratch ? 8 * kMergeWords : kGradScratch) + 15) & ~15;
+// per-warp scratch sub-offsets (bytes).  bufA and bufB hold the (key,
+// element) words of a pass and the merge's levels in turn; the one not
+// holding the sorted words then takes the FP64 cumulative weights and the
+// gradient-column scratch.
 struct WarpOff {
     int bufA, bufB, splitfrac, k1, k2, dk1, dk2, kg, normf, splitpos, colA, colB, total;
 };
@@ -756,15 +759,16 @@ __device__ __forceinline__ unsigned hi32(unsigned long long w) { return (unsigne
 // the front half smallest-first from the start, the back half largest-first
 // from the end, as two independent chains.  Only the key halves are
 // compared: every element of A precedes every element of B, so on equal keys
-// A's word comes first (the stable order).  Branch-free steps; an exhausted
-// side reads as ~0 (front) or 0 (back), keys no word can hold (NaN keys never
-// reach the merge).
+// A's word comes first (the stable order).  No bounds are checked: past a
+// side's end of the range lies the next word of its run (which follows every
+// word of the other side still in the range: the ranges end at a merge-path
+// split) or the run's sentinel (key ~0 after a run, 0 before it, keys no word
+// holds since NaN keys never reach the merge).
 __device__ __forceinline__ void merge_seg(const unsigned long long* ki, unsigned long long* ko, int s, int e,
                                           int a0, int a1, int b0, int b1) {
     const int len = e - s, nb = len >> 1;
     int fa = a0, fb = b0, ba = a1, bb = b1;
-    unsigned long long xa = fa < a1 ? ki[fa] : ~0ull, yb = fb < b1 ? ki[fb] : ~0ull;
-    unsigned long long xA = ba > a0 ? ki[ba - 1] : 0ull, yB = bb > b0 ? ki[bb - 1] : 0ull;
+    unsigned long long xa = ki[fa], yb = ki[fb], xA = ki[ba - 1], yB = ki[bb - 1];
 #pragma unroll 1
     for (int t = 0; t < nb; ++t) {
         const bool ta = hi32(xa) <= hi32(yb), tA = hi32(xA) > hi32(yB);
@@ -774,10 +778,8 @@ __device__ __forceinline__ void merge_seg(const unsigned long long* ki, unsigned
         fb += !ta;
         ba -= tA;
         bb -= !tA;
-        const bool ok = ta ? fa < a1 : fb < b1;
-        const bool ok2 = tA ? ba > a0 : bb > b0;
-        const unsigned long long nv = ok ? ki[ta ? fa : fb] : ~0ull;
-        const unsigned long long nv2 = ok2 ? ki[tA ? ba - 1 : bb - 1] : 0ull;
+        const unsigned long long nv = ki[ta ? fa : fb];
+        const unsigned long long nv2 = ki[tA ? ba - 1 : bb - 1];
         xa = ta ? nv : xa;
         yb = ta ? yb : nv;
         xA = tA ? nv2 : xA;
@@ -803,17 +805,20 @@ __device__ __forceinline__ int merge_lane_start(int ng, int level, int l) {
     return st + ((l - lp) * sz) / (lq - lp);
 }
 
-// Stable merge sort of ng sorted rows of ng words (row i = elements i*ng ..
-// i*ng+ng-1).  The rows start in buffer `start`; returns the buffer holding
-// the result.  At each level every lane merges the output range mtab gives it
-// (inside one pair of runs): one merge-path search finds the split of its
-// first position, the next lane's search gives the split of its last (a
-// pair's end needs none).  A level whose every pair is already in order
-// (left run's last word below the right run's first) is skipped; in the
-// overlap passes of typical k-distributions that holds for about one level
-// in four.  Within a merge every word of the left run has a smaller element
-// part than every word of the right run, so comparing whole words is the
-// stable merge.
+// Stable merge sort of ng sorted rows of ng words.  Layout of every level:
+// run r of length `run` (the last one may be shorter) at r * (run + 2) + 1,
+// the word 0 before it and ~0 after it, and right after the last run's ~0 a
+// further pair 0, ~0 (the empty right run of an unpaired last run).  The rows start
+// in buffer `start` in that layout (run = ng); the result is one run at
+// offset 1 of the returned buffer.  At each level every lane merges the
+// output range mtab gives it (inside one pair of runs): one merge-path
+// search finds the split of its first position, the next lane's search gives
+// the split of its last (a pair's end needs none).  A level whose every pair
+// is already in order (left run's last word below the right run's first) is
+// copied instead; in the overlap passes of typical k-distributions that holds
+// for about one level in four.  Within a merge every word of the left run has
+// a smaller element part than every word of the right run, so comparing
+// whole words is the stable merge.
 template <int NGC>
 __device__ int merge_rows(const WarpPtr& wp, const short* mtab, int ng_run, int lane, int start) {
     const int ng = NGC ? NGC : ng_run;
@@ -823,35 +828,51 @@ __device__ int merge_rows(const WarpPtr& wp, const short* mtab, int ng_run, int 
     for (int run = ng; run < n; run <<= 1, ++level) {
         const unsigned long long* ki = cur ? wp.bufB : wp.bufA;
         unsigned long long* ko = cur ? wp.bufA : wp.bufB;
-        const int two = run << 1;
-        {   // every pair of runs already in order (one lane per pair): the level is the identity
-            const int ms = lane * two;
-            bool inorder = true;
-            if (ms + run < n) inorder = ki[ms + run - 1] < ki[ms + run];
-            if (__all_sync(kFull, inorder)) continue;
+        const int two = run << 1, sin = run + 2, sout = two + 2;
+        const int nout = (n + two - 1) / two;   // runs after this level
+        bool inorder = true;                    // pair `lane` already in order
+        if (lane * two + run < n) inorder = ki[2 * lane * sin + run] < ki[(2 * lane + 1) * sin + 1];
+        const bool copy = __all_sync(kFull, inorder);
+        if (lane < nout) {                      // the output runs' sentinels
+            ko[lane * sout] = 0ull;
+            ko[lane * sout + 1 + min(two, n - lane * two)] = ~0ull;
+        }
+        if (lane == 0) {
+            const int last = (nout - 1) * sout + 2 + (n - (nout - 1) * two);
+            ko[last] = 0ull;
+            ko[last + 1] = ~0ull;
         }
         const int s = mtab[level * 33 + lane], e = mtab[level * 33 + lane + 1];
-        const int ms = (s / two) * two;
+        const int p = s / two, ms = p * two;
         const int m = min(run, n - ms), ny = max(0, min(run, n - ms - run));
         const int kk = s - ms;
-        int as = 0;                             // split of s: words taken from the pair's left run
-        if (s < n) {
-            const unsigned* kh = (const unsigned*)ki + 1;   // the key halves
-            int lo = max(0, kk - ny), hi = min(kk, m);
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (kh[2 * (ms + mid)] <= kh[2 * (ms + run + kk - mid - 1)]) lo = mid + 1; else hi = mid;
+        const int abase = 2 * p * sin + 1, bbase = ny > 0 ? abase + sin : abase + m + 2;
+        const int obase = p * sout + 1 - ms;
+        if (copy) {
+            for (int k = s; k < e; ++k) {
+                const int o = k - ms;
+                ko[obase + k] = ki[o < m ? abase + o : bbase + (o - m)];
             }
-            as = lo;
-        }
-        const int as_next = __shfl_down_sync(kFull, as, 1);
-        if (s < e) {
-            int ae = m, be = ny;
-            if (e < ms + m + ny) {              // ends inside the pair: the next lane's split
-                ae = as_next;
-                be = (e - ms) - as_next;
+        } else {
+            int as = 0;                         // split of s: words taken from the pair's left run
+            if (s < n) {
+                const unsigned* kh = (const unsigned*)ki + 1;   // the key halves
+                int lo = max(0, kk - ny), hi = min(kk, m);
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (kh[2 * (abase + mid)] <= kh[2 * (bbase + kk - mid - 1)]) lo = mid + 1; else hi = mid;
+                }
+                as = lo;
             }
-            merge_seg(ki, ko, s, e, ms + as, ms + ae, ms + run + (kk - as), ms + run + be);
+            const int as_next = __shfl_down_sync(kFull, as, 1);
+            if (s < e) {
+                int ae = m, be = ny;
+                if (e < ms + m + ny) {          // ends inside the pair: the next lane's split
+                    ae = as_next;
+                    be = (e - ms) - as_next;
+                }
+                merge_seg(ki, ko, obase + s, obase + e, abase + as, abase + ae, bbase + (kk - as), bbase + be);
+            }
         }
         __syncwarp();
         cur ^= 1;
@@ -959,7 +980,7 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
         float val[NCV];
 #pragma unroll
         for (int c = 0; c < NCV; ++c) val[c] = w * (uu[c] + vv[c]);
-        if (p == nsp) {                         // the split element closes bin b
+        if (p == nsp) {
             const float f = (float)wp.splitfrac[b];
 #pragma unroll
             for (int c = 0; c < NCV; ++c) {
@@ -1029,16 +1050,25 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     monoB = __all_sync(kFull, monoB);
     const unsigned long long* A = wp.bufA;
     if (monoB) {
-        unsigned long long* W = wp.bufB;            // row-major words
+        // row-major words: contiguous in bufA, and in bufB in the merge's
+        // layout (row i at i (ng + 2) + 1 between sentinels)
+        unsigned long long* W = wp.bufA;
+        unsigned long long* Wg = wp.bufB;
         bool finite = true;                         // no NaN key
         {
             int i = lane / ng, j = lane - (lane / ng) * ng;
             for (int e = lane; e < nloop; e += 32) {
                 const float kv = key_of(P, wp, i, j);
                 finite = finite && kv == kv;
-                W[e] = pack(kv, i, j);
+                const unsigned long long w = pack(kv, i, j);
+                W[e] = w;
+                Wg[e + 2 * i + 1] = w;
                 j += 32;
                 while (j >= ng) { j -= ng; ++i; }
+            }
+            if (lane <= ng) {
+                Wg[lane * (ng + 2)] = 0ull;
+                Wg[lane * (ng + 2) + (lane < ng ? ng + 1 : 1)] = ~0ull;
             }
         }
         monoB = __all_sync(kFull, finite);
@@ -1047,10 +1077,9 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         if (lane + 1 < ng) disjoint = W[(lane + 1) * ng] > W[lane * ng + ng - 1];
         disjoint = __all_sync(kFull, disjoint);
         if (monoB && disjoint) {
-            A = W;
             dg.block_passes += (lane == 0);
-        } else if (monoB && merge_rows<NGC>(wp, wp.mtab, ng, lane, 1) != 0) {
-            A = W;
+        } else if (monoB) {
+            A = (merge_rows<NGC>(wp, wp.mtab, ng, lane, 1) ? wp.bufB : wp.bufA) + 1;
         }
     }
     // inputs whose rows are not sorted (a k-distribution not monotone in g)
@@ -1071,7 +1100,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     // scratch lives in the buffer not holding A, its result replaces A
     auto heapsort_pass = [&]() {
         __syncwarp();
-        unsigned long long* Aw = (A == wp.bufA) ? wp.bufA : wp.bufB;
+        unsigned long long* Aw = (A >= wp.bufB) ? wp.bufB : wp.bufA;
         for (int e = lane; e < nloop; e += 32) {
             const int i = e / ng, j = e - i * ng;
             Aw[e] = ((unsigned long long)__float_as_uint(key_of(P, wp, i, j)) << 32) | (unsigned)e;
@@ -1093,7 +1122,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     if (need_exact) heapsort_pass();
     double* gd = nullptr;
     for (int attempt = 0; attempt < 2; ++attempt) {
-        gd = (double*)((A == wp.bufA) ? wp.bufB : wp.bufA);   // free buffer
+        gd = (double*)((A >= wp.bufB) ? wp.bufA : wp.bufB);   // free buffer
         double run = 0.0;
         unsigned kbp = p0 >= 1 && p0 < p1 ? (unsigned)(A[p0 - 1] >> 32) : 0u;
         bool anytie = false;

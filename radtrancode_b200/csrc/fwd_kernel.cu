@@ -152,11 +152,11 @@ __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 
 // bytes of one element buffer: the NG rows of 64-bit words with a sentinel
 // word on either side of each and one sentinel pair after the last (the
-// merge's layout), or the scratch of grad_columns (U/V tables 4 NG float4, the
+// merge's layout), or the scratch of grad_columns (U/V tables 6 NG float4, the
 // closing-split partials 8 x NG floats, the chunk-end partials 8 x 32 floats
 // and 32 shorts), whichever is larger, for NG up to 22
 constexpr int kNgDev = 22;
-constexpr int kGradScratch = 64 * kNgDev + 32 * kNgDev + 32 * 32 + 2 * 32;
+constexpr int kGradScratch = 96 * kNgDev + 32 * kNgDev + 32 * 32 + 2 * 32;
 constexpr int kMergeWords = kN + 2 * kNgDev + 2;
 constexpr int kElemBuf = ((8 * kMergeWords > kGradScratch ? 8 * kMergeWords : kGradScratch) + 15) & ~15;
 // per-warp scratch sub-offsets (bytes).  bufA and bufB hold the (key,
@@ -829,7 +829,8 @@ __device__ int merge_rows(const WarpPtr& wp, const short* mtab, int ng_run, int 
         const unsigned long long* ki = cur ? wp.bufB : wp.bufA;
         unsigned long long* ko = cur ? wp.bufA : wp.bufB;
         const int two = run << 1, sin = run + 2, sout = two + 2;
-        const int nout = (n + two - 1) / two;   // runs after this level
+        const int sh = level + 1;               // two = ng << sh, n / two = ng >> sh
+        const int nout = (ng + (1 << sh) - 1) >> sh;   // runs after this level
         bool inorder = true;                    // pair `lane` already in order
         if (lane * two + run < n) inorder = ki[2 * lane * sin + run] < ki[(2 * lane + 1) * sin + 1];
         const bool copy = __all_sync(kFull, inorder);
@@ -843,7 +844,7 @@ __device__ int merge_rows(const WarpPtr& wp, const short* mtab, int ng_run, int 
             ko[last + 1] = ~0ull;
         }
         const int s = mtab[level * 33 + lane], e = mtab[level * 33 + lane + 1];
-        const int p = s / two, ms = p * two;
+        const int p = (s / ng) >> sh, ms = p * two;
         const int m = min(run, n - ms), ny = max(0, min(run, n - ms - run));
         const int kk = s - ms;
         const int abase = 2 * p * sin + 1, bbase = ny > 0 ? abase + sin : abase + m + 2;
@@ -914,8 +915,9 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
                                              const float* colP, float* colN, const int (&cmap)[kMaxCols], int nz,
                                              int ng, int nloop, int c_last, int p0, int p1, int ch, int lane) {
     const int ncol = P.ncol;
-    float4* UV = (float4*)scratch;             // U rows [ng][2 float4], then V rows [ng][2 float4]
-    float* Eb = (float*)(UV + 4 * ng);         // [ng][8] partial of bin b up to its closing split
+    float4* UV = (float4*)scratch;             // U rows [ng][3 float4], then V rows [ng][3 float4]
+                                               // (8 values and a pad: rows 48 B apart spread over the banks)
+    float* Eb = (float*)(UV + 6 * ng);         // [ng][8] partial of bin b up to its closing split
     float4* Lp = (float4*)(Eb + 8 * ng);       // [32][2] chunk-end partial of each lane
     short* BL = (short*)(Lp + 2 * 32);         // [32] its bin (-1: empty chunk)
     if (lane < ng) {
@@ -939,10 +941,10 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
                 }
             }
         }
-        UV[2 * x] = make_float4(u[0], u[1], u[2], u[3]);
-        UV[2 * x + 1] = make_float4(u[4], u[5], u[6], u[7]);
-        UV[2 * ng + 2 * x] = make_float4(v[0], v[1], v[2], v[3]);
-        UV[2 * ng + 2 * x + 1] = make_float4(v[4], v[5], v[6], v[7]);
+        UV[3 * x] = make_float4(u[0], u[1], u[2], u[3]);
+        UV[3 * x + 1] = make_float4(u[4], u[5], u[6], u[7]);
+        UV[3 * ng + 3 * x] = make_float4(v[0], v[1], v[2], v[3]);
+        UV[3 * ng + 3 * x + 1] = make_float4(v[4], v[5], v[6], v[7]);
     }
     __syncwarp();
     int b = 0;
@@ -965,14 +967,14 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
         const float w = wtab[q];
         float uu[8], vv[8];
         {
-            const float4 u0 = UV[2 * i], v0 = UV[2 * ng + 2 * j];
+            const float4 u0 = UV[3 * i], v0 = UV[3 * ng + 3 * j];
             uu[0] = u0.x; uu[1] = u0.y; uu[2] = u0.z; uu[3] = u0.w;
             vv[0] = v0.x; vv[1] = v0.y; vv[2] = v0.z; vv[3] = v0.w;
             if (NCV == 5) {
-                uu[4] = ((const float*)(UV + 2 * i + 1))[0];
-                vv[4] = ((const float*)(UV + 2 * ng + 2 * j + 1))[0];
+                uu[4] = ((const float*)(UV + 3 * i + 1))[0];
+                vv[4] = ((const float*)(UV + 3 * ng + 3 * j + 1))[0];
             } else if (NCV == 8) {
-                const float4 u1 = UV[2 * i + 1], v1 = UV[2 * ng + 2 * j + 1];
+                const float4 u1 = UV[3 * i + 1], v1 = UV[3 * ng + 3 * j + 1];
                 uu[4] = u1.x; uu[5] = u1.y; uu[6] = u1.z; uu[7] = u1.w;
                 vv[4] = v1.x; vv[5] = v1.y; vv[6] = v1.z; vv[7] = v1.w;
             }
@@ -1087,11 +1089,12 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     const bool need_exact = !monoB;
 
     // ---- cumulative weights, bin boundaries, tie checks --------------------
-    // Each lane takes a chunk of consecutive sorted positions: FP64 prefix of
-    // the weights (exact in any order) into scratch; then one lane per g
-    // boundary binary-searches its split position (the first position whose
-    // cumulative weight reaches g_ord(b+1), rankg.f:119-129) and forms the
-    // split fraction.
+    // Each lane takes a chunk of consecutive sorted positions: the FP64 prefix
+    // of the weights inside its chunk into scratch, and a warp scan of the
+    // chunk totals (every partial sum is exact, so any order gives the
+    // reference's values); then one lane per g boundary finds its split
+    // position (the first position whose cumulative weight reaches
+    // g_ord(b+1), rankg.f:119-129) and forms the split fraction.
     const int ch = (nloop + 31) >> 5;
     const int p0 = min(lane * ch, nloop), p1 = min(p0 + ch, nloop);
     bool exact = false, irregular = false, gerr = false;
@@ -1142,23 +1145,35 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             if (lane >= o) incl = __dadd_rn(incl, t);
         }
         const double base = __dsub_rn(incl, run);   // exact: every partial sum is exact
-        for (int p = p0; p < p1; ++p) gd[p] = __dadd_rn(gd[p], base);
         __syncwarp();
+        // boundary b = lane: the lane L whose chunk the prefix reaches g_ord(b+1)
+        // in (a search over the lanes' totals), then the position inside it
+        const double gb = lane < ng ? g_ord[lane + 1] : 0.0;
+        int L = 0;
+#pragma unroll
+        for (int st = 16; st >= 1; st >>= 1) {
+            const double v = __shfl_sync(kFull, incl, L + st - 1);
+            if (v < gb) L += st;
+        }
+        const double tot = __shfl_sync(kFull, incl, 31);
+        const double bL = __shfl_sync(kFull, base, L);
         int sp = nloop;
         bool risky = false;
         if (lane < ng) {
-            const double gb = g_ord[lane + 1];
-            int lo = 0, hi = nloop;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (gd[mid] >= gb) hi = mid; else lo = mid + 1;
+            const int c0 = min(L * ch, nloop);
+            if (tot >= gb) {
+                int lo = c0, hi = min(c0 + ch, nloop);
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (__dadd_rn(gd[mid], bL) >= gb) hi = mid; else lo = mid + 1;
+                }
+                sp = lo;
             }
-            sp = lo;
             if (sp < nloop) {
                 const unsigned long long word = A[sp];
                 const unsigned q = (unsigned)word & 0xffffu;
                 const unsigned kb = (unsigned)(word >> 32);
-                const double gprev = sp > 0 ? gd[sp - 1] : 0.0;
+                const double gprev = sp > c0 ? __dadd_rn(gd[sp - 1], bL) : bL;
                 wp.splitpos[lane] = sp;
                 wp.splitfrac[lane] = __ddiv_rn(__dsub_rn(gb, gprev), (double)wtab[q]);
                 const bool tl = sp >= 1 && kb == (unsigned)(A[sp - 1] >> 32);

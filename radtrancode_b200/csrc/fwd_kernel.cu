@@ -152,19 +152,18 @@ __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 
 // bytes of one element buffer: the NG rows of 64-bit words with a sentinel
 // word on either side of each and one sentinel pair after the last (the
-// merge's layout), or the scratch of grad_columns (U/V tables 6 NG float4, the
-// closing-split partials 8 x NG floats, the chunk-end partials 8 x 32 floats
-// and 32 shorts), whichever is larger, for NG up to 22
+// merge's layout), or the gradient-column tables (6 NG float4), whichever is
+// larger, for NG up to 22
 constexpr int kNgDev = 22;
-constexpr int kGradScratch = 96 * kNgDev + 32 * kNgDev + 32 * 32 + 2 * 32;
+constexpr int kGradScratch = 96 * kNgDev;
 constexpr int kMergeWords = kN + 2 * kNgDev + 2;
 constexpr int kElemBuf = ((8 * kMergeWords > kGradScratch ? 8 * kMergeWords : kGradScratch) + 15) & ~15;
 // per-warp scratch sub-offsets (bytes).  bufA and bufB hold the (key,
 // element) words of a pass and the merge's levels in turn; the one not
 // holding the sorted words then takes the FP64 cumulative weights and the
-// gradient-column scratch.
+// gradient-column tables.
 struct WarpOff {
-    int bufA, bufB, splitfrac, k1, k2, dk1, dk2, kg, normf, splitpos, colA, colB, total;
+    int bufA, bufB, splitfrac, k1, k2, dk1, dk2, kg, splitpos, colA, colB, total;
 };
 __host__ __device__ inline WarpOff warp_off(int ncol) {
     WarpOff w;
@@ -180,7 +179,6 @@ __host__ __device__ inline WarpOff warp_off(int ncol) {
     w.dk1 = o; o += 4 * kMaxNg;
     w.dk2 = o; o += 4 * kMaxNg;
     w.kg = o; o += 4 * kMaxNg;
-    w.normf = o; o += 4 * kMaxNg;
     w.splitpos = o; o += 4 * kMaxNg;
     w.colA = o; o += 4 * kMaxNg * nc;
     w.colB = o; o += 4 * kMaxNg * nc;
@@ -739,7 +737,7 @@ struct PassCtx {
 struct WarpPtr {
     unsigned long long *bufA, *bufB;
     const short* mtab;       // lanes' merge output ranges (merge_lane_start), per CTA
-    float *k1, *k2, *dk1, *dk2, *kg, *normf;
+    float *k1, *k2, *dk1, *dk2, *kg;
     double* splitfrac;
     int* splitpos;
 };
@@ -898,28 +896,13 @@ __device__ __forceinline__ float elem_grad(const PassCtx& P, int gcol, int c, in
 // Gradient columns of one sorted pass.  They feed the Jacobian alone (never a
 // sort key), so they need not follow the reference's summation order.  Every
 // column is v_c(i, j) = U[i][c] + V[j][c] (T: dk1(i)[a1] + dk2(j) a2; earlier
-// gas: u(i); added gas: k2(j)).  Bin b of column c is the sum over its sorted
-// positions of w * v_c (split elements shared f : 1 - f), divided by the
-// bin's normalisation.  Each lane sums its chunk of positions; at a split it
-// writes the closing bin's partial to Eb[b] (one lane holds each split) and
-// restarts; its chunk-end partial goes to Lp with its bin in BL.  One lane
-// per bin then adds Eb[b] and the chunk-end partials of the lanes between
-// the bin's two boundaries that belong to it, in lane order (deterministic,
-// no atomics).  cmap[0..nz): the columns computed (slot k holds column
-// cmap[k]); every other column is zero in this pass.  NCV: the slots computed
-// per element (4, 5 or 8, at least nz).  scratch: the free element buffer
-// (kGradScratch bytes).
-template <int NCV>
-__device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
-                                             const unsigned long long* A, void* scratch, const float* wtab,
-                                             const float* colP, float* colN, const int (&cmap)[kMaxCols], int nz,
-                                             int ng, int nloop, int c_last, int p0, int p1, int ch, int lane) {
-    const int ncol = P.ncol;
-    float4* UV = (float4*)scratch;             // U rows [ng][3 float4], then V rows [ng][3 float4]
-                                               // (8 values and a pad: rows 48 B apart spread over the banks)
-    float* Eb = (float*)(UV + 6 * ng);         // [ng][8] partial of bin b up to its closing split
-    float4* Lp = (float4*)(Eb + 8 * ng);       // [32][2] chunk-end partial of each lane
-    short* BL = (short*)(Lp + 2 * 32);         // [32] its bin (-1: empty chunk)
+// gas: u(i); added gas: k2(j)).  column_tables writes U and V for the columns
+// a pass can make non-zero (cmap[0..nz): slot k holds column cmap[k]; a
+// column of a gas not yet added is zero and not computed): rows of 8 values
+// and a pad (48 B apart, spread over the banks), U rows then V rows.
+__device__ __forceinline__ void column_tables(const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
+                                              const float* colP, float4* UV, const int (&cmap)[kMaxCols], int nz,
+                                              int ng, int lane) {
     if (lane < ng) {
         const int x = lane;
         float u[kMaxCols], v[kMaxCols];
@@ -946,93 +929,94 @@ __device__ __forceinline__ void grad_columns(const SpecDev& S, const PassCtx& P,
         UV[3 * ng + 3 * x] = make_float4(v[0], v[1], v[2], v[3]);
         UV[3 * ng + 3 * x + 1] = make_float4(v[4], v[5], v[6], v[7]);
     }
-    __syncwarp();
-    int b = 0;
-    {
-        int lo = 0, hi = c_last;                // first boundary at or after p0
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (wp.splitpos[mid] < p0) lo = mid + 1; else hi = mid;
-        }
-        b = lo;
-    }
-    int nsp = b < c_last ? wp.splitpos[b] : nloop;
-    float acc[NCV];
+}
+
+// k(g) and the gradient columns of one sorted pass, one lane per bin
+// (rankg.f:118-146).  k: the split remainder, the whole elements and the
+// split fraction, then / sngl(sum), every operation rounded as in the
+// reference.  The gradient columns take the same walk: bin b of column c is
+// the sum of share * w * v_c over the bin's elements (split elements shared
+// f : 1 - f), divided by the same normalisation.  NCV: the slots computed per
+// element (4, 5 or 8, at least nz).
+template <int NCV>
+__device__ __forceinline__ void bins_and_columns(const PassCtx& P, const WarpPtr& wp, const unsigned long long* A,
+                                                 const float4* UV, const float* wtab, float* colN,
+                                                 const int (&cmap)[kMaxCols], int nz, int ng, int nloop,
+                                                 int c_last, int lane) {
+    if (lane >= ng) return;
+    const int bb = lane;
+    float acc = 0.0f, nf = 0.0f;            // nf == 0: bin never reached
+    float gc[NCV];
 #pragma unroll
-    for (int c = 0; c < NCV; ++c) acc[c] = 0.0f;
-#pragma unroll 1
-    for (int p = p0; p < p1; ++p) {
-        const unsigned q = (unsigned)A[p] & 0xffffu;
+    for (int c = 0; c < NCV; ++c) gc[c] = 0.0f;
+    auto add_columns = [&](unsigned q, float sw) {   // sw: share x weight of element q
         const int i = q >> 5, j = q & 31;
-        const float w = wtab[q];
         float uu[8], vv[8];
-        {
-            const float4 u0 = UV[3 * i], v0 = UV[3 * ng + 3 * j];
-            uu[0] = u0.x; uu[1] = u0.y; uu[2] = u0.z; uu[3] = u0.w;
-            vv[0] = v0.x; vv[1] = v0.y; vv[2] = v0.z; vv[3] = v0.w;
-            if (NCV == 5) {
-                uu[4] = ((const float*)(UV + 3 * i + 1))[0];
-                vv[4] = ((const float*)(UV + 3 * ng + 3 * j + 1))[0];
-            } else if (NCV == 8) {
-                const float4 u1 = UV[3 * i + 1], v1 = UV[3 * ng + 3 * j + 1];
-                uu[4] = u1.x; uu[5] = u1.y; uu[6] = u1.z; uu[7] = u1.w;
-                vv[4] = v1.x; vv[5] = v1.y; vv[6] = v1.z; vv[7] = v1.w;
-            }
+        const float4 u0 = UV[3 * i], v0 = UV[3 * ng + 3 * j];
+        uu[0] = u0.x; uu[1] = u0.y; uu[2] = u0.z; uu[3] = u0.w;
+        vv[0] = v0.x; vv[1] = v0.y; vv[2] = v0.z; vv[3] = v0.w;
+        if (NCV == 5) {
+            uu[4] = ((const float*)(UV + 3 * i + 1))[0];
+            vv[4] = ((const float*)(UV + 3 * ng + 3 * j + 1))[0];
+        } else if (NCV == 8) {
+            const float4 u1 = UV[3 * i + 1], v1 = UV[3 * ng + 3 * j + 1];
+            uu[4] = u1.x; uu[5] = u1.y; uu[6] = u1.z; uu[7] = u1.w;
+            vv[4] = v1.x; vv[5] = v1.y; vv[6] = v1.z; vv[7] = v1.w;
         }
-        float val[NCV];
 #pragma unroll
-        for (int c = 0; c < NCV; ++c) val[c] = w * (uu[c] + vv[c]);
-        if (p == nsp) {
-            const float f = (float)wp.splitfrac[b];
-#pragma unroll
-            for (int c = 0; c < NCV; ++c) {
-                Eb[b * 8 + c] = fmaf(f, val[c], acc[c]);
-                acc[c] = (1.0f - f) * val[c];
-            }
-            ++b;
-            nsp = b < c_last ? wp.splitpos[b] : nloop;
-        } else {
-#pragma unroll
-            for (int c = 0; c < NCV; ++c) acc[c] += val[c];
+        for (int c = 0; c < NCV; ++c) gc[c] = fmaf(sw, uu[c] + vv[c], gc[c]);
+    };
+    if (bb <= c_last) {
+        double sum = 0.0;
+        int p = 0;
+        if (bb > 0) {
+            const int s = wp.splitpos[bb - 1];
+            const double frac = wp.splitfrac[bb - 1];
+            const unsigned long long word = A[s];
+            const unsigned q = (unsigned)word & 0xffffu;
+            const float w = wtab[q];
+            const float sr = __double2float_rn(__dsub_rn(1.0, frac));
+            acc = __fmul_rn(__fmul_rn(sr, funkey((unsigned)(word >> 32))), w);
+            sum = __dmul_rn(__dsub_rn(1.0, frac), (double)w);
+            add_columns(q, __fmul_rn(sr, w));
+            p = s + 1;
         }
-    }
-    {
-        float a8[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) a8[c] = c < NCV ? acc[c < NCV ? c : 0] : 0.0f;
-        Lp[2 * lane] = make_float4(a8[0], a8[1], a8[2], a8[3]);
-        Lp[2 * lane + 1] = make_float4(a8[4], a8[5], a8[6], a8[7]);
-    }
-    BL[lane] = (short)(p0 < p1 ? b : -1);
-    __syncwarp();
-    if (lane < ng) {
-        const int bb = lane;
-        const float nf = wp.normf[bb];
-        float tot[NCV];
-#pragma unroll
-        for (int c = 0; c < NCV; ++c) tot[c] = 0.0f;
-        if (nf != 0.0f && bb <= c_last) {
-            const int Lfrom = bb == 0 ? 0 : wp.splitpos[bb - 1] / ch;
-            const int Lto = bb < c_last ? wp.splitpos[bb] / ch : (nloop - 1) / ch;
+        const bool closes = bb < c_last;
+        const int pend = closes ? wp.splitpos[bb] : nloop;
 #pragma unroll 1
-            for (int L = Lfrom; L <= Lto; ++L)
-                if (BL[L] == bb) {
-                    const float* src = (const float*)(Lp + 2 * L);
-#pragma unroll
-                    for (int c = 0; c < NCV; ++c) tot[c] += src[c];
-                }
-            if (bb < c_last) {
-#pragma unroll
-                for (int c = 0; c < NCV; ++c) tot[c] += Eb[bb * 8 + c];
-            }
+        for (; p < pend; ++p) {
+            const unsigned long long word = A[p];
+            const unsigned q = (unsigned)word & 0xffffu;
+            const float w = wtab[q];
+            acc = __fadd_rn(acc, __fmul_rn(funkey((unsigned)(word >> 32)), w));
+            sum = __dadd_rn(sum, (double)w);
+            add_columns(q, w);
         }
-#pragma unroll
-        for (int c = 0; c < kMaxCols; ++c)
-            if (c < ncol) colN[c * kMaxNg + bb] = 0.0f;
-#pragma unroll
-        for (int k = 0; k < NCV; ++k)
-            if (k < nz) colN[cmap[k] * kMaxNg + bb] = nf != 0.0f ? tot[k] / nf : 0.0f;
+        nf = 1.0f;
+        if (closes) {
+            const int s = wp.splitpos[bb];
+            const double frac = wp.splitfrac[bb];
+            const unsigned long long word = A[s];
+            const unsigned q = (unsigned)word & 0xffffu;
+            const float w = wtab[q];
+            const float sf = __double2float_rn(frac);
+            acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(sf, funkey((unsigned)(word >> 32))), w));
+            sum = __dadd_rn(sum, __dmul_rn(frac, (double)w));
+            add_columns(q, __fmul_rn(sf, w));
+            nf = __double2float_rn(sum);
+            acc = __fdiv_rn(acc, nf);
+        } else if (bb == ng - 1) {
+            nf = __double2float_rn(sum);
+            acc = __fdiv_rn(acc, nf);
+        }
     }
+    wp.kg[bb] = acc;
+#pragma unroll
+    for (int c = 0; c < kMaxCols; ++c)
+        if (c < P.ncol) colN[c * kMaxNg + bb] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < NCV; ++k)
+        if (k < nz) colN[cmap[k] * kMaxNg + bb] = nf != 0.0f ? gc[k] / nf : 0.0f;
 }
 
 template <int NGC>
@@ -1267,61 +1251,10 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         return;
     }
 
-    // ---- k(g): one lane per bin (rankg.f:118-146) -------------------------
-    // split remainder, whole elements, split fraction, then / sngl(sum), every
-    // operation rounded as in the reference; the divisor is kept for the
-    // gradient columns.
-    if (lane < ng) {
-        const int bb = lane;
-        float acc = 0.0f, nf = 0.0f;        // nf == 0: bin never reached
-        if (bb <= c_last) {
-            double sum = 0.0;
-            int p = 0;
-            if (bb > 0) {
-                const int s = wp.splitpos[bb - 1];
-                const double frac = wp.splitfrac[bb - 1];
-                const unsigned long long word = A[s];
-                const unsigned q = (unsigned)word & 0xffffu;
-                const float w = wtab[q];
-                const float sr = __double2float_rn(__dsub_rn(1.0, frac));
-                acc = __fmul_rn(__fmul_rn(sr, funkey((unsigned)(word >> 32))), w);
-                sum = __dmul_rn(__dsub_rn(1.0, frac), (double)w);
-                p = s + 1;
-            }
-            const bool closes = bb < c_last;
-            const int pend = closes ? wp.splitpos[bb] : nloop;
-#pragma unroll 1
-            for (; p < pend; ++p) {
-                const unsigned long long word = A[p];
-                const unsigned q = (unsigned)word & 0xffffu;
-                const float w = wtab[q];
-                acc = __fadd_rn(acc, __fmul_rn(funkey((unsigned)(word >> 32)), w));
-                sum = __dadd_rn(sum, (double)w);
-            }
-            nf = 1.0f;
-            if (closes) {
-                const int s = wp.splitpos[bb];
-                const double frac = wp.splitfrac[bb];
-                const unsigned long long word = A[s];
-                const unsigned q = (unsigned)word & 0xffffu;
-                const float w = wtab[q];
-                const float sf = __double2float_rn(frac);
-                acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(sf, funkey((unsigned)(word >> 32))), w));
-                sum = __dadd_rn(sum, __dmul_rn(frac, (double)w));
-                nf = __double2float_rn(sum);
-                acc = __fdiv_rn(acc, nf);
-            } else if (bb == ng - 1) {
-                nf = __double2float_rn(sum);
-                acc = __fdiv_rn(acc, nf);
-            }
-        }
-        wp.kg[bb] = acc;
-        wp.normf[bb] = nf;
-    }
-    // ---- gradient columns ----------------------------------------------------
+    // ---- k(g) and gradient columns -------------------------------------------
     // A column of a gas not yet added (gas index above igas) is zero in this
     // pass; the others are computed, their arithmetic specialised on how many
-    // there are
+    // there are.  Their tables go to the free buffer (the prefix is done with).
     int cmap[kMaxCols], nz = 0;
 #pragma unroll
     for (int c = 0; c < kMaxCols; ++c) {
@@ -1331,9 +1264,13 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             if (g == S.ngas || g <= P.igas) cmap[nz++] = c;
         }
     }
-    if (nz <= 4) grad_columns<4>(S, P, wp, A, gd, wtab, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
-    else if (nz == 5) grad_columns<5>(S, P, wp, A, gd, wtab, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
-    else grad_columns<8>(S, P, wp, A, gd, wtab, colP, colN, cmap, nz, ng, nloop, c_last, p0, p1, ch, lane);
+    float4* UV = (float4*)gd;
+    __syncwarp();
+    column_tables(S, P, wp, colP, UV, cmap, nz, ng, lane);
+    __syncwarp();
+    if (nz <= 4) bins_and_columns<4>(P, wp, A, UV, wtab, colN, cmap, nz, ng, nloop, c_last, lane);
+    else if (nz == 5) bins_and_columns<5>(P, wp, A, UV, wtab, colN, cmap, nz, ng, nloop, c_last, lane);
+    else bins_and_columns<8>(P, wp, A, UV, wtab, colN, cmap, nz, ng, nloop, c_last, lane);
     __syncwarp();
 }
 
@@ -1402,7 +1339,6 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
     wp.dk1 = (float*)(wsm + wo.dk1);
     wp.dk2 = (float*)(wsm + wo.dk2);
     wp.kg = (float*)(wsm + wo.kg);
-    wp.normf = (float*)(wsm + wo.normf);
     wp.splitfrac = (double*)(wsm + wo.splitfrac);
     wp.splitpos = (int*)(wsm + wo.splitpos);
     float* colA = (float*)(wsm + wo.colA);

@@ -215,7 +215,7 @@ __host__ __device__ inline Layout make_layout(int ng, int nsw, int ncol, int nlm
     int o = 0;
     Lo.off_gord = o; o += 8 * (kMaxNg + 3);
     Lo.off_delg = o; o += 4 * kMaxNg;
-    Lo.off_wtab = o; o += 4 * 32 * kNgDev;       // element weights by (i << 5 | j)
+    Lo.off_wtab = o; o += 4 * 33 * kNgDev;       // element weights w(i, j) at 33 i + j (rows spread over the banks)
     Lo.off_mtab = o; o += 2 * kMergeLevels * 33;  // lanes' merge ranges
     o = align16(o);
     Lo.off_region = o;
@@ -974,7 +974,7 @@ __device__ __forceinline__ void bins_and_columns(const PassCtx& P, const WarpPtr
             const double frac = wp.splitfrac[bb - 1];
             const unsigned long long word = A[s];
             const unsigned q = (unsigned)word & 0xffffu;
-            const float w = wtab[q];
+            const float w = wtab[q + (q >> 5)];
             const float sr = __double2float_rn(__dsub_rn(1.0, frac));
             acc = __fmul_rn(__fmul_rn(sr, funkey((unsigned)(word >> 32))), w);
             sum = __dmul_rn(__dsub_rn(1.0, frac), (double)w);
@@ -987,7 +987,7 @@ __device__ __forceinline__ void bins_and_columns(const PassCtx& P, const WarpPtr
         for (; p < pend; ++p) {
             const unsigned long long word = A[p];
             const unsigned q = (unsigned)word & 0xffffu;
-            const float w = wtab[q];
+            const float w = wtab[q + (q >> 5)];
             acc = __fadd_rn(acc, __fmul_rn(funkey((unsigned)(word >> 32)), w));
             sum = __dadd_rn(sum, (double)w);
             add_columns(q, w);
@@ -998,7 +998,7 @@ __device__ __forceinline__ void bins_and_columns(const PassCtx& P, const WarpPtr
             const double frac = wp.splitfrac[bb];
             const unsigned long long word = A[s];
             const unsigned q = (unsigned)word & 0xffffu;
-            const float w = wtab[q];
+            const float w = wtab[q + (q >> 5)];
             const float sf = __double2float_rn(frac);
             acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(sf, funkey((unsigned)(word >> 32))), w));
             sum = __dadd_rn(sum, __dmul_rn(frac, (double)w));
@@ -1117,7 +1117,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
             const unsigned long long word = A[p];
             const unsigned q = (unsigned)word & 0xffffu;
             const unsigned kb = (unsigned)(word >> 32);
-            run = __dadd_rn(run, (double)wtab[q]);
+            run = __dadd_rn(run, (double)wtab[q + (q >> 5)]);
             gd[p] = run;
             anytie |= (p >= 1 && kb == kbp);         // fkey folds -0 onto +0
             kbp = kb;
@@ -1159,7 +1159,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
                 const unsigned kb = (unsigned)(word >> 32);
                 const double gprev = sp > c0 ? __dadd_rn(gd[sp - 1], bL) : bL;
                 wp.splitpos[lane] = sp;
-                wp.splitfrac[lane] = __ddiv_rn(__dsub_rn(gb, gprev), (double)wtab[q]);
+                wp.splitfrac[lane] = __ddiv_rn(__dsub_rn(gb, gprev), (double)wtab[q + (q >> 5)]);
                 const bool tl = sp >= 1 && kb == (unsigned)(A[sp - 1] >> 32);
                 const bool tr = sp + 1 < nloop && kb == (unsigned)(A[sp + 1] >> 32);
                 risky = tl || tr;
@@ -1208,7 +1208,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
                 const unsigned q = (unsigned)word & 0xffffu;
                 const int i = q >> 5, j = q & 31;
                 const float cval = funkey((unsigned)(word >> 32));
-                const float w = wtab[q];
+                const float w = wtab[q + (q >> 5)];
                 const double gcur = __dadd_rn(gprev, (double)w);
                 if (ig >= ng) { atomicOr(B.status, kStGord); break; }
                 if (gcur < g_ord[ig + 1]) {
@@ -1311,7 +1311,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
     const PathOff po = path_off(nlmax_max, B.ng, nsw_max);
     double* g_ord = (double*)(smem + Lo.off_gord);
     float* delg = (float*)(smem + Lo.off_delg);
-    float* wtab = (float*)(smem + Lo.off_wtab);   // w(i, j) = delg(i) delg(j), the overlap's element weights
+    float* wtab = (float*)(smem + Lo.off_wtab);   // w(i, j) = delg(i) delg(j) at 33 i + j: the overlap's element weights, read with q + (q >> 5) for q = i << 5 | j
     char* region = smem + Lo.off_region;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ng = NGC ? NGC : B.ng;   // NGC > 0: the instance for NG = NGC (== B.ng)
@@ -1322,7 +1322,7 @@ fwd_kernel(BatchDev B, int nsw_max, int ncol_max, int nlmax_max, int npath_max) 
     for (int i = tid; i < ng; i += kThreads) delg[i] = B.delg[i];
     for (int q = tid; q < ng * 32; q += kThreads) {
         const int j = q & 31;
-        wtab[q] = j < ng ? __fmul_rn(B.delg[q >> 5], B.delg[j]) : 0.0f;
+        wtab[q + (q >> 5)] = j < ng ? __fmul_rn(B.delg[q >> 5], B.delg[j]) : 0.0f;
     }
     short* mtab = (short*)(smem + Lo.off_mtab);
     for (int i = tid; i < kMergeLevels * 33; i += kThreads) mtab[i] = (short)merge_lane_start(ng, i / 33, i % 33);

@@ -848,6 +848,7 @@ __device__ int merge_rows(const WarpPtr& wp, const short* mtab, int ng_run, int 
         const int abase = 2 * p * sin + 1, bbase = ny > 0 ? abase + sin : abase + m + 2;
         const int obase = p * sout + 1 - ms;
         if (copy) {
+#pragma unroll 1
             for (int k = s; k < e; ++k) {
                 const int o = k - ms;
                 ko[obase + k] = ki[o < m ? abase + o : bbase + (o - m)];
@@ -1043,6 +1044,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         bool finite = true;                         // no NaN key
         {
             int i = lane / ng, j = lane - (lane / ng) * ng;
+#pragma unroll 1
             for (int e = lane; e < nloop; e += 32) {
                 const float kv = key_of(P, wp, i, j);
                 finite = finite && kv == kv;
@@ -1088,6 +1090,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     auto heapsort_pass = [&]() {
         __syncwarp();
         unsigned long long* Aw = (A >= wp.bufB) ? wp.bufB : wp.bufA;
+#pragma unroll 1
         for (int e = lane; e < nloop; e += 32) {
             const int i = e / ng, j = e - i * ng;
             Aw[e] = ((unsigned long long)__float_as_uint(key_of(P, wp, i, j)) << 32) | (unsigned)e;
@@ -1095,6 +1098,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         __syncwarp();
         if (lane == 0) heapsort_words(nloop, Aw);
         __syncwarp();
+#pragma unroll 1
         for (int p = lane; p < nloop; p += 32) {
             const unsigned long long w = Aw[p];
             const int e = (int)(unsigned)w;
@@ -1113,6 +1117,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         double run = 0.0;
         unsigned kbp = p0 >= 1 && p0 < p1 ? (unsigned)(A[p0 - 1] >> 32) : 0u;
         bool anytie = false;
+#pragma unroll 1
         for (int p = p0; p < p1; ++p) {
             const unsigned long long word = A[p];
             const unsigned q = (unsigned)word & 0xffffu;
@@ -1185,6 +1190,7 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     if (gerr) atomicOr(B.status, kStGord);
     __syncwarp();
     if (dbg_perm) {
+#pragma unroll 1
         for (int p = lane; p < nloop; p += 32) {
             const unsigned q = (unsigned)A[p] & 0xffffu;
             dbg_perm[p] = (int16_t)((q >> 5) * ng + (q & 31));
@@ -1197,12 +1203,14 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
         // sequential rankg walk (rankg.f:118-152) by lane 0
         dg.irregular += (lane == 0);
         if (lane == 0) {
+#pragma unroll 1
             for (int bb = 0; bb < ng; ++bb) {
                 wp.kg[bb] = 0.0f;
                 for (int c = 0; c < ncol; ++c) colN[c * kMaxNg + bb] = 0.0f;
             }
             int ig = 0;
             double sum = 0.0, gprev = 0.0;
+#pragma unroll 1
             for (int p = 0; p < nloop; ++p) {
                 const unsigned long long word = A[p];
                 const unsigned q = (unsigned)word & 0xffffu;

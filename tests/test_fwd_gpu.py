@@ -67,6 +67,35 @@ def test_config2_small_bins_bit_exact(ctx, oracle, strict):
     assert jac_err(g, g64, job.nv) <= JAC_TOL
 
 
+@pytest.mark.parametrize("ng", [2, 5, 10, 13, 21, 22])
+def test_other_ng_bins_bit_exact_every_tile(ctx, oracle, ng):
+    """NG other than 20 runs the generic kernel instance: merge levels with an
+    unpaired last run (odd NG), a last level shorter than its pair, the
+    largest NG; g-bins identical to the mixed oracle under every tile."""
+    kt = synth.make_ktables(synth.ABSORBERS_C2, np_=20, nt=15, ng=ng, vmin=600.0, delv=0.4, nbin=8, seed=70 + ng)
+    job = synth.make_job(kt, synth.ABSORBERS_C2, nlayer=40, seed=71 + ng, nwave=8, vmr_perturb=0.3)
+    cia = synth.make_cia(70 + ng)
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    (c0, g0, gt0), (operm, osplit, oties) = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED, debug=True)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    a_orc = assignment(operm, osplit, kt.ng)
+    ctx.set_debug(True)
+    try:
+        for tile in (8, 4, 2):
+            ctx.set_tile(tile)
+            c, g, gt = ctx.cirsrtfg_wave(job)
+            perm, split = ctx.debug_bins(job)
+            assert ctx.stats()["sort_passes"] == int((operm[..., 0] >= 0).sum())
+            assert np.array_equal(assignment(perm, split, kt.ng), a_orc)
+            assert np.array_equal(split, osplit)
+            assert rad_err(c, c64) <= RAD_TOL
+            assert jac_err(g, g64, job.nv) <= JAC_TOL
+    finally:
+        ctx.set_debug(False)
+        ctx.set_tile(0)
+
+
 def test_config2_golden_fixture(ctx):
     kt, cia, job = synth.config2(nwave=8, nlayer=30, nbin=8)
     c, g, gt = _run(ctx, kt, cia, job)

@@ -96,6 +96,32 @@ def test_other_ng_bins_bit_exact_every_tile(ctx, oracle, ng):
         ctx.set_tile(0)
 
 
+def test_k_distribution_not_monotone_in_g_takes_the_reference_heapsort(ctx, oracle):
+    """A table whose k values are not sorted in g (the g axis of one gas
+    permuted): its rows are not sorted, so those passes skip the merge and take
+    the reference heapsort in-kernel; the whole sorted order is the oracle's."""
+    kt, cia, job = synth.config2(nwave=8, nlayer=40, nbin=8)
+    perm_g = np.random.default_rng(5).permutation(kt.ng)
+    t = kt.table(1)                      # C2H6
+    t[...] = t[..., perm_g]
+    ctx.set_ktables(kt)
+    ctx.set_cia(cia)
+    ctx.set_debug(True)
+    try:
+        c, g, gt = ctx.cirsrtfg_wave(job)
+        perm, split = ctx.debug_bins(job)
+        st = ctx.stats()
+    finally:
+        ctx.set_debug(False)
+    (c0, g0, gt0), (operm, osplit, oties) = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_MIXED, debug=True)
+    assert st["exact_passes"] > 0
+    assert np.array_equal(assignment(perm, split, kt.ng), assignment(operm, osplit, kt.ng))
+    assert np.array_equal(split, osplit)
+    c64, g64, _ = oracle.cirsrtfg_wave(kt, cia, job, oracle.ORC_FP64)
+    assert rad_err(c, c64) <= RAD_TOL
+    assert jac_err(g, g64, job.nv) <= JAC_TOL
+
+
 def test_config2_golden_fixture(ctx):
     kt, cia, job = synth.config2(nwave=8, nlayer=30, nbin=8)
     c, g, gt = _run(ctx, kt, cia, job)

@@ -898,37 +898,37 @@ __device__ __forceinline__ float elem_grad(const PassCtx& P, int gcol, int c, in
 // sort key), so they need not follow the reference's summation order.  Every
 // column is v_c(i, j) = U[i][c] + V[j][c] (T: dk1(i)[a1] + dk2(j) a2; earlier
 // gas: u(i); added gas: k2(j)).  column_tables writes U and V for the columns
-// a pass can make non-zero (cmap[0..nz): slot k holds column cmap[k]; a
-// column of a gas not yet added is zero and not computed): rows of 8 values
-// and a pad (48 B apart, spread over the banks), U rows then V rows.
+// a pass can make non-zero (slots 0..nz-1: slot k holds column
+// (cm >> 3k) & 7; a column of a gas not yet added is zero and not computed):
+// rows of 8 values and a pad (48 B apart, spread over the banks), U rows then
+// V rows.  One slot per iteration, kept rolled (the kernel is bound by its
+// instruction cache).
 __device__ __forceinline__ void column_tables(const SpecDev& S, const PassCtx& P, const WarpPtr& wp,
-                                              const float* colP, float4* UV, const int (&cmap)[kMaxCols], int nz,
+                                              const float* colP, float4* UV, unsigned cm, int nz,
                                               int ng, int lane) {
     if (lane < ng) {
         const int x = lane;
-        float u[kMaxCols], v[kMaxCols];
-#pragma unroll
+        float* Ur = (float*)(UV + 3 * x);
+        float* Vr = (float*)(UV + 3 * ng + 3 * x);
+#pragma unroll 1
         for (int k = 0; k < kMaxCols; ++k) {
-            u[k] = 0.0f;
-            v[k] = 0.0f;
+            float u = 0.0f, v = 0.0f;
             if (k < nz) {
-                const int c = cmap[k];
+                const int c = (cm >> (3 * k)) & 7;
                 const int gcol = S.col_gas[c];
-                if (gcol == S.ngas) {                  // temperature: dk1(i)[*a1] + dk2(j)*a2
-                    u[k] = P.first ? wp.dk1[x] * P.a1 : wp.dk1[x];
-                    v[k] = wp.dk2[x] * P.a2;
-                } else if (gcol == P.igas) {           // the gas being added: k2(j)
-                    v[k] = wp.k2[x];
-                } else if (gcol < P.igas) {            // an earlier gas
-                    if (!P.first) u[k] = colP[c * kMaxNg + x];
-                    else if (gcol == 0) u[k] = wp.k1[x];
+                if (gcol == S.ngas) {
+                    u = P.first ? wp.dk1[x] * P.a1 : wp.dk1[x];
+                    v = wp.dk2[x] * P.a2;
+                } else if (gcol == P.igas) {
+                    v = wp.k2[x];
+                } else if (gcol < P.igas) {
+                    if (!P.first) u = colP[c * kMaxNg + x];
+                    else if (gcol == 0) u = wp.k1[x];
                 }
             }
+            Ur[k] = u;
+            Vr[k] = v;
         }
-        UV[3 * x] = make_float4(u[0], u[1], u[2], u[3]);
-        UV[3 * x + 1] = make_float4(u[4], u[5], u[6], u[7]);
-        UV[3 * ng + 3 * x] = make_float4(v[0], v[1], v[2], v[3]);
-        UV[3 * ng + 3 * x + 1] = make_float4(v[4], v[5], v[6], v[7]);
     }
 }
 
@@ -942,7 +942,7 @@ __device__ __forceinline__ void column_tables(const SpecDev& S, const PassCtx& P
 template <int NCV>
 __device__ __forceinline__ void bins_and_columns(const PassCtx& P, const WarpPtr& wp, const unsigned long long* A,
                                                  const float4* UV, const float* wtab, float* colN,
-                                                 const int (&cmap)[kMaxCols], int nz, int ng, int nloop,
+                                                 unsigned cm, int nz, int ng, int nloop,
                                                  int c_last, int lane) {
     if (lane >= ng) return;
     const int bb = lane;
@@ -1017,7 +1017,7 @@ __device__ __forceinline__ void bins_and_columns(const PassCtx& P, const WarpPtr
         if (c < P.ncol) colN[c * kMaxNg + bb] = 0.0f;
 #pragma unroll
     for (int k = 0; k < NCV; ++k)
-        if (k < nz) colN[cmap[k] * kMaxNg + bb] = nf != 0.0f ? gc[k] / nf : 0.0f;
+        if (k < nz) colN[((cm >> (3 * k)) & 7) * kMaxNg + bb] = nf != 0.0f ? gc[k] / nf : 0.0f;
 }
 
 template <int NGC>
@@ -1263,22 +1263,25 @@ __device__ void sort_pass(const BatchDev& B, const SpecDev& S, const PassCtx& P,
     // A column of a gas not yet added (gas index above igas) is zero in this
     // pass; the others are computed, their arithmetic specialised on how many
     // there are.  Their tables go to the free buffer (the prefix is done with).
-    int cmap[kMaxCols], nz = 0;
+    unsigned cm = 0;                            // slot k holds column (cm >> 3k) & 7
+    int nz = 0;
 #pragma unroll
     for (int c = 0; c < kMaxCols; ++c) {
-        cmap[c] = 0;
         if (c < P.ncol) {
             const int g = S.col_gas[c];
-            if (g == S.ngas || g <= P.igas) cmap[nz++] = c;
+            if (g == S.ngas || g <= P.igas) {
+                cm |= (unsigned)c << (3 * nz);
+                ++nz;
+            }
         }
     }
     float4* UV = (float4*)gd;
     __syncwarp();
-    column_tables(S, P, wp, colP, UV, cmap, nz, ng, lane);
+    column_tables(S, P, wp, colP, UV, cm, nz, ng, lane);
     __syncwarp();
-    if (nz <= 4) bins_and_columns<4>(P, wp, A, UV, wtab, colN, cmap, nz, ng, nloop, c_last, lane);
-    else if (nz == 5) bins_and_columns<5>(P, wp, A, UV, wtab, colN, cmap, nz, ng, nloop, c_last, lane);
-    else bins_and_columns<8>(P, wp, A, UV, wtab, colN, cmap, nz, ng, nloop, c_last, lane);
+    if (nz <= 4) bins_and_columns<4>(P, wp, A, UV, wtab, colN, cm, nz, ng, nloop, c_last, lane);
+    else if (nz == 5) bins_and_columns<5>(P, wp, A, UV, wtab, colN, cm, nz, ng, nloop, c_last, lane);
+    else bins_and_columns<8>(P, wp, A, UV, wtab, colN, cm, nz, ng, nloop, c_last, lane);
     __syncwarp();
 }
 
